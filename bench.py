@@ -1,0 +1,429 @@
+#!/usr/bin/env python
+"""Benchmark of the LBVH microbench (1,048,576 triangles, 4,194,304 rays, seed 7).
+
+One step = build the triangle LBVH, trace 4,194,304 closest-hit rays, refit after
+vertex jitter, build the LBVH over 1,048,576 query boxes and run the cross overlap
+query.  Metric: Mrays/s of the whole step (rays / step time); the per-phase times,
+LBVH Mtri/s and traversal Mrays/s are reported beside it.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl lux|reference]
+
+N > 1 runs under torchrun: every rank runs an independent replica (the build is a
+global sort, so ranks share nothing) and value = all ranks' rays / max rank time.
+--impl reference times the reference's own CPU code (oracle/_ref) on bounded samples.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+from lux_b200 import workloads as W  # noqa: E402
+
+N_TRIS = 1 << 20
+N_RAYS = 1 << 22
+N_QUERIES = 1 << 20
+SEED = 7
+WORKLOAD = ("LBVH microbench: 1,048,576 soup triangles (lognormal edges, median 2e-3), "
+            "4,194,304 uniform rays, refit after N(0,1e-4) jitter, 1,048,576 query boxes "
+            "(half extent 1e-3), seed 7")
+METRIC = "Mrays/s"
+# Algorithmic bytes (per unit) used for the roofline: build 120 B/tri, refit 104 B/tri,
+# traversal 32 B ray + 8 B hit + 32 B per box test + 36 B per triangle test.
+BUILD_BYTES_PER_TRI = 120
+REFIT_BYTES_PER_TRI = 104
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle sampling during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.QUERY}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except (FileNotFoundError, OSError):
+            self.proc = None
+        time.sleep(0.15)
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.15)
+        self.proc.terminate()
+        self.proc.wait()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        with open(self.path) as f:
+            for line in f:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) < 9:
+                    continue
+                try:
+                    sm.append(float(parts[1]))
+                    smax.append(float(parts[2]))
+                except ValueError:
+                    continue
+                for name, flag in zip(names, parts[5:9]):
+                    if flag.lower() == "active":
+                        reasons.add(name)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ------------------------------------------------------------------ reference CPU arm
+
+def reference_step_estimate(data: dict, ray_sample: int, threads: int) -> dict:
+    """Times the reference's own host code (oracle/_ref) on bounded samples of the step.
+
+    Build: build_cpu_lbvh_tree over all 1,048,576 triangles (the reference builder is
+    single threaded).  Trace: intersect_cpu_bvh_tree on `ray_sample` rays over all host
+    threads, scaled to 4,194,304.  Refit: the reference refit re-runs its whole layout
+    (bvh/gpu_bvh.cu:597-613); on the host that is a rebuild, timed as one.  Query build
+    + overlap: a second build over the query boxes plus the oracle port's overlap
+    traversal over a sample of queries, scaled.
+    """
+    from oracle.bindings import Oracle, Ref
+
+    ref = Ref()
+    tris = data["triangles"]
+    rays = data["rays"][:ray_sample]
+    t0 = time.perf_counter()
+    tree = ref.tree_create(tris)
+    t_build = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    ref.tree_trace(tree, rays, threads=threads)
+    t_trace = (time.perf_counter() - t0) * (N_RAYS / len(rays))
+    ref.tree_destroy(tree)
+    t0 = time.perf_counter()
+    ref.tree_destroy(ref.tree_create(data["refit_triangles"]))
+    t_refit = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    ref.tree_destroy(ref.tree_create(data["queries"], kind=1))
+    t_qbuild = time.perf_counter() - t0
+    ora = Oracle()
+    tree = ora.build(ora.triangle_bounds(data["refit_triangles"]))
+    qs = data["queries"][: N_QUERIES // 16]
+    t0 = time.perf_counter()
+    ora.overlap(tree, qs, self_pairs=False, max_pairs=1 << 22)
+    t_overlap = (time.perf_counter() - t0) * 16
+    total = t_build + t_trace + t_refit + t_qbuild + t_overlap
+    return {"step_s": total, "build_s": t_build, "trace_s": t_trace, "refit_s": t_refit,
+            "query_build_s": t_qbuild, "overlap_s": t_overlap}
+
+
+def run_reference(args) -> None:
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from oracle.bindings import Ref
+
+    if not Ref.available():
+        print(json.dumps({"impl": "reference",
+                          "unavailable": "oracle/_ref/libluxref.so was not built "
+                                         "(reference sources absent when built)"}))
+        return
+    threads = os.cpu_count() or 1
+    data = W.lbvh_microbench(N_TRIS, N_RAYS, N_QUERIES, SEED)
+    sample = 16384
+    for _ in range(args.warmup):
+        reference_step_estimate(data, 2048, threads)
+    steps = [reference_step_estimate(data, sample, threads) for _ in range(args.steps)]
+    step_s = statistics.median(s["step_s"] for s in steps)
+    value = N_RAYS / step_s / 1e6
+    line = {
+        "impl": "reference",
+        "metric": METRIC, "value": value, "unit": "Mrays/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": step_s * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD},
+        "cpu_baseline": {
+            "value": value, "unit": "Mrays/s", "cores": threads, "kind": "reference",
+            "sample": (f"reference host code: full 1,048,576-triangle builds (1 thread), "
+                       f"{sample} of 4,194,304 rays traced on {threads} threads and scaled, "
+                       f"overlap on 1/16 of the queries scaled"),
+        },
+        "e2e": {"value": value, "unit": "Mrays/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+        "phases_ms": {k: statistics.median(s[k] for s in steps) * 1e3
+                      for k in ["build_s", "trace_s", "refit_s", "query_build_s", "overlap_s"]},
+    }
+    print(json.dumps(line))
+
+
+# ------------------------------------------------------------------ GPU arm
+
+def run_lux(args) -> None:
+    import torch
+
+    import lux_b200
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    dev = torch.device("cuda", local)
+    data = W.lbvh_microbench(N_TRIS, N_RAYS, N_QUERIES, SEED)
+    d_tris = torch.from_numpy(data["triangles"]).to(dev)
+    d_rays = torch.from_numpy(data["rays"]).to(dev)
+    d_refit = torch.from_numpy(data["refit_triangles"]).to(dev)
+    d_queries = torch.from_numpy(data["queries"]).to(dev)
+    hit_id = torch.empty(N_RAYS, dtype=torch.int32, device=dev)
+    hit_t = torch.empty(N_RAYS, dtype=torch.float32, device=dev)
+    max_pairs = 1 << 21
+    pairs = torch.empty((max_pairs, 2), dtype=torch.int32, device=dev)
+    found = torch.zeros(1, dtype=torch.int64, device=dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+
+    stream = torch.cuda.current_stream(dev)
+    ctx = lux_b200.Context(local, stream.cuda_stream)
+    bvh = ctx.build_lbvh(d_tris)
+    qbvh = ctx.build_lbvh(d_queries, kind=lux_b200.PRIM_AABBS)
+    lib = ctx._lib
+    found_ptr = found.data_ptr()
+
+    phases = ["build", "trace", "refit", "query_build", "overlap"]
+
+    def step(ev=None):
+        if ev:
+            ev[0].record(stream)
+        bvh.rebuild(d_tris)
+        if ev:
+            ev[1].record(stream)
+        bvh.trace_closest(d_rays, hit_id, hit_t)
+        if ev:
+            ev[2].record(stream)
+        bvh.refit(d_refit)
+        if ev:
+            ev[3].record(stream)
+        qbvh.rebuild(d_queries)
+        if ev:
+            ev[4].record(stream)
+        status = lib.lux_overlap_cross(ctx.handle, bvh.handle, qbvh.handle, pairs.data_ptr(),
+                                       max_pairs, found_ptr)
+        if status:
+            lux_b200._check(status)
+        if ev:
+            ev[5].record(stream)
+
+    for _ in range(max(args.warmup, 1)):
+        step()
+        flush.zero_()
+    torch.cuda.synchronize()
+
+    evs = [[torch.cuda.Event(enable_timing=True) for _ in range(6)] for _ in range(args.steps)]
+    clocks = ClockSampler(local)
+    launches0 = ctx.launch_count()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    wall0 = time.perf_counter()
+    for k in range(args.steps):
+        flush.zero_()          # L2 flush between timed steps (outside the step events)
+        step(evs[k])
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - wall0
+    clock_info = clocks.stop()
+    if dist:
+        dist.barrier()
+    launches = ctx.launch_count() - launches0
+    ctx.synchronize()
+
+    per_phase = {p: [] for p in phases}
+    totals = []
+    for e in evs:
+        for i, p in enumerate(phases):
+            per_phase[p].append(e[i].elapsed_time(e[i + 1]))
+        totals.append(e[0].elapsed_time(e[5]))
+    step_ms = float(np.sum(totals)) / args.steps
+    if dist:
+        t = torch.tensor([step_ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        step_ms = float(t.item())
+    value = world * N_RAYS / (step_ms * 1e-3) / 1e6
+    phase_ms = {p: float(np.mean(v)) for p, v in per_phase.items()}
+
+    # Roofline of the dominant kernel (the traversal: one launch per trace phase).
+    box_tests, tri_tests = bvh.trace_stats(d_rays)
+    trace_bytes = N_RAYS * (32 + 8) + 32 * box_tests + 36 * tri_tests
+    peak, peak_kind = measured_peaks()
+    dominant = max(phase_ms, key=phase_ms.get)
+    if dominant == "trace":
+        achieved = trace_bytes / (phase_ms["trace"] * 1e-3) / 1e9
+        alg = trace_bytes
+    elif dominant == "build":
+        alg = BUILD_BYTES_PER_TRI * N_TRIS
+        achieved = alg / (phase_ms["build"] * 1e-3) / 1e9
+    else:
+        alg = trace_bytes
+        achieved = trace_bytes / (phase_ms["trace"] * 1e-3) / 1e9
+        dominant = "trace"
+
+    found_count = int(found.item())
+    hits = int((hit_id >= 0).sum().item())
+
+    e2e = None
+    cpu_baseline = None
+    if rank == 0 and not args.skip_e2e:
+        e2e = measure_e2e(ctx, data, args, dev)
+    if rank == 0 and world == 1 and not args.skip_cpu_baseline:
+        cpu_baseline = measure_cpu_baseline(data)
+
+    line = {
+        "metric": METRIC, "value": value, "unit": "Mrays/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "l2": "flushed between timed steps (256 MiB write)",
+                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+        "phases_ms": phase_ms,
+        "lbvh_mtri_s": N_TRIS / (phase_ms["build"] * 1e-3) / 1e6,
+        "trace_mrays_s": N_RAYS / (phase_ms["trace"] * 1e-3) / 1e6,
+        "refit_mtri_s": N_TRIS / (phase_ms["refit"] * 1e-3) / 1e6,
+        "hits": hits, "overlap_pairs": found_count,
+        "roofline": {"bound": "hbm", "kernel": "k_trace" if dominant == "trace" else dominant,
+                     "achieved": achieved, "peak": peak, "peak_kind": peak_kind,
+                     "unit": "GB/s", "frac": achieved / peak, "traffic": None,
+                     "algorithmic_bytes_per_launch": alg,
+                     "box_tests_per_ray": box_tests / N_RAYS,
+                     "tri_tests_per_ray": tri_tests / N_RAYS},
+        "clocks": clock_info,
+        "gpu_launches": launches,
+        "wall_s_timed_region": wall,
+        "e2e": e2e,
+        "cpu_baseline": cpu_baseline,
+    }
+    if rank == 0:
+        print(json.dumps(line))
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def measure_e2e(ctx, data, args, dev) -> dict:
+    """The same step through the C ABI with pinned host buffers: copies are timed."""
+    import torch
+
+    import lux_b200
+
+    def pinned(a):
+        t = torch.from_numpy(a).pin_memory()
+        return t
+
+    h_tris = pinned(data["triangles"])
+    h_rays = pinned(data["rays"])
+    h_refit = pinned(data["refit_triangles"])
+    h_queries = pinned(data["queries"])
+    h_id = torch.empty(N_RAYS, dtype=torch.int32).pin_memory()
+    h_t = torch.empty(N_RAYS, dtype=torch.float32).pin_memory()
+    max_pairs = 1 << 21
+    h_pairs = torch.empty((max_pairs, 2), dtype=torch.int32).pin_memory()
+    found = np.zeros(1, np.int64)
+    lib = ctx._lib
+
+    bvh = ctx.build_lbvh(h_tris)
+    qbvh = ctx.build_lbvh(h_queries, kind=lux_b200.PRIM_AABBS)
+
+    def step():
+        bvh.rebuild(h_tris)
+        bvh.trace_closest(h_rays, h_id, h_t)
+        bvh.refit(h_refit)
+        qbvh.rebuild(h_queries)
+        lux_b200._check(lib.lux_overlap_cross(ctx.handle, bvh.handle, qbvh.handle,
+                                              h_pairs.data_ptr(), max_pairs,
+                                              found.ctypes.data))
+
+    for _ in range(max(args.warmup, 1)):
+        step()
+    steps = max(3, min(args.steps, 10))
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        step()
+    ctx.synchronize()
+    dt = (time.perf_counter() - t0) / steps
+    h2d = sum(d.nbytes for d in (data["triangles"], data["rays"], data["refit_triangles"],
+                                  data["queries"]))
+    d2h = N_RAYS * 8 + min(int(found[0]), max_pairs) * 8 + 8
+    bvh.close()
+    qbvh.close()
+    return {"value": N_RAYS / dt / 1e6, "unit": "Mrays/s", "h2d_bytes_per_step": h2d,
+            "d2h_bytes_per_step": d2h, "ms_per_step": dt * 1e3, "steps": steps,
+            "host_buffers": "pinned"}
+
+
+def measure_cpu_baseline(data) -> dict | None:
+    try:
+        from oracle.bindings import Ref
+    except Exception:
+        return None
+    if not Ref.available():
+        return None
+    threads = os.cpu_count() or 1
+    est = reference_step_estimate(data, 16384, threads)
+    return {"value": N_RAYS / est["step_s"] / 1e6, "unit": "Mrays/s", "cores": threads,
+            "kind": "reference",
+            "sample": ("reference host code: full 1,048,576-triangle builds (1 thread), 16384 "
+                       f"of 4,194,304 rays on {threads} threads scaled, overlap on 1/16 of "
+                       "the queries (oracle port) scaled"),
+            "phases_ms": {k: v * 1e3 for k, v in est.items()}}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="lux", choices=["lux", "reference"])
+    ap.add_argument("--skip-e2e", action="store_true")
+    ap.add_argument("--skip-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_lux(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,154 @@
+/*
+ * lux_gpu.h -- C ABI of the B200 LBVH + wavefront path-tracing library (liblux_gpu.so).
+ *
+ * Every entry point returns an int status (LUX_OK == 0).  On failure the status names
+ * the class of error and lux_last_error() returns a thread-local message.  Handles are
+ * opaque; the device memory behind a handle is owned by it.
+ *
+ * Memory: every array argument may point to host memory or to device memory of the
+ * context's device; the library inspects each pointer.  Device inputs and outputs are
+ * stream ordered on the context's stream and the call returns without waiting.  A host
+ * input is staged to the device inside the call; a call with any host output waits
+ * for its own work before returning (the behaviour of the reference's std::vector
+ * API).  One context per host thread, or external locking: a context carries mutable
+ * scratch state.
+ *
+ * Layouts:
+ *   triangles  9 floats per triangle: v0.xyz v1.xyz v2.xyz            (geometry/triangle.h:9-11)
+ *   aabbs      6 floats per box: min.xyz max.xyz                      (core/aabb.cuh:10-12)
+ *   rays       8 floats per ray: origin.xyz t_min direction.xyz t_max  (core/ray.cuh:10-16,
+ *              reordered into two 16-byte halves; time is not used by the BVH queries)
+ *   pairs      2 int32 per pair (a, b)                                 (bvh/bvh_overlap.cuh:10-13)
+ * Primitive ids are the input indices 0..n-1.
+ *
+ * Reference interfaces replaced (paths relative to the reference's src/):
+ *   bvh/gpu_bvh.cuh:50-61, bvh/bvh_overlap.cuh:21-23, integrator/integrator.h:15-22,
+ *   integrator/wavefront_pt.cuh:14-28, scene/prepared_scene.h:35-39.
+ */
+#ifndef LUX_GPU_H
+#define LUX_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LUX_ABI_VERSION 1
+
+enum lux_status {
+    LUX_OK = 0,
+    LUX_ERR_INVALID_ARGUMENT = 1,  /* bad size, null handle, unknown enum value */
+    LUX_ERR_CUDA = 2,              /* a CUDA runtime call failed */
+    LUX_ERR_OUT_OF_MEMORY = 3,     /* device allocation failed */
+    LUX_ERR_MISMATCH = 4,          /* refit input does not match the built topology */
+    LUX_ERR_DEVICE_CHECK = 5,      /* a kernel's bounded loop or bounds check tripped */
+    LUX_ERR_QUEUE_OVERFLOW = 6,    /* a work queue exceeded its capacity */
+    LUX_ERR_BUDGET = 7             /* request does not fit the memory budget */
+};
+
+enum lux_prim_kind { LUX_PRIM_TRIANGLES = 0, LUX_PRIM_AABBS = 1 };
+
+typedef struct lux_ctx lux_ctx;
+typedef struct lux_bvh lux_bvh;
+
+/* ------------------------------------------------------------------ context */
+
+/* Creates a context on `device`.  stream: a cudaStream_t, or NULL for a stream the
+ * context creates and owns. */
+int lux_ctx_create(lux_ctx** out, int device, void* stream);
+int lux_ctx_destroy(lux_ctx* ctx);
+/* Re-targets later calls to another cudaStream_t (NULL: the context's own stream). */
+int lux_ctx_set_stream(lux_ctx* ctx, void* stream);
+/* Waits for all work the context queued. */
+int lux_ctx_synchronize(lux_ctx* ctx);
+/* Thread-local description of the last failure on this thread ("" if none). */
+const char* lux_last_error(void);
+int lux_abi_version(void);
+/* Number of kernels this context has launched so far (for launch accounting). */
+int lux_ctx_launch_count(lux_ctx* ctx, int64_t* count);
+
+/* ------------------------------------------------------------------ LBVH */
+
+/*
+ * Builds a linear BVH over n primitives: per-primitive boxes, their union, 30-bit
+ * (morton_bits 30) or 63-bit (63) Morton codes of the box centroids normalised to the
+ * union, a stable radix sort of the codes, the Karras hierarchy and a bottom-up box
+ * pass.  Bit-exact with build_cpu_lbvh_tree (bvh/cpu_lbvh_builder.h:163-259) for 30
+ * bits.  Replaces build_gpu_lbvh (bvh/gpu_bvh.cuh:51).  n == 0 yields an empty BVH.
+ */
+int lux_lbvh_build(lux_ctx* ctx, const float* prims, int32_t n, int32_t kind,
+                   int32_t morton_bits, lux_bvh** out);
+
+/*
+ * New primitive geometry, same primitive count and order: recomputes leaf and node
+ * boxes bottom-up over the existing topology (Morton order is kept, as in
+ * refit_gpu_lbvh, bvh/gpu_bvh.cu:597-613).  LUX_ERR_MISMATCH on a count mismatch.
+ * Replaces refit_gpu_lbvh (bvh/gpu_bvh.cuh:52).
+ */
+int lux_lbvh_refit(lux_ctx* ctx, lux_bvh* bvh, const float* prims, int32_t n);
+
+/*
+ * Rebuilds `bvh` in place over a new primitive set of the same kind (any count): the
+ * handle's device storage is reused when large enough, so a resident BVH can be
+ * rebuilt every frame without device allocation.  Same results as lux_lbvh_build.
+ */
+int lux_lbvh_rebuild(lux_ctx* ctx, lux_bvh* bvh, const float* prims, int32_t n);
+
+int lux_bvh_destroy(lux_bvh* bvh);
+
+/* Primitive count, kind, Morton width and the root box (6 floats, host). */
+int lux_bvh_info(lux_ctx* ctx, const lux_bvh* bvh, int32_t* n, int32_t* kind,
+                 int32_t* morton_bits, float* root_bounds);
+
+/*
+ * Copies the BVH out in the reference's host tree layout (CpuBvhTree,
+ * bvh/cpu_bvh.h:15-32; download_bvh_for_validation, bvh/gpu_bvh.cu:615-665): internal
+ * node i (0 <= i < n-1) is Karras node i, leaf k is node n-1+k in sorted order.
+ * Any output may be NULL.  sorted_codes: n uint64 (30-bit codes widen to 64);
+ * sorted_ids: n; node_left/right: 2n-1 (-1 on leaves); node_bounds: (2n-1)*6 floats.
+ */
+int lux_bvh_download(lux_ctx* ctx, const lux_bvh* bvh, uint64_t* sorted_codes,
+                     int32_t* sorted_ids, int32_t* node_left, int32_t* node_right,
+                     float* node_bounds);
+
+/*
+ * Closest hit of each ray against a triangle BVH.  Visits nodes in the reference's
+ * stackless order (bvh/bvh_device.cuh:43-90: left child first, strict t < best), so
+ * equal-t ties resolve exactly as the reference GPU path does.  No hit: id -1, t +inf.
+ * Replaces intersect_gpu_bvh_stackless (bvh/gpu_bvh.cuh:60-62).
+ */
+int lux_trace_closest(lux_ctx* ctx, const lux_bvh* bvh, const float* rays, int32_t nrays,
+                      int32_t* hit_id, float* hit_t);
+
+/*
+ * Traversal statistics of lux_trace_closest for the same rays, without writing hits:
+ * totals[0] += box tests, totals[1] += triangle tests (int64, host or device).  The
+ * counts equal the reference's node visits and triangle tests (bvh/bvh_device.cuh:59-87)
+ * because the visit order is the same; they define the traversal's algorithmic bytes.
+ */
+int lux_trace_closest_stats(lux_ctx* ctx, const lux_bvh* bvh, const float* rays,
+                            int32_t nrays, int64_t* totals);
+
+/* Any hit (occlusion) in [t_min, t_max]: hit_id receives some hit primitive or -1.
+ * Whether a ray is occluded equals whether lux_trace_closest finds a hit. */
+int lux_trace_any(lux_ctx* ctx, const lux_bvh* bvh, const float* rays, int32_t nrays,
+                  int32_t* hit_id);
+
+/*
+ * Box-overlap pairs.  Self: every (a, b), a < b, whose boxes overlap
+ * (query_aabb_overlaps_self, bvh/bvh_overlap.cuh:21).  Cross: every (left, right)
+ * primitive pair (query_aabb_overlaps_cross, bvh/bvh_overlap.cuh:22-23).  At most
+ * max_pairs pairs are written (in no particular order); *found receives the total, so
+ * *found > max_pairs means truncated.
+ */
+int lux_overlap_self(lux_ctx* ctx, const lux_bvh* bvh, int32_t* pairs, int64_t max_pairs,
+                     int64_t* found);
+int lux_overlap_cross(lux_ctx* ctx, const lux_bvh* left, const lux_bvh* right,
+                      int32_t* pairs, int64_t max_pairs, int64_t* found);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* LUX_GPU_H */

@@ -1,0 +1,492 @@
+// extern "C" boundary of liblux_gpu.so (declared in include/lux_gpu.h).
+//
+// Responsibilities: argument validation, status codes and the thread-local error text,
+// host/device pointer classification with staging of host buffers, and the device
+// error word that bounded kernel loops report through.
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/lux_gpu.h"
+#include "lux_internal.h"
+
+namespace {
+
+thread_local std::string g_error;
+
+bool is_device_pointer(const void* p) {
+    if (!p) return false;
+    cudaPointerAttributes attr;
+    cudaError_t err = cudaPointerGetAttributes(&attr, p);
+    if (err != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return attr.type == cudaMemoryTypeDevice || attr.type == cudaMemoryTypeManaged;
+}
+
+// Carves device staging regions for host arguments out of the context's staging buffer.
+struct Staging {
+    lux_ctx* ctx;
+    struct Item {
+        const void* host_in;   // copy host -> device before the work
+        void* host_out;        // copy device -> host after the work
+        size_t bytes;
+        size_t offset;
+        void** device;
+    };
+    std::vector<Item> items;
+    size_t total = 0;
+
+    explicit Staging(lux_ctx* c) : ctx(c) {}
+
+    // in: the argument is read by the device; out: it is written by the device.
+    void add(const void* arg, size_t bytes, bool in, bool out, void** device) {
+        if (!arg || bytes == 0) {
+            *device = const_cast<void*>(arg);
+            return;
+        }
+        if (is_device_pointer(arg)) {
+            *device = const_cast<void*>(arg);
+            return;
+        }
+        Item it{in ? arg : nullptr, out ? const_cast<void*>(arg) : nullptr, bytes, total, device};
+        total += (bytes + 255) & ~size_t(255);
+        items.push_back(it);
+    }
+
+    bool has_host_output() const {
+        for (const Item& it : items)
+            if (it.host_out) return true;
+        return false;
+    }
+
+    int begin() {
+        if (items.empty()) return LUX_OK;
+        if (total > ctx->staging_bytes) {
+            if (ctx->staging) {
+                cudaStreamSynchronize(ctx->stream);
+                cudaFree(ctx->staging);
+                ctx->staging = nullptr;
+                ctx->staging_bytes = 0;
+            }
+            cudaError_t err = cudaMalloc(&ctx->staging, total);
+            if (err != cudaSuccess) {
+                cudaGetLastError();
+                return lux::fail(LUX_ERR_OUT_OF_MEMORY, "staging allocation failed");
+            }
+            ctx->staging_bytes = total;
+        }
+        char* base = static_cast<char*>(ctx->staging);
+        for (Item& it : items) {
+            *it.device = base + it.offset;
+            if (it.host_in) {
+                cudaError_t err = cudaMemcpyAsync(base + it.offset, it.host_in, it.bytes,
+                                                  cudaMemcpyHostToDevice, ctx->stream);
+                if (err != cudaSuccess) return lux::cuda_fail(err, "host to device copy");
+            }
+        }
+        return LUX_OK;
+    }
+
+    int finish() {
+        char* base = static_cast<char*>(ctx->staging);
+        for (Item& it : items) {
+            if (!it.host_out) continue;
+            cudaError_t err = cudaMemcpyAsync(it.host_out, base + it.offset, it.bytes,
+                                              cudaMemcpyDeviceToHost, ctx->stream);
+            if (err != cudaSuccess) return lux::cuda_fail(err, "device to host copy");
+        }
+        return LUX_OK;
+    }
+};
+
+int check_ctx(lux_ctx* ctx) {
+    if (!ctx) return lux::fail(LUX_ERR_INVALID_ARGUMENT, "null context");
+    cudaError_t err = cudaSetDevice(ctx->device);
+    return lux::cuda_fail(err, "cudaSetDevice");
+}
+
+// Waits for the stream, then reports (and clears) the device error word.
+int sync_and_check(lux_ctx* ctx) {
+    cudaError_t err = cudaStreamSynchronize(ctx->stream);
+    if (err != cudaSuccess) return lux::cuda_fail(err, "stream synchronize");
+    int word = 0;
+    err = cudaMemcpy(&word, ctx->d_error, sizeof(int), cudaMemcpyDeviceToHost);
+    if (err != cudaSuccess) return lux::cuda_fail(err, "error word read");
+    if (word) {
+        cudaMemset(ctx->d_error, 0, sizeof(int));
+        std::string what;
+        if (word & lux::kErrClimbBound) what += " bottom-up level bound exceeded;";
+        if (word & lux::kErrStackOverflow) what += " traversal stack overflow;";
+        if (word & lux::kErrLoopBound) what += " bounded loop exhausted;";
+        if (word & lux::kErrQueueOverflow) {
+            return lux::fail(LUX_ERR_QUEUE_OVERFLOW, "device check:" + what + " queue overflow");
+        }
+        return lux::fail(LUX_ERR_DEVICE_CHECK, "device check:" + what);
+    }
+    return LUX_OK;
+}
+
+int finish_call(lux_ctx* ctx, Staging& staging) {
+    int st = staging.finish();
+    if (st) return st;
+    if (staging.has_host_output()) return sync_and_check(ctx);
+    return lux::cuda_fail(cudaGetLastError(), "launch");
+}
+
+}  // namespace
+
+namespace lux {
+
+int fail(int status, const std::string& message) {
+    g_error = message;
+    return status;
+}
+
+int cuda_fail(cudaError_t err, const char* what) {
+    if (err == cudaSuccess) return LUX_OK;
+    g_error = std::string(what) + ": " + cudaGetErrorString(err);
+    return err == cudaErrorMemoryAllocation ? LUX_ERR_OUT_OF_MEMORY : LUX_ERR_CUDA;
+}
+
+int ensure_scratch(lux_ctx* ctx, size_t bytes) {
+    if (bytes <= ctx->scratch_bytes) return LUX_OK;
+    if (ctx->scratch) {
+        cudaStreamSynchronize(ctx->stream);
+        cudaFree(ctx->scratch);
+        ctx->scratch = nullptr;
+        ctx->scratch_bytes = 0;
+    }
+    size_t want = std::max(bytes, size_t(1) << 20);
+    cudaError_t err = cudaMalloc(&ctx->scratch, want);
+    if (err != cudaSuccess) {
+        cudaGetLastError();
+        return fail(LUX_ERR_OUT_OF_MEMORY, "scratch allocation failed");
+    }
+    ctx->scratch_bytes = want;
+    return LUX_OK;
+}
+
+}  // namespace lux
+
+extern "C" {
+
+int lux_abi_version(void) { return LUX_ABI_VERSION; }
+
+const char* lux_last_error(void) { return g_error.c_str(); }
+
+int lux_ctx_create(lux_ctx** out, int device, void* stream) {
+    if (!out) return lux::fail(LUX_ERR_INVALID_ARGUMENT, "null output");
+    *out = nullptr;
+    int count = 0;
+    cudaError_t err = cudaGetDeviceCount(&count);
+    if (err != cudaSuccess) return lux::cuda_fail(err, "cudaGetDeviceCount");
+    if (device < 0 || device >= count)
+        return lux::fail(LUX_ERR_INVALID_ARGUMENT, "device index out of range");
+    err = cudaSetDevice(device);
+    if (err != cudaSuccess) return lux::cuda_fail(err, "cudaSetDevice");
+    lux_ctx* ctx = new (std::nothrow) lux_ctx();
+    if (!ctx) return lux::fail(LUX_ERR_OUT_OF_MEMORY, "context allocation failed");
+    ctx->device = device;
+    cudaDeviceGetAttribute(&ctx->sm_count, cudaDevAttrMultiProcessorCount, device);
+    if (stream) {
+        ctx->stream = static_cast<cudaStream_t>(stream);
+    } else {
+        err = cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking);
+        if (err != cudaSuccess) {
+            delete ctx;
+            return lux::cuda_fail(err, "cudaStreamCreate");
+        }
+        ctx->stream = ctx->own_stream;
+    }
+    err = cudaMalloc(&ctx->d_error, sizeof(int));
+    if (err == cudaSuccess) err = cudaMemset(ctx->d_error, 0, sizeof(int));
+    if (err != cudaSuccess) {
+        if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
+        delete ctx;
+        return lux::cuda_fail(err, "context init");
+    }
+    *out = ctx;
+    return LUX_OK;
+}
+
+int lux_ctx_destroy(lux_ctx* ctx) {
+    if (!ctx) return LUX_OK;
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    if (ctx->scratch) cudaFree(ctx->scratch);
+    if (ctx->staging) cudaFree(ctx->staging);
+    if (ctx->d_error) cudaFree(ctx->d_error);
+    if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
+    delete ctx;
+    return LUX_OK;
+}
+
+int lux_ctx_set_stream(lux_ctx* ctx, void* stream) {
+    if (int st = check_ctx(ctx)) return st;
+    ctx->stream = stream ? static_cast<cudaStream_t>(stream) : ctx->own_stream;
+    if (!ctx->stream) {
+        cudaError_t err = cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking);
+        if (err != cudaSuccess) return lux::cuda_fail(err, "cudaStreamCreate");
+        ctx->stream = ctx->own_stream;
+    }
+    return LUX_OK;
+}
+
+int lux_ctx_synchronize(lux_ctx* ctx) {
+    if (int st = check_ctx(ctx)) return st;
+    return sync_and_check(ctx);
+}
+
+int lux_ctx_launch_count(lux_ctx* ctx, int64_t* count) {
+    if (!ctx || !count) return lux::fail(LUX_ERR_INVALID_ARGUMENT, "null argument");
+    *count = ctx->launches;
+    return LUX_OK;
+}
+
+int lux_lbvh_build(lux_ctx* ctx, const float* prims, int32_t n, int32_t kind,
+                   int32_t morton_bits, lux_bvh** out) {
+    if (int st = check_ctx(ctx)) return st;
+    if (!out) return lux::fail(LUX_ERR_INVALID_ARGUMENT, "null output");
+    *out = nullptr;
+    if (n < 0 || (n > 0 && !prims)) return lux::fail(LUX_ERR_INVALID_ARGUMENT, "bad primitive array");
+    if (n > (1 << 30)) return lux::fail(LUX_ERR_INVALID_ARGUMENT, "too many primitives (max 2^30)");
+    if (kind != LUX_PRIM_TRIANGLES && kind != LUX_PRIM_AABBS)
+        return lux::fail(LUX_ERR_INVALID_ARGUMENT, "unknown primitive kind");
+    if (morton_bits != 30 && morton_bits != 63)
+        return lux::fail(LUX_ERR_INVALID_ARGUMENT, "morton_bits must be 30 or 63");
+    lux_bvh* bvh = new (std::nothrow) lux_bvh();
+    if (!bvh) return lux::fail(LUX_ERR_OUT_OF_MEMORY, "bvh allocation failed");
+    bvh->n = n;
+    bvh->kind = kind;
+    bvh->morton_bits = morton_bits;
+    bvh->device = ctx->device;
+    int st = lux::lbvh_alloc(ctx, bvh);
+    if (st) {
+        delete bvh;
+        return st;
+    }
+    size_t per = kind == LUX_PRIM_TRIANGLES ? 9 : 6;
+    Staging staging(ctx);
+    void* d_prims = nullptr;
+    staging.add(prims, sizeof(float) * per * static_cast<size_t>(n), true, false, &d_prims);
+    st = staging.begin();
+    if (!st) st = lux::lbvh_build(ctx, bvh, static_cast<const float*>(d_prims));
+    if (!st) st = finish_call(ctx, staging);
+    // Host-staged inputs must outlive the kernels that read them.
+    if (!st && !staging.items.empty()) st = sync_and_check(ctx);
+    if (st) {
+        lux::lbvh_free(bvh);
+        delete bvh;
+        return st;
+    }
+    *out = bvh;
+    return LUX_OK;
+}
+
+int lux_lbvh_rebuild(lux_ctx* ctx, lux_bvh* bvh, const float* prims, int32_t n) {
+    if (int st = check_ctx(ctx)) return st;
+    if (!bvh) return lux::fail(LUX_ERR_INVALID_ARGUMENT, "null bvh");
+    if (n < 0 || (n > 0 && !prims)) return lux::fail(LUX_ERR_INVALID_ARGUMENT, "bad primitive array");
+    if (n > (1 << 30)) return lux::fail(LUX_ERR_INVALID_ARGUMENT, "too many primitives (max 2^30)");
+    if (n > bvh->capacity) {
+        cudaStreamSynchronize(ctx->stream);
+        lux::lbvh_free(bvh);
+        bvh->capacity = 0;
+        bvh->n = n;
+        if (int st = lux::lbvh_alloc(ctx, bvh)) {
+            bvh->n = 0;
+            return st;
+        }
+    }
+    bvh->n = n;
+    size_t per = bvh->kind == LUX_PRIM_TRIANGLES ? 9 : 6;
+    Staging staging(ctx);
+    void* d_prims = nullptr;
+    staging.add(prims, sizeof(float) * per * static_cast<size_t>(n), true, false, &d_prims);
+    int st = staging.begin();
+    if (!st) st = lux::lbvh_build(ctx, bvh, static_cast<const float*>(d_prims));
+    if (!st) st = finish_call(ctx, staging);
+    if (!st && !staging.items.empty()) st = sync_and_check(ctx);
+    return st;
+}
+
+int lux_lbvh_refit(lux_ctx* ctx, lux_bvh* bvh, const float* prims, int32_t n) {
+    if (int st = check_ctx(ctx)) return st;
+    if (!bvh) return lux::fail(LUX_ERR_INVALID_ARGUMENT, "null bvh");
+    if (n != bvh->n) return lux::fail(LUX_ERR_MISMATCH, "refit primitive count differs from build");
+    if (n > 0 && !prims) return lux::fail(LUX_ERR_INVALID_ARGUMENT, "bad primitive array");
+    size_t per = bvh->kind == LUX_PRIM_TRIANGLES ? 9 : 6;
+    Staging staging(ctx);
+    void* d_prims = nullptr;
+    staging.add(prims, sizeof(float) * per * static_cast<size_t>(n), true, false, &d_prims);
+    int st = staging.begin();
+    if (!st) st = lux::lbvh_refit(ctx, bvh, static_cast<const float*>(d_prims));
+    if (!st) st = finish_call(ctx, staging);
+    if (!st && !staging.items.empty()) st = sync_and_check(ctx);
+    return st;
+}
+
+int lux_bvh_destroy(lux_bvh* bvh) {
+    if (!bvh) return LUX_OK;
+    cudaSetDevice(bvh->device);
+    lux::lbvh_free(bvh);
+    delete bvh;
+    return LUX_OK;
+}
+
+int lux_bvh_info(lux_ctx* ctx, const lux_bvh* bvh, int32_t* n, int32_t* kind,
+                 int32_t* morton_bits, float* root_bounds) {
+    if (int st = check_ctx(ctx)) return st;
+    if (!bvh) return lux::fail(LUX_ERR_INVALID_ARGUMENT, "null bvh");
+    if (n) *n = bvh->n;
+    if (kind) *kind = bvh->kind;
+    if (morton_bits) *morton_bits = bvh->morton_bits;
+    if (root_bounds) {
+        if (bvh->n <= 0) {
+            for (int a = 0; a < 3; ++a) {
+                root_bounds[a] = INFINITY;
+                root_bounds[3 + a] = -INFINITY;
+            }
+            return LUX_OK;
+        }
+        Staging staging(ctx);
+        void* d_root = nullptr;
+        staging.add(root_bounds, sizeof(float) * 6, false, true, &d_root);
+        int st = staging.begin();
+        if (st) return st;
+        cudaError_t err = cudaMemcpyAsync(d_root, bvh->root, sizeof(float) * 6,
+                                          cudaMemcpyDeviceToDevice, ctx->stream);
+        if (err != cudaSuccess) return lux::cuda_fail(err, "root copy");
+        return finish_call(ctx, staging);
+    }
+    return LUX_OK;
+}
+
+int lux_bvh_download(lux_ctx* ctx, const lux_bvh* bvh, uint64_t* sorted_codes,
+                     int32_t* sorted_ids, int32_t* node_left, int32_t* node_right,
+                     float* node_bounds) {
+    if (int st = check_ctx(ctx)) return st;
+    if (!bvh) return lux::fail(LUX_ERR_INVALID_ARGUMENT, "null bvh");
+    size_t n = static_cast<size_t>(bvh->n);
+    if (n == 0) return LUX_OK;
+    size_t count = 2 * n - 1;
+    Staging staging(ctx);
+    void *d_codes, *d_ids, *d_left, *d_right, *d_bounds;
+    staging.add(sorted_codes, 8 * n, false, true, &d_codes);
+    staging.add(sorted_ids, 4 * n, false, true, &d_ids);
+    staging.add(node_left, 4 * count, false, true, &d_left);
+    staging.add(node_right, 4 * count, false, true, &d_right);
+    staging.add(node_bounds, 24 * count, false, true, &d_bounds);
+    int st = staging.begin();
+    if (st) return st;
+    if (d_ids) {
+        cudaError_t err = cudaMemcpyAsync(d_ids, bvh->sorted_ids, 4 * n,
+                                          cudaMemcpyDeviceToDevice, ctx->stream);
+        if (err != cudaSuccess) return lux::cuda_fail(err, "sorted id copy");
+    }
+    st = lux::lbvh_export(ctx, bvh, static_cast<uint64_t*>(d_codes), static_cast<int*>(d_left),
+                          static_cast<int*>(d_right), static_cast<float*>(d_bounds));
+    if (st) return st;
+    return finish_call(ctx, staging);
+}
+
+static int check_query(lux_ctx* ctx, const lux_bvh* bvh, const float* rays, int32_t nrays) {
+    if (int st = check_ctx(ctx)) return st;
+    if (!bvh) return lux::fail(LUX_ERR_INVALID_ARGUMENT, "null bvh");
+    if (bvh->kind != LUX_PRIM_TRIANGLES)
+        return lux::fail(LUX_ERR_INVALID_ARGUMENT, "ray queries need a triangle BVH");
+    if (nrays < 0 || (nrays > 0 && !rays)) return lux::fail(LUX_ERR_INVALID_ARGUMENT, "bad ray array");
+    return LUX_OK;
+}
+
+int lux_trace_closest(lux_ctx* ctx, const lux_bvh* bvh, const float* rays, int32_t nrays,
+                      int32_t* hit_id, float* hit_t) {
+    if (int st = check_query(ctx, bvh, rays, nrays)) return st;
+    if (nrays > 0 && !hit_id) return lux::fail(LUX_ERR_INVALID_ARGUMENT, "null hit_id");
+    Staging staging(ctx);
+    void *d_rays, *d_id, *d_t;
+    size_t r = static_cast<size_t>(nrays);
+    staging.add(rays, 32 * r, true, false, &d_rays);
+    staging.add(hit_id, 4 * r, false, true, &d_id);
+    staging.add(hit_t, 4 * r, false, true, &d_t);
+    int st = staging.begin();
+    if (st) return st;
+    st = lux::trace_closest(ctx, bvh, static_cast<const float*>(d_rays), nrays,
+                            static_cast<int*>(d_id), static_cast<float*>(d_t));
+    if (st) return st;
+    st = finish_call(ctx, staging);
+    if (!st && !staging.items.empty() && !staging.has_host_output()) st = sync_and_check(ctx);
+    return st;
+}
+
+int lux_trace_closest_stats(lux_ctx* ctx, const lux_bvh* bvh, const float* rays,
+                            int32_t nrays, int64_t* totals) {
+    if (int st = check_query(ctx, bvh, rays, nrays)) return st;
+    if (!totals) return lux::fail(LUX_ERR_INVALID_ARGUMENT, "null totals");
+    Staging staging(ctx);
+    void *d_rays, *d_tot;
+    staging.add(rays, 32 * static_cast<size_t>(nrays), true, false, &d_rays);
+    staging.add(totals, 16, true, true, &d_tot);
+    int st = staging.begin();
+    if (st) return st;
+    st = lux::trace_stats(ctx, bvh, static_cast<const float*>(d_rays), nrays,
+                          static_cast<unsigned long long*>(d_tot));
+    if (st) return st;
+    return finish_call(ctx, staging);
+}
+
+int lux_trace_any(lux_ctx* ctx, const lux_bvh* bvh, const float* rays, int32_t nrays,
+                  int32_t* hit_id) {
+    if (int st = check_query(ctx, bvh, rays, nrays)) return st;
+    if (nrays > 0 && !hit_id) return lux::fail(LUX_ERR_INVALID_ARGUMENT, "null hit_id");
+    Staging staging(ctx);
+    void *d_rays, *d_id;
+    size_t r = static_cast<size_t>(nrays);
+    staging.add(rays, 32 * r, true, false, &d_rays);
+    staging.add(hit_id, 4 * r, false, true, &d_id);
+    int st = staging.begin();
+    if (st) return st;
+    st = lux::trace_any(ctx, bvh, static_cast<const float*>(d_rays), nrays,
+                        static_cast<int*>(d_id));
+    if (st) return st;
+    st = finish_call(ctx, staging);
+    if (!st && !staging.items.empty() && !staging.has_host_output()) st = sync_and_check(ctx);
+    return st;
+}
+
+static int overlap_common(lux_ctx* ctx, const lux_bvh* tree, const lux_bvh* queries, bool self,
+                          int32_t* pairs, int64_t max_pairs, int64_t* found) {
+    if (int st = check_ctx(ctx)) return st;
+    if (!tree || !queries) return lux::fail(LUX_ERR_INVALID_ARGUMENT, "null bvh");
+    if (max_pairs < 0 || (max_pairs > 0 && !pairs) || !found)
+        return lux::fail(LUX_ERR_INVALID_ARGUMENT, "bad pair buffer");
+    Staging staging(ctx);
+    void *d_pairs, *d_found;
+    staging.add(pairs, 8 * static_cast<size_t>(max_pairs), false, true, &d_pairs);
+    staging.add(found, 8, false, true, &d_found);
+    int st = staging.begin();
+    if (st) return st;
+    st = lux::overlap(ctx, tree, queries, self, static_cast<int*>(d_pairs), max_pairs,
+                      static_cast<unsigned long long*>(d_found));
+    if (st) return st;
+    return finish_call(ctx, staging);
+}
+
+int lux_overlap_self(lux_ctx* ctx, const lux_bvh* bvh, int32_t* pairs, int64_t max_pairs,
+                     int64_t* found) {
+    return overlap_common(ctx, bvh, bvh, true, pairs, max_pairs, found);
+}
+
+int lux_overlap_cross(lux_ctx* ctx, const lux_bvh* left, const lux_bvh* right,
+                      int32_t* pairs, int64_t max_pairs, int64_t* found) {
+    return overlap_common(ctx, left, right, false, pairs, max_pairs, found);
+}
+
+}  // extern "C"

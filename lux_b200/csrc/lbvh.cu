@@ -1,0 +1,585 @@
+// LBVH construction and refit for sm_100a.
+//
+// Pipeline (one stream, no host synchronisation):
+//   1. k_root_reduce   per-primitive boxes -> union (order-free atomics on ordered ints)
+//   2. k_morton        30-/63-bit Morton code of each box centroid
+//   3. radix sort      stable LSD sort of (code, input index), 8-bit digits
+//   4. k_karras        Karras 2012 hierarchy over the sorted codes
+//   5. k_leaf_climb    leaf boxes + triangle records in sorted order, then one bottom-up
+//                      climb per leaf that writes every child box into its parent
+//
+// Reference counterparts (src/): bvh/gpu_bvh.cu:135-149 (codes), 582-584 (sort),
+// 151-180 (hierarchy), 182-214 (bottom-up boxes), 535-613 (build/refit drivers);
+// bvh/cpu_lbvh_builder.h:163-259 (the host builder the results are bit-exact with).
+// The reference's separate subtree-size, preorder and escape passes (gpu_bvh.cu:216-363)
+// have no counterpart: traversal walks the Karras nodes directly.
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdint>
+
+#include "../../include/lux_gpu.h"
+#include "lux_internal.h"
+
+namespace lux {
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kRadix = 256;
+constexpr int kSortItems = 16;
+constexpr int kSortTile = kThreads * kSortItems;  // keys per tile
+constexpr int kScanThreads = 1024;
+constexpr int kClimbBound = 160;                 // > max tree depth (64 + 96 bits)
+
+LUX_D unsigned lanemask_lt() {
+    unsigned m;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+    return m;
+}
+
+template <int Kind>
+LUX_D void load_prim(const float* prims, int i, f3& v0, f3& v1, f3& v2, box3& b) {
+    if (Kind == LUX_PRIM_TRIANGLES) {
+        const float* t = prims + static_cast<size_t>(i) * 9;
+        v0 = make_f3(t[0], t[1], t[2]);
+        v1 = make_f3(t[3], t[4], t[5]);
+        v2 = make_f3(t[6], t[7], t[8]);
+        b = triangle_box(v0, v1, v2);
+    } else {
+        const float* t = prims + static_cast<size_t>(i) * 6;
+        b = box3{make_f3(t[0], t[1], t[2]), make_f3(t[3], t[4], t[5])};
+        v0 = v1 = v2 = make_f3(0, 0, 0);
+    }
+}
+
+// ---------------------------------------------------------------- 1. root box
+
+template <int Kind>
+__global__ void __launch_bounds__(kThreads) k_root_reduce(const float* prims, int n,
+                                                          unsigned* root_ord) {
+    float lo[3] = {INFINITY, INFINITY, INFINITY};
+    float hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        f3 v0, v1, v2;
+        box3 b;
+        load_prim<Kind>(prims, i, v0, v1, v2, b);
+        lo[0] = fminf(lo[0], b.lo.x); lo[1] = fminf(lo[1], b.lo.y); lo[2] = fminf(lo[2], b.lo.z);
+        hi[0] = fmaxf(hi[0], b.hi.x); hi[1] = fmaxf(hi[1], b.hi.y); hi[2] = fmaxf(hi[2], b.hi.z);
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            lo[a] = fminf(lo[a], __shfl_xor_sync(0xffffffffu, lo[a], off));
+            hi[a] = fmaxf(hi[a], __shfl_xor_sync(0xffffffffu, hi[a], off));
+        }
+    }
+    if ((threadIdx.x & 31) == 0) {
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            atomicMin(root_ord + a, float_to_ordered(lo[a]));
+            atomicMin(root_ord + 3 + a, ~float_to_ordered(hi[a]));
+        }
+    }
+}
+
+LUX_D box3 decode_root(const unsigned* root_ord) {
+    return box3{make_f3(ordered_to_float(root_ord[0]), ordered_to_float(root_ord[1]),
+                        ordered_to_float(root_ord[2])),
+                make_f3(ordered_to_float(~root_ord[3]), ordered_to_float(~root_ord[4]),
+                        ordered_to_float(~root_ord[5]))};
+}
+
+// ---------------------------------------------------------------- 2. Morton codes
+
+template <int Kind, typename Key>
+__global__ void __launch_bounds__(kThreads) k_morton(const float* prims, int n,
+                                                     const unsigned* root_ord, Key* codes) {
+    box3 root = decode_root(root_ord);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        f3 v0, v1, v2;
+        box3 b;
+        load_prim<Kind>(prims, i, v0, v1, v2, b);
+        if (sizeof(Key) == 4) {
+            codes[i] = static_cast<Key>(morton30(b, root));
+        } else {
+            codes[i] = static_cast<Key>(morton63(b, root));
+        }
+    }
+}
+
+// ---------------------------------------------------------------- 3. radix sort
+
+template <typename Key>
+LUX_D unsigned digit_of(Key k, int shift) {
+    return static_cast<unsigned>(k >> shift) & (kRadix - 1);
+}
+
+// Per-tile digit counts, stored digit-major: hist[d * tiles + tile].
+template <typename Key>
+__global__ void __launch_bounds__(kThreads) k_sort_upsweep(const Key* keys, int n, int shift,
+                                                           unsigned* hist, int tiles) {
+    __shared__ unsigned counts[kRadix];
+    counts[threadIdx.x] = 0;
+    __syncthreads();
+    int base = blockIdx.x * kSortTile;
+#pragma unroll 4
+    for (int j = 0; j < kSortItems; ++j) {
+        int idx = base + j * kThreads + threadIdx.x;
+        bool valid = idx < n;
+        unsigned d = valid ? digit_of(keys[idx], shift) : kRadix;
+        unsigned peers = __match_any_sync(0xffffffffu, d);
+        if (valid && (threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(&counts[d], __popc(peers));
+    }
+    __syncthreads();
+    hist[threadIdx.x * tiles + blockIdx.x] = counts[threadIdx.x];
+}
+
+// Exclusive scan of `count` words in place, one block.
+__global__ void __launch_bounds__(kScanThreads) k_scan_exclusive(unsigned* data, int count) {
+    __shared__ unsigned sums[kScanThreads];
+    int per = (count + kScanThreads - 1) / kScanThreads;
+    int begin = threadIdx.x * per;
+    int end = min(count, begin + per);
+    unsigned local = 0;
+    for (int i = begin; i < end; ++i) local += data[i];
+    sums[threadIdx.x] = local;
+    __syncthreads();
+    // Hillis-Steele over the 1024 partial sums.
+    for (int off = 1; off < kScanThreads; off <<= 1) {
+        unsigned v = threadIdx.x >= off ? sums[threadIdx.x - off] : 0;
+        __syncthreads();
+        sums[threadIdx.x] += v;
+        __syncthreads();
+    }
+    unsigned run = sums[threadIdx.x] - local;
+    for (int i = begin; i < end; ++i) {
+        unsigned v = data[i];
+        data[i] = run;
+        run += v;
+    }
+}
+
+// Stable scatter of one tile.  Warp w owns tile keys [w*512, w*512+512), visited in
+// rounds of 32 consecutive keys; a key's rank is (count of its digit in this warp's
+// earlier rounds) + (peers with the same digit in lower lanes), then offset by the same
+// digit's counts in earlier warps and earlier tiles, so equal digits keep input order.
+template <typename Key, bool First>
+__global__ void __launch_bounds__(kThreads) k_sort_downsweep(const Key* keys_in,
+                                                             const int* vals_in, Key* keys_out,
+                                                             int* vals_out, int n, int shift,
+                                                             const unsigned* scanned,
+                                                             int tiles, int* error) {
+    constexpr int kWarps = kThreads / 32;
+    constexpr int kWarpSpan = kSortTile / kWarps;
+    __shared__ unsigned wcount[kWarps][kRadix];
+    __shared__ unsigned gbase[kRadix];
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    for (int i = threadIdx.x; i < kWarps * kRadix; i += kThreads) (&wcount[0][0])[i] = 0;
+    gbase[threadIdx.x] = scanned[threadIdx.x * tiles + blockIdx.x];
+    __syncthreads();
+
+    const unsigned lt = lanemask_lt();
+    const int base = blockIdx.x * kSortTile + warp * kWarpSpan;
+    Key k[kSortItems];
+    int v[kSortItems];
+    unsigned rank[kSortItems];
+#pragma unroll
+    for (int j = 0; j < kSortItems; ++j) {
+        int idx = base + j * 32 + lane;
+        bool valid = idx < n;
+        k[j] = valid ? keys_in[idx] : Key(0);
+        v[j] = First ? idx : (valid ? vals_in[idx] : 0);
+        unsigned d = valid ? digit_of(k[j], shift) : kRadix;
+        unsigned peers = __match_any_sync(0xffffffffu, d);
+        unsigned before = valid ? wcount[warp][d] : 0u;
+        __syncwarp();
+        if (valid && lane == __ffs(peers) - 1) wcount[warp][d] = before + __popc(peers);
+        __syncwarp();
+        rank[j] = valid ? before + __popc(peers & lt) : 0xffffffffu;
+    }
+    __syncthreads();
+    {
+        unsigned run = 0;
+#pragma unroll
+        for (int w = 0; w < kWarps; ++w) {
+            unsigned c = wcount[w][threadIdx.x];
+            wcount[w][threadIdx.x] = run;
+            run += c;
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < kSortItems; ++j) {
+        if (rank[j] == 0xffffffffu) continue;
+        unsigned d = digit_of(k[j], shift);
+        unsigned pos = gbase[d] + wcount[warp][d] + rank[j];
+        if (pos >= static_cast<unsigned>(n)) {  // cannot happen for a consistent histogram
+            atomicOr(error, kErrLoopBound);
+            continue;
+        }
+        keys_out[pos] = k[j];
+        vals_out[pos] = v[j];
+    }
+}
+
+// ---------------------------------------------------------------- 4. Karras hierarchy
+
+LUX_D int clz64(unsigned long long x) { return __clzll(static_cast<long long>(x)); }
+
+// Common-prefix length of sorted keys i and j.  30-bit codes: the reference's merged
+// key (code << 32) | index (bvh/gpu_bvh.cu:66-74).  63-bit codes: the code prefix, and
+// the index prefix beyond it when the codes are equal.
+template <typename Key>
+LUX_D int delta(const Key* codes, int i, int j) {
+    if (sizeof(Key) == 4) {
+        unsigned long long ki = (static_cast<unsigned long long>(codes[i]) << 32) | unsigned(i);
+        unsigned long long kj = (static_cast<unsigned long long>(codes[j]) << 32) | unsigned(j);
+        return clz64(ki ^ kj);
+    } else {
+        unsigned long long x = static_cast<unsigned long long>(codes[i] ^ codes[j]);
+        if (x) return clz64(x);
+        return 64 + __clz(static_cast<int>(unsigned(i) ^ unsigned(j)));
+    }
+}
+
+template <typename Key>
+__global__ void __launch_bounds__(kThreads) k_karras(const Key* codes, int n, BvhNode* nodes,
+                                                     int* node_parent, int* leaf_parent) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n - 1) return;
+    int first, last;
+    if (i == 0) {
+        first = 0;
+        last = n - 1;
+        node_parent[0] = -1;
+    } else {
+        // determine_range (bvh/gpu_bvh.cu:76-105).
+        int dl = delta(codes, i, i - 1);
+        int dr = delta(codes, i, i + 1);
+        int dir = dr > dl ? 1 : -1;
+        int dmin = min(dl, dr);
+        int lmax = 2;
+        for (;;) {
+            int c = i + dir * lmax;
+            if (c < 0 || c >= n) break;
+            if (delta(codes, i, c) <= dmin) break;
+            lmax <<= 1;
+        }
+        int len = 0;
+        for (int step = lmax >> 1; step > 0; step >>= 1) {
+            int c = i + (len + step) * dir;
+            if (c < 0 || c >= n) continue;
+            if (delta(codes, i, c) > dmin) len += step;
+        }
+        int other = i + len * dir;
+        first = dir < 0 ? other : i;
+        last = dir < 0 ? i : other;
+    }
+    // find_split (bvh/gpu_bvh.cu:107-121).
+    int node_delta = delta(codes, first, last);
+    int split = first;
+    int stride = last - first;
+    do {
+        stride = (stride + 1) >> 1;
+        int mid = split + stride;
+        if (mid < last && delta(codes, first, mid) > node_delta) split = mid;
+    } while (stride > 1);
+
+    int left = first == split ? ~split : split;
+    int right = last == split + 1 ? ~(split + 1) : split + 1;
+    reinterpret_cast<int2*>(&nodes[i].ch)[0] = make_int2(left, right);
+    if (left < 0) leaf_parent[split] = i << 1;
+    else node_parent[split] = i << 1;
+    if (right < 0) leaf_parent[split + 1] = (i << 1) | 1;
+    else node_parent[split + 1] = (i << 1) | 1;
+}
+
+// ---------------------------------------------------------------- 5. boxes bottom-up
+
+LUX_D void store_slot(BvhNode* node, int slot, const box3& b) {
+    float* f = reinterpret_cast<float*>(node);
+    if (slot == 0) {
+        __stcg(reinterpret_cast<float4*>(f), make_float4(b.lo.x, b.lo.y, b.lo.z, b.hi.x));
+        __stcg(reinterpret_cast<float2*>(f + 4), make_float2(b.hi.y, b.hi.z));
+    } else {
+        __stcg(reinterpret_cast<float2*>(f + 6), make_float2(b.lo.x, b.lo.y));
+        __stcg(reinterpret_cast<float4*>(f + 8), make_float4(b.lo.z, b.hi.x, b.hi.y, b.hi.z));
+    }
+}
+
+LUX_D box3 load_slot_cg(const BvhNode* node, int slot) {
+    const float* f = reinterpret_cast<const float*>(node);
+    if (slot == 0) {
+        float4 a = __ldcg(reinterpret_cast<const float4*>(f));
+        float2 b = __ldcg(reinterpret_cast<const float2*>(f + 4));
+        return box3{make_f3(a.x, a.y, a.z), make_f3(a.w, b.x, b.y)};
+    }
+    float2 a = __ldcg(reinterpret_cast<const float2*>(f + 6));
+    float4 b = __ldcg(reinterpret_cast<const float4*>(f + 8));
+    return box3{make_f3(a.x, a.y, b.x), make_f3(b.y, b.z, b.w)};
+}
+
+// One thread per sorted leaf.  The leaf box (and, for triangles, the sorted triangle
+// record) is written; then the thread climbs: it stores its box into the parent's
+// slot, and the second of the two children to arrive (atomic counter) unions both
+// slots and continues upward, so every node box is the union of its children's boxes
+// (merge_bounds_kernel, bvh/gpu_bvh.cu:182-214).  The counter is reset by its second
+// arrival, so flags are zero again when the pass ends.
+template <int Kind>
+__global__ void __launch_bounds__(kThreads) k_leaf_climb(const float* prims, int n,
+                                                         const int* sorted_ids,
+                                                         TriRecord* tris, BvhNode* nodes,
+                                                         const int* node_parent,
+                                                         const int* leaf_parent,
+                                                         unsigned* flags, float* root,
+                                                         int* error) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    int pid = sorted_ids[k];
+    if (pid < 0 || pid >= n) {  // cannot happen for a consistent sort
+        atomicOr(error, kErrLoopBound);
+        return;
+    }
+    f3 v0, v1, v2;
+    box3 b;
+    load_prim<Kind>(prims, pid, v0, v1, v2, b);
+    if (Kind == LUX_PRIM_TRIANGLES) {
+        f3 e1 = v1 - v0;
+        f3 e2 = v2 - v0;
+        TriRecord r;
+        r.p0 = make_float4(v0.x, v0.y, v0.z, __int_as_float(pid));
+        r.p1 = make_float4(e1.x, e1.y, e1.z, 0.0f);
+        r.p2 = make_float4(e2.x, e2.y, e2.z, 0.0f);
+        tris[k] = r;
+    }
+    if (n == 1) {
+        root[0] = b.lo.x; root[1] = b.lo.y; root[2] = b.lo.z;
+        root[3] = b.hi.x; root[4] = b.hi.y; root[5] = b.hi.z;
+        return;
+    }
+    int code = leaf_parent[k];
+    for (int level = 0; level < kClimbBound; ++level) {
+        int p = code >> 1;
+        int slot = code & 1;
+        if (code < 0 || p >= n - 1) break;  // parent links out of range: report below
+        store_slot(nodes + p, slot, b);
+        __threadfence();
+        unsigned prior = atomicAdd(flags + p, 1u);
+        if (prior == 0) return;  // the sibling finishes this node
+        flags[p] = 0;
+        __threadfence();
+        box3 sib = load_slot_cg(nodes + p, slot ^ 1);
+        b = slot ? box_union(sib, b) : box_union(b, sib);
+        if (p == 0) {
+            root[0] = b.lo.x; root[1] = b.lo.y; root[2] = b.lo.z;
+            root[3] = b.hi.x; root[4] = b.hi.y; root[5] = b.hi.z;
+            return;
+        }
+        code = node_parent[p];
+    }
+    atomicOr(error, kErrClimbBound);
+}
+
+// ---------------------------------------------------------------- export
+
+// Host tree layout (bvh/cpu_bvh.h:15-32): internal i, then leaf k at n-1+k.
+template <typename Key>
+__global__ void k_export(BvhView v, const Key* codes, unsigned long long* codes64, int* left,
+                         int* right, float* bounds) {
+    int n = v.n;
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n && codes64) codes64[i] = static_cast<unsigned long long>(codes[i]);
+    if (i >= 2 * n - 1) return;
+    box3 b;
+    int l = -1, r = -1;
+    if (i < n - 1) {
+        BvhNode nd = load_node(v.nodes, i);
+        b = box_union(node_left_box(nd), node_right_box(nd));
+        l = nd.ch.x < 0 ? n - 1 + ~nd.ch.x : nd.ch.x;
+        r = nd.ch.y < 0 ? n - 1 + ~nd.ch.y : nd.ch.y;
+    } else {
+        b = leaf_box(v, i - (n - 1));
+    }
+    if (left) left[i] = l;
+    if (right) right[i] = r;
+    if (bounds) {
+        float* o = bounds + static_cast<size_t>(i) * 6;
+        o[0] = b.lo.x; o[1] = b.lo.y; o[2] = b.lo.z;
+        o[3] = b.hi.x; o[4] = b.hi.y; o[5] = b.hi.z;
+    }
+}
+
+int grid_for(int count, int threads = kThreads) { return (count + threads - 1) / threads; }
+
+int stride_grid(const lux_ctx* ctx, int count) {
+    return std::max(1, std::min(grid_for(count), ctx->sm_count * 8));
+}
+
+template <typename Key>
+int radix_sort(lux_ctx* ctx, Key* keys, int* vals, int n, int bits) {
+    int tiles = grid_for(n, kSortTile);
+    size_t key_bytes = (static_cast<size_t>(n) * sizeof(Key) + 255) & ~size_t(255);
+    size_t val_bytes = (static_cast<size_t>(n) * sizeof(int) + 255) & ~size_t(255);
+    size_t hist_bytes = static_cast<size_t>(kRadix) * tiles * sizeof(unsigned);
+    int st = ensure_scratch(ctx, key_bytes + val_bytes + hist_bytes);
+    if (st) return st;
+    char* s = static_cast<char*>(ctx->scratch);
+    Key* keys_alt = reinterpret_cast<Key*>(s);
+    int* vals_alt = reinterpret_cast<int*>(s + key_bytes);
+    unsigned* hist = reinterpret_cast<unsigned*>(s + key_bytes + val_bytes);
+    int passes = (bits + 7) / 8;
+    // Even pass count: the result lands back in (keys, vals).
+    if (passes & 1) ++passes;
+    Key* kin = keys;
+    int* vin = vals;
+    Key* kout = keys_alt;
+    int* vout = vals_alt;
+    for (int p = 0; p < passes; ++p) {
+        int shift = 8 * p;
+        k_sort_upsweep<Key><<<tiles, kThreads, 0, ctx->stream>>>(kin, n, shift, hist, tiles);
+        k_scan_exclusive<<<1, kScanThreads, 0, ctx->stream>>>(hist, kRadix * tiles);
+        if (p == 0) {
+            k_sort_downsweep<Key, true><<<tiles, kThreads, 0, ctx->stream>>>(
+                kin, vin, kout, vout, n, shift, hist, tiles, ctx->d_error);
+        } else {
+            k_sort_downsweep<Key, false><<<tiles, kThreads, 0, ctx->stream>>>(
+                kin, vin, kout, vout, n, shift, hist, tiles, ctx->d_error);
+        }
+        ctx->launches += 3;
+        std::swap(kin, kout);
+        std::swap(vin, vout);
+    }
+    return cuda_fail(cudaGetLastError(), "radix sort");
+}
+
+template <int Kind>
+int climb(lux_ctx* ctx, lux_bvh* bvh, const float* prims) {
+    k_leaf_climb<Kind><<<grid_for(bvh->n), kThreads, 0, ctx->stream>>>(
+        prims, bvh->n, bvh->sorted_ids, bvh->tris, bvh->nodes, bvh->node_parent,
+        bvh->leaf_parent, bvh->flags, bvh->root, ctx->d_error);
+    ctx->launches += 1;
+    return cuda_fail(cudaGetLastError(), "k_leaf_climb");
+}
+
+template <int Kind, typename Key>
+int build_typed(lux_ctx* ctx, lux_bvh* bvh, const float* prims) {
+    int n = bvh->n;
+    Key* codes = static_cast<Key*>(bvh->codes);
+    unsigned* root_ord = reinterpret_cast<unsigned*>(bvh->root + 8);
+    cudaError_t err = cudaMemsetAsync(root_ord, 0xff, 6 * sizeof(unsigned), ctx->stream);
+    if (err != cudaSuccess) return cuda_fail(err, "memset root");
+    k_root_reduce<Kind><<<stride_grid(ctx, n), kThreads, 0, ctx->stream>>>(prims, n, root_ord);
+    k_morton<Kind, Key><<<stride_grid(ctx, n), kThreads, 0, ctx->stream>>>(prims, n, root_ord,
+                                                                           codes);
+    ctx->launches += 2;
+    int st = radix_sort<Key>(ctx, codes, bvh->sorted_ids, n, sizeof(Key) == 4 ? 30 : 63);
+    if (st) return st;
+    if (n == 1) {
+        // A lone leaf has no parent (the storage may hold a larger earlier tree).
+        cudaError_t e = cudaMemsetAsync(bvh->leaf_parent, 0xff, sizeof(int), ctx->stream);
+        if (e != cudaSuccess) return cuda_fail(e, "memset leaf parent");
+    } else {
+        k_karras<Key><<<grid_for(n - 1), kThreads, 0, ctx->stream>>>(
+            codes, n, bvh->nodes, bvh->node_parent, bvh->leaf_parent);
+        ctx->launches += 1;
+    }
+    return climb<Kind>(ctx, bvh, prims);
+}
+
+}  // namespace
+
+size_t lbvh_scratch_bytes(int n, int morton_bits) {
+    size_t key = morton_bits == 63 ? 8 : 4;
+    int tiles = (n + kSortTile - 1) / kSortTile;
+    return ((static_cast<size_t>(n) * key + 255) & ~size_t(255))
+         + ((static_cast<size_t>(n) * 4 + 255) & ~size_t(255))
+         + static_cast<size_t>(kRadix) * tiles * 4;
+}
+
+int lbvh_alloc(lux_ctx* ctx, lux_bvh* bvh) {
+    (void)ctx;
+    bvh->capacity = std::max(bvh->capacity, std::max(bvh->n, 1));
+    int n = bvh->capacity;
+    size_t key = bvh->morton_bits == 63 ? 8 : 4;
+    struct Req {
+        void** ptr;
+        size_t bytes;
+    } reqs[] = {
+        {reinterpret_cast<void**>(&bvh->nodes), sizeof(BvhNode) * std::max(n - 1, 1)},
+        {reinterpret_cast<void**>(&bvh->tris),
+         bvh->kind == LUX_PRIM_TRIANGLES ? sizeof(TriRecord) * n : 16},
+        {reinterpret_cast<void**>(&bvh->sorted_ids), sizeof(int) * n},
+        {reinterpret_cast<void**>(&bvh->leaf_parent), sizeof(int) * n},
+        {reinterpret_cast<void**>(&bvh->node_parent), sizeof(int) * std::max(n - 1, 1)},
+        {reinterpret_cast<void**>(&bvh->flags), sizeof(unsigned) * std::max(n - 1, 1)},
+        {&bvh->codes, key * n},
+        {reinterpret_cast<void**>(&bvh->root), sizeof(float) * 16},
+    };
+    for (auto& r : reqs) {
+        cudaError_t err = cudaMalloc(r.ptr, r.bytes);
+        if (err != cudaSuccess) {
+            cudaGetLastError();
+            lbvh_free(bvh);
+            return fail(LUX_ERR_OUT_OF_MEMORY, "lbvh allocation failed");
+        }
+    }
+    cudaError_t err = cudaMemset(bvh->flags, 0, sizeof(unsigned) * std::max(n - 1, 1));
+    if (err == cudaSuccess) err = cudaMemset(bvh->leaf_parent, 0xff, sizeof(int) * n);
+    return cuda_fail(err, "lbvh init");
+}
+
+void lbvh_free(lux_bvh* bvh) {
+    void* ptrs[] = {bvh->nodes, bvh->tris, bvh->sorted_ids, bvh->leaf_parent, bvh->node_parent,
+                    bvh->flags, bvh->codes, bvh->root};
+    for (void* p : ptrs) {
+        if (p) cudaFree(p);
+    }
+    bvh->nodes = nullptr;
+    bvh->tris = nullptr;
+    bvh->sorted_ids = nullptr;
+    bvh->leaf_parent = nullptr;
+    bvh->node_parent = nullptr;
+    bvh->flags = nullptr;
+    bvh->codes = nullptr;
+    bvh->root = nullptr;
+}
+
+int lbvh_build(lux_ctx* ctx, lux_bvh* bvh, const float* prims) {
+    if (bvh->n <= 0) return LUX_OK;
+    bool wide = bvh->morton_bits == 63;
+    if (bvh->kind == LUX_PRIM_TRIANGLES) {
+        return wide ? build_typed<LUX_PRIM_TRIANGLES, unsigned long long>(ctx, bvh, prims)
+                    : build_typed<LUX_PRIM_TRIANGLES, unsigned>(ctx, bvh, prims);
+    }
+    return wide ? build_typed<LUX_PRIM_AABBS, unsigned long long>(ctx, bvh, prims)
+                : build_typed<LUX_PRIM_AABBS, unsigned>(ctx, bvh, prims);
+}
+
+int lbvh_refit(lux_ctx* ctx, lux_bvh* bvh, const float* prims) {
+    if (bvh->n <= 0) return LUX_OK;
+    return bvh->kind == LUX_PRIM_TRIANGLES ? climb<LUX_PRIM_TRIANGLES>(ctx, bvh, prims)
+                                           : climb<LUX_PRIM_AABBS>(ctx, bvh, prims);
+}
+
+int lbvh_export(lux_ctx* ctx, const lux_bvh* bvh, uint64_t* codes64, int* left, int* right,
+                float* bounds) {
+    int n = bvh->n;
+    if (n <= 0) return LUX_OK;
+    int count = 2 * n - 1;
+    auto* c64 = reinterpret_cast<unsigned long long*>(codes64);
+    if (bvh->morton_bits == 63) {
+        k_export<unsigned long long><<<grid_for(count), kThreads, 0, ctx->stream>>>(
+            bvh->view(), static_cast<const unsigned long long*>(bvh->codes), c64, left, right,
+            bounds);
+    } else {
+        k_export<unsigned><<<grid_for(count), kThreads, 0, ctx->stream>>>(
+            bvh->view(), static_cast<const unsigned*>(bvh->codes), c64, left, right, bounds);
+    }
+    ctx->launches += 1;
+    return cuda_fail(cudaGetLastError(), "k_export");
+}
+
+}  // namespace lux

@@ -1,0 +1,80 @@
+// Device-side LBVH layout shared by the build, refit, traversal and overlap kernels.
+//
+// Internal node i is Karras node i (the same numbering as bvh/gpu_bvh.cu:151-180 and
+// the host tree of bvh/cpu_lbvh_builder.h).  Unlike the reference's 32-byte
+// one-box-per-node stackless records (bvh/bvh_device.cuh:12-17), a node here carries
+// the boxes of BOTH children, so a traversal step tests two boxes per 64-byte fetch
+// and never fetches a leaf node at all.
+#pragma once
+
+#include "lux_math.cuh"
+
+namespace lux {
+
+// Child handle: >= 0 internal node index; < 0 leaf, sorted leaf index k = ~handle.
+LUX_HD bool is_leaf_handle(int h) { return h < 0; }
+
+struct alignas(16) BvhNode {
+    float4 a;  // left.lo.x  left.lo.y  left.lo.z  left.hi.x
+    float4 b;  // left.hi.y  left.hi.z  right.lo.x right.lo.y
+    float4 c;  // right.lo.z right.hi.x right.hi.y right.hi.z
+    int4 ch;   // left handle, right handle, unused, unused
+};
+static_assert(sizeof(BvhNode) == 64, "one node is one 64-byte record");
+
+// Triangle in Morton order: v0, e1 = v1 - v0, e2 = v2 - v0 (the rounded edges the
+// reference's Moller-Trumbore forms), primitive id in p0.w.
+struct alignas(16) TriRecord {
+    float4 p0;  // v0.xyz, primitive id (int bits)
+    float4 p1;  // e1.xyz, 0
+    float4 p2;  // e2.xyz, 0
+};
+
+LUX_HD box3 node_left_box(const BvhNode& n) {
+    return box3{make_f3(n.a.x, n.a.y, n.a.z), make_f3(n.a.w, n.b.x, n.b.y)};
+}
+LUX_HD box3 node_right_box(const BvhNode& n) {
+    return box3{make_f3(n.b.z, n.b.w, n.c.x), make_f3(n.c.y, n.c.z, n.c.w)};
+}
+
+// Non-owning view passed by value into kernels.
+struct BvhView {
+    const BvhNode* nodes = nullptr;     // n - 1 internal nodes
+    const TriRecord* tris = nullptr;    // n triangles in sorted order (triangle BVHs)
+    const int* sorted_ids = nullptr;    // n: input index of sorted leaf k
+    const int* leaf_parent = nullptr;   // n: (parent << 1) | slot, -1 for a lone leaf
+    const float* root = nullptr;        // 6 floats: union of all boxes
+    int n = 0;
+};
+
+LUX_D box3 load_root(const float* root) {
+    return box3{make_f3(root[0], root[1], root[2]), make_f3(root[3], root[4], root[5])};
+}
+
+LUX_D BvhNode load_node(const BvhNode* nodes, int i) {
+    BvhNode n;
+    const float4* p = reinterpret_cast<const float4*>(nodes + i);
+    n.a = __ldg(p + 0);
+    n.b = __ldg(p + 1);
+    n.c = __ldg(p + 2);
+    n.ch = __ldg(reinterpret_cast<const int4*>(p + 3));
+    return n;
+}
+
+// Box of sorted leaf k: the slot its parent stores (for a one-primitive tree, the root).
+LUX_D box3 leaf_box(const BvhView& v, int k) {
+    int code = v.leaf_parent[k];
+    if (code < 0 || (code >> 1) >= v.n - 1) return load_root(v.root);
+    BvhNode p = load_node(v.nodes, code >> 1);
+    return (code & 1) ? node_right_box(p) : node_left_box(p);
+}
+
+// Device error word bits (ctx-owned, read back by the host at synchronisation points).
+enum : int {
+    kErrClimbBound = 1,      // bottom-up pass exceeded its level bound
+    kErrStackOverflow = 2,   // traversal stack overflow
+    kErrLoopBound = 4,       // a bounded loop ran out of iterations
+    kErrQueueOverflow = 8,   // a work queue exceeded capacity
+};
+
+}  // namespace lux

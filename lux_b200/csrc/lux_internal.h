@@ -1,0 +1,76 @@
+// Host-side internals shared by the C-ABI layer and the kernel launchers.
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <cuda_runtime.h>
+
+#include "lux_bvh.cuh"
+
+struct lux_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaStream_t own_stream = nullptr;
+    int sm_count = 148;
+    int* d_error = nullptr;          // device error word (lux::kErr* bits)
+    int64_t launches = 0;            // kernels launched through this context
+    // Growable device scratch, reused across calls on this context.
+    void* scratch = nullptr;
+    size_t scratch_bytes = 0;
+    // Growable device staging for host inputs / outputs.
+    void* staging = nullptr;
+    size_t staging_bytes = 0;
+};
+
+struct lux_bvh {
+    int n = 0;
+    int capacity = 0;       // primitives the device storage can hold
+    int kind = 0;           // LUX_PRIM_TRIANGLES / LUX_PRIM_AABBS
+    int morton_bits = 30;
+    int device = 0;
+    lux::BvhNode* nodes = nullptr;      // n - 1
+    lux::TriRecord* tris = nullptr;     // n (triangle BVHs)
+    int* sorted_ids = nullptr;          // n
+    int* leaf_parent = nullptr;         // n
+    int* node_parent = nullptr;         // n - 1
+    unsigned* flags = nullptr;          // n - 1, zero between passes
+    void* codes = nullptr;              // n sorted codes (uint32 or uint64)
+    float* root = nullptr;              // 6
+    lux::BvhView view() const {
+        lux::BvhView v;
+        v.nodes = nodes;
+        v.tris = tris;
+        v.sorted_ids = sorted_ids;
+        v.leaf_parent = leaf_parent;
+        v.root = root;
+        v.n = n;
+        return v;
+    }
+};
+
+namespace lux {
+
+// Status helpers (defined in capi.cu).
+int fail(int status, const std::string& message);
+int cuda_fail(cudaError_t err, const char* what);
+int ensure_scratch(lux_ctx* ctx, size_t bytes);
+
+// LBVH (lbvh.cu).  prims are device pointers.
+int lbvh_alloc(lux_ctx* ctx, lux_bvh* bvh);
+int lbvh_build(lux_ctx* ctx, lux_bvh* bvh, const float* prims);
+int lbvh_refit(lux_ctx* ctx, lux_bvh* bvh, const float* prims);
+void lbvh_free(lux_bvh* bvh);
+int lbvh_export(lux_ctx* ctx, const lux_bvh* bvh, uint64_t* codes64, int* left, int* right,
+                float* bounds);
+size_t lbvh_scratch_bytes(int n, int morton_bits);
+
+// Queries (traverse.cu).  All pointers are device pointers.
+int trace_closest(lux_ctx* ctx, const lux_bvh* bvh, const float* rays, int nrays, int* hit_id,
+                  float* hit_t);
+int trace_any(lux_ctx* ctx, const lux_bvh* bvh, const float* rays, int nrays, int* hit_id);
+int trace_stats(lux_ctx* ctx, const lux_bvh* bvh, const float* rays, int nrays,
+                unsigned long long* totals);
+int overlap(lux_ctx* ctx, const lux_bvh* tree, const lux_bvh* queries, bool self, int* pairs,
+            int64_t max_pairs, unsigned long long* d_found);
+
+}  // namespace lux

@@ -1,0 +1,282 @@
+// Ray traversal (closest hit, any hit) and box-overlap queries over the LBVH.
+//
+// Closest hit reproduces the reference's stackless walk (bvh/bvh_device.cuh:43-90)
+// decision for decision, at half the node fetches:
+//   * nodes are visited left child first, so the visit order is the reference's
+//     preorder and equal-t ties keep the first triangle found;
+//   * both child boxes are tested when their parent is fetched; a right child that is
+//     deferred keeps its slab entry distance tn, and when popped it is skipped iff
+//     tn > best_t, which is exactly the reference's slab verdict for that node under
+//     the t_max current at its visit (its t_max-free part was already checked);
+//   * triangles pass iff t_min < t < best_t (strict, as geometry/triangle.h:51).
+// Overlap queries follow bvh/bvh_overlap.cu:25-184 (self pairs a < b; cross pairs
+// (left, right)), with warp-aggregated appends instead of a block-wide staging loop.
+
+#include <cuda_runtime.h>
+
+#include "../../include/lux_gpu.h"
+#include "lux_internal.h"
+
+namespace lux {
+namespace {
+
+constexpr int kTraceThreads = 128;
+constexpr int kStack = 96;  // > max Karras depth: 64 (30-bit keys) or 95 (63-bit + index)
+
+struct RayHit {
+    int k;      // sorted leaf index of the best hit, -1 none
+    float t;
+};
+
+LUX_D ray3 load_ray(const float4* rays, int i) {
+    float4 a = __ldg(rays + 2 * i);
+    float4 b = __ldg(rays + 2 * i + 1);
+    return ray3{make_f3(a.x, a.y, a.z), a.w, make_f3(b.x, b.y, b.z), b.w};
+}
+
+struct TraceCounts {
+    unsigned boxes = 0;
+    unsigned tris = 0;
+};
+
+template <bool AnyHit, bool Count = false>
+LUX_D RayHit trace_one(const BvhView& bvh, const ray3& ray, int* error,
+                       TraceCounts* counts = nullptr) {
+    RayHit best{-1, ray.tmax};
+    if (bvh.n <= 0) return best;
+    slab_ray sr = make_slab_ray(ray);
+    float tn;
+    if (Count) counts->boxes += 1;
+    if (!slab_hit(sr, load_root(bvh.root), best.t, tn)) return best;
+
+    int stack_h[kStack];
+    float stack_t[kStack];
+    int sp = 0;
+    int cur = bvh.n == 1 ? ~0 : 0;
+    // A tree visit touches each node at most once: 2n steps bound any correct walk.
+    const long long bound = 2ll * bvh.n + 64;
+    for (long long step = 0;; ++step) {
+        if (step > bound || cur >= bvh.n - 1 || ~cur >= bvh.n) {
+            atomicOr(error, kErrLoopBound);
+            return RayHit{-1, ray.tmax};
+        }
+        if (cur >= 0) {
+            BvhNode nd = load_node(bvh.nodes, cur);
+            float tl, tr;
+            if (Count) counts->boxes += 2;
+            bool hl = slab_hit(sr, node_left_box(nd), best.t, tl);
+            bool hr = slab_hit(sr, node_right_box(nd), best.t, tr);
+            if (hl) {
+                if (hr) {
+                    if (sp < kStack) {
+                        stack_h[sp] = nd.ch.y;
+                        stack_t[sp] = tr;
+                        ++sp;
+                    } else {
+                        atomicOr(error, kErrStackOverflow);
+                        return RayHit{-1, ray.tmax};
+                    }
+                }
+                cur = nd.ch.x;
+                continue;
+            }
+            if (hr) {
+                cur = nd.ch.y;
+                continue;
+            }
+        } else {
+            int k = ~cur;
+            const float4* tp = reinterpret_cast<const float4*>(bvh.tris + k);
+            float4 p0 = __ldg(tp);
+            float4 p1 = __ldg(tp + 1);
+            float4 p2 = __ldg(tp + 2);
+            float t, u, v;
+            if (Count) counts->tris += 1;
+            if (moller_trumbore(ray.o, ray.d, make_f3(p0.x, p0.y, p0.z),
+                                make_f3(p1.x, p1.y, p1.z), make_f3(p2.x, p2.y, p2.z), t, u, v)
+                && t > ray.tmin && t < best.t) {
+                best.k = k;
+                best.t = t;
+                if (AnyHit) return best;
+            }
+        }
+        // Pop the next deferred right child that still passes under the current best.
+        bool resumed = false;
+        while (sp > 0) {
+            --sp;
+            if (!(stack_t[sp] > best.t)) {
+                cur = stack_h[sp];
+                resumed = true;
+                break;
+            }
+        }
+        if (!resumed) break;
+    }
+    return best;
+}
+
+template <bool AnyHit>
+__global__ void __launch_bounds__(kTraceThreads) k_trace(BvhView bvh, const float4* rays,
+                                                         int nrays, int* hit_id, float* hit_t,
+                                                         int* error) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nrays) return;
+    ray3 ray = load_ray(rays, i);
+    RayHit h = trace_one<AnyHit>(bvh, ray, error);
+    int id = -1;
+    if (h.k >= 0) id = __float_as_int(__ldg(reinterpret_cast<const float*>(bvh.tris + h.k) + 3));
+    hit_id[i] = id;
+    if (hit_t) hit_t[i] = h.k >= 0 ? h.t : INFINITY;
+}
+
+// Totals of box and triangle tests over all rays (one atomic pair per warp).
+__global__ void __launch_bounds__(kTraceThreads) k_trace_stats(BvhView bvh, const float4* rays,
+                                                               int nrays,
+                                                               unsigned long long* totals,
+                                                               int* error) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    TraceCounts c;
+    if (i < nrays) {
+        ray3 ray = load_ray(rays, i);
+        trace_one<false, true>(bvh, ray, error, &c);
+    }
+    unsigned long long b = c.boxes, t = c.tris;
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+        b += __shfl_xor_sync(0xffffffffu, b, off);
+        t += __shfl_xor_sync(0xffffffffu, t, off);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicAdd(totals, b);
+        atomicAdd(totals + 1, t);
+    }
+}
+
+// ---------------------------------------------------------------- overlap
+
+LUX_D bool boxes_overlap(const box3& a, const box3& b) {
+    // AABB::overlaps (core/aabb.cuh:68-72).
+    return !(b.lo.x > a.hi.x || b.hi.x < a.lo.x || b.lo.y > a.hi.y || b.hi.y < a.lo.y
+             || b.lo.z > a.hi.z || b.hi.z < a.lo.z);
+}
+
+// Append one pair; the lanes that append in the same step share one atomic.
+LUX_D void append_pair(int a, int b, int* pairs, long long max_pairs,
+                       unsigned long long* counter) {
+    unsigned active = __activemask();
+    int lane = threadIdx.x & 31;
+    int leader = __ffs(active) - 1;
+    unsigned long long base = 0;
+    if (lane == leader) base = atomicAdd(counter, static_cast<unsigned long long>(__popc(active)));
+    base = __shfl_sync(active, base, leader);
+    unsigned lt;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(lt));
+    unsigned long long slot = base + __popc(active & lt);
+    if (slot < static_cast<unsigned long long>(max_pairs)) {
+        reinterpret_cast<int2*>(pairs)[slot] = make_int2(a, b);
+    }
+}
+
+// One thread per query leaf (sorted order of the query tree).  self: the query tree is
+// the tree itself and only partners with a larger primitive id are reported.
+template <bool Self>
+__global__ void __launch_bounds__(kTraceThreads) k_overlap(BvhView tree, BvhView queries,
+                                                           int* pairs, long long max_pairs,
+                                                           unsigned long long* counter,
+                                                           int* error) {
+    int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= queries.n || tree.n <= 0) return;
+    box3 qb = leaf_box(queries, q);
+    int qid = queries.sorted_ids[q];
+    if (!boxes_overlap(load_root(tree.root), qb)) return;
+    int stack[kStack];
+    int sp = 0;
+    int cur = tree.n == 1 ? ~0 : 0;
+    const long long bound = 2ll * tree.n + 64;
+    for (long long step = 0;; ++step) {
+        if (step > bound || cur >= tree.n - 1 || ~cur >= tree.n) {
+            atomicOr(error, kErrLoopBound);
+            return;
+        }
+        if (cur >= 0) {
+            BvhNode nd = load_node(tree.nodes, cur);
+            bool hl = boxes_overlap(node_left_box(nd), qb);
+            bool hr = boxes_overlap(node_right_box(nd), qb);
+            if (hl) {
+                if (hr) {
+                    if (sp < kStack) {
+                        stack[sp++] = nd.ch.y;
+                    } else {
+                        atomicOr(error, kErrStackOverflow);
+                        return;
+                    }
+                }
+                cur = nd.ch.x;
+                continue;
+            }
+            if (hr) {
+                cur = nd.ch.y;
+                continue;
+            }
+        } else {
+            int pid = tree.sorted_ids[~cur];
+            if (!Self || pid > qid) {
+                if (Self) append_pair(qid, pid, pairs, max_pairs, counter);
+                else append_pair(pid, qid, pairs, max_pairs, counter);
+            }
+        }
+        if (sp == 0) break;
+        cur = stack[--sp];
+    }
+}
+
+}  // namespace
+
+int trace_closest(lux_ctx* ctx, const lux_bvh* bvh, const float* rays, int nrays, int* hit_id,
+                  float* hit_t) {
+    if (nrays <= 0) return LUX_OK;
+    int grid = (nrays + kTraceThreads - 1) / kTraceThreads;
+    k_trace<false><<<grid, kTraceThreads, 0, ctx->stream>>>(
+        bvh->view(), reinterpret_cast<const float4*>(rays), nrays, hit_id, hit_t, ctx->d_error);
+    ctx->launches += 1;
+    return cuda_fail(cudaGetLastError(), "k_trace closest");
+}
+
+int trace_any(lux_ctx* ctx, const lux_bvh* bvh, const float* rays, int nrays, int* hit_id) {
+    if (nrays <= 0) return LUX_OK;
+    int grid = (nrays + kTraceThreads - 1) / kTraceThreads;
+    k_trace<true><<<grid, kTraceThreads, 0, ctx->stream>>>(
+        bvh->view(), reinterpret_cast<const float4*>(rays), nrays, hit_id, nullptr,
+        ctx->d_error);
+    ctx->launches += 1;
+    return cuda_fail(cudaGetLastError(), "k_trace any");
+}
+
+int trace_stats(lux_ctx* ctx, const lux_bvh* bvh, const float* rays, int nrays,
+                unsigned long long* totals) {
+    if (nrays <= 0) return LUX_OK;
+    int grid = (nrays + kTraceThreads - 1) / kTraceThreads;
+    k_trace_stats<<<grid, kTraceThreads, 0, ctx->stream>>>(
+        bvh->view(), reinterpret_cast<const float4*>(rays), nrays, totals, ctx->d_error);
+    ctx->launches += 1;
+    return cuda_fail(cudaGetLastError(), "k_trace_stats");
+}
+
+int overlap(lux_ctx* ctx, const lux_bvh* tree, const lux_bvh* queries, bool self, int* pairs,
+            int64_t max_pairs, unsigned long long* d_found) {
+    cudaError_t err = cudaMemsetAsync(d_found, 0, sizeof(unsigned long long), ctx->stream);
+    if (err != cudaSuccess) return cuda_fail(err, "overlap counter");
+    if (queries->n <= 0 || tree->n <= 0) return LUX_OK;
+    int grid = (queries->n + kTraceThreads - 1) / kTraceThreads;
+    if (self) {
+        k_overlap<true><<<grid, kTraceThreads, 0, ctx->stream>>>(
+            tree->view(), queries->view(), pairs, max_pairs, d_found, ctx->d_error);
+    } else {
+        k_overlap<false><<<grid, kTraceThreads, 0, ctx->stream>>>(
+            tree->view(), queries->view(), pairs, max_pairs, d_found, ctx->d_error);
+    }
+    ctx->launches += 1;
+    return cuda_fail(cudaGetLastError(), "k_overlap");
+}
+
+}  // namespace lux

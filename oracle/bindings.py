@@ -1,0 +1,193 @@
+"""ctypes bindings of the oracle libraries -- test infrastructure only.
+
+* Oracle: the plain-C restatement (oracle/lux_oracle.c -> oracle/liblux_oracle.so).
+* Ref: the reference's own host code (oracle/_ref/libluxref.so, built from the reference
+  sources by oracle/build.py; present wherever it was built).
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use this module.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_LIB = os.path.join(HERE, "liblux_oracle.so")
+REF_LIB = os.path.join(HERE, "_ref", "libluxref.so")
+
+_P = ctypes.c_void_p
+_I = ctypes.c_int
+_I64 = ctypes.c_int64
+
+
+def _addr(a):
+    return None if a is None else a.ctypes.data
+
+
+class Oracle:
+    def __init__(self, path: str = ORACLE_LIB):
+        if not os.path.exists(path):
+            raise FileNotFoundError(f"{path} missing: run `python oracle/build.py`")
+        lib = ctypes.CDLL(path)
+        lib.orc_triangle_bounds.argtypes = [_P, _I, _P]
+        lib.orc_root_bounds.argtypes = [_P, _I, _P]
+        lib.orc_morton30.argtypes = [_P, _I, _P, _P]
+        lib.orc_morton63.argtypes = [_P, _I, _P, _P]
+        lib.orc_stable_order.argtypes = [_P, _I, _P]
+        lib.orc_lbvh_build.argtypes = [_P, _I, _I, _P, _P, _P, _P, _P, _P]
+        lib.orc_lbvh_build.restype = _I
+        lib.orc_trace.argtypes = [_P, _P, _P, _P, _I, _P, _I, _I, _I, _P, _P, _P]
+        lib.orc_overlap.argtypes = [_P, _P, _P, _I, _P, _I, _I, _P, _I64]
+        lib.orc_overlap.restype = _I64
+        self.lib = lib
+
+    def triangle_bounds(self, tris: np.ndarray) -> np.ndarray:
+        tris = np.ascontiguousarray(tris, np.float32)
+        n = tris.size // 9
+        out = np.empty((n, 6), np.float32)
+        self.lib.orc_triangle_bounds(tris.ctypes.data, n, out.ctypes.data)
+        return out
+
+    def build(self, bounds: np.ndarray, morton_bits: int = 30) -> dict:
+        bounds = np.ascontiguousarray(bounds, np.float32)
+        n = bounds.size // 6
+        count = max(2 * n - 1, 0)
+        out = {
+            "sorted_codes": np.zeros(n, np.uint64),
+            "sorted_ids": np.zeros(n, np.int32),
+            "child": np.zeros(max(2 * (n - 1), 1), np.uint32),
+            "node_left": np.zeros(count, np.int32),
+            "node_right": np.zeros(count, np.int32),
+            "node_bounds": np.zeros((count, 6), np.float32),
+        }
+        if n:
+            self.lib.orc_lbvh_build(bounds.ctypes.data, n, morton_bits,
+                                    out["sorted_codes"].ctypes.data,
+                                    out["sorted_ids"].ctypes.data, out["child"].ctypes.data,
+                                    out["node_left"].ctypes.data,
+                                    out["node_right"].ctypes.data,
+                                    out["node_bounds"].ctypes.data)
+        out["n"] = n
+        return out
+
+    def trace(self, tris: np.ndarray, tree: dict, rays: np.ndarray, any_hit: bool = False,
+              ignored: int = -1, stats: bool = False):
+        tris = np.ascontiguousarray(tris, np.float32)
+        rays = np.ascontiguousarray(rays, np.float32)
+        nrays = rays.size // 8
+        hit_id = np.empty(nrays, np.int32)
+        hit_t = np.empty(nrays, np.float32)
+        st = np.zeros((nrays, 2), np.int64) if stats else None
+        self.lib.orc_trace(tris.ctypes.data, tree["node_bounds"].ctypes.data,
+                           tree["child"].ctypes.data, tree["sorted_ids"].ctypes.data,
+                           tree["n"], rays.ctypes.data, nrays, int(any_hit), ignored,
+                           hit_id.ctypes.data, hit_t.ctypes.data, _addr(st))
+        return (hit_id, hit_t, st) if stats else (hit_id, hit_t)
+
+    def overlap(self, tree: dict, queries: np.ndarray, self_pairs: bool,
+                max_pairs: int = 1 << 24):
+        queries = np.ascontiguousarray(queries, np.float32)
+        nq = queries.size // 6
+        pairs = np.zeros((max_pairs, 2), np.int32)
+        found = self.lib.orc_overlap(tree["node_bounds"].ctypes.data, tree["child"].ctypes.data,
+                                     tree["sorted_ids"].ctypes.data, tree["n"],
+                                     queries.ctypes.data, nq, int(self_pairs),
+                                     pairs.ctypes.data, max_pairs)
+        return pairs[:min(found, max_pairs)], found
+
+
+class Ref:
+    """The reference's own host code."""
+
+    def __init__(self, path: str = REF_LIB):
+        if not os.path.exists(path):
+            raise FileNotFoundError(f"{path} missing (built only where the reference exists)")
+        lib = ctypes.CDLL(path)
+        lib.ref_lbvh_build.argtypes = [_P, _I, _I, _P, _P, _P, _P, _P]
+        lib.ref_lbvh_build.restype = _I
+        lib.ref_build_and_trace.argtypes = [_P, _I, _P, _I, _I, _I, _P, _P]
+        lib.ref_cornell_scene.argtypes = [_I, _I, _P, _P, _P, _P]
+        lib.ref_cornell_scene.restype = _I
+        lib.ref_cornell_render.argtypes = [_I, _I, _I, _I, ctypes.c_uint64, _I, _I, _I,
+                                           _P, _P, _P]
+        lib.ref_tree_create.argtypes = [_P, _I, _I]
+        lib.ref_tree_create.restype = _P
+        lib.ref_tree_destroy.argtypes = [_P]
+        lib.ref_tree_trace.argtypes = [_P, _P, _I, _I, _P, _P]
+        self.lib = lib
+
+    def tree_create(self, prims: np.ndarray, kind: int = 0):
+        """Builds and keeps a host tree (build_cpu_lbvh_tree); returns an opaque handle."""
+        prims = np.ascontiguousarray(prims, np.float32)
+        n = prims.size // (9 if kind == 0 else 6)
+        return self.lib.ref_tree_create(prims.ctypes.data, n, kind)
+
+    def tree_destroy(self, handle) -> None:
+        self.lib.ref_tree_destroy(handle)
+
+    def tree_trace(self, handle, rays: np.ndarray, threads: int = 1):
+        """Closest hit through intersect_cpu_bvh_tree on a kept tree."""
+        rays = np.ascontiguousarray(rays, np.float32)
+        nrays = rays.size // 8
+        hit_id = np.empty(nrays, np.int32)
+        hit_t = np.empty(nrays, np.float32)
+        self.lib.ref_tree_trace(handle, rays.ctypes.data, nrays, threads, hit_id.ctypes.data,
+                                hit_t.ctypes.data)
+        return hit_id, hit_t
+
+    @staticmethod
+    def available(path: str = REF_LIB) -> bool:
+        return os.path.exists(path)
+
+    def lbvh_build(self, prims: np.ndarray, kind: int = 0) -> dict:
+        prims = np.ascontiguousarray(prims, np.float32)
+        n = prims.size // (9 if kind == 0 else 6)
+        count = max(2 * n - 1, 0)
+        out = {
+            "sorted_codes": np.zeros(n, np.uint32),
+            "sorted_ids": np.zeros(n, np.int32),
+            "node_left": np.zeros(count, np.int32),
+            "node_right": np.zeros(count, np.int32),
+            "node_bounds": np.zeros((count, 6), np.float32),
+        }
+        if n:
+            self.lib.ref_lbvh_build(prims.ctypes.data, n, kind, out["sorted_codes"].ctypes.data,
+                                    out["sorted_ids"].ctypes.data, out["node_left"].ctypes.data,
+                                    out["node_right"].ctypes.data,
+                                    out["node_bounds"].ctypes.data)
+        return out
+
+    def build_and_trace(self, tris: np.ndarray, rays: np.ndarray, gpu_order: bool = True,
+                        threads: int = 1):
+        tris = np.ascontiguousarray(tris, np.float32)
+        rays = np.ascontiguousarray(rays, np.float32)
+        nrays = rays.size // 8
+        hit_id = np.empty(nrays, np.int32)
+        hit_t = np.empty(nrays, np.float32)
+        self.lib.ref_build_and_trace(tris.ctypes.data, tris.size // 9, rays.ctypes.data, nrays,
+                                     0 if gpu_order else 1, threads, hit_id.ctypes.data,
+                                     hit_t.ctypes.data)
+        return hit_id, hit_t
+
+    def cornell_scene(self, width: int = 256, height: int = 256) -> dict:
+        tris = np.zeros((64, 9), np.float32)
+        mids = np.zeros(64, np.int32)
+        mats = np.zeros((16, 7), np.float32)
+        cam = np.zeros(12, np.float32)
+        n = self.lib.ref_cornell_scene(width, height, tris.ctypes.data, mids.ctypes.data,
+                                       mats.ctypes.data, cam.ctypes.data)
+        nm = int(mids[:n].max()) + 1
+        return {"triangles": tris[:n], "material_ids": mids[:n], "materials": mats[:nm],
+                "camera": cam.reshape(4, 3)}
+
+    def cornell_render(self, width: int, height: int, spp: int, max_depth: int, seed: int,
+                       rows=None, threads: int = 1, samples: bool = False):
+        y0, y1 = rows if rows is not None else (0, height)
+        total = np.zeros((height * width, 3), np.float32)
+        total2 = np.zeros((height * width, 3), np.float32)
+        smp = np.zeros(((y1 - y0) * width, spp, 3), np.float32) if samples else None
+        self.lib.ref_cornell_render(width, height, spp, max_depth, seed, y0, y1, threads,
+                                    total.ctypes.data, total2.ctypes.data, _addr(smp))
+        return (total, total2, smp) if samples else (total, total2)

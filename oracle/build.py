@@ -1,0 +1,71 @@
+"""Build recipes for the oracle (test infrastructure; nothing in the product loads these).
+
+1. oracle/liblux_oracle.so: the plain-C restatement in oracle/lux_oracle.c.
+2. oracle/_ref/libluxref.so: the reference's own host code.
+
+Compiles, in place and without the reference's build system, the handful of
+reference translation units the CPU path needs (integrator/cpu_path_tracer.cpp,
+light/light_distribution.cpp, scene/prepared_scene_cpu.cpp; everything else on the
+path is header-only) together with oracle/ref_harness.cpp.  Output goes only to
+oracle/_ref/.  Test infrastructure: nothing in the product loads this library.
+"""
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF_ROOT = os.environ.get("LUX_REFERENCE_ROOT", "/root/reference")
+OUT_DIR = os.path.join(HERE, "_ref")
+OUT = os.path.join(OUT_DIR, "libluxref.so")
+ORACLE_OUT = os.path.join(HERE, "liblux_oracle.so")
+
+REF_SOURCES = [
+    "src/integrator/cpu_path_tracer.cpp",
+    "src/light/light_distribution.cpp",
+    "src/scene/prepared_scene_cpu.cpp",
+]
+
+# The reference's Release configuration: -O3, x86-64 baseline ISA (SSE2, so no FMA
+# contraction is possible), IEEE semantics (no -ffast-math).
+CXXFLAGS = ["-std=c++20", "-O3", "-fPIC", "-ffp-contract=off", "-pthread"]
+
+
+def _stale(out, inputs):
+    if not os.path.exists(out):
+        return True
+    return os.path.getmtime(out) < max(os.path.getmtime(p) for p in inputs)
+
+
+def build_oracle(force=False):
+    """Compile the C restatement (single precision, no contraction)."""
+    srcs = [os.path.join(HERE, "lux_oracle.c")]
+    if force or _stale(ORACLE_OUT, srcs):
+        cmd = ["gcc", "-std=c11", "-O2", "-fPIC", "-shared", "-ffp-contract=off",
+               "-o", ORACLE_OUT, *srcs, "-lm"]
+        subprocess.run(cmd, check=True)
+    return ORACLE_OUT
+
+
+def build_ref(force=False):
+    """Compile the reference harness; returns None when the reference is absent."""
+    src_dir = os.path.join(REF_ROOT, "src")
+    if not os.path.isdir(src_dir):
+        return None
+    harness = os.path.join(HERE, "ref_harness.cpp")
+    inputs = [harness] + [os.path.join(REF_ROOT, s) for s in REF_SOURCES]
+    if not force and not _stale(OUT, inputs):
+        return OUT
+    os.makedirs(OUT_DIR, exist_ok=True)
+    cmd = ["g++", *CXXFLAGS, "-shared", "-I", src_dir, "-o", OUT, *inputs]
+    subprocess.run(cmd, check=True)
+    return OUT
+
+
+def build(force=False):
+    return build_oracle(force), build_ref(force)
+
+
+if __name__ == "__main__":
+    oracle_path, ref_path = build(force="--force" in sys.argv)
+    print(oracle_path)
+    print(ref_path if ref_path else "reference sources not present; reference harness not built")

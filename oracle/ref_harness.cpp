@@ -1,0 +1,368 @@
+// Test infrastructure only: a C-ABI harness around the reference's OWN host code,
+// compiled from the reference sources in place (see oracle/build.py) into
+// oracle/_ref/libluxref.so.  Nothing in the product links or loads this file; the
+// tests use it to pin the oracle restatement (oracle/lux_oracle.c) and bench.py
+// times it as the reference CPU arm.
+//
+// Reference entry points exercised (paths relative to the reference's src/):
+//   build_cpu_lbvh_tree            bvh/cpu_lbvh_builder.h:163-259
+//   lbvh_detail::centroid_to_morton bvh/cpu_lbvh_builder.h:55-61
+//   intersect_cpu_bvh_tree         bvh/cpu_bvh_traversal.h:84-95 (CPU stack order)
+//   intersect_bvh_device_impl      bvh/bvh_device.cuh:43-90 (GPU stackless order; the
+//                                  header is host-compilable because its device
+//                                  qualifiers collapse to `inline` outside nvcc)
+//   make_cornell_box               scene/cornell_box.h:31-56
+//   make_pinhole_camera            camera/pinhole_camera.h:13-17 (camera of
+//                                  app/render_runner.cpp:85-90)
+//   trace_path                     integrator/cpu_path_tracer.cpp:403-498
+//   make_render_sampler            integrator/render_context.h:45-54
+//
+// The stackless node array that intersect_bvh_device_impl walks is produced here
+// from the host tree by a plain preorder walk (left child first, escape = the node
+// after the subtree), which is the layout bvh/gpu_bvh.cu:241-363 computes on device.
+
+#include <algorithm>
+#include <cstdint>
+#include <cstring>
+#include <thread>
+#include <vector>
+
+#include "bvh/bvh_build_input.h"
+#include "bvh/bvh_device.cuh"
+#include "bvh/cpu_bvh_traversal.h"
+#include "bvh/cpu_lbvh_builder.h"
+#include "camera/pinhole_camera.h"
+#include "integrator/cpu_path_tracer.h"
+#include "integrator/render_context.h"
+#include "scene/cornell_box.h"
+#include "scene/prepared_scene.h"
+#include "scene/scene_light_sampler.h"
+
+namespace {
+
+std::vector<BvhBuildPrimitive> make_primitives(const float* prims, int n, int kind) {
+    std::vector<BvhBuildPrimitive> out;
+    out.reserve(n);
+    for (int i = 0; i < n; ++i) {
+        AABB bounds;
+        if (kind == 0) {
+            const float* t = prims + size_t(i) * 9;
+            Triangle tri{vec3(t[0], t[1], t[2]), vec3(t[3], t[4], t[5]), vec3(t[6], t[7], t[8])};
+            bounds = triangle_bounds(tri);
+        } else {
+            const float* b = prims + size_t(i) * 6;
+            bounds = AABB(vec3(b[0], b[1], b[2]), vec3(b[3], b[4], b[5]));
+        }
+        out.push_back(BvhBuildPrimitive{bounds, bounds.centroid(), i, -1, -1, i,
+                                        PrimitiveKind::Triangle});
+    }
+    return out;
+}
+
+std::vector<Triangle> make_triangles(const float* tris, int n) {
+    std::vector<Triangle> out(n);
+    for (int i = 0; i < n; ++i) {
+        const float* t = tris + size_t(i) * 9;
+        out[i] = Triangle{vec3(t[0], t[1], t[2]), vec3(t[3], t[4], t[5]), vec3(t[6], t[7], t[8])};
+    }
+    return out;
+}
+
+// Ray record of include/lux_gpu.h: origin.xyz, t_min, direction.xyz, t_max.
+Ray make_ray(const float* r) {
+    return Ray(vec3(r[0], r[1], r[2]), vec3(r[4], r[5], r[6]), r[3], r[7]);
+}
+
+// Preorder (left first) flattening of the host tree into the 32-byte stackless records.
+void flatten_preorder(const CpuBvhTree& tree, std::vector<GpuBvhNode>& out) {
+    out.assign(tree.nodes.size(), GpuBvhNode{});
+    std::vector<int> subtree(tree.nodes.size(), 1);
+    // Children always have larger indices in the host layout? Not guaranteed, so
+    // compute subtree sizes with an explicit post-order walk.
+    std::vector<std::pair<int, int>> stack;  // (node, state)
+    stack.push_back({tree.root_node, 0});
+    while (!stack.empty()) {
+        auto [node, state] = stack.back();
+        stack.pop_back();
+        const CpuBvhNode& nd = tree.nodes[node];
+        if (nd.is_leaf()) { subtree[node] = 1; continue; }
+        if (state == 0) {
+            stack.push_back({node, 1});
+            stack.push_back({nd.right, 0});
+            stack.push_back({nd.left, 0});
+        } else {
+            subtree[node] = 1 + subtree[nd.left] + subtree[nd.right];
+        }
+    }
+    int total = static_cast<int>(tree.nodes.size());
+    std::vector<std::pair<int, int>> walk;  // (node, preorder slot)
+    walk.push_back({tree.root_node, 0});
+    while (!walk.empty()) {
+        auto [node, pre] = walk.back();
+        walk.pop_back();
+        const CpuBvhNode& nd = tree.nodes[node];
+        int next = pre + subtree[node];
+        GpuBvhNode rec;
+        rec.bounds = nd.bounds;
+        rec.escape = next < total ? next : -1;
+        if (nd.is_leaf()) {
+            rec.primitive_id = tree.primitive_ids[nd.first_primitive];
+        } else {
+            rec.primitive_id = -1;
+            walk.push_back({nd.right, pre + 1 + subtree[nd.left]});
+            walk.push_back({nd.left, pre + 1});
+        }
+        out[pre] = rec;
+    }
+}
+
+template <typename Fn>
+void parallel_for(int count, int threads, Fn fn) {
+    threads = std::max(1, threads);
+    if (threads == 1 || count < 2 * threads) {
+        fn(0, count);
+        return;
+    }
+    std::vector<std::thread> pool;
+    int chunk = (count + threads - 1) / threads;
+    for (int t = 0; t < threads; ++t) {
+        int begin = t * chunk;
+        int end = std::min(count, begin + chunk);
+        if (begin >= end) break;
+        pool.emplace_back([=]() { fn(begin, end); });
+    }
+    for (auto& th : pool) th.join();
+}
+
+struct CornellSetup {
+    PreparedScene prepared;
+    SceneLightSampler lights;
+    explicit CornellSetup(int width, int height)
+        : prepared(make_scene(width, height)),
+          lights(make_scene_light_sampler(prepared.host_scene(), prepared.light_sampling(),
+                                          LightSamplerKind::Power)) {
+        prepared.prepare_host_bvh();
+    }
+    static Scene make_scene(int width, int height) {
+        Scene scene = make_cornell_box();
+        scene.camera = make_pinhole_camera(vec3(0, 1, 3.35f), vec3(0, 1, 0.9f), 40.0f,
+                                           Float(width) / Float(height));
+        return scene;
+    }
+};
+
+// One camera sample through the reference loop body of
+// integrator/cpu_path_tracer.cpp:525-558 (same draw order: jitter x, jitter y, lens 2D, time).
+vec3 reference_sample(const CornellSetup& setup, const RenderSettings& settings,
+                      int width, int height, int x, int y, int s) {
+    const Scene& scene = setup.prepared.host_scene();
+    int pixel = y * width + x;
+    SamplerState sampler = make_render_sampler(settings, pixel, s);
+    Float jx = sampler_get_1d(sampler);
+    Float jy = sampler_get_1d(sampler);
+    Float u = (Float(x) + jx) / Float(width);
+    Float v = (Float(height - 1 - y) + jy) / Float(height);
+    CameraSample cs;
+    cs.p_film = vec2(u, v);
+    cs.p_lens = sampler_get_2d(sampler);
+    cs.time = sampler_get_1d(sampler);
+    CameraRay generated = generate_camera_ray(scene.camera, cs);
+    if (!generated.valid) return vec3(0);
+    return trace_path(scene, setup.prepared.host_bvh(), setup.lights, generated.ray, sampler,
+                      settings.max_depth);
+}
+
+}  // namespace
+
+extern "C" {
+
+int ref_lbvh_build(const float* prims, int n, int kind, uint32_t* sorted_codes,
+                   int32_t* sorted_prim_ids, int32_t* node_left, int32_t* node_right,
+                   float* node_bounds) {
+    if (n <= 0) return 0;
+    std::vector<BvhBuildPrimitive> primitives = make_primitives(prims, n, kind);
+    AABB scene_bounds;
+    for (const auto& p : primitives) scene_bounds.expand(p.bounds);
+    CpuBvhTree tree = build_cpu_lbvh_tree(primitives);
+    for (int i = 0; i < n; ++i) {
+        int id = tree.primitive_ids[i];
+        sorted_prim_ids[i] = id;
+        if (sorted_codes) {
+            sorted_codes[i] = n == 1 ? 0u
+                : lbvh_detail::centroid_to_morton(scene_bounds, primitives[id].centroid);
+        }
+    }
+    int count = static_cast<int>(tree.nodes.size());
+    for (int i = 0; i < count; ++i) {
+        const CpuBvhNode& nd = tree.nodes[i];
+        if (node_left) node_left[i] = nd.is_leaf() ? -1 : nd.left;
+        if (node_right) node_right[i] = nd.is_leaf() ? -1 : nd.right;
+        if (node_bounds) {
+            float* b = node_bounds + size_t(i) * 6;
+            b[0] = nd.bounds.p_min.x; b[1] = nd.bounds.p_min.y; b[2] = nd.bounds.p_min.z;
+            b[3] = nd.bounds.p_max.x; b[4] = nd.bounds.p_max.y; b[5] = nd.bounds.p_max.z;
+        }
+    }
+    return count;
+}
+
+// Builds the host tree over triangles, then traces rays.  mode 0: the reference's GPU
+// stackless traversal order (left first) run on the host; mode 1: the reference's CPU
+// stack traversal (right child popped first).
+int ref_build_and_trace(const float* tris, int ntri, const float* rays, int nrays, int mode,
+                        int threads, int32_t* hit_id, float* hit_t) {
+    if (ntri <= 0) {
+        for (int i = 0; i < nrays; ++i) { hit_id[i] = -1; hit_t[i] = INFINITY; }
+        return 0;
+    }
+    std::vector<BvhBuildPrimitive> primitives = make_primitives(tris, ntri, 0);
+    CpuBvhTree tree = build_cpu_lbvh_tree(primitives);
+    std::vector<Triangle> triangles = make_triangles(tris, ntri);
+    if (mode == 0) {
+        std::vector<GpuBvhNode> nodes;
+        flatten_preorder(tree, nodes);
+        GpuBvhView view{nodes.data(), static_cast<int>(nodes.size()), AABB{}};
+        parallel_for(nrays, threads, [&](int begin, int end) {
+            for (int i = begin; i < end; ++i) {
+                int pid; Float t, u, v;
+                bool found = intersect_bvh_device(view, triangles.data(),
+                                                  make_ray(rays + size_t(i) * 8), pid, t, u, v);
+                hit_id[i] = found ? pid : -1;
+                hit_t[i] = found ? t : INFINITY;
+            }
+        });
+    } else {
+        parallel_for(nrays, threads, [&](int begin, int end) {
+            for (int i = begin; i < end; ++i) {
+                int pid; Float t, u, v;
+                auto isect = [&](int prim, const Ray& r, CpuBvhPrimitiveHit& h) {
+                    Float uu, vv;
+                    bool ok = intersect_triangle(r, triangles[prim], h.t, uu, vv);
+                    h.u = uu; h.v = vv;
+                    return ok;
+                };
+                bool found = intersect_cpu_bvh_tree(tree, make_ray(rays + size_t(i) * 8), isect,
+                                                    pid, t, u, v);
+                hit_id[i] = found ? pid : -1;
+                hit_t[i] = found ? t : INFINITY;
+            }
+        });
+    }
+    return 0;
+}
+
+// A built host tree kept alive across calls, so that build and traversal can be timed
+// separately (bench.py's reference arm).
+struct RefTree {
+    CpuBvhTree tree;
+    std::vector<Triangle> triangles;
+};
+
+void* ref_tree_create(const float* prims, int n, int kind) {
+    RefTree* t = new RefTree();
+    if (n > 0) {
+        t->tree = build_cpu_lbvh_tree(make_primitives(prims, n, kind));
+        if (kind == 0) t->triangles = make_triangles(prims, n);
+    }
+    return t;
+}
+
+void ref_tree_destroy(void* handle) { delete static_cast<RefTree*>(handle); }
+
+// Closest hit through intersect_cpu_bvh_tree (the reference CPU traversal).
+int ref_tree_trace(void* handle, const float* rays, int nrays, int threads, int32_t* hit_id,
+                   float* hit_t) {
+    RefTree* t = static_cast<RefTree*>(handle);
+    parallel_for(nrays, threads, [&](int begin, int end) {
+        for (int i = begin; i < end; ++i) {
+            int pid = -1;
+            Float tt = INFINITY, u, v;
+            bool found = false;
+            if (!t->tree.empty()) {
+                auto isect = [&](int prim, const Ray& r, CpuBvhPrimitiveHit& h) {
+                    Float uu, vv;
+                    bool ok = intersect_triangle(r, t->triangles[prim], h.t, uu, vv);
+                    h.u = uu; h.v = vv;
+                    return ok;
+                };
+                found = intersect_cpu_bvh_tree(t->tree, make_ray(rays + size_t(i) * 8), isect,
+                                               pid, tt, u, v);
+            }
+            hit_id[i] = found ? pid : -1;
+            hit_t[i] = found ? tt : INFINITY;
+        }
+    });
+    return 0;
+}
+
+// Cornell box geometry as the reference builds it: 36 triangles (world space, 9
+// floats each), their material ids, the 4 materials (type, albedo rgb, emission rgb),
+// and the pinhole camera (origin, lower_left, horizontal, vertical).
+int ref_cornell_scene(int width, int height, float* tris, int32_t* material_ids,
+                      float* materials, float* camera) {
+    Scene scene = CornellSetup::make_scene(width, height);
+    finalize_scene(scene);
+    int count = scene_triangle_count(scene);
+    for (int i = 0; i < count; ++i) {
+        SceneTriangle st = scene_triangle_view(scene, i);
+        const vec3* v = &st.triangle.v0;
+        for (int k = 0; k < 3; ++k) {
+            tris[i * 9 + k * 3 + 0] = v[k].x;
+            tris[i * 9 + k * 3 + 1] = v[k].y;
+            tris[i * 9 + k * 3 + 2] = v[k].z;
+        }
+        material_ids[i] = st.material_id;
+    }
+    for (size_t m = 0; m < scene.materials.size(); ++m) {
+        const Material& mat = scene.materials[m];
+        float* o = materials + m * 7;
+        o[0] = static_cast<float>(static_cast<int>(mat.type));
+        o[1] = mat.albedo.x; o[2] = mat.albedo.y; o[3] = mat.albedo.z;
+        o[4] = mat.emission.x; o[5] = mat.emission.y; o[6] = mat.emission.z;
+    }
+    const PerspectiveCamera& c = scene.camera.perspective;
+    const vec3* cv[4] = {&c.origin, &c.lower_left, &c.horizontal, &c.vertical};
+    for (int k = 0; k < 4; ++k) {
+        camera[k * 3 + 0] = cv[k]->x; camera[k * 3 + 1] = cv[k]->y; camera[k * 3 + 2] = cv[k]->z;
+    }
+    return count;
+}
+
+// Renders pixel rows [y0, y1) of the Cornell box through the reference trace_path with
+// settings.seed = seed.  sum/sumsq receive per-pixel RGB sums over samples (row-major,
+// full image indexing); samples (optional) receives every sample's RGB as
+// [pixel][sample][3] for the rows rendered.
+int ref_cornell_render(int width, int height, int spp, int max_depth, uint64_t seed,
+                       int y0, int y1, int threads, float* sum, float* sumsq, float* samples) {
+    CornellSetup setup(width, height);
+    RenderSettings settings;
+    settings.max_depth = max_depth;
+    settings.seed = seed;
+    settings.light_sampler_kind = LightSamplerKind::Power;
+    int rows = y1 - y0;
+    parallel_for(rows * width, threads, [&](int begin, int end) {
+        for (int idx = begin; idx < end; ++idx) {
+            int y = y0 + idx / width;
+            int x = idx % width;
+            int pixel = y * width + x;
+            double acc[3] = {0, 0, 0}, acc2[3] = {0, 0, 0};
+            for (int s = 0; s < spp; ++s) {
+                vec3 L = reference_sample(setup, settings, width, height, x, y, s);
+                acc[0] += L.x; acc[1] += L.y; acc[2] += L.z;
+                acc2[0] += double(L.x) * L.x; acc2[1] += double(L.y) * L.y;
+                acc2[2] += double(L.z) * L.z;
+                if (samples) {
+                    float* o = samples + (size_t(idx) * spp + s) * 3;
+                    o[0] = L.x; o[1] = L.y; o[2] = L.z;
+                }
+            }
+            for (int k = 0; k < 3; ++k) {
+                if (sum) sum[size_t(pixel) * 3 + k] = static_cast<float>(acc[k]);
+                if (sumsq) sumsq[size_t(pixel) * 3 + k] = static_cast<float>(acc2[k]);
+            }
+        }
+    });
+    return 0;
+}
+
+}  // extern "C"

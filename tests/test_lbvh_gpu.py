@@ -1,0 +1,215 @@
+"""LBVH CUDA path vs the oracle, through the C ABI (B200)."""
+import numpy as np
+import pytest
+
+import lux_b200
+from lux_b200 import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+
+def _bounds(oracle, case):
+    prims = case["prims"]
+    return oracle.triangle_bounds(prims) if int(case["kind"]) == 0 else prims
+
+
+def _assert_tree_equal(got, want, codes_too=True):
+    assert np.array_equal(got.sorted_ids, want["sorted_ids"])
+    assert np.array_equal(got.node_left, want["node_left"])
+    assert np.array_equal(got.node_right, want["node_right"])
+    assert np.array_equal(got.node_bounds, want["node_bounds"])
+    if codes_too and len(got.sorted_ids) > 1:
+        assert np.array_equal(got.sorted_codes, want["sorted_codes"].astype(np.uint64))
+
+
+def test_build_matches_reference_fixtures(ctx, golden_lbvh):
+    for name, case in golden_lbvh.items():
+        kind = int(case["kind"])
+        bvh = ctx.build_lbvh(case["prims"], kind=kind)
+        _assert_tree_equal(bvh.download(), case)
+
+
+def test_trace_matches_reference_fixtures(ctx, golden_lbvh):
+    for name, case in golden_lbvh.items():
+        if int(case["kind"]) != 0:
+            continue
+        bvh = ctx.build_lbvh(case["prims"])
+        hid, ht = bvh.trace_closest(case["rays"])
+        assert np.array_equal(hid, case["hit_id_gpu_order"]), name
+        assert np.array_equal(ht, case["hit_t_gpu_order"]), name
+        aid = bvh.trace_any(case["rays"])
+        assert np.array_equal(aid >= 0, hid >= 0), name
+
+
+@pytest.mark.parametrize("n,seed", [(1, 1), (2, 2), (5, 3), (4095, 4), (4096, 5), (4097, 6),
+                                    (100_000, 7)])
+@pytest.mark.parametrize("bits", [30, 63])
+def test_build_matches_oracle(ctx, oracle, n, seed, bits):
+    tris = W.soup_triangles(n, seed=seed)
+    want = oracle.build(oracle.triangle_bounds(tris), morton_bits=bits)
+    got = ctx.build_lbvh(tris, morton_bits=bits).download()
+    _assert_tree_equal(got, want)
+
+
+def test_duplicate_codes_keep_input_order(ctx, oracle):
+    base = W.soup_triangles(64, seed=9)
+    tris = np.concatenate([np.tile(base[:1], (3000, 1)), base, np.tile(base[5:6], (2000, 1))])
+    for bits in (30, 63):
+        want = oracle.build(oracle.triangle_bounds(tris), morton_bits=bits)
+        _assert_tree_equal(ctx.build_lbvh(tris, morton_bits=bits).download(), want)
+
+
+def test_trace_matches_oracle_with_ties(ctx, oracle):
+    # A grid of coplanar unit quads (two triangles each): rays through shared edges and
+    # vertices hit several triangles at the same t.
+    g = 24
+    tris = []
+    for i in range(g):
+        for j in range(g):
+            p0 = (i / g, j / g, 0.5); p1 = ((i + 1) / g, j / g, 0.5)
+            p2 = ((i + 1) / g, (j + 1) / g, 0.5); p3 = (i / g, (j + 1) / g, 0.5)
+            tris.append(p0 + p1 + p2)
+            tris.append(p0 + p2 + p3)
+    tris = np.array(tris, np.float32)
+    xs = (np.arange(4 * g) / (4 * g)).astype(np.float32)
+    xx, yy = np.meshgrid(xs, xs)
+    rays = np.zeros((xx.size, 8), np.float32)
+    rays[:, 0] = xx.ravel(); rays[:, 1] = yy.ravel(); rays[:, 2] = 1.0
+    rays[:, 6] = -1.0; rays[:, 7] = np.inf
+    tree = oracle.build(oracle.triangle_bounds(tris))
+    want_id, want_t = oracle.trace(tris, tree, rays)
+    bvh = ctx.build_lbvh(tris)
+    got_id, got_t = bvh.trace_closest(rays)
+    assert (want_id >= 0).mean() > 0.9
+    assert np.array_equal(got_id, want_id)
+    assert np.array_equal(got_t, want_t)
+
+
+def test_trace_matches_oracle_random(ctx, oracle):
+    tris = W.soup_triangles(200_000, seed=11)
+    rays = W.uniform_rays(60_000, seed=12)
+    tree = oracle.build(oracle.triangle_bounds(tris))
+    want_id, want_t = oracle.trace(tris, tree, rays)
+    bvh = ctx.build_lbvh(tris)
+    got_id, got_t = bvh.trace_closest(rays)
+    assert (want_id >= 0).sum() > 1000
+    assert np.array_equal(got_id, want_id)
+    assert np.array_equal(got_t, want_t)
+    any_id = bvh.trace_any(rays)
+    assert np.array_equal(any_id >= 0, want_id >= 0)
+
+
+def test_refit_matches_rebuild_bounds(ctx, oracle):
+    tris = W.soup_triangles(50_000, seed=13)
+    moved = W.jitter_triangles(tris, seed=14)
+    bvh = ctx.build_lbvh(tris)
+    before = bvh.download()
+    assert lux_b200.refit_gpu_lbvh(bvh, moved)
+    after = bvh.download()
+    # Topology and order are kept; every box is recomputed from the moved geometry.
+    assert np.array_equal(after.sorted_ids, before.sorted_ids)
+    assert np.array_equal(after.node_left, before.node_left)
+    n = len(tris)
+    leaf_boxes = oracle.triangle_bounds(moved)[after.sorted_ids]
+    assert np.array_equal(after.node_bounds[n - 1:], leaf_boxes)
+    ni = n - 1
+    left, right, nb = after.node_left, after.node_right, after.node_bounds
+    union = np.concatenate([np.minimum(nb[left[:ni], :3], nb[right[:ni], :3]),
+                            np.maximum(nb[left[:ni], 3:], nb[right[:ni], 3:])], axis=1)
+    assert np.array_equal(nb[:ni], union)
+    assert np.array_equal(bvh.root_bounds(),
+                          np.concatenate([leaf_boxes[:, :3].min(0), leaf_boxes[:, 3:].max(0)]))
+    # Traversal over the refit tree equals the oracle over the same refit tree.
+    rays = W.uniform_rays(20_000, seed=15)
+    tree = oracle.build(oracle.triangle_bounds(tris))
+    tree["node_bounds"] = after.node_bounds
+    want_id, want_t = oracle.trace(moved, tree, rays)
+    got_id, got_t = bvh.trace_closest(rays)
+    assert np.array_equal(got_id, want_id) and np.array_equal(got_t, want_t)
+    # A count mismatch is refused, as refit_gpu_lbvh returns false.
+    assert not lux_b200.refit_gpu_lbvh(bvh, moved[:-1])
+
+
+def test_overlap_self_and_cross_match_oracle(ctx, oracle):
+    boxes = W.query_boxes(30_000, seed=16, half_extent=0.004)
+    tree = oracle.build(boxes)
+    want_pairs, want_found = oracle.overlap(tree, boxes, self_pairs=True)
+    bvh = ctx.build_lbvh(boxes, kind=lux_b200.PRIM_AABBS)
+    res = bvh.overlap_self(max_pairs=want_found + 10)
+    assert res.found_count == want_found and not res.truncated
+    assert set(map(tuple, res.pairs.tolist())) == set(map(tuple, want_pairs.tolist()))
+    assert np.all(res.pairs[:, 0] < res.pairs[:, 1])
+
+    queries = W.query_boxes(20_000, seed=17, half_extent=0.003)
+    qbvh = ctx.build_lbvh(queries, kind=lux_b200.PRIM_AABBS)
+    want_pairs, want_found = oracle.overlap(tree, queries, self_pairs=False)
+    res = bvh.overlap_cross(qbvh, max_pairs=want_found + 10)
+    assert res.found_count == want_found
+    assert set(map(tuple, res.pairs.tolist())) == set(map(tuple, want_pairs.tolist()))
+
+    # Truncation: found counts every pair, at most max_pairs are written.
+    res = bvh.overlap_cross(qbvh, max_pairs=100)
+    assert res.truncated and res.found_count == want_found and len(res.pairs) == 100
+    assert set(map(tuple, res.pairs.tolist())) <= set(map(tuple, want_pairs.tolist()))
+
+
+def test_empty_and_single(ctx):
+    empty = ctx.build_lbvh(np.zeros((0, 9), np.float32))
+    rays = W.uniform_rays(10)
+    hid, ht = empty.trace_closest(rays)
+    assert np.all(hid == -1) and np.all(np.isinf(ht))
+    res = empty.overlap_self()
+    assert res.found_count == 0
+    one = ctx.build_lbvh(np.array([[0, 0, 0, 1, 0, 0, 0, 1, 0]], np.float32))
+    r = np.array([[0.2, 0.2, 1, 0, 0, 0, -1, np.inf]], np.float32)
+    hid, ht = one.trace_closest(r)
+    assert hid[0] == 0 and ht[0] == np.float32(1.0)
+
+
+def test_device_pointers_stream_ordered(ctx, oracle):
+    torch = pytest.importorskip("torch")
+    tris = W.soup_triangles(30_000, seed=18)
+    rays = W.uniform_rays(10_000, seed=19)
+    dt = torch.from_numpy(tris).cuda()
+    dr = torch.from_numpy(rays).cuda()
+    ctx.set_stream(torch.cuda.current_stream().cuda_stream)
+    try:
+        bvh = ctx.build_lbvh(dt)
+        hid = torch.empty(len(rays), dtype=torch.int32, device="cuda")
+        ht = torch.empty(len(rays), dtype=torch.float32, device="cuda")
+        bvh.trace_closest(dr, hid, ht)
+        torch.cuda.synchronize()
+        want_id, want_t = oracle.trace(tris, oracle.build(oracle.triangle_bounds(tris)), rays)
+        assert np.array_equal(hid.cpu().numpy(), want_id)
+        assert np.array_equal(ht.cpu().numpy(), want_t)
+    finally:
+        ctx.set_stream(None)
+
+
+def test_full_size_microbench_properties(ctx):
+    """1,048,576 triangles / 4,194,304 rays: size-independent checks at full size."""
+    data = W.lbvh_microbench(n_rays=1 << 22)
+    tris, rays = data["triangles"], data["rays"]
+    bvh = ctx.build_lbvh(tris)
+    t = bvh.download()
+    n = len(tris)
+    assert np.all(np.diff(t.sorted_codes.astype(np.int64)) >= 0)
+    assert np.array_equal(np.sort(t.sorted_ids), np.arange(n))
+    same = t.sorted_codes[1:] == t.sorted_codes[:-1]
+    assert np.all(t.sorted_ids[1:][same] > t.sorted_ids[:-1][same])
+    # every node reached exactly once from the root
+    child = np.concatenate([t.node_left[: n - 1], t.node_right[: n - 1]])
+    assert np.array_equal(np.sort(child), np.arange(1, 2 * n - 1))
+    hid, ht = bvh.trace_closest(rays)
+    hit = hid >= 0
+    assert 0.2 < hit.mean() < 0.99
+    # Every reported hit is a real intersection at the reported t (float64 recheck).
+    idx = np.nonzero(hit)[0][:: max(1, hit.sum() // 20000)]
+    v = tris[hid[idx]].reshape(-1, 3, 3).astype(np.float64)
+    o = rays[idx, 0:3].astype(np.float64); d = rays[idx, 4:7].astype(np.float64)
+    p = o + d * ht[idx, None].astype(np.float64)
+    nrm = np.cross(v[:, 1] - v[:, 0], v[:, 2] - v[:, 0])
+    dist = np.abs(np.einsum("ij,ij->i", p - v[:, 0], nrm)) / np.linalg.norm(nrm, axis=1)
+    assert np.percentile(dist, 99) < 1e-5
+    aid = bvh.trace_any(rays)
+    assert np.array_equal(aid >= 0, hit)
