@@ -204,6 +204,9 @@ def run_lux(args) -> None:
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
 
     dev = torch.device("cuda", local)
+    # A dedicated stream for everything (the legacy default stream has handle 0, which
+    # the C ABI reads as "use the context's own stream").
+    torch.cuda.set_stream(torch.cuda.Stream(dev))
     data = W.lbvh_microbench(N_TRIS, N_RAYS, N_QUERIES, SEED)
     d_tris = torch.from_numpy(data["triangles"]).to(dev)
     d_rays = torch.from_numpy(data["rays"]).to(dev)
@@ -217,6 +220,7 @@ def run_lux(args) -> None:
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
 
     stream = torch.cuda.current_stream(dev)
+    assert stream.cuda_stream != 0
     ctx = lux_b200.Context(local, stream.cuda_stream)
     bvh = ctx.build_lbvh(d_tris)
     qbvh = ctx.build_lbvh(d_queries, kind=lux_b200.PRIM_AABBS)
@@ -411,6 +415,7 @@ def measure_cpu_baseline(data) -> dict | None:
 
 
 def main():
+    global N_TRIS, N_RAYS, N_QUERIES, WORKLOAD
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=50)
@@ -418,7 +423,15 @@ def main():
     ap.add_argument("--impl", default="lux", choices=["lux", "reference"])
     ap.add_argument("--skip-e2e", action="store_true")
     ap.add_argument("--skip-cpu-baseline", action="store_true")
+    ap.add_argument("--tris", type=int, default=N_TRIS,
+                    help="smaller cases for profiling captures only")
+    ap.add_argument("--rays", type=int, default=N_RAYS)
+    ap.add_argument("--queries", type=int, default=N_QUERIES)
     args = ap.parse_args()
+    if (args.tris, args.rays, args.queries) != (N_TRIS, N_RAYS, N_QUERIES):
+        N_TRIS, N_RAYS, N_QUERIES = args.tris, args.rays, args.queries
+        WORKLOAD = (f"LBVH microbench generator at reduced size (profiling case): {N_TRIS} "
+                    f"triangles, {N_RAYS} rays, {N_QUERIES} query boxes, seed 7")
     if args.impl == "reference":
         run_reference(args)
     else:
