@@ -224,6 +224,8 @@ def run_lux(args) -> None:
     ctx = lux_b200.Context(local, stream.cuda_stream)
     bvh = ctx.build_lbvh(d_tris)
     qbvh = ctx.build_lbvh(d_queries, kind=lux_b200.PRIM_AABBS)
+    ctx.set_option(lux_b200.OPT_TRACE_VARIANT, args.trace_variant)
+    ctx.set_option(lux_b200.OPT_TRACE_BUDGET, args.trace_budget)
     lib = ctx._lib
     found_ptr = found.data_ptr()
 
@@ -427,6 +429,9 @@ def main():
                     help="smaller cases for profiling captures only")
     ap.add_argument("--rays", type=int, default=N_RAYS)
     ap.add_argument("--queries", type=int, default=N_QUERIES)
+    ap.add_argument("--trace-variant", type=int, default=0,
+                    help="0 auto, 1 one thread per ray, 2 persistent (tunable)")
+    ap.add_argument("--trace-budget", type=int, default=32)
     args = ap.parse_args()
     if (args.tris, args.rays, args.queries) != (N_TRIS, N_RAYS, N_QUERIES):
         N_TRIS, N_RAYS, N_QUERIES = args.tris, args.rays, args.queries

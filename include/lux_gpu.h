@@ -68,6 +68,13 @@ int lux_abi_version(void);
 /* Number of kernels this context has launched so far (for launch accounting). */
 int lux_ctx_launch_count(lux_ctx* ctx, int64_t* count);
 
+/* Tunables (set by the autotuner or the caller; results never depend on them).
+ *   LUX_OPT_TRACE_VARIANT  0 auto, 1 one thread per ray, 2 persistent warps with refill
+ *   LUX_OPT_TRACE_BUDGET   traversal steps per refill round of the persistent kernel */
+enum lux_option { LUX_OPT_TRACE_VARIANT = 1, LUX_OPT_TRACE_BUDGET = 2 };
+int lux_ctx_set_option(lux_ctx* ctx, int32_t option, int64_t value);
+int lux_ctx_get_option(lux_ctx* ctx, int32_t option, int64_t* value);
+
 /* ------------------------------------------------------------------ LBVH */
 
 /*

@@ -37,6 +37,9 @@ LUX_ERR_BUDGET = 7
 PRIM_TRIANGLES = 0
 PRIM_AABBS = 1
 
+OPT_TRACE_VARIANT = 1   # 0 auto, 1 one thread per ray, 2 persistent warps with refill
+OPT_TRACE_BUDGET = 2    # traversal steps per refill round
+
 # Every symbol include/lux_gpu.h declares, with its ctypes signature.
 _P = ctypes.c_void_p
 _I32 = ctypes.c_int32
@@ -49,6 +52,8 @@ SIGNATURES = {
     "lux_ctx_set_stream": (ctypes.c_int, [_P, _P]),
     "lux_ctx_synchronize": (ctypes.c_int, [_P]),
     "lux_ctx_launch_count": (ctypes.c_int, [_P, ctypes.POINTER(_I64)]),
+    "lux_ctx_set_option": (ctypes.c_int, [_P, _I32, _I64]),
+    "lux_ctx_get_option": (ctypes.c_int, [_P, _I32, ctypes.POINTER(_I64)]),
     "lux_lbvh_build": (ctypes.c_int, [_P, _P, _I32, _I32, _I32, ctypes.POINTER(_P)]),
     "lux_lbvh_refit": (ctypes.c_int, [_P, _P, _P, _I32]),
     "lux_lbvh_rebuild": (ctypes.c_int, [_P, _P, _P, _I32]),
@@ -133,6 +138,14 @@ class Context:
 
     def synchronize(self) -> None:
         _check(self._lib.lux_ctx_synchronize(self._h))
+
+    def set_option(self, option: int, value: int) -> None:
+        _check(self._lib.lux_ctx_set_option(self._h, option, value))
+
+    def get_option(self, option: int) -> int:
+        v = _I64()
+        _check(self._lib.lux_ctx_get_option(self._h, option, ctypes.byref(v)))
+        return v.value
 
     def launch_count(self) -> int:
         v = _I64()

@@ -207,6 +207,8 @@ int lux_ctx_create(lux_ctx** out, int device, void* stream) {
     }
     err = cudaMalloc(&ctx->d_error, sizeof(int));
     if (err == cudaSuccess) err = cudaMemset(ctx->d_error, 0, sizeof(int));
+    if (err == cudaSuccess) err = cudaMalloc(&ctx->d_counter, 64);
+    if (err == cudaSuccess) err = cudaMemset(ctx->d_counter, 0, 64);
     if (err != cudaSuccess) {
         if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
         delete ctx;
@@ -223,9 +225,35 @@ int lux_ctx_destroy(lux_ctx* ctx) {
     if (ctx->scratch) cudaFree(ctx->scratch);
     if (ctx->staging) cudaFree(ctx->staging);
     if (ctx->d_error) cudaFree(ctx->d_error);
+    if (ctx->d_counter) cudaFree(ctx->d_counter);
     if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
     delete ctx;
     return LUX_OK;
+}
+
+int lux_ctx_set_option(lux_ctx* ctx, int32_t option, int64_t value) {
+    if (!ctx) return lux::fail(LUX_ERR_INVALID_ARGUMENT, "null context");
+    switch (option) {
+        case LUX_OPT_TRACE_VARIANT:
+            if (value < 0 || value > 2) return lux::fail(LUX_ERR_INVALID_ARGUMENT, "trace variant 0..2");
+            ctx->trace_variant = static_cast<int>(value);
+            return LUX_OK;
+        case LUX_OPT_TRACE_BUDGET:
+            if (value < 1 || value > 4096) return lux::fail(LUX_ERR_INVALID_ARGUMENT, "trace budget 1..4096");
+            ctx->trace_budget = static_cast<int>(value);
+            return LUX_OK;
+        default:
+            return lux::fail(LUX_ERR_INVALID_ARGUMENT, "unknown option");
+    }
+}
+
+int lux_ctx_get_option(lux_ctx* ctx, int32_t option, int64_t* value) {
+    if (!ctx || !value) return lux::fail(LUX_ERR_INVALID_ARGUMENT, "null argument");
+    switch (option) {
+        case LUX_OPT_TRACE_VARIANT: *value = ctx->trace_variant; return LUX_OK;
+        case LUX_OPT_TRACE_BUDGET: *value = ctx->trace_budget; return LUX_OK;
+        default: return lux::fail(LUX_ERR_INVALID_ARGUMENT, "unknown option");
+    }
 }
 
 int lux_ctx_set_stream(lux_ctx* ctx, void* stream) {

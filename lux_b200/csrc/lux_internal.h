@@ -14,6 +14,10 @@ struct lux_ctx {
     int sm_count = 148;
     int* d_error = nullptr;          // device error word (lux::kErr* bits)
     int64_t launches = 0;            // kernels launched through this context
+    unsigned* d_counter = nullptr;   // device work counter (persistent kernels)
+    // Tunables (lux_ctx_set_option).
+    int trace_variant = 0;           // lux::kTraceAuto / kTraceStatic / kTracePersistent
+    int trace_budget = 32;           // traversal steps per refill round
     // Growable device scratch, reused across calls on this context.
     void* scratch = nullptr;
     size_t scratch_bytes = 0;
@@ -49,6 +53,8 @@ struct lux_bvh {
 };
 
 namespace lux {
+
+enum : int { kTraceAuto = 0, kTraceStatic = 1, kTracePersistent = 2 };
 
 // Status helpers (defined in capi.cu).
 int fail(int status, const std::string& message);

@@ -140,6 +140,38 @@ LUX_HD bool slab_hit(const slab_ray& r, const box3& b, float tmax, float& tn) {
     return !(tn > fminf(tmax, tf));
 }
 
+// Octant form of the same slab test for rays with no parallel axis: the near plane of
+// axis a is lo_a when 1/d_a > 0 and hi_a otherwise, which yields exactly the values the
+// reference's per-box swap (core/aabb.cuh:100-104) produces, without the compare and
+// swap per box.  neg bit a: 1/d_a < 0.
+struct octant_ray {
+    f3 o;
+    f3 inv;
+    float tmin;
+    unsigned neg;
+};
+
+LUX_HD octant_ray make_octant_ray(const slab_ray& s) {
+    octant_ray r;
+    r.o = s.o;
+    r.inv = s.inv;
+    r.tmin = s.tmin;
+    r.neg = (s.inv.x < 0.0f ? 1u : 0u) | (s.inv.y < 0.0f ? 2u : 0u) | (s.inv.z < 0.0f ? 4u : 0u);
+    return r;
+}
+
+LUX_HD bool octant_hit(const octant_ray& r, const box3& b, float tmax, float& tn) {
+    float nx = (r.neg & 1u) ? b.hi.x : b.lo.x, fx = (r.neg & 1u) ? b.lo.x : b.hi.x;
+    float ny = (r.neg & 2u) ? b.hi.y : b.lo.y, fy = (r.neg & 2u) ? b.lo.y : b.hi.y;
+    float nz = (r.neg & 4u) ? b.hi.z : b.lo.z, fz = (r.neg & 4u) ? b.lo.z : b.hi.z;
+    float t0x = mul(sub(nx, r.o.x), r.inv.x), t1x = mul(sub(fx, r.o.x), r.inv.x);
+    float t0y = mul(sub(ny, r.o.y), r.inv.y), t1y = mul(sub(fy, r.o.y), r.inv.y);
+    float t0z = mul(sub(nz, r.o.z), r.inv.z), t1z = mul(sub(fz, r.o.z), r.inv.z);
+    tn = fmaxf(fmaxf(r.tmin, t0x), fmaxf(t0y, t0z));
+    float tf = fminf(fminf(tmax, t1x), fminf(t1y, t1z));
+    return !(tn > tf);
+}
+
 // Moller-Trumbore (geometry/triangle.h:33-52) on the stored form (v0, e1 = v1 - v0,
 // e2 = v2 - v0): the edges are the same rounded differences the reference forms.
 // Returns the raw t; the caller applies t_min < t < t_max.

@@ -129,6 +129,157 @@ __global__ void __launch_bounds__(kTraceThreads) k_trace(BvhView bvh, const floa
     if (hit_t) hit_t[i] = h.k >= 0 ? h.t : INFINITY;
 }
 
+// Persistent traversal: each warp keeps 32 rays in flight and advances each by at most
+// `budget` steps per round; lanes whose ray finished fetch the next ray index with one
+// warp-aggregated atomic, so lanes do not idle until the longest ray of a static warp
+// finishes.  A step is one node fetch (two child boxes) or one triangle test followed by
+// the pops it enables.  Decisions are those of trace_one, step for step.
+LUX_D unsigned lanemask_lt_u() {
+    unsigned m;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+    return m;
+}
+
+template <bool AnyHit>
+__global__ void __launch_bounds__(kTraceThreads) k_trace_persistent(
+        BvhView bvh, const float4* rays, int nrays, int* hit_id, float* hit_t,
+        unsigned* ray_counter, int budget, int* error) {
+    const unsigned lane = threadIdx.x & 31;
+    const unsigned lt = lanemask_lt_u();
+    const box3 root = load_root(bvh.root);
+    const long long bound = 2ll * bvh.n + 64;
+
+    int ray_idx = -1;   // >= 0 active ray, -1 needs a ray, -2 no rays left
+    ray3 ray;
+    slab_ray sr;
+    octant_ray orr;
+    bool fast = true;
+    float best_t = 0.0f;
+    int best_k = -1;
+    int cur = 0;
+    int sp = 0;
+    long long steps = 0;
+    bool root_missed = false;
+    int stack_h[kStack];
+    float stack_t[kStack];
+
+    for (;;) {
+        // Refill finished lanes (one atomic per warp).
+        bool need = ray_idx == -1;
+        unsigned need_mask = __ballot_sync(0xffffffffu, need);
+        if (need_mask) {
+            int leader = __ffs(need_mask) - 1;
+            unsigned base = 0;
+            if (lane == leader) base = atomicAdd(ray_counter, __popc(need_mask));
+            base = __shfl_sync(0xffffffffu, base, leader);
+            if (need) {
+                unsigned idx = base + __popc(need_mask & lt);
+                if (idx >= static_cast<unsigned>(nrays)) {
+                    ray_idx = -2;
+                } else {
+                    ray_idx = static_cast<int>(idx);
+                    ray = load_ray(rays, ray_idx);
+                    sr = make_slab_ray(ray);
+                    fast = sr.parallel == 0;
+                    orr = make_octant_ray(sr);
+                    best_t = ray.tmax;
+                    best_k = -1;
+                    sp = 0;
+                    steps = 0;
+                    float tn;
+                    root_missed = bvh.n <= 0 || !slab_hit(sr, root, best_t, tn);
+                    cur = bvh.n == 1 ? ~0 : 0;
+                }
+            }
+        }
+        if (__all_sync(0xffffffffu, ray_idx == -2)) break;
+
+        bool done = false;
+        if (ray_idx >= 0) {
+            if (root_missed) done = true;
+            for (int s = 0; s < budget && !done; ++s) {
+                if (++steps > bound || cur >= bvh.n - 1 || ~cur >= bvh.n) {
+                    atomicOr(error, kErrLoopBound);
+                    best_k = -1;
+                    best_t = ray.tmax;
+                    done = true;
+                    break;
+                }
+                bool pop = true;
+                if (cur >= 0) {
+                    BvhNode nd = load_node(bvh.nodes, cur);
+                    float tl, tr;
+                    bool hl, hr;
+                    if (fast) {
+                        hl = octant_hit(orr, node_left_box(nd), best_t, tl);
+                        hr = octant_hit(orr, node_right_box(nd), best_t, tr);
+                    } else {
+                        hl = slab_hit(sr, node_left_box(nd), best_t, tl);
+                        hr = slab_hit(sr, node_right_box(nd), best_t, tr);
+                    }
+                    if (hl) {
+                        if (hr) {
+                            if (sp >= kStack) {
+                                atomicOr(error, kErrStackOverflow);
+                                best_k = -1;
+                                best_t = ray.tmax;
+                                done = true;
+                                break;
+                            }
+                            stack_h[sp] = nd.ch.y;
+                            stack_t[sp] = tr;
+                            ++sp;
+                        }
+                        cur = nd.ch.x;
+                        pop = false;
+                    } else if (hr) {
+                        cur = nd.ch.y;
+                        pop = false;
+                    }
+                } else {
+                    int k = ~cur;
+                    const float4* tp = reinterpret_cast<const float4*>(bvh.tris + k);
+                    float4 p0 = __ldg(tp);
+                    float4 p1 = __ldg(tp + 1);
+                    float4 p2 = __ldg(tp + 2);
+                    float t, u, v;
+                    if (moller_trumbore(ray.o, ray.d, make_f3(p0.x, p0.y, p0.z),
+                                        make_f3(p1.x, p1.y, p1.z), make_f3(p2.x, p2.y, p2.z),
+                                        t, u, v)
+                        && t > ray.tmin && t < best_t) {
+                        best_k = k;
+                        best_t = t;
+                        if (AnyHit) {
+                            done = true;
+                            break;
+                        }
+                    }
+                }
+                if (pop) {
+                    bool resumed = false;
+                    while (sp > 0) {
+                        --sp;
+                        if (!(stack_t[sp] > best_t)) {
+                            cur = stack_h[sp];
+                            resumed = true;
+                            break;
+                        }
+                    }
+                    if (!resumed) done = true;
+                }
+            }
+        }
+        if (done) {
+            int id = -1;
+            if (best_k >= 0)
+                id = __float_as_int(__ldg(reinterpret_cast<const float*>(bvh.tris + best_k) + 3));
+            hit_id[ray_idx] = id;
+            if (hit_t) hit_t[ray_idx] = best_k >= 0 ? best_t : INFINITY;
+            ray_idx = -1;
+        }
+    }
+}
+
 // Totals of box and triangle tests over all rays (one atomic pair per warp).
 __global__ void __launch_bounds__(kTraceThreads) k_trace_stats(BvhView bvh, const float4* rays,
                                                                int nrays,
@@ -230,26 +381,45 @@ __global__ void __launch_bounds__(kTraceThreads) k_overlap(BvhView tree, BvhView
     }
 }
 
+template <bool AnyHit>
+int launch_trace(lux_ctx* ctx, const lux_bvh* bvh, const float* rays, int nrays, int* hit_id,
+                 float* hit_t) {
+    if (nrays <= 0) return LUX_OK;
+    const float4* r4 = reinterpret_cast<const float4*>(rays);
+    if (ctx->trace_variant == kTraceStatic) {
+        int grid = (nrays + kTraceThreads - 1) / kTraceThreads;
+        k_trace<AnyHit><<<grid, kTraceThreads, 0, ctx->stream>>>(bvh->view(), r4, nrays, hit_id,
+                                                                 hit_t, ctx->d_error);
+        ctx->launches += 1;
+        return cuda_fail(cudaGetLastError(), "k_trace");
+    }
+    static int blocks_per_sm[2] = {0, 0};
+    int& bps = blocks_per_sm[AnyHit ? 1 : 0];
+    if (bps == 0) {
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_trace_persistent<AnyHit>,
+                                                      kTraceThreads, 0);
+        if (bps <= 0) bps = 1;
+    }
+    int grid = ctx->sm_count * bps;
+    int needed = (nrays + kTraceThreads - 1) / kTraceThreads;
+    if (grid > needed) grid = needed;
+    cudaError_t err = cudaMemsetAsync(ctx->d_counter, 0, sizeof(unsigned), ctx->stream);
+    if (err != cudaSuccess) return cuda_fail(err, "ray counter reset");
+    k_trace_persistent<AnyHit><<<grid, kTraceThreads, 0, ctx->stream>>>(
+        bvh->view(), r4, nrays, hit_id, hit_t, ctx->d_counter, ctx->trace_budget, ctx->d_error);
+    ctx->launches += 1;
+    return cuda_fail(cudaGetLastError(), "k_trace_persistent");
+}
+
 }  // namespace
 
 int trace_closest(lux_ctx* ctx, const lux_bvh* bvh, const float* rays, int nrays, int* hit_id,
                   float* hit_t) {
-    if (nrays <= 0) return LUX_OK;
-    int grid = (nrays + kTraceThreads - 1) / kTraceThreads;
-    k_trace<false><<<grid, kTraceThreads, 0, ctx->stream>>>(
-        bvh->view(), reinterpret_cast<const float4*>(rays), nrays, hit_id, hit_t, ctx->d_error);
-    ctx->launches += 1;
-    return cuda_fail(cudaGetLastError(), "k_trace closest");
+    return launch_trace<false>(ctx, bvh, rays, nrays, hit_id, hit_t);
 }
 
 int trace_any(lux_ctx* ctx, const lux_bvh* bvh, const float* rays, int nrays, int* hit_id) {
-    if (nrays <= 0) return LUX_OK;
-    int grid = (nrays + kTraceThreads - 1) / kTraceThreads;
-    k_trace<true><<<grid, kTraceThreads, 0, ctx->stream>>>(
-        bvh->view(), reinterpret_cast<const float4*>(rays), nrays, hit_id, nullptr,
-        ctx->d_error);
-    ctx->launches += 1;
-    return cuda_fail(cudaGetLastError(), "k_trace any");
+    return launch_trace<true>(ctx, bvh, rays, nrays, hit_id, nullptr);
 }
 
 int trace_stats(lux_ctx* ctx, const lux_bvh* bvh, const float* rays, int nrays,

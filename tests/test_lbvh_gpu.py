@@ -99,6 +99,29 @@ def test_trace_matches_oracle_random(ctx, oracle):
     assert np.array_equal(any_id >= 0, want_id >= 0)
 
 
+@pytest.mark.parametrize("variant,budget", [(1, 32), (2, 1), (2, 7), (2, 32), (2, 256)])
+def test_trace_variants_identical(ctx, oracle, variant, budget):
+    """Tunables change speed only: every traversal variant returns the oracle's hits."""
+    tris = W.soup_triangles(100_000, seed=21)
+    rays = W.uniform_rays(30_000, seed=22)
+    rays[:5, 4:7] = [[1, 0, 0], [0, 1e-13, 1], [0, 0, -1], [0, 1, 0], [1e-14, 0, 1]]
+    rays[:5, 4:7] /= np.linalg.norm(rays[:5, 4:7], axis=1, keepdims=True)
+    tree = oracle.build(oracle.triangle_bounds(tris))
+    want_id, want_t = oracle.trace(tris, tree, rays)
+    bvh = ctx.build_lbvh(tris)
+    try:
+        ctx.set_option(lux_b200.OPT_TRACE_VARIANT, variant)
+        ctx.set_option(lux_b200.OPT_TRACE_BUDGET, budget)
+        got_id, got_t = bvh.trace_closest(rays)
+        any_id = bvh.trace_any(rays)
+    finally:
+        ctx.set_option(lux_b200.OPT_TRACE_VARIANT, 0)
+        ctx.set_option(lux_b200.OPT_TRACE_BUDGET, 32)
+    assert np.array_equal(got_id, want_id)
+    assert np.array_equal(got_t, want_t)
+    assert np.array_equal(any_id >= 0, want_id >= 0)
+
+
 def test_refit_matches_rebuild_bounds(ctx, oracle):
     tris = W.soup_triangles(50_000, seed=13)
     moved = W.jitter_triangles(tris, seed=14)
