@@ -70,8 +70,9 @@ int lux_ctx_launch_count(lux_ctx* ctx, int64_t* count);
 
 /* Tunables (set by the autotuner or the caller; results never depend on them).
  *   LUX_OPT_TRACE_VARIANT  0 auto, 1 one thread per ray, 2 persistent warps with refill
- *   LUX_OPT_TRACE_BUDGET   traversal steps per refill round of the persistent kernel */
-enum lux_option { LUX_OPT_TRACE_VARIANT = 1, LUX_OPT_TRACE_BUDGET = 2 };
+ *   LUX_OPT_TRACE_BUDGET   traversal steps per refill round of the persistent kernel
+ *   LUX_OPT_RENDER_BATCH   paths in flight per wavefront batch (device memory ~200 B each) */
+enum lux_option { LUX_OPT_TRACE_VARIANT = 1, LUX_OPT_TRACE_BUDGET = 2, LUX_OPT_RENDER_BATCH = 3 };
 int lux_ctx_set_option(lux_ctx* ctx, int32_t option, int64_t value);
 int lux_ctx_get_option(lux_ctx* ctx, int32_t option, int64_t* value);
 
@@ -153,6 +154,128 @@ int lux_overlap_self(lux_ctx* ctx, const lux_bvh* bvh, int32_t* pairs, int64_t m
                      int64_t* found);
 int lux_overlap_cross(lux_ctx* ctx, const lux_bvh* left, const lux_bvh* right,
                       int32_t* pairs, int64_t max_pairs, int64_t* found);
+
+/* ------------------------------------------------------------------ scenes and rendering */
+
+typedef struct lux_scene lux_scene;
+
+/* Material (material/material.h:29-40; constant emission).  type: 0 Lambert,
+ * 1 thin Lambert, 2 GGX, 3 dielectric, 4 interface (null), 5 transparent (tinted filter). */
+typedef struct lux_material {
+    int32_t type;
+    float albedo[3];
+    float emission[3];
+    int32_t emission_two_sided;   /* 0: single sided (EmissionSidedness::SingleSided) */
+    float roughness;
+    float metallic;
+    float eta;
+} lux_material;
+
+/* Indexed triangle mesh in object space (scene/scene_data.h:36-44).  normals and uvs
+ * may be NULL (all zero, as add_triangle stores them). */
+typedef struct lux_mesh_desc {
+    const float* vertices;        /* vertex_count * 3 */
+    const float* normals;         /* vertex_count * 3 or NULL */
+    const float* uvs;             /* vertex_count * 2 or NULL */
+    int32_t vertex_count;
+    const uint32_t* indices;      /* triangle_count * 3 */
+    const int32_t* material_ids;  /* triangle_count */
+    int32_t triangle_count;
+} lux_mesh_desc;
+
+/* Instance (scene/scene_data.h:46-51): row-major 3x4 object-to-world matrix (the
+ * implicit last row is 0 0 0 1) and its inverse; world_to_object all zero asks the
+ * library to invert (inverse_affine, core/mat4.cuh:131-160). */
+typedef struct lux_instance_desc {
+    int32_t mesh;
+    int32_t material_override;    /* -1: per-triangle materials */
+    float object_to_world[12];
+    float world_to_object[12];
+} lux_instance_desc;
+
+/* Explicit light (light/light.h:66-79).  kind: 1 point (vec = position, value =
+ * intensity), 2 distant (vec = direction to light, value = radiance), 3 uniform
+ * infinite (value = radiance).  Emissive triangles become area lights automatically. */
+typedef struct lux_light_desc {
+    int32_t kind;
+    float vec[3];
+    float value[3];
+} lux_light_desc;
+
+/* Perspective camera (camera/camera.h:29-38). */
+typedef struct lux_camera_desc {
+    float origin[3], lower_left[3], horizontal[3], vertical[3], lens_u[3], lens_v[3];
+    float lens_radius;
+} lux_camera_desc;
+
+/* make_perspective_camera (camera/camera.h:96-126) on the host: vertical field of view
+ * in degrees, film aspect, lens radius (0: pinhole) and focal distance (<= 0: the
+ * look-at distance). */
+int lux_camera_perspective(const float origin[3], const float look_at[3], float vfov_degrees,
+                           float aspect, float lens_radius, float focal_distance,
+                           lux_camera_desc* out);
+
+typedef struct lux_scene_desc {
+    const lux_material* materials;
+    int32_t material_count;
+    const lux_mesh_desc* meshes;
+    int32_t mesh_count;
+    const lux_instance_desc* instances;
+    int32_t instance_count;
+    const lux_light_desc* lights;
+    int32_t light_count;
+    lux_camera_desc camera;
+} lux_scene_desc;
+
+/* RenderSettings (integrator/render_context.h:16-24).  light_sampler: 0 uniform,
+ * 1 power (the reference default). */
+typedef struct lux_render_request {
+    int32_t width, height, spp, max_depth;
+    uint64_t seed;
+    int32_t frame_index, sample_offset;
+    int32_t light_sampler;
+} lux_render_request;
+
+/*
+ * Uploads a scene: world-space triangle records, one BLAS per mesh and a TLAS over the
+ * instances (the LBVH above), materials and the light tables the reference prepares
+ * on the host (scene/scene_prepare.h:268-387: area lights in scene-triangle order, then
+ * explicit lights, power alias table).  Replaces PreparedScene::prepare_gpu
+ * (scene/prepared_scene.h:35-39).
+ */
+int lux_scene_create(lux_ctx* ctx, const lux_scene_desc* desc, lux_scene** out);
+int lux_scene_destroy(lux_scene* scene);
+
+/* Number of scene triangles, area lights and all lights. */
+int lux_scene_info(const lux_scene* scene, int32_t* triangles, int32_t* area_lights,
+                   int32_t* lights);
+
+/*
+ * New vertex positions for one mesh (same count): world triangles are recomputed and
+ * the mesh's BLAS and the TLAS are refit (not rebuilt) for animation between frames.
+ * Area-light areas and powers are not re-derived (the light tables are the
+ * construction-time ones).
+ */
+int lux_scene_update_mesh(lux_ctx* ctx, lux_scene* scene, int32_t mesh, const float* vertices);
+
+/*
+ * Wavefront path tracing (WavefrontPathTracer::render, integrator/wavefront_pt.cu:51-84):
+ * film_sum receives width*height*3 floats, the per-pixel SUM over spp (Film::pixels,
+ * film/film.h:19-21).  Camera rays, closest hits, per-material shading with NEE, MIS and
+ * Russian roulette, and shadow rays through pass-through surfaces follow the reference
+ * CPU tracer's arithmetic (integrator/cpu_path_tracer.cpp:403-498).
+ */
+int lux_render(lux_ctx* ctx, const lux_scene* scene, const lux_render_request* req,
+               float* film_sum);
+
+/* Same paths, but every sample's radiance is written: samples[(pixel*spp + s)*3 + c]
+ * (pixel = y*width + x).  For validation against per-sample reference values. */
+int lux_render_samples(lux_ctx* ctx, const lux_scene* scene, const lux_render_request* req,
+                       float* samples);
+
+/* Rays traced by the last lux_render* on this context: [0] camera + extension rays,
+ * [1] shadow-ray segments (each pass-through re-launch counts), host int64[2]. */
+int lux_render_ray_counts(lux_ctx* ctx, int64_t* counts);
 
 #ifdef __cplusplus
 }

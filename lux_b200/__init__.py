@@ -63,6 +63,15 @@ SIGNATURES = {
     "lux_bvh_download": (ctypes.c_int, [_P, _P, _P, _P, _P, _P, _P]),
     "lux_trace_closest": (ctypes.c_int, [_P, _P, _P, _I32, _P, _P]),
     "lux_trace_any": (ctypes.c_int, [_P, _P, _P, _I32, _P]),
+    "lux_camera_perspective": (ctypes.c_int, [_P, _P, ctypes.c_float, ctypes.c_float,
+                                              ctypes.c_float, ctypes.c_float, _P]),
+    "lux_scene_create": (ctypes.c_int, [_P, _P, ctypes.POINTER(_P)]),
+    "lux_scene_destroy": (ctypes.c_int, [_P]),
+    "lux_scene_info": (ctypes.c_int, [_P, _P, _P, _P]),
+    "lux_scene_update_mesh": (ctypes.c_int, [_P, _P, _I32, _P]),
+    "lux_render": (ctypes.c_int, [_P, _P, _P, _P]),
+    "lux_render_samples": (ctypes.c_int, [_P, _P, _P, _P]),
+    "lux_render_ray_counts": (ctypes.c_int, [_P, _P]),
     "lux_overlap_self": (ctypes.c_int, [_P, _P, _P, _I64, _P]),
     "lux_overlap_cross": (ctypes.c_int, [_P, _P, _P, _P, _I64, _P]),
 }

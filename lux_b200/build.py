@@ -24,6 +24,14 @@ NVCC_FLAGS = [
 ]
 
 
+# Translation units whose device arithmetic must not be contracted into FMAs (the path
+# tracer restates the reference's host arithmetic operation by operation).
+PER_FILE_FLAGS = {
+    "wavefront.cu": ["-fmad=false"],
+    "scene.cu": ["-fmad=false"],
+}
+
+
 def _sources():
     return sorted(os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith(".cu"))
 
@@ -37,7 +45,8 @@ def _headers():
 
 def _compile(src, verbose):
     obj = os.path.join(OBJ_DIR, os.path.basename(src)[:-3] + ".o")
-    cmd = [NVCC, *NVCC_FLAGS, "-c", src, "-o", obj]
+    cmd = [NVCC, *NVCC_FLAGS, *PER_FILE_FLAGS.get(os.path.basename(src), []), "-c", src,
+           "-o", obj]
     if verbose:
         cmd.insert(1, "-Xptxas=-v")
     res = subprocess.run(cmd, capture_output=True, text=True)

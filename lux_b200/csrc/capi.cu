@@ -14,6 +14,7 @@
 
 #include "../../include/lux_gpu.h"
 #include "lux_internal.h"
+#include "pt_scene.h"
 
 namespace {
 
@@ -226,6 +227,7 @@ int lux_ctx_destroy(lux_ctx* ctx) {
     if (ctx->staging) cudaFree(ctx->staging);
     if (ctx->d_error) cudaFree(ctx->d_error);
     if (ctx->d_counter) cudaFree(ctx->d_counter);
+    lux::render_runtime_free(ctx);
     if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
     delete ctx;
     return LUX_OK;
@@ -242,6 +244,10 @@ int lux_ctx_set_option(lux_ctx* ctx, int32_t option, int64_t value) {
             if (value < 1 || value > 4096) return lux::fail(LUX_ERR_INVALID_ARGUMENT, "trace budget 1..4096");
             ctx->trace_budget = static_cast<int>(value);
             return LUX_OK;
+        case LUX_OPT_RENDER_BATCH:
+            if (value < 1 || value > (1 << 28)) return lux::fail(LUX_ERR_INVALID_ARGUMENT, "render batch 1..2^28");
+            ctx->render_batch = static_cast<int>(value);
+            return LUX_OK;
         default:
             return lux::fail(LUX_ERR_INVALID_ARGUMENT, "unknown option");
     }
@@ -252,6 +258,7 @@ int lux_ctx_get_option(lux_ctx* ctx, int32_t option, int64_t* value) {
     switch (option) {
         case LUX_OPT_TRACE_VARIANT: *value = ctx->trace_variant; return LUX_OK;
         case LUX_OPT_TRACE_BUDGET: *value = ctx->trace_budget; return LUX_OK;
+        case LUX_OPT_RENDER_BATCH: *value = ctx->render_batch; return LUX_OK;
         default: return lux::fail(LUX_ERR_INVALID_ARGUMENT, "unknown option");
     }
 }
@@ -515,6 +522,88 @@ int lux_overlap_self(lux_ctx* ctx, const lux_bvh* bvh, int32_t* pairs, int64_t m
 int lux_overlap_cross(lux_ctx* ctx, const lux_bvh* left, const lux_bvh* right,
                       int32_t* pairs, int64_t max_pairs, int64_t* found) {
     return overlap_common(ctx, left, right, false, pairs, max_pairs, found);
+}
+
+// ------------------------------------------------------------------ scenes and rendering
+
+int lux_scene_create(lux_ctx* ctx, const lux_scene_desc* desc, lux_scene** out) {
+    if (int st = check_ctx(ctx)) return st;
+    if (!desc || !out) return lux::fail(LUX_ERR_INVALID_ARGUMENT, "null argument");
+    *out = nullptr;
+    return lux::scene_create(ctx, desc, out);
+}
+
+int lux_camera_perspective(const float origin[3], const float look_at[3], float vfov_degrees,
+                           float aspect, float lens_radius, float focal_distance,
+                           lux_camera_desc* out) {
+    if (!origin || !look_at || !out) return lux::fail(LUX_ERR_INVALID_ARGUMENT, "null argument");
+    return lux::camera_perspective(origin, look_at, vfov_degrees, aspect, lens_radius,
+                                   focal_distance, out);
+}
+
+int lux_scene_destroy(lux_scene* scene) {
+    if (!scene) return LUX_OK;
+    cudaSetDevice(scene->device);
+    cudaDeviceSynchronize();
+    lux::scene_free(scene);
+    delete scene;
+    return LUX_OK;
+}
+
+int lux_scene_info(const lux_scene* scene, int32_t* triangles, int32_t* area_lights,
+                   int32_t* lights) {
+    if (!scene) return lux::fail(LUX_ERR_INVALID_ARGUMENT, "null scene");
+    if (triangles) *triangles = scene->triangle_count;
+    if (area_lights) *area_lights = scene->area_light_count;
+    if (lights) *lights = scene->view.light_count;
+    return LUX_OK;
+}
+
+int lux_scene_update_mesh(lux_ctx* ctx, lux_scene* scene, int32_t mesh, const float* vertices) {
+    if (int st = check_ctx(ctx)) return st;
+    if (!scene || !vertices) return lux::fail(LUX_ERR_INVALID_ARGUMENT, "null argument");
+    return lux::scene_update_mesh(ctx, scene, mesh, vertices);
+}
+
+static int render_common(lux_ctx* ctx, const lux_scene* scene, const lux_render_request* req,
+                         float* out, bool per_sample) {
+    if (int st = check_ctx(ctx)) return st;
+    if (!scene || !req || !out) return lux::fail(LUX_ERR_INVALID_ARGUMENT, "null argument");
+    if (req->width <= 0 || req->height <= 0 || req->spp <= 0)
+        return lux::fail(LUX_ERR_INVALID_ARGUMENT, "render requires a non-empty film");
+    if (req->max_depth < 0 || req->max_depth > 1000)
+        return lux::fail(LUX_ERR_INVALID_ARGUMENT, "max_depth must be in 0..1000");
+    if (req->light_sampler != 0 && req->light_sampler != 1)
+        return lux::fail(LUX_ERR_INVALID_ARGUMENT, "light sampler: 0 uniform or 1 power");
+    if (static_cast<long long>(req->width) * req->height > (1ll << 30))
+        return lux::fail(LUX_ERR_INVALID_ARGUMENT, "image too large");
+    size_t pixels = static_cast<size_t>(req->width) * req->height;
+    size_t count = per_sample ? pixels * static_cast<size_t>(req->spp) : pixels;
+    Staging staging(ctx);
+    void* d_out = nullptr;
+    staging.add(out, sizeof(float) * 3 * count, false, true, &d_out);
+    int st = staging.begin();
+    if (st) return st;
+    st = lux::render(ctx, scene, *req, static_cast<float*>(d_out), per_sample);
+    if (st) return st;
+    st = finish_call(ctx, staging);
+    if (st) return st;
+    return sync_and_check(ctx);
+}
+
+int lux_render(lux_ctx* ctx, const lux_scene* scene, const lux_render_request* req,
+               float* film_sum) {
+    return render_common(ctx, scene, req, film_sum, false);
+}
+
+int lux_render_samples(lux_ctx* ctx, const lux_scene* scene, const lux_render_request* req,
+                       float* samples) {
+    return render_common(ctx, scene, req, samples, true);
+}
+
+int lux_render_ray_counts(lux_ctx* ctx, int64_t* counts) {
+    if (!ctx || !counts) return lux::fail(LUX_ERR_INVALID_ARGUMENT, "null argument");
+    return lux::render_ray_counts(ctx, counts);
 }
 
 }  // extern "C"

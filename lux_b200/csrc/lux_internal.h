@@ -18,6 +18,8 @@ struct lux_ctx {
     // Tunables (lux_ctx_set_option).
     int trace_variant = 0;           // lux::kTraceAuto / kTraceStatic / kTracePersistent
     int trace_budget = 32;           // traversal steps per refill round
+    int render_batch = 1 << 22;      // paths in flight per wavefront batch
+    void* render_runtime = nullptr;  // wavefront buffers, grown on demand
     // Growable device scratch, reused across calls on this context.
     void* scratch = nullptr;
     size_t scratch_bytes = 0;

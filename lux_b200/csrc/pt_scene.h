@@ -1,0 +1,54 @@
+// Host-side scene object of the path tracer (lux_scene) and the wavefront runtime.
+#pragma once
+
+#include <cstdint>
+#include <vector>
+
+#include "lux_internal.h"
+#include "pt_device.cuh"
+
+struct lux_scene {
+    int device = 0;
+    int triangle_count = 0;
+    int area_light_count = 0;
+    // Host copies kept for refits and light-table queries.
+    std::vector<lux::pt::Instance> instances;
+    std::vector<int> mesh_triangle_offset;  // first scene triangle per (instance order)
+    std::vector<std::vector<float>> mesh_vertices;     // object space, per mesh
+    std::vector<std::vector<uint32_t>> mesh_indices;   // per mesh
+    std::vector<int> tlas_instance_host;
+    // Device data.
+    lux::pt::Material* materials = nullptr;
+    lux::pt::SceneTri* tris = nullptr;
+    lux::pt::SceneTriShading* shading = nullptr;
+    lux::pt::Instance* d_instances = nullptr;
+    int* tlas_instance = nullptr;
+    lux::BvhView* blas_views = nullptr;
+    std::vector<lux_bvh*> blas;
+    lux_bvh* tlas = nullptr;
+    lux::pt::Light* lights = nullptr;
+    lux::pt::AliasEntry* light_alias = nullptr;
+    lux::pt::AliasEntry* light_alias_uniform = nullptr;  // unused placeholder
+    int* primitive_light = nullptr;
+    float* tri_soup = nullptr;          // per-mesh object-space soups for refits (device)
+    std::vector<size_t> soup_offset;    // float offset of each mesh's soup
+    float* tlas_boxes = nullptr;        // instance world boxes (device)
+    lux::pt::SceneView view;            // device pointers + counts (TLAS/BLAS filled in)
+};
+
+namespace lux {
+
+int scene_create(lux_ctx* ctx, const lux_scene_desc* desc, lux_scene** out);
+void scene_free(lux_scene* scene);
+int scene_update_mesh(lux_ctx* ctx, lux_scene* scene, int mesh, const float* vertices);
+int camera_perspective(const float* origin, const float* look_at, float vfov, float aspect,
+                       float lens_radius, float focal_distance, lux_camera_desc* out);
+
+// Wavefront renderer (wavefront.cu).  out is a device pointer: film sums (width*height*3)
+// or, when per_sample, every sample's radiance ((pixel*spp + s)*3).
+int render(lux_ctx* ctx, const lux_scene* scene, const lux_render_request& req, float* out,
+           bool per_sample);
+int render_ray_counts(lux_ctx* ctx, int64_t* counts);
+void render_runtime_free(lux_ctx* ctx);
+
+}  // namespace lux

@@ -1,0 +1,574 @@
+// Scene upload for the path tracer: world-space triangles, BLAS per mesh, TLAS over
+// instances, materials and light tables.
+//
+// Host arithmetic restates the reference's host preparation so that every uploaded
+// value is bit-identical to what the reference computes (paths relative to src/):
+//   transform_point / transform_normal / transform_bounds   core/mat4.cuh:173-275
+//   inverse_affine                                          core/mat4.cuh:131-160
+//   scene triangle order (instances, then local triangles)  scene/scene_data.h:282-329
+//   prepare_scene_light_sampling (area + explicit lights)   scene/scene_prepare.h:268-387
+//   build_alias_table_from_weights                          light/light_distribution.cpp:8-61
+// The host compiler evaluates these without contraction (x86-64 baseline ISA).
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "../../include/lux_gpu.h"
+#include "pt_scene.h"
+
+namespace lux {
+namespace {
+
+using pt::AliasEntry;
+using pt::Instance;
+using pt::Light;
+using pt::Material;
+
+struct V3 {
+    float x, y, z;
+};
+V3 v3(float x, float y, float z) { return V3{x, y, z}; }
+V3 operator-(V3 a, V3 b) { return v3(a.x - b.x, a.y - b.y, a.z - b.z); }
+float dot3(V3 a, V3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+V3 cross3(V3 a, V3 b) {
+    return v3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+}
+float len3(V3 a) { return std::sqrt(dot3(a, a)); }
+V3 normalize3(V3 v) {
+    float l = len3(v);
+    if (!(l > 0)) return v;
+    float inv = 1.0f / l;
+    return v3(v.x * inv, v.y * inv, v.z * inv);
+}
+
+// transform_point (core/mat4.cuh:173-184) on a row-major 3x4 affine matrix.
+V3 transform_point(const float* m, V3 p) {
+    float x = m[0] * p.x + m[1] * p.y + m[2] * p.z + m[3];
+    float y = m[4] * p.x + m[5] * p.y + m[6] * p.z + m[7];
+    float z = m[8] * p.x + m[9] * p.y + m[10] * p.z + m[11];
+    float w = 0.0f * p.x + 0.0f * p.y + 0.0f * p.z + 1.0f;
+    return w == 1 ? v3(x, y, z) : v3(x / w, y / w, z / w);
+}
+
+// transform_normal (core/mat4.cuh:207-230): adjugate-transpose, then normalize.
+V3 transform_normal(const float* m, V3 n) {
+    float a00 = m[5] * m[10] - m[6] * m[9];
+    float a01 = m[6] * m[8] - m[4] * m[10];
+    float a02 = m[4] * m[9] - m[5] * m[8];
+    float a10 = m[2] * m[9] - m[1] * m[10];
+    float a11 = m[0] * m[10] - m[2] * m[8];
+    float a12 = m[1] * m[8] - m[0] * m[9];
+    float a20 = m[1] * m[6] - m[2] * m[5];
+    float a21 = m[2] * m[4] - m[0] * m[6];
+    float a22 = m[0] * m[5] - m[1] * m[4];
+    V3 t = v3(a00 * n.x + a01 * n.y + a02 * n.z, a10 * n.x + a11 * n.y + a12 * n.z,
+              a20 * n.x + a21 * n.y + a22 * n.z);
+    return normalize3(t);
+}
+
+// transform_instance_normal (scene/scene_data.h:223-229).
+V3 instance_normal(const float* m, V3 n) {
+    if (dot3(n, n) == 0) return v3(0, 0, 0);
+    V3 t = transform_normal(m, n);
+    if (dot3(t, t) == 0) return v3(0, 0, 0);
+    return normalize3(t);
+}
+
+// inverse_affine (core/mat4.cuh:131-160).
+void inverse_affine(const float* m, float* r) {
+    float a00 = m[0], a01 = m[1], a02 = m[2];
+    float a10 = m[4], a11 = m[5], a12 = m[6];
+    float a20 = m[8], a21 = m[9], a22 = m[10];
+    float det = a00 * (a11 * a22 - a12 * a21) - a01 * (a10 * a22 - a12 * a20)
+              + a02 * (a10 * a21 - a11 * a20);
+    for (int i = 0; i < 12; ++i) r[i] = (i % 5 == 0) ? 1.0f : 0.0f;
+    if (std::fabs(det) <= 1e-12f) return;
+    float inv_det = 1.0f / det;
+    r[0] = (a11 * a22 - a12 * a21) * inv_det;
+    r[1] = -(a01 * a22 - a02 * a21) * inv_det;
+    r[2] = (a01 * a12 - a02 * a11) * inv_det;
+    r[4] = -(a10 * a22 - a12 * a20) * inv_det;
+    r[5] = (a00 * a22 - a02 * a20) * inv_det;
+    r[6] = -(a00 * a12 - a02 * a10) * inv_det;
+    r[8] = (a10 * a21 - a11 * a20) * inv_det;
+    r[9] = -(a00 * a21 - a01 * a20) * inv_det;
+    r[10] = (a00 * a11 - a01 * a10) * inv_det;
+    float tx = m[3], ty = m[7], tz = m[11];
+    r[3] = -(r[0] * tx + r[1] * ty + r[2] * tz);
+    r[7] = -(r[4] * tx + r[5] * ty + r[6] * tz);
+    r[11] = -(r[8] * tx + r[9] * ty + r[10] * tz);
+}
+
+float luminance(V3 v) { return 0.2126f * v.x + 0.7152f * v.y + 0.0722f * v.z; }
+
+struct Box {
+    V3 lo{INFINITY, INFINITY, INFINITY}, hi{-INFINITY, -INFINITY, -INFINITY};
+    void expand(V3 p) {
+        lo = v3(std::fmin(lo.x, p.x), std::fmin(lo.y, p.y), std::fmin(lo.z, p.z));
+        hi = v3(std::fmax(hi.x, p.x), std::fmax(hi.y, p.y), std::fmax(hi.z, p.z));
+    }
+    bool empty() const { return lo.x > hi.x || lo.y > hi.y || lo.z > hi.z; }
+};
+
+// build_alias_table_from_weights (light/light_distribution.cpp:8-61).
+std::vector<AliasEntry> alias_from_weights(const std::vector<float>& weights) {
+    int count = static_cast<int>(weights.size());
+    std::vector<AliasEntry> table(count);
+    if (count <= 0) return table;
+    float total = 0;
+    for (float w : weights) total += std::fmax(0.0f, w);
+    if (total <= 0) return {};
+    std::vector<float> scaled(count, 0);
+    std::vector<int> small, large;
+    for (int i = 0; i < count; ++i) {
+        float pmf = std::fmax(0.0f, weights[i]) / total;
+        table[i].pmf = pmf;
+        table[i].alias = i;
+        table[i].probability = 1.0f;
+        scaled[i] = pmf * static_cast<float>(count);
+        if (scaled[i] < 1.0f) small.push_back(i);
+        else large.push_back(i);
+    }
+    while (!small.empty() && !large.empty()) {
+        int less = small.back();
+        small.pop_back();
+        int more = large.back();
+        large.pop_back();
+        table[less].probability = scaled[less];
+        table[less].alias = more;
+        scaled[more] = (scaled[more] + scaled[less]) - 1.0f;
+        if (scaled[more] < 1.0f) small.push_back(more);
+        else large.push_back(more);
+    }
+    for (int i : large) { table[i].probability = 1.0f; table[i].alias = i; }
+    for (int i : small) { table[i].probability = 1.0f; table[i].alias = i; }
+    return table;
+}
+
+template <typename T>
+int upload(T** dst, const std::vector<T>& src, cudaStream_t stream) {
+    size_t bytes = sizeof(T) * std::max<size_t>(src.size(), 1);
+    cudaError_t err = cudaMalloc(reinterpret_cast<void**>(dst), bytes);
+    if (err != cudaSuccess) {
+        cudaGetLastError();
+        return fail(LUX_ERR_OUT_OF_MEMORY, "scene allocation failed");
+    }
+    if (!src.empty()) {
+        err = cudaMemcpyAsync(*dst, src.data(), sizeof(T) * src.size(), cudaMemcpyHostToDevice,
+                              stream);
+        if (err != cudaSuccess) return cuda_fail(err, "scene upload");
+    }
+    return LUX_OK;
+}
+
+Material to_material(const lux_material& m) {
+    Material r;
+    r.type = m.type;
+    r.albedo = make_f3(m.albedo[0], m.albedo[1], m.albedo[2]);
+    r.emission = make_f3(m.emission[0], m.emission[1], m.emission[2]);
+    r.two_sided = m.emission_two_sided ? 1 : 0;
+    r.roughness = m.roughness;
+    r.metallic = m.metallic;
+    r.eta = m.eta;
+    return r;
+}
+
+bool is_emissive(const lux_material& m) {
+    return std::fmax(m.emission[0], std::fmax(m.emission[1], m.emission[2])) > 0;
+}
+
+// World triangles and shading records of one instance, appended in local order.
+void instance_triangles(const lux_mesh_desc& mesh, const Instance& inst, int instance_id,
+                        int material_override, std::vector<pt::SceneTri>& tris,
+                        std::vector<pt::SceneTriShading>& shading) {
+    for (int t = 0; t < mesh.triangle_count; ++t) {
+        uint32_t idx[3] = {mesh.indices[3 * t], mesh.indices[3 * t + 1], mesh.indices[3 * t + 2]};
+        V3 w[3];
+        V3 n[3];
+        float uv[3][2] = {{0, 0}, {0, 0}, {0, 0}};
+        bool has_normals = mesh.normals != nullptr;
+        for (int k = 0; k < 3; ++k) {
+            const float* p = mesh.vertices + 3 * size_t(idx[k]);
+            w[k] = transform_point(inst.m, v3(p[0], p[1], p[2]));
+            if (mesh.normals) {
+                const float* q = mesh.normals + 3 * size_t(idx[k]);
+                n[k] = instance_normal(inst.m, v3(q[0], q[1], q[2]));
+                if (dot3(n[k], n[k]) <= 0) has_normals = false;
+            } else {
+                n[k] = v3(0, 0, 0);
+            }
+            if (mesh.uvs) {
+                uv[k][0] = mesh.uvs[2 * size_t(idx[k])];
+                uv[k][1] = mesh.uvs[2 * size_t(idx[k]) + 1];
+            }
+        }
+        int material = material_override >= 0 ? material_override : mesh.material_ids[t];
+        pt::SceneTri st;
+        int bits;
+        std::memcpy(&bits, &material, 4);
+        float fb;
+        std::memcpy(&fb, &material, 4);
+        st.v0 = make_float4(w[0].x, w[0].y, w[0].z, fb);
+        std::memcpy(&fb, &instance_id, 4);
+        st.v1 = make_float4(w[1].x, w[1].y, w[1].z, fb);
+        std::memcpy(&fb, &t, 4);
+        st.v2 = make_float4(w[2].x, w[2].y, w[2].z, fb);
+        tris.push_back(st);
+        pt::SceneTriShading sh;
+        sh.n0 = make_float4(n[0].x, n[0].y, n[0].z, uv[0][0]);
+        sh.n1 = make_float4(n[1].x, n[1].y, n[1].z, uv[0][1]);
+        sh.n2 = make_float4(n[2].x, n[2].y, n[2].z, uv[1][0]);
+        sh.uv = make_float4(uv[1][1], uv[2][0], uv[2][1], has_normals ? 1.0f : 0.0f);
+        shading.push_back(sh);
+        (void)bits;
+    }
+}
+
+std::vector<float> mesh_soup(const lux_mesh_desc& mesh, const float* vertices) {
+    std::vector<float> soup(size_t(mesh.triangle_count) * 9);
+    for (int t = 0; t < mesh.triangle_count; ++t) {
+        for (int k = 0; k < 3; ++k) {
+            const float* p = vertices + 3 * size_t(mesh.indices[3 * t + k]);
+            soup[size_t(t) * 9 + k * 3 + 0] = p[0];
+            soup[size_t(t) * 9 + k * 3 + 1] = p[1];
+            soup[size_t(t) * 9 + k * 3 + 2] = p[2];
+        }
+    }
+    return soup;
+}
+
+// Instance world box: transform_bounds (core/mat4.cuh:259-275) of the mesh box
+// (finalize_scene_mesh, scene/scene_data.h:215-220).
+Box instance_box(const std::vector<float>& soup, int triangle_count, const float* m) {
+    Box mesh_box;
+    for (size_t i = 0; i < size_t(triangle_count) * 3; ++i)
+        mesh_box.expand(v3(soup[3 * i], soup[3 * i + 1], soup[3 * i + 2]));
+    Box out;
+    if (mesh_box.empty()) return out;
+    for (int z = 0; z <= 1; ++z)
+        for (int y = 0; y <= 1; ++y)
+            for (int x = 0; x <= 1; ++x)
+                out.expand(transform_point(m, v3(x ? mesh_box.hi.x : mesh_box.lo.x,
+                                                 y ? mesh_box.hi.y : mesh_box.lo.y,
+                                                 z ? mesh_box.hi.z : mesh_box.lo.z)));
+    return out;
+}
+
+}  // namespace
+
+void scene_free(lux_scene* s) {
+    void* ptrs[] = {s->materials, s->tris, s->shading, s->d_instances, s->tlas_instance,
+                    s->blas_views, s->lights, s->light_alias, s->primitive_light, s->tri_soup,
+                    s->tlas_boxes};
+    for (void* p : ptrs)
+        if (p) cudaFree(p);
+    for (lux_bvh* b : s->blas) lux_bvh_destroy(b);
+    if (s->tlas) lux_bvh_destroy(s->tlas);
+    s->blas.clear();
+    s->tlas = nullptr;
+}
+
+int scene_create(lux_ctx* ctx, const lux_scene_desc* d, lux_scene** out) {
+    if (d->material_count < 0 || d->mesh_count < 0 || d->instance_count < 0 || d->light_count < 0)
+        return fail(LUX_ERR_INVALID_ARGUMENT, "negative scene counts");
+    for (int i = 0; i < d->mesh_count; ++i) {
+        const lux_mesh_desc& m = d->meshes[i];
+        if (m.triangle_count < 0 || m.vertex_count < 0 || (m.triangle_count > 0 &&
+            (!m.indices || !m.vertices || !m.material_ids)))
+            return fail(LUX_ERR_INVALID_ARGUMENT, "bad mesh description");
+        for (int t = 0; t < 3 * m.triangle_count; ++t)
+            if (m.indices[t] >= static_cast<uint32_t>(m.vertex_count))
+                return fail(LUX_ERR_INVALID_ARGUMENT, "mesh index out of range");
+        for (int t = 0; t < m.triangle_count; ++t)
+            if (m.material_ids[t] < 0 || m.material_ids[t] >= d->material_count)
+                return fail(LUX_ERR_INVALID_ARGUMENT, "material id out of range");
+    }
+    for (int i = 0; i < d->material_count; ++i)
+        if (d->materials[i].type < 0 || d->materials[i].type > 5)
+            return fail(LUX_ERR_INVALID_ARGUMENT, "unknown material type");
+    for (int i = 0; i < d->instance_count; ++i) {
+        const lux_instance_desc& in = d->instances[i];
+        if (in.mesh < 0 || in.mesh >= d->mesh_count)
+            return fail(LUX_ERR_INVALID_ARGUMENT, "instance mesh out of range");
+        if (in.material_override >= d->material_count)
+            return fail(LUX_ERR_INVALID_ARGUMENT, "instance material out of range");
+    }
+    for (int i = 0; i < d->light_count; ++i)
+        if (d->lights[i].kind < 1 || d->lights[i].kind > 3)
+            return fail(LUX_ERR_INVALID_ARGUMENT, "unknown light kind");
+
+    lux_scene* s = new (std::nothrow) lux_scene();
+    if (!s) return fail(LUX_ERR_OUT_OF_MEMORY, "scene allocation failed");
+    s->device = ctx->device;
+
+    // Instances and world triangles in scene-triangle order.
+    std::vector<pt::SceneTri> tris;
+    std::vector<pt::SceneTriShading> shading;
+    std::vector<int> primitive_light;
+    for (int i = 0; i < d->instance_count; ++i) {
+        const lux_instance_desc& in = d->instances[i];
+        Instance inst;
+        std::memcpy(inst.m, in.object_to_world, sizeof(inst.m));
+        bool given = false;
+        for (int k = 0; k < 12; ++k) given |= in.world_to_object[k] != 0.0f;
+        if (given) std::memcpy(inst.inv, in.world_to_object, sizeof(inst.inv));
+        else inverse_affine(inst.m, inst.inv);
+        inst.blas = in.mesh;
+        inst.first_primitive = static_cast<int>(tris.size());
+        s->instances.push_back(inst);
+        instance_triangles(d->meshes[in.mesh], inst, i, in.material_override, tris, shading);
+    }
+    s->triangle_count = static_cast<int>(tris.size());
+
+    // Light tables (scene/scene_prepare.h:268-387).
+    std::vector<Light> lights;
+    std::vector<float> cdf;
+    float total_power = 0;
+    primitive_light.assign(tris.size(), -1);
+    auto append = [&](const Light& l, float power) -> int {
+        if (power <= 0) return -1;
+        total_power += power;
+        lights.push_back(l);
+        cdf.push_back(total_power);
+        return static_cast<int>(lights.size()) - 1;
+    };
+    for (size_t t = 0; t < tris.size(); ++t) {
+        int material;
+        std::memcpy(&material, &tris[t].v0.w, 4);
+        const lux_material& mat = d->materials[material];
+        if (!is_emissive(mat)) continue;
+        V3 a = v3(tris[t].v0.x, tris[t].v0.y, tris[t].v0.z);
+        V3 b = v3(tris[t].v1.x, tris[t].v1.y, tris[t].v1.z);
+        V3 c = v3(tris[t].v2.x, tris[t].v2.y, tris[t].v2.z);
+        float area = 0.5f * len3(cross3(b - a, c - a));
+        if (area <= 0) continue;
+        Light l;
+        l.kind = 0;
+        l.primitive = static_cast<int>(t);
+        l.two_sided = mat.emission_two_sided ? 1 : 0;
+        l.area = area;
+        l.emission = make_f3(mat.emission[0], mat.emission[1], mat.emission[2]);
+        l.vec = make_f3(0, 0, 0);
+        float power = area * std::fmax(1e-6f, luminance(v3(mat.emission[0], mat.emission[1],
+                                                           mat.emission[2])));
+        int index = append(l, power);
+        if (index >= 0) {
+            int& stored = primitive_light[t];
+            stored = stored == -1 ? index : -2;
+        }
+    }
+    s->area_light_count = static_cast<int>(lights.size());
+    for (int i = 0; i < d->light_count; ++i) {
+        const lux_light_desc& ld = d->lights[i];
+        Light l;
+        l.kind = ld.kind;
+        l.primitive = -1;
+        l.two_sided = 0;
+        l.area = 0;
+        l.emission = make_f3(ld.value[0], ld.value[1], ld.value[2]);
+        V3 vec = v3(ld.vec[0], ld.vec[1], ld.vec[2]);
+        if (ld.kind == 2) vec = normalize3(vec);  // add_distant_light stores it normalised
+        l.vec = make_f3(vec.x, vec.y, vec.z);
+        append(l, std::fmax(1e-6f, luminance(v3(ld.value[0], ld.value[1], ld.value[2]))));
+    }
+    std::vector<float> weights;
+    float prev = 0;
+    for (float c : cdf) {
+        weights.push_back(c - prev);
+        prev = c;
+    }
+    std::vector<AliasEntry> alias = total_power > 0 ? alias_from_weights(weights)
+                                                    : std::vector<AliasEntry>{};
+
+    // Uploads.
+    std::vector<Material> mats;
+    for (int i = 0; i < d->material_count; ++i) mats.push_back(to_material(d->materials[i]));
+    int st = upload(&s->materials, mats, ctx->stream);
+    if (!st) st = upload(&s->tris, tris, ctx->stream);
+    if (!st) st = upload(&s->shading, shading, ctx->stream);
+    if (!st) st = upload(&s->d_instances, s->instances, ctx->stream);
+    if (!st) st = upload(&s->lights, lights, ctx->stream);
+    if (!st) st = upload(&s->light_alias, alias, ctx->stream);
+    if (!st) st = upload(&s->primitive_light, primitive_light, ctx->stream);
+
+    // BLAS per mesh over object-space soups.
+    std::vector<float> all_soup;
+    for (int m = 0; m < d->mesh_count && !st; ++m) {
+        const lux_mesh_desc& mesh = d->meshes[m];
+        s->mesh_vertices.emplace_back(mesh.vertices, mesh.vertices + 3 * size_t(mesh.vertex_count));
+        s->mesh_indices.emplace_back(mesh.indices, mesh.indices + 3 * size_t(mesh.triangle_count));
+        std::vector<float> soup = mesh_soup(mesh, mesh.vertices);
+        s->soup_offset.push_back(all_soup.size());
+        all_soup.insert(all_soup.end(), soup.begin(), soup.end());
+    }
+    if (!st) st = upload(&s->tri_soup, all_soup, ctx->stream);
+    std::vector<BvhView> views;
+    for (int m = 0; m < d->mesh_count && !st; ++m) {
+        lux_bvh* b = nullptr;
+        st = lux_lbvh_build(ctx, s->tri_soup + s->soup_offset[m], d->meshes[m].triangle_count,
+                            LUX_PRIM_TRIANGLES, 30, &b);
+        if (!st) {
+            s->blas.push_back(b);
+            views.push_back(b->view());
+        }
+    }
+    if (!st) st = upload(&s->blas_views, views, ctx->stream);
+
+    // TLAS over non-empty instance boxes (collect_scene_tlas_build_primitives,
+    // scene/scene_prepare.h:441-462): primitive k is instance tlas_instance[k].
+    std::vector<float> boxes;
+    for (int i = 0; i < d->instance_count && !st; ++i) {
+        const lux_mesh_desc& mesh = d->meshes[d->instances[i].mesh];
+        std::vector<float> soup = mesh_soup(mesh, mesh.vertices);
+        Box b = instance_box(soup, mesh.triangle_count, s->instances[i].m);
+        if (b.empty()) continue;
+        s->tlas_instance_host.push_back(i);
+        float f[6] = {b.lo.x, b.lo.y, b.lo.z, b.hi.x, b.hi.y, b.hi.z};
+        boxes.insert(boxes.end(), f, f + 6);
+    }
+    if (!st) st = upload(&s->tlas_boxes, boxes, ctx->stream);
+    if (!st) st = upload(&s->tlas_instance, s->tlas_instance_host, ctx->stream);
+    if (!st) {
+        st = lux_lbvh_build(ctx, s->tlas_boxes, static_cast<int>(s->tlas_instance_host.size()),
+                            LUX_PRIM_AABBS, 30, &s->tlas);
+    }
+    if (!st) st = cuda_fail(cudaStreamSynchronize(ctx->stream), "scene upload");
+    if (st) {
+        scene_free(s);
+        delete s;
+        return st;
+    }
+
+    pt::SceneView& v = s->view;
+    v.materials = s->materials;
+    v.material_count = d->material_count;
+    v.tris = s->tris;
+    v.shading = s->shading;
+    v.primitive_count = s->triangle_count;
+    v.instances = s->d_instances;
+    v.instance_count = d->instance_count;
+    v.tlas = s->tlas->view();
+    v.tlas_instance = s->tlas_instance;
+    v.blas = s->blas_views;
+    v.lights = s->lights;
+    v.light_count = static_cast<int>(lights.size());
+    v.total_light_power = total_power;
+    v.light_alias = alias.empty() ? nullptr : s->light_alias;
+    v.light_sampler = 1;
+    v.primitive_light = s->primitive_light;
+    v.has_two_level = s->tlas->n > 0 && d->instance_count > 0;
+    const lux_camera_desc& c = d->camera;
+    v.camera.origin = make_f3(c.origin[0], c.origin[1], c.origin[2]);
+    v.camera.lower_left = make_f3(c.lower_left[0], c.lower_left[1], c.lower_left[2]);
+    v.camera.horizontal = make_f3(c.horizontal[0], c.horizontal[1], c.horizontal[2]);
+    v.camera.vertical = make_f3(c.vertical[0], c.vertical[1], c.vertical[2]);
+    v.camera.lens_u = make_f3(c.lens_u[0], c.lens_u[1], c.lens_u[2]);
+    v.camera.lens_v = make_f3(c.lens_v[0], c.lens_v[1], c.lens_v[2]);
+    v.camera.lens_radius = c.lens_radius;
+    *out = s;
+    return LUX_OK;
+}
+
+// make_perspective_camera (camera/camera.h:77-126) with make_camera_frame (:77-88).
+int camera_perspective(const float* origin, const float* look_at, float vfov, float aspect,
+                       float lens_radius, float focal_distance, lux_camera_desc* out) {
+    const float pi = 3.14159265358979323846f;
+    V3 o = v3(origin[0], origin[1], origin[2]);
+    V3 at = v3(look_at[0], look_at[1], look_at[2]);
+    V3 forward = normalize3(at - o);
+    V3 up_world = v3(0, 1, 0);
+    V3 right = normalize3(cross3(up_world, forward));
+    if (dot3(right, right) == 0) right = normalize3(cross3(v3(0, 0, 1), forward));
+    V3 up = cross3(forward, right);
+    float theta = vfov * pi / 180.0f;
+    float vh = 2.0f * std::tan(theta * 0.5f);
+    float vw = aspect * vh;
+    float focus = focal_distance > 0 ? focal_distance : len3(at - o);
+    if (focus <= 0) focus = 1;
+    auto scale = [](V3 v, float s) { return v3(v.x * s, v.y * s, v.z * s); };
+    V3 horizontal = scale(right, vw * focus);
+    V3 vertical = scale(up, vh * focus);
+    V3 f = scale(forward, focus);
+    V3 ll = v3(o.x + f.x, o.y + f.y, o.z + f.z);
+    V3 h2 = scale(horizontal, 0.5f);
+    V3 v2 = scale(vertical, 0.5f);
+    ll = v3(ll.x - h2.x, ll.y - h2.y, ll.z - h2.z);
+    ll = v3(ll.x - v2.x, ll.y - v2.y, ll.z - v2.z);
+    auto put = [](float* d, V3 v) { d[0] = v.x; d[1] = v.y; d[2] = v.z; };
+    put(out->origin, o);
+    put(out->lower_left, ll);
+    put(out->horizontal, horizontal);
+    put(out->vertical, vertical);
+    put(out->lens_u, right);
+    put(out->lens_v, up);
+    out->lens_radius = lens_radius;
+    return LUX_OK;
+}
+
+int scene_update_mesh(lux_ctx* ctx, lux_scene* s, int mesh, const float* vertices) {
+    if (mesh < 0 || mesh >= static_cast<int>(s->blas.size()))
+        return fail(LUX_ERR_INVALID_ARGUMENT, "mesh out of range");
+    std::vector<float>& verts = s->mesh_vertices[mesh];
+    std::memcpy(verts.data(), vertices, sizeof(float) * verts.size());
+    lux_mesh_desc md{};
+    md.vertices = verts.data();
+    md.vertex_count = static_cast<int>(verts.size() / 3);
+    md.indices = s->mesh_indices[mesh].data();
+    md.triangle_count = static_cast<int>(s->mesh_indices[mesh].size() / 3);
+    std::vector<float> soup = mesh_soup(md, verts.data());
+    cudaError_t err = cudaMemcpyAsync(s->tri_soup + s->soup_offset[mesh], soup.data(),
+                                      sizeof(float) * soup.size(), cudaMemcpyHostToDevice,
+                                      ctx->stream);
+    if (err != cudaSuccess) return cuda_fail(err, "mesh upload");
+    int st = lux_lbvh_refit(ctx, s->blas[mesh], s->tri_soup + s->soup_offset[mesh],
+                            md.triangle_count);
+    if (st) return st;
+    // World triangles of every instance of this mesh (normals unchanged).
+    std::vector<pt::SceneTri> tris;
+    std::vector<pt::SceneTriShading> shading;
+    std::vector<float> boxes;
+    for (size_t i = 0; i < s->instances.size(); ++i) {
+        if (s->instances[i].blas != mesh) continue;
+        tris.clear();
+        shading.clear();
+        md.material_ids = nullptr;
+        std::vector<int> mids(md.triangle_count, 0);
+        md.material_ids = mids.data();
+        instance_triangles(md, s->instances[i], static_cast<int>(i), 0, tris, shading);
+        // Keep the uploaded material ids: patch positions only.
+        std::vector<pt::SceneTri> old(tris.size());
+        err = cudaMemcpy(old.data(), s->tris + s->instances[i].first_primitive,
+                         sizeof(pt::SceneTri) * old.size(), cudaMemcpyDeviceToHost);
+        if (err != cudaSuccess) return cuda_fail(err, "triangle download");
+        for (size_t t = 0; t < tris.size(); ++t) tris[t].v0.w = old[t].v0.w;
+        err = cudaMemcpyAsync(s->tris + s->instances[i].first_primitive, tris.data(),
+                              sizeof(pt::SceneTri) * tris.size(), cudaMemcpyHostToDevice,
+                              ctx->stream);
+        if (err != cudaSuccess) return cuda_fail(err, "triangle upload");
+    }
+    for (size_t k = 0; k < s->tlas_instance_host.size(); ++k) {
+        const Instance& inst = s->instances[s->tlas_instance_host[k]];
+        Box b = instance_box(mesh_soup(lux_mesh_desc{s->mesh_vertices[inst.blas].data(), nullptr,
+                                                     nullptr,
+                                                     static_cast<int>(s->mesh_vertices[inst.blas].size() / 3),
+                                                     s->mesh_indices[inst.blas].data(), nullptr,
+                                                     static_cast<int>(s->mesh_indices[inst.blas].size() / 3)},
+                                       s->mesh_vertices[inst.blas].data()),
+                             static_cast<int>(s->mesh_indices[inst.blas].size() / 3), inst.m);
+        float f[6] = {b.lo.x, b.lo.y, b.lo.z, b.hi.x, b.hi.y, b.hi.z};
+        boxes.insert(boxes.end(), f, f + 6);
+    }
+    err = cudaMemcpyAsync(s->tlas_boxes, boxes.data(), sizeof(float) * boxes.size(),
+                          cudaMemcpyHostToDevice, ctx->stream);
+    if (err != cudaSuccess) return cuda_fail(err, "instance box upload");
+    st = lux_lbvh_refit(ctx, s->tlas, s->tlas_boxes, static_cast<int>(s->tlas_instance_host.size()));
+    if (st) return st;
+    return cuda_fail(cudaStreamSynchronize(ctx->stream), "mesh update");
+}
+
+}  // namespace lux

@@ -112,11 +112,33 @@ class Ref:
         lib.ref_cornell_scene.restype = _I
         lib.ref_cornell_render.argtypes = [_I, _I, _I, _I, ctypes.c_uint64, _I, _I, _I,
                                            _P, _P, _P]
+        lib.ref_render_scene.argtypes = [_P, _I, _P, _P, _I, _P, _I, _P, _I, _I, _I, _I,
+                                         ctypes.c_uint64, _I, _I, _I, _I, _P]
         lib.ref_tree_create.argtypes = [_P, _I, _I]
         lib.ref_tree_create.restype = _P
         lib.ref_tree_destroy.argtypes = [_P]
         lib.ref_tree_trace.argtypes = [_P, _P, _I, _I, _P, _P]
         self.lib = lib
+
+    def render_scene(self, tris, material_ids, materials, lights, camera, width, height, spp,
+                     max_depth, seed, light_sampler=1, rows=None, threads=1):
+        """Per-sample radiance [pixel][spp][3] of a single-mesh scene (see ref_harness.cpp).
+
+        materials: N x 11 (type, albedo3, emission3, roughness, metallic, eta, two_sided);
+        lights: L x 7 (kind, vec3, value3); camera: origin3, look_at3, vfov, aspect.
+        """
+        tris = np.ascontiguousarray(tris, np.float32)
+        mids = np.ascontiguousarray(material_ids, np.int32)
+        mats = np.ascontiguousarray(materials, np.float32)
+        lights = np.ascontiguousarray(lights, np.float32).reshape(-1, 7)
+        cam = np.ascontiguousarray(camera, np.float32)
+        y0, y1 = rows if rows is not None else (0, height)
+        out = np.zeros(((y1 - y0) * width, spp, 3), np.float32)
+        self.lib.ref_render_scene(tris.ctypes.data, len(tris), mids.ctypes.data, mats.ctypes.data,
+                                  len(mats), lights.ctypes.data if len(lights) else None,
+                                  len(lights), cam.ctypes.data, width, height, spp, max_depth,
+                                  seed, light_sampler, y0, y1, threads, out.ctypes.data)
+        return out
 
     def tree_create(self, prims: np.ndarray, kind: int = 0):
         """Builds and keeps a host tree (build_cpu_lbvh_tree); returns an opaque handle."""

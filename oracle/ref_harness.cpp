@@ -365,4 +365,72 @@ int ref_cornell_render(int width, int height, int spp, int max_depth, uint64_t s
     return 0;
 }
 
+// A general single-mesh scene through the reference's own authoring and tracing code:
+// triangles (world space, 9 floats) with material ids; materials as 11 floats each
+// (type, albedo rgb, emission rgb, roughness, metallic, eta, two-sided flag); explicit
+// lights as 7 floats (kind 1 point / 2 distant / 3 uniform infinite, vec3, value3);
+// camera: origin3, look_at3, vertical fov degrees, aspect (make_pinhole_camera).
+// samples receives [pixel][spp][3] for rows [y0, y1).
+int ref_render_scene(const float* tris, int ntri, const int32_t* mids, const float* mats, int nmat,
+                     const float* lights, int nlights, const float* cam, int width, int height,
+                     int spp, int max_depth, uint64_t seed, int light_sampler, int y0, int y1,
+                     int threads, float* samples) {
+    Scene scene;
+    for (int m = 0; m < nmat; ++m) {
+        const float* f = mats + size_t(m) * 11;
+        scene.materials.push_back(Material(static_cast<MaterialType>(static_cast<int>(f[0])),
+                                           vec3(f[1], f[2], f[3]), vec3(f[4], f[5], f[6]), f[7],
+                                           f[8], f[9],
+                                           f[10] != 0 ? EmissionSidedness::DoubleSided
+                                                      : EmissionSidedness::SingleSided));
+    }
+    for (int t = 0; t < ntri; ++t) {
+        const float* v = tris + size_t(t) * 9;
+        add_triangle(scene, Triangle{vec3(v[0], v[1], v[2]), vec3(v[3], v[4], v[5]),
+                                     vec3(v[6], v[7], v[8])},
+                     mids[t]);
+    }
+    for (int l = 0; l < nlights; ++l) {
+        const float* f = lights + size_t(l) * 7;
+        int kind = static_cast<int>(f[0]);
+        if (kind == 1) add_point_light(scene, vec3(f[1], f[2], f[3]), vec3(f[4], f[5], f[6]));
+        if (kind == 2) add_distant_light(scene, vec3(f[1], f[2], f[3]), vec3(f[4], f[5], f[6]));
+        if (kind == 3) add_uniform_infinite_light(scene, vec3(f[4], f[5], f[6]));
+    }
+    scene.camera = make_pinhole_camera(vec3(cam[0], cam[1], cam[2]), vec3(cam[3], cam[4], cam[5]),
+                                       cam[6], cam[7]);
+    PreparedScene prepared(std::move(scene));
+    prepared.prepare_host_bvh();
+    SceneLightSampler lights_sampler = make_scene_light_sampler(
+        prepared.host_scene(), prepared.light_sampling(),
+        light_sampler == 0 ? LightSamplerKind::Uniform : LightSamplerKind::Power);
+    RenderSettings settings;
+    settings.max_depth = max_depth;
+    settings.seed = seed;
+    const Scene& sc = prepared.host_scene();
+    parallel_for((y1 - y0) * width, threads, [&](int begin, int end) {
+        for (int idx = begin; idx < end; ++idx) {
+            int y = y0 + idx / width;
+            int x = idx % width;
+            int pixel = y * width + x;
+            for (int s = 0; s < spp; ++s) {
+                SamplerState sampler = make_render_sampler(settings, pixel, s);
+                Float jx = sampler_get_1d(sampler);
+                Float jy = sampler_get_1d(sampler);
+                CameraSample cs;
+                cs.p_film = vec2((Float(x) + jx) / Float(width),
+                                 (Float(height - 1 - y) + jy) / Float(height));
+                cs.p_lens = sampler_get_2d(sampler);
+                cs.time = sampler_get_1d(sampler);
+                CameraRay generated = generate_camera_ray(sc.camera, cs);
+                vec3 L = trace_path(sc, prepared.host_bvh(), lights_sampler, generated.ray, sampler,
+                                    max_depth);
+                float* o = samples + (size_t(idx) * spp + s) * 3;
+                o[0] = L.x; o[1] = L.y; o[2] = L.z;
+            }
+        }
+    });
+    return 0;
+}
+
 }  // extern "C"

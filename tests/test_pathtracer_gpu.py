@@ -1,0 +1,190 @@
+"""Wavefront path tracer vs the reference CPU tracer (B200).
+
+The GPU tracer draws the same random numbers in the same order and restates the same
+arithmetic, so most samples agree to ~1e-6; the few that differ are paths where CUDA's
+sinf/cosf/powf rounded a last bit differently and a later discrete decision flipped.
+Criteria: (1) per-sample agreement within 1e-4 relative for >= 99% of samples; (2) the
+north_star's per-pixel mean within 3 sigma at equal spp (fraction of pixels with |z| > 3
+at most 1%); (3) film sums equal the sum of the per-sample values in sample order.
+"""
+import os
+
+import numpy as np
+import pytest
+
+import lux_b200
+from lux_b200 import scene as S
+from oracle.bindings import Ref
+
+pytestmark = pytest.mark.gpu
+
+ROOT = os.path.abspath(os.path.join(os.path.dirname(__file__), ".."))
+THREADS = os.cpu_count() or 1
+
+
+def _agreement(gpu, ref, rtol=1e-4):
+    close = np.all(np.abs(gpu - ref) <= rtol * (1.0 + np.abs(ref)), axis=-1)
+    return close.mean()
+
+
+def _z_fraction(gpu, ref):
+    """Fraction of pixel-channels whose mean differs by more than 3 sigma."""
+    n = gpu.shape[1]
+    mg, mr = gpu.mean(axis=1), ref.mean(axis=1)
+    vg, vr = gpu.var(axis=1, ddof=1), ref.var(axis=1, ddof=1)
+    se = np.sqrt((vg + vr) / n)
+    diff = np.abs(mg - mr)
+    # Zero variance on both sides: the means must then be equal.
+    outside = np.where(se > 0, diff > 3 * se, diff > 0)
+    return outside.mean()
+
+
+def _ref_arrays(b: S.SceneBuilder):
+    tris = b.world_triangles()
+    mids = np.asarray(b._mids, np.int32)
+    mats = np.array([[m.type, *m.albedo, *m.emission, m.roughness, m.metallic, m.eta,
+                      m.emission_two_sided] for m in b.materials], np.float32)
+    lights = np.array([[l.kind, *l.vec, *l.value] for l in b.lights], np.float32).reshape(-1, 7)
+    return tris, mids, mats, lights
+
+
+def test_cornell_matches_reference_fixture(ctx):
+    g = np.load(os.path.join(ROOT, "tests", "golden", "cornell_reference.npz"))
+    w, h, spp, depth, seed = (int(g[k]) for k in ("width", "height", "spp", "max_depth", "seed"))
+    b = S.make_cornell_scene(w, h)
+    assert np.array_equal(b.world_triangles(), g["triangles"])
+    sc = S.Scene(ctx, b)
+    req = S.request(w, h, spp, depth, seed)
+    samples = S.render_samples(ctx, sc, req)
+    assert _agreement(samples, g["samples"]) >= 0.99
+    assert _z_fraction(samples, g["samples"]) <= 0.01
+    film = S.render(ctx, sc, req).reshape(-1, 3)
+    want = np.zeros_like(film)
+    for s in range(spp):
+        want = (want + samples[:, s]).astype(np.float32)
+    assert np.array_equal(film, want)
+    rel = np.abs(film - g["film_sum"]) / (1 + np.abs(g["film_sum"]))
+    assert np.quantile(rel, 0.99) < 1e-4
+
+
+@pytest.mark.skipif(not Ref.available(), reason="reference harness not built")
+def test_cornell_config1_shape_matches_reference_live(ctx):
+    """Config-1 settings (power sampler, depth 4, seed 1) at 96x96, 16 spp."""
+    w = h = 96
+    spp, depth, seed = 16, 4, 1
+    sc = S.Scene(ctx, S.make_cornell_scene(w, h))
+    gpu = S.render_samples(ctx, sc, S.request(w, h, spp, depth, seed))
+    ref = Ref()
+    _, _, want = ref.cornell_render(w, h, spp, depth, seed, threads=THREADS, samples=True)
+    assert _agreement(gpu, want) >= 0.99
+    assert _z_fraction(gpu, want) <= 0.01
+    counts = S.ray_counts(ctx)
+    assert counts[0] >= w * h * spp and counts[1] > 0
+
+
+def material_zoo(width=48, height=48):
+    """Every BSDF and light kind the wavefront path supports, in one closed room."""
+    b = S.SceneBuilder()
+    f = np.float32
+    white = b.add_material(S.lambert((f(0.75), f(0.75), f(0.72))))
+    blue = b.add_material(S.lambert((f(0.2), f(0.3), f(0.7))))
+    glossy = b.add_material(S.ggx((f(0.8), f(0.6), f(0.3)), f(0.3), f(0.0)))
+    metal = b.add_material(S.ggx((f(0.9), f(0.9), f(0.9)), f(0.15), f(1.0)))
+    thin = b.add_material(S.material(S.THIN_LAMBERT, (f(0.6), f(0.8), f(0.6))))
+    glass = b.add_material(S.dielectric((1, 1, 1), f(1.5)))
+    tint = b.add_material(S.tinted_filter((f(0.25), f(0.65), f(1.0))))
+    iface = b.add_material(S.interface())
+    light = b.add_material(S.emissive((12.0, 11.0, 9.0)))
+    light2 = b.add_material(S.emissive((3.0, 3.0, 5.0), two_sided=True))
+    b.add_quad((-1, 0, 2), (1, 0, 2), (1, 0, -1), (-1, 0, -1), white)        # floor
+    b.add_quad((-1, 2, -1), (1, 2, -1), (1, 2, 2), (-1, 2, 2), white)        # ceiling
+    b.add_quad((-1, 0, -1), (1, 0, -1), (1, 2, -1), (-1, 2, -1), blue)       # back
+    b.add_quad((-1, 0, 2), (-1, 0, -1), (-1, 2, -1), (-1, 2, 2), glossy)     # left (GGX)
+    b.add_quad((1, 0, -1), (1, 0, 2), (1, 2, 2), (1, 2, -1), metal)          # right (metal)
+    b.add_quad((-0.8, 0.1, 0.2), (-0.2, 0.1, 0.2), (-0.2, 0.8, 0.2), (-0.8, 0.8, 0.2), thin)
+    # glass box
+    x0, y0, z0, x1, y1, z1 = 0.2, 0.0, 0.3, 0.7, 0.6, 0.8
+    p = [(x0, y0, z0), (x0, y0, z1), (x0, y1, z0), (x0, y1, z1),
+         (x1, y0, z0), (x1, y0, z1), (x1, y1, z0), (x1, y1, z1)]
+    for q in [(0, 4, 6, 2), (5, 1, 3, 7), (1, 0, 2, 3), (4, 5, 7, 6), (2, 6, 7, 3), (1, 5, 4, 0)]:
+        b.add_quad(p[q[0]], p[q[1]], p[q[2]], p[q[3]], glass)
+    b.add_quad((-0.9, 1.2, 1.0), (0.9, 1.2, 1.0), (0.9, 1.2, 0.4), (-0.9, 1.2, 0.4), tint)
+    b.add_quad((-0.5, 0.9, 1.3), (0.5, 0.9, 1.3), (0.5, 1.6, 1.3), (-0.5, 1.6, 1.3), iface)
+    b.add_quad((-0.3, 1.99, 0.3), (0.3, 1.99, 0.3), (0.3, 1.99, 0.9), (-0.3, 1.99, 0.9), light)
+    b.add_quad((0.5, 1.5, -0.95), (0.9, 1.5, -0.95), (0.9, 1.9, -0.95), (0.5, 1.9, -0.95), light2)
+    b.add_point_light((0.0, 1.7, 1.5), (2.0, 2.0, 2.0))
+    b.add_distant_light((-0.3, 1.0, 0.4), (0.3, 0.3, 0.3))
+    b.add_uniform_infinite_light((0.05, 0.05, 0.08))
+    cam = ((0.0, 1.0, 3.2), (0.0, 0.9, 0.5), 45.0, float(f(width) / f(height)))
+    b.set_pinhole_camera(*cam)
+    return b, cam
+
+
+@pytest.mark.skipif(not Ref.available(), reason="reference harness not built")
+@pytest.mark.parametrize("sampler,depth", [(S.SAMPLER_POWER, 6), (S.SAMPLER_UNIFORM, 3)])
+def test_material_zoo_matches_reference_live(ctx, sampler, depth):
+    w = h = 48
+    spp, seed = 32, 5
+    b, cam = material_zoo(w, h)
+    sc = S.Scene(ctx, b)
+    gpu = S.render_samples(ctx, sc, S.request(w, h, spp, depth, seed, light_sampler=sampler))
+    tris, mids, mats, lights = _ref_arrays(b)
+    camera = np.array([*cam[0], *cam[1], cam[2], cam[3]], np.float32)
+    ref = Ref().render_scene(tris, mids, mats, lights, camera, w, h, spp, depth, seed,
+                             light_sampler=sampler, threads=THREADS)
+    assert np.isfinite(gpu).all()
+    assert _agreement(gpu, ref) >= 0.97
+    assert _z_fraction(gpu, ref) <= 0.01
+    # The scene exercises every path: lights, passthrough and glass contribute.
+    assert gpu.mean() > 0
+
+
+def test_render_is_deterministic_and_batches_agree(ctx):
+    w = h = 40
+    sc = S.Scene(ctx, S.make_cornell_scene(w, h))
+    req = S.request(w, h, 12, 4, 3)
+    a = S.render(ctx, sc, req)
+    b = S.render(ctx, sc, req)
+    assert np.array_equal(a, b)
+    old = ctx.get_option(3)
+    try:
+        ctx.set_option(3, 1000)   # force many small batches (pixel ranges x 1 sample)
+        c = S.render(ctx, sc, req)
+        ctx.set_option(3, 5 * w * h)  # sample ranges of 5
+        d = S.render(ctx, sc, req)
+    finally:
+        ctx.set_option(3, old)
+    assert np.array_equal(a, c)
+    assert np.array_equal(a, d)
+
+
+def test_sample_offset_and_frame_index_continue_the_sequence(ctx):
+    """RenderSettings::sample_offset (integrator/render_context.h:52): two halves of the
+    samples rendered separately equal the full render's samples."""
+    w = h = 24
+    sc = S.Scene(ctx, S.make_cornell_scene(w, h))
+    full = S.render_samples(ctx, sc, S.request(w, h, 8, 4, 9))
+    first = S.render_samples(ctx, sc, S.request(w, h, 4, 4, 9))
+    second = S.render_samples(ctx, sc, S.request(w, h, 4, 4, 9, sample_offset=4))
+    assert np.array_equal(full[:, :4], first)
+    assert np.array_equal(full[:, 4:], second)
+    other = S.render_samples(ctx, sc, S.request(w, h, 8, 4, 9, frame_index=1))
+    assert not np.array_equal(full, other)
+
+
+def test_invalid_requests_fail_cleanly(ctx):
+    sc = S.Scene(ctx, S.make_cornell_scene(8, 8))
+    for bad in [S.request(0, 8, 1, 4), S.request(8, 8, 0, 4), S.request(8, 8, 1, -1),
+                S.request(8, 8, 1, 4, light_sampler=2)]:
+        with pytest.raises(lux_b200.LuxError) as e:
+            S.render(ctx, sc, bad)
+        assert e.value.status == lux_b200.LUX_ERR_INVALID_ARGUMENT
+
+
+def test_empty_scene_renders_black(ctx):
+    b = S.SceneBuilder()
+    b.add_material(S.lambert((0.5, 0.5, 0.5)))
+    b.set_pinhole_camera((0, 0, 3), (0, 0, 0), 40.0, 1.0)
+    sc = S.Scene(ctx, b)
+    film = S.render(ctx, sc, S.request(8, 8, 2, 3))
+    assert np.all(film == 0)
