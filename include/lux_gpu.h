@@ -105,6 +105,15 @@ int lux_lbvh_rebuild(lux_ctx* ctx, lux_bvh* bvh, const float* prims, int32_t n);
 
 int lux_bvh_destroy(lux_bvh* bvh);
 
+/*
+ * Attaches triangles (n x 9 floats, input order) to a BVH built from boxes, so that the
+ * ray queries accept it: the reference builds from BvhBuildPrimitive boxes and passes
+ * the triangles only at query time (intersect_gpu_bvh_stackless, bvh/gpu_bvh.cu:893-915).
+ * Results equal those of a BVH built from the triangles when the boxes are the
+ * triangles' boxes.
+ */
+int lux_bvh_attach_triangles(lux_ctx* ctx, lux_bvh* bvh, const float* tris, int32_t n);
+
 /* Primitive count, kind, Morton width and the root box (6 floats, host). */
 int lux_bvh_info(lux_ctx* ctx, const lux_bvh* bvh, int32_t* n, int32_t* kind,
                  int32_t* morton_bits, float* root_bounds);

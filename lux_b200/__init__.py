@@ -59,6 +59,7 @@ SIGNATURES = {
     "lux_lbvh_rebuild": (ctypes.c_int, [_P, _P, _P, _I32]),
     "lux_trace_closest_stats": (ctypes.c_int, [_P, _P, _P, _I32, _P]),
     "lux_bvh_destroy": (ctypes.c_int, [_P]),
+    "lux_bvh_attach_triangles": (ctypes.c_int, [_P, _P, _P, _I32]),
     "lux_bvh_info": (ctypes.c_int, [_P, _P, _P, _P, _P, _P]),
     "lux_bvh_download": (ctypes.c_int, [_P, _P, _P, _P, _P, _P, _P]),
     "lux_trace_closest": (ctypes.c_int, [_P, _P, _P, _I32, _P, _P]),
@@ -200,6 +201,11 @@ class Bvh:
         per = 9 if self.kind == PRIM_TRIANGLES else 6
         _check(self.ctx._lib.lux_lbvh_refit(self.ctx._h, self._h, _ptr(prims),
                                             _count(prims, per)))
+
+    def attach_triangles(self, tris) -> None:
+        """Makes a box BVH answer triangle ray queries (triangles in input order)."""
+        _check(self.ctx._lib.lux_bvh_attach_triangles(self.ctx._h, self._h, _ptr(tris),
+                                                      _count(tris, 9)))
 
     def rebuild(self, prims) -> None:
         per = 9 if self.kind == PRIM_TRIANGLES else 6

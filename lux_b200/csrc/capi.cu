@@ -302,6 +302,7 @@ int lux_lbvh_build(lux_ctx* ctx, const float* prims, int32_t n, int32_t kind,
     bvh->kind = kind;
     bvh->morton_bits = morton_bits;
     bvh->device = ctx->device;
+    bvh->has_triangles = kind == LUX_PRIM_TRIANGLES;
     int st = lux::lbvh_alloc(ctx, bvh);
     if (st) {
         delete bvh;
@@ -341,6 +342,7 @@ int lux_lbvh_rebuild(lux_ctx* ctx, lux_bvh* bvh, const float* prims, int32_t n) 
         }
     }
     bvh->n = n;
+    bvh->has_triangles = bvh->kind == LUX_PRIM_TRIANGLES;  // attached triangles go stale
     size_t per = bvh->kind == LUX_PRIM_TRIANGLES ? 9 : 6;
     Staging staging(ctx);
     void* d_prims = nullptr;
@@ -365,6 +367,22 @@ int lux_lbvh_refit(lux_ctx* ctx, lux_bvh* bvh, const float* prims, int32_t n) {
     if (!st) st = lux::lbvh_refit(ctx, bvh, static_cast<const float*>(d_prims));
     if (!st) st = finish_call(ctx, staging);
     if (!st && !staging.items.empty()) st = sync_and_check(ctx);
+    return st;
+}
+
+int lux_bvh_attach_triangles(lux_ctx* ctx, lux_bvh* bvh, const float* tris, int32_t n) {
+    if (int st = check_ctx(ctx)) return st;
+    if (!bvh) return lux::fail(LUX_ERR_INVALID_ARGUMENT, "null bvh");
+    if (n != bvh->n) return lux::fail(LUX_ERR_MISMATCH, "triangle count differs from the BVH's");
+    if (n > 0 && !tris) return lux::fail(LUX_ERR_INVALID_ARGUMENT, "null triangles");
+    Staging staging(ctx);
+    void* d_tris = nullptr;
+    staging.add(tris, sizeof(float) * 9 * static_cast<size_t>(n), true, false, &d_tris);
+    int st = staging.begin();
+    if (!st) st = lux::lbvh_attach_triangles(ctx, bvh, static_cast<const float*>(d_tris));
+    if (!st) st = finish_call(ctx, staging);
+    if (!st && !staging.items.empty()) st = sync_and_check(ctx);
+    if (!st) bvh->has_triangles = true;
     return st;
 }
 
@@ -435,8 +453,9 @@ int lux_bvh_download(lux_ctx* ctx, const lux_bvh* bvh, uint64_t* sorted_codes,
 static int check_query(lux_ctx* ctx, const lux_bvh* bvh, const float* rays, int32_t nrays) {
     if (int st = check_ctx(ctx)) return st;
     if (!bvh) return lux::fail(LUX_ERR_INVALID_ARGUMENT, "null bvh");
-    if (bvh->kind != LUX_PRIM_TRIANGLES)
-        return lux::fail(LUX_ERR_INVALID_ARGUMENT, "ray queries need a triangle BVH");
+    if (!bvh->has_triangles)
+        return lux::fail(LUX_ERR_INVALID_ARGUMENT,
+                         "ray queries need a triangle BVH (or lux_bvh_attach_triangles)");
     if (nrays < 0 || (nrays > 0 && !rays)) return lux::fail(LUX_ERR_INVALID_ARGUMENT, "bad ray array");
     return LUX_OK;
 }

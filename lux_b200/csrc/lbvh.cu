@@ -535,8 +535,7 @@ int lbvh_alloc(lux_ctx* ctx, lux_bvh* bvh) {
         size_t bytes;
     } reqs[] = {
         {reinterpret_cast<void**>(&bvh->nodes), sizeof(BvhNode) * std::max(n - 1, 1)},
-        {reinterpret_cast<void**>(&bvh->tris),
-         bvh->kind == LUX_PRIM_TRIANGLES ? sizeof(TriRecord) * n : 16},
+        {reinterpret_cast<void**>(&bvh->tris), sizeof(TriRecord) * n},
         {reinterpret_cast<void**>(&bvh->sorted_ids), sizeof(int) * n},
         {reinterpret_cast<void**>(&bvh->leaf_parent), sizeof(int) * n},
         {reinterpret_cast<void**>(&bvh->node_parent), sizeof(int) * std::max(n - 1, 1)},
@@ -582,6 +581,40 @@ int lbvh_build(lux_ctx* ctx, lux_bvh* bvh, const float* prims) {
     }
     return wide ? build_typed<LUX_PRIM_AABBS, unsigned long long>(ctx, bvh, prims)
                 : build_typed<LUX_PRIM_AABBS, unsigned>(ctx, bvh, prims);
+}
+
+namespace {
+
+// Triangle records in sorted order from triangles given in input order.
+__global__ void k_attach(const float* tris, int n, const int* sorted_ids, TriRecord* out,
+                         int* error) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    int pid = sorted_ids[k];
+    if (pid < 0 || pid >= n) {
+        atomicOr(error, kErrLoopBound);
+        return;
+    }
+    f3 v0, v1, v2;
+    box3 b;
+    load_prim<LUX_PRIM_TRIANGLES>(tris, pid, v0, v1, v2, b);
+    f3 e1 = v1 - v0;
+    f3 e2 = v2 - v0;
+    TriRecord r;
+    r.p0 = make_float4(v0.x, v0.y, v0.z, __int_as_float(pid));
+    r.p1 = make_float4(e1.x, e1.y, e1.z, 0.0f);
+    r.p2 = make_float4(e2.x, e2.y, e2.z, 0.0f);
+    out[k] = r;
+}
+
+}  // namespace
+
+int lbvh_attach_triangles(lux_ctx* ctx, lux_bvh* bvh, const float* tris) {
+    if (bvh->n <= 0) return LUX_OK;
+    k_attach<<<grid_for(bvh->n), kThreads, 0, ctx->stream>>>(tris, bvh->n, bvh->sorted_ids,
+                                                              bvh->tris, ctx->d_error);
+    ctx->launches += 1;
+    return cuda_fail(cudaGetLastError(), "k_attach");
 }
 
 int lbvh_refit(lux_ctx* ctx, lux_bvh* bvh, const float* prims) {

@@ -31,6 +31,7 @@ struct lux_ctx {
 struct lux_bvh {
     int n = 0;
     int capacity = 0;       // primitives the device storage can hold
+    bool has_triangles = false;  // TriRecord array valid (triangle BVHs, or attached)
     int kind = 0;           // LUX_PRIM_TRIANGLES / LUX_PRIM_AABBS
     int morton_bits = 30;
     int device = 0;
@@ -71,6 +72,7 @@ void lbvh_free(lux_bvh* bvh);
 int lbvh_export(lux_ctx* ctx, const lux_bvh* bvh, uint64_t* codes64, int* left, int* right,
                 float* bounds);
 size_t lbvh_scratch_bytes(int n, int morton_bits);
+int lbvh_attach_triangles(lux_ctx* ctx, lux_bvh* bvh, const float* tris);
 
 // Queries (traverse.cu).  All pointers are device pointers.
 int trace_closest(lux_ctx* ctx, const lux_bvh* bvh, const float* rays, int nrays, int* hit_id,

@@ -176,6 +176,26 @@ def test_overlap_self_and_cross_match_oracle(ctx, oracle):
     assert set(map(tuple, res.pairs.tolist())) <= set(map(tuple, want_pairs.tolist()))
 
 
+def test_box_bvh_with_attached_triangles(ctx, oracle):
+    """The reference builds from BvhBuildPrimitive boxes and passes triangles at query
+    time (bvh/gpu_bvh.cu:893-915): a box BVH + attached triangles answers exactly as the
+    triangle BVH does."""
+    tris = W.soup_triangles(40_000, seed=31)
+    rays = W.uniform_rays(20_000, seed=32)
+    boxes = oracle.triangle_bounds(tris)
+    box_bvh = ctx.build_lbvh(boxes, kind=lux_b200.PRIM_AABBS)
+    with pytest.raises(lux_b200.LuxError):
+        box_bvh.trace_closest(rays)
+    box_bvh.attach_triangles(tris)
+    got_id, got_t = box_bvh.trace_closest(rays)
+    want_id, want_t = ctx.build_lbvh(tris).trace_closest(rays)
+    assert np.array_equal(got_id, want_id) and np.array_equal(got_t, want_t)
+    assert (got_id >= 0).sum() > 100
+    with pytest.raises(lux_b200.LuxError) as e:
+        box_bvh.attach_triangles(tris[:-1])
+    assert e.value.status == lux_b200.LUX_ERR_MISMATCH
+
+
 def test_empty_and_single(ctx):
     empty = ctx.build_lbvh(np.zeros((0, 9), np.float32))
     rays = W.uniform_rays(10)
