@@ -286,6 +286,65 @@ int lux_render_samples(lux_ctx* ctx, const lux_scene* scene, const lux_render_re
  * [1] shadow-ray segments (each pass-through re-launch counts), host int64[2]. */
 int lux_render_ray_counts(lux_ctx* ctx, int64_t* counts);
 
+/* ------------------------------------------------------------------ batched / served rendering */
+
+/*
+ * A render server keeps scenes resident and renders many requests at once with one
+ * persistent path pool: whenever paths finish, their slots are refilled with camera
+ * paths of any admitted request (continuous batching at path granularity), so bounces
+ * of different depths, requests and scenes share every kernel launch.  Each pool
+ * iteration (new paths, extend, shade, shadow, retire) is one CUDA graph launch and
+ * never waits for the host.  Films accumulate in 64-bit fixed point (2^-32), which is
+ * order-independent: a request's film is bit-identical whether it renders alone or
+ * mixed with others.  It differs from lux_render's sample-order float sum by float
+ * rounding only.  Requests are admitted in submission order while the device-memory
+ * budget (pool + films) allows; a request that could never fit is rejected with
+ * LUX_ERR_BUDGET.  The server owns a private context and worker thread; scenes must
+ * stay alive until the server is destroyed.  All lux_server_* calls are thread-safe.
+ * (No reference counterpart: the reference renders one request at a time,
+ * integrator/wavefront_scheduler.cu:73-131.)
+ */
+typedef struct lux_server lux_server;
+
+typedef struct lux_server_options {
+    int64_t pool_paths;            /* paths in flight; 0: 4,194,304 */
+    int64_t memory_budget_bytes;   /* pool + request films; 0: 120 GiB */
+    int32_t max_requests;          /* requests admitted at once; 0: 256 */
+} lux_server_options;
+
+enum lux_request_state {
+    LUX_REQ_QUEUED = 0,
+    LUX_REQ_RUNNING = 1,
+    LUX_REQ_DONE = 2,
+    LUX_REQ_CANCELLED = 3,
+    LUX_REQ_FAILED = 4
+};
+
+int lux_server_create(int device, lux_scene* const* scenes, int32_t scene_count,
+                      const lux_server_options* options, lux_server** out);
+/* Queues a render of scenes[scene]; film_sum (host or device, width*height*3 floats) is
+ * written when the request completes and must stay valid until then. */
+int lux_server_submit(lux_server* server, int32_t scene, const lux_render_request* req,
+                      float* film_sum, int64_t* request_id);
+int lux_server_poll(lux_server* server, int64_t request_id, int32_t* state);
+/* Waits up to timeout_us (< 0: forever) for a final state (done, cancelled, failed). */
+int lux_server_wait(lux_server* server, int64_t request_id, int64_t timeout_us,
+                    int32_t* state);
+/* Waits until every submitted request reached a final state. */
+int lux_server_wait_all(lux_server* server, int64_t timeout_us);
+/* Queued requests are dropped; running ones stop contributing and finish early. */
+int lux_server_cancel(lux_server* server, int64_t request_id);
+/* New vertex positions for one mesh of one resident scene: applied between pool
+ * iterations as a refit (lux_scene_update_mesh), so later paths see the new frame. */
+int lux_server_update_mesh(lux_server* server, int32_t scene, int32_t mesh,
+                           const float* vertices);
+/* Host timestamps (steady clock, ns) of submission, admission and completion. */
+int lux_server_request_times(lux_server* server, int64_t request_id, int64_t* times);
+/* [0] pool iterations, [1] camera + extension rays, [2] shadow segments, [3] requests
+ * completed, [4] requests admitted, [5] refits applied, [6] bytes in use. */
+int lux_server_stats(lux_server* server, int64_t* stats);
+int lux_server_destroy(lux_server* server);
+
 #ifdef __cplusplus
 }
 #endif

@@ -73,6 +73,16 @@ SIGNATURES = {
     "lux_render": (ctypes.c_int, [_P, _P, _P, _P]),
     "lux_render_samples": (ctypes.c_int, [_P, _P, _P, _P]),
     "lux_render_ray_counts": (ctypes.c_int, [_P, _P]),
+    "lux_server_create": (ctypes.c_int, [ctypes.c_int, _P, _I32, _P, ctypes.POINTER(_P)]),
+    "lux_server_submit": (ctypes.c_int, [_P, _I32, _P, _P, ctypes.POINTER(_I64)]),
+    "lux_server_poll": (ctypes.c_int, [_P, _I64, ctypes.POINTER(_I32)]),
+    "lux_server_wait": (ctypes.c_int, [_P, _I64, _I64, ctypes.POINTER(_I32)]),
+    "lux_server_wait_all": (ctypes.c_int, [_P, _I64]),
+    "lux_server_cancel": (ctypes.c_int, [_P, _I64]),
+    "lux_server_update_mesh": (ctypes.c_int, [_P, _I32, _I32, _P]),
+    "lux_server_request_times": (ctypes.c_int, [_P, _I64, _P]),
+    "lux_server_stats": (ctypes.c_int, [_P, _P]),
+    "lux_server_destroy": (ctypes.c_int, [_P]),
     "lux_overlap_self": (ctypes.c_int, [_P, _P, _P, _I64, _P]),
     "lux_overlap_cross": (ctypes.c_int, [_P, _P, _P, _P, _I64, _P]),
 }

@@ -1,0 +1,859 @@
+// Render server: batched / continuous multi-request path tracing over resident scenes.
+//
+// One persistent path pool of P slots.  Each pool iteration (one CUDA graph launch):
+//   k_plan      pops min(free slots, unissued tickets) slots; resets this iteration's
+//               queue counters (single thread)
+//   k_generate  turns tickets into camera paths: ticket t -> (request, pixel, sample)
+//               through the admitted requests' ticket ranges (binary search)
+//   k_extend    closest hits of every queued path (mixed depths, requests and scenes);
+//               misses retire
+//   k_shade     per-material shading (the same per-path code as lux_render)
+//   k_shadow    NEE shadow rays
+//   k_retire    finished paths add their radiance to their request's film in 64-bit
+//               fixed point (order-independent), count towards completion, and return
+//               their slot to the free list
+// Tickets enumerate each request's paths pixel-major (pixel = idx / spp), so the random
+// numbers of a path depend only on (request seed, pixel, sample): a request renders the
+// same whether alone or mixed.  The host worker thread admits requests by memory budget,
+// uploads request slots and ticket ranges between launches (stream order), keeps two
+// iterations in flight, and delivers films when a request's retired-path count reaches
+// its path count.
+// No reference counterpart: the reference renders one request per call with a host
+// loop over batches and bounces (integrator/wavefront_scheduler.cu:73-131).
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <new>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "../../include/lux_gpu.h"
+#include "pt_kernels.cuh"
+#include "pt_scene.h"
+
+namespace lux {
+namespace pt {
+namespace {
+
+constexpr int kMaxRequests = 1024;
+constexpr float kFixedScale = 4294967296.0f;  // 2^32
+constexpr float kFixedMax = 1e9f;             // per-sample clamp keeps 64-bit sums exact
+
+struct ReqSlot {
+    int scene, width, height, spp, max_depth, light_sampler, cancelled, pad;
+    uint64_t seed;
+    int frame_index, sample_offset;
+    long long ticket_start, total;
+    unsigned long long* film;
+};
+
+struct TicketMap {
+    int count;
+    int pad;
+    long long start[kMaxRequests];
+    int slot[kMaxRequests];
+};
+
+struct ServerState {
+    int free_count;
+    int gen_count;
+    int gen_free_base;
+    int pad0;
+    long long gen_ticket;
+    long long next_ticket;
+    long long ticket_limit;
+    int count_ray[2];
+    int count_mat[kClasses];
+    int count_shadow;
+    int count_term;
+    int pad1;
+    unsigned long long rays[2];
+};
+
+struct ServerDev {
+    PathPool pool;
+    int* req_of;
+    int* qterm;
+    int* free_list;
+    ServerState* st;
+    const ReqSlot* req;
+    const TicketMap* tmap;
+    const SceneView* scenes;
+    unsigned long long* done;
+    int* error;
+};
+
+__global__ void k_plan(ServerState* st, int cur, int nxt) {
+    int free = st->free_count;
+    long long avail = st->ticket_limit - st->next_ticket;
+    if (avail < 0) avail = 0;
+    int n = static_cast<int>(min(static_cast<long long>(free), avail));
+    st->gen_count = n;
+    st->gen_free_base = free - n;
+    st->free_count = free - n;
+    st->gen_ticket = st->next_ticket;
+    st->next_ticket += n;
+    st->count_ray[nxt] = 0;
+    for (int k = 0; k < kClasses; ++k) st->count_mat[k] = 0;
+    st->count_shadow = 0;
+    st->count_term = 0;
+}
+
+__global__ void __launch_bounds__(kThreads) k_generate(ServerDev d, int cur) {
+    const int n = d.st->gen_count;
+    const int base = d.st->gen_free_base;
+    const long long t0 = d.st->gen_ticket;
+    const int stride = gridDim.x * blockDim.x;
+    const int rounds = (n + stride - 1) / stride;
+    for (int r = 0; r < rounds; ++r) {
+        int i = r * stride + blockIdx.x * blockDim.x + threadIdx.x;
+        bool active = i < n;
+        bool dead = false;
+        int slot = 0;
+        if (active) {
+            slot = d.free_list[base + i];
+            long long t = t0 + i;
+            int lo = 0, hi = d.tmap->count - 1;
+            while (lo < hi) {
+                int mid = (lo + hi + 1) >> 1;
+                if (d.tmap->start[mid] <= t) lo = mid;
+                else hi = mid - 1;
+            }
+            int rs = d.tmap->slot[lo];
+            const ReqSlot& q = d.req[rs];
+            long long idx = t - q.ticket_start;
+            d.req_of[slot] = rs;
+            if (q.cancelled || idx < 0 || idx >= q.total) {
+                if (!q.cancelled) atomicOr(d.error, kErrLoopBound);
+                dead = true;
+            } else {
+                init_path(d.pool, d.scenes[q.scene].camera, slot,
+                          static_cast<int>(idx / q.spp), static_cast<int>(idx % q.spp),
+                          CameraParams{q.width, q.height, q.seed, q.frame_index, q.sample_offset});
+            }
+        }
+        int qr = append(&d.st->count_ray[cur], 0, active && !dead);
+        if (qr >= 0) d.pool.qray[cur][qr] = slot;
+        int qt = append(&d.st->count_term, 0, active && dead);
+        if (qt >= 0) d.qterm[qt] = slot;
+    }
+}
+
+__global__ void __launch_bounds__(kThreads) k_extend_s(ServerDev d, int cur) {
+    const int n = d.st->count_ray[cur];
+    if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&d.st->rays[0], static_cast<unsigned long long>(n));
+    const int stride = gridDim.x * blockDim.x;
+    const int rounds = (n + stride - 1) / stride;
+    for (int r = 0; r < rounds; ++r) {
+        int i = r * stride + blockIdx.x * blockDim.x + threadIdx.x;
+        bool active = i < n;
+        int p = active ? d.pool.qray[cur][i] : 0;
+        int cls = -1;
+        if (active) {
+            const ReqSlot& q = d.req[d.req_of[p]];
+            cls = extend_path(d.pool, d.scenes[q.scene], q.light_sampler, p, d.error);
+        }
+        bool hit = cls >= 0;
+        int slot = append(d.st->count_mat, hit ? cls : 0, hit);
+        if (hit) d.pool.qmat[cls * d.pool.capacity + slot] = p;
+        int qt = append(&d.st->count_term, 0, active && !hit);
+        if (qt >= 0) d.qterm[qt] = p;
+    }
+}
+
+__global__ void __launch_bounds__(kThreads) k_shade_s(ServerDev d, int cur, int nxt) {
+    (void)cur;
+    int c[kClasses];
+    int total = 0;
+    for (int k = 0; k < kClasses; ++k) {
+        c[k] = d.st->count_mat[k];
+        total += c[k];
+    }
+    const int stride = gridDim.x * blockDim.x;
+    const int rounds = (total + stride - 1) / stride;
+    for (int r = 0; r < rounds; ++r) {
+        int i = r * stride + blockIdx.x * blockDim.x + threadIdx.x;
+        bool active = i < total;
+        int cls = 0, j = i;
+        while (cls < kClasses - 1 && j >= c[cls]) j -= c[cls++];
+        int p = active ? d.pool.qmat[cls * d.pool.capacity + j] : 0;
+        ShadeOut o;
+        if (active) {
+            const ReqSlot& q = d.req[d.req_of[p]];
+            o = shade_path(d.pool, d.scenes[q.scene], q.light_sampler, q.max_depth, p);
+        }
+        int s = append(&d.st->count_shadow, 0, o.shadow);
+        if (o.shadow) d.pool.qshadow[s] = p;
+        s = append(&d.st->count_ray[nxt], 0, o.spawn);
+        if (o.spawn) d.pool.qray[nxt][s] = p;
+        s = append(&d.st->count_term, 0, active && !o.spawn);
+        if (s >= 0) d.qterm[s] = p;
+    }
+}
+
+__global__ void __launch_bounds__(kThreads) k_shadow_s(ServerDev d) {
+    const int n = d.st->count_shadow;
+    unsigned long long segments = 0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        int p = d.pool.qshadow[i];
+        shadow_path(d.pool, d.scenes[d.req[d.req_of[p]].scene], p, d.error, segments);
+    }
+    warp_add(&d.st->rays[1], segments);
+}
+
+LUX_D unsigned long long to_fixed(float v) {
+    v = fminf(fmaxf(v, 0.0f), kFixedMax);  // NaN -> 0
+    return static_cast<unsigned long long>(__float2ll_rn(v * kFixedScale));
+}
+
+__global__ void __launch_bounds__(kThreads) k_retire(ServerDev d) {
+    const int n = d.st->count_term;
+    const int stride = gridDim.x * blockDim.x;
+    const int rounds = (n + stride - 1) / stride;
+    for (int r = 0; r < rounds; ++r) {
+        int i = r * stride + blockIdx.x * blockDim.x + threadIdx.x;
+        bool active = i < n;
+        int p = active ? d.qterm[i] : 0;
+        int rs = active ? d.req_of[p] : -1;
+        if (active) {
+            const ReqSlot& q = d.req[rs];
+            if (!q.cancelled) {
+                int pixel = d.pool.meta[p].x;
+                float4 rad = d.pool.rad[p];
+                unsigned long long* f = q.film + 3 * static_cast<size_t>(pixel);
+                atomicAdd(f, to_fixed(rad.x));
+                atomicAdd(f + 1, to_fixed(rad.y));
+                atomicAdd(f + 2, to_fixed(rad.z));
+            }
+        }
+        // completion counts: one atomic per (warp, request)
+        unsigned mask = __ballot_sync(0xffffffffu, active);
+        if (active) {
+            unsigned peers = __match_any_sync(mask, rs);
+            if (static_cast<int>(threadIdx.x & 31) == __ffs(peers) - 1)
+                atomicAdd(d.done + rs, static_cast<unsigned long long>(__popc(peers)));
+        }
+        int s = append(&d.st->free_count, 0, active);
+        if (s >= 0) d.free_list[s] = p;
+    }
+}
+
+__global__ void k_init_free(int* free_list, int n) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        free_list[i] = i;
+}
+
+__global__ void k_fixed_to_float(const unsigned long long* film, float* out, size_t n) {
+    for (size_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x)
+        out[i] = __ll2float_rn(static_cast<long long>(film[i])) * (1.0f / kFixedScale);
+}
+
+int64_t now_ns() {
+    return std::chrono::duration_cast<std::chrono::nanoseconds>(
+               std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+bool is_device_ptr(const void* p) {
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+}  // namespace
+}  // namespace pt
+}  // namespace lux
+
+struct lux_server_request {
+    int64_t id = 0;
+    int scene = 0;
+    lux_render_request req{};
+    float* out = nullptr;
+    bool out_device = false;
+    int state = LUX_REQ_QUEUED;
+    int slot = -1;
+    long long ticket_start = 0, total = 0;
+    unsigned long long* film = nullptr;
+    float* staging = nullptr;
+    size_t bytes = 0;
+    int64_t t_submit = 0, t_admit = 0, t_done = 0;
+    int64_t admit_iter = 0;   // first pool iteration launched after the admission
+    bool cancel_requested = false;
+    cudaEvent_t delivered = nullptr;
+};
+
+struct lux_server {
+    lux_ctx* ctx = nullptr;
+    std::vector<lux_scene*> scenes;
+    lux::pt::SceneView* d_scenes = nullptr;
+    lux::pt::PathPool pool;
+    int* req_of = nullptr;
+    int* qterm = nullptr;
+    int* free_list = nullptr;
+    lux::pt::ServerState* st = nullptr;
+    lux::pt::ReqSlot* d_req = nullptr;
+    lux::pt::ReqSlot* h_req = nullptr;         // pinned mirror
+    lux::pt::TicketMap* d_tmap = nullptr;
+    lux::pt::TicketMap* h_tmap = nullptr;      // pinned mirror
+    unsigned long long* d_done = nullptr;
+    unsigned long long* h_done[2] = {nullptr, nullptr};  // pinned, per in-flight iteration
+    lux::pt::ServerState* h_state[2] = {nullptr, nullptr};
+    long long* h_limit = nullptr;              // pinned ticket limit
+    cudaEvent_t iter_done[2] = {nullptr, nullptr};
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    int max_requests = 256;
+    int64_t budget = 0;
+    int64_t used = 0;
+    int64_t pool_bytes = 0;
+    long long ticket_limit = 0;
+    // host state
+    std::mutex mu;
+    std::condition_variable wake;
+    std::condition_variable finished;
+    std::deque<int64_t> pending;
+    std::map<int64_t, std::unique_ptr<lux_server_request>> requests;
+    std::vector<int> free_slots;
+    std::vector<int64_t> active;               // admitted, in ticket order
+    std::vector<int64_t> delivering;
+    struct MeshUpdate {
+        int scene, mesh;
+        std::vector<float> vertices;
+    };
+    std::deque<MeshUpdate> updates;
+    int64_t next_id = 1;
+    int64_t launched = 0;    // pool iterations launched
+    int64_t collected = 0;   // iterations whose counters were read back
+    bool stop = false;
+    int64_t iterations = 0, completed = 0, admitted = 0, refits = 0;
+    unsigned long long rays[2] = {0, 0};
+    int error_status = 0;
+    std::thread worker;
+};
+
+namespace {
+
+using lux::pt::ReqSlot;
+
+int server_fail(int st, const std::string& m) { return lux::fail(st, m); }
+
+int64_t request_cost(const lux_server_request& r) {
+    int64_t pixels = static_cast<int64_t>(r.req.width) * r.req.height;
+    return pixels * 3 * 8 + (r.out_device ? 0 : pixels * 3 * 4);
+}
+
+void upload_tmap(lux_server* s) {
+    s->h_tmap->count = 0;
+    for (int64_t id : s->active) {
+        auto& r = *s->requests[id];
+        int k = s->h_tmap->count++;
+        s->h_tmap->start[k] = r.ticket_start;
+        s->h_tmap->slot[k] = r.slot;
+    }
+    size_t bytes = offsetof(lux::pt::TicketMap, start) + sizeof(long long) * lux::pt::kMaxRequests
+                 + sizeof(int) * lux::pt::kMaxRequests;
+    cudaMemcpyAsync(s->d_tmap, s->h_tmap, bytes, cudaMemcpyHostToDevice, s->ctx->stream);
+}
+
+// Admits queued requests in order while slots and budget allow.  Called with mu held.
+void admit(lux_server* s) {
+    bool changed = false;
+    while (!s->pending.empty() && !s->free_slots.empty()) {
+        auto& r = *s->requests[s->pending.front()];
+        int64_t cost = request_cost(r);
+        if (s->used + cost > s->budget) break;
+        cudaStream_t stream = s->ctx->stream;
+        size_t n = static_cast<size_t>(r.req.width) * r.req.height * 3;
+        if (cudaMallocAsync(reinterpret_cast<void**>(&r.film), n * 8, stream) != cudaSuccess) {
+            cudaGetLastError();
+            break;
+        }
+        if (!r.out_device &&
+            cudaMallocAsync(reinterpret_cast<void**>(&r.staging), n * 4, stream) != cudaSuccess) {
+            cudaGetLastError();
+            cudaFreeAsync(r.film, stream);
+            r.film = nullptr;
+            break;
+        }
+        cudaMemsetAsync(r.film, 0, n * 8, stream);
+        r.slot = s->free_slots.back();
+        s->free_slots.pop_back();
+        r.bytes = cost;
+        s->used += cost;
+        r.total = static_cast<long long>(r.req.width) * r.req.height * r.req.spp;
+        r.ticket_start = s->ticket_limit;
+        s->ticket_limit += r.total;
+        ReqSlot q{};
+        q.scene = r.scene;
+        q.width = r.req.width;
+        q.height = r.req.height;
+        q.spp = r.req.spp;
+        q.max_depth = r.req.max_depth;
+        q.light_sampler = r.req.light_sampler;
+        q.cancelled = 0;
+        q.seed = r.req.seed;
+        q.frame_index = r.req.frame_index;
+        q.sample_offset = r.req.sample_offset;
+        q.ticket_start = r.ticket_start;
+        q.total = r.total;
+        q.film = r.film;
+        s->h_req[r.slot] = q;
+        cudaMemcpyAsync(s->d_req + r.slot, s->h_req + r.slot, sizeof(ReqSlot),
+                        cudaMemcpyHostToDevice, stream);
+        cudaMemsetAsync(s->d_done + r.slot, 0, sizeof(unsigned long long), stream);
+        r.state = LUX_REQ_RUNNING;
+        r.t_admit = lux::pt::now_ns();
+        r.admit_iter = s->launched;
+        s->active.push_back(r.id);
+        s->pending.pop_front();
+        ++s->admitted;
+        changed = true;
+    }
+    if (changed) {
+        upload_tmap(s);
+        *s->h_limit = s->ticket_limit;
+        cudaMemcpyAsync(&s->st->ticket_limit, s->h_limit, sizeof(long long),
+                        cudaMemcpyHostToDevice, s->ctx->stream);
+    }
+}
+
+// Finishes requests whose retired-path count reached their path count.  done: the
+// counters read back after pool iteration `iter` (-1: none); a request admitted after
+// that iteration was launched is not judged by them (its slot may still show the
+// previous occupant's count).  mu held.
+void collect(lux_server* s, const unsigned long long* done, int64_t iter) {
+    bool changed = false;
+    cudaStream_t stream = s->ctx->stream;
+    for (size_t k = 0; k < s->active.size();) {
+        auto& r = *s->requests[s->active[k]];
+        if (!done || iter < r.admit_iter || static_cast<long long>(done[r.slot]) < r.total) {
+            ++k;
+            continue;
+        }
+        size_t n = static_cast<size_t>(r.req.width) * r.req.height * 3;
+        if (!r.cancel_requested) {
+            float* dst = r.out_device ? r.out : r.staging;
+            int grid = std::max(1, std::min(s->ctx->sm_count * 4, static_cast<int>((n + 255) / 256)));
+            lux::pt::k_fixed_to_float<<<grid, 256, 0, stream>>>(r.film, dst, n);
+            if (!r.out_device)
+                cudaMemcpyAsync(r.out, r.staging, n * 4, cudaMemcpyDeviceToHost, stream);
+        }
+        cudaFreeAsync(r.film, stream);
+        if (r.staging) cudaFreeAsync(r.staging, stream);
+        r.film = nullptr;
+        r.staging = nullptr;
+        cudaEventCreateWithFlags(&r.delivered, cudaEventDisableTiming);
+        cudaEventRecord(r.delivered, stream);
+        s->free_slots.push_back(r.slot);
+        s->used -= r.bytes;
+        s->delivering.push_back(r.id);
+        s->active.erase(s->active.begin() + k);
+        changed = true;
+    }
+    if (changed) upload_tmap(s);
+    for (size_t k = 0; k < s->delivering.size();) {
+        auto& r = *s->requests[s->delivering[k]];
+        if (cudaEventQuery(r.delivered) != cudaSuccess) {
+            cudaGetLastError();
+            ++k;
+            continue;
+        }
+        cudaEventDestroy(r.delivered);
+        r.delivered = nullptr;
+        r.state = r.cancel_requested ? LUX_REQ_CANCELLED : LUX_REQ_DONE;
+        r.t_done = lux::pt::now_ns();
+        ++s->completed;
+        s->delivering.erase(s->delivering.begin() + k);
+        s->finished.notify_all();
+    }
+}
+
+void fail_all(lux_server* s, int status) {
+    s->error_status = status;
+    for (auto& kv : s->requests) {
+        auto& r = *kv.second;
+        if (r.state == LUX_REQ_QUEUED || r.state == LUX_REQ_RUNNING) r.state = LUX_REQ_FAILED;
+    }
+    s->pending.clear();
+    s->active.clear();
+    s->finished.notify_all();
+}
+
+void worker_main(lux_server* s) {
+    cudaSetDevice(s->ctx->device);
+    std::unique_lock<std::mutex> lk(s->mu);
+    for (;;) {
+        if (s->stop) break;
+        if (s->error_status == 0) admit(s);
+        while (!s->updates.empty()) {
+            auto u = std::move(s->updates.front());
+            s->updates.pop_front();
+            lk.unlock();
+            int st = lux::scene_update_mesh(s->ctx, s->scenes[u.scene], u.mesh, u.vertices.data());
+            lk.lock();
+            if (st == LUX_OK) ++s->refits;
+        }
+        bool busy = !s->active.empty() || !s->delivering.empty();
+        if (!busy && s->launched == s->collected) {
+            s->wake.wait(lk, [&] {
+                return s->stop || (!s->pending.empty() && !s->free_slots.empty()) ||
+                       !s->updates.empty();
+            });
+            continue;
+        }
+        // Keep up to two iterations in flight: launch one, then read the older one's
+        // counters while the newer runs.
+        bool launch = !s->active.empty() && s->launched - s->collected < 2;
+        int64_t launch_index = s->launched;
+        if (launch) ++s->launched;
+        lk.unlock();
+        if (launch) {
+            int parity = static_cast<int>(launch_index & 1);
+            cudaGraphLaunch(s->graph[parity], s->ctx->stream);
+            cudaMemcpyAsync(s->h_done[parity], s->d_done,
+                            sizeof(unsigned long long) * s->max_requests, cudaMemcpyDeviceToHost,
+                            s->ctx->stream);
+            cudaMemcpyAsync(s->h_state[parity], s->st, sizeof(lux::pt::ServerState),
+                            cudaMemcpyDeviceToHost, s->ctx->stream);
+            cudaEventRecord(s->iter_done[parity], s->ctx->stream);
+        }
+        int err_word = 0;
+        int64_t read_iter = -1;
+        if (s->collected < s->launched) {
+            read_iter = s->collected;
+            cudaError_t e = cudaEventSynchronize(s->iter_done[static_cast<int>(read_iter & 1)]);
+            if (e != cudaSuccess) {
+                lk.lock();
+                fail_all(s, LUX_ERR_CUDA);
+                continue;
+            }
+            cudaMemcpy(&err_word, s->ctx->d_error, sizeof(int), cudaMemcpyDeviceToHost);
+        } else {
+            cudaStreamSynchronize(s->ctx->stream);
+        }
+        lk.lock();
+        if (read_iter >= 0) {
+            int parity = static_cast<int>(read_iter & 1);
+            s->collected = read_iter + 1;
+            ++s->iterations;
+            s->rays[0] = s->h_state[parity]->rays[0];
+            s->rays[1] = s->h_state[parity]->rays[1];
+            if (err_word) {
+                cudaMemset(s->ctx->d_error, 0, sizeof(int));
+                fail_all(s, LUX_ERR_DEVICE_CHECK);
+                continue;
+            }
+            collect(s, s->h_done[parity], read_iter);
+        } else {
+            collect(s, nullptr, -1);
+        }
+    }
+}
+
+int build_graphs(lux_server* s) {
+    using namespace lux::pt;
+    ServerDev d;
+    d.pool = s->pool;
+    d.req_of = s->req_of;
+    d.qterm = s->qterm;
+    d.free_list = s->free_list;
+    d.st = s->st;
+    d.req = s->d_req;
+    d.tmap = s->d_tmap;
+    d.scenes = s->d_scenes;
+    d.done = s->d_done;
+    d.error = s->ctx->d_error;
+    int grid = s->ctx->sm_count * 8;
+    cudaStream_t stream = s->ctx->stream;
+    for (int cur = 0; cur < 2; ++cur) {
+        int nxt = cur ^ 1;
+        cudaGraph_t g;
+        cudaError_t err = cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal);
+        if (err != cudaSuccess) return lux::cuda_fail(err, "graph capture");
+        k_plan<<<1, 1, 0, stream>>>(s->st, cur, nxt);
+        k_generate<<<grid, kThreads, 0, stream>>>(d, cur);
+        k_extend_s<<<grid, kThreads, 0, stream>>>(d, cur);
+        k_shade_s<<<grid, kThreads, 0, stream>>>(d, cur, nxt);
+        k_shadow_s<<<grid, kThreads, 0, stream>>>(d);
+        k_retire<<<grid, kThreads, 0, stream>>>(d);
+        err = cudaStreamEndCapture(stream, &g);
+        if (err != cudaSuccess) return lux::cuda_fail(err, "graph capture end");
+        err = cudaGraphInstantiate(&s->graph[cur], g, 0);
+        cudaGraphDestroy(g);
+        if (err != cudaSuccess) return lux::cuda_fail(err, "graph instantiate");
+    }
+    return LUX_OK;
+}
+
+void server_release(lux_server* s) {
+    for (int k = 0; k < 2; ++k) {
+        if (s->graph[k]) cudaGraphExecDestroy(s->graph[k]);
+        if (s->iter_done[k]) cudaEventDestroy(s->iter_done[k]);
+        if (s->h_done[k]) cudaFreeHost(s->h_done[k]);
+        if (s->h_state[k]) cudaFreeHost(s->h_state[k]);
+    }
+    lux::pt::path_pool_free(s->pool);
+    void* dev[] = {s->d_scenes, s->req_of, s->qterm, s->free_list, s->st, s->d_req, s->d_tmap,
+                   s->d_done};
+    for (void* p : dev)
+        if (p) cudaFree(p);
+    if (s->h_req) cudaFreeHost(s->h_req);
+    if (s->h_tmap) cudaFreeHost(s->h_tmap);
+    if (s->h_limit) cudaFreeHost(s->h_limit);
+    for (auto& kv : s->requests) {
+        if (kv.second->film) cudaFree(kv.second->film);
+        if (kv.second->staging) cudaFree(kv.second->staging);
+        if (kv.second->delivered) cudaEventDestroy(kv.second->delivered);
+    }
+    if (s->ctx) lux_ctx_destroy(s->ctx);
+}
+
+}  // namespace
+
+extern "C" {
+
+int lux_server_create(int device, lux_scene* const* scenes, int32_t scene_count,
+                      const lux_server_options* options, lux_server** out) {
+    using namespace lux::pt;
+    if (!out || (scene_count > 0 && !scenes) || scene_count <= 0)
+        return server_fail(LUX_ERR_INVALID_ARGUMENT, "server needs at least one scene");
+    *out = nullptr;
+    lux_server_options opt{};
+    if (options) opt = *options;
+    int64_t pool_paths = opt.pool_paths > 0 ? opt.pool_paths : (1 << 22);
+    if (pool_paths > (1 << 28)) return server_fail(LUX_ERR_INVALID_ARGUMENT, "pool too large");
+    int max_requests = opt.max_requests > 0 ? opt.max_requests : 256;
+    if (max_requests > kMaxRequests)
+        return server_fail(LUX_ERR_INVALID_ARGUMENT, "max_requests above 1024");
+    for (int i = 0; i < scene_count; ++i)
+        if (!scenes[i]) return server_fail(LUX_ERR_INVALID_ARGUMENT, "null scene");
+    auto* s = new (std::nothrow) lux_server();
+    if (!s) return server_fail(LUX_ERR_OUT_OF_MEMORY, "server allocation failed");
+    int st = lux_ctx_create(&s->ctx, device, nullptr);
+    if (st) {
+        delete s;
+        return st;
+    }
+    s->scenes.assign(scenes, scenes + scene_count);
+    s->max_requests = max_requests;
+    s->budget = opt.memory_budget_bytes > 0 ? opt.memory_budget_bytes : (int64_t(120) << 30);
+    int cap = static_cast<int>(pool_paths);
+    st = path_pool_alloc(s->pool, cap);
+    std::vector<SceneView> views;
+    for (lux_scene* sc : s->scenes) views.push_back(sc->view);
+    auto dmalloc = [&](void** p, size_t bytes) {
+        if (st) return;
+        if (cudaMalloc(p, bytes) != cudaSuccess) {
+            cudaGetLastError();
+            st = server_fail(LUX_ERR_OUT_OF_MEMORY, "server allocation failed");
+        }
+    };
+    dmalloc(reinterpret_cast<void**>(&s->d_scenes), sizeof(SceneView) * views.size());
+    dmalloc(reinterpret_cast<void**>(&s->req_of), sizeof(int) * cap);
+    dmalloc(reinterpret_cast<void**>(&s->qterm), sizeof(int) * cap);
+    dmalloc(reinterpret_cast<void**>(&s->free_list), sizeof(int) * cap);
+    dmalloc(reinterpret_cast<void**>(&s->st), sizeof(ServerState));
+    dmalloc(reinterpret_cast<void**>(&s->d_req), sizeof(ReqSlot) * max_requests);
+    dmalloc(reinterpret_cast<void**>(&s->d_tmap), sizeof(TicketMap));
+    dmalloc(reinterpret_cast<void**>(&s->d_done), sizeof(unsigned long long) * max_requests);
+    auto hmalloc = [&](void** p, size_t bytes) {
+        if (st) return;
+        if (cudaMallocHost(p, bytes) != cudaSuccess) {
+            cudaGetLastError();
+            st = server_fail(LUX_ERR_OUT_OF_MEMORY, "pinned allocation failed");
+        }
+    };
+    hmalloc(reinterpret_cast<void**>(&s->h_req), sizeof(ReqSlot) * max_requests);
+    hmalloc(reinterpret_cast<void**>(&s->h_tmap), sizeof(TicketMap));
+    hmalloc(reinterpret_cast<void**>(&s->h_limit), sizeof(long long));
+    for (int k = 0; k < 2; ++k) {
+        hmalloc(reinterpret_cast<void**>(&s->h_done[k]), sizeof(unsigned long long) * max_requests);
+        hmalloc(reinterpret_cast<void**>(&s->h_state[k]), sizeof(ServerState));
+        if (!st) cudaEventCreateWithFlags(&s->iter_done[k], cudaEventDisableTiming);
+    }
+    if (!st) {
+        cudaStream_t stream = s->ctx->stream;
+        cudaMemcpyAsync(s->d_scenes, views.data(), sizeof(SceneView) * views.size(),
+                        cudaMemcpyHostToDevice, stream);
+        ServerState init{};
+        init.free_count = cap;
+        cudaMemcpyAsync(s->st, &init, sizeof(init), cudaMemcpyHostToDevice, stream);
+        k_init_free<<<s->ctx->sm_count * 4, 256, 0, stream>>>(s->free_list, cap);
+        cudaMemsetAsync(s->d_done, 0, sizeof(unsigned long long) * max_requests, stream);
+        std::memset(s->h_tmap, 0, sizeof(TicketMap));
+        std::memset(s->h_done[0], 0, sizeof(unsigned long long) * max_requests);
+        std::memset(s->h_done[1], 0, sizeof(unsigned long long) * max_requests);
+        cudaMemcpyAsync(s->d_tmap, s->h_tmap, sizeof(TicketMap), cudaMemcpyHostToDevice, stream);
+        st = lux::cuda_fail(cudaStreamSynchronize(stream), "server init");
+    }
+    if (!st) st = build_graphs(s);
+    if (st) {
+        server_release(s);
+        delete s;
+        return st;
+    }
+    s->pool_bytes = static_cast<int64_t>(cap) * (16 * 12 + 4 * 7 + 4 * kClasses);
+    s->used = s->pool_bytes;
+    for (int k = max_requests - 1; k >= 0; --k) s->free_slots.push_back(k);
+    s->worker = std::thread(worker_main, s);
+    *out = s;
+    return LUX_OK;
+}
+
+int lux_server_submit(lux_server* s, int32_t scene, const lux_render_request* req,
+                      float* film_sum, int64_t* request_id) {
+    if (!s || !req || !film_sum || !request_id)
+        return server_fail(LUX_ERR_INVALID_ARGUMENT, "null argument");
+    if (scene < 0 || scene >= static_cast<int>(s->scenes.size()))
+        return server_fail(LUX_ERR_INVALID_ARGUMENT, "scene index out of range");
+    if (req->width <= 0 || req->height <= 0 || req->spp <= 0)
+        return server_fail(LUX_ERR_INVALID_ARGUMENT, "render requires a non-empty film");
+    if (req->max_depth < 0 || req->max_depth > 1000)
+        return server_fail(LUX_ERR_INVALID_ARGUMENT, "max_depth must be in 0..1000");
+    if (req->light_sampler != 0 && req->light_sampler != 1)
+        return server_fail(LUX_ERR_INVALID_ARGUMENT, "light sampler: 0 uniform or 1 power");
+    if (static_cast<long long>(req->width) * req->height > (1ll << 30))
+        return server_fail(LUX_ERR_INVALID_ARGUMENT, "image too large");
+    auto r = std::make_unique<lux_server_request>();
+    r->scene = scene;
+    r->req = *req;
+    r->out = film_sum;
+    r->out_device = lux::pt::is_device_ptr(film_sum);
+    r->t_submit = lux::pt::now_ns();
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (s->error_status) return server_fail(s->error_status, "server failed earlier");
+    if (s->pool_bytes + request_cost(*r) > s->budget)
+        return server_fail(LUX_ERR_BUDGET, "request film does not fit the memory budget");
+    r->id = s->next_id++;
+    *request_id = r->id;
+    s->pending.push_back(r->id);
+    s->requests[r->id] = std::move(r);
+    s->wake.notify_all();
+    return LUX_OK;
+}
+
+int lux_server_poll(lux_server* s, int64_t id, int32_t* state) {
+    if (!s || !state) return server_fail(LUX_ERR_INVALID_ARGUMENT, "null argument");
+    std::lock_guard<std::mutex> lk(s->mu);
+    auto it = s->requests.find(id);
+    if (it == s->requests.end()) return server_fail(LUX_ERR_INVALID_ARGUMENT, "unknown request");
+    *state = it->second->state;
+    return LUX_OK;
+}
+
+static bool final_state(int st) {
+    return st == LUX_REQ_DONE || st == LUX_REQ_CANCELLED || st == LUX_REQ_FAILED;
+}
+
+int lux_server_wait(lux_server* s, int64_t id, int64_t timeout_us, int32_t* state) {
+    if (!s) return server_fail(LUX_ERR_INVALID_ARGUMENT, "null server");
+    std::unique_lock<std::mutex> lk(s->mu);
+    auto it = s->requests.find(id);
+    if (it == s->requests.end()) return server_fail(LUX_ERR_INVALID_ARGUMENT, "unknown request");
+    lux_server_request* r = it->second.get();
+    auto pred = [&] { return final_state(r->state); };
+    if (timeout_us < 0) s->finished.wait(lk, pred);
+    else s->finished.wait_for(lk, std::chrono::microseconds(timeout_us), pred);
+    if (state) *state = r->state;
+    return LUX_OK;
+}
+
+int lux_server_wait_all(lux_server* s, int64_t timeout_us) {
+    if (!s) return server_fail(LUX_ERR_INVALID_ARGUMENT, "null server");
+    std::unique_lock<std::mutex> lk(s->mu);
+    auto pred = [&] {
+        for (auto& kv : s->requests)
+            if (!final_state(kv.second->state)) return false;
+        return true;
+    };
+    bool ok = timeout_us < 0 ? (s->finished.wait(lk, pred), true)
+                             : s->finished.wait_for(lk, std::chrono::microseconds(timeout_us), pred);
+    if (s->error_status) return server_fail(s->error_status, "server failed");
+    return ok ? LUX_OK : server_fail(LUX_ERR_INVALID_ARGUMENT, "timed out");
+}
+
+int lux_server_cancel(lux_server* s, int64_t id) {
+    if (!s) return server_fail(LUX_ERR_INVALID_ARGUMENT, "null server");
+    std::lock_guard<std::mutex> lk(s->mu);
+    auto it = s->requests.find(id);
+    if (it == s->requests.end()) return server_fail(LUX_ERR_INVALID_ARGUMENT, "unknown request");
+    lux_server_request& r = *it->second;
+    if (r.state == LUX_REQ_QUEUED) {
+        s->pending.erase(std::remove(s->pending.begin(), s->pending.end(), id), s->pending.end());
+        r.state = LUX_REQ_CANCELLED;
+        r.cancel_requested = true;
+        s->finished.notify_all();
+    } else if (r.state == LUX_REQ_RUNNING && !r.cancel_requested) {
+        r.cancel_requested = true;
+        s->h_req[r.slot].cancelled = 1;
+        cudaMemcpyAsync(&s->d_req[r.slot].cancelled, &s->h_req[r.slot].cancelled, sizeof(int),
+                        cudaMemcpyHostToDevice, s->ctx->stream);
+    }
+    return LUX_OK;
+}
+
+int lux_server_update_mesh(lux_server* s, int32_t scene, int32_t mesh, const float* vertices) {
+    if (!s || !vertices) return server_fail(LUX_ERR_INVALID_ARGUMENT, "null argument");
+    if (scene < 0 || scene >= static_cast<int>(s->scenes.size()))
+        return server_fail(LUX_ERR_INVALID_ARGUMENT, "scene index out of range");
+    lux_scene* sc = s->scenes[scene];
+    if (mesh < 0 || mesh >= static_cast<int>(sc->mesh_vertices.size()))
+        return server_fail(LUX_ERR_INVALID_ARGUMENT, "mesh out of range");
+    lux_server::MeshUpdate u{scene, mesh,
+                             std::vector<float>(vertices, vertices + sc->mesh_vertices[mesh].size())};
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->updates.push_back(std::move(u));
+    s->wake.notify_all();
+    return LUX_OK;
+}
+
+int lux_server_request_times(lux_server* s, int64_t id, int64_t* times) {
+    if (!s || !times) return server_fail(LUX_ERR_INVALID_ARGUMENT, "null argument");
+    std::lock_guard<std::mutex> lk(s->mu);
+    auto it = s->requests.find(id);
+    if (it == s->requests.end()) return server_fail(LUX_ERR_INVALID_ARGUMENT, "unknown request");
+    times[0] = it->second->t_submit;
+    times[1] = it->second->t_admit;
+    times[2] = it->second->t_done;
+    return LUX_OK;
+}
+
+int lux_server_stats(lux_server* s, int64_t* stats) {
+    if (!s || !stats) return server_fail(LUX_ERR_INVALID_ARGUMENT, "null argument");
+    std::lock_guard<std::mutex> lk(s->mu);
+    stats[0] = s->iterations;
+    stats[1] = static_cast<int64_t>(s->rays[0]);
+    stats[2] = static_cast<int64_t>(s->rays[1]);
+    stats[3] = s->completed;
+    stats[4] = s->admitted;
+    stats[5] = s->refits;
+    stats[6] = s->used;
+    return LUX_OK;
+}
+
+int lux_server_destroy(lux_server* s) {
+    if (!s) return LUX_OK;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->stop = true;
+        s->wake.notify_all();
+    }
+    if (s->worker.joinable()) s->worker.join();
+    cudaSetDevice(s->ctx->device);
+    cudaStreamSynchronize(s->ctx->stream);
+    server_release(s);
+    delete s;
+    return LUX_OK;
+}
+
+}  // extern "C"

@@ -1,4 +1,4 @@
-// Wavefront path tracer for sm_100a.
+// Single-request wavefront path tracer for sm_100a.
 //
 // A render is a sequence of batches; a batch holds (pixel range) x (sample range) paths,
 // pixel-major, so a pixel's samples are adjacent.  Per bounce d:
@@ -13,761 +13,108 @@
 // the reference CPU tracer's float accumulation order (cpu_path_tracer.cpp:543-558).
 //
 // Reference counterparts (src/): integrator/wavefront_kernels.cu:234-715,
-// integrator/wavefront_scheduler.cu:73-131, integrator/cpu_path_tracer.cpp:27-158,403-498.
-// Queue sizes live on the device; kernels use grid-stride loops over them, so no bounce
-// waits for the host.
+// integrator/wavefront_scheduler.cu:73-131.  Queue sizes live on the device; kernels
+// use grid-stride loops over them, so no bounce waits for the host.
 
 #include <cuda_runtime.h>
 
 #include <algorithm>
 #include <cstring>
+#include <new>
 
 #include "../../include/lux_gpu.h"
+#include "pt_kernels.cuh"
 #include "pt_scene.h"
 
 namespace lux {
 namespace pt {
 namespace {
 
-constexpr int kThreads = 256;
-constexpr int kStack = 72;
-constexpr int kClasses = 5;       // Lambert, thin Lambert, GGX, dielectric, pass-through
-constexpr int kSlots = 8;         // per-bounce counters: ray, 5 material queues, shadow
-constexpr int kShadowSegments = 1024;
+constexpr int kSlots = 8;  // per-bounce counters: ray, 5 material queues, shadow
 
 struct Runtime {
-    int capacity = 0;
+    PathPool pool;
     int max_depth = -1;
-    float4* thr_eta = nullptr;      // throughput.rgb, eta scale
-    float4* rad = nullptr;          // radiance.rgb
-    float4* prev = nullptr;         // previous sample reference position, pdf
-    int4* meta = nullptr;           // pixel, sample, depth | passthrough << 16, measure | flags << 8
-    uint4* rng = nullptr;           // PCG state lo/hi, inc lo/hi
-    float4* ray_o = nullptr;        // origin, t_min
-    float4* ray_d = nullptr;        // direction, t_max
-    float4* hit = nullptr;          // t, u, v, primitive (int bits)
-    float4* sh_o = nullptr;         // origin, t_max
-    float4* sh_d = nullptr;         // direction, ignored primitive (int bits)
-    float4* sh_c = nullptr;         // contribution.rgb, mis weight
-    float4* sh_t = nullptr;         // throughput.rgb at the vertex
-    int* qray[2] = {nullptr, nullptr};
-    int* qmat = nullptr;            // kClasses * capacity
-    int* qshadow = nullptr;
-    int* counts = nullptr;          // (max_depth + 2) * kSlots
+    int* counts = nullptr;               // (max_depth + 2) * kSlots
     unsigned long long* rays = nullptr;  // [0] camera + extension, [1] shadow segments
     long long last_counts[2] = {0, 0};
 };
 
-LUX_D unsigned lanemask_lt() {
-    unsigned m;
-    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
-    return m;
-}
-
-// Warp-aggregated append: lanes with the same queue share one atomic.
-LUX_D int append(int* counter_base, int queue, bool active) {
-    unsigned mask = __ballot_sync(0xffffffffu, active);
-    if (!active) return -1;
-    unsigned peers = __match_any_sync(mask, queue);
-    int leader = __ffs(peers) - 1;
-    int base = 0;
-    if (static_cast<int>(threadIdx.x & 31) == leader) base = atomicAdd(counter_base + queue, __popc(peers));
-    base = __shfl_sync(peers, base, leader);
-    return base + __popc(peers & lanemask_lt());
-}
-
-LUX_D f3 xyz(const float4& v) { return make_f3(v.x, v.y, v.z); }
-
-// ------------------------------------------------------------------ traversal
-
-struct SceneHit {
-    int prim = -1;
-    float t = 0, u = 0, v = 0;
-};
-
-// transform_point / transform_vector with the implicit row (0 0 0 1)
-// (core/mat4.cuh:173-199).
-LUX_D f3 xform_point(const float* m, f3 p) {
-    float x = add(add(add(mul(m[0], p.x), mul(m[1], p.y)), mul(m[2], p.z)), m[3]);
-    float y = add(add(add(mul(m[4], p.x), mul(m[5], p.y)), mul(m[6], p.z)), m[7]);
-    float z = add(add(add(mul(m[8], p.x), mul(m[9], p.y)), mul(m[10], p.z)), m[11]);
-    float w = add(add(add(mul(0.0f, p.x), mul(0.0f, p.y)), mul(0.0f, p.z)), 1.0f);
-    return w == 1.0f ? make_f3(x, y, z) : make_f3(x / w, y / w, z / w);
-}
-LUX_D f3 xform_vector(const float* m, f3 v) {
-    return make_f3(add(add(mul(m[0], v.x), mul(m[1], v.y)), mul(m[2], v.z)),
-                   add(add(mul(m[4], v.x), mul(m[5], v.y)), mul(m[6], v.z)),
-                   add(add(mul(m[8], v.x), mul(m[9], v.y)), mul(m[10], v.z)));
-}
-
-// Closest hit inside one BLAS in object space, reference order (bvh/bvh_device.cuh:92-134
-// with GpuMeshPrimitiveIntersector, scene/gpu_scene_bvh.cuh:15-42).  best_t enters as the
-// current bound; returns the local triangle id or -1.
-LUX_D int blas_closest(const BvhView& b, f3 o, f3 d, float tmin, float& best_t, float& bu,
-                       float& bv, int ignored_local, int* error) {
-    if (b.n <= 0) return -1;
-    ray3 r{o, tmin, d, best_t};
-    slab_ray sr = make_slab_ray(r);
-    float tn;
-    if (!slab_hit(sr, load_root(b.root), best_t, tn)) return -1;
-    int stack_h[kStack];
-    float stack_t[kStack];
-    int sp = 0;
-    int cur = b.n == 1 ? ~0 : 0;
-    int best = -1;
-    const long long bound = 2ll * b.n + 64;
-    for (long long step = 0;; ++step) {
-        if (step > bound || cur >= b.n - 1 || ~cur >= b.n) {
-            atomicOr(error, kErrLoopBound);
-            return -1;
-        }
-        bool pop = true;
-        if (cur >= 0) {
-            BvhNode nd = load_node(b.nodes, cur);
-            float tl, tr;
-            bool hl = slab_hit(sr, node_left_box(nd), best_t, tl);
-            bool hr = slab_hit(sr, node_right_box(nd), best_t, tr);
-            if (hl) {
-                if (hr) {
-                    if (sp >= kStack) {
-                        atomicOr(error, kErrStackOverflow);
-                        return -1;
-                    }
-                    stack_h[sp] = nd.ch.y;
-                    stack_t[sp] = tr;
-                    ++sp;
-                }
-                cur = nd.ch.x;
-                pop = false;
-            } else if (hr) {
-                cur = nd.ch.y;
-                pop = false;
-            }
-        } else {
-            const float4* tp = reinterpret_cast<const float4*>(b.tris + ~cur);
-            float4 p0 = __ldg(tp);
-            int local = __float_as_int(p0.w);
-            if (local != ignored_local) {
-                float4 p1 = __ldg(tp + 1);
-                float4 p2 = __ldg(tp + 2);
-                float t, u, v;
-                if (moller_trumbore(o, d, xyz(p0), xyz(p1), xyz(p2), t, u, v) && t > tmin
-                    && t < best_t) {
-                    best = local;
-                    best_t = t;
-                    bu = u;
-                    bv = v;
-                }
-            }
-        }
-        if (pop) {
-            bool resumed = false;
-            while (sp > 0) {
-                --sp;
-                if (!(stack_t[sp] > best_t)) {
-                    cur = stack_h[sp];
-                    resumed = true;
-                    break;
-                }
-            }
-            if (!resumed) break;
-        }
-    }
-    return best;
-}
-
-// Two-level closest hit (intersect_scene_bvh_device, scene/gpu_scene_bvh.cuh:44-135):
-// TLAS over instance boxes in reference order; at each instance leaf the ray is taken
-// to object space and its BLAS searched with t_max = the current best.  ignored: scene
-// triangle id skipped (shadow rays leaving a surface), -1 none.
-LUX_D SceneHit scene_closest(const SceneView& sc, f3 o, f3 d, float tmin, float tmax,
-                             int ignored, int* error) {
-    SceneHit h;
-    h.t = tmax;
-    if (!sc.has_two_level) return h;
-    const BvhView& tl = sc.tlas;
-    ray3 r{o, tmin, d, tmax};
-    slab_ray sr = make_slab_ray(r);
-    float tn;
-    if (!slab_hit(sr, load_root(tl.root), h.t, tn)) return h;
-    int ign_instance = -1, ign_local = -1;
-    if (ignored >= 0) {
-        float4 v1 = __ldg(&sc.tris[ignored].v1);
-        float4 v2 = __ldg(&sc.tris[ignored].v2);
-        ign_instance = __float_as_int(v1.w);
-        ign_local = __float_as_int(v2.w);
-    }
-    int stack_h[kStack];
-    float stack_t[kStack];
-    int sp = 0;
-    int cur = tl.n == 1 ? ~0 : 0;
-    const long long bound = 2ll * tl.n + 64;
-    for (long long step = 0;; ++step) {
-        if (step > bound || cur >= tl.n - 1 || ~cur >= tl.n) {
-            atomicOr(error, kErrLoopBound);
-            return SceneHit{-1, tmax, 0, 0};
-        }
-        bool pop = true;
-        if (cur >= 0) {
-            BvhNode nd = load_node(tl.nodes, cur);
-            float a, b;
-            bool hl = slab_hit(sr, node_left_box(nd), h.t, a);
-            bool hr = slab_hit(sr, node_right_box(nd), h.t, b);
-            if (hl) {
-                if (hr) {
-                    if (sp >= kStack) {
-                        atomicOr(error, kErrStackOverflow);
-                        return SceneHit{-1, tmax, 0, 0};
-                    }
-                    stack_h[sp] = nd.ch.y;
-                    stack_t[sp] = b;
-                    ++sp;
-                }
-                cur = nd.ch.x;
-                pop = false;
-            } else if (hr) {
-                cur = nd.ch.y;
-                pop = false;
-            }
-        } else {
-            int inst_id = sc.tlas_instance[tl.sorted_ids[~cur]];
-            const Instance& inst = sc.instances[inst_id];
-            f3 lo = xform_point(inst.inv, o);
-            f3 ld = xform_vector(inst.inv, d);
-            float best = h.t;
-            float u = 0, v = 0;
-            int local = blas_closest(sc.blas[inst.blas], lo, ld, tmin, best, u, v,
-                                     inst_id == ign_instance ? ign_local : -1, error);
-            if (local >= 0 && best < h.t) {
-                h.prim = inst.first_primitive + local;
-                h.t = best;
-                h.u = u;
-                h.v = v;
-            }
-        }
-        if (pop) {
-            bool resumed = false;
-            while (sp > 0) {
-                --sp;
-                if (!(stack_t[sp] > h.t)) {
-                    cur = stack_h[sp];
-                    resumed = true;
-                    break;
-                }
-            }
-            if (!resumed) break;
-        }
-    }
-    return h;
-}
-
-// ------------------------------------------------------------------ lights
-
-LUX_D float light_pmf(const SceneView& sc, int index) {  // gpu_scene_light_sampler.cuh:9-45
-    if (index < 0 || index >= sc.light_count || sc.total_light_power <= 0) return 0;
-    if (sc.light_sampler == 0) return 1.0f / static_cast<float>(sc.light_count);
-    return sc.light_alias ? sc.light_alias[index].pmf : 0.0f;
-}
-
-// sample_alias_table_index (light/light_sampler.h:71-82).
-LUX_D int sample_alias(const AliasEntry* table, int count, float u) {
-    float scaled = mul(fminf(u, 0.99999994f), static_cast<float>(count));
-    int column = static_cast<int>(scaled);
-    if (column >= count) column = count - 1;
-    float threshold = sub(scaled, static_cast<float>(column));
-    const AliasEntry& e = table[column];
-    int index = threshold < e.probability ? column : e.alias;
-    return index >= 0 && index < count ? index : -1;
-}
-
-struct LightLi {
-    f3 wi, position, radiance;
-    float distance = INFINITY;
-    float pdf = 0;
-    int measure = kMeasureSolidAngle;
-    bool valid = false;
-};
-
-LUX_D f3 sample_triangle_area(f3 v0, f3 v1, f3 v2, float ux, float uy) {  // light_sampler.h:361-367
-    float s = sqrtf(ux);
-    float b0 = sub(1.0f, s);
-    float b1 = mul(s, sub(1.0f, uy));
-    float b2 = mul(s, uy);
-    return (v0 * b0 + v1 * b1) + v2 * b2;
-}
-
-LUX_D float solid_angle_pdf(f3 lpos, f3 lnormal, int two_sided, float pdf_area, f3 ref) {
-    f3 to = lpos - ref;  // pdf_solid_angle (light/light_sampler.h:380-390)
-    float d2 = length2(to);
-    if (d2 <= mul(kRayEpsilon, kRayEpsilon) || pdf_area <= 0) return 0;
-    f3 wi = vdiv(to, sqrtf(d2));
-    float c = emission_cosine(lnormal, -wi, two_sided);
-    if (c <= 0) return 0;
-    return mul(pdf_area, d2) / c;
-}
-
-// sample_light_li (scene/scene_light_sampler.h:212-265 / gpu_scene_light_sampler.cuh:133-193).
-LUX_D LightLi sample_light(const SceneView& sc, f3 p, float select_u, float comp_u, float ux,
-                           float uy) {
-    (void)comp_u;
-    LightLi li;
-    if (sc.light_count <= 0 || sc.total_light_power <= 0) return li;
-    int index;
-    if (sc.light_sampler == 0) {
-        index = static_cast<int>(mul(fminf(select_u, 0.99999994f), static_cast<float>(sc.light_count)));
-        if (index >= sc.light_count) index = sc.light_count - 1;
-    } else {
-        if (!sc.light_alias) return li;
-        index = sample_alias(sc.light_alias, sc.light_count, select_u);
-    }
-    if (index < 0) return li;
-    float pmf = light_pmf(sc, index);
-    if (!(pmf > 0)) return li;
-    const Light L = sc.lights[index];
-    if (L.kind == 0) {
-        const SceneTri& t = sc.tris[L.primitive];
-        f3 v0 = xyz(t.v0), v1 = xyz(t.v1), v2 = xyz(t.v2);
-        f3 pos = sample_triangle_area(v0, v1, v2, ux, uy);
-        f3 n = triangle_normal(v0, v1, v2);
-        float pdf_area = L.area > 0 ? 1.0f / L.area : 0.0f;
-        f3 to = pos - p;
-        float d2 = length2(to);
-        if (d2 <= mul(kRayEpsilon, kRayEpsilon)) return li;
-        li.distance = sqrtf(d2);
-        li.wi = vdiv(to, li.distance);
-        li.position = pos;
-        li.radiance = eval_emission(L.emission, L.two_sided, n, -li.wi);
-        li.pdf = mul(pmf, solid_angle_pdf(pos, n, L.two_sided, pdf_area, p));
-        li.measure = kMeasureSolidAngle;
-        li.valid = max_component(li.radiance) > 0 && li.pdf > 0;
-        return li;
-    }
-    if (L.kind == 1) {  // sample_point_light (light/light.h:161-175)
-        f3 to = L.vec - p;
-        float d2 = length2(to);
-        if (d2 <= mul(kRayEpsilon, kRayEpsilon)) return li;
-        li.distance = sqrtf(d2);
-        li.wi = vdiv(to, li.distance);
-        li.position = L.vec;
-        li.radiance = vdiv(L.emission, d2);
-        li.pdf = 1.0f;
-        li.measure = kMeasureDiscrete;
-        li.valid = max_component(li.radiance) > 0;
-    } else if (L.kind == 2) {  // sample_distant_light (light/light.h:177-187)
-        li.wi = normalize(L.vec);
-        li.distance = INFINITY;
-        li.radiance = L.emission;
-        li.pdf = 1.0f;
-        li.measure = kMeasureDiscrete;
-        li.valid = max_component(li.radiance) > 0;
-    } else {  // uniform infinite (light/light.h:144-150, 189-197)
-        float z = sub(1.0f, mul(2.0f, ux));
-        float r = sqrtf(fmaxf(0.0f, sub(1.0f, mul(z, z))));
-        float phi = mul(mul(2.0f, kPi), uy);
-        li.wi = make_f3(mul(r, cosf(phi)), z, mul(r, sinf(phi)));
-        li.distance = INFINITY;
-        li.radiance = L.emission;
-        li.pdf = 1.0f / mul(4.0f, kPi);
-        li.measure = kMeasureSolidAngle;
-        li.valid = max_component(li.radiance) > 0;
-    }
-    li.pdf = mul(li.pdf, pmf);
-    return li;
-}
-
-LUX_D f3 infinite_le(const SceneView& sc) {  // infinite_lights_le
-    f3 le = splat(0);
-    for (int i = 0; i < sc.light_count; ++i)
-        if (sc.lights[i].kind == 3) le = le + sc.lights[i].emission;
-    return le;
-}
-
-LUX_D float infinite_pdf(const SceneView& sc) {  // infinite_lights_pdf_li
-    float pdf = 0;
-    for (int i = 0; i < sc.light_count; ++i)
-        if (sc.lights[i].kind == 3) pdf = add(pdf, mul(light_pmf(sc, i), 1.0f / mul(4.0f, kPi)));
-    return pdf;
-}
-
-// ------------------------------------------------------------------ path state helpers
-
-struct PathState {
-    f3 thr;
-    float eta;
-    f3 prev_pos;
-    float prev_pdf;
-    int pixel, sample, depth, passthrough, measure;
-    unsigned flags;
-};
-
-LUX_D PathState load_state(const Runtime& rt, int p) {
-    PathState s;
-    float4 a = rt.thr_eta[p];
-    float4 b = rt.prev[p];
-    int4 m = rt.meta[p];
-    s.thr = xyz(a);
-    s.eta = a.w;
-    s.prev_pos = xyz(b);
-    s.prev_pdf = b.w;
-    s.pixel = m.x;
-    s.sample = m.y;
-    s.depth = m.z & 0xffff;
-    s.passthrough = (m.z >> 16) & 0xffff;
-    s.measure = m.w & 0xff;
-    s.flags = static_cast<unsigned>(m.w) >> 8;
-    return s;
-}
-
-LUX_D void store_state(const Runtime& rt, int p, const PathState& s) {
-    rt.thr_eta[p] = make_float4(s.thr.x, s.thr.y, s.thr.z, s.eta);
-    rt.prev[p] = make_float4(s.prev_pos.x, s.prev_pos.y, s.prev_pos.z, s.prev_pdf);
-    rt.meta[p] = make_int4(s.pixel, s.sample, s.depth | (s.passthrough << 16),
-                           s.measure | static_cast<int>(s.flags << 8));
-}
-
-LUX_D Pcg load_rng(const Runtime& rt, int p) {
-    uint4 r = rt.rng[p];
-    Pcg g;
-    g.state = static_cast<uint64_t>(r.x) | (static_cast<uint64_t>(r.y) << 32);
-    g.inc = static_cast<uint64_t>(r.z) | (static_cast<uint64_t>(r.w) << 32);
-    return g;
-}
-
-LUX_D void store_rng(const Runtime& rt, int p, const Pcg& g) {
-    rt.rng[p] = make_uint4(static_cast<unsigned>(g.state), static_cast<unsigned>(g.state >> 32),
-                           static_cast<unsigned>(g.inc), static_cast<unsigned>(g.inc >> 32));
-}
-
-LUX_D void add_radiance(const Runtime& rt, int p, f3 v) {
-    float4 r = rt.rad[p];
-    rt.rad[p] = make_float4(add(r.x, v.x), add(r.y, v.y), add(r.z, v.z), 0.0f);
-}
-
-LUX_D int material_of(const SceneView& sc, int prim) {
-    return __float_as_int(__ldg(&sc.tris[prim].v0.w));
-}
-
-LUX_D int material_class(int type) {
-    switch (type) {
-        case kLambert: return 0;
-        case kThinLambert: return 1;
-        case kGgx: return 2;
-        case kDielectric: return 3;
-        default: return 4;
-    }
-}
-
 struct Batch {
     int pixel0, pixels;     // pixel range
     int sample0, samples;   // sample range (request-relative)
-    int width, height;
-    int max_depth;
-    uint64_t seed;
-    int frame_index, sample_offset;
+    CameraParams cam;
 };
 
-// ------------------------------------------------------------------ kernels
-
-// Camera rays (generate_camera_rays_kernel, wavefront_kernels.cu:234-270; draw order of
-// cpu_path_tracer.cpp:532-542: jitter x, jitter y, lens 2D, time).
-__global__ void __launch_bounds__(kThreads) k_camera(Runtime rt, SceneView sc, Batch b) {
+__global__ void __launch_bounds__(kThreads) k_camera(PathPool rt, int* counts, SceneView sc,
+                                                     Batch b) {
     int n = b.pixels * b.samples;
-    if (blockIdx.x == 0 && threadIdx.x == 0) rt.counts[0] = n;
+    if (blockIdx.x == 0 && threadIdx.x == 0) counts[0] = n;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        int pixel = b.pixel0 + i / b.samples;
-        int sample = b.sample0 + i % b.samples;
-        int x = pixel % b.width;
-        int y = pixel / b.width;
-        Pcg g = make_sampler(b.seed, b.frame_index, pixel, sample + b.sample_offset);
-        float jx = g.next_float();
-        float jy = g.next_float();
-        float u = add(static_cast<float>(x), jx) / static_cast<float>(b.width);
-        float v = add(static_cast<float>(b.height - 1 - y), jy) / static_cast<float>(b.height);
-        float lx = g.next_float();
-        float ly = g.next_float();
-        (void)g.next_float();  // time
-        f3 o, d;
-        camera_ray(sc.camera, u, v, lx, ly, o, d);
-        PathState s;
-        s.thr = splat(1.0f);
-        s.eta = 1.0f;
-        s.prev_pos = splat(0.0f);
-        s.prev_pdf = 0.0f;
-        s.pixel = pixel;
-        s.sample = sample;
-        s.depth = 0;
-        s.passthrough = 0;
-        s.measure = kMeasureNone;
-        s.flags = 0;
-        store_state(rt, i, s);
-        store_rng(rt, i, g);
-        rt.rad[i] = make_float4(0, 0, 0, 0);
-        rt.ray_o[i] = make_float4(o.x, o.y, o.z, kRayEpsilon);
-        rt.ray_d[i] = make_float4(d.x, d.y, d.z, INFINITY);
+        init_path(rt, sc.camera, i, b.pixel0 + i / b.samples, b.sample0 + i % b.samples, b.cam);
         rt.qray[0][i] = i;
     }
 }
 
-__global__ void __launch_bounds__(kThreads) k_extend(Runtime rt, SceneView sc, int depth,
-                                                     int* error) {
-    const int* counts = rt.counts + depth * kSlots;
-    int* mat_counts = rt.counts + depth * kSlots + 1;
-    int n = counts[0];
+__global__ void __launch_bounds__(kThreads) k_extend(PathPool rt, int* counts, SceneView sc,
+                                                     int sampler, int depth, int* error) {
+    int n = counts[depth * kSlots];
+    int* mat_counts = counts + depth * kSlots + 1;
     const int* q = rt.qray[depth & 1];
-    int rounds = (n + gridDim.x * blockDim.x - 1) / (gridDim.x * blockDim.x);
+    int stride = gridDim.x * blockDim.x;
+    int rounds = (n + stride - 1) / stride;
     for (int r = 0; r < rounds; ++r) {
-        int i = (r * gridDim.x + blockIdx.x) * blockDim.x + threadIdx.x;
+        int i = r * stride + blockIdx.x * blockDim.x + threadIdx.x;
         bool active = i < n;
         int p = active ? q[i] : 0;
-        int cls = 0;
-        bool hit = false;
-        if (active) {
-            float4 a = rt.ray_o[p];
-            float4 b = rt.ray_d[p];
-            SceneHit h = scene_closest(sc, xyz(a), xyz(b), a.w, b.w, -1, error);
-            if (h.prim >= 0) {
-                hit = true;
-                rt.hit[p] = make_float4(h.t, h.u, h.v, __int_as_float(h.prim));
-                cls = material_class(sc.materials[material_of(sc, h.prim)].type);
-            } else {
-                // Environment (cpu_path_tracer.cpp:415-428).
-                f3 le = infinite_le(sc);
-                if (max_component(le) > 0) {
-                    PathState s = load_state(rt, p);
-                    if (s.depth == 0 || is_delta(s.flags)) {
-                        add_radiance(rt, p, s.thr * le);
-                    } else if (s.measure == kMeasureSolidAngle && s.prev_pdf > 0) {
-                        float w = power_heuristic(s.prev_pdf, infinite_pdf(sc));
-                        add_radiance(rt, p, (s.thr * le) * w);
-                    }
-                }
-            }
-        }
-        int slot = append(mat_counts, cls, hit);
+        int cls = active ? extend_path(rt, sc, sampler, p, error) : -1;
+        bool hit = cls >= 0;
+        int slot = append(mat_counts, hit ? cls : 0, hit);
         if (hit) rt.qmat[cls * rt.capacity + slot] = p;
     }
 }
 
-// Emission seen at a hit (surface_light_le + area_light_pdf_solid_angle,
-// scene/scene_light_sampler.h:318-465), constant emission.
-LUX_D f3 surface_le(const SceneView& sc, int prim, const Material& m, f3 ng, f3 wo) {
-    int li = sc.primitive_light[prim];
-    if (li >= 0 && li < sc.light_count && sc.lights[li].kind == 0) {
-        const Light& L = sc.lights[li];
-        return eval_emission(L.emission, L.two_sided, ng, wo);
+__global__ void __launch_bounds__(kThreads) k_shade(PathPool rt, int* counts, SceneView sc,
+                                                    int sampler, int depth, int max_depth) {
+    const int* mc = counts + depth * kSlots + 1;
+    int* next_count = counts + (depth + 1) * kSlots;
+    int* shadow_count = counts + depth * kSlots + 6;
+    int c[kClasses];
+    int total = 0;
+    for (int k = 0; k < kClasses; ++k) {
+        c[k] = mc[k];
+        total += c[k];
     }
-    if (max_component(m.emission) <= 0) return splat(0);
-    return eval_emission(m.emission, m.two_sided, ng, wo);
-}
-
-LUX_D float surface_light_pdf(const SceneView& sc, int prim, f3 ng, f3 pos, f3 ref) {
-    int li = sc.primitive_light[prim];
-    if (li >= 0 && li < sc.light_count && sc.lights[li].kind == 0 && sc.lights[li].area > 0) {
-        const Light& L = sc.lights[li];
-        return mul(light_pmf(sc, li), solid_angle_pdf(pos, ng, L.two_sided, 1.0f / L.area, ref));
-    }
-    return 0.0f;
-}
-
-__global__ void __launch_bounds__(kThreads) k_shade(Runtime rt, SceneView sc, int depth,
-                                                    int max_depth, int* error) {
-    (void)error;
-    const int* mc = rt.counts + depth * kSlots + 1;
-    int* next_count = rt.counts + (depth + 1) * kSlots;
-    int* shadow_count = rt.counts + depth * kSlots + 6;
-    int c0 = mc[0], c1 = mc[1], c2 = mc[2], c3 = mc[3], c4 = mc[4];
-    int total = c0 + c1 + c2 + c3 + c4;
     int* qnext = rt.qray[(depth + 1) & 1];
-    int rounds = (total + gridDim.x * blockDim.x - 1) / (gridDim.x * blockDim.x);
+    int stride = gridDim.x * blockDim.x;
+    int rounds = (total + stride - 1) / stride;
     for (int r = 0; r < rounds; ++r) {
-        int i = (r * gridDim.x + blockIdx.x) * blockDim.x + threadIdx.x;
+        int i = r * stride + blockIdx.x * blockDim.x + threadIdx.x;
         bool active = i < total;
         int cls = 0, j = i;
-        if (j >= c0) { j -= c0; cls = 1;
-            if (j >= c1) { j -= c1; cls = 2;
-                if (j >= c2) { j -= c2; cls = 3;
-                    if (j >= c3) { j -= c3; cls = 4; } } } }
+        while (cls < kClasses - 1 && j >= c[cls]) j -= c[cls++];
         int p = active ? rt.qmat[cls * rt.capacity + j] : 0;
-        bool spawn = false, shadow = false;
-        float4 new_o, new_d;
-        float4 s_o, s_d, s_c, s_t;
-        if (active) {
-            float4 ra = rt.ray_o[p], rb = rt.ray_d[p], hh = rt.hit[p];
-            f3 ro = xyz(ra), rd = xyz(rb);
-            int prim = __float_as_int(hh.w);
-            float t = hh.x, hu = hh.y, hv = hh.z;
-            const SceneTri tri = sc.tris[prim];
-            f3 v0 = xyz(tri.v0), v1 = xyz(tri.v1), v2 = xyz(tri.v2);
-            const Material m = sc.materials[__float_as_int(tri.v0.w)];
-            PathState s = load_state(rt, p);
-            f3 pos = ro + rd * t;                    // Ray::at
-            f3 ng = triangle_normal(v0, v1, v2);
-            f3 wo = -rd;
-            // Emission with MIS (cpu_path_tracer.cpp:434-447).
-            f3 le = surface_le(sc, prim, m, ng, wo);
-            if (max_component(le) > 0) {
-                if (s.depth == 0 || is_delta(s.flags)) {
-                    add_radiance(rt, p, s.thr * le);
-                } else if (s.measure == kMeasureSolidAngle && s.prev_pdf > 0) {
-                    float lpdf = surface_light_pdf(sc, prim, ng, pos, s.prev_pos);
-                    add_radiance(rt, p, (s.thr * le) * power_heuristic(s.prev_pdf, lpdf));
-                }
-            }
-            if (is_passthrough(m)) {  // cpu_path_tracer.cpp:449-455
-                s.thr = s.thr * passthrough_transmittance(m);
-                if (max_component(s.thr) > 0 && depth < max_depth) {
-                    s.passthrough += 1;
-                    f3 no = pos + rd * kRayEpsilon;
-                    new_o = make_float4(no.x, no.y, no.z, kRayEpsilon);
-                    new_d = make_float4(rd.x, rd.y, rd.z, INFINITY);
-                    spawn = true;
-                }
-                store_state(rt, p, s);
-            } else if (is_scattering(m) && depth < max_depth && s.depth < max_depth) {
-                SceneTriShading sh = sc.shading[prim];
-                f3 ns = shading_normal(sh, ng, hu, hv);
-                if (dot(ng, ns) < 0) ns = -ns;   // make_surface_interaction
-                Interaction it{pos, ng, ns, wo};
-                Pcg g = load_rng(rt, p);
-                if (has_direct_lighting_lobe(m)) {  // estimate_direct_light, :122-158
-                    float su = g.next_float();
-                    float cu = g.next_float();
-                    float lx = g.next_float();
-                    float ly = g.next_float();
-                    LightLi li = sample_light(sc, pos, su, cu, lx, ly);
-                    if (li.valid && li.pdf > 0) {
-                        f3 f = eval_bsdf(m, it, li.wi);
-                        float cs = abs_cosine(ns, li.wi);
-                        float pb = pdf_bsdf(m, it, li.wi);
-                        if (max_component(f) > 0 && max_component(li.radiance) > 0 && cs > 0) {
-                            f3 contrib = (f * li.radiance) * (cs / li.pdf);
-                            float mis = li.measure == kMeasureDiscrete ? 1.0f
-                                                                       : power_heuristic(li.pdf, pb);
-                            f3 off = dot(li.wi, ng) >= 0 ? ng : -ng;
-                            f3 so = pos + off * kRayEpsilon;
-                            f3 sd = li.wi;
-                            float smax = INFINITY;
-                            bool ok = true;
-                            if (li.distance < INFINITY) {  // trace_shadow(from, to)
-                                f3 to = li.position - so;
-                                float dist = length(to);
-                                if (dist <= kRayEpsilon) ok = false;
-                                else {
-                                    sd = vdiv(to, dist);
-                                    smax = sub(dist, kRayEpsilon);
-                                }
-                            }
-                            if (ok) {
-                                shadow = true;
-                                s_o = make_float4(so.x, so.y, so.z, smax);
-                                s_d = make_float4(sd.x, sd.y, sd.z, __int_as_float(prim));
-                                s_c = make_float4(contrib.x, contrib.y, contrib.z, mis);
-                                s_t = make_float4(s.thr.x, s.thr.y, s.thr.z, 0.0f);
-                            }
-                        }
-                    }
-                }
-                float bx = g.next_float();
-                float by = g.next_float();
-                BsdfSample bs = sample_bsdf(m, it, bx, by);
-                if (bs.pdf > 0 && max_component(bs.weight) > 0) {
-                    f3 nthr = s.thr * bs.weight;
-                    float neta = mul(s.eta, is_transmission(bs.flags) && bs.eta > 0
-                                                ? mul(bs.eta, bs.eta) : 1.0f);
-                    bool alive = true;
-                    if (s.depth > 2) {  // path_transport.cuh:58-84
-                        float prob = fminf(0.95f, mul(max_component(nthr), neta));
-                        float ru = g.next_float();
-                        if (ru <= prob) nthr = vdiv(nthr, prob);
-                        else alive = false;
-                    }
-                    if (alive) {
-                        s.thr = nthr;
-                        s.eta = neta;
-                        s.prev_pdf = bs.pdf;
-                        s.measure = bs.measure;
-                        s.flags = bs.flags;
-                        s.prev_pos = pos;
-                        s.depth += 1;
-                        f3 off = dot(bs.wi, ng) >= 0 ? ng : -ng;   // spawn_scatter_ray
-                        f3 no = pos + off * kRayEpsilon;
-                        new_o = make_float4(no.x, no.y, no.z, kRayEpsilon);
-                        new_d = make_float4(bs.wi.x, bs.wi.y, bs.wi.z, INFINITY);
-                        spawn = true;
-                    }
-                }
-                store_state(rt, p, s);
-                store_rng(rt, p, g);
-            }
-        }
-        int slot = append(shadow_count, 0, shadow);
-        if (shadow) {
-            rt.sh_o[p] = s_o;
-            rt.sh_d[p] = s_d;
-            rt.sh_c[p] = s_c;
-            rt.sh_t[p] = s_t;
-            rt.qshadow[slot] = p;
-        }
-        slot = append(next_count, 0, spawn);
-        if (spawn) {
-            rt.ray_o[p] = new_o;
-            rt.ray_d[p] = new_d;
-            qnext[slot] = p;
-        }
+        ShadeOut o;
+        if (active) o = shade_path(rt, sc, sampler, max_depth, p);
+        int slot = append(shadow_count, 0, o.shadow);
+        if (o.shadow) rt.qshadow[slot] = p;
+        slot = append(next_count, 0, o.spawn);
+        if (o.spawn) qnext[slot] = p;
     }
 }
 
-// Shadow rays (trace_shadow, cpu_path_tracer.cpp:27-73): closest hits through
-// pass-through surfaces multiply the transmittance; an opaque hit blocks.
-__global__ void __launch_bounds__(kThreads) k_shadow(Runtime rt, SceneView sc, int depth,
-                                                     int* error) {
-    int n = rt.counts[depth * kSlots + 6];
+__global__ void __launch_bounds__(kThreads) k_shadow(PathPool rt, int* counts,
+                                                     unsigned long long* rays, SceneView sc,
+                                                     int depth, int* error) {
+    int n = counts[depth * kSlots + 6];
     unsigned long long segments = 0;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        int p = rt.qshadow[i];
-        float4 a = rt.sh_o[p], b = rt.sh_d[p];
-        f3 o = xyz(a), d = xyz(b);
-        float tmax = a.w;
-        float tmin = kRayEpsilon;
-        int ignored = __float_as_int(b.w);
-        f3 tr = splat(1.0f);
-        bool blocked = false;
-        for (int seg = 0;; ++seg) {
-            if (seg >= kShadowSegments) {
-                atomicOr(error, kErrLoopBound);
-                blocked = true;
-                break;
-            }
-            ++segments;
-            SceneHit h = scene_closest(sc, o, d, tmin, tmax, ignored, error);
-            if (h.prim < 0) break;
-            const Material m = sc.materials[material_of(sc, h.prim)];
-            if (!is_passthrough(m)) {
-                blocked = true;
-                break;
-            }
-            tr = tr * passthrough_transmittance(m);
-            if (max_component(tr) <= 0) break;
-            float adv = add(h.t, kRayEpsilon);
-            if (adv >= tmax) break;
-            o = o + d * adv;
-            tmax = sub(tmax, adv);
-            tmin = kRayEpsilon;
-            ignored = -1;
-        }
-        if (!blocked && max_component(tr) > 0) {
-            float4 c = rt.sh_c[p], t = rt.sh_t[p];
-            f3 contrib = (xyz(c) * tr) * c.w;
-            add_radiance(rt, p, xyz(t) * contrib);
-        }
-    }
-#pragma unroll
-    for (int off = 16; off > 0; off >>= 1) segments += __shfl_xor_sync(0xffffffffu, segments, off);
-    if ((threadIdx.x & 31) == 0 && segments) atomicAdd(rt.rays + 1, segments);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        shadow_path(rt, sc, rt.qshadow[i], error, segments);
+    warp_add(rays + 1, segments);
 }
 
 // Per-pixel film accumulation in sample order; or every sample's radiance.
-__global__ void __launch_bounds__(kThreads) k_flush(Runtime rt, Batch b, float* film,
+__global__ void __launch_bounds__(kThreads) k_flush(PathPool rt, Batch b, float* film,
                                                     float* samples, int spp) {
     for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < b.pixels; j += gridDim.x * blockDim.x) {
         int pixel = b.pixel0 + j;
@@ -795,22 +142,63 @@ __global__ void __launch_bounds__(kThreads) k_flush(Runtime rt, Batch b, float* 
     }
 }
 
-__global__ void k_count_rays(Runtime rt, int depth_slots) {
+__global__ void k_count_rays(const int* counts, unsigned long long* rays, int depth_slots) {
     unsigned long long total = 0;
-    for (int d = 0; d < depth_slots; ++d) total += static_cast<unsigned>(rt.counts[d * kSlots]);
-    atomicAdd(rt.rays, total);
+    for (int d = 0; d < depth_slots; ++d) total += static_cast<unsigned>(counts[d * kSlots]);
+    atomicAdd(rays, total);
 }
 
 Runtime* runtime_of(lux_ctx* ctx) { return static_cast<Runtime*>(ctx->render_runtime); }
 
 void runtime_release(Runtime* rt) {
-    void* ptrs[] = {rt->thr_eta, rt->rad, rt->prev, rt->meta, rt->rng, rt->ray_o, rt->ray_d,
-                    rt->hit, rt->sh_o, rt->sh_d, rt->sh_c, rt->sh_t, rt->qray[0], rt->qray[1],
-                    rt->qmat, rt->qshadow, rt->counts, rt->rays};
-    for (void* p : ptrs)
-        if (p) cudaFree(p);
+    path_pool_free(rt->pool);
+    if (rt->counts) cudaFree(rt->counts);
+    if (rt->rays) cudaFree(rt->rays);
+    long long keep[2] = {rt->last_counts[0], rt->last_counts[1]};
     *rt = Runtime{};
+    rt->last_counts[0] = keep[0];
+    rt->last_counts[1] = keep[1];
 }
+
+}  // namespace
+
+void path_pool_free(PathPool& p) {
+    void* ptrs[] = {p.thr_eta, p.rad, p.prev, p.meta, p.rng, p.ray_o, p.ray_d, p.hit, p.sh_o,
+                    p.sh_d, p.sh_c, p.sh_t, p.qray[0], p.qray[1], p.qmat, p.qshadow};
+    for (void* q : ptrs)
+        if (q) cudaFree(q);
+    p = PathPool{};
+}
+
+// Shared by the server: device buffers of a path pool of `capacity` paths.
+int path_pool_alloc(PathPool& p, int capacity) {
+    size_t c = static_cast<size_t>(capacity);
+    struct Req {
+        void** ptr;
+        size_t bytes;
+    } reqs[] = {
+        {reinterpret_cast<void**>(&p.thr_eta), 16 * c}, {reinterpret_cast<void**>(&p.rad), 16 * c},
+        {reinterpret_cast<void**>(&p.prev), 16 * c}, {reinterpret_cast<void**>(&p.meta), 16 * c},
+        {reinterpret_cast<void**>(&p.rng), 16 * c}, {reinterpret_cast<void**>(&p.ray_o), 16 * c},
+        {reinterpret_cast<void**>(&p.ray_d), 16 * c}, {reinterpret_cast<void**>(&p.hit), 16 * c},
+        {reinterpret_cast<void**>(&p.sh_o), 16 * c}, {reinterpret_cast<void**>(&p.sh_d), 16 * c},
+        {reinterpret_cast<void**>(&p.sh_c), 16 * c}, {reinterpret_cast<void**>(&p.sh_t), 16 * c},
+        {reinterpret_cast<void**>(&p.qray[0]), 4 * c}, {reinterpret_cast<void**>(&p.qray[1]), 4 * c},
+        {reinterpret_cast<void**>(&p.qmat), 4 * c * kClasses},
+        {reinterpret_cast<void**>(&p.qshadow), 4 * c},
+    };
+    for (auto& r : reqs) {
+        cudaError_t err = cudaMalloc(r.ptr, r.bytes);
+        if (err != cudaSuccess) {
+            cudaGetLastError();
+            return fail(LUX_ERR_OUT_OF_MEMORY, "path pool allocation failed");
+        }
+    }
+    p.capacity = capacity;
+    return LUX_OK;
+}
+
+namespace {
 
 int runtime_reserve(lux_ctx* ctx, int capacity, int max_depth) {
     Runtime* rt = runtime_of(ctx);
@@ -819,38 +207,21 @@ int runtime_reserve(lux_ctx* ctx, int capacity, int max_depth) {
         if (!rt) return fail(LUX_ERR_OUT_OF_MEMORY, "runtime allocation failed");
         ctx->render_runtime = rt;
     }
-    if (rt->capacity >= capacity && rt->max_depth >= max_depth) return LUX_OK;
+    if (rt->pool.capacity >= capacity && rt->max_depth >= max_depth) return LUX_OK;
     cudaStreamSynchronize(ctx->stream);
-    long long keep_counts[2] = {rt->last_counts[0], rt->last_counts[1]};
     runtime_release(rt);
-    rt->last_counts[0] = keep_counts[0];
-    rt->last_counts[1] = keep_counts[1];
-    size_t c = static_cast<size_t>(capacity);
-    struct Req {
-        void** p;
-        size_t bytes;
-    } reqs[] = {
-        {reinterpret_cast<void**>(&rt->thr_eta), 16 * c}, {reinterpret_cast<void**>(&rt->rad), 16 * c},
-        {reinterpret_cast<void**>(&rt->prev), 16 * c}, {reinterpret_cast<void**>(&rt->meta), 16 * c},
-        {reinterpret_cast<void**>(&rt->rng), 16 * c}, {reinterpret_cast<void**>(&rt->ray_o), 16 * c},
-        {reinterpret_cast<void**>(&rt->ray_d), 16 * c}, {reinterpret_cast<void**>(&rt->hit), 16 * c},
-        {reinterpret_cast<void**>(&rt->sh_o), 16 * c}, {reinterpret_cast<void**>(&rt->sh_d), 16 * c},
-        {reinterpret_cast<void**>(&rt->sh_c), 16 * c}, {reinterpret_cast<void**>(&rt->sh_t), 16 * c},
-        {reinterpret_cast<void**>(&rt->qray[0]), 4 * c}, {reinterpret_cast<void**>(&rt->qray[1]), 4 * c},
-        {reinterpret_cast<void**>(&rt->qmat), 4 * c * kClasses},
-        {reinterpret_cast<void**>(&rt->qshadow), 4 * c},
-        {reinterpret_cast<void**>(&rt->counts), sizeof(int) * kSlots * (max_depth + 2)},
-        {reinterpret_cast<void**>(&rt->rays), 16},
-    };
-    for (auto& r : reqs) {
-        cudaError_t err = cudaMalloc(r.p, r.bytes);
-        if (err != cudaSuccess) {
-            cudaGetLastError();
-            runtime_release(rt);
-            return fail(LUX_ERR_OUT_OF_MEMORY, "wavefront runtime allocation failed");
-        }
+    int st = path_pool_alloc(rt->pool, capacity);
+    cudaError_t err = cudaSuccess;
+    if (!st) err = cudaMalloc(&rt->counts, sizeof(int) * kSlots * (max_depth + 2));
+    if (!st && err == cudaSuccess) err = cudaMalloc(&rt->rays, 16);
+    if (!st && err != cudaSuccess) {
+        cudaGetLastError();
+        st = fail(LUX_ERR_OUT_OF_MEMORY, "wavefront runtime allocation failed");
     }
-    rt->capacity = capacity;
+    if (st) {
+        runtime_release(rt);
+        return st;
+    }
     rt->max_depth = max_depth;
     return LUX_OK;
 }
@@ -880,18 +251,16 @@ int render(lux_ctx* ctx, const lux_scene* scene, const lux_render_request& req, 
     const long long total_paths = static_cast<long long>(pixels) * req.spp;
     // Batch: whole pixels' sample ranges, at most ctx->render_batch paths.
     int batch_cap = std::max(1, ctx->render_batch);
-    int samples_per_batch = static_cast<int>(std::min<long long>(req.spp, std::max(1, batch_cap / std::max(pixels, 1))));
-    int pixels_per_batch = samples_per_batch >= req.spp || samples_per_batch > 1
-                               ? pixels
-                               : std::min(pixels, batch_cap);
-    if (samples_per_batch < 1) samples_per_batch = 1;
-    int capacity = static_cast<int>(std::min<long long>(total_paths,
-                                                         static_cast<long long>(pixels_per_batch) * samples_per_batch));
+    int samples_per_batch = static_cast<int>(
+        std::min<long long>(req.spp, std::max(1, batch_cap / std::max(pixels, 1))));
+    int pixels_per_batch = samples_per_batch > 1 || samples_per_batch >= req.spp
+                               ? pixels : std::min(pixels, batch_cap);
+    int capacity = static_cast<int>(std::min<long long>(
+        total_paths, static_cast<long long>(pixels_per_batch) * samples_per_batch));
     int st = runtime_reserve(ctx, std::max(capacity, 1), req.max_depth);
     if (st) return st;
     Runtime& rt = *runtime_of(ctx);
-    SceneView sc = scene->view;
-    sc.light_sampler = req.light_sampler;
+    const SceneView& sc = scene->view;
     cudaStream_t s = ctx->stream;
     int grid = ctx->sm_count * 8;
     cudaError_t err = cudaMemsetAsync(rt.rays, 0, 16, s);
@@ -906,25 +275,23 @@ int render(lux_ctx* ctx, const lux_scene* scene, const lux_render_request& req, 
             b.pixels = std::min(pixels_per_batch, pixels - p0);
             b.sample0 = s0;
             b.samples = ns;
-            b.width = req.width;
-            b.height = req.height;
-            b.max_depth = req.max_depth;
-            b.seed = req.seed;
-            b.frame_index = req.frame_index;
-            b.sample_offset = req.sample_offset;
+            b.cam = CameraParams{req.width, req.height, req.seed, req.frame_index, req.sample_offset};
             err = cudaMemsetAsync(rt.counts, 0, sizeof(int) * kSlots * (req.max_depth + 2), s);
             if (err != cudaSuccess) return cuda_fail(err, "counter reset");
-            k_camera<<<grid, kThreads, 0, s>>>(rt, sc, b);
+            k_camera<<<grid, kThreads, 0, s>>>(rt.pool, rt.counts, sc, b);
             ctx->launches += 1;
             for (int d = 0; d <= req.max_depth; ++d) {
-                k_extend<<<grid, kThreads, 0, s>>>(rt, sc, d, ctx->d_error);
-                k_shade<<<grid, kThreads, 0, s>>>(rt, sc, d, req.max_depth, ctx->d_error);
-                k_shadow<<<grid, kThreads, 0, s>>>(rt, sc, d, ctx->d_error);
+                k_extend<<<grid, kThreads, 0, s>>>(rt.pool, rt.counts, sc, req.light_sampler, d,
+                                                   ctx->d_error);
+                k_shade<<<grid, kThreads, 0, s>>>(rt.pool, rt.counts, sc, req.light_sampler, d,
+                                                  req.max_depth);
+                k_shadow<<<grid, kThreads, 0, s>>>(rt.pool, rt.counts, rt.rays, sc, d, ctx->d_error);
                 ctx->launches += 3;
             }
-            k_count_rays<<<1, 1, 0, s>>>(rt, req.max_depth + 1);
-            k_flush<<<std::max(1, std::min(grid, (b.pixels + kThreads - 1) / kThreads)), kThreads, 0, s>>>(
-                rt, b, per_sample ? nullptr : out, per_sample ? out : nullptr, req.spp);
+            k_count_rays<<<1, 1, 0, s>>>(rt.counts, rt.rays, req.max_depth + 1);
+            int fgrid = std::max(1, std::min(grid, (b.pixels + kThreads - 1) / kThreads));
+            k_flush<<<fgrid, kThreads, 0, s>>>(rt.pool, b, per_sample ? nullptr : out,
+                                               per_sample ? out : nullptr, req.spp);
             ctx->launches += 2;
             err = cudaGetLastError();
             if (err != cudaSuccess) return cuda_fail(err, "render launch");
