@@ -119,7 +119,13 @@ __global__ void __launch_bounds__(kThreads) k_generate(ServerDev d, int cur) {
         bool active = i < n;
         bool dead = false;
         int slot = 0;
-        if (active) {
+        if (active && d.tmap->count <= 0) {  // cannot happen: tickets imply a request
+            slot = d.free_list[base + i];
+            d.req_of[slot] = 0;
+            d.pool.meta[slot].x = -1;
+            atomicOr(d.error, kErrLoopBound);
+            dead = true;
+        } else if (active) {
             slot = d.free_list[base + i];
             long long t = t0 + i;
             int lo = 0, hi = d.tmap->count - 1;
@@ -134,6 +140,7 @@ __global__ void __launch_bounds__(kThreads) k_generate(ServerDev d, int cur) {
             d.req_of[slot] = rs;
             if (q.cancelled || idx < 0 || idx >= q.total) {
                 if (!q.cancelled) atomicOr(d.error, kErrLoopBound);
+                d.pool.meta[slot].x = -1;  // no film contribution
                 dead = true;
             } else {
                 init_path(d.pool, d.scenes[q.scene].camera, slot,
@@ -226,8 +233,8 @@ __global__ void __launch_bounds__(kThreads) k_retire(ServerDev d) {
         int rs = active ? d.req_of[p] : -1;
         if (active) {
             const ReqSlot& q = d.req[rs];
-            if (!q.cancelled) {
-                int pixel = d.pool.meta[p].x;
+            int pixel = d.pool.meta[p].x;
+            if (!q.cancelled && pixel >= 0 && pixel < q.width * q.height) {
                 float4 rad = d.pool.rad[p];
                 unsigned long long* f = q.film + 3 * static_cast<size_t>(pixel);
                 atomicAdd(f, to_fixed(rad.x));
