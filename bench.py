@@ -416,9 +416,270 @@ def measure_cpu_baseline(data) -> dict | None:
             "phases_ms": {k: v * 1e3 for k, v in est.items()}}
 
 
+# ------------------------------------------------------------------ render configurations
+
+def _render_setup(local=0):
+    import torch
+
+    import lux_b200
+
+    torch.cuda.set_device(local)
+    torch.cuda.set_stream(torch.cuda.Stream(torch.device("cuda", local)))
+    stream = torch.cuda.current_stream()
+    return torch, lux_b200.Context(local, stream.cuda_stream), stream
+
+
+def run_cornell(args) -> None:
+    """Config 1: the Cornell box, 256x256, 64 spp, depth 4, power light sampler, seed 1."""
+    torch, ctx, stream = _render_setup()
+    from lux_b200 import scene as S
+
+    W = H = 256
+    spp, depth, seed = 64, 4, 1
+    sc = S.Scene(ctx, S.make_cornell_scene(W, H))
+    req = S.request(W, H, spp, depth, seed)
+    film = torch.zeros((H, W, 3), dtype=torch.float32, device="cuda")
+    for _ in range(max(args.warmup, 1)):
+        S.render(ctx, sc, req, film)
+    torch.cuda.synchronize()
+    launches0 = ctx.launch_count()
+    clocks = ClockSampler(0)
+    clocks.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        S.render(ctx, sc, req, film)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    clock_info = clocks.stop()
+    ms = e0.elapsed_time(e1) / args.steps
+    rays = S.ray_counts(ctx)
+    total_rays = sum(rays)
+    value = total_rays / (ms * 1e-3) / 1e6
+    # e2e: host film through the C ABI (device -> host copy timed).
+    host_film = np.zeros((H, W, 3), np.float32)
+    t0 = time.perf_counter()
+    for _ in range(max(3, min(args.steps, 10))):
+        S.render(ctx, sc, req, host_film)
+    e2e_ms = (time.perf_counter() - t0) / max(3, min(args.steps, 10)) * 1e3
+    cpu = None
+    if not args.skip_cpu_baseline:
+        from oracle.bindings import Ref
+        if Ref.available():
+            threads = os.cpu_count() or 1
+            rows = 32
+            t0 = time.perf_counter()
+            Ref().cornell_render(W, H, spp, depth, seed, rows=(0, rows), threads=threads)
+            cpu_s = (time.perf_counter() - t0) * (H / rows)
+            cpu = {"value": total_rays / cpu_s / 1e6, "unit": "Mrays/s", "cores": threads,
+                   "kind": "reference",
+                   "sample": f"reference trace_path on rows 0..{rows} of 256 ({threads} threads), "
+                             "scaled; ray count of the same config"}
+    line = {"metric": "Mrays/s (Cornell 256^2, 64 spp, depth 4)", "value": value, "unit": "Mrays/s",
+            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic",
+            "config": {"workload": "Cornell box 256x256, 64 spp, max depth 4, power light "
+                                   "sampler, seed 1", "l2": "scene L2/L1 resident"},
+            "rays": {"camera_extension": rays[0], "shadow_segments": rays[1]},
+            "clocks": clock_info, "gpu_launches": ctx.launch_count() - launches0,
+            "e2e": {"value": total_rays / (e2e_ms * 1e-3) / 1e6, "unit": "Mrays/s",
+                    "h2d_bytes_per_step": 0, "d2h_bytes_per_step": W * H * 12,
+                    "ms_per_step": e2e_ms},
+            "cpu_baseline": cpu}
+    print(json.dumps(line))
+
+
+def run_batched(args) -> None:
+    """Config 4: 64 requests over 4 resident scenes, server vs the per-request path."""
+    torch, ctx, stream = _render_setup()
+    from lux_b200 import scene as S
+    from lux_b200 import scenes as SC
+    from lux_b200 import server as SV
+
+    builders = SC.resident_scenes(512, 512)
+    scenes = [S.Scene(ctx, b) for b in builders]
+    reqs = SC.batched_requests(args.requests, seed=11)
+    films_plain = [torch.zeros((r["height"], r["width"], 3), device="cuda") for r in reqs]
+    films_batch = [torch.zeros((r["height"], r["width"], 3), device="cuda") for r in reqs]
+    rr = [S.request(r["width"], r["height"], r["spp"], r["max_depth"], r["seed"]) for r in reqs]
+    # Plain per-request path: lux_render one request after the other, with this build's
+    # default 4M-path batches and with the reference scheduler's 65,536-path batches
+    # (RenderSettings::batch_size, integrator/render_context.h:18).
+    S.render(ctx, scenes[0], S.request(64, 64, 4, 4, 1))
+    torch.cuda.synchronize()
+
+    def plain_pass(batch):
+        ctx.set_option(3, batch)
+        rays = 0
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for r, q, f in zip(reqs, rr, films_plain):
+            S.render(ctx, scenes[r["scene"]], q, f)
+            rays += sum(S.ray_counts(ctx))
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return rays, e0.elapsed_time(e1) * 1e-3
+
+    ref_rays, ref_s = plain_pass(65536) if not args.skip_reference_batch else (0, float("nan"))
+    plain_rays, plain_s = plain_pass(1 << 22)
+    # Batched: one server, all requests submitted at once.
+    with SV.Server(scenes, pool_paths=args.pool) as srv:
+        warm, _ = srv.submit(0, S.request(64, 64, 4, 4, 1))
+        srv.wait(warm)
+        base = srv.stats()
+        ids = [srv.submit(r["scene"], q, f)[0] for r, q, f in zip(reqs, rr, films_batch)]
+        srv.wait_all()
+        stats = srv.stats()
+        t_sub = min(srv.times(i)[0] for i in ids)
+        t_done = max(srv.times(i)[2] for i in ids)
+    batch_s = (t_done - t_sub) * 1e-9
+    batch_rays = (stats["rays"] - base["rays"]) + (stats["shadow_rays"] - base["shadow_rays"])
+    rel = max(float(((a - b).abs() / (1 + b.abs())).max()) for a, b in zip(films_batch, films_plain))
+    value = batch_rays / batch_s / 1e6
+    line = {"metric": "Mrays/s (batched: 64 mixed requests over 4 resident scenes)",
+            "value": value, "unit": "Mrays/s", "n_gpus": 1, "steps": 1, "warmup": 1,
+            "ms_per_step": batch_s * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"{args.requests} requests: resolution log-uniform 128^2..1024^2,"
+                                   " spp log-uniform 16..256, depth uniform 4..12, seed 11; scenes:"
+                                   " Cornell, displaced icosphere + glass (332,836 tris),"
+                                   " 2,097,152-tri soup, 16x16 icosphere grid",
+                       "pool_paths": args.pool},
+            "plain_per_request": {"value": plain_rays / plain_s / 1e6, "unit": "Mrays/s",
+                                  "seconds": plain_s, "rays": plain_rays,
+                                  "batch_paths": 1 << 22},
+            "plain_per_request_reference_batch": {
+                "value": ref_rays / ref_s / 1e6 if ref_rays else None, "unit": "Mrays/s",
+                "seconds": ref_s, "batch_paths": 65536},
+            "speedup_vs_plain": (batch_rays / batch_s) / (plain_rays / plain_s),
+            "speedup_vs_plain_reference_batch": ((batch_rays / batch_s) / (ref_rays / ref_s)
+                                                 if ref_rays else None),
+            "rays": batch_rays, "iterations": stats["iterations"] - base["iterations"],
+            "max_rel_film_difference_vs_plain": rel}
+    print(json.dumps(line))
+
+
+def _poisson_arrivals(rate: float, count: int, seed: int) -> np.ndarray:
+    u = W.splitmix_uniform(seed, 31, count)
+    return np.cumsum(-np.log(1.0 - u) / rate)
+
+
+def _displaced(base: np.ndarray, frame: int) -> np.ndarray:
+    """Sinusoidal vertex displacement of the animated icosphere at a frame."""
+    v = base.copy()
+    phase = 0.35 * frame
+    v[:, 1] += 0.02 * np.sin(6.0 * v[:, 0] + phase)
+    return v
+
+
+def run_serving(args) -> None:
+    """Config 5: Poisson arrivals over the resident scenes; the displaced icosphere is
+    refit every frame; p50/p99 latency and Mrays/s, against a FIFO one-request-at-a-time
+    server built from the per-request path's measured service times."""
+    import threading
+
+    torch, ctx, stream = _render_setup()
+    from lux_b200 import scene as S
+    from lux_b200 import scenes as SC
+    from lux_b200 import server as SV
+
+    builders = SC.resident_scenes(512, 512)
+    scenes = [S.Scene(ctx, b) for b in builders]
+    anim_scene, anim_mesh = 1, 1
+    base = builders[anim_scene].meshes[anim_mesh].vertices.copy()
+    frame_s = 1.0 / 30.0
+    rates = [float(r) for r in args.rates.split(",")]
+    results = []
+    for ri, rate in enumerate(rates):
+        reqs = SC.batched_requests(args.requests, seed=100 + ri)
+        if args.request_scale != 1.0:
+            for r in reqs:
+                side = max(16, int(r["width"] * args.request_scale))
+                r["width"] = r["height"] = side
+                r["spp"] = max(1, int(r["spp"] * args.request_scale))
+        arrivals = _poisson_arrivals(rate, len(reqs), seed=200 + ri)
+        rr = [S.request(r["width"], r["height"], r["spp"], r["max_depth"], r["seed"])
+              for r in reqs]
+        films = [torch.zeros((r["height"], r["width"], 3), device="cuda") for r in reqs]
+        # Per-request service times (plain path), for the FIFO comparison.
+        service, plain_rays = [], 0
+        for r, q, f in zip(reqs, rr, films):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            S.render(ctx, scenes[r["scene"]], q, f)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            service.append(e0.elapsed_time(e1) * 1e-3)
+            plain_rays += sum(S.ray_counts(ctx))
+        free_at, fifo_lat = 0.0, []
+        for a, sv in zip(arrivals, service):
+            start = max(a, free_at)
+            free_at = start + sv
+            fifo_lat.append(free_at - a)
+        with SV.Server(scenes, pool_paths=args.pool) as srv:
+            warm, _ = srv.submit(0, S.request(32, 32, 2, 2, 1))
+            srv.wait(warm)
+            base_stats = srv.stats()
+            ids = [None] * len(reqs)
+            stop = threading.Event()
+
+            def animate():
+                frame = 0
+                while not stop.wait(frame_s):
+                    frame += 1
+                    srv.update_mesh(anim_scene, anim_mesh, _displaced(base, frame))
+
+            anim = threading.Thread(target=animate)
+            anim.start()
+            t0 = time.perf_counter()
+            for k, (r, q, f) in enumerate(zip(reqs, rr, films)):
+                delay = arrivals[k] - (time.perf_counter() - t0)
+                if delay > 0:
+                    time.sleep(delay)
+                ids[k] = srv.submit(r["scene"], q, f)[0]
+            try:
+                srv.wait_all(timeout_s=600)
+            finally:
+                stop.set()
+                anim.join()
+            stats = srv.stats()
+            lat = [(srv.times(i)[2] - srv.times(i)[0]) * 1e-9 for i in ids]
+            span = (max(srv.times(i)[2] for i in ids) - min(srv.times(i)[0] for i in ids)) * 1e-9
+        rays = (stats["rays"] - base_stats["rays"]) + (stats["shadow_rays"] - base_stats["shadow_rays"])
+        results.append({"rate_req_s": rate, "requests": len(reqs),
+                        "p50_ms": float(np.percentile(lat, 50) * 1e3),
+                        "p99_ms": float(np.percentile(lat, 99) * 1e3),
+                        "mrays_s": rays / span / 1e6, "refits": stats["refits"],
+                        "fifo_plain_p50_ms": float(np.percentile(fifo_lat, 50) * 1e3),
+                        "fifo_plain_p99_ms": float(np.percentile(fifo_lat, 99) * 1e3),
+                        "fifo_plain_mrays_s": plain_rays / max(free_at, 1e-9) / 1e6})
+    best = max(results, key=lambda r: r["mrays_s"])
+    line = {"metric": "p50/p99 render-request latency and Mrays/s (served)",
+            "value": best["mrays_s"], "unit": "Mrays/s", "n_gpus": 1, "steps": len(rates),
+            "warmup": 1, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "Poisson arrivals over the 4 resident scenes; requests from the "
+                                   "batched distribution scaled by %g; displaced icosphere refit "
+                                   "every 1/30 s" % args.request_scale,
+                       "pool_paths": args.pool},
+            "sweep": results}
+    print(json.dumps(line))
+
+
 def main():
     global N_TRIS, N_RAYS, N_QUERIES, WORKLOAD
     ap = argparse.ArgumentParser()
+    ap.add_argument("--config", default="lbvh", choices=["lbvh", "cornell", "batched", "serving"],
+                    help="lbvh: the LBVH microbench (default); cornell: config 1; batched: "
+                         "config 4; serving: config 5")
+    ap.add_argument("--rates", default="10,50,100,200,500")
+    ap.add_argument("--request-scale", type=float, default=0.25,
+                    help="serving: scale of request resolution and spp")
+    ap.add_argument("--requests", type=int, default=64)
+    ap.add_argument("--skip-reference-batch", action="store_true",
+                    help="batched: skip the plain pass at the reference's 65,536-path batch")
+    ap.add_argument("--pool", type=int, default=1 << 22)
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=5)
@@ -437,7 +698,13 @@ def main():
         N_TRIS, N_RAYS, N_QUERIES = args.tris, args.rays, args.queries
         WORKLOAD = (f"LBVH microbench generator at reduced size (profiling case): {N_TRIS} "
                     f"triangles, {N_RAYS} rays, {N_QUERIES} query boxes, seed 7")
-    if args.impl == "reference":
+    if args.config == "cornell" and args.impl == "lux":
+        run_cornell(args)
+    elif args.config == "batched":
+        run_batched(args)
+    elif args.config == "serving":
+        run_serving(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_lux(args)

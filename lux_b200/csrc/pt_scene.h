@@ -33,6 +33,15 @@ struct lux_scene {
     float* tri_soup = nullptr;          // per-mesh object-space soups for refits (device)
     std::vector<size_t> soup_offset;    // float offset of each mesh's soup
     float* tlas_boxes = nullptr;        // instance world boxes (device)
+    // Device buffers of vertex updates, allocated on a mesh's first update.
+    struct MeshRefit {
+        float* vertices = nullptr;       // object space, 3 per vertex
+        uint32_t* indices = nullptr;     // 3 per triangle
+        int* instances = nullptr;        // instances of the mesh, then their TLAS entries
+        int instance_count = 0;
+        int entry_count = 0;
+    };
+    std::vector<MeshRefit> refit;
     lux::pt::SceneView view;            // device pointers + counts (TLAS/BLAS filled in)
 };
 
@@ -40,7 +49,11 @@ namespace lux {
 
 int scene_create(lux_ctx* ctx, const lux_scene_desc* desc, lux_scene** out);
 void scene_free(lux_scene* scene);
-int scene_update_mesh(lux_ctx* ctx, lux_scene* scene, int mesh, const float* vertices);
+// Replaces one mesh's vertices (same count and topology) and refits its BLAS and the TLAS,
+// all in stream order on ctx->stream.  With sync, waits and reports device errors; without,
+// the caller's next synchronisation does.
+int scene_update_mesh(lux_ctx* ctx, lux_scene* scene, int mesh, const float* vertices,
+                      bool sync = true);
 int camera_perspective(const float* origin, const float* look_at, float vfov, float aspect,
                        float lens_radius, float focal_distance, lux_camera_desc* out);
 

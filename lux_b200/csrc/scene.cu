@@ -262,6 +262,12 @@ Box instance_box(const std::vector<float>& soup, int triangle_count, const float
 }  // namespace
 
 void scene_free(lux_scene* s) {
+    for (auto& r : s->refit) {
+        cudaFree(r.vertices);
+        cudaFree(r.indices);
+        cudaFree(r.instances);
+    }
+    s->refit.clear();
     void* ptrs[] = {s->materials, s->tris, s->shading, s->d_instances, s->tlas_instance,
                     s->blas_views, s->lights, s->light_alias, s->primitive_light, s->tri_soup,
                     s->tlas_boxes};
@@ -510,65 +516,185 @@ int camera_perspective(const float* origin, const float* look_at, float vfov, fl
     return LUX_OK;
 }
 
-int scene_update_mesh(lux_ctx* ctx, lux_scene* s, int mesh, const float* vertices) {
+// ---------------------------------------------------------------- vertex updates
+// A vertex update runs on the device in stream order: vertex upload, object-space soup,
+// BLAS refit, world positions of every instance of the mesh, instance boxes from the
+// refit BLAS's root box (the mesh box: the union of its triangle boxes), TLAS refit.
+// The arithmetic is the host restatement's (transform_point, transform_bounds), written
+// with round-to-nearest intrinsics so that nothing is contracted, so a refit scene holds
+// the values a scene created from the same vertices would.
+namespace {
+
+constexpr int kRefitThreads = 256;
+
+__device__ float3 world_point(const float* m, float px, float py, float pz) {
+    float x = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(m[0], px), __fmul_rn(m[1], py)),
+                                  __fmul_rn(m[2], pz)), m[3]);
+    float y = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(m[4], px), __fmul_rn(m[5], py)),
+                                  __fmul_rn(m[6], pz)), m[7]);
+    float z = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(m[8], px), __fmul_rn(m[9], py)),
+                                  __fmul_rn(m[10], pz)), m[11]);
+    float w = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(0.0f, px), __fmul_rn(0.0f, py)),
+                                  __fmul_rn(0.0f, pz)), 1.0f);
+    if (w == 1.0f) return make_float3(x, y, z);
+    return make_float3(__fdiv_rn(x, w), __fdiv_rn(y, w), __fdiv_rn(z, w));
+}
+
+// mesh_soup on the device: 9 floats per triangle.
+__global__ void k_mesh_soup(const float* vertices, int vertex_count, const uint32_t* indices,
+                            int triangle_count, float* soup, int* error) {
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < triangle_count;
+         t += gridDim.x * blockDim.x) {
+        for (int k = 0; k < 3; ++k) {
+            uint32_t v = indices[3 * size_t(t) + k];
+            if (v >= static_cast<uint32_t>(vertex_count)) {  // validated at scene creation
+                atomicOr(error, kErrLoopBound);
+                v = 0;
+            }
+            soup[size_t(t) * 9 + 3 * k + 0] = vertices[3 * size_t(v) + 0];
+            soup[size_t(t) * 9 + 3 * k + 1] = vertices[3 * size_t(v) + 1];
+            soup[size_t(t) * 9 + 3 * k + 2] = vertices[3 * size_t(v) + 2];
+        }
+    }
+}
+
+// World positions of the mesh's triangles in each of its instances (instance_triangles);
+// the .w tags (material, instance, local triangle) are left as uploaded.
+__global__ void k_instance_positions(const float* soup, int triangle_count,
+                                     const pt::Instance* instances, const int* ids,
+                                     int instance_count, pt::SceneTri* tris) {
+    int64_t total = int64_t(triangle_count) * instance_count;
+    for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < total;
+         i += int64_t(gridDim.x) * blockDim.x) {
+        int j = static_cast<int>(i / triangle_count);
+        int t = static_cast<int>(i - int64_t(j) * triangle_count);
+        const pt::Instance& inst = instances[ids[j]];
+        const float* p = soup + size_t(t) * 9;
+        float3 w0 = world_point(inst.m, p[0], p[1], p[2]);
+        float3 w1 = world_point(inst.m, p[3], p[4], p[5]);
+        float3 w2 = world_point(inst.m, p[6], p[7], p[8]);
+        pt::SceneTri* dst = tris + inst.first_primitive + t;
+        dst->v0 = make_float4(w0.x, w0.y, w0.z, dst->v0.w);
+        dst->v1 = make_float4(w1.x, w1.y, w1.z, dst->v1.w);
+        dst->v2 = make_float4(w2.x, w2.y, w2.z, dst->v2.w);
+    }
+}
+
+// transform_bounds of the mesh box for each TLAS entry of the mesh (instance_box).
+__global__ void k_instance_boxes(const float* mesh_box, const pt::Instance* instances,
+                                 const int* tlas_instance, const int* entries, int entry_count,
+                                 float* tlas_boxes) {
+    int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= entry_count) return;
+    int k = entries[j];
+    const pt::Instance& inst = instances[tlas_instance[k]];
+    float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+    bool empty = mesh_box[0] > mesh_box[3] || mesh_box[1] > mesh_box[4] ||
+                 mesh_box[2] > mesh_box[5];
+    if (!empty) {
+        for (int c = 0; c < 8; ++c) {
+            int x = c & 1, y = (c >> 1) & 1, z = c >> 2;
+            float3 w = world_point(inst.m, x ? mesh_box[3] : mesh_box[0],
+                                   y ? mesh_box[4] : mesh_box[1], z ? mesh_box[5] : mesh_box[2]);
+            lo[0] = fminf(lo[0], w.x); lo[1] = fminf(lo[1], w.y); lo[2] = fminf(lo[2], w.z);
+            hi[0] = fmaxf(hi[0], w.x); hi[1] = fmaxf(hi[1], w.y); hi[2] = fmaxf(hi[2], w.z);
+        }
+    }
+    for (int a = 0; a < 3; ++a) {
+        tlas_boxes[6 * k + a] = lo[a];
+        tlas_boxes[6 * k + 3 + a] = hi[a];
+    }
+}
+
+int blocks_for(lux_ctx* ctx, int64_t items) {
+    int64_t b = (items + kRefitThreads - 1) / kRefitThreads;
+    return static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(b, int64_t(ctx->sm_count) * 8)));
+}
+
+// First update of a mesh: device vertex/index buffers and its instance/TLAS-entry lists.
+int prepare_refit(lux_scene* s, int mesh) {
+    if (s->refit.size() < s->blas.size()) s->refit.resize(s->blas.size());
+    lux_scene::MeshRefit& r = s->refit[mesh];
+    if (r.vertices) return LUX_OK;
+    std::vector<int> lists;
+    for (size_t i = 0; i < s->instances.size(); ++i)
+        if (s->instances[i].blas == mesh) lists.push_back(static_cast<int>(i));
+    int instance_count = static_cast<int>(lists.size());
+    for (size_t k = 0; k < s->tlas_instance_host.size(); ++k)
+        if (s->instances[s->tlas_instance_host[k]].blas == mesh) lists.push_back(static_cast<int>(k));
+    const auto& verts = s->mesh_vertices[mesh];
+    const auto& idx = s->mesh_indices[mesh];
+    cudaError_t err = cudaMalloc(&r.vertices, sizeof(float) * std::max<size_t>(1, verts.size()));
+    if (err == cudaSuccess)
+        err = cudaMalloc(&r.indices, sizeof(uint32_t) * std::max<size_t>(1, idx.size()));
+    if (err == cudaSuccess)
+        err = cudaMalloc(&r.instances, sizeof(int) * std::max<size_t>(1, lists.size()));
+    if (err == cudaSuccess && !idx.empty())
+        err = cudaMemcpy(r.indices, idx.data(), sizeof(uint32_t) * idx.size(),
+                         cudaMemcpyHostToDevice);
+    if (err == cudaSuccess && !lists.empty())
+        err = cudaMemcpy(r.instances, lists.data(), sizeof(int) * lists.size(),
+                         cudaMemcpyHostToDevice);
+    if (err != cudaSuccess) {
+        cudaFree(r.vertices);
+        cudaFree(r.indices);
+        cudaFree(r.instances);
+        r = lux_scene::MeshRefit{};
+        return cuda_fail(err, "mesh update buffers");
+    }
+    r.instance_count = instance_count;
+    r.entry_count = static_cast<int>(lists.size()) - instance_count;
+    return LUX_OK;
+}
+
+}  // namespace
+
+int scene_update_mesh(lux_ctx* ctx, lux_scene* s, int mesh, const float* vertices, bool sync) {
     if (mesh < 0 || mesh >= static_cast<int>(s->blas.size()))
         return fail(LUX_ERR_INVALID_ARGUMENT, "mesh out of range");
+    if (int st = prepare_refit(s, mesh)) return st;
     std::vector<float>& verts = s->mesh_vertices[mesh];
     std::memcpy(verts.data(), vertices, sizeof(float) * verts.size());
-    lux_mesh_desc md{};
-    md.vertices = verts.data();
-    md.vertex_count = static_cast<int>(verts.size() / 3);
-    md.indices = s->mesh_indices[mesh].data();
-    md.triangle_count = static_cast<int>(s->mesh_indices[mesh].size() / 3);
-    std::vector<float> soup = mesh_soup(md, verts.data());
-    cudaError_t err = cudaMemcpyAsync(s->tri_soup + s->soup_offset[mesh], soup.data(),
-                                      sizeof(float) * soup.size(), cudaMemcpyHostToDevice,
-                                      ctx->stream);
-    if (err != cudaSuccess) return cuda_fail(err, "mesh upload");
-    int st = lux_lbvh_refit(ctx, s->blas[mesh], s->tri_soup + s->soup_offset[mesh],
-                            md.triangle_count);
-    if (st) return st;
-    // World triangles of every instance of this mesh (normals unchanged).
-    std::vector<pt::SceneTri> tris;
-    std::vector<pt::SceneTriShading> shading;
-    std::vector<float> boxes;
-    for (size_t i = 0; i < s->instances.size(); ++i) {
-        if (s->instances[i].blas != mesh) continue;
-        tris.clear();
-        shading.clear();
-        md.material_ids = nullptr;
-        std::vector<int> mids(md.triangle_count, 0);
-        md.material_ids = mids.data();
-        instance_triangles(md, s->instances[i], static_cast<int>(i), 0, tris, shading);
-        // Keep the uploaded material ids: patch positions only.
-        std::vector<pt::SceneTri> old(tris.size());
-        err = cudaMemcpy(old.data(), s->tris + s->instances[i].first_primitive,
-                         sizeof(pt::SceneTri) * old.size(), cudaMemcpyDeviceToHost);
-        if (err != cudaSuccess) return cuda_fail(err, "triangle download");
-        for (size_t t = 0; t < tris.size(); ++t) tris[t].v0.w = old[t].v0.w;
-        err = cudaMemcpyAsync(s->tris + s->instances[i].first_primitive, tris.data(),
-                              sizeof(pt::SceneTri) * tris.size(), cudaMemcpyHostToDevice,
-                              ctx->stream);
-        if (err != cudaSuccess) return cuda_fail(err, "triangle upload");
+    const lux_scene::MeshRefit& r = s->refit[mesh];
+    const int triangle_count = static_cast<int>(s->mesh_indices[mesh].size() / 3);
+    const int vertex_count = static_cast<int>(verts.size() / 3);
+    if (triangle_count == 0) return LUX_OK;
+    float* soup = s->tri_soup + s->soup_offset[mesh];
+    cudaStream_t stream = ctx->stream;
+    // From pageable memory the copy is staged before the call returns.
+    cudaError_t err = cudaMemcpyAsync(r.vertices, verts.data(), sizeof(float) * verts.size(),
+                                      cudaMemcpyHostToDevice, stream);
+    if (err != cudaSuccess) return cuda_fail(err, "vertex upload");
+    k_mesh_soup<<<blocks_for(ctx, triangle_count), kRefitThreads, 0, stream>>>(
+        r.vertices, vertex_count, r.indices, triangle_count, soup, ctx->d_error);
+    ctx->launches += 1;
+    if (int st = lbvh_refit(ctx, s->blas[mesh], soup)) return st;
+    if (r.instance_count > 0) {
+        k_instance_positions<<<blocks_for(ctx, int64_t(triangle_count) * r.instance_count),
+                               kRefitThreads, 0, stream>>>(soup, triangle_count, s->d_instances,
+                                                           r.instances, r.instance_count, s->tris);
+        ctx->launches += 1;
     }
-    for (size_t k = 0; k < s->tlas_instance_host.size(); ++k) {
-        const Instance& inst = s->instances[s->tlas_instance_host[k]];
-        Box b = instance_box(mesh_soup(lux_mesh_desc{s->mesh_vertices[inst.blas].data(), nullptr,
-                                                     nullptr,
-                                                     static_cast<int>(s->mesh_vertices[inst.blas].size() / 3),
-                                                     s->mesh_indices[inst.blas].data(), nullptr,
-                                                     static_cast<int>(s->mesh_indices[inst.blas].size() / 3)},
-                                       s->mesh_vertices[inst.blas].data()),
-                             static_cast<int>(s->mesh_indices[inst.blas].size() / 3), inst.m);
-        float f[6] = {b.lo.x, b.lo.y, b.lo.z, b.hi.x, b.hi.y, b.hi.z};
-        boxes.insert(boxes.end(), f, f + 6);
+    if (r.entry_count > 0) {
+        k_instance_boxes<<<(r.entry_count + kRefitThreads - 1) / kRefitThreads, kRefitThreads, 0,
+                           stream>>>(s->blas[mesh]->root, s->d_instances, s->tlas_instance,
+                                     r.instances + r.instance_count, r.entry_count, s->tlas_boxes);
+        ctx->launches += 1;
+        if (int st = lbvh_refit(ctx, s->tlas, s->tlas_boxes)) return st;
     }
-    err = cudaMemcpyAsync(s->tlas_boxes, boxes.data(), sizeof(float) * boxes.size(),
-                          cudaMemcpyHostToDevice, ctx->stream);
-    if (err != cudaSuccess) return cuda_fail(err, "instance box upload");
-    st = lux_lbvh_refit(ctx, s->tlas, s->tlas_boxes, static_cast<int>(s->tlas_instance_host.size()));
-    if (st) return st;
-    return cuda_fail(cudaStreamSynchronize(ctx->stream), "mesh update");
+    err = cudaGetLastError();
+    if (err != cudaSuccess) return cuda_fail(err, "mesh update");
+    if (!sync) return LUX_OK;
+    err = cudaStreamSynchronize(stream);
+    if (err != cudaSuccess) return cuda_fail(err, "mesh update");
+    int word = 0;
+    err = cudaMemcpy(&word, ctx->d_error, sizeof(int), cudaMemcpyDeviceToHost);
+    if (err != cudaSuccess) return cuda_fail(err, "mesh update");
+    if (word) {
+        cudaMemset(ctx->d_error, 0, sizeof(int));
+        return fail(LUX_ERR_DEVICE_CHECK, "mesh update: device check failed");
+    }
+    return LUX_OK;
 }
 
 }  // namespace lux

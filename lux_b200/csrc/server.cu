@@ -502,13 +502,25 @@ void worker_main(lux_server* s) {
     for (;;) {
         if (s->stop) break;
         if (s->error_status == 0) admit(s);
-        while (!s->updates.empty()) {
-            auto u = std::move(s->updates.front());
-            s->updates.pop_front();
+        if (!s->updates.empty()) {
+            // One batch of vertex updates per iteration, the latest per mesh; updates that
+            // arrive while it is applied wait for the next iteration, so a producer faster
+            // than the refits cannot starve the render.
+            std::deque<lux_server::MeshUpdate> batch;
+            batch.swap(s->updates);
             lk.unlock();
-            int st = lux::scene_update_mesh(s->ctx, s->scenes[u.scene], u.mesh, u.vertices.data());
+            int64_t applied = 0;
+            for (size_t k = 0; k < batch.size(); ++k) {
+                bool superseded = false;
+                for (size_t j = k + 1; j < batch.size() && !superseded; ++j)
+                    superseded = batch[j].scene == batch[k].scene && batch[j].mesh == batch[k].mesh;
+                if (superseded) continue;
+                if (lux::scene_update_mesh(s->ctx, s->scenes[batch[k].scene], batch[k].mesh,
+                                           batch[k].vertices.data(), false) == LUX_OK)
+                    ++applied;
+            }
             lk.lock();
-            if (st == LUX_OK) ++s->refits;
+            s->refits += applied;
         }
         bool busy = !s->active.empty() || !s->delivering.empty();
         if (!busy && s->launched == s->collected) {

@@ -188,3 +188,35 @@ def test_empty_scene_renders_black(ctx):
     sc = S.Scene(ctx, b)
     film = S.render(ctx, sc, S.request(8, 8, 2, 3))
     assert np.all(film == 0)
+
+
+def test_device_mesh_update_matches_a_fresh_scene(ctx):
+    """lux_scene_update_mesh on a mesh with two transformed instances renders like a
+    scene created from the moved vertices (world triangles and instance boxes are
+    computed with the host restatement's arithmetic)."""
+    from lux_b200 import scenes as SC
+
+    def build(vertices=None):
+        b = S.make_cornell_scene(32, 32)
+        v, idx = SC.displaced_sphere(4, (0.0, 0.0, 0.0), 0.3, 0.04, 5)
+        if vertices is not None:
+            v = vertices
+        rough = b.add_material(S.ggx((0.8, 0.5, 0.3), 0.35, 0.0))
+        mesh = b.add_mesh(S.Mesh(v, idx, np.full(len(idx), rough, np.int32)))
+        c, s_ = np.float32(np.cos(0.7)), np.float32(np.sin(0.7))
+        b.add_instance(mesh, np.array([[c, 0, s_, 0.5], [0, 1.3, 0, 0.6], [-s_, 0, c, 0.9]],
+                                      np.float32))
+        b.add_instance(mesh, np.array([[0.8, 0, 0, -0.4], [0, 0.8, 0, 1.2], [0, 0, 0.8, 0.4]],
+                                      np.float32))
+        return b, mesh, v
+
+    b, mesh, v = build()
+    sc = S.Scene(ctx, b)
+    moved = v.copy()
+    moved[:, 1] += np.float32(0.03) * np.sin(5.0 * moved[:, 2]).astype(np.float32)
+    sc.update_mesh(mesh, moved)
+    req = S.request(32, 32, 4, 5, 3)
+    got = S.render_samples(ctx, sc, req)
+    fresh = S.render_samples(ctx, S.Scene(ctx, build(moved)[0]), req)
+    same = np.all(got == fresh, axis=-1)
+    assert same.mean() > 0.999, same.mean()

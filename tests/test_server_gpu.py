@@ -112,3 +112,22 @@ def test_refit_between_frames(ctx):
     fresh = S.render(ctx, S.Scene(ctx, b2), S.request(32, 32, 4, 5, 1))
     rel = np.abs(f1 - fresh) / (1 + np.abs(fresh))
     assert np.mean(rel < 1e-4) > 0.99
+
+
+def test_refits_faster_than_iterations_do_not_starve_requests(ctx):
+    from lux_b200 import scenes as SC
+    b = SC.heavy_render_scene(32, 32)
+    sc = S.Scene(ctx, b)
+    base = b.meshes[1].vertices.copy()
+    with SV.Server([sc], pool_paths=1 << 15) as srv:
+        ids = [srv.submit(0, S.request(32, 32, 16, 6, k))[0] for k in range(4)]
+        pushed = 0
+        for k in range(200):
+            moved = base.copy()
+            moved[:, 1] += 0.01 * np.sin(3.0 * moved[:, 0] + 0.1 * k)
+            srv.update_mesh(0, 1, moved)
+            pushed += 1
+        srv.wait_all(timeout_s=120)
+        assert all(srv.poll(i) == SV.DONE for i in ids)
+        refits = srv.stats()["refits"]
+        assert 1 <= refits <= pushed
