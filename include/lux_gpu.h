@@ -130,6 +130,33 @@ int lux_bvh_download(lux_ctx* ctx, const lux_bvh* bvh, uint64_t* sorted_codes,
                      float* node_bounds);
 
 /*
+ * No counterpart in the reference.  The Morton half of lux_lbvh_build (primitive boxes,
+ * their union, 30- or 63-bit codes, stable radix sort) written into arrays the caller
+ * owns, with every temporary in one static device array of LUX_STATIC_SORT_SCRATCH_BYTES
+ * that the library holds on each GPU it is loaded on until the process exits.  The call
+ * allocates no device memory.  It is meant for callers that cannot allocate: code whose
+ * device memory is already promised to a fixed budget (a server that admits work by
+ * bytes, where a cudaMalloc could fail or take memory owed to other requests), and
+ * per-frame loops that cannot take the device-wide synchronisation that cudaMalloc and
+ * cudaFree may bring.
+ * prims (n x 9 floats for triangles, n x 6 for boxes), sorted_codes (n uint64; 30-bit
+ * codes widen) and sorted_ids (n) are device pointers on the context's device.  The
+ * results equal lux_bvh_download's sorted_codes and sorted_ids after lux_lbvh_build of
+ * the same input.  n above LUX_STATIC_SORT_MAX_PRIMS is rejected with
+ * LUX_ERR_INVALID_ARGUMENT.
+ * The first call on a device looks up the array's device address for that device; make
+ * that first call before any stream capture.  Each call waits for its stream and reports
+ * device checks.  All calls on one device share the one array and each call overwrites
+ * it: calls whose GPU work overlaps (other streams, contexts or host threads on the same
+ * device) race, so the caller must order them.
+ */
+#define LUX_STATIC_SORT_MAX_PRIMS 1048576
+#define LUX_STATIC_SORT_SCRATCH_BYTES 12845312
+int lux_lbvh_morton_sort_static(lux_ctx* ctx, const float* prims, int32_t n, int32_t kind,
+                                int32_t morton_bits, uint64_t* sorted_codes,
+                                int32_t* sorted_ids);
+
+/*
  * Closest hit of each ray against a triangle BVH.  Visits nodes in the reference's
  * stackless order (bvh/bvh_device.cuh:43-90: left child first, strict t < best), so
  * equal-t ties resolve exactly as the reference GPU path does.  No hit: id -1, t +inf.

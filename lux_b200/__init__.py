@@ -62,6 +62,7 @@ SIGNATURES = {
     "lux_bvh_attach_triangles": (ctypes.c_int, [_P, _P, _P, _I32]),
     "lux_bvh_info": (ctypes.c_int, [_P, _P, _P, _P, _P, _P]),
     "lux_bvh_download": (ctypes.c_int, [_P, _P, _P, _P, _P, _P, _P]),
+    "lux_lbvh_morton_sort_static": (ctypes.c_int, [_P, _P, _I32, _I32, _I32, _P, _P]),
     "lux_trace_closest": (ctypes.c_int, [_P, _P, _P, _I32, _P, _P]),
     "lux_trace_any": (ctypes.c_int, [_P, _P, _P, _I32, _P]),
     "lux_camera_perspective": (ctypes.c_int, [_P, _P, ctypes.c_float, ctypes.c_float,

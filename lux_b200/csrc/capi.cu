@@ -422,6 +422,30 @@ int lux_bvh_info(lux_ctx* ctx, const lux_bvh* bvh, int32_t* n, int32_t* kind,
     return LUX_OK;
 }
 
+// Allocation-free Morton sort: argument checks here, the work and the static array's
+// per-device set-up in lbvh.cu.
+int lux_lbvh_morton_sort_static(lux_ctx* ctx, const float* prims, int32_t n, int32_t kind,
+                                int32_t morton_bits, uint64_t* sorted_codes,
+                                int32_t* sorted_ids) {
+    if (int st = check_ctx(ctx)) return st;
+    if (kind != LUX_PRIM_TRIANGLES && kind != LUX_PRIM_AABBS)
+        return lux::fail(LUX_ERR_INVALID_ARGUMENT, "unknown primitive kind");
+    if (morton_bits != 30 && morton_bits != 63)
+        return lux::fail(LUX_ERR_INVALID_ARGUMENT, "morton_bits must be 30 or 63");
+    if (n > LUX_STATIC_SORT_MAX_PRIMS)
+        return lux::fail(LUX_ERR_INVALID_ARGUMENT,
+                         "lux_lbvh_morton_sort_static: " + std::to_string(n) +
+                             " primitives exceed LUX_STATIC_SORT_MAX_PRIMS (" +
+                             std::to_string(LUX_STATIC_SORT_MAX_PRIMS) + ")");
+    if (n < 0) return lux::fail(LUX_ERR_INVALID_ARGUMENT, "negative primitive count");
+    if (n > 0 && (!is_device_pointer(prims) || !is_device_pointer(sorted_codes) ||
+                  !is_device_pointer(sorted_ids)))
+        return lux::fail(LUX_ERR_INVALID_ARGUMENT,
+                         "lux_lbvh_morton_sort_static takes device pointers only");
+    return lux::lbvh_morton_sort_static(ctx, prims, n, kind, morton_bits, sorted_codes,
+                                        sorted_ids);
+}
+
 int lux_bvh_download(lux_ctx* ctx, const lux_bvh* bvh, uint64_t* sorted_codes,
                      int32_t* sorted_ids, int32_t* node_left, int32_t* node_right,
                      float* node_bounds) {

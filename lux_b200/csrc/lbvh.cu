@@ -18,6 +18,7 @@
 
 #include <algorithm>
 #include <cstdint>
+#include <mutex>
 
 #include "../../include/lux_gpu.h"
 #include "lux_internal.h"
@@ -639,6 +640,153 @@ int lbvh_export(lux_ctx* ctx, const lux_bvh* bvh, uint64_t* codes64, int* left, 
     }
     ctx->launches += 1;
     return cuda_fail(cudaGetLastError(), "k_export");
+}
+
+}  // namespace lux
+
+// ---------------------------------------------------------------- no-allocation sort
+// lux_lbvh_morton_sort_static keeps every temporary of the Morton sort in this array
+// instead of context scratch, so that a call allocates no device memory.  The module
+// holds it on every GPU it is loaded on until the process exits.  Layout in bytes:
+//   [0, 24)      six ordered-int root words (start at all ones: the identity of min)
+//   [64, 68)     device error word (starts at zero)
+//   [256, ...)   digit histograms, kRadix x tiles words (fully rewritten every pass)
+//   then keys    LUX_STATIC_SORT_MAX_PRIMS x 8 bytes: 63-bit alternate keys, or both
+//                30-bit key buffers
+//   then values  LUX_STATIC_SORT_MAX_PRIMS x 4 bytes: alternate primitive ids
+namespace lux {
+namespace {
+
+constexpr int kStaticMaxPrims = LUX_STATIC_SORT_MAX_PRIMS;
+constexpr int kStaticMaxTiles = (kStaticMaxPrims + kSortTile - 1) / kSortTile;
+constexpr size_t kStaticHeaderBytes = 256;
+constexpr size_t kStaticHistBytes = size_t(kRadix) * kStaticMaxTiles * sizeof(unsigned);
+constexpr size_t kStaticKeyBytes = size_t(kStaticMaxPrims) * 8;
+constexpr size_t kStaticValBytes = size_t(kStaticMaxPrims) * 4;
+constexpr size_t kStaticBytes = kStaticHeaderBytes + kStaticHistBytes + kStaticKeyBytes +
+                                kStaticValBytes;
+static_assert(kStaticBytes == LUX_STATIC_SORT_SCRATCH_BYTES, "static sort array size");
+static_assert(kStaticHistBytes % 256 == 0 && kStaticKeyBytes % 256 == 0, "region alignment");
+constexpr int kMaxDevices = 64;
+
+}  // namespace
+}  // namespace lux
+
+static __device__ __align__(256) unsigned char lux_static_sort_scratch[lux::kStaticBytes];
+
+namespace lux {
+namespace {
+
+// Device address of the array on `device`, which must be current.  Looked up once per
+// device (the first call on it), then reused.
+int static_sort_scratch(int device, unsigned char** out) {
+    static std::mutex mu;
+    static unsigned char* address[kMaxDevices] = {};
+    if (device < 0 || device >= kMaxDevices)
+        return fail(LUX_ERR_INVALID_ARGUMENT, "device ordinal out of range for the static sort");
+    std::lock_guard<std::mutex> lk(mu);
+    if (!address[device]) {
+        void* p = nullptr;
+        cudaError_t err = cudaGetSymbolAddress(&p, lux_static_sort_scratch);
+        if (err != cudaSuccess) return cuda_fail(err, "cudaGetSymbolAddress(static sort array)");
+        address[device] = static_cast<unsigned char*>(p);
+    }
+    *out = address[device];
+    return LUX_OK;
+}
+
+__global__ void k_widen_codes(const unsigned* codes, int n, unsigned long long* out) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        out[i] = codes[i];
+}
+
+// Root box, Morton codes and the LSD sort over explicit buffers: the even pass count
+// leaves the result in (keys, vals).
+template <int Kind, typename Key>
+int morton_sort_into(lux_ctx* ctx, const float* prims, int n, Key* keys, Key* keys_alt,
+                     int* vals, int* vals_alt, unsigned* hist, unsigned* root_ord, int* error) {
+    cudaStream_t stream = ctx->stream;
+    k_root_reduce<Kind><<<stride_grid(ctx, n), kThreads, 0, stream>>>(prims, n, root_ord);
+    k_morton<Kind, Key><<<stride_grid(ctx, n), kThreads, 0, stream>>>(prims, n, root_ord, keys);
+    ctx->launches += 2;
+    const int tiles = grid_for(n, kSortTile);
+    int passes = (sizeof(Key) == 4 ? 30 + 7 : 63 + 7) / 8;
+    if (passes & 1) ++passes;
+    Key* kin = keys;
+    Key* kout = keys_alt;
+    int* vin = vals;
+    int* vout = vals_alt;
+    for (int p = 0; p < passes; ++p) {
+        int shift = 8 * p;
+        k_sort_upsweep<Key><<<tiles, kThreads, 0, stream>>>(kin, n, shift, hist, tiles);
+        k_scan_exclusive<<<1, kScanThreads, 0, stream>>>(hist, kRadix * tiles);
+        if (p == 0) {
+            k_sort_downsweep<Key, true><<<tiles, kThreads, 0, stream>>>(
+                kin, vin, kout, vout, n, shift, hist, tiles, error);
+        } else {
+            k_sort_downsweep<Key, false><<<tiles, kThreads, 0, stream>>>(
+                kin, vin, kout, vout, n, shift, hist, tiles, error);
+        }
+        ctx->launches += 3;
+        std::swap(kin, kout);
+        std::swap(vin, vout);
+    }
+    return cuda_fail(cudaGetLastError(), "static morton sort");
+}
+
+}  // namespace
+
+int lbvh_morton_sort_static(lux_ctx* ctx, const float* prims, int n, int kind, int morton_bits,
+                            uint64_t* sorted_codes, int* sorted_ids) {
+    if (n < 0 || n > kStaticMaxPrims)
+        return fail(LUX_ERR_INVALID_ARGUMENT,
+                    "static morton sort: n = " + std::to_string(n) + " is outside 0.." +
+                        std::to_string(kStaticMaxPrims) + " (the static array's limit)");
+    unsigned char* base = nullptr;
+    if (int st = static_sort_scratch(ctx->device, &base)) return st;
+    if (n == 0) return LUX_OK;
+    unsigned* root_ord = reinterpret_cast<unsigned*>(base);
+    int* error = reinterpret_cast<int*>(base + 64);
+    unsigned* hist = reinterpret_cast<unsigned*>(base + kStaticHeaderBytes);
+    unsigned char* keys = base + kStaticHeaderBytes + kStaticHistBytes;
+    int* vals_alt = reinterpret_cast<int*>(keys + kStaticKeyBytes);
+    auto* codes64 = reinterpret_cast<unsigned long long*>(sorted_codes);
+    cudaStream_t stream = ctx->stream;
+    // The array keeps the previous call's contents: reset the words that must start at a
+    // fixed value.  Histograms, keys and values are fully written before they are read.
+    cudaError_t err = cudaMemsetAsync(root_ord, 0xff, 6 * sizeof(unsigned), stream);
+    if (err == cudaSuccess) err = cudaMemsetAsync(error, 0, sizeof(int), stream);
+    if (err != cudaSuccess) return cuda_fail(err, "static sort reset");
+    int st;
+    if (morton_bits == 63) {
+        auto* alt = reinterpret_cast<unsigned long long*>(keys);
+        st = kind == LUX_PRIM_TRIANGLES
+                 ? morton_sort_into<LUX_PRIM_TRIANGLES>(ctx, prims, n, codes64, alt, sorted_ids,
+                                                        vals_alt, hist, root_ord, error)
+                 : morton_sort_into<LUX_PRIM_AABBS>(ctx, prims, n, codes64, alt, sorted_ids,
+                                                    vals_alt, hist, root_ord, error);
+    } else {
+        auto* k30 = reinterpret_cast<unsigned*>(keys);
+        auto* alt = k30 + kStaticMaxPrims;
+        st = kind == LUX_PRIM_TRIANGLES
+                 ? morton_sort_into<LUX_PRIM_TRIANGLES>(ctx, prims, n, k30, alt, sorted_ids,
+                                                        vals_alt, hist, root_ord, error)
+                 : morton_sort_into<LUX_PRIM_AABBS>(ctx, prims, n, k30, alt, sorted_ids,
+                                                    vals_alt, hist, root_ord, error);
+        if (!st) {
+            k_widen_codes<<<stride_grid(ctx, n), kThreads, 0, stream>>>(k30, n, codes64);
+            ctx->launches += 1;
+            st = cuda_fail(cudaGetLastError(), "k_widen_codes");
+        }
+    }
+    if (st) return st;
+    err = cudaStreamSynchronize(stream);
+    if (err != cudaSuccess) return cuda_fail(err, "static morton sort");
+    int word = 0;
+    err = cudaMemcpy(&word, error, sizeof(int), cudaMemcpyDeviceToHost);
+    if (err != cudaSuccess) return cuda_fail(err, "static sort error word");
+    if (word) return fail(LUX_ERR_DEVICE_CHECK, "static morton sort: device check failed");
+    return LUX_OK;
 }
 
 }  // namespace lux

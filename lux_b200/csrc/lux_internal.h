@@ -72,6 +72,10 @@ void lbvh_free(lux_bvh* bvh);
 int lbvh_export(lux_ctx* ctx, const lux_bvh* bvh, uint64_t* codes64, int* left, int* right,
                 float* bounds);
 size_t lbvh_scratch_bytes(int n, int morton_bits);
+// Morton codes and their stable sort into caller device arrays, temporaries in the
+// module's static array (no device allocation; synchronous).
+int lbvh_morton_sort_static(lux_ctx* ctx, const float* prims, int n, int kind, int morton_bits,
+                            uint64_t* sorted_codes, int* sorted_ids);
 int lbvh_attach_triangles(lux_ctx* ctx, lux_bvh* bvh, const float* tris);
 
 // Queries (traverse.cu).  All pointers are device pointers.
