@@ -429,14 +429,36 @@ def _render_setup(local=0):
     return torch, lux_b200.Context(local, stream.cuda_stream), stream
 
 
-def run_cornell(args) -> None:
-    """Config 1: the Cornell box, 256x256, 64 spp, depth 4, power light sampler, seed 1."""
+def _reference_scene_arrays(b):
+    """A SceneBuilder as the reference harness's single-mesh arrays (world triangles)."""
+    tris = b.world_triangles()
+    mids = b.world_material_ids()
+    mats = np.array([[m.type, *m.albedo, *m.emission, m.roughness, m.metallic, m.eta,
+                      m.emission_two_sided] for m in b.materials], np.float32)
+    lights = np.array([[l.kind, *l.vec, *l.value] for l in b.lights], np.float32).reshape(-1, 7)
+    return tris, mids, mats, lights
+
+
+RENDER_CONFIGS = {
+    # name: (width, height, spp, depth, seed, metric, workload)
+    "cornell": (256, 256, 64, 4, 1, "Mrays/s (Cornell 256^2, 64 spp, depth 4)",
+                "Cornell box 256x256, 64 spp, max depth 4, power light sampler, seed 1"),
+    "heavy": (1024, 1024, 256, 8, 1, "Mrays/s (heavy render 1024^2, 256 spp, depth 8)",
+              "Cornell box + displaced icosphere (327,680 tris, GGX 0.3) + glass icosphere "
+              "(5,120 tris, IOR 1.5), 1024x1024, 256 spp, max depth 8, power light sampler, "
+              "seed 1"),
+}
+
+
+def run_render(args, name: str) -> None:
+    """Config 1 (Cornell) or config 3 (heavy render): one lux_render per step."""
     torch, ctx, stream = _render_setup()
     from lux_b200 import scene as S
+    from lux_b200 import scenes as SC
 
-    W = H = 256
-    spp, depth, seed = 64, 4, 1
-    sc = S.Scene(ctx, S.make_cornell_scene(W, H))
+    W, H, spp, depth, seed, metric, workload = RENDER_CONFIGS[name]
+    builder = S.make_cornell_scene(W, H) if name == "cornell" else SC.heavy_render_scene(W, H)
+    sc = S.Scene(ctx, builder)
     req = S.request(W, H, spp, depth, seed)
     film = torch.zeros((H, W, 3), dtype=torch.float32, device="cuda")
     for _ in range(max(args.warmup, 1)):
@@ -452,37 +474,55 @@ def run_cornell(args) -> None:
     e1.record(stream)
     torch.cuda.synchronize()
     clock_info = clocks.stop()
+    launches = ctx.launch_count() - launches0
     ms = e0.elapsed_time(e1) / args.steps
     rays = S.ray_counts(ctx)
     total_rays = sum(rays)
     value = total_rays / (ms * 1e-3) / 1e6
     # e2e: host film through the C ABI (device -> host copy timed).
     host_film = np.zeros((H, W, 3), np.float32)
+    e2e_steps = max(1, min(args.steps, 10 if name == "cornell" else 2))
     t0 = time.perf_counter()
-    for _ in range(max(3, min(args.steps, 10))):
+    for _ in range(e2e_steps):
         S.render(ctx, sc, req, host_film)
-    e2e_ms = (time.perf_counter() - t0) / max(3, min(args.steps, 10)) * 1e3
+    e2e_ms = (time.perf_counter() - t0) / e2e_steps * 1e3
     cpu = None
     if not args.skip_cpu_baseline:
         from oracle.bindings import Ref
         if Ref.available():
             threads = os.cpu_count() or 1
-            rows = 32
+            rows = 32 if name == "cornell" else 2
             t0 = time.perf_counter()
-            Ref().cornell_render(W, H, spp, depth, seed, rows=(0, rows), threads=threads)
-            cpu_s = (time.perf_counter() - t0) * (H / rows)
+            if name == "cornell":
+                Ref().cornell_render(W, H, spp, depth, seed, rows=(0, rows), threads=threads)
+            else:
+                tris, mids, mats, lights = _reference_scene_arrays(builder)
+                cam = np.array([0, 1, 3.35, 0, 1, 0.9, 40.0, np.float32(W) / np.float32(H)],
+                               np.float32)
+                Ref().render_scene(tris, mids, mats, lights, cam, W, H, spp, depth, seed,
+                                   rows=(H // 2, H // 2 + rows), threads=threads)
+            cpu_s = time.perf_counter() - t0
+            if name != "cornell":
+                # Subtract the harness's scene set-up and host BVH build (a call with no rows).
+                t0 = time.perf_counter()
+                Ref().render_scene(tris, mids, mats, lights, cam, W, H, spp, depth, seed,
+                                   rows=(0, 0), threads=threads)
+                cpu_s -= time.perf_counter() - t0
+            cpu_s *= H / rows
             cpu = {"value": total_rays / cpu_s / 1e6, "unit": "Mrays/s", "cores": threads,
                    "kind": "reference",
-                   "sample": f"reference trace_path on rows 0..{rows} of 256 ({threads} threads), "
-                             "scaled; ray count of the same config"}
-    line = {"metric": "Mrays/s (Cornell 256^2, 64 spp, depth 4)", "value": value, "unit": "Mrays/s",
+                   "sample": f"reference trace_path on {rows} of {H} rows ({threads} threads), "
+                             "scaled to the frame; ray count of the same config"
+                             + ("" if name == "cornell" else "; host BVH build excluded")}
+    line = {"metric": metric, "value": value, "unit": "Mrays/s",
             "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic",
-            "config": {"workload": "Cornell box 256x256, 64 spp, max depth 4, power light "
-                                   "sampler, seed 1", "l2": "scene L2/L1 resident"},
+            "config": {"workload": workload,
+                       "l2": "scene L2/L1 resident" if name == "cornell" else
+                             "path state 4M paths x 192 B > L2"},
             "rays": {"camera_extension": rays[0], "shadow_segments": rays[1]},
-            "clocks": clock_info, "gpu_launches": ctx.launch_count() - launches0,
+            "clocks": clock_info, "gpu_launches": launches,
             "e2e": {"value": total_rays / (e2e_ms * 1e-3) / 1e6, "unit": "Mrays/s",
                     "h2d_bytes_per_step": 0, "d2h_bytes_per_step": W * H * 12,
                     "ms_per_step": e2e_ms},
@@ -617,7 +657,8 @@ def run_serving(args) -> None:
             start = max(a, free_at)
             free_at = start + sv
             fifo_lat.append(free_at - a)
-        with SV.Server(scenes, pool_paths=args.pool) as srv:
+        with SV.Server(scenes, pool_paths=args.pool,
+                       memory_budget_bytes=int(args.budget_gb * 1e9)) as srv:
             warm, _ = srv.submit(0, S.request(32, 32, 2, 2, 1))
             srv.wait(warm)
             base_stats = srv.stats()
@@ -662,7 +703,7 @@ def run_serving(args) -> None:
             "config": {"workload": "Poisson arrivals over the 4 resident scenes; requests from the "
                                    "batched distribution scaled by %g; displaced icosphere refit "
                                    "every 1/30 s" % args.request_scale,
-                       "pool_paths": args.pool},
+                       "pool_paths": args.pool, "memory_budget_gb": args.budget_gb},
             "sweep": results}
     print(json.dumps(line))
 
@@ -670,10 +711,12 @@ def run_serving(args) -> None:
 def main():
     global N_TRIS, N_RAYS, N_QUERIES, WORKLOAD
     ap = argparse.ArgumentParser()
-    ap.add_argument("--config", default="lbvh", choices=["lbvh", "cornell", "batched", "serving"],
-                    help="lbvh: the LBVH microbench (default); cornell: config 1; batched: "
-                         "config 4; serving: config 5")
+    ap.add_argument("--config", default="lbvh", choices=["lbvh", "cornell", "heavy", "batched", "serving"],
+                    help="lbvh: the LBVH microbench (default); cornell: config 1; heavy: config 3; "
+                         "batched: config 4; serving: config 5")
     ap.add_argument("--rates", default="10,50,100,200,500")
+    ap.add_argument("--budget-gb", type=float, default=120.0,
+                    help="serving: device-memory admission budget for queues and films")
     ap.add_argument("--request-scale", type=float, default=0.25,
                     help="serving: scale of request resolution and spp")
     ap.add_argument("--requests", type=int, default=64)
@@ -698,8 +741,8 @@ def main():
         N_TRIS, N_RAYS, N_QUERIES = args.tris, args.rays, args.queries
         WORKLOAD = (f"LBVH microbench generator at reduced size (profiling case): {N_TRIS} "
                     f"triangles, {N_RAYS} rays, {N_QUERIES} query boxes, seed 7")
-    if args.config == "cornell" and args.impl == "lux":
-        run_cornell(args)
+    if args.config in ("cornell", "heavy") and args.impl == "lux":
+        run_render(args, args.config)
     elif args.config == "batched":
         run_batched(args)
     elif args.config == "serving":

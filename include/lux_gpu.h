@@ -130,6 +130,26 @@ int lux_bvh_download(lux_ctx* ctx, const lux_bvh* bvh, uint64_t* sorted_codes,
                      float* node_bounds);
 
 /*
+ * Structure check of a built BVH: sorted ids form a permutation, the root box is the
+ * union of the leaf boxes, codes are sorted, every parent link matches its child slot
+ * and a traversal from the root reaches every node exactly once.  *valid = 1 or 0; on 0,
+ * `message` (capacity bytes, may be NULL) receives the reason.  Returns LUX_OK unless the
+ * check itself could not run.  Replaces validate_gpu_bvh_structure
+ * (bvh/gpu_bvh.cuh:53; bvh/gpu_bvh.cu:667-829), with the same messages.
+ */
+int lux_bvh_validate_structure(lux_ctx* ctx, const lux_bvh* bvh, int32_t* valid, char* message,
+                               int32_t message_capacity);
+
+/*
+ * The structure check, then: the BVH holds each of the n primitives (host or device
+ * array, n x 9 floats for triangles, n x 6 for boxes) exactly once, each leaf box within
+ * 1e-4 of its primitive's box.  Replaces validate_gpu_bvh_matches_primitives
+ * (bvh/gpu_bvh.cuh:54-56; bvh/gpu_bvh.cu:831-891).
+ */
+int lux_bvh_validate_primitives(lux_ctx* ctx, const lux_bvh* bvh, const float* prims, int32_t n,
+                                int32_t* valid, char* message, int32_t message_capacity);
+
+/*
  * No counterpart in the reference.  The Morton half of lux_lbvh_build (primitive boxes,
  * their union, 30- or 63-bit codes, stable radix sort) written into arrays the caller
  * owns, with every temporary in one static device array of LUX_STATIC_SORT_SCRATCH_BYTES

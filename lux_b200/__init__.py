@@ -62,6 +62,8 @@ SIGNATURES = {
     "lux_bvh_attach_triangles": (ctypes.c_int, [_P, _P, _P, _I32]),
     "lux_bvh_info": (ctypes.c_int, [_P, _P, _P, _P, _P, _P]),
     "lux_bvh_download": (ctypes.c_int, [_P, _P, _P, _P, _P, _P, _P]),
+    "lux_bvh_validate_structure": (ctypes.c_int, [_P, _P, _P, _P, _I32]),
+    "lux_bvh_validate_primitives": (ctypes.c_int, [_P, _P, _P, _I32, _P, _P, _I32]),
     "lux_lbvh_morton_sort_static": (ctypes.c_int, [_P, _P, _I32, _I32, _I32, _P, _P]),
     "lux_trace_closest": (ctypes.c_int, [_P, _P, _P, _I32, _P, _P]),
     "lux_trace_any": (ctypes.c_int, [_P, _P, _P, _I32, _P]),
@@ -250,6 +252,20 @@ class Bvh:
                                                   ids.ctypes.data, left.ctypes.data,
                                                   right.ctypes.data, bounds.ctypes.data))
         return HostTree(codes, ids, left, right, bounds)
+
+    def validate(self, prims=None) -> tuple[bool, str]:
+        """validate_gpu_bvh_structure / validate_gpu_bvh_matches_primitives: (ok, message)."""
+        valid = ctypes.c_int32()
+        msg = ctypes.create_string_buffer(256)
+        if prims is None:
+            _check(self.ctx._lib.lux_bvh_validate_structure(self.ctx._h, self._h,
+                                                            ctypes.byref(valid), msg, 256))
+        else:
+            per = 9 if self.kind == PRIM_TRIANGLES else 6
+            _check(self.ctx._lib.lux_bvh_validate_primitives(
+                self.ctx._h, self._h, _ptr(prims), _count(prims, per), ctypes.byref(valid),
+                msg, 256))
+        return bool(valid.value), msg.value.decode()
 
     def trace_closest(self, rays, hit_id=None, hit_t=None):
         nrays = _count(rays, 8)

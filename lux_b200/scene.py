@@ -183,6 +183,15 @@ class SceneBuilder:
             out.append(w.reshape(-1, 9).astype(np.float32))
         return np.concatenate(out) if out else np.zeros((0, 9), np.float32)
 
+    def world_material_ids(self) -> np.ndarray:
+        """Material id of each scene triangle, in world_triangles order."""
+        out = []
+        for mesh_id, _, override in self.instances:
+            mesh = self.default_mesh() if mesh_id == self._default_mesh else self.meshes[mesh_id]
+            ids = np.asarray(mesh.material_ids, np.int32)
+            out.append(np.full(len(ids), override, np.int32) if override >= 0 else ids)
+        return np.concatenate(out) if out else np.zeros(0, np.int32)
+
 
 class Scene:
     """A lux_scene handle resident on the context's device."""

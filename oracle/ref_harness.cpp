@@ -384,11 +384,25 @@ int ref_render_scene(const float* tris, int ntri, const int32_t* mids, const flo
                                            f[10] != 0 ? EmissionSidedness::DoubleSided
                                                       : EmissionSidedness::SingleSided));
     }
-    for (int t = 0; t < ntri; ++t) {
-        const float* v = tris + size_t(t) * 9;
-        add_triangle(scene, Triangle{vec3(v[0], v[1], v[2]), vec3(v[3], v[4], v[5]),
-                                     vec3(v[6], v[7], v[8])},
-                     mids[t]);
+    // One append_indexed_mesh (scene/scene_edit.h:98-163) instead of add_triangle per
+    // triangle: the same default-mesh data (three vertices per triangle, zero normals and
+    // uvs), but one geometry-cache refresh instead of one per triangle, which is
+    // quadratic in the triangle count.
+    {
+        std::vector<vec3> vertices;
+        std::vector<TriangleIndices> indices;
+        std::vector<int> material_ids(mids, mids + ntri);
+        vertices.reserve(size_t(ntri) * 3);
+        indices.reserve(ntri);
+        for (int t = 0; t < ntri; ++t) {
+            const float* v = tris + size_t(t) * 9;
+            uint32_t first = static_cast<uint32_t>(vertices.size());
+            vertices.push_back(vec3(v[0], v[1], v[2]));
+            vertices.push_back(vec3(v[3], v[4], v[5]));
+            vertices.push_back(vec3(v[6], v[7], v[8]));
+            indices.push_back(TriangleIndices{first, first + 1, first + 2});
+        }
+        if (ntri > 0) append_indexed_mesh(scene, vertices, {}, {}, indices, material_ids);
     }
     for (int l = 0; l < nlights; ++l) {
         const float* f = lights + size_t(l) * 7;

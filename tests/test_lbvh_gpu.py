@@ -256,3 +256,31 @@ def test_full_size_microbench_properties(ctx):
     assert np.percentile(dist, 99) < 1e-5
     aid = bvh.trace_any(rays)
     assert np.array_equal(aid >= 0, hit)
+
+
+@pytest.mark.parametrize("n,bits", [(1, 30), (2, 63), (1000, 30), (20000, 63)])
+def test_validators_accept_built_trees(ctx, n, bits):
+    tris = W.soup_triangles(n, 13)
+    bvh = ctx.build_lbvh(tris, lux_b200.PRIM_TRIANGLES, bits)
+    assert bvh.validate() == (True, "")
+    assert bvh.validate(tris) == (True, "")
+    boxes = W.query_boxes(n, 14)
+    bb = ctx.build_lbvh(boxes, lux_b200.PRIM_AABBS, bits)
+    assert bb.validate(boxes) == (True, "")
+
+
+def test_validators_report_the_reference_messages(ctx):
+    tris = W.soup_triangles(4096, 15)
+    bvh = ctx.build_lbvh(tris, lux_b200.PRIM_TRIANGLES, 30)
+    moved = tris.copy()
+    moved[17, :3] += np.float32(0.25)
+    assert bvh.validate(moved) == (False, "BVH primitive bounds do not match scene primitive")
+    assert bvh.validate(tris[:4095]) == (
+        False, "BVH primitive count does not match scene primitive count")
+    bvh.refit(moved)
+    assert bvh.validate(moved) == (True, "")
+    empty = ctx.build_lbvh(np.zeros((0, 9), np.float32), lux_b200.PRIM_TRIANGLES, 30)
+    assert empty.validate() == (False, "BVH is not valid")
+    assert empty.validate(np.zeros((0, 9), np.float32)) == (True, "")
+    assert bvh.validate(np.zeros((0, 9), np.float32)) == (
+        False, "BVH contains primitives for an empty scene")

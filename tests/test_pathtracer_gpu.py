@@ -41,7 +41,7 @@ def _z_fraction(gpu, ref):
 
 def _ref_arrays(b: S.SceneBuilder):
     tris = b.world_triangles()
-    mids = np.asarray(b._mids, np.int32)
+    mids = b.world_material_ids()
     mats = np.array([[m.type, *m.albedo, *m.emission, m.roughness, m.metallic, m.eta,
                       m.emission_two_sided] for m in b.materials], np.float32)
     lights = np.array([[l.kind, *l.vec, *l.value] for l in b.lights], np.float32).reshape(-1, 7)
