@@ -735,7 +735,7 @@ def main():
     ap.add_argument("--queries", type=int, default=N_QUERIES)
     ap.add_argument("--trace-variant", type=int, default=0,
                     help="0 auto, 1 one thread per ray, 2 persistent (tunable)")
-    ap.add_argument("--trace-budget", type=int, default=32)
+    ap.add_argument("--trace-budget", type=int, default=16)
     args = ap.parse_args()
     if (args.tris, args.rays, args.queries) != (N_TRIS, N_RAYS, N_QUERIES):
         N_TRIS, N_RAYS, N_QUERIES = args.tris, args.rays, args.queries

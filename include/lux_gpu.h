@@ -69,7 +69,9 @@ int lux_abi_version(void);
 int lux_ctx_launch_count(lux_ctx* ctx, int64_t* count);
 
 /* Tunables (set by the autotuner or the caller; results never depend on them).
- *   LUX_OPT_TRACE_VARIANT  0 auto, 1 one thread per ray, 2 persistent warps with refill
+ *   LUX_OPT_TRACE_VARIANT  0 auto (4), 1 one thread per ray, 2 persistent warps with
+ *                          refill, 3 one thread per ray over 4-wide nodes, 4 persistent
+ *                          warps with refill over 4-wide nodes
  *   LUX_OPT_TRACE_BUDGET   traversal steps per refill round of the persistent kernel
  *   LUX_OPT_RENDER_BATCH   paths in flight per wavefront batch (device memory ~200 B each) */
 enum lux_option { LUX_OPT_TRACE_VARIANT = 1, LUX_OPT_TRACE_BUDGET = 2, LUX_OPT_RENDER_BATCH = 3 };

@@ -237,7 +237,7 @@ int lux_ctx_set_option(lux_ctx* ctx, int32_t option, int64_t value) {
     if (!ctx) return lux::fail(LUX_ERR_INVALID_ARGUMENT, "null context");
     switch (option) {
         case LUX_OPT_TRACE_VARIANT:
-            if (value < 0 || value > 2) return lux::fail(LUX_ERR_INVALID_ARGUMENT, "trace variant 0..2");
+            if (value < 0 || value > 4) return lux::fail(LUX_ERR_INVALID_ARGUMENT, "trace variant 0..4");
             ctx->trace_variant = static_cast<int>(value);
             return LUX_OK;
         case LUX_OPT_TRACE_BUDGET:

@@ -559,7 +559,10 @@ int lbvh_alloc(lux_ctx* ctx, lux_bvh* bvh) {
 
 void lbvh_free(lux_bvh* bvh) {
     void* ptrs[] = {bvh->nodes, bvh->tris, bvh->sorted_ids, bvh->leaf_parent, bvh->node_parent,
-                    bvh->flags, bvh->codes, bvh->root};
+                    bvh->flags, bvh->codes, bvh->root, bvh->wide};
+    bvh->wide = nullptr;
+    bvh->wide_capacity = 0;
+    bvh->wide_current = false;
     for (void* p : ptrs) {
         if (p) cudaFree(p);
     }
@@ -574,6 +577,7 @@ void lbvh_free(lux_bvh* bvh) {
 }
 
 int lbvh_build(lux_ctx* ctx, lux_bvh* bvh, const float* prims) {
+    bvh->wide_current = false;
     if (bvh->n <= 0) return LUX_OK;
     bool wide = bvh->morton_bits == 63;
     if (bvh->kind == LUX_PRIM_TRIANGLES) {
@@ -619,9 +623,137 @@ int lbvh_attach_triangles(lux_ctx* ctx, lux_bvh* bvh, const float* tris) {
 }
 
 int lbvh_refit(lux_ctx* ctx, lux_bvh* bvh, const float* prims) {
+    bvh->wide_current = false;
     if (bvh->n <= 0) return LUX_OK;
     return bvh->kind == LUX_PRIM_TRIANGLES ? climb<LUX_PRIM_TRIANGLES>(ctx, bvh, prims)
                                            : climb<LUX_PRIM_AABBS>(ctx, bvh, prims);
+}
+
+namespace {
+
+struct WideSlots {
+    box3 box[4];
+    int ch[4];
+    int count;
+    LUX_D void add(int handle, const box3& b) {
+        if (count >= 4) return;
+        box[count] = b;
+        ch[count] = handle;
+        ++count;
+    }
+};
+
+// Biased exponent of an axis grid: from 2^e >= extent / 255, raised until the top grid
+// point decodes at or above hi.
+LUX_D unsigned wide_exponent(float origin, float hi) {
+    float extent = sub(hi, origin);
+    int e = -126;
+    if (extent > 0.0f) {
+        int ex;
+        frexpf(extent / 255.0f, &ex);
+        e = max(ex, -126);
+    }
+    while (e < 127 && wide_decode(origin, 255u, wide_scale(static_cast<unsigned>(e + 127))) < hi)
+        ++e;
+    return static_cast<unsigned>(e + 127);
+}
+
+// Outward-rounded grid coordinates of [lo, hi]: the largest q_lo whose decode is <= lo
+// and the smallest q_hi whose decode is >= hi.
+LUX_D void wide_quantize(float origin, unsigned biased, float lo, float hi, unsigned& qlo,
+                         unsigned& qhi) {
+    const float scale = wide_scale(biased);
+    const float inv = wide_scale(254u - biased);  // 2^-e, exact for the exponents used
+    const float fa = floorf(mul(sub(lo, origin), inv));
+    int a = fa >= 255.0f ? 255 : (fa > 0.0f ? static_cast<int>(fa) : 0);
+    while (a > 0 && wide_decode(origin, static_cast<unsigned>(a), scale) > lo) --a;
+    const float fb = ceilf(mul(sub(hi, origin), inv));
+    int b = fb >= 255.0f ? 255 : (fb > 0.0f ? static_cast<int>(fb) : 0);
+    while (b < 255 && wide_decode(origin, static_cast<unsigned>(b), scale) < hi) ++b;
+    qlo = static_cast<unsigned>(a);
+    qhi = static_cast<unsigned>(b);
+}
+
+// Wide node i from binary node i and its internal children (see WideNode).
+__global__ void __launch_bounds__(kThreads) k_widen(const BvhNode* nodes, int n,
+                                                    WideNode* wide, int* error) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n - 1) return;
+    WideSlots s;
+    s.count = 0;
+    BvhNode nd = load_node(nodes, i);
+#pragma unroll
+    for (int side = 0; side < 2; ++side) {
+        int h = side ? nd.ch.y : nd.ch.x;
+        if (h >= n - 1) {  // cannot happen for a consistent hierarchy
+            atomicOr(error, kErrLoopBound);
+            continue;
+        }
+        if (h >= 0) {
+            BvhNode cn = load_node(nodes, h);
+            s.add(cn.ch.x, node_left_box(cn));
+            s.add(cn.ch.y, node_right_box(cn));
+        } else {
+            s.add(h, side ? node_right_box(nd) : node_left_box(nd));
+        }
+    }
+    box3 u = box_union(node_left_box(nd), node_right_box(nd));
+    float o[3] = {u.lo.x, u.lo.y, u.lo.z};
+    float top[3] = {u.hi.x, u.hi.y, u.hi.z};
+    bool finite = true;
+    for (int a = 0; a < 3; ++a) finite = finite && isfinite(o[a]) && isfinite(top[a]);
+    unsigned ebits[3] = {127u, 127u, 127u};
+    unsigned lo_w[3] = {0, 0, 0}, hi_w[3] = {0, 0, 0};
+    if (finite) {
+        for (int a = 0; a < 3; ++a) ebits[a] = wide_exponent(o[a], top[a]);
+        for (int c = 0; c < s.count; ++c) {
+            float lo[3] = {s.box[c].lo.x, s.box[c].lo.y, s.box[c].lo.z};
+            float hi[3] = {s.box[c].hi.x, s.box[c].hi.y, s.box[c].hi.z};
+            for (int a = 0; a < 3; ++a) {
+                unsigned ql, qh;
+                wide_quantize(o[a], ebits[a], lo[a], hi[a], ql, qh);
+                lo_w[a] |= ql << (8 * c);
+                hi_w[a] |= qh << (8 * c);
+            }
+        }
+    }
+    unsigned meta = ebits[0] | (ebits[1] << 8) | (ebits[2] << 16) |
+                    (static_cast<unsigned>(s.count) << 24) | (finite ? 0u : kWideUnbounded);
+    int ch[4] = {0, 0, 0, 0};
+    for (int c = 0; c < s.count; ++c) ch[c] = s.ch[c];
+    WideNode w;
+    w.q0 = make_float4(o[0], o[1], o[2], __uint_as_float(meta));
+    w.q1 = make_float4(__uint_as_float(lo_w[0]), __uint_as_float(lo_w[1]),
+                       __uint_as_float(lo_w[2]), __uint_as_float(hi_w[0]));
+    w.q2 = make_float4(__uint_as_float(hi_w[1]), __uint_as_float(hi_w[2]), __int_as_float(ch[0]),
+                       __int_as_float(ch[1]));
+    w.q3 = make_float4(__int_as_float(ch[2]), __int_as_float(ch[3]), 0.0f, 0.0f);
+    wide[i] = w;
+}
+
+}  // namespace
+
+int lbvh_ensure_wide(lux_ctx* ctx, lux_bvh* bvh) {
+    if (bvh->wide_current || bvh->n <= 1) return LUX_OK;
+    int need = std::max(bvh->capacity - 1, 1);
+    if (bvh->wide_capacity < need) {
+        if (bvh->wide) cudaFree(bvh->wide);
+        bvh->wide = nullptr;
+        bvh->wide_capacity = 0;
+        cudaError_t err = cudaMalloc(&bvh->wide, sizeof(WideNode) * size_t(need));
+        if (err != cudaSuccess) {
+            cudaGetLastError();
+            bvh->wide = nullptr;
+            return fail(LUX_ERR_OUT_OF_MEMORY, "wide node allocation failed");
+        }
+        bvh->wide_capacity = need;
+    }
+    k_widen<<<grid_for(bvh->n - 1), kThreads, 0, ctx->stream>>>(bvh->nodes, bvh->n, bvh->wide,
+                                                                 ctx->d_error);
+    ctx->launches += 1;
+    int st = cuda_fail(cudaGetLastError(), "k_widen");
+    if (!st) bvh->wide_current = true;
+    return st;
 }
 
 int lbvh_export(lux_ctx* ctx, const lux_bvh* bvh, uint64_t* codes64, int* left, int* right,

@@ -37,9 +37,36 @@ LUX_HD box3 node_right_box(const BvhNode& n) {
     return box3{make_f3(n.b.z, n.b.w, n.c.x), make_f3(n.c.y, n.c.z, n.c.w)};
 }
 
+// 4-wide node of binary internal node i: its grandchildren in left-first order, a leaf
+// child standing for itself, so 2 to 4 children.  One is built for every internal node;
+// a walk from the root enters only those at even binary depth.  Child boxes are stored
+// quantised to 8 bits per plane on a per-axis power-of-two grid anchored at the node's
+// lower corner, rounded outward, so each decoded box contains the exact one; the node is
+// 64 bytes.  Decoded boxes only steer the walk: a leaf is accepted by the exact test of
+// its own box (the slot of its binary parent) when the walk reaches it.
+//   q0 = origin.xyz, meta (bits 0-23: biased exponents x, y, z; 24-26: child count;
+//        27: unbounded, every child passes)
+//   q1 = lo.x, lo.y, lo.z, hi.x bytes of children 0..3 (byte c of each word: child c)
+//   q2 = hi.y, hi.z bytes, child handles 0, 1
+//   q3 = child handles 2, 3, 0, 0
+struct alignas(16) WideNode {
+    float4 q0, q1, q2, q3;
+};
+static_assert(sizeof(WideNode) == 64, "one wide node is one 64-byte record");
+
+constexpr unsigned kWideUnbounded = 1u << 27;
+
+LUX_D float wide_scale(unsigned biased) { return __int_as_float(static_cast<int>(biased) << 23); }
+
+// Decoded coordinate origin + q * 2^e (q * 2^e is exact, so the sum rounds once).
+LUX_D float wide_decode(float origin, unsigned q, float scale) {
+    return add(mul(static_cast<float>(q), scale), origin);
+}
+
 // Non-owning view passed by value into kernels.
 struct BvhView {
     const BvhNode* nodes = nullptr;     // n - 1 internal nodes
+    const WideNode* wide = nullptr;     // n - 1 wide nodes (ray queries), indexed as nodes
     const TriRecord* tris = nullptr;    // n triangles in sorted order (triangle BVHs)
     const int* sorted_ids = nullptr;    // n: input index of sorted leaf k
     const int* leaf_parent = nullptr;   // n: (parent << 1) | slot, -1 for a lone leaf

@@ -16,8 +16,8 @@ struct lux_ctx {
     int64_t launches = 0;            // kernels launched through this context
     unsigned* d_counter = nullptr;   // device work counter (persistent kernels)
     // Tunables (lux_ctx_set_option).
-    int trace_variant = 0;           // lux::kTraceAuto / kTraceStatic / kTracePersistent
-    int trace_budget = 32;           // traversal steps per refill round
+    int trace_variant = 0;           // lux::kTrace* (auto: wide persistent)
+    int trace_budget = 16;           // traversal steps per refill round
     int render_batch = 1 << 22;      // paths in flight per wavefront batch
     void* render_runtime = nullptr;  // wavefront buffers, grown on demand
     // Growable device scratch, reused across calls on this context.
@@ -43,9 +43,13 @@ struct lux_bvh {
     unsigned* flags = nullptr;          // n - 1, zero between passes
     void* codes = nullptr;              // n sorted codes (uint32 or uint64)
     float* root = nullptr;              // 6
+    lux::WideNode* wide = nullptr;      // capacity - 1, built on demand for ray queries
+    bool wide_current = false;          // wide matches nodes (cleared by build/refit)
+    int wide_capacity = 0;              // wide nodes allocated
     lux::BvhView view() const {
         lux::BvhView v;
         v.nodes = nodes;
+        v.wide = wide;
         v.tris = tris;
         v.sorted_ids = sorted_ids;
         v.leaf_parent = leaf_parent;
@@ -57,7 +61,13 @@ struct lux_bvh {
 
 namespace lux {
 
-enum : int { kTraceAuto = 0, kTraceStatic = 1, kTracePersistent = 2 };
+enum : int {
+    kTraceAuto = 0,
+    kTraceStatic = 1,
+    kTracePersistent = 2,
+    kTraceWide = 3,
+    kTraceWidePersistent = 4
+};
 
 // Status helpers (defined in capi.cu).
 int fail(int status, const std::string& message);
@@ -68,6 +78,9 @@ int ensure_scratch(lux_ctx* ctx, size_t bytes);
 int lbvh_alloc(lux_ctx* ctx, lux_bvh* bvh);
 int lbvh_build(lux_ctx* ctx, lux_bvh* bvh, const float* prims);
 int lbvh_refit(lux_ctx* ctx, lux_bvh* bvh, const float* prims);
+// Brings the 4-wide nodes up to date with the binary nodes (stream-ordered; allocates
+// them on first use).  Every ray query calls it; builds and refits mark them stale.
+int lbvh_ensure_wide(lux_ctx* ctx, lux_bvh* bvh);
 void lbvh_free(lux_bvh* bvh);
 int lbvh_export(lux_ctx* ctx, const lux_bvh* bvh, uint64_t* codes64, int* left, int* right,
                 float* bounds);

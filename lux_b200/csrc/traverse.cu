@@ -14,8 +14,11 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include "../../include/lux_gpu.h"
 #include "lux_internal.h"
+#include "lux_wide.cuh"
 
 namespace lux {
 namespace {
@@ -127,6 +130,40 @@ __global__ void __launch_bounds__(kTraceThreads) k_trace(BvhView bvh, const floa
     if (h.k >= 0) id = __float_as_int(__ldg(reinterpret_cast<const float*>(bvh.tris + h.k) + 3));
     hit_id[i] = id;
     if (hit_t) hit_t[i] = h.k >= 0 ? h.t : INFINITY;
+}
+
+// One ray per thread over the 4-wide nodes (lux_wide.cuh): the same verdicts as
+// trace_one with half the dependent node fetches.
+template <bool AnyHit>
+__global__ void __launch_bounds__(kTraceThreads) k_trace_wide(BvhView bvh, const float4* rays,
+                                                              int nrays, int* hit_id,
+                                                              float* hit_t, int* error) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nrays) return;
+    const ray3 ray = load_ray(rays, i);
+    const slab_ray sr = make_slab_ray(ray);
+    float best_t = ray.tmax;
+    int best_k = -1;
+    bool ok = wide_walk(bvh, sr, best_t, error, [&](int k, float& bt) -> bool {
+        const float4* tp = reinterpret_cast<const float4*>(bvh.tris + k);
+        float4 p0 = __ldg(tp);
+        float4 p1 = __ldg(tp + 1);
+        float4 p2 = __ldg(tp + 2);
+        float t, u, v;
+        if (moller_trumbore(ray.o, ray.d, make_f3(p0.x, p0.y, p0.z), make_f3(p1.x, p1.y, p1.z),
+                            make_f3(p2.x, p2.y, p2.z), t, u, v)
+            && t > ray.tmin && t < bt) {
+            best_k = k;
+            bt = t;
+            return AnyHit;
+        }
+        return false;
+    });
+    if (!ok) best_k = -1;
+    int id = -1;
+    if (best_k >= 0) id = __float_as_int(__ldg(reinterpret_cast<const float*>(bvh.tris + best_k) + 3));
+    hit_id[i] = id;
+    if (hit_t) hit_t[i] = best_k >= 0 ? best_t : INFINITY;
 }
 
 // Persistent traversal: each warp keeps 32 rays in flight and advances each by at most
@@ -280,6 +317,142 @@ __global__ void __launch_bounds__(kTraceThreads) k_trace_persistent(
     }
 }
 
+// Persistent warps with refill (as k_trace_persistent) over the 4-wide nodes: a step is
+// one wide-node fetch (four child boxes) or one triangle test, followed by the pops it
+// enables.  Decisions are those of wide_walk, step for step.
+// 8 resident blocks per SM (at most 64 registers): occupancy hides the node-load latency
+// that bounds this kernel, and the cap costs no spills.
+template <bool AnyHit>
+__global__ void __launch_bounds__(kTraceThreads, 8) k_trace_wide_persistent(
+        BvhView bvh, const float4* rays, int nrays, int* hit_id, float* hit_t,
+        unsigned* ray_counter, int budget, int* error) {
+    const unsigned lane = threadIdx.x & 31;
+    const unsigned lt = lanemask_lt_u();
+    const box3 root = load_root(bvh.root);
+    const long long bound = 2ll * bvh.n + 64;
+
+    int ray_idx = -1;   // >= 0 active ray, -1 needs a ray, -2 no rays left
+    ray3 ray;
+    slab_ray sr;
+    octant_ray orr;
+    float best_t = 0.0f;
+    int best_k = -1;
+    int cur = 0;
+    int sp = 0;
+    long long steps = 0;
+    bool root_missed = false;
+    int stack_h[kWideStack];
+    float stack_t[kWideStack];
+
+    for (;;) {
+        bool need = ray_idx == -1;
+        unsigned need_mask = __ballot_sync(0xffffffffu, need);
+        if (need_mask) {
+            int leader = __ffs(need_mask) - 1;
+            unsigned base = 0;
+            if (lane == leader) base = atomicAdd(ray_counter, __popc(need_mask));
+            base = __shfl_sync(0xffffffffu, base, leader);
+            if (need) {
+                unsigned idx = base + __popc(need_mask & lt);
+                if (idx >= static_cast<unsigned>(nrays)) {
+                    ray_idx = -2;
+                } else {
+                    ray_idx = static_cast<int>(idx);
+                    ray = load_ray(rays, ray_idx);
+                    sr = make_slab_ray(ray);
+                    orr = make_octant_ray(sr);
+                    best_t = ray.tmax;
+                    best_k = -1;
+                    sp = 0;
+                    steps = 0;
+                    float tn;
+                    root_missed = bvh.n <= 0 || !slab_hit(sr, root, best_t, tn);
+                    cur = bvh.n == 1 ? ~0 : 0;
+                }
+            }
+        }
+        if (__all_sync(0xffffffffu, ray_idx == -2)) break;
+
+        bool done = false;
+        if (ray_idx >= 0) {
+            if (root_missed) done = true;
+            for (int s = 0; s < budget && !done; ++s) {
+                if (++steps > bound || cur >= bvh.n - 1 || ~cur >= bvh.n) {
+                    atomicOr(error, kErrLoopBound);
+                    best_k = -1;
+                    best_t = ray.tmax;
+                    done = true;
+                    break;
+                }
+                bool pop = true;
+                if (cur >= 0) {
+                    const WideNode w = load_wide(bvh.wide, cur);
+                    float t[4];
+                    unsigned m = wide_test(w, sr, orr, best_t, t);
+                    if (m) {
+                        const int f = __ffs(m) - 1;
+                        if (sp + __popc(m) - 1 > kWideStack) {
+                            atomicOr(error, kErrStackOverflow);
+                            best_k = -1;
+                            best_t = ray.tmax;
+                            done = true;
+                            break;
+                        }
+#pragma unroll
+                        for (int c = 3; c >= 1; --c) {
+                            if (c > f && ((m >> c) & 1u)) {
+                                stack_h[sp] = wide_ref(w, c);
+                                stack_t[sp] = t[c];
+                                ++sp;
+                            }
+                        }
+                        cur = wide_ref(w, f);
+                        pop = false;
+                    }
+                } else if (leaf_hit(bvh, ~cur, sr, orr, best_t)) {
+                    int k = ~cur;
+                    const float4* tp = reinterpret_cast<const float4*>(bvh.tris + k);
+                    float4 p0 = __ldg(tp);
+                    float4 p1 = __ldg(tp + 1);
+                    float4 p2 = __ldg(tp + 2);
+                    float t, u, v;
+                    if (moller_trumbore(ray.o, ray.d, make_f3(p0.x, p0.y, p0.z),
+                                        make_f3(p1.x, p1.y, p1.z), make_f3(p2.x, p2.y, p2.z),
+                                        t, u, v)
+                        && t > ray.tmin && t < best_t) {
+                        best_k = k;
+                        best_t = t;
+                        if (AnyHit) {
+                            done = true;
+                            break;
+                        }
+                    }
+                }
+                if (pop) {
+                    bool resumed = false;
+                    while (sp > 0) {
+                        --sp;
+                        if (!(stack_t[sp] > best_t)) {
+                            cur = stack_h[sp];
+                            resumed = true;
+                            break;
+                        }
+                    }
+                    if (!resumed) done = true;
+                }
+            }
+        }
+        if (done) {
+            int id = -1;
+            if (best_k >= 0)
+                id = __float_as_int(__ldg(reinterpret_cast<const float*>(bvh.tris + best_k) + 3));
+            hit_id[ray_idx] = id;
+            if (hit_t) hit_t[ray_idx] = best_k >= 0 ? best_t : INFINITY;
+            ray_idx = -1;
+        }
+    }
+}
+
 // Totals of box and triangle tests over all rays (one atomic pair per warp).
 __global__ void __launch_bounds__(kTraceThreads) k_trace_stats(BvhView bvh, const float4* rays,
                                                                int nrays,
@@ -386,6 +559,32 @@ int launch_trace(lux_ctx* ctx, const lux_bvh* bvh, const float* rays, int nrays,
                  float* hit_t) {
     if (nrays <= 0) return LUX_OK;
     const float4* r4 = reinterpret_cast<const float4*>(rays);
+    if (ctx->trace_variant == kTraceWidePersistent || ctx->trace_variant == kTraceAuto) {
+        if (int st = lbvh_ensure_wide(ctx, const_cast<lux_bvh*>(bvh))) return st;
+        static int blocks_per_sm[2] = {0, 0};
+        int& bps = blocks_per_sm[AnyHit ? 1 : 0];
+        if (bps == 0) {
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_trace_wide_persistent<AnyHit>,
+                                                          kTraceThreads, 0);
+            if (bps <= 0) bps = 1;
+        }
+        int grid = std::min(ctx->sm_count * bps, (nrays + kTraceThreads - 1) / kTraceThreads);
+        cudaError_t err = cudaMemsetAsync(ctx->d_counter, 0, sizeof(unsigned), ctx->stream);
+        if (err != cudaSuccess) return cuda_fail(err, "ray counter reset");
+        k_trace_wide_persistent<AnyHit><<<grid, kTraceThreads, 0, ctx->stream>>>(
+            bvh->view(), r4, nrays, hit_id, hit_t, ctx->d_counter, ctx->trace_budget,
+            ctx->d_error);
+        ctx->launches += 1;
+        return cuda_fail(cudaGetLastError(), "k_trace_wide_persistent");
+    }
+    if (ctx->trace_variant == kTraceWide) {
+        if (int st = lbvh_ensure_wide(ctx, const_cast<lux_bvh*>(bvh))) return st;
+        int grid = (nrays + kTraceThreads - 1) / kTraceThreads;
+        k_trace_wide<AnyHit><<<grid, kTraceThreads, 0, ctx->stream>>>(
+            bvh->view(), r4, nrays, hit_id, hit_t, ctx->d_error);
+        ctx->launches += 1;
+        return cuda_fail(cudaGetLastError(), "k_trace_wide");
+    }
     if (ctx->trace_variant == kTraceStatic) {
         int grid = (nrays + kTraceThreads - 1) / kTraceThreads;
         k_trace<AnyHit><<<grid, kTraceThreads, 0, ctx->stream>>>(bvh->view(), r4, nrays, hit_id,

@@ -99,7 +99,7 @@ def test_trace_matches_oracle_random(ctx, oracle):
     assert np.array_equal(any_id >= 0, want_id >= 0)
 
 
-@pytest.mark.parametrize("variant,budget", [(1, 32), (2, 1), (2, 7), (2, 32), (2, 256)])
+@pytest.mark.parametrize("variant,budget", [(1, 32), (2, 1), (2, 7), (2, 32), (2, 256), (3, 32), (4, 1), (4, 16), (4, 64)])
 def test_trace_variants_identical(ctx, oracle, variant, budget):
     """Tunables change speed only: every traversal variant returns the oracle's hits."""
     tris = W.soup_triangles(100_000, seed=21)
@@ -116,7 +116,7 @@ def test_trace_variants_identical(ctx, oracle, variant, budget):
         any_id = bvh.trace_any(rays)
     finally:
         ctx.set_option(lux_b200.OPT_TRACE_VARIANT, 0)
-        ctx.set_option(lux_b200.OPT_TRACE_BUDGET, 32)
+        ctx.set_option(lux_b200.OPT_TRACE_BUDGET, 16)
     assert np.array_equal(got_id, want_id)
     assert np.array_equal(got_t, want_t)
     assert np.array_equal(any_id >= 0, want_id >= 0)
@@ -284,3 +284,68 @@ def test_validators_report_the_reference_messages(ctx):
     assert empty.validate(np.zeros((0, 9), np.float32)) == (True, "")
     assert bvh.validate(np.zeros((0, 9), np.float32)) == (
         False, "BVH contains primitives for an empty scene")
+
+
+def _with_variant(ctx, variant, fn):
+    try:
+        ctx.set_option(lux_b200.OPT_TRACE_VARIANT, variant)
+        return fn()
+    finally:
+        ctx.set_option(lux_b200.OPT_TRACE_VARIANT, 0)
+
+
+@pytest.mark.parametrize("bits", [30, 63])
+def test_wide_walk_matches_binary_walk_through_refits_and_ties(ctx, oracle, bits):
+    """The 4-wide walk returns the binary walk's closest and first-found hits, including
+    equal-t ties between duplicated triangles, and follows refits and rebuilds."""
+    tris = W.soup_triangles(60_000, seed=31)
+    tris = np.concatenate([tris, tris[:5000]])          # exact duplicates: t ties
+    rays = W.uniform_rays(40_000, seed=32)
+    bvh = ctx.build_lbvh(tris, lux_b200.PRIM_TRIANGLES, bits)
+    for step in range(3):
+        ref_c = _with_variant(ctx, 1, lambda: bvh.trace_closest(rays))
+        ref_a = _with_variant(ctx, 1, lambda: bvh.trace_any(rays))
+        for variant in (3, 4):
+            got_c = _with_variant(ctx, variant, lambda: bvh.trace_closest(rays))
+            got_a = _with_variant(ctx, variant, lambda: bvh.trace_any(rays))
+            assert np.array_equal(got_c[0], ref_c[0]) and np.array_equal(got_c[1], ref_c[1])
+            assert np.array_equal(got_a, ref_a)
+        if step == 0:
+            tris = W.jitter_triangles(tris, seed=33)
+            bvh.refit(tris)
+        else:
+            tris = W.soup_triangles(70_000, seed=34)
+            bvh.rebuild(tris)
+    tree = oracle.build(oracle.triangle_bounds(tris))
+    want_id, want_t = oracle.trace(tris, tree, rays)
+    assert np.array_equal(got_c[0], want_id) and np.array_equal(got_c[1], want_t)
+
+
+@pytest.mark.parametrize("case", ["planar", "huge", "tiny", "far_offset"])
+def test_wide_walk_exact_on_degenerate_extents(ctx, oracle, case):
+    """Quantised wide nodes steer only: on flat, huge, tiny and far-offset geometry the
+    wide walks return the binary walk's (and the oracle's) hits exactly."""
+    tris = W.soup_triangles(20_000, seed=41).reshape(-1, 3, 3)
+    rays = W.uniform_rays(20_000, seed=42)
+    if case == "planar":
+        tris[:, :, 2] = np.float32(0.5)                  # zero extent in z
+    elif case == "huge":
+        tris = tris * np.float32(1e20)
+        rays[:, :3] *= np.float32(1e20)
+    elif case == "tiny":
+        tris = tris * np.float32(1e-20)
+        rays[:, :3] *= np.float32(1e-20)
+    else:
+        tris = tris + np.float32(3e4)                    # ulp(3e4) ~ 2e-3: coarse grids
+        rays[:, :3] += np.float32(3e4)
+    tris = np.ascontiguousarray(tris.reshape(-1, 9), np.float32)
+    bvh = ctx.build_lbvh(tris)
+    want = _with_variant(ctx, 1, lambda: bvh.trace_closest(rays))
+    tree = oracle.build(oracle.triangle_bounds(tris))
+    oid, ot = oracle.trace(tris, tree, rays)
+    assert np.array_equal(want[0], oid) and np.array_equal(want[1], ot)
+    for variant in (3, 4):
+        got = _with_variant(ctx, variant, lambda: bvh.trace_closest(rays))
+        assert np.array_equal(got[0], want[0]) and np.array_equal(got[1], want[1])
+        got_a = _with_variant(ctx, variant, lambda: bvh.trace_any(rays))
+        assert np.array_equal(got_a, _with_variant(ctx, 1, lambda: bvh.trace_any(rays)))
