@@ -514,6 +514,25 @@ def run_render(args, name: str) -> None:
                    "sample": f"reference trace_path on {rows} of {H} rows ({threads} threads), "
                              "scaled to the frame; ray count of the same config"
                              + ("" if name == "cornell" else "; host BVH build excluded")}
+    # Image error against the FP64 high-spp oracle (tests/golden/make_fp64.py): relative
+    # RMSE and measured / noise-predicted MSE (1 for an unbiased renderer).
+    fp64 = None
+    fixture = os.path.join(os.path.dirname(os.path.abspath(__file__)), "tests", "golden",
+                           f"{name}_fp64.npz")
+    if os.path.exists(fixture):
+        g = np.load(fixture)
+        x0, y0, x1, y1 = (int(v) for v in g["rect"]) if "rect" in g else (0, 0, W, H)
+        img = film.double().cpu().numpy()[y0:y1, x0:x1] / spp
+        ref = g["mean"].astype(np.float64)
+        var = g["var"].astype(np.float64)
+        mse = float(np.mean((img - ref) ** 2))
+        oracle_noise = float(np.mean(var / int(g["spp"])))
+        rms = float(np.sqrt(np.mean(ref ** 2)))
+        fp64 = {"relative_rmse": float(np.sqrt(max(mse - oracle_noise, 0.0))) / rms,
+                "relative_rmse_raw": float(np.sqrt(mse)) / rms,
+                "mse_over_noise": mse / (float(np.mean(var / spp)) + oracle_noise),
+                "oracle_spp": int(g["spp"]),
+                "pixels": "all" if "rect" not in g else f"crop x{x0}..{x1} y{y0}..{y1}"}
     line = {"metric": metric, "value": value, "unit": "Mrays/s",
             "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
@@ -526,7 +545,7 @@ def run_render(args, name: str) -> None:
             "e2e": {"value": total_rays / (e2e_ms * 1e-3) / 1e6, "unit": "Mrays/s",
                     "h2d_bytes_per_step": 0, "d2h_bytes_per_step": W * H * 12,
                     "ms_per_step": e2e_ms},
-            "cpu_baseline": cpu}
+            "cpu_baseline": cpu, "image_error_vs_fp64_oracle": fp64}
     print(json.dumps(line))
 
 

@@ -3,6 +3,7 @@
 * Oracle: the plain-C restatement (oracle/lux_oracle.c -> oracle/liblux_oracle.so).
 * Ref: the reference's own host code (oracle/_ref/libluxref.so, built from the reference
   sources by oracle/build.py; present wherever it was built).
+* PT64: the FP64 high-spp path-tracing oracle (oracle/pt64.c -> oracle/liblux_pt64.so).
 
 Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use this module.
 """
@@ -16,6 +17,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_LIB = os.path.join(HERE, "liblux_oracle.so")
 REF_LIB = os.path.join(HERE, "_ref", "libluxref.so")
+PT64_LIB = os.path.join(HERE, "liblux_pt64.so")
 
 _P = ctypes.c_void_p
 _I = ctypes.c_int
@@ -213,3 +215,37 @@ class Ref:
         self.lib.ref_cornell_render(width, height, spp, max_depth, seed, y0, y1, threads,
                                     total.ctypes.data, total2.ctypes.data, _addr(smp))
         return (total, total2, smp) if samples else (total, total2)
+
+
+class PT64:
+    """FP64 high-spp path-tracing oracle (oracle/pt64.c)."""
+
+    def __init__(self, path: str = PT64_LIB):
+        lib = ctypes.CDLL(path)
+        lib.pt64_render.argtypes = [_P, _I, _P, _P, _I, _P, _I, _P, _I, _I, _I, _I,
+                                    ctypes.c_uint64, _I, _I, _I, _I, _I, _P, _P]
+        lib.pt64_render.restype = _I
+        self.lib = lib
+
+    def render(self, tris, material_ids, materials, lights, camera_frame, width, height, spp,
+               max_depth, seed=1, rect=None, threads=1):
+        """Per-pixel mean radiance and per-sample variance (double) over rect
+        (x0, y0, x1, y1), shape (rows, cols, 3) each.  camera_frame: origin, lower_left,
+        horizontal, vertical (12 floats)."""
+        x0, y0, x1, y1 = rect if rect is not None else (0, 0, width, height)
+        tris = np.ascontiguousarray(tris, np.float32)
+        mids = np.ascontiguousarray(material_ids, np.int32)
+        mats = np.ascontiguousarray(materials, np.float32)
+        lights = np.ascontiguousarray(lights, np.float32).reshape(-1, 7)
+        cam = np.ascontiguousarray(camera_frame, np.float32)
+        mean = np.zeros((y1 - y0, x1 - x0, 3), np.float64)
+        var = np.zeros_like(mean)
+        self.lib.pt64_render(tris.ctypes.data, len(tris), mids.ctypes.data, mats.ctypes.data,
+                             len(mats), lights.ctypes.data if len(lights) else None, len(lights),
+                             cam.ctypes.data, width, height, spp, max_depth, seed, x0, y0, x1, y1,
+                             threads, mean.ctypes.data, var.ctypes.data)
+        return mean, var
+
+    @staticmethod
+    def available() -> bool:
+        return os.path.exists(PT64_LIB)

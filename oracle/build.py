@@ -1,7 +1,8 @@
 """Build recipes for the oracle (test infrastructure; nothing in the product loads these).
 
 1. oracle/liblux_oracle.so: the plain-C restatement in oracle/lux_oracle.c.
-2. oracle/_ref/libluxref.so: the reference's own host code.
+2. oracle/liblux_pt64.so: the FP64 path-tracing oracle in oracle/pt64.c.
+3. oracle/_ref/libluxref.so: the reference's own host code.
 
 Compiles, in place and without the reference's build system, the handful of
 reference translation units the CPU path needs (integrator/cpu_path_tracer.cpp,
@@ -18,6 +19,7 @@ REF_ROOT = os.environ.get("LUX_REFERENCE_ROOT", "/root/reference")
 OUT_DIR = os.path.join(HERE, "_ref")
 OUT = os.path.join(OUT_DIR, "libluxref.so")
 ORACLE_OUT = os.path.join(HERE, "liblux_oracle.so")
+PT64_OUT = os.path.join(HERE, "liblux_pt64.so")
 
 REF_SOURCES = [
     "src/integrator/cpu_path_tracer.cpp",
@@ -46,6 +48,16 @@ def build_oracle(force=False):
     return ORACLE_OUT
 
 
+def build_pt64(force=False):
+    """Compile the FP64 path-tracing oracle (double precision, pthreads)."""
+    srcs = [os.path.join(HERE, "pt64.c")]
+    if force or _stale(PT64_OUT, srcs):
+        cmd = ["gcc", "-std=c11", "-O3", "-fPIC", "-shared", "-pthread", "-ffp-contract=off",
+               "-o", PT64_OUT, *srcs, "-lm"]
+        subprocess.run(cmd, check=True)
+    return PT64_OUT
+
+
 def build_ref(force=False):
     """Compile the reference harness; returns None when the reference is absent."""
     src_dir = os.path.join(REF_ROOT, "src")
@@ -62,6 +74,7 @@ def build_ref(force=False):
 
 
 def build(force=False):
+    build_pt64(force)
     return build_oracle(force), build_ref(force)
 
 

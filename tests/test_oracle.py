@@ -125,3 +125,31 @@ def test_oracle_matches_reference_live(oracle, n, seed):
     oid, ot = oracle.trace(tris, o, rays)
     assert np.array_equal(oid, rid)
     assert np.array_equal(ot, rt)
+
+
+@pytest.mark.skipif(not Ref.available(), reason="reference harness not built")
+def test_fp64_oracle_agrees_with_reference_cpu_tracer():
+    """The FP64 oracle and the reference's own CPU tracer estimate the same image: per-
+    pixel z-scores are standard normal and the MSE is what their noise predicts."""
+    from lux_b200 import scene as S
+    from oracle import build as oracle_build
+    from oracle.bindings import PT64
+    oracle_build.build_pt64()
+    w = h = 24
+    spp = 256
+    b = S.make_cornell_scene(w, h)
+    tris = b.world_triangles()
+    mids = b.world_material_ids()
+    mats = np.array([[m.type, *m.albedo, *m.emission, m.roughness, m.metallic, m.eta,
+                      m.emission_two_sided] for m in b.materials], np.float32)
+    c = b.camera
+    frame = np.array([*c.origin, *c.lower_left, *c.horizontal, *c.vertical], np.float32)
+    mo, vo = PT64().render(tris, mids, mats, np.zeros((0, 7), np.float32), frame, w, h, spp, 4,
+                           seed=9, threads=4)
+    tot, tot2 = Ref().cornell_render(w, h, spp, 4, 1, threads=4)
+    mr = (tot.astype(np.float64) / spp).reshape(h, w, 3)
+    vr = ((tot2.astype(np.float64) / spp).reshape(h, w, 3) - mr ** 2) * spp / (spp - 1)
+    z = (mo - mr) / np.sqrt(vo / spp + vr / spp + 1e-30)
+    assert abs(z.mean()) < 0.15 and 0.85 < z.std() < 1.15
+    ratio = np.mean((mo - mr) ** 2) / np.mean(vo / spp + vr / spp)
+    assert 0.8 < ratio < 1.2

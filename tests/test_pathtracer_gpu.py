@@ -220,3 +220,44 @@ def test_device_mesh_update_matches_a_fresh_scene(ctx):
     fresh = S.render_samples(ctx, S.Scene(ctx, build(moved)[0]), req)
     same = np.all(got == fresh, axis=-1)
     assert same.mean() > 0.999, same.mean()
+
+
+def _fp64_check(film_mean, fixture, spp):
+    """Relative RMSE of the render against the FP64 oracle, with the oracle's own noise
+    (its per-sample variance / its spp) taken out of the mean squared error, and the
+    ratio of measured to noise-predicted MSE (1 for an unbiased renderer)."""
+    ref = fixture["mean"].astype(np.float64)
+    var = fixture["var"].astype(np.float64)
+    mse = np.mean((film_mean - ref) ** 2)
+    oracle_noise = np.mean(var / int(fixture["spp"]))
+    predicted = np.mean(var / spp) + oracle_noise
+    rel_rmse = np.sqrt(max(mse - oracle_noise, 0.0)) / np.sqrt(np.mean(ref ** 2))
+    return rel_rmse, mse / predicted
+
+
+def test_cornell_config_is_unbiased_against_fp64_oracle(ctx):
+    """Cornell 256^2, 64 spp, depth 4, seed 1 against the 2048-spp FP64 oracle: the error
+    is Monte Carlo noise only (MSE ratio ~1) and the relative RMSE is stated."""
+    g = np.load(os.path.join(ROOT, "tests", "golden", "cornell_fp64.npz"))
+    sc = S.Scene(ctx, S.make_cornell_scene(256, 256))
+    film = S.render(ctx, sc, S.request(256, 256, 64, 4, 1)).astype(np.float64) / 64
+    rel_rmse, ratio = _fp64_check(film, g, 64)
+    assert 0.9 < ratio < 1.1, ratio
+    assert rel_rmse < 0.2, rel_rmse
+    # At 8192 spp the relative RMSE is under 1% (noise shrinks as 1/sqrt(spp)).
+    film = S.render(ctx, sc, S.request(256, 256, 8192, 4, 1)).astype(np.float64) / 8192
+    rel_rmse, ratio = _fp64_check(film, g, 8192)
+    assert rel_rmse < 0.01 and 0.8 < ratio < 1.2, (rel_rmse, ratio)
+
+
+def test_heavy_config_crop_is_unbiased_against_fp64_oracle(ctx):
+    """Heavy render (1024^2, depth 8, GGX + glass) at 64 spp against the FP64 oracle's
+    4096-spp centre crop."""
+    from lux_b200 import scenes as SC
+    g = np.load(os.path.join(ROOT, "tests", "golden", "heavy_fp64.npz"))
+    x0, y0, x1, y1 = (int(v) for v in g["rect"])
+    sc = S.Scene(ctx, SC.heavy_render_scene(1024, 1024))
+    film = S.render(ctx, sc, S.request(1024, 1024, 64, 8, 1)).astype(np.float64) / 64
+    rel_rmse, ratio = _fp64_check(film[y0:y1, x0:x1], g, 64)
+    assert 0.8 < ratio < 1.25, ratio
+    assert rel_rmse < 0.3, rel_rmse
