@@ -41,6 +41,7 @@ METRIC = "Mrays/s"
 # Algorithmic bytes (per unit) used for the roofline: build 120 B/tri, refit 104 B/tri,
 # traversal 32 B ray + 8 B hit + 32 B per box test + 36 B per triangle test.
 BUILD_BYTES_PER_TRI = 120
+TRACE_DRAM_BYTES_PER_RAY = (1.282381e9 + 0.044999e9) / 1048576
 REFIT_BYTES_PER_TRI = 104
 
 
@@ -292,6 +293,9 @@ def run_lux(args) -> None:
     phase_ms = {p: float(np.mean(v)) for p, v in per_phase.items()}
 
     # Roofline of the dominant kernel (the traversal: one launch per trace phase).
+    # DRAM traffic per ray of k_trace_wide_persistent from one ncu capture of this
+    # generator at 1,048,576 triangles and 1,048,576 rays (1.282 GB read + 0.045 GB
+    # written), scaled by the ray count.
     box_tests, tri_tests = bvh.trace_stats(d_rays)
     trace_bytes = N_RAYS * (32 + 8) + 32 * box_tests + 36 * tri_tests
     peak, peak_kind = measured_peaks()
@@ -307,6 +311,7 @@ def run_lux(args) -> None:
         achieved = trace_bytes / (phase_ms["trace"] * 1e-3) / 1e9
         dominant = "trace"
 
+    trace_traffic = TRACE_DRAM_BYTES_PER_RAY * N_RAYS if dominant == "trace" else None
     found_count = int(found.item())
     hits = int((hit_id >= 0).sum().item())
 
@@ -329,9 +334,12 @@ def run_lux(args) -> None:
         "trace_mrays_s": N_RAYS / (phase_ms["trace"] * 1e-3) / 1e6,
         "refit_mtri_s": N_TRIS / (phase_ms["refit"] * 1e-3) / 1e6,
         "hits": hits, "overlap_pairs": found_count,
-        "roofline": {"bound": "hbm", "kernel": "k_trace" if dominant == "trace" else dominant,
+        "roofline": {"bound": "hbm",
+                     "kernel": "k_trace_wide_persistent" if dominant == "trace" else dominant,
                      "achieved": achieved, "peak": peak, "peak_kind": peak_kind,
-                     "unit": "GB/s", "frac": achieved / peak, "traffic": None,
+                     "unit": "GB/s", "frac": achieved / peak, "traffic": trace_traffic,
+                     "traffic_source": "ncu dram__bytes_read+write of k_trace_wide_persistent "
+                                       "at 1,048,576 rays, scaled by rays",
                      "algorithmic_bytes_per_launch": alg,
                      "box_tests_per_ray": box_tests / N_RAYS,
                      "tri_tests_per_ray": tri_tests / N_RAYS},
