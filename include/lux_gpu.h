@@ -73,8 +73,15 @@ int lux_ctx_launch_count(lux_ctx* ctx, int64_t* count);
  *                          refill, 3 one thread per ray over 4-wide nodes, 4 persistent
  *                          warps with refill over 4-wide nodes
  *   LUX_OPT_TRACE_BUDGET   traversal steps per refill round of the persistent kernel
- *   LUX_OPT_RENDER_BATCH   paths in flight per wavefront batch (device memory ~200 B each) */
-enum lux_option { LUX_OPT_TRACE_VARIANT = 1, LUX_OPT_TRACE_BUDGET = 2, LUX_OPT_RENDER_BATCH = 3 };
+ *   LUX_OPT_RENDER_BATCH   paths in flight per wavefront batch (device memory ~200 B each)
+ *   LUX_OPT_PATH_BUDGET    traversal steps per refill round of the path tracer's extension and
+ *                          shadow kernels (variant 1 uses one thread per path instead) */
+enum lux_option {
+    LUX_OPT_TRACE_VARIANT = 1,
+    LUX_OPT_TRACE_BUDGET = 2,
+    LUX_OPT_RENDER_BATCH = 3,
+    LUX_OPT_PATH_BUDGET = 4
+};
 int lux_ctx_set_option(lux_ctx* ctx, int32_t option, int64_t value);
 int lux_ctx_get_option(lux_ctx* ctx, int32_t option, int64_t* value);
 

@@ -29,6 +29,7 @@ NVCC_FLAGS = [
 PER_FILE_FLAGS = {
     "wavefront.cu": ["-fmad=false"],
     "scene.cu": ["-fmad=false"],
+    "server.cu": ["-fmad=false"],
 }
 
 

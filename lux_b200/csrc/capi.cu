@@ -244,6 +244,10 @@ int lux_ctx_set_option(lux_ctx* ctx, int32_t option, int64_t value) {
             if (value < 1 || value > 4096) return lux::fail(LUX_ERR_INVALID_ARGUMENT, "trace budget 1..4096");
             ctx->trace_budget = static_cast<int>(value);
             return LUX_OK;
+        case LUX_OPT_PATH_BUDGET:
+            if (value < 1 || value > 4096) return lux::fail(LUX_ERR_INVALID_ARGUMENT, "path budget 1..4096");
+            ctx->path_budget = static_cast<int>(value);
+            return LUX_OK;
         case LUX_OPT_RENDER_BATCH:
             if (value < 1 || value > (1 << 28)) return lux::fail(LUX_ERR_INVALID_ARGUMENT, "render batch 1..2^28");
             ctx->render_batch = static_cast<int>(value);
@@ -259,6 +263,7 @@ int lux_ctx_get_option(lux_ctx* ctx, int32_t option, int64_t* value) {
         case LUX_OPT_TRACE_VARIANT: *value = ctx->trace_variant; return LUX_OK;
         case LUX_OPT_TRACE_BUDGET: *value = ctx->trace_budget; return LUX_OK;
         case LUX_OPT_RENDER_BATCH: *value = ctx->render_batch; return LUX_OK;
+        case LUX_OPT_PATH_BUDGET: *value = ctx->path_budget; return LUX_OK;
         default: return lux::fail(LUX_ERR_INVALID_ARGUMENT, "unknown option");
     }
 }

@@ -17,7 +17,8 @@ struct lux_ctx {
     unsigned* d_counter = nullptr;   // device work counter (persistent kernels)
     // Tunables (lux_ctx_set_option).
     int trace_variant = 0;           // lux::kTrace* (auto: wide persistent)
-    int trace_budget = 16;           // traversal steps per refill round
+    int trace_budget = 16;           // traversal steps per refill round (ray queries)
+    int path_budget = 32;            // traversal steps per refill round (path tracer)
     int render_batch = 1 << 22;      // paths in flight per wavefront batch
     void* render_runtime = nullptr;  // wavefront buffers, grown on demand
     // Growable device scratch, reused across calls on this context.

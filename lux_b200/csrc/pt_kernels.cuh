@@ -251,6 +251,198 @@ LUX_D SceneHit scene_closest(const SceneView& sc, f3 o, f3 d, float tmin, float 
     return h;
 }
 
+// scene_closest as a resumable walk: step() advances by one node visit or one triangle
+// (or instance) test, followed by the pops it enables, so a kernel can interleave many
+// walks per warp and refill lanes as walks finish.  The decisions, in order, are those
+// of scene_closest / blas_closest above, so the result is the same.  The four stacks
+// live apart from the scalar state, which then stays in registers.
+struct WalkStacks {
+    int t_h[kStack];
+    float t_t[kStack];
+    int b_h[kStack];
+    float b_t[kStack];
+};
+
+struct TwoLevelWalk {
+    f3 o, d;
+    float tmin;
+    slab_ray sr;
+    SceneHit hit;                 // best so far (hit.t is the current bound)
+    int ign_instance, ign_local;
+    int t_cur, t_sp;
+    long long t_steps;
+    bool in_blas;
+    const BvhNode* b_nodes;
+    const TriRecord* b_tris;
+    int b_n, b_cur, b_sp, b_ignored, b_first;
+    long long b_steps;
+    f3 lo, ld;
+    slab_ray lsr;
+    bool done;
+
+    LUX_D void init(const SceneView& sc, f3 ro, f3 rd, float rtmin, float rtmax, int ignored) {
+        o = ro;
+        d = rd;
+        tmin = rtmin;
+        hit = SceneHit{};
+        hit.t = rtmax;
+        in_blas = false;
+        t_sp = 0;
+        t_steps = 0;
+        done = true;
+        if (!sc.has_two_level) return;
+        ign_instance = -1;
+        ign_local = -1;
+        if (ignored >= 0) {
+            float4 v1 = __ldg(&sc.tris[ignored].v1);
+            float4 v2 = __ldg(&sc.tris[ignored].v2);
+            ign_instance = __float_as_int(v1.w);
+            ign_local = __float_as_int(v2.w);
+        }
+        sr = make_slab_ray(ray3{o, tmin, d, rtmax});
+        float tn;
+        if (!slab_hit(sr, load_root(sc.tlas.root), hit.t, tn)) return;
+        t_cur = sc.tlas.n == 1 ? ~0 : 0;
+        done = false;
+    }
+
+    LUX_D void fail(int* error, int bit, float rtmax) {
+        atomicOr(error, bit);
+        hit = SceneHit{};
+        hit.t = rtmax;
+        done = true;
+    }
+
+    // Resumes the deepest deferred TLAS child that still passes; false when none is left.
+    LUX_D bool pop_tlas(const WalkStacks& k) {
+        while (t_sp > 0) {
+            --t_sp;
+            if (!(k.t_t[t_sp] > hit.t)) {
+                t_cur = k.t_h[t_sp];
+                return true;
+            }
+        }
+        return false;
+    }
+    LUX_D bool pop_blas(const WalkStacks& k) {
+        while (b_sp > 0) {
+            --b_sp;
+            if (!(k.b_t[b_sp] > hit.t)) {
+                b_cur = k.b_h[b_sp];
+                return true;
+            }
+        }
+        return false;
+    }
+
+    // One step; returns true when the walk is complete (hit holds the result).
+    LUX_D bool step(const SceneView& sc, WalkStacks& k, int* error) {
+        if (done) return true;
+        const BvhView& tl = sc.tlas;
+        if (in_blas) {
+            if (++b_steps > 2ll * b_n + 64 || b_cur >= b_n - 1 || ~b_cur >= b_n) {
+                fail(error, kErrLoopBound, INFINITY);
+                return true;
+            }
+            bool pop = true;
+            if (b_cur >= 0) {
+                BvhNode nd = load_node(b_nodes, b_cur);
+                float tl_, tr_;
+                bool hl = slab_hit(lsr, node_left_box(nd), hit.t, tl_);
+                bool hr = slab_hit(lsr, node_right_box(nd), hit.t, tr_);
+                if (hl) {
+                    if (hr) {
+                        if (b_sp >= kStack) {
+                            fail(error, kErrStackOverflow, INFINITY);
+                            return true;
+                        }
+                        k.b_h[b_sp] = nd.ch.y;
+                        k.b_t[b_sp] = tr_;
+                        ++b_sp;
+                    }
+                    b_cur = nd.ch.x;
+                    pop = false;
+                } else if (hr) {
+                    b_cur = nd.ch.y;
+                    pop = false;
+                }
+            } else {
+                const float4* tp = reinterpret_cast<const float4*>(b_tris + ~b_cur);
+                float4 p0 = __ldg(tp);
+                int local = __float_as_int(p0.w);
+                if (local != b_ignored) {
+                    float4 p1 = __ldg(tp + 1);
+                    float4 p2 = __ldg(tp + 2);
+                    float t, u, v;
+                    if (moller_trumbore(lo, ld, xyz(p0), xyz(p1), xyz(p2), t, u, v) && t > tmin
+                        && t < hit.t) {
+                        hit.prim = b_first + local;
+                        hit.t = t;
+                        hit.u = u;
+                        hit.v = v;
+                    }
+                }
+            }
+            if (pop && !pop_blas(k)) {
+                in_blas = false;
+                if (!pop_tlas(k)) done = true;
+            }
+            return done;
+        }
+        if (++t_steps > 2ll * tl.n + 64 || t_cur >= tl.n - 1 || ~t_cur >= tl.n) {
+            fail(error, kErrLoopBound, INFINITY);
+            return true;
+        }
+        bool pop = true;
+        if (t_cur >= 0) {
+            BvhNode nd = load_node(tl.nodes, t_cur);
+            float a, b;
+            bool hl = slab_hit(sr, node_left_box(nd), hit.t, a);
+            bool hr = slab_hit(sr, node_right_box(nd), hit.t, b);
+            if (hl) {
+                if (hr) {
+                    if (t_sp >= kStack) {
+                        fail(error, kErrStackOverflow, INFINITY);
+                        return true;
+                    }
+                    k.t_h[t_sp] = nd.ch.y;
+                    k.t_t[t_sp] = b;
+                    ++t_sp;
+                }
+                t_cur = nd.ch.x;
+                pop = false;
+            } else if (hr) {
+                t_cur = nd.ch.y;
+                pop = false;
+            }
+        } else {
+            const int inst_id = sc.tlas_instance[tl.sorted_ids[~t_cur]];
+            const Instance& inst = sc.instances[inst_id];
+            const BvhView& b = sc.blas[inst.blas];
+            if (b.n > 0) {
+                lo = xform_point(inst.inv, o);
+                ld = xform_vector(inst.inv, d);
+                lsr = make_slab_ray(ray3{lo, tmin, ld, hit.t});
+                float tn;
+                if (slab_hit(lsr, load_root(b.root), hit.t, tn)) {
+                    in_blas = true;
+                    b_nodes = b.nodes;
+                    b_tris = b.tris;
+                    b_n = b.n;
+                    b_cur = b.n == 1 ? ~0 : 0;
+                    b_sp = 0;
+                    b_steps = 0;
+                    b_ignored = inst_id == ign_instance ? ign_local : -1;
+                    b_first = inst.first_primitive;
+                    return false;
+                }
+            }
+        }
+        if (pop && !pop_tlas(k)) done = true;
+        return done;
+    }
+};
+
 // ------------------------------------------------------------------ lights
 
 LUX_D float light_pmf(const SceneView& sc, int sampler, int index) {  // gpu_scene_light_sampler.cuh:9-45
@@ -510,12 +702,10 @@ LUX_D void init_path(const PathPool& rt, const Camera& cam, int p, int pixel, in
     rt.ray_d[p] = make_float4(d.x, d.y, d.z, INFINITY);
 }
 
-// Closest hit of path p's ray: returns the material class of the hit, or -1 after adding
-// the environment's radiance on a miss (cpu_path_tracer.cpp:415-428).
-LUX_D int extend_path(const PathPool& rt, const SceneView& sc, int sampler, int p, int* error) {
-    float4 a = rt.ray_o[p];
-    float4 b = rt.ray_d[p];
-    SceneHit h = scene_closest(sc, xyz(a), xyz(b), a.w, b.w, -1, error);
+// Records the closest hit h of path p's ray: returns the material class of the hit, or
+// -1 after adding the environment's radiance on a miss (cpu_path_tracer.cpp:415-428).
+LUX_D int extend_finish(const PathPool& rt, const SceneView& sc, int sampler, int p,
+                        const SceneHit& h) {
     if (h.prim >= 0) {
         rt.hit[p] = make_float4(h.t, h.u, h.v, __int_as_float(h.prim));
         return material_class(sc.materials[material_of(sc, h.prim)].type);
@@ -531,6 +721,149 @@ LUX_D int extend_path(const PathPool& rt, const SceneView& sc, int sampler, int 
         }
     }
     return -1;
+}
+
+// Closest hit of path p's ray (one walk to completion), then extend_finish.
+LUX_D int extend_path(const PathPool& rt, const SceneView& sc, int sampler, int p, int* error) {
+    float4 a = rt.ray_o[p];
+    float4 b = rt.ray_d[p];
+    SceneHit h = scene_closest(sc, xyz(a), xyz(b), a.w, b.w, -1, error);
+    return extend_finish(rt, sc, sampler, p, h);
+}
+
+// Closest hits of the paths in queue q[0, n) by persistent warps: each lane advances its
+// walk by at most `budget` steps per round, and lanes whose walk finished hand it to
+// finish() and take the next path through one warp-aggregated atomic on *next_item, so
+// lanes do not idle behind the longest walk of a static warp.  tag_of(p) picks a path's
+// scene once (view(tag) returns it); finish(p, hit) is called by every lane of the warp
+// each round, with p = -1 for lanes that did not finish, so it may append to queues
+// with warp-collective operations.
+template <typename TagOf, typename View, typename Finish>
+LUX_D void refill_walks(const PathPool& rt, const int* q, int n, int* next_item, int budget,
+                        int* error, TagOf tag_of, View view, Finish finish) {
+    const unsigned lane = threadIdx.x & 31;
+    const unsigned lt = lanemask_lt();
+    int p = -1;  // >= 0 active path, -1 needs one, -2 none left
+    int tag = 0;
+    TwoLevelWalk w;
+    WalkStacks stacks;
+    for (;;) {
+        const bool need = p == -1;
+        const unsigned m = __ballot_sync(0xffffffffu, need);
+        if (m) {
+            const int leader = __ffs(m) - 1;
+            int base = 0;
+            if (static_cast<int>(lane) == leader) base = atomicAdd(next_item, __popc(m));
+            base = __shfl_sync(0xffffffffu, base, leader);
+            if (need) {
+                const int idx = base + __popc(m & lt);
+                if (idx >= n) {
+                    p = -2;
+                } else {
+                    p = q[idx];
+                    tag = tag_of(p);
+                    const float4 a = rt.ray_o[p];
+                    const float4 b = rt.ray_d[p];
+                    w.init(view(tag), xyz(a), xyz(b), a.w, b.w, -1);
+                }
+            }
+        }
+        if (__all_sync(0xffffffffu, p == -2)) break;
+        bool finished = false;
+        if (p >= 0) {
+            const SceneView& sc = view(tag);
+            for (int s = 0; s < budget && !finished; ++s) finished = w.step(sc, stacks, error);
+        }
+        SceneHit h = w.hit;
+        if (h.prim < 0) h.t = INFINITY;
+        finish(finished ? p : -1, tag, h);
+        if (finished) p = -1;
+    }
+}
+
+// Shadow rays of the paths in queue q[0, n) by persistent warps with refilling lanes:
+// each lane walks its ray's segments through pass-through surfaces exactly as
+// shadow_path does (the same segment loop, one resumable walk per segment) and adds the
+// NEE contribution when the ray is not blocked.
+template <typename TagOf, typename View>
+LUX_D void refill_shadows(const PathPool& rt, const int* q, int n, int* next_item, int budget,
+                          int* error, TagOf tag_of, View view, unsigned long long& segments) {
+    const unsigned lane = threadIdx.x & 31;
+    const unsigned lt = lanemask_lt();
+    int p = -1;  // >= 0 active path, -1 needs one, -2 none left
+    int tag = 0, seg = 0;
+    f3 o, d, tr;
+    float tmax = 0;
+    TwoLevelWalk w;
+    WalkStacks stacks;
+    for (;;) {
+        const bool need = p == -1;
+        const unsigned m = __ballot_sync(0xffffffffu, need);
+        if (m) {
+            const int leader = __ffs(m) - 1;
+            int base = 0;
+            if (static_cast<int>(lane) == leader) base = atomicAdd(next_item, __popc(m));
+            base = __shfl_sync(0xffffffffu, base, leader);
+            if (need) {
+                const int idx = base + __popc(m & lt);
+                if (idx >= n) {
+                    p = -2;
+                } else {
+                    p = q[idx];
+                    tag = tag_of(p);
+                    const float4 a = rt.sh_o[p];
+                    const float4 b = rt.sh_d[p];
+                    o = xyz(a);
+                    d = xyz(b);
+                    tmax = a.w;
+                    tr = splat(1.0f);
+                    seg = 0;
+                    ++segments;
+                    w.init(view(tag), o, d, kRayEpsilon, tmax, __float_as_int(b.w));
+                }
+            }
+        }
+        if (__all_sync(0xffffffffu, p == -2)) break;
+        if (p < 0) continue;
+        const SceneView& sc = view(tag);
+        for (int s = 0; s < budget; ++s) {
+            if (!w.step(sc, stacks, error)) continue;
+            bool end = false, blocked = false;
+            const SceneHit& h = w.hit;
+            if (h.prim < 0) {
+                end = true;
+            } else {
+                const Material mat = sc.materials[material_of(sc, h.prim)];
+                if (!is_passthrough(mat)) {
+                    blocked = true;
+                    end = true;
+                } else {
+                    tr = tr * passthrough_transmittance(mat);
+                    const float adv = add(h.t, kRayEpsilon);
+                    if (max_component(tr) <= 0 || adv >= tmax) {
+                        end = true;
+                    } else if (++seg >= kShadowSegments) {
+                        atomicOr(error, kErrLoopBound);
+                        blocked = true;
+                        end = true;
+                    } else {
+                        o = o + d * adv;
+                        tmax = sub(tmax, adv);
+                        ++segments;
+                        w.init(sc, o, d, kRayEpsilon, tmax, -1);
+                    }
+                }
+            }
+            if (end) {
+                if (!blocked && max_component(tr) > 0) {
+                    const float4 c = rt.sh_c[p], t = rt.sh_t[p];
+                    add_radiance(rt, p, xyz(t) * ((xyz(c) * tr) * c.w));
+                }
+                p = -1;
+                break;
+            }
+        }
+    }
 }
 
 struct ShadeOut {

@@ -5,10 +5,10 @@
 //               queue counters (single thread)
 //   k_generate  turns tickets into camera paths: ticket t -> (request, pixel, sample)
 //               through the admitted requests' ticket ranges (binary search)
-//   k_extend    closest hits of every queued path (mixed depths, requests and scenes);
-//               misses retire
+//   k_extend    closest hits of every queued path (mixed depths, requests and scenes)
+//               by persistent warps with refilling lanes; misses retire
 //   k_shade     per-material shading (the same per-path code as lux_render)
-//   k_shadow    NEE shadow rays
+//   k_shadow    NEE shadow rays (persistent warps with refilling lanes)
 //   k_retire    finished paths add their radiance to their request's film in 64-bit
 //               fixed point (order-independent), count towards completion, and return
 //               their slot to the free list
@@ -75,7 +75,9 @@ struct ServerState {
     int count_mat[kClasses];
     int count_shadow;
     int count_term;
-    int pad1;
+    int extend_next;   // refill cursor of k_extend_s
+    int shadow_next;   // refill cursor of k_shadow_s
+    int pad2;
     unsigned long long rays[2];
 };
 
@@ -106,6 +108,8 @@ __global__ void k_plan(ServerState* st, int cur, int nxt) {
     for (int k = 0; k < kClasses; ++k) st->count_mat[k] = 0;
     st->count_shadow = 0;
     st->count_term = 0;
+    st->extend_next = 0;
+    st->shadow_next = 0;
 }
 
 __global__ void __launch_bounds__(kThreads) k_generate(ServerDev d, int cur) {
@@ -155,26 +159,25 @@ __global__ void __launch_bounds__(kThreads) k_generate(ServerDev d, int cur) {
     }
 }
 
-__global__ void __launch_bounds__(kThreads) k_extend_s(ServerDev d, int cur) {
+__global__ void __launch_bounds__(kThreads) k_extend_s(ServerDev d, int cur, int budget) {
     const int n = d.st->count_ray[cur];
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&d.st->rays[0], static_cast<unsigned long long>(n));
-    const int stride = gridDim.x * blockDim.x;
-    const int rounds = (n + stride - 1) / stride;
-    for (int r = 0; r < rounds; ++r) {
-        int i = r * stride + blockIdx.x * blockDim.x + threadIdx.x;
-        bool active = i < n;
-        int p = active ? d.pool.qray[cur][i] : 0;
-        int cls = -1;
-        if (active) {
-            const ReqSlot& q = d.req[d.req_of[p]];
-            cls = extend_path(d.pool, d.scenes[q.scene], q.light_sampler, p, d.error);
-        }
-        bool hit = cls >= 0;
-        int slot = append(d.st->count_mat, hit ? cls : 0, hit);
-        if (hit) d.pool.qmat[cls * d.pool.capacity + slot] = p;
-        int qt = append(&d.st->count_term, 0, active && !hit);
-        if (qt >= 0) d.qterm[qt] = p;
-    }
+    refill_walks(
+        d.pool, d.pool.qray[cur], n, &d.st->extend_next, budget, d.error,
+        [&](int p) { return d.req_of[p]; },
+        [&](int rs) -> const SceneView& { return d.scenes[d.req[rs].scene]; },
+        [&](int p, int rs, const SceneHit& h) {
+            int cls = -1;
+            if (p >= 0) {
+                const ReqSlot& q = d.req[rs];
+                cls = extend_finish(d.pool, d.scenes[q.scene], q.light_sampler, p, h);
+            }
+            const bool hit = cls >= 0;
+            const int slot = append(d.st->count_mat, hit ? cls : 0, hit);
+            if (hit) d.pool.qmat[cls * d.pool.capacity + slot] = p;
+            const int qt = append(&d.st->count_term, 0, p >= 0 && !hit);
+            if (qt >= 0) d.qterm[qt] = p;
+        });
 }
 
 __global__ void __launch_bounds__(kThreads) k_shade_s(ServerDev d, int cur, int nxt) {
@@ -207,13 +210,12 @@ __global__ void __launch_bounds__(kThreads) k_shade_s(ServerDev d, int cur, int 
     }
 }
 
-__global__ void __launch_bounds__(kThreads) k_shadow_s(ServerDev d) {
-    const int n = d.st->count_shadow;
+__global__ void __launch_bounds__(kThreads) k_shadow_s(ServerDev d, int budget) {
     unsigned long long segments = 0;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        int p = d.pool.qshadow[i];
-        shadow_path(d.pool, d.scenes[d.req[d.req_of[p]].scene], p, d.error, segments);
-    }
+    refill_shadows(
+        d.pool, d.pool.qshadow, d.st->count_shadow, &d.st->shadow_next, budget, d.error,
+        [&](int p) { return d.req_of[p]; },
+        [&](int rs) -> const SceneView& { return d.scenes[d.req[rs].scene]; }, segments);
     warp_add(&d.st->rays[1], segments);
 }
 
@@ -593,6 +595,12 @@ int build_graphs(lux_server* s) {
     d.done = s->d_done;
     d.error = s->ctx->d_error;
     int grid = s->ctx->sm_count * 8;
+    int extend_blocks = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&extend_blocks, k_extend_s, kThreads, 0);
+    const int extend_grid = s->ctx->sm_count * std::max(extend_blocks, 1);
+    int shadow_blocks = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&shadow_blocks, k_shadow_s, kThreads, 0);
+    const int shadow_grid = s->ctx->sm_count * std::max(shadow_blocks, 1);
     cudaStream_t stream = s->ctx->stream;
     for (int cur = 0; cur < 2; ++cur) {
         int nxt = cur ^ 1;
@@ -601,9 +609,9 @@ int build_graphs(lux_server* s) {
         if (err != cudaSuccess) return lux::cuda_fail(err, "graph capture");
         k_plan<<<1, 1, 0, stream>>>(s->st, cur, nxt);
         k_generate<<<grid, kThreads, 0, stream>>>(d, cur);
-        k_extend_s<<<grid, kThreads, 0, stream>>>(d, cur);
+        k_extend_s<<<extend_grid, kThreads, 0, stream>>>(d, cur, s->ctx->path_budget);
         k_shade_s<<<grid, kThreads, 0, stream>>>(d, cur, nxt);
-        k_shadow_s<<<grid, kThreads, 0, stream>>>(d);
+        k_shadow_s<<<shadow_grid, kThreads, 0, stream>>>(d, s->ctx->path_budget);
         k_retire<<<grid, kThreads, 0, stream>>>(d);
         err = cudaStreamEndCapture(stream, &g);
         if (err != cudaSuccess) return lux::cuda_fail(err, "graph capture end");

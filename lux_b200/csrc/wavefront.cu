@@ -30,7 +30,8 @@ namespace lux {
 namespace pt {
 namespace {
 
-constexpr int kSlots = 8;  // per-bounce counters: ray, 5 material queues, shadow
+constexpr int kSlots = 9;  // per-bounce counters: ray, 5 material queues, shadow, extend and
+                           // shadow cursors
 
 struct Runtime {
     PathPool pool;
@@ -74,6 +75,23 @@ __global__ void __launch_bounds__(kThreads) k_extend(PathPool rt, int* counts, S
     }
 }
 
+// k_extend with refilling lanes (refill_walks); the cursor is the bounce's spare slot.
+__global__ void __launch_bounds__(kThreads) k_extend_refill(PathPool rt, int* counts,
+                                                            SceneView sc, int sampler, int depth,
+                                                            int budget, int* error) {
+    int* c = counts + depth * kSlots;
+    int* mat_counts = c + 1;
+    refill_walks(
+        rt, rt.qray[depth & 1], c[0], c + 7, budget, error, [](int) { return 0; },
+        [&](int) -> const SceneView& { return sc; },
+        [&](int p, int, const SceneHit& h) {
+            const int cls = p >= 0 ? extend_finish(rt, sc, sampler, p, h) : -1;
+            const bool hit = cls >= 0;
+            const int slot = append(mat_counts, hit ? cls : 0, hit);
+            if (hit) rt.qmat[cls * rt.capacity + slot] = p;
+        });
+}
+
 __global__ void __launch_bounds__(kThreads) k_shade(PathPool rt, int* counts, SceneView sc,
                                                     int sampler, int depth, int max_depth) {
     const int* mc = counts + depth * kSlots + 1;
@@ -110,6 +128,19 @@ __global__ void __launch_bounds__(kThreads) k_shadow(PathPool rt, int* counts,
     unsigned long long segments = 0;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
         shadow_path(rt, sc, rt.qshadow[i], error, segments);
+    warp_add(rays + 1, segments);
+}
+
+// k_shadow with refilling lanes (refill_shadows); the cursor is the bounce's slot 8.
+__global__ void __launch_bounds__(kThreads) k_shadow_refill(PathPool rt, int* counts,
+                                                            unsigned long long* rays,
+                                                            SceneView sc, int depth, int budget,
+                                                            int* error) {
+    int* c = counts + depth * kSlots;
+    unsigned long long segments = 0;
+    refill_shadows(
+        rt, rt.qshadow, c[6], c + 8, budget, error, [](int) { return 0; },
+        [&](int) -> const SceneView& { return sc; }, segments);
     warp_add(rays + 1, segments);
 }
 
@@ -263,6 +294,18 @@ int render(lux_ctx* ctx, const lux_scene* scene, const lux_render_request& req, 
     const SceneView& sc = scene->view;
     cudaStream_t s = ctx->stream;
     int grid = ctx->sm_count * 8;
+    static int refill_blocks = 0;
+    if (refill_blocks == 0) {
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&refill_blocks, k_extend_refill, kThreads, 0);
+        if (refill_blocks <= 0) refill_blocks = 1;
+    }
+    const int refill_grid = ctx->sm_count * refill_blocks;
+    static int shadow_blocks = 0;
+    if (shadow_blocks == 0) {
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&shadow_blocks, k_shadow_refill, kThreads, 0);
+        if (shadow_blocks <= 0) shadow_blocks = 1;
+    }
+    const int shadow_grid = ctx->sm_count * shadow_blocks;
     cudaError_t err = cudaMemsetAsync(rt.rays, 0, 16, s);
     if (!per_sample && err == cudaSuccess)
         err = cudaMemsetAsync(out, 0, sizeof(float) * 3 * size_t(pixels), s);
@@ -281,11 +324,23 @@ int render(lux_ctx* ctx, const lux_scene* scene, const lux_render_request& req, 
             k_camera<<<grid, kThreads, 0, s>>>(rt.pool, rt.counts, sc, b);
             ctx->launches += 1;
             for (int d = 0; d <= req.max_depth; ++d) {
-                k_extend<<<grid, kThreads, 0, s>>>(rt.pool, rt.counts, sc, req.light_sampler, d,
-                                                   ctx->d_error);
+                if (ctx->trace_variant == kTraceStatic) {
+                    k_extend<<<grid, kThreads, 0, s>>>(rt.pool, rt.counts, sc, req.light_sampler,
+                                                       d, ctx->d_error);
+                } else {
+                    k_extend_refill<<<refill_grid, kThreads, 0, s>>>(
+                        rt.pool, rt.counts, sc, req.light_sampler, d, ctx->path_budget,
+                        ctx->d_error);
+                }
                 k_shade<<<grid, kThreads, 0, s>>>(rt.pool, rt.counts, sc, req.light_sampler, d,
                                                   req.max_depth);
-                k_shadow<<<grid, kThreads, 0, s>>>(rt.pool, rt.counts, rt.rays, sc, d, ctx->d_error);
+                if (ctx->trace_variant == kTraceStatic) {
+                    k_shadow<<<grid, kThreads, 0, s>>>(rt.pool, rt.counts, rt.rays, sc, d,
+                                                       ctx->d_error);
+                } else {
+                    k_shadow_refill<<<shadow_grid, kThreads, 0, s>>>(
+                        rt.pool, rt.counts, rt.rays, sc, d, ctx->path_budget, ctx->d_error);
+                }
                 ctx->launches += 3;
             }
             k_count_rays<<<1, 1, 0, s>>>(rt.counts, rt.rays, req.max_depth + 1);
