@@ -376,6 +376,7 @@ enum lux_request_state {
     LUX_REQ_FAILED = 4
 };
 
+/* scenes: 1 to 64 resident scenes, created on `device`; they must outlive the server. */
 int lux_server_create(int device, lux_scene* const* scenes, int32_t scene_count,
                       const lux_server_options* options, lux_server** out);
 /* Queues a render of scenes[scene]; film_sum (host or device, width*height*3 floats) is

@@ -90,9 +90,30 @@ struct ServerDev {
     const ReqSlot* req;
     const TicketMap* tmap;
     const SceneView* scenes;
+    int scene_count;
     unsigned long long* done;
     int* error;
 };
+
+constexpr int kMaxScenes = 64;
+static_assert(sizeof(SceneView) % 4 == 0, "scene views are staged as words");
+
+// Each kernel first copies the scene table into shared memory (dynamic, scene_count
+// views), so per-path and per-step scene reads are shared-memory reads rather than
+// dependent global loads.
+extern __shared__ __align__(16) unsigned char g_stage[];
+
+LUX_D const SceneView* stage_scenes(const ServerDev& d) {
+    SceneView* dst = reinterpret_cast<SceneView*>(g_stage);
+    const int words = d.scene_count * static_cast<int>(sizeof(SceneView) / 4);
+    const int* src = reinterpret_cast<const int*>(d.scenes);
+    int* out = reinterpret_cast<int*>(dst);
+    for (int i = threadIdx.x; i < words; i += blockDim.x) out[i] = src[i];
+    __syncthreads();
+    return dst;
+}
+
+LUX_HD size_t scene_stage_bytes(int scene_count) { return sizeof(SceneView) * static_cast<size_t>(scene_count); }
 
 __global__ void k_plan(ServerState* st, int cur, int nxt) {
     int free = st->free_count;
@@ -112,7 +133,21 @@ __global__ void k_plan(ServerState* st, int cur, int nxt) {
     st->shadow_next = 0;
 }
 
+// Ticket t of request q is its path idx = t - ticket_start, sample-major: pixel
+// idx % (width * height), sample idx / (width * height).  Consecutive tickets are
+// neighbouring pixels, and one pixel's samples are a frame apart, so retiring paths
+// rarely meet on the same film words.
 __global__ void __launch_bounds__(kThreads) k_generate(ServerDev d, int cur) {
+    const SceneView* scenes = stage_scenes(d);
+    // The ticket map follows the scene table in shared memory.
+    const int tcount = min(d.tmap->count, kMaxRequests);
+    long long* tstart = reinterpret_cast<long long*>(g_stage + scene_stage_bytes(d.scene_count));
+    int* tslot = reinterpret_cast<int*>(tstart + kMaxRequests);
+    for (int k = threadIdx.x; k < tcount; k += blockDim.x) {
+        tstart[k] = d.tmap->start[k];
+        tslot[k] = d.tmap->slot[k];
+    }
+    __syncthreads();
     const int n = d.st->gen_count;
     const int base = d.st->gen_free_base;
     const long long t0 = d.st->gen_ticket;
@@ -123,7 +158,7 @@ __global__ void __launch_bounds__(kThreads) k_generate(ServerDev d, int cur) {
         bool active = i < n;
         bool dead = false;
         int slot = 0;
-        if (active && d.tmap->count <= 0) {  // cannot happen: tickets imply a request
+        if (active && tcount <= 0) {  // cannot happen: tickets imply a request
             slot = d.free_list[base + i];
             d.req_of[slot] = 0;
             d.pool.meta[slot].x = -1;
@@ -132,23 +167,25 @@ __global__ void __launch_bounds__(kThreads) k_generate(ServerDev d, int cur) {
         } else if (active) {
             slot = d.free_list[base + i];
             long long t = t0 + i;
-            int lo = 0, hi = d.tmap->count - 1;
+            int lo = 0, hi = tcount - 1;
             while (lo < hi) {
                 int mid = (lo + hi + 1) >> 1;
-                if (d.tmap->start[mid] <= t) lo = mid;
+                if (tstart[mid] <= t) lo = mid;
                 else hi = mid - 1;
             }
-            int rs = d.tmap->slot[lo];
+            int rs = tslot[lo];
             const ReqSlot& q = d.req[rs];
             long long idx = t - q.ticket_start;
             d.req_of[slot] = rs;
-            if (q.cancelled || idx < 0 || idx >= q.total) {
+            if (q.cancelled || idx < 0 || idx >= q.total || q.scene < 0 ||
+                q.scene >= d.scene_count) {
                 if (!q.cancelled) atomicOr(d.error, kErrLoopBound);
                 d.pool.meta[slot].x = -1;  // no film contribution
                 dead = true;
             } else {
-                init_path(d.pool, d.scenes[q.scene].camera, slot,
-                          static_cast<int>(idx / q.spp), static_cast<int>(idx % q.spp),
+                const long long npix = static_cast<long long>(q.width) * q.height;
+                init_path(d.pool, scenes[q.scene].camera, slot, static_cast<int>(idx % npix),
+                          static_cast<int>(idx / npix),
                           CameraParams{q.width, q.height, q.seed, q.frame_index, q.sample_offset});
             }
         }
@@ -160,17 +197,18 @@ __global__ void __launch_bounds__(kThreads) k_generate(ServerDev d, int cur) {
 }
 
 __global__ void __launch_bounds__(kThreads) k_extend_s(ServerDev d, int cur, int budget) {
+    const SceneView* scenes = stage_scenes(d);
     const int n = d.st->count_ray[cur];
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&d.st->rays[0], static_cast<unsigned long long>(n));
     refill_walks(
         d.pool, d.pool.qray[cur], n, &d.st->extend_next, budget, d.error,
         [&](int p) { return d.req_of[p]; },
-        [&](int rs) -> const SceneView& { return d.scenes[d.req[rs].scene]; },
+        [&](int rs) -> const SceneView& { return scenes[d.req[rs].scene]; },
         [&](int p, int rs, const SceneHit& h) {
             int cls = -1;
             if (p >= 0) {
                 const ReqSlot& q = d.req[rs];
-                cls = extend_finish(d.pool, d.scenes[q.scene], q.light_sampler, p, h);
+                cls = extend_finish(d.pool, scenes[q.scene], q.light_sampler, p, h);
             }
             const bool hit = cls >= 0;
             const int slot = append(d.st->count_mat, hit ? cls : 0, hit);
@@ -182,6 +220,7 @@ __global__ void __launch_bounds__(kThreads) k_extend_s(ServerDev d, int cur, int
 
 __global__ void __launch_bounds__(kThreads) k_shade_s(ServerDev d, int cur, int nxt) {
     (void)cur;
+    const SceneView* scenes = stage_scenes(d);
     int c[kClasses];
     int total = 0;
     for (int k = 0; k < kClasses; ++k) {
@@ -199,7 +238,7 @@ __global__ void __launch_bounds__(kThreads) k_shade_s(ServerDev d, int cur, int 
         ShadeOut o;
         if (active) {
             const ReqSlot& q = d.req[d.req_of[p]];
-            o = shade_path(d.pool, d.scenes[q.scene], q.light_sampler, q.max_depth, p);
+            o = shade_path(d.pool, scenes[q.scene], q.light_sampler, q.max_depth, p);
         }
         int s = append(&d.st->count_shadow, 0, o.shadow);
         if (o.shadow) d.pool.qshadow[s] = p;
@@ -211,11 +250,12 @@ __global__ void __launch_bounds__(kThreads) k_shade_s(ServerDev d, int cur, int 
 }
 
 __global__ void __launch_bounds__(kThreads) k_shadow_s(ServerDev d, int budget) {
+    const SceneView* scenes = stage_scenes(d);
     unsigned long long segments = 0;
     refill_shadows(
         d.pool, d.pool.qshadow, d.st->count_shadow, &d.st->shadow_next, budget, d.error,
         [&](int p) { return d.req_of[p]; },
-        [&](int rs) -> const SceneView& { return d.scenes[d.req[rs].scene]; }, segments);
+        [&](int rs) -> const SceneView& { return scenes[d.req[rs].scene]; }, segments);
     warp_add(&d.st->rays[1], segments);
 }
 
@@ -592,14 +632,19 @@ int build_graphs(lux_server* s) {
     d.req = s->d_req;
     d.tmap = s->d_tmap;
     d.scenes = s->d_scenes;
+    d.scene_count = static_cast<int>(s->scenes.size());
     d.done = s->d_done;
     d.error = s->ctx->d_error;
+    const size_t stage = scene_stage_bytes(d.scene_count);
+    const size_t gen_stage = stage + (sizeof(long long) + sizeof(int)) * kMaxRequests;
+    cudaFuncSetAttribute(k_generate, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         static_cast<int>(gen_stage));
     int grid = s->ctx->sm_count * 8;
     int extend_blocks = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&extend_blocks, k_extend_s, kThreads, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&extend_blocks, k_extend_s, kThreads, stage);
     const int extend_grid = s->ctx->sm_count * std::max(extend_blocks, 1);
     int shadow_blocks = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&shadow_blocks, k_shadow_s, kThreads, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&shadow_blocks, k_shadow_s, kThreads, stage);
     const int shadow_grid = s->ctx->sm_count * std::max(shadow_blocks, 1);
     cudaStream_t stream = s->ctx->stream;
     for (int cur = 0; cur < 2; ++cur) {
@@ -608,10 +653,10 @@ int build_graphs(lux_server* s) {
         cudaError_t err = cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal);
         if (err != cudaSuccess) return lux::cuda_fail(err, "graph capture");
         k_plan<<<1, 1, 0, stream>>>(s->st, cur, nxt);
-        k_generate<<<grid, kThreads, 0, stream>>>(d, cur);
-        k_extend_s<<<extend_grid, kThreads, 0, stream>>>(d, cur, s->ctx->path_budget);
-        k_shade_s<<<grid, kThreads, 0, stream>>>(d, cur, nxt);
-        k_shadow_s<<<shadow_grid, kThreads, 0, stream>>>(d, s->ctx->path_budget);
+        k_generate<<<grid, kThreads, gen_stage, stream>>>(d, cur);
+        k_extend_s<<<extend_grid, kThreads, stage, stream>>>(d, cur, s->ctx->path_budget);
+        k_shade_s<<<grid, kThreads, stage, stream>>>(d, cur, nxt);
+        k_shadow_s<<<shadow_grid, kThreads, stage, stream>>>(d, s->ctx->path_budget);
         k_retire<<<grid, kThreads, 0, stream>>>(d);
         err = cudaStreamEndCapture(stream, &g);
         if (err != cudaSuccess) return lux::cuda_fail(err, "graph capture end");
@@ -662,6 +707,8 @@ int lux_server_create(int device, lux_scene* const* scenes, int32_t scene_count,
     int max_requests = opt.max_requests > 0 ? opt.max_requests : 256;
     if (max_requests > kMaxRequests)
         return server_fail(LUX_ERR_INVALID_ARGUMENT, "max_requests above 1024");
+    if (scene_count > lux::pt::kMaxScenes)
+        return server_fail(LUX_ERR_INVALID_ARGUMENT, "a server holds at most 64 resident scenes");
     for (int i = 0; i < scene_count; ++i)
         if (!scenes[i]) return server_fail(LUX_ERR_INVALID_ARGUMENT, "null scene");
     auto* s = new (std::nothrow) lux_server();
