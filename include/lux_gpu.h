@@ -85,6 +85,22 @@ enum lux_option {
 int lux_ctx_set_option(lux_ctx* ctx, int32_t option, int64_t value);
 int lux_ctx_get_option(lux_ctx* ctx, int32_t option, int64_t* value);
 
+/* ------------------------------------------------------------------ film encoding */
+
+/*
+ * Encodes a film of per-pixel sums (width * height * 3 floats, host or device) the way
+ * the reference's image writers do, into `out` (host or device):
+ *   LUX_FILM_PPM8         bytes of write_ppm (film/ppm.h:37-56): sum / spp, Reinhard,
+ *                         clamp, gamma 1/2.2, x 255.999 truncated; rows top first
+ *   LUX_FILM_PPM8_LINEAR  bytes of write_debug_ppm_linear (film/ppm.h:58-75)
+ *   LUX_FILM_PFM          float32 pixels of write_pfm (film/pfm.h:27-40): sum / spp, rows
+ *                         bottom first
+ * out holds width * height * 3 bytes (PPM) or floats (PFM); headers are the caller's.
+ */
+enum lux_film_format { LUX_FILM_PPM8 = 0, LUX_FILM_PPM8_LINEAR = 1, LUX_FILM_PFM = 2 };
+int lux_film_encode(lux_ctx* ctx, const float* film_sum, int32_t width, int32_t height,
+                    int32_t spp, int32_t format, void* out);
+
 /* ------------------------------------------------------------------ LBVH */
 
 /*

@@ -13,6 +13,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OBJ_DIR = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "liblux_gpu.so")
+CLI = os.path.join(HERE, "lux-render")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
 NVCC_FLAGS = [
@@ -62,6 +63,7 @@ def build(force=False, verbose=False):
     deps = sources + _headers() + [os.path.abspath(__file__)]
     if not force and os.path.exists(LIB):
         if os.path.getmtime(LIB) >= max(os.path.getmtime(p) for p in deps):
+            build_cli()
             return LIB
     with concurrent.futures.ThreadPoolExecutor(max_workers=os.cpu_count() or 4) as pool:
         results = list(pool.map(lambda s: _compile(s, verbose), sources))
@@ -72,7 +74,20 @@ def build(force=False, verbose=False):
     cmd = [NVCC, "-shared", "-gencode", "arch=compute_100a,code=sm_100a", "-o", LIB, *objs,
            "-lcudart"]
     subprocess.run(cmd, check=True)
+    build_cli(force=True)
     return LIB
+
+
+def build_cli(force=False):
+    """The lux-render command line (C++20 over the C ABI), next to the library."""
+    src = os.path.join(HERE, "cli", "lux_render.cpp")
+    if not force and os.path.exists(CLI) and os.path.getmtime(CLI) >= max(
+            os.path.getmtime(src), os.path.getmtime(LIB)):
+        return CLI
+    cmd = ["g++", "-std=c++20", "-O2", "-Wall", "-I", os.path.join(HERE, "..", "include"), src,
+           "-L", HERE, "-llux_gpu", "-Wl,-rpath,$ORIGIN", "-o", CLI]
+    subprocess.run(cmd, check=True)
+    return CLI
 
 
 if __name__ == "__main__":

@@ -142,6 +142,16 @@ class Ref:
                                   seed, light_sampler, y0, y1, threads, out.ctypes.data)
         return out
 
+    def write_image(self, film_sum: np.ndarray, spp: int, path: str, kind: int = 0) -> bytes:
+        """The reference's write_ppm (0), write_debug_ppm_linear (1) or write_pfm (2) on a
+        film of sums (height, width, 3); returns the file's bytes."""
+        h, w = film_sum.shape[:2]
+        f = np.ascontiguousarray(film_sum, np.float32)
+        self.lib.ref_write_image.argtypes = [_P, _I, _I, _I, ctypes.c_char_p, _I]
+        self.lib.ref_write_image(f.ctypes.data, w, h, spp, path.encode(), kind)
+        with open(path, "rb") as fh:
+            return fh.read()
+
     def tree_create(self, prims: np.ndarray, kind: int = 0):
         """Builds and keeps a host tree (build_cpu_lbvh_tree); returns an opaque handle."""
         prims = np.ascontiguousarray(prims, np.float32)

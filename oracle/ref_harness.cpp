@@ -32,6 +32,8 @@
 #include "bvh/cpu_bvh_traversal.h"
 #include "bvh/cpu_lbvh_builder.h"
 #include "camera/pinhole_camera.h"
+#include "film/pfm.h"
+#include "film/ppm.h"
 #include "integrator/cpu_path_tracer.h"
 #include "integrator/render_context.h"
 #include "scene/cornell_box.h"
@@ -444,6 +446,19 @@ int ref_render_scene(const float* tris, int ntri, const int32_t* mids, const flo
             }
         }
     });
+    return 0;
+}
+
+// The reference's own image writers on a film of per-pixel sums: kind 0 write_ppm,
+// 1 write_debug_ppm_linear, 2 write_pfm (film/ppm.h:37-79, film/pfm.h:27-40).
+int ref_write_image(const float* pixels, int width, int height, int spp, const char* path,
+                    int kind) {
+    std::vector<vec3> px(static_cast<size_t>(width) * height);
+    for (size_t i = 0; i < px.size(); ++i)
+        px[i] = vec3(pixels[3 * i], pixels[3 * i + 1], pixels[3 * i + 2]);
+    if (kind == 0) write_ppm(path, px, width, height, spp);
+    else if (kind == 1) write_debug_ppm_linear(path, px, width, height, spp);
+    else write_pfm(path, px, width, height, spp);
     return 0;
 }
 
