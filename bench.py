@@ -570,6 +570,11 @@ def run_batched(args) -> None:
     films_plain = [torch.zeros((r["height"], r["width"], 3), device="cuda") for r in reqs]
     films_batch = [torch.zeros((r["height"], r["width"], 3), device="cuda") for r in reqs]
     rr = [S.request(r["width"], r["height"], r["spp"], r["max_depth"], r["seed"]) for r in reqs]
+    # Autotuned tunables (lux_autotune_render) on a probe of the mixed workload's heaviest
+    # resident scene, used by both the plain path and the server.
+    from lux_b200 import autotune
+    tune = autotune.autotune_render(ctx, scenes[1], S.request(512, 512, 16, 8, 3))
+    path_budget = tune.budget
     # Plain per-request path: lux_render one request after the other, with this build's
     # default 4M-path batches and with the reference scheduler's 65,536-path batches
     # (RenderSettings::batch_size, integrator/render_context.h:18).
@@ -589,9 +594,9 @@ def run_batched(args) -> None:
         return rays, e0.elapsed_time(e1) * 1e-3
 
     ref_rays, ref_s = plain_pass(65536) if not args.skip_reference_batch else (0, float("nan"))
-    plain_rays, plain_s = plain_pass(1 << 22)
+    plain_rays, plain_s = plain_pass(max(tune.render_batch, 1 << 22))
     # Batched: one server, all requests submitted at once.
-    with SV.Server(scenes, pool_paths=args.pool) as srv:
+    with SV.Server(scenes, pool_paths=args.pool, path_budget=path_budget) as srv:
         warm, _ = srv.submit(0, S.request(64, 64, 4, 4, 1))
         srv.wait(warm)
         base = srv.stats()
@@ -612,7 +617,9 @@ def run_batched(args) -> None:
                                    " spp log-uniform 16..256, depth uniform 4..12, seed 11; scenes:"
                                    " Cornell, displaced icosphere + glass (332,836 tris),"
                                    " 2,097,152-tri soup, 16x16 icosphere grid",
-                       "pool_paths": args.pool},
+                       "pool_paths": args.pool,
+                       "autotuned": {"trace_variant": tune.trace_variant, "path_budget": tune.budget,
+                                     "render_batch": tune.render_batch}},
             "plain_per_request": {"value": plain_rays / plain_s / 1e6, "unit": "Mrays/s",
                                   "seconds": plain_s, "rays": plain_rays,
                                   "batch_paths": 1 << 22},

@@ -85,6 +85,26 @@ enum lux_option {
 int lux_ctx_set_option(lux_ctx* ctx, int32_t option, int64_t value);
 int lux_ctx_get_option(lux_ctx* ctx, int32_t option, int64_t* value);
 
+/*
+ * Autotuner (no reference counterpart): times candidate settings on the caller's own
+ * workload, keeps the fastest in the context and reports it.  Tunables never change
+ * results.  lux_autotune_trace: LUX_OPT_TRACE_VARIANT x LUX_OPT_TRACE_BUDGET on n
+ * closest-hit rays (device pointer, the lux_trace_closest layout) against `bvh`.
+ * lux_autotune_render: one thread per path vs refilling lanes x LUX_OPT_PATH_BUDGET x
+ * LUX_OPT_RENDER_BATCH on a probe render of `scene` (use a probe the size of the real
+ * renders).  default_ms is the time with the options in effect before tuning.
+ */
+typedef struct lux_tune_result {
+    int32_t trace_variant;
+    int32_t budget;
+    int64_t render_batch;     /* 0 for ray-query tuning */
+    float best_ms;
+    float default_ms;
+    int32_t candidates;
+} lux_tune_result;
+int lux_autotune_trace(lux_ctx* ctx, lux_bvh* bvh, const float* rays, int32_t n,
+                       lux_tune_result* out);
+
 /* ------------------------------------------------------------------ film encoding */
 
 /*
@@ -348,6 +368,9 @@ int lux_scene_update_mesh(lux_ctx* ctx, lux_scene* scene, int32_t mesh, const fl
  */
 int lux_render(lux_ctx* ctx, const lux_scene* scene, const lux_render_request* req,
                float* film_sum);
+/* Autotuner of the path tracer's tunables on a probe render (see lux_autotune_trace). */
+int lux_autotune_render(lux_ctx* ctx, const lux_scene* scene, const lux_render_request* probe,
+                        lux_tune_result* out);
 
 /* Same paths, but every sample's radiance is written: samples[(pixel*spp + s)*3 + c]
  * (pixel = y*width + x).  For validation against per-sample reference values. */
@@ -382,6 +405,7 @@ typedef struct lux_server_options {
     int64_t pool_paths;            /* paths in flight; 0: 4,194,304 */
     int64_t memory_budget_bytes;   /* pool + request films; 0: 120 GiB */
     int32_t max_requests;          /* requests admitted at once; 0: 256 */
+    int32_t path_budget;           /* LUX_OPT_PATH_BUDGET of the server's kernels; 0: 32 */
 } lux_server_options;
 
 enum lux_request_state {

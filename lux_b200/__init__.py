@@ -64,6 +64,8 @@ SIGNATURES = {
     "lux_bvh_attach_triangles": (ctypes.c_int, [_P, _P, _P, _I32]),
     "lux_bvh_info": (ctypes.c_int, [_P, _P, _P, _P, _P, _P]),
     "lux_bvh_download": (ctypes.c_int, [_P, _P, _P, _P, _P, _P, _P]),
+    "lux_autotune_trace": (ctypes.c_int, [_P, _P, _P, _I32, _P]),
+    "lux_autotune_render": (ctypes.c_int, [_P, _P, _P, _P]),
     "lux_film_encode": (ctypes.c_int, [_P, _P, _I32, _I32, _I32, _I32, _P]),
     "lux_bvh_validate_structure": (ctypes.c_int, [_P, _P, _P, _P, _I32]),
     "lux_bvh_validate_primitives": (ctypes.c_int, [_P, _P, _P, _I32, _P, _P, _I32]),

@@ -718,6 +718,7 @@ int lux_server_create(int device, lux_scene* const* scenes, int32_t scene_count,
         delete s;
         return st;
     }
+    if (opt.path_budget > 0) s->ctx->path_budget = std::min(opt.path_budget, 4096);
     s->scenes.assign(scenes, scenes + scene_count);
     s->max_requests = max_requests;
     s->budget = opt.memory_budget_bytes > 0 ? opt.memory_budget_bytes : (int64_t(120) << 30);

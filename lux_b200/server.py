@@ -14,17 +14,17 @@ QUEUED, RUNNING, DONE, CANCELLED, FAILED = range(5)
 
 class ServerOptions(ctypes.Structure):
     _fields_ = [("pool_paths", ctypes.c_int64), ("memory_budget_bytes", ctypes.c_int64),
-                ("max_requests", ctypes.c_int32)]
+                ("max_requests", ctypes.c_int32), ("path_budget", ctypes.c_int32)]
 
 
 class Server:
     def __init__(self, scenes: list[Scene], device: int = 0, pool_paths: int = 0,
-                 memory_budget_bytes: int = 0, max_requests: int = 0):
+                 memory_budget_bytes: int = 0, max_requests: int = 0, path_budget: int = 0):
         lib = load_library()
         self._lib = lib
         self.scenes = list(scenes)  # keep the scenes alive
         arr = (ctypes.c_void_p * len(scenes))(*[s.handle.value for s in scenes])
-        opts = ServerOptions(pool_paths, memory_budget_bytes, max_requests)
+        opts = ServerOptions(pool_paths, memory_budget_bytes, max_requests, path_budget)
         h = ctypes.c_void_p()
         _check(lib.lux_server_create(device, arr, len(scenes), ctypes.byref(opts), ctypes.byref(h)))
         self._h = h

@@ -349,3 +349,23 @@ def test_wide_walk_exact_on_degenerate_extents(ctx, oracle, case):
         assert np.array_equal(got[0], want[0]) and np.array_equal(got[1], want[1])
         got_a = _with_variant(ctx, variant, lambda: bvh.trace_any(rays))
         assert np.array_equal(got_a, _with_variant(ctx, 1, lambda: bvh.trace_any(rays)))
+
+
+def test_autotune_trace_keeps_results_and_picks_a_candidate(ctx):
+    import torch
+    from lux_b200 import autotune
+    tris = W.soup_triangles(200_000, seed=51)
+    rays = W.uniform_rays(100_000, seed=52)
+    bvh = ctx.build_lbvh(tris)
+    before = bvh.trace_closest(rays)
+    variant0 = ctx.get_option(lux_b200.OPT_TRACE_VARIANT)
+    budget0 = ctx.get_option(lux_b200.OPT_TRACE_BUDGET)
+    try:
+        res = autotune.autotune_trace(ctx, bvh, torch.from_numpy(rays).cuda())
+        assert res.candidates >= 5 and res.best_ms <= res.default_ms
+        assert ctx.get_option(lux_b200.OPT_TRACE_VARIANT) == res.trace_variant
+        after = bvh.trace_closest(rays)
+        assert np.array_equal(after[0], before[0]) and np.array_equal(after[1], before[1])
+    finally:
+        ctx.set_option(lux_b200.OPT_TRACE_VARIANT, variant0)
+        ctx.set_option(lux_b200.OPT_TRACE_BUDGET, budget0)

@@ -261,3 +261,20 @@ def test_heavy_config_crop_is_unbiased_against_fp64_oracle(ctx):
     rel_rmse, ratio = _fp64_check(film[y0:y1, x0:x1], g, 64)
     assert 0.8 < ratio < 1.25, ratio
     assert rel_rmse < 0.3, rel_rmse
+
+
+def test_autotune_render_keeps_the_image(ctx):
+    from lux_b200 import autotune
+    from lux_b200 import scenes as SC
+    sc = S.Scene(ctx, SC.heavy_render_scene(96, 96))
+    req = S.request(96, 96, 8, 6, 2)
+    want = S.render(ctx, sc, req)
+    saved = [ctx.get_option(o) for o in (1, 3, 4)]
+    try:
+        res = autotune.autotune_render(ctx, sc, req)
+        assert res.candidates >= 6 and res.best_ms <= res.default_ms
+        assert ctx.get_option(lux_b200.OPT_PATH_BUDGET) == res.budget
+        assert np.array_equal(S.render(ctx, sc, req), want)
+    finally:
+        for o, v in zip((1, 3, 4), saved):
+            ctx.set_option(o, v)
