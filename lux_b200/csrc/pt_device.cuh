@@ -185,6 +185,7 @@ struct SceneView {
     int light_sampler;               // 0 uniform, 1 power
     const int* primitive_light;      // scene triangle -> light index (-1 none, -2 several)
     bool has_two_level;
+    bool has_passthrough;            // some material is an interface or transparent filter
     Camera camera;
 };
 

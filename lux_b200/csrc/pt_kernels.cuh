@@ -279,8 +279,11 @@ struct TwoLevelWalk {
     f3 lo, ld;
     slab_ray lsr;
     bool done;
+    bool any_hit;                 // end at the first accepted triangle (occlusion only)
 
-    LUX_D void init(const SceneView& sc, f3 ro, f3 rd, float rtmin, float rtmax, int ignored) {
+    LUX_D void init(const SceneView& sc, f3 ro, f3 rd, float rtmin, float rtmax, int ignored,
+                    bool first_hit = false) {
+        any_hit = first_hit;
         o = ro;
         d = rd;
         tmin = rtmin;
@@ -380,6 +383,10 @@ struct TwoLevelWalk {
                         hit.t = t;
                         hit.u = u;
                         hit.v = v;
+                        if (any_hit) {
+                            done = true;
+                            return true;
+                        }
                     }
                 }
             }
@@ -784,7 +791,9 @@ LUX_D void refill_walks(const PathPool& rt, const int* q, int n, int* next_item,
 // Shadow rays of the paths in queue q[0, n) by persistent warps with refilling lanes:
 // each lane walks its ray's segments through pass-through surfaces exactly as
 // shadow_path does (the same segment loop, one resumable walk per segment) and adds the
-// NEE contribution when the ray is not blocked.
+// NEE contribution when the ray is not blocked.  In a scene without pass-through
+// materials the first hit already blocks the ray, and a hit exists exactly when a
+// closest hit does, so the walk ends at the first accepted triangle.
 template <typename TagOf, typename View>
 LUX_D void refill_shadows(const PathPool& rt, const int* q, int n, int* next_item, int budget,
                           int* error, TagOf tag_of, View view, unsigned long long& segments) {
@@ -819,7 +828,8 @@ LUX_D void refill_shadows(const PathPool& rt, const int* q, int n, int* next_ite
                     tr = splat(1.0f);
                     seg = 0;
                     ++segments;
-                    w.init(view(tag), o, d, kRayEpsilon, tmax, __float_as_int(b.w));
+                    const SceneView& sv = view(tag);
+                    w.init(sv, o, d, kRayEpsilon, tmax, __float_as_int(b.w), !sv.has_passthrough);
                 }
             }
         }

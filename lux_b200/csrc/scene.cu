@@ -468,6 +468,10 @@ int scene_create(lux_ctx* ctx, const lux_scene_desc* d, lux_scene** out) {
     v.light_sampler = 1;
     v.primitive_light = s->primitive_light;
     v.has_two_level = s->tlas->n > 0 && d->instance_count > 0;
+    v.has_passthrough = false;
+    for (int i = 0; i < d->material_count; ++i)
+        v.has_passthrough = v.has_passthrough || d->materials[i].type == pt::kInterface ||
+                            d->materials[i].type == pt::kTransparent;
     const lux_camera_desc& c = d->camera;
     v.camera.origin = make_f3(c.origin[0], c.origin[1], c.origin[2]);
     v.camera.lower_left = make_f3(c.lower_left[0], c.lower_left[1], c.lower_left[2]);
