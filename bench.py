@@ -188,6 +188,23 @@ def run_reference(args) -> None:
 
 # ------------------------------------------------------------------ GPU arm
 
+def max_over_ranks(value: float, dist, device) -> float:
+    """The largest per-rank value: a multi-GPU step lasts as long as its slowest rank.
+    Works with any process group (NCCL on GPUs; the CPU tests use gloo)."""
+    if dist is None:
+        return value
+    import torch
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(units_per_rank: int, world: int, step_ms: float) -> float:
+    """Whole-job throughput in millions of units per second: every rank processes the
+    same units per step (replicas), timed by the slowest rank."""
+    return world * units_per_rank / (step_ms * 1e-3) / 1e6
+
+
 def run_lux(args) -> None:
     import torch
 
@@ -285,11 +302,8 @@ def run_lux(args) -> None:
             per_phase[p].append(e[i].elapsed_time(e[i + 1]))
         totals.append(e[0].elapsed_time(e[5]))
     step_ms = float(np.sum(totals)) / args.steps
-    if dist:
-        t = torch.tensor([step_ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        step_ms = float(t.item())
-    value = world * N_RAYS / (step_ms * 1e-3) / 1e6
+    step_ms = max_over_ranks(step_ms, dist, dev)
+    value = whole_job_rate(N_RAYS, world, step_ms)
     phase_ms = {p: float(np.mean(v)) for p, v in per_phase.items()}
 
     # Roofline of the dominant kernel (the traversal: one launch per trace phase).
