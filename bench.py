@@ -479,6 +479,10 @@ def run_render(args, name: str) -> None:
     from lux_b200 import scenes as SC
 
     W, H, spp, depth, seed, metric, workload = RENDER_CONFIGS[name]
+    if args.render_size or args.render_spp:  # reduced profiling case of the same scene
+        W = H = args.render_size or W
+        spp = args.render_spp or spp
+        workload = f"{workload} (reduced profiling case: {W}x{H}, {spp} spp)"
     builder = S.make_cornell_scene(W, H) if name == "cornell" else SC.heavy_render_scene(W, H)
     sc = S.Scene(ctx, builder)
     req = S.request(W, H, spp, depth, seed)
@@ -541,7 +545,7 @@ def run_render(args, name: str) -> None:
     fp64 = None
     fixture = os.path.join(os.path.dirname(os.path.abspath(__file__)), "tests", "golden",
                            f"{name}_fp64.npz")
-    if os.path.exists(fixture):
+    if os.path.exists(fixture) and not (args.render_size or args.render_spp):
         g = np.load(fixture)
         x0, y0, x1, y1 = (int(v) for v in g["rect"]) if "rect" in g else (0, 0, W, H)
         img = film.double().cpu().numpy()[y0:y1, x0:x1] / spp
@@ -763,6 +767,10 @@ def main():
                     help="lbvh: the LBVH microbench (default); cornell: config 1; heavy: config 3; "
                          "batched: config 4; serving: config 5")
     ap.add_argument("--rates", default="10,50,100,200,500")
+    ap.add_argument("--render-size", type=int, default=0,
+                    help="cornell/heavy: film side override (profiling cases only)")
+    ap.add_argument("--render-spp", type=int, default=0,
+                    help="cornell/heavy: samples per pixel override (profiling cases only)")
     ap.add_argument("--budget-gb", type=float, default=120.0,
                     help="serving: device-memory admission budget for queues and films")
     ap.add_argument("--request-scale", type=float, default=0.25,
