@@ -632,6 +632,18 @@ LUX_D void add_radiance(const PathPool& rt, int p, f3 v) {
     rt.rad[p] = make_float4(add(r.x, v.x), add(r.y, v.y), add(r.z, v.z), 0.0f);
 }
 
+// Moves path p's state (everything but the per-bounce hit and shadow records) from pool
+// src to slot q of pool dst.
+LUX_D void copy_path(const PathPool& src, int p, const PathPool& dst, int q) {
+    dst.thr_eta[q] = src.thr_eta[p];
+    dst.rad[q] = src.rad[p];
+    dst.prev[q] = src.prev[p];
+    dst.meta[q] = src.meta[p];
+    dst.rng[q] = src.rng[p];
+    dst.ray_o[q] = src.ray_o[p];
+    dst.ray_d[q] = src.ray_d[p];
+}
+
 LUX_D int material_of(const SceneView& sc, int prim) {
     return __float_as_int(__ldg(&sc.tris[prim].v0.w));
 }
@@ -738,7 +750,8 @@ LUX_D int extend_path(const PathPool& rt, const SceneView& sc, int sampler, int 
     return extend_finish(rt, sc, sampler, p, h);
 }
 
-// Closest hits of the paths in queue q[0, n) by persistent warps: each lane advances its
+// Closest hits of the paths in queue q[0, n) (q null: paths 0..n-1) by persistent warps:
+// each lane advances its
 // walk by at most `budget` steps per round, and lanes whose walk finished hand it to
 // finish() and take the next path through one warp-aggregated atomic on *next_item, so
 // lanes do not idle behind the longest walk of a static warp.  tag_of(p) picks a path's
@@ -767,7 +780,7 @@ LUX_D void refill_walks(const PathPool& rt, const int* q, int n, int* next_item,
                 if (idx >= n) {
                     p = -2;
                 } else {
-                    p = q[idx];
+                    p = q ? q[idx] : idx;
                     tag = tag_of(p);
                     const float4 a = rt.ray_o[p];
                     const float4 b = rt.ray_d[p];
@@ -793,10 +806,12 @@ LUX_D void refill_walks(const PathPool& rt, const int* q, int n, int* next_item,
 // shadow_path does (the same segment loop, one resumable walk per segment) and adds the
 // NEE contribution when the ray is not blocked.  In a scene without pass-through
 // materials the first hit already blocks the ray, and a hit exists exactly when a
-// closest hit does, so the walk ends at the first accepted triangle.
-template <typename TagOf, typename View>
+// closest hit does, so the walk ends at the first accepted triangle.  deposit(p, value)
+// adds the contribution to wherever path p's radiance lives.
+template <typename TagOf, typename View, typename Deposit>
 LUX_D void refill_shadows(const PathPool& rt, const int* q, int n, int* next_item, int budget,
-                          int* error, TagOf tag_of, View view, unsigned long long& segments) {
+                          int* error, TagOf tag_of, View view, Deposit deposit,
+                          unsigned long long& segments) {
     const unsigned lane = threadIdx.x & 31;
     const unsigned lt = lanemask_lt();
     int p = -1;  // >= 0 active path, -1 needs one, -2 none left
@@ -867,7 +882,7 @@ LUX_D void refill_shadows(const PathPool& rt, const int* q, int n, int* next_ite
             if (end) {
                 if (!blocked && max_component(tr) > 0) {
                     const float4 c = rt.sh_c[p], t = rt.sh_t[p];
-                    add_radiance(rt, p, xyz(t) * ((xyz(c) * tr) * c.w));
+                    deposit(p, xyz(t) * ((xyz(c) * tr) * c.w));
                 }
                 p = -1;
                 break;

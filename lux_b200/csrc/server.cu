@@ -1,8 +1,12 @@
 // Render server: batched / continuous multi-request path tracing over resident scenes.
 //
-// One persistent path pool of P slots.  Each pool iteration (one CUDA graph launch):
-//   k_plan      pops min(free slots, unissued tickets) slots; resets this iteration's
-//               queue counters (single thread)
+// Two path pools of P slots that alternate between iterations: an iteration's live paths
+// occupy slots [0, live) of its pool, new camera paths are appended after them, and
+// shading moves each continuing path to the next free slot of the other pool, so every
+// stage reads path state in nearly slot order.  Each pool iteration (one CUDA graph
+// launch):
+//   k_plan      issues min(free slots, unissued tickets) tickets; resets this
+//               iteration's queue counters (single thread)
 //   k_generate  turns tickets into camera paths: ticket t -> (request, pixel, sample)
 //               through the admitted requests' ticket ranges (binary search)
 //   k_extend    closest hits of every queued path (mixed depths, requests and scenes)
@@ -10,8 +14,7 @@
 //   k_shade     per-material shading (the same per-path code as lux_render)
 //   k_shadow    NEE shadow rays (persistent warps with refilling lanes)
 //   k_retire    finished paths add their radiance to their request's film in 64-bit
-//               fixed point (order-independent), count towards completion, and return
-//               their slot to the free list
+//               fixed point (order-independent) and count towards completion
 // Tickets enumerate each request's paths pixel-major (pixel = idx / spp), so the random
 // numbers of a path depend only on (request seed, pixel, sample): a request renders the
 // same whether alone or mixed.  The host worker thread admits requests by memory budget,
@@ -64,10 +67,10 @@ struct TicketMap {
 };
 
 struct ServerState {
-    int free_count;
-    int gen_count;
-    int gen_free_base;
-    int pad0;
+    int live;          // live paths in this iteration's pool, slots [0, live)
+    int live_next;     // continuing paths appended to the other pool
+    int gen_count;     // tickets issued this iteration
+    int gen_live;      // of which started paths (slots live + [0, gen_live))
     long long gen_ticket;
     long long next_ticket;
     long long ticket_limit;
@@ -82,10 +85,11 @@ struct ServerState {
 };
 
 struct ServerDev {
-    PathPool pool;
-    int* req_of;
+    PathPool pool[2];  // path state alternates between the two; queues, hit and shadow
+                       // records are shared (pool[1] aliases pool[0]'s)
+    int* req_of[2];    // request slot of each path, per pool
+    int* sh_dest;      // where a shadow ray's path now lives: 2 * slot + (1: other pool)
     int* qterm;
-    int* free_list;
     ServerState* st;
     const ReqSlot* req;
     const TicketMap* tmap;
@@ -115,17 +119,17 @@ LUX_D const SceneView* stage_scenes(const ServerDev& d) {
 
 LUX_HD size_t scene_stage_bytes(int scene_count) { return sizeof(SceneView) * static_cast<size_t>(scene_count); }
 
-__global__ void k_plan(ServerState* st, int cur, int nxt) {
-    int free = st->free_count;
+__global__ void k_plan(ServerState* st, int capacity) {
+    const int live = st->live_next;  // the previous iteration's continuing paths
+    st->live = live;
+    st->live_next = 0;
     long long avail = st->ticket_limit - st->next_ticket;
     if (avail < 0) avail = 0;
-    int n = static_cast<int>(min(static_cast<long long>(free), avail));
+    const int n = static_cast<int>(min(static_cast<long long>(capacity - live), avail));
     st->gen_count = n;
-    st->gen_free_base = free - n;
-    st->free_count = free - n;
+    st->gen_live = 0;
     st->gen_ticket = st->next_ticket;
     st->next_ticket += n;
-    st->count_ray[nxt] = 0;
     for (int k = 0; k < kClasses; ++k) st->count_mat[k] = 0;
     st->count_shadow = 0;
     st->count_term = 0;
@@ -149,78 +153,87 @@ __global__ void __launch_bounds__(kThreads) k_generate(ServerDev d, int cur) {
     }
     __syncthreads();
     const int n = d.st->gen_count;
-    const int base = d.st->gen_free_base;
+    const int live = d.st->live;
     const long long t0 = d.st->gen_ticket;
+    const PathPool& pool = d.pool[cur];
     const int stride = gridDim.x * blockDim.x;
     const int rounds = (n + stride - 1) / stride;
     for (int r = 0; r < rounds; ++r) {
-        int i = r * stride + blockIdx.x * blockDim.x + threadIdx.x;
-        bool active = i < n;
+        const int i = r * stride + blockIdx.x * blockDim.x + threadIdx.x;
+        const bool active = i < n;
         bool dead = false;
-        int slot = 0;
+        int rs = -1;
+        long long idx = 0;
         if (active && tcount <= 0) {  // cannot happen: tickets imply a request
-            slot = d.free_list[base + i];
-            d.req_of[slot] = 0;
-            d.pool.meta[slot].x = -1;
             atomicOr(d.error, kErrLoopBound);
-            dead = true;
         } else if (active) {
-            slot = d.free_list[base + i];
-            long long t = t0 + i;
+            const long long t = t0 + i;
             int lo = 0, hi = tcount - 1;
             while (lo < hi) {
                 int mid = (lo + hi + 1) >> 1;
                 if (tstart[mid] <= t) lo = mid;
                 else hi = mid - 1;
             }
-            int rs = tslot[lo];
+            rs = tslot[lo];
             const ReqSlot& q = d.req[rs];
-            long long idx = t - q.ticket_start;
-            d.req_of[slot] = rs;
+            idx = t - q.ticket_start;
             if (q.cancelled || idx < 0 || idx >= q.total || q.scene < 0 ||
                 q.scene >= d.scene_count) {
                 if (!q.cancelled) atomicOr(d.error, kErrLoopBound);
-                d.pool.meta[slot].x = -1;  // no film contribution
-                dead = true;
-            } else {
-                const long long npix = static_cast<long long>(q.width) * q.height;
-                init_path(d.pool, scenes[q.scene].camera, slot, static_cast<int>(idx % npix),
-                          static_cast<int>(idx / npix),
-                          CameraParams{q.width, q.height, q.seed, q.frame_index, q.sample_offset});
+                dead = true;  // counts towards completion, contributes nothing
             }
         }
-        int qr = append(&d.st->count_ray[cur], 0, active && !dead);
-        if (qr >= 0) d.pool.qray[cur][qr] = slot;
-        int qt = append(&d.st->count_term, 0, active && dead);
-        if (qt >= 0) d.qterm[qt] = slot;
+        const bool start = active && rs >= 0 && !dead;
+        const int slot = append(&d.st->gen_live, 0, start);
+        if (start) {
+            const ReqSlot& q = d.req[rs];
+            const long long npix = static_cast<long long>(q.width) * q.height;
+            init_path(pool, scenes[q.scene].camera, live + slot, static_cast<int>(idx % npix),
+                      static_cast<int>(idx / npix),
+                      CameraParams{q.width, q.height, q.seed, q.frame_index, q.sample_offset});
+            d.req_of[cur][live + slot] = rs;
+        }
+        // Tickets of cancelled requests are done at once (one atomic per warp and request).
+        const bool skip = active && rs >= 0 && dead;
+        const unsigned mask = __ballot_sync(0xffffffffu, skip);
+        if (skip) {
+            const unsigned peers = __match_any_sync(mask, rs);
+            if (static_cast<int>(threadIdx.x & 31) == __ffs(peers) - 1)
+                atomicAdd(d.done + rs, static_cast<unsigned long long>(__popc(peers)));
+        }
     }
 }
 
 __global__ void __launch_bounds__(kThreads) k_extend_s(ServerDev d, int cur, int budget) {
     const SceneView* scenes = stage_scenes(d);
-    const int n = d.st->count_ray[cur];
+    const int n = d.st->live + d.st->gen_live;  // slots [0, n) of this iteration's pool
+    const PathPool& pool = d.pool[cur];
+    const int* req_of = d.req_of[cur];
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&d.st->rays[0], static_cast<unsigned long long>(n));
     refill_walks(
-        d.pool, d.pool.qray[cur], n, &d.st->extend_next, budget, d.error,
-        [&](int p) { return d.req_of[p]; },
+        pool, nullptr, n, &d.st->extend_next, budget, d.error,
+        [&](int p) { return req_of[p]; },
         [&](int rs) -> const SceneView& { return scenes[d.req[rs].scene]; },
         [&](int p, int rs, const SceneHit& h) {
             int cls = -1;
             if (p >= 0) {
                 const ReqSlot& q = d.req[rs];
-                cls = extend_finish(d.pool, scenes[q.scene], q.light_sampler, p, h);
+                cls = extend_finish(pool, scenes[q.scene], q.light_sampler, p, h);
             }
             const bool hit = cls >= 0;
             const int slot = append(d.st->count_mat, hit ? cls : 0, hit);
-            if (hit) d.pool.qmat[cls * d.pool.capacity + slot] = p;
+            if (hit) pool.qmat[cls * pool.capacity + slot] = p;
             const int qt = append(&d.st->count_term, 0, p >= 0 && !hit);
             if (qt >= 0) d.qterm[qt] = p;
         });
 }
 
-__global__ void __launch_bounds__(kThreads) k_shade_s(ServerDev d, int cur, int nxt) {
-    (void)cur;
+// Shading in place; a path that continues moves to the other pool at the next
+// appended slot, so the next iteration reads its paths in slot order.
+__global__ void __launch_bounds__(kThreads) k_shade_s(ServerDev d, int cur) {
     const SceneView* scenes = stage_scenes(d);
+    const int nxt = cur ^ 1;
+    const PathPool& pool = d.pool[cur];
     int c[kClasses];
     int total = 0;
     for (int k = 0; k < kClasses; ++k) {
@@ -230,32 +243,44 @@ __global__ void __launch_bounds__(kThreads) k_shade_s(ServerDev d, int cur, int 
     const int stride = gridDim.x * blockDim.x;
     const int rounds = (total + stride - 1) / stride;
     for (int r = 0; r < rounds; ++r) {
-        int i = r * stride + blockIdx.x * blockDim.x + threadIdx.x;
-        bool active = i < total;
+        const int i = r * stride + blockIdx.x * blockDim.x + threadIdx.x;
+        const bool active = i < total;
         int cls = 0, j = i;
         while (cls < kClasses - 1 && j >= c[cls]) j -= c[cls++];
-        int p = active ? d.pool.qmat[cls * d.pool.capacity + j] : 0;
+        const int p = active ? pool.qmat[cls * pool.capacity + j] : 0;
+        const int rs = active ? d.req_of[cur][p] : 0;
         ShadeOut o;
         if (active) {
-            const ReqSlot& q = d.req[d.req_of[p]];
-            o = shade_path(d.pool, scenes[q.scene], q.light_sampler, q.max_depth, p);
+            const ReqSlot& q = d.req[rs];
+            o = shade_path(pool, scenes[q.scene], q.light_sampler, q.max_depth, p);
         }
-        int s = append(&d.st->count_shadow, 0, o.shadow);
-        if (o.shadow) d.pool.qshadow[s] = p;
-        s = append(&d.st->count_ray[nxt], 0, o.spawn);
-        if (o.spawn) d.pool.qray[nxt][s] = p;
-        s = append(&d.st->count_term, 0, active && !o.spawn);
-        if (s >= 0) d.qterm[s] = p;
+        const int s = append(&d.st->count_shadow, 0, o.shadow);
+        if (o.shadow) pool.qshadow[s] = p;
+        const int q = append(&d.st->live_next, 0, o.spawn);
+        if (o.spawn) {
+            copy_path(pool, p, d.pool[nxt], q);
+            d.req_of[nxt][q] = rs;
+        }
+        if (active) d.sh_dest[p] = o.spawn ? 2 * q + 1 : 2 * p;
+        const int t = append(&d.st->count_term, 0, active && !o.spawn);
+        if (t >= 0) d.qterm[t] = p;
     }
 }
 
-__global__ void __launch_bounds__(kThreads) k_shadow_s(ServerDev d, int budget) {
+__global__ void __launch_bounds__(kThreads) k_shadow_s(ServerDev d, int cur, int budget) {
     const SceneView* scenes = stage_scenes(d);
+    const PathPool& pool = d.pool[cur];
+    const int* req_of = d.req_of[cur];
     unsigned long long segments = 0;
     refill_shadows(
-        d.pool, d.pool.qshadow, d.st->count_shadow, &d.st->shadow_next, budget, d.error,
-        [&](int p) { return d.req_of[p]; },
-        [&](int rs) -> const SceneView& { return scenes[d.req[rs].scene]; }, segments);
+        pool, pool.qshadow, d.st->count_shadow, &d.st->shadow_next, budget, d.error,
+        [&](int p) { return req_of[p]; },
+        [&](int rs) -> const SceneView& { return scenes[d.req[rs].scene]; },
+        [&](int p, f3 v) {
+            const int dest = d.sh_dest[p];
+            add_radiance(d.pool[cur ^ (dest & 1)], dest >> 1, v);
+        },
+        segments);
     warp_add(&d.st->rays[1], segments);
 }
 
@@ -264,7 +289,8 @@ LUX_D unsigned long long to_fixed(float v) {
     return static_cast<unsigned long long>(__float2ll_rn(v * kFixedScale));
 }
 
-__global__ void __launch_bounds__(kThreads) k_retire(ServerDev d) {
+__global__ void __launch_bounds__(kThreads) k_retire(ServerDev d, int cur) {
+    const PathPool& pool = d.pool[cur];
     const int n = d.st->count_term;
     const int stride = gridDim.x * blockDim.x;
     const int rounds = (n + stride - 1) / stride;
@@ -272,12 +298,12 @@ __global__ void __launch_bounds__(kThreads) k_retire(ServerDev d) {
         int i = r * stride + blockIdx.x * blockDim.x + threadIdx.x;
         bool active = i < n;
         int p = active ? d.qterm[i] : 0;
-        int rs = active ? d.req_of[p] : -1;
+        int rs = active ? d.req_of[cur][p] : -1;
         if (active) {
             const ReqSlot& q = d.req[rs];
-            int pixel = d.pool.meta[p].x;
+            int pixel = pool.meta[p].x;
             if (!q.cancelled && pixel >= 0 && pixel < q.width * q.height) {
-                float4 rad = d.pool.rad[p];
+                float4 rad = pool.rad[p];
                 unsigned long long* f = q.film + 3 * static_cast<size_t>(pixel);
                 atomicAdd(f, to_fixed(rad.x));
                 atomicAdd(f + 1, to_fixed(rad.y));
@@ -291,14 +317,7 @@ __global__ void __launch_bounds__(kThreads) k_retire(ServerDev d) {
             if (static_cast<int>(threadIdx.x & 31) == __ffs(peers) - 1)
                 atomicAdd(d.done + rs, static_cast<unsigned long long>(__popc(peers)));
         }
-        int s = append(&d.st->free_count, 0, active);
-        if (s >= 0) d.free_list[s] = p;
     }
-}
-
-__global__ void k_init_free(int* free_list, int n) {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-        free_list[i] = i;
 }
 
 __global__ void k_fixed_to_float(const unsigned long long* film, float* out, size_t n) {
@@ -346,10 +365,10 @@ struct lux_server {
     lux_ctx* ctx = nullptr;
     std::vector<lux_scene*> scenes;
     lux::pt::SceneView* d_scenes = nullptr;
-    lux::pt::PathPool pool;
-    int* req_of = nullptr;
+    lux::pt::PathPool pool[2];      // pool[1] owns only its path-state arrays
+    int* req_of[2] = {nullptr, nullptr};
+    int* sh_dest = nullptr;
     int* qterm = nullptr;
-    int* free_list = nullptr;
     lux::pt::ServerState* st = nullptr;
     lux::pt::ReqSlot* d_req = nullptr;
     lux::pt::ReqSlot* h_req = nullptr;         // pinned mirror
@@ -624,10 +643,12 @@ void worker_main(lux_server* s) {
 int build_graphs(lux_server* s) {
     using namespace lux::pt;
     ServerDev d;
-    d.pool = s->pool;
-    d.req_of = s->req_of;
+    for (int k = 0; k < 2; ++k) {
+        d.pool[k] = s->pool[k];
+        d.req_of[k] = s->req_of[k];
+    }
+    d.sh_dest = s->sh_dest;
     d.qterm = s->qterm;
-    d.free_list = s->free_list;
     d.st = s->st;
     d.req = s->d_req;
     d.tmap = s->d_tmap;
@@ -648,16 +669,15 @@ int build_graphs(lux_server* s) {
     const int shadow_grid = s->ctx->sm_count * std::max(shadow_blocks, 1);
     cudaStream_t stream = s->ctx->stream;
     for (int cur = 0; cur < 2; ++cur) {
-        int nxt = cur ^ 1;
         cudaGraph_t g;
         cudaError_t err = cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal);
         if (err != cudaSuccess) return lux::cuda_fail(err, "graph capture");
-        k_plan<<<1, 1, 0, stream>>>(s->st, cur, nxt);
+        k_plan<<<1, 1, 0, stream>>>(s->st, s->pool[0].capacity);
         k_generate<<<grid, kThreads, gen_stage, stream>>>(d, cur);
         k_extend_s<<<extend_grid, kThreads, stage, stream>>>(d, cur, s->ctx->path_budget);
-        k_shade_s<<<grid, kThreads, stage, stream>>>(d, cur, nxt);
-        k_shadow_s<<<shadow_grid, kThreads, stage, stream>>>(d, s->ctx->path_budget);
-        k_retire<<<grid, kThreads, 0, stream>>>(d);
+        k_shade_s<<<grid, kThreads, stage, stream>>>(d, cur);
+        k_shadow_s<<<shadow_grid, kThreads, stage, stream>>>(d, cur, s->ctx->path_budget);
+        k_retire<<<grid, kThreads, 0, stream>>>(d, cur);
         err = cudaStreamEndCapture(stream, &g);
         if (err != cudaSuccess) return lux::cuda_fail(err, "graph capture end");
         err = cudaGraphInstantiate(&s->graph[cur], g, 0);
@@ -674,9 +694,11 @@ void server_release(lux_server* s) {
         if (s->h_done[k]) cudaFreeHost(s->h_done[k]);
         if (s->h_state[k]) cudaFreeHost(s->h_state[k]);
     }
-    lux::pt::path_pool_free(s->pool);
-    void* dev[] = {s->d_scenes, s->req_of, s->qterm, s->free_list, s->st, s->d_req, s->d_tmap,
-                   s->d_done};
+    lux::pt::path_pool_free(s->pool[0]);
+    const lux::pt::PathPool& p1 = s->pool[1];
+    void* dev[] = {s->d_scenes, s->req_of[0], s->req_of[1], s->sh_dest, s->qterm, s->st,
+                   s->d_req, s->d_tmap, s->d_done, p1.thr_eta, p1.rad, p1.prev, p1.meta,
+                   p1.rng, p1.ray_o, p1.ray_d};
     for (void* p : dev)
         if (p) cudaFree(p);
     if (s->h_req) cudaFreeHost(s->h_req);
@@ -723,7 +745,7 @@ int lux_server_create(int device, lux_scene* const* scenes, int32_t scene_count,
     s->max_requests = max_requests;
     s->budget = opt.memory_budget_bytes > 0 ? opt.memory_budget_bytes : (int64_t(120) << 30);
     int cap = static_cast<int>(pool_paths);
-    st = path_pool_alloc(s->pool, cap);
+    st = path_pool_alloc(s->pool[0], cap);
     std::vector<SceneView> views;
     for (lux_scene* sc : s->scenes) views.push_back(sc->view);
     auto dmalloc = [&](void** p, size_t bytes) {
@@ -734,9 +756,23 @@ int lux_server_create(int device, lux_scene* const* scenes, int32_t scene_count,
         }
     };
     dmalloc(reinterpret_cast<void**>(&s->d_scenes), sizeof(SceneView) * views.size());
-    dmalloc(reinterpret_cast<void**>(&s->req_of), sizeof(int) * cap);
+    // The second pool: its own path state, the first pool's queues and records.
+    if (!st) {
+        PathPool& p1 = s->pool[1];
+        p1 = s->pool[0];
+        p1.thr_eta = p1.rad = p1.prev = p1.ray_o = p1.ray_d = nullptr;
+        p1.meta = nullptr;
+        p1.rng = nullptr;
+    }
+    for (float4** a : {&s->pool[1].thr_eta, &s->pool[1].rad, &s->pool[1].prev, &s->pool[1].ray_o,
+                       &s->pool[1].ray_d})
+        dmalloc(reinterpret_cast<void**>(a), sizeof(float4) * cap);
+    dmalloc(reinterpret_cast<void**>(&s->pool[1].meta), sizeof(int4) * cap);
+    dmalloc(reinterpret_cast<void**>(&s->pool[1].rng), sizeof(uint4) * cap);
+    dmalloc(reinterpret_cast<void**>(&s->req_of[0]), sizeof(int) * cap);
+    dmalloc(reinterpret_cast<void**>(&s->req_of[1]), sizeof(int) * cap);
+    dmalloc(reinterpret_cast<void**>(&s->sh_dest), sizeof(int) * cap);
     dmalloc(reinterpret_cast<void**>(&s->qterm), sizeof(int) * cap);
-    dmalloc(reinterpret_cast<void**>(&s->free_list), sizeof(int) * cap);
     dmalloc(reinterpret_cast<void**>(&s->st), sizeof(ServerState));
     dmalloc(reinterpret_cast<void**>(&s->d_req), sizeof(ReqSlot) * max_requests);
     dmalloc(reinterpret_cast<void**>(&s->d_tmap), sizeof(TicketMap));
@@ -760,10 +796,8 @@ int lux_server_create(int device, lux_scene* const* scenes, int32_t scene_count,
         cudaStream_t stream = s->ctx->stream;
         cudaMemcpyAsync(s->d_scenes, views.data(), sizeof(SceneView) * views.size(),
                         cudaMemcpyHostToDevice, stream);
-        ServerState init{};
-        init.free_count = cap;
+        ServerState init{};  // no live paths
         cudaMemcpyAsync(s->st, &init, sizeof(init), cudaMemcpyHostToDevice, stream);
-        k_init_free<<<s->ctx->sm_count * 4, 256, 0, stream>>>(s->free_list, cap);
         cudaMemsetAsync(s->d_done, 0, sizeof(unsigned long long) * max_requests, stream);
         std::memset(s->h_tmap, 0, sizeof(TicketMap));
         std::memset(s->h_done[0], 0, sizeof(unsigned long long) * max_requests);
@@ -777,7 +811,8 @@ int lux_server_create(int device, lux_scene* const* scenes, int32_t scene_count,
         delete s;
         return st;
     }
-    s->pool_bytes = static_cast<int64_t>(cap) * (16 * 12 + 4 * 7 + 4 * kClasses);
+    // Pool, queues and records, plus the second pool's path state and request slots.
+    s->pool_bytes = static_cast<int64_t>(cap) * (16 * 12 + 4 * 7 + 4 * kClasses + 16 * 7 + 4 + 4);
     s->used = s->pool_bytes;
     for (int k = max_requests - 1; k >= 0; --k) s->free_slots.push_back(k);
     s->worker = std::thread(worker_main, s);

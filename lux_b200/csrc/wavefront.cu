@@ -140,7 +140,8 @@ __global__ void __launch_bounds__(kThreads) k_shadow_refill(PathPool rt, int* co
     unsigned long long segments = 0;
     refill_shadows(
         rt, rt.qshadow, c[6], c + 8, budget, error, [](int) { return 0; },
-        [&](int) -> const SceneView& { return sc; }, segments);
+        [&](int) -> const SceneView& { return sc; },
+        [&](int p, f3 v) { add_radiance(rt, p, v); }, segments);
     warp_add(rays + 1, segments);
 }
 

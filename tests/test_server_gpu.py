@@ -61,7 +61,7 @@ def test_request_is_identical_alone_and_in_the_mix(scenes):
 def test_budget_admission_queues_and_rejects(scenes):
     film_bytes = 64 * 64 * 3 * 12   # fixed-point film + host staging
     pool = 1 << 14
-    pool_bytes = pool * (16 * 12 + 4 * 7 + 4 * 5)
+    pool_bytes = pool * (16 * 12 + 4 * 7 + 4 * 5 + 16 * 7 + 4 + 4)   # two pools
     budget = pool_bytes + 2 * film_bytes + 100       # two requests at a time
     with SV.Server(scenes, pool_paths=pool, memory_budget_bytes=budget) as srv:
         ids = [srv.submit(s, r)[0] for s, r in REQUESTS]
