@@ -437,8 +437,10 @@ int lux_server_update_mesh(lux_server* server, int32_t scene, int32_t mesh,
                            const float* vertices);
 /* Host timestamps (steady clock, ns) of submission, admission and completion. */
 int lux_server_request_times(lux_server* server, int64_t request_id, int64_t* times);
-/* [0] pool iterations, [1] camera + extension rays, [2] shadow segments, [3] requests
- * completed, [4] requests admitted, [5] refits applied, [6] bytes in use. */
+/* stats[9]: [0] pool iterations, [1] camera + extension rays, [2] shadow segments,
+ * [3] requests completed, [4] requests admitted, [5] refits applied, [6] bytes in use,
+ * [7] longest worker pass between admission checks (ns), [8] longest wait for one
+ * iteration's results (ns). */
 int lux_server_stats(lux_server* server, int64_t* stats);
 int lux_server_destroy(lux_server* server);
 

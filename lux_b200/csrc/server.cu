@@ -380,6 +380,11 @@ struct lux_server {
     long long* h_limit = nullptr;              // pinned ticket limit
     cudaEvent_t iter_done[2] = {nullptr, nullptr};
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    // Request films come from this pool, which keeps freed memory (release threshold at
+    // its maximum): the default pool returns memory to the driver at every stream
+    // synchronisation and maps it again on the next allocation, which stalled the worker
+    // for hundreds of milliseconds.
+    cudaMemPool_t film_pool = nullptr;
     int max_requests = 256;
     int64_t budget = 0;
     int64_t used = 0;
@@ -404,6 +409,8 @@ struct lux_server {
     int64_t collected = 0;   // iterations whose counters were read back
     bool stop = false;
     int64_t iterations = 0, completed = 0, admitted = 0, refits = 0;
+    int64_t longest_pass_ns = 0;      // longest worker loop pass (admission latency bound)
+    int64_t longest_wait_ns = 0;      // longest wait for one iteration's counters
     unsigned long long rays[2] = {0, 0};
     int error_status = 0;
     std::thread worker;
@@ -442,12 +449,14 @@ void admit(lux_server* s) {
         if (s->used + cost > s->budget) break;
         cudaStream_t stream = s->ctx->stream;
         size_t n = static_cast<size_t>(r.req.width) * r.req.height * 3;
-        if (cudaMallocAsync(reinterpret_cast<void**>(&r.film), n * 8, stream) != cudaSuccess) {
+        if (cudaMallocFromPoolAsync(reinterpret_cast<void**>(&r.film), n * 8, s->film_pool,
+                                    stream) != cudaSuccess) {
             cudaGetLastError();
             break;
         }
         if (!r.out_device &&
-            cudaMallocAsync(reinterpret_cast<void**>(&r.staging), n * 4, stream) != cudaSuccess) {
+            cudaMallocFromPoolAsync(reinterpret_cast<void**>(&r.staging), n * 4, s->film_pool,
+                                    stream) != cudaSuccess) {
             cudaGetLastError();
             cudaFreeAsync(r.film, stream);
             r.film = nullptr;
@@ -560,7 +569,13 @@ void fail_all(lux_server* s, int status) {
 void worker_main(lux_server* s) {
     cudaSetDevice(s->ctx->device);
     std::unique_lock<std::mutex> lk(s->mu);
+    int64_t pass_start = lux::pt::now_ns();
     for (;;) {
+        {
+            const int64_t t = lux::pt::now_ns();
+            s->longest_pass_ns = std::max(s->longest_pass_ns, t - pass_start);
+            pass_start = t;
+        }
         if (s->stop) break;
         if (s->error_status == 0) admit(s);
         if (!s->updates.empty()) {
@@ -589,11 +604,15 @@ void worker_main(lux_server* s) {
                 return s->stop || (!s->pending.empty() && !s->free_slots.empty()) ||
                        !s->updates.empty();
             });
+            pass_start = lux::pt::now_ns();  // idling is not a stall
             continue;
         }
         // Keep up to two iterations in flight: launch one, then read the older one's
         // counters while the newer runs.
         bool launch = !s->active.empty() && s->launched - s->collected < 2;
+        cudaEvent_t delivering_event = s->delivering.empty()
+                                           ? nullptr
+                                           : s->requests[s->delivering.front()]->delivered;
         int64_t launch_index = s->launched;
         if (launch) ++s->launched;
         lk.unlock();
@@ -609,19 +628,23 @@ void worker_main(lux_server* s) {
         }
         int err_word = 0;
         int64_t read_iter = -1;
+        int64_t wait_ns = 0;
         if (s->collected < s->launched) {
             read_iter = s->collected;
+            const int64_t w0 = lux::pt::now_ns();
             cudaError_t e = cudaEventSynchronize(s->iter_done[static_cast<int>(read_iter & 1)]);
+            wait_ns = lux::pt::now_ns() - w0;
             if (e != cudaSuccess) {
                 lk.lock();
                 fail_all(s, LUX_ERR_CUDA);
                 continue;
             }
             cudaMemcpy(&err_word, s->ctx->d_error, sizeof(int), cudaMemcpyDeviceToHost);
-        } else {
-            cudaStreamSynchronize(s->ctx->stream);
+        } else if (delivering_event) {
+            cudaEventSynchronize(delivering_event);  // the oldest film delivery
         }
         lk.lock();
+        s->longest_wait_ns = std::max(s->longest_wait_ns, wait_ns);
         if (read_iter >= 0) {
             int parity = static_cast<int>(read_iter & 1);
             s->collected = read_iter + 1;
@@ -688,6 +711,7 @@ int build_graphs(lux_server* s) {
 }
 
 void server_release(lux_server* s) {
+    if (s->ctx) cudaStreamSynchronize(s->ctx->stream);
     for (int k = 0; k < 2; ++k) {
         if (s->graph[k]) cudaGraphExecDestroy(s->graph[k]);
         if (s->iter_done[k]) cudaEventDestroy(s->iter_done[k]);
@@ -705,10 +729,13 @@ void server_release(lux_server* s) {
     if (s->h_tmap) cudaFreeHost(s->h_tmap);
     if (s->h_limit) cudaFreeHost(s->h_limit);
     for (auto& kv : s->requests) {
-        if (kv.second->film) cudaFree(kv.second->film);
-        if (kv.second->staging) cudaFree(kv.second->staging);
+        cudaStream_t stream = s->ctx ? s->ctx->stream : nullptr;
+        if (kv.second->film) cudaFreeAsync(kv.second->film, stream);
+        if (kv.second->staging) cudaFreeAsync(kv.second->staging, stream);
         if (kv.second->delivered) cudaEventDestroy(kv.second->delivered);
     }
+    if (s->ctx) cudaStreamSynchronize(s->ctx->stream);
+    if (s->film_pool) cudaMemPoolDestroy(s->film_pool);
     if (s->ctx) lux_ctx_destroy(s->ctx);
 }
 
@@ -741,6 +768,20 @@ int lux_server_create(int device, lux_scene* const* scenes, int32_t scene_count,
         return st;
     }
     if (opt.path_budget > 0) s->ctx->path_budget = std::min(opt.path_budget, 4096);
+    {
+        cudaMemPoolProps props{};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = device;
+        if (cudaMemPoolCreate(&s->film_pool, &props) == cudaSuccess) {
+            uint64_t keep = ~uint64_t(0);
+            cudaMemPoolSetAttribute(s->film_pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        } else {
+            cudaGetLastError();
+            s->film_pool = nullptr;
+            st = server_fail(LUX_ERR_CUDA, "film memory pool");
+        }
+    }
     s->scenes.assign(scenes, scenes + scene_count);
     s->max_requests = max_requests;
     s->budget = opt.memory_budget_bytes > 0 ? opt.memory_budget_bytes : (int64_t(120) << 30);
@@ -948,6 +989,8 @@ int lux_server_stats(lux_server* s, int64_t* stats) {
     stats[4] = s->admitted;
     stats[5] = s->refits;
     stats[6] = s->used;
+    stats[7] = s->longest_pass_ns;
+    stats[8] = s->longest_wait_ns;
     return LUX_OK;
 }
 

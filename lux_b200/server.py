@@ -68,10 +68,10 @@ class Server:
         return int(t[0]), int(t[1]), int(t[2])
 
     def stats(self) -> dict:
-        s = np.zeros(7, np.int64)
+        s = np.zeros(9, np.int64)
         _check(self._lib.lux_server_stats(self._h, s.ctypes.data))
         keys = ["iterations", "rays", "shadow_rays", "completed", "admitted", "refits",
-                "bytes_in_use"]
+                "bytes_in_use", "longest_pass_ns", "longest_wait_ns"]
         return dict(zip(keys, (int(v) for v in s)))
 
     def close(self) -> None:
