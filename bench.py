@@ -752,7 +752,10 @@ def run_serving(args) -> None:
                         "mrays_s": rays / span / 1e6, "refits": stats["refits"],
                         "fifo_plain_p50_ms": float(np.percentile(fifo_lat, 50) * 1e3),
                         "fifo_plain_p99_ms": float(np.percentile(fifo_lat, 99) * 1e3),
-                        "fifo_plain_mrays_s": plain_rays / max(free_at, 1e-9) / 1e6})
+                        "fifo_plain_mrays_s": plain_rays / max(free_at, 1e-9) / 1e6,
+                        "plain_service_ms": {"p50": float(np.percentile(service, 50) * 1e3),
+                                             "max": float(np.max(service) * 1e3),
+                                             "argmax": int(np.argmax(service))}})
     best = max(results, key=lambda r: r["mrays_s"])
     line = {"metric": "p50/p99 render-request latency and Mrays/s (served)",
             "value": best["mrays_s"], "unit": "Mrays/s", "n_gpus": 1, "steps": len(rates),
