@@ -296,12 +296,22 @@ typedef struct lux_instance_desc {
 
 /* Explicit light (light/light.h:66-79).  kind: 1 point (vec = position, value =
  * intensity), 2 distant (vec = direction to light, value = radiance), 3 uniform
- * infinite (value = radiance).  Emissive triangles become area lights automatically. */
+ * infinite (value = radiance), 4 image infinite (image = index into the scene's
+ * images, value = scale; add_image_infinite_light, scene/scene_build.h:40-89).
+ * Emissive triangles become area lights automatically. */
 typedef struct lux_light_desc {
     int32_t kind;
     float vec[3];
     float value[3];
+    int32_t image;
 } lux_light_desc;
+
+/* Latitude-longitude environment image: width * height RGB texels, row 0 at the +y
+ * pole (theta 0), column 0 at phi 0 (the +x axis), phi growing towards +z. */
+typedef struct lux_env_image {
+    const float* pixels;
+    int32_t width, height;
+} lux_env_image;
 
 /* Perspective camera (camera/camera.h:29-38). */
 typedef struct lux_camera_desc {
@@ -326,6 +336,8 @@ typedef struct lux_scene_desc {
     const lux_light_desc* lights;
     int32_t light_count;
     lux_camera_desc camera;
+    const lux_env_image* images;
+    int32_t image_count;
 } lux_scene_desc;
 
 /* RenderSettings (integrator/render_context.h:16-24).  light_sampler: 0 uniform,

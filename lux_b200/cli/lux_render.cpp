@@ -9,9 +9,8 @@
 // sample.  Images are written as the reference writes them: PPM through write_ppm's
 // tone map, PFM when the path ends in ".pfm" (the pixel transforms run on the device,
 // lux_film_encode).  This build renders on the GPU only: without -gpu it still renders
-// on the GPU and says so.  Scenes that need asset files or an environment image
-// (image-env, bunny, dragon, lux-cover), the BVH light sampler and the debug probes/AOVs
-// are reported as unsupported.
+// on the GPU and says so.  Scenes that need asset files (bunny, dragon, lux-cover), the
+// BVH light sampler and the debug probes/AOVs are reported as unsupported.
 
 #include <chrono>
 #include <cmath>
@@ -135,7 +134,7 @@ void usage(const char* exe) {
     std::printf(
         "Usage: %s [scene] [options]\n"
         "  -scene NAME             cornell, direct-light, point-light, distant-light,\n"
-        "                          uniform-env, transparent-filter\n"
+        "                          uniform-env, image-env, transparent-filter\n"
         "  -width N / -height N / -size W H   film size (default 256x256)\n"
         "  -spp N                  samples per pixel (default 64)\n"
         "  -depth N                maximum path depth (default 4)\n"
@@ -154,6 +153,8 @@ struct SceneData {
     std::vector<uint32_t> indices;
     std::vector<int32_t> material_ids;
     std::vector<lux_light_desc> lights;
+    std::vector<std::vector<float>> image_pixels;
+    std::vector<lux_env_image> images;
     float cam_origin[3], cam_look_at[3], cam_vfov;
 };
 
@@ -265,6 +266,18 @@ void uniform_env(SceneData& s) {
     probe_base(s);
     add_light(s, 3, {0, 0, 0}, {0.15f, 0.18f, 0.25f});
 }
+// make_image_env_scene (app/render_runner.cpp:127-136): a 2x2 latitude-longitude image.
+void image_env(SceneData& s) {
+    probe_base(s);
+    s.image_pixels.push_back({1.4f, 1.0f, 0.7f, 0.2f, 0.3f, 0.8f,
+                              0.1f, 0.2f, 0.5f, 0.8f, 1.1f, 1.5f});
+    lux_env_image im{};
+    im.width = 2;
+    im.height = 2;
+    s.images.push_back(im);
+    add_light(s, 4, {0, 0, 0}, {0.35f, 0.35f, 0.35f});
+    s.lights.back().image = 0;
+}
 // make_transparent_filter_scene (scene/transparent_filter.h:9-40), runner camera :138-144.
 void transparent_filter(SceneData& s) {
     int receiver = lambert(s, 0.75f, 0.75f, 0.75f);
@@ -293,7 +306,7 @@ constexpr SceneEntry kScenes[] = {
     {"cornell", cornell},         {"direct-light", direct_light},
     {"point-light", point_light}, {"distant-light", distant_light},
     {"uniform-env", uniform_env}, {"transparent-filter", transparent_filter},
-    {"image-env", nullptr},       {"bunny", nullptr},
+    {"image-env", image_env},     {"bunny", nullptr},
     {"dragon", nullptr},          {"lux-cover", nullptr},
 };
 
@@ -349,8 +362,8 @@ int main(int argc, char** argv) {
         return 1;
     }
     if (!entry->make) {
-        std::fprintf(stderr, "Scene setup failed: scene '%s' needs asset files or an environment "
-                             "image, which this build does not load\n", c.scene.c_str());
+        std::fprintf(stderr, "Scene setup failed: scene '%s' needs asset files, which this build "
+                             "does not load\n", c.scene.c_str());
         return 1;
     }
     if (!c.gpu) std::printf("Rendering on the GPU (the only path of this build)\n");
@@ -378,6 +391,9 @@ int main(int argc, char** argv) {
     desc.instance_count = 1;
     desc.lights = data.lights.empty() ? nullptr : data.lights.data();
     desc.light_count = static_cast<int32_t>(data.lights.size());
+    for (size_t k = 0; k < data.images.size(); ++k) data.images[k].pixels = data.image_pixels[k].data();
+    desc.images = data.images.empty() ? nullptr : data.images.data();
+    desc.image_count = static_cast<int32_t>(data.images.size());
     if (check(lux_camera_perspective(data.cam_origin, data.cam_look_at, data.cam_vfov, aspect,
                                      0.0f, 1.0f, &desc.camera),
               "Scene setup"))

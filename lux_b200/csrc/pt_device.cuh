@@ -148,12 +148,22 @@ struct Instance {
 };
 
 struct Light {  // light/light.h:86-93 for the kinds this path supports
-    int kind;              // 0 area, 1 point, 2 distant, 3 uniform infinite
-    int primitive;         // area: scene triangle id
+    int kind;              // 0 area, 1 point, 2 distant, 3 uniform infinite, 4 image infinite
+    int primitive;         // area: scene triangle id; image infinite: index into env
     int two_sided;
     float area;
-    f3 emission;           // area emission / point intensity / radiance
+    f3 emission;           // area emission / point intensity / radiance / image scale
     f3 vec;                // point position / distant direction to light
+};
+
+// Image infinite light (ImageInfiniteLight, light/light.h:79-87): latitude-longitude
+// texels (RGB, unscaled) and the running sum of their sampling weights.
+struct EnvLight {
+    const float* pixels;   // width * height * 3
+    const float* cdf;      // width * height
+    int width, height;
+    float total;
+    f3 scale;
 };
 
 struct AliasEntry {  // light/light_distribution.h:22-26
@@ -180,6 +190,7 @@ struct SceneView {
     const BvhView* blas;       // one per mesh
     const Light* lights;
     int light_count;
+    const EnvLight* env;             // image infinite lights, by Light::primitive
     float total_light_power;
     const AliasEntry* light_alias;   // power alias table, light_count entries
     int light_sampler;               // 0 uniform, 1 power

@@ -495,10 +495,83 @@ LUX_D float solid_angle_pdf(f3 lpos, f3 lnormal, int two_sided, float pdf_area, 
     return mul(pdf_area, d2) / c;
 }
 
+// ------------------------------------------------------------------ image infinite lights
+// direction_to_latlong_uv / latlong_uv_to_direction / image_env_lookup /
+// image_infinite_pdf_for_texel / sample_image_infinite_light / image_infinite_pdf
+// (light/light.h:144-269).
+
+LUX_D float2 env_uv(f3 wi) {
+    f3 w = normalize(wi);
+    float phi = atan2f(w.z, w.x);
+    if (phi < 0) phi = add(phi, 2.0f * kPi);
+    float theta = acosf(fmaxf(-1.0f, fminf(1.0f, w.y)));
+    return make_float2(mul(phi, 0.5f * kInvPi), mul(theta, kInvPi));
+}
+
+LUX_D int env_texel(const EnvLight& e, float2 uv) {
+    int x = static_cast<int>(fminf(static_cast<float>(e.width - 1), floorf(mul(uv.x, static_cast<float>(e.width)))));
+    int y = static_cast<int>(fminf(static_cast<float>(e.height - 1), floorf(mul(uv.y, static_cast<float>(e.height)))));
+    return y * e.width + x;
+}
+
+LUX_D f3 env_lookup(const EnvLight& e, f3 wi) {
+    if (!e.pixels || e.width <= 0 || e.height <= 0) return splat(0);
+    const int i = env_texel(e, env_uv(wi));
+    const float* p = e.pixels + 3 * static_cast<size_t>(i);
+    return make_f3(p[0], p[1], p[2]) * e.scale;
+}
+
+LUX_D float env_pdf_texel(const EnvLight& e, int index, float v) {
+    if (!e.cdf || e.width <= 0 || e.height <= 0 || e.total <= 0) return 0;
+    const int count = e.width * e.height;
+    if (index < 0 || index >= count) return 0;
+    float w = index == 0 ? e.cdf[0] : sub(e.cdf[index], e.cdf[index - 1]);
+    if (w <= 0) return 0;
+    float theta = mul(kPi, v);
+    float sin_theta = fmaxf(1e-6f, sinf(theta));
+    float uv_pdf = mul(w / e.total, static_cast<float>(count));
+    return uv_pdf / mul(mul(mul(2.0f, kPi), kPi), sin_theta);
+}
+
+LUX_D float env_pdf(const EnvLight& e, f3 wi) {
+    if (!e.pixels || !e.cdf || e.width <= 0 || e.height <= 0 || e.total <= 0) return 0;
+    const float2 uv = env_uv(wi);
+    return env_pdf_texel(e, env_texel(e, uv), uv.y);
+}
+
+// Texel by the running sums (the first texel whose sum reaches the target; a binary
+// search finds the same texel as the reference's linear scan), then a uniform point in
+// it.
+LUX_D LightLi env_sample(const EnvLight& e, float select_u, float ux, float uy) {
+    LightLi li;
+    if (!e.pixels || !e.cdf || e.width <= 0 || e.height <= 0 || e.total <= 0) return li;
+    const int count = e.width * e.height;
+    const float target = mul(fminf(select_u, 0.99999994f), e.total);
+    int lo = 0, hi = count - 1;
+    while (lo < hi) {
+        int mid = (lo + hi) >> 1;
+        if (target <= e.cdf[mid]) hi = mid;
+        else lo = mid + 1;
+    }
+    const int index = target <= e.cdf[lo] ? lo : count - 1;
+    const int x = index % e.width, y = index / e.width;
+    const float u = add(static_cast<float>(x), ux) / static_cast<float>(e.width);
+    const float v = add(static_cast<float>(y), uy) / static_cast<float>(e.height);
+    const float phi = mul(mul(2.0f, kPi), u);
+    const float theta = mul(kPi, v);
+    const float st = sinf(theta);
+    li.wi = make_f3(mul(cosf(phi), st), cosf(theta), mul(sinf(phi), st));
+    li.distance = INFINITY;
+    li.radiance = env_lookup(e, li.wi);
+    li.pdf = env_pdf_texel(e, index, v);
+    li.measure = kMeasureSolidAngle;
+    li.valid = max_component(li.radiance) > 0 && li.pdf > 0;
+    return li;
+}
+
 // sample_light_li (scene/scene_light_sampler.h:212-265 / gpu_scene_light_sampler.cuh:133-193).
 LUX_D LightLi sample_light(const SceneView& sc, int sampler, f3 p, float select_u, float comp_u, float ux,
                            float uy) {
-    (void)comp_u;
     LightLi li;
     if (sc.light_count <= 0 || sc.total_light_power <= 0) return li;
     int index;
@@ -549,6 +622,9 @@ LUX_D LightLi sample_light(const SceneView& sc, int sampler, f3 p, float select_
         li.pdf = 1.0f;
         li.measure = kMeasureDiscrete;
         li.valid = max_component(li.radiance) > 0;
+    } else if (L.kind == 4) {  // image infinite: the component draw picks the texel
+        if (!sc.env || L.primitive < 0) return li;
+        li = env_sample(sc.env[L.primitive], comp_u, ux, uy);
     } else {  // uniform infinite (light/light.h:144-150, 189-197)
         float z = sub(1.0f, mul(2.0f, ux));
         float r = sqrtf(fmaxf(0.0f, sub(1.0f, mul(z, z))));
@@ -564,17 +640,26 @@ LUX_D LightLi sample_light(const SceneView& sc, int sampler, f3 p, float select_
     return li;
 }
 
-LUX_D f3 infinite_le(const SceneView& sc) {  // infinite_lights_le
+LUX_D f3 infinite_le(const SceneView& sc, f3 dir) {  // infinite_lights_le
     f3 le = splat(0);
-    for (int i = 0; i < sc.light_count; ++i)
-        if (sc.lights[i].kind == 3) le = le + sc.lights[i].emission;
+    for (int i = 0; i < sc.light_count; ++i) {
+        const Light& L = sc.lights[i];
+        if (L.kind == 3) le = le + L.emission;
+        else if (L.kind == 4 && sc.env && L.primitive >= 0) le = le + env_lookup(sc.env[L.primitive], dir);
+    }
     return le;
 }
 
-LUX_D float infinite_pdf(const SceneView& sc, int sampler) {  // infinite_lights_pdf_li
+LUX_D float infinite_pdf(const SceneView& sc, int sampler, f3 dir) {  // infinite_lights_pdf_li
     float pdf = 0;
-    for (int i = 0; i < sc.light_count; ++i)
-        if (sc.lights[i].kind == 3) pdf = add(pdf, mul(light_pmf(sc, sampler, i), 1.0f / mul(4.0f, kPi)));
+    for (int i = 0; i < sc.light_count; ++i) {
+        const Light& L = sc.lights[i];
+        if (L.kind == 3) {
+            pdf = add(pdf, mul(light_pmf(sc, sampler, i), 1.0f / mul(4.0f, kPi)));
+        } else if (L.kind == 4 && sc.env && L.primitive >= 0) {
+            pdf = add(pdf, mul(light_pmf(sc, sampler, i), env_pdf(sc.env[L.primitive], dir)));
+        }
+    }
     return pdf;
 }
 
@@ -729,13 +814,14 @@ LUX_D int extend_finish(const PathPool& rt, const SceneView& sc, int sampler, in
         rt.hit[p] = make_float4(h.t, h.u, h.v, __int_as_float(h.prim));
         return material_class(sc.materials[material_of(sc, h.prim)].type);
     }
-    f3 le = infinite_le(sc);
+    const f3 dir = xyz(rt.ray_d[p]);
+    f3 le = infinite_le(sc, dir);
     if (max_component(le) > 0) {
         PathState s = load_state(rt, p);
         if (s.depth == 0 || is_delta(s.flags)) {
             add_radiance(rt, p, s.thr * le);
         } else if (s.measure == kMeasureSolidAngle && s.prev_pdf > 0) {
-            float w = power_heuristic(s.prev_pdf, infinite_pdf(sc, sampler));
+            float w = power_heuristic(s.prev_pdf, infinite_pdf(sc, sampler, dir));
             add_radiance(rt, p, (s.thr * le) * w);
         }
     }

@@ -33,6 +33,9 @@ struct lux_scene {
     float* tri_soup = nullptr;          // per-mesh object-space soups for refits (device)
     std::vector<size_t> soup_offset;    // float offset of each mesh's soup
     float* tlas_boxes = nullptr;        // instance world boxes (device)
+    float* env_pixels = nullptr;        // image-light texels (device)
+    float* env_cdf = nullptr;           // image-light running weights (device)
+    lux::pt::EnvLight* d_env = nullptr; // image lights (device)
     // Device buffers of vertex updates, allocated on a mesh's first update.
     struct MeshRefit {
         float* vertices = nullptr;       // object space, 3 per vertex

@@ -270,7 +270,7 @@ void scene_free(lux_scene* s) {
     s->refit.clear();
     void* ptrs[] = {s->materials, s->tris, s->shading, s->d_instances, s->tlas_instance,
                     s->blas_views, s->lights, s->light_alias, s->primitive_light, s->tri_soup,
-                    s->tlas_boxes};
+                    s->tlas_boxes, s->env_pixels, s->env_cdf, s->d_env};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     for (lux_bvh* b : s->blas) lux_bvh_destroy(b);
@@ -304,9 +304,19 @@ int scene_create(lux_ctx* ctx, const lux_scene_desc* d, lux_scene** out) {
         if (in.material_override >= d->material_count)
             return fail(LUX_ERR_INVALID_ARGUMENT, "instance material out of range");
     }
-    for (int i = 0; i < d->light_count; ++i)
-        if (d->lights[i].kind < 1 || d->lights[i].kind > 3)
+    for (int i = 0; i < d->light_count; ++i) {
+        if (d->lights[i].kind < 1 || d->lights[i].kind > 4)
             return fail(LUX_ERR_INVALID_ARGUMENT, "unknown light kind");
+        if (d->lights[i].kind == 4) {
+            const int im = d->lights[i].image;
+            if (im < 0 || im >= d->image_count || !d->images)
+                return fail(LUX_ERR_INVALID_ARGUMENT, "image light without a valid image");
+            const lux_env_image& e = d->images[im];
+            if (!e.pixels || e.width <= 0 || e.height <= 0 ||
+                static_cast<long long>(e.width) * e.height > (1ll << 26))
+                return fail(LUX_ERR_INVALID_ARGUMENT, "bad environment image");
+        }
+    }
 
     lux_scene* s = new (std::nothrow) lux_scene();
     if (!s) return fail(LUX_ERR_OUT_OF_MEMORY, "scene allocation failed");
@@ -369,6 +379,12 @@ int scene_create(lux_ctx* ctx, const lux_scene_desc* d, lux_scene** out) {
         }
     }
     s->area_light_count = static_cast<int>(lights.size());
+    // Image lights: texels and running weights (make_image_light_asset,
+    // scene/scene_build.h:40-65): weight = max(0, luminance(texel * scale)) * sin(theta)
+    // at the row centre, summed in row-major order in float.
+    std::vector<float> env_pixels, env_cdf;
+    std::vector<pt::EnvLight> env;          // pixels/cdf hold offsets until upload
+    std::vector<std::pair<size_t, size_t>> env_offsets;
     for (int i = 0; i < d->light_count; ++i) {
         const lux_light_desc& ld = d->lights[i];
         Light l;
@@ -380,7 +396,33 @@ int scene_create(lux_ctx* ctx, const lux_scene_desc* d, lux_scene** out) {
         V3 vec = v3(ld.vec[0], ld.vec[1], ld.vec[2]);
         if (ld.kind == 2) vec = normalize3(vec);  // add_distant_light stores it normalised
         l.vec = make_f3(vec.x, vec.y, vec.z);
-        append(l, std::fmax(1e-6f, luminance(v3(ld.value[0], ld.value[1], ld.value[2]))));
+        float power = std::fmax(1e-6f, luminance(v3(ld.value[0], ld.value[1], ld.value[2])));
+        if (ld.kind == 4) {
+            const lux_env_image& im = d->images[ld.image];
+            const float kPi = 3.14159265358979323846f;
+            pt::EnvLight e{};
+            e.width = im.width;
+            e.height = im.height;
+            e.scale = l.emission;
+            env_offsets.emplace_back(env_pixels.size(), env_cdf.size());
+            float sum = 0;
+            for (int y = 0; y < im.height; ++y) {
+                float theta = kPi * ((static_cast<float>(y) + 0.5f) / static_cast<float>(im.height));
+                float sin_theta = std::fmax(0.0f, std::sin(theta));
+                for (int x = 0; x < im.width; ++x) {
+                    const float* px = im.pixels + 3 * (static_cast<size_t>(y) * im.width + x);
+                    V3 radiance = v3(px[0] * ld.value[0], px[1] * ld.value[1], px[2] * ld.value[2]);
+                    sum += std::fmax(0.0f, luminance(radiance)) * sin_theta;
+                    env_cdf.push_back(sum);
+                    env_pixels.insert(env_pixels.end(), px, px + 3);
+                }
+            }
+            e.total = sum;
+            l.primitive = static_cast<int>(env.size());
+            env.push_back(e);
+            power = std::fmax(1e-6f, sum);
+        }
+        append(l, power);
     }
     std::vector<float> weights;
     float prev = 0;
@@ -399,6 +441,15 @@ int scene_create(lux_ctx* ctx, const lux_scene_desc* d, lux_scene** out) {
     if (!st) st = upload(&s->shading, shading, ctx->stream);
     if (!st) st = upload(&s->d_instances, s->instances, ctx->stream);
     if (!st) st = upload(&s->lights, lights, ctx->stream);
+    if (!st && !env.empty()) {
+        st = upload(&s->env_pixels, env_pixels, ctx->stream);
+        if (!st) st = upload(&s->env_cdf, env_cdf, ctx->stream);
+        for (size_t k = 0; k < env.size() && !st; ++k) {
+            env[k].pixels = s->env_pixels + env_offsets[k].first;
+            env[k].cdf = s->env_cdf + env_offsets[k].second;
+        }
+        if (!st) st = upload(&s->d_env, env, ctx->stream);
+    }
     if (!st) st = upload(&s->light_alias, alias, ctx->stream);
     if (!st) st = upload(&s->primitive_light, primitive_light, ctx->stream);
 
@@ -462,6 +513,7 @@ int scene_create(lux_ctx* ctx, const lux_scene_desc* d, lux_scene** out) {
     v.tlas_instance = s->tlas_instance;
     v.blas = s->blas_views;
     v.lights = s->lights;
+    v.env = s->d_env;
     v.light_count = static_cast<int>(lights.size());
     v.total_light_power = total_power;
     v.light_alias = alias.empty() ? nullptr : s->light_alias;

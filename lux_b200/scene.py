@@ -16,7 +16,7 @@ import numpy as np
 from . import _check, _ptr, load_library
 
 LAMBERT, THIN_LAMBERT, GGX, DIELECTRIC, INTERFACE, TRANSPARENT = range(6)
-LIGHT_POINT, LIGHT_DISTANT, LIGHT_UNIFORM_INFINITE = 1, 2, 3
+LIGHT_POINT, LIGHT_DISTANT, LIGHT_UNIFORM_INFINITE, LIGHT_IMAGE_INFINITE = 1, 2, 3, 4
 SAMPLER_UNIFORM, SAMPLER_POWER = 0, 1
 
 _F3 = ctypes.c_float * 3
@@ -42,7 +42,12 @@ class InstanceDesc(ctypes.Structure):
 
 
 class LightDesc(ctypes.Structure):
-    _fields_ = [("kind", ctypes.c_int32), ("vec", _F3), ("value", _F3)]
+    _fields_ = [("kind", ctypes.c_int32), ("vec", _F3), ("value", _F3), ("image", ctypes.c_int32)]
+
+
+class EnvImageDesc(ctypes.Structure):
+    _fields_ = [("pixels", ctypes.c_void_p), ("width", ctypes.c_int32),
+                ("height", ctypes.c_int32)]
 
 
 class CameraDesc(ctypes.Structure):
@@ -55,7 +60,8 @@ class SceneDesc(ctypes.Structure):
                 ("meshes", ctypes.c_void_p), ("mesh_count", ctypes.c_int32),
                 ("instances", ctypes.c_void_p), ("instance_count", ctypes.c_int32),
                 ("lights", ctypes.c_void_p), ("light_count", ctypes.c_int32),
-                ("camera", CameraDesc)]
+                ("camera", CameraDesc), ("images", ctypes.c_void_p),
+                ("image_count", ctypes.c_int32)]
 
 
 class RenderRequest(ctypes.Structure):
@@ -113,6 +119,7 @@ class SceneBuilder:
     meshes: list = field(default_factory=list)
     instances: list = field(default_factory=list)   # (mesh, 3x4 matrix, override)
     lights: list = field(default_factory=list)
+    images: list = field(default_factory=list)      # (height, width, 3) float32 images
     camera: CameraDesc | None = None
     _default_mesh: int = -1
     _tris: list = field(default_factory=list)
@@ -152,6 +159,14 @@ class SceneBuilder:
 
     def add_uniform_infinite_light(self, radiance):
         self.lights.append(LightDesc(LIGHT_UNIFORM_INFINITE, _F3(0, 0, 0), _F3(*radiance)))
+
+    def add_image_infinite_light(self, pixels, scale=(1.0, 1.0, 1.0)):
+        """add_image_infinite_light (scene/scene_build.h:67-89): pixels is an
+        (height, width, 3) latitude-longitude image, row 0 at the +y pole."""
+        img = np.ascontiguousarray(pixels, np.float32)
+        self.images.append(img)
+        self.lights.append(LightDesc(LIGHT_IMAGE_INFINITE, _F3(0, 0, 0), _F3(*scale),
+                                     len(self.images) - 1))
 
     def set_pinhole_camera(self, origin, look_at, vfov_degrees, aspect):
         """make_pinhole_camera (camera/pinhole_camera.h:13-17): lens 0, focal distance 1."""
@@ -221,11 +236,16 @@ class Scene:
                                       _F12(*([0.0] * 12))))
         inst_arr = (InstanceDesc * max(len(insts), 1))(*insts)
         light_arr = (LightDesc * max(len(builder.lights), 1))(*builder.lights)
+        images = [np.ascontiguousarray(im, np.float32) for im in builder.images]
+        keep += images
+        img_arr = (EnvImageDesc * max(len(images), 1))(
+            *[EnvImageDesc(im.ctypes.data, im.shape[1], im.shape[0]) for im in images])
         desc = SceneDesc(ctypes.addressof(mats), len(builder.materials),
                          ctypes.addressof(mesh_arr), len(meshes),
                          ctypes.addressof(inst_arr), len(insts),
                          ctypes.addressof(light_arr), len(builder.lights),
-                         builder.camera if builder.camera is not None else CameraDesc())
+                         builder.camera if builder.camera is not None else CameraDesc(),
+                         ctypes.addressof(img_arr), len(images))
         handle = ctypes.c_void_p()
         _check(lib.lux_scene_create(ctx.handle, ctypes.byref(desc), ctypes.byref(handle)))
         self._h = handle

@@ -115,7 +115,7 @@ class Ref:
         lib.ref_cornell_render.argtypes = [_I, _I, _I, _I, ctypes.c_uint64, _I, _I, _I,
                                            _P, _P, _P]
         lib.ref_render_scene.argtypes = [_P, _I, _P, _P, _I, _P, _I, _P, _I, _I, _I, _I,
-                                         ctypes.c_uint64, _I, _I, _I, _I, _P]
+                                         ctypes.c_uint64, _I, _I, _I, _I, _P, _P, _I, _I]
         lib.ref_tree_create.argtypes = [_P, _I, _I]
         lib.ref_tree_create.restype = _P
         lib.ref_tree_destroy.argtypes = [_P]
@@ -123,7 +123,7 @@ class Ref:
         self.lib = lib
 
     def render_scene(self, tris, material_ids, materials, lights, camera, width, height, spp,
-                     max_depth, seed, light_sampler=1, rows=None, threads=1):
+                     max_depth, seed, light_sampler=1, rows=None, threads=1, env_image=None):
         """Per-sample radiance [pixel][spp][3] of a single-mesh scene (see ref_harness.cpp).
 
         materials: N x 11 (type, albedo3, emission3, roughness, metallic, eta, two_sided);
@@ -136,10 +136,14 @@ class Ref:
         cam = np.ascontiguousarray(camera, np.float32)
         y0, y1 = rows if rows is not None else (0, height)
         out = np.zeros(((y1 - y0) * width, spp, 3), np.float32)
+        env = None if env_image is None else np.ascontiguousarray(env_image, np.float32)
         self.lib.ref_render_scene(tris.ctypes.data, len(tris), mids.ctypes.data, mats.ctypes.data,
                                   len(mats), lights.ctypes.data if len(lights) else None,
                                   len(lights), cam.ctypes.data, width, height, spp, max_depth,
-                                  seed, light_sampler, y0, y1, threads, out.ctypes.data)
+                                  seed, light_sampler, y0, y1, threads, out.ctypes.data,
+                                  None if env is None else env.ctypes.data,
+                                  0 if env is None else env.shape[1],
+                                  0 if env is None else env.shape[0])
         return out
 
     def write_image(self, film_sum: np.ndarray, spp: int, path: str, kind: int = 0) -> bytes:

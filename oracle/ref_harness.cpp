@@ -376,7 +376,8 @@ int ref_cornell_render(int width, int height, int spp, int max_depth, uint64_t s
 int ref_render_scene(const float* tris, int ntri, const int32_t* mids, const float* mats, int nmat,
                      const float* lights, int nlights, const float* cam, int width, int height,
                      int spp, int max_depth, uint64_t seed, int light_sampler, int y0, int y1,
-                     int threads, float* samples) {
+                     int threads, float* samples, const float* env_pixels, int env_width,
+                     int env_height) {
     Scene scene;
     for (int m = 0; m < nmat; ++m) {
         const float* f = mats + size_t(m) * 11;
@@ -412,6 +413,12 @@ int ref_render_scene(const float* tris, int ntri, const int32_t* mids, const flo
         if (kind == 1) add_point_light(scene, vec3(f[1], f[2], f[3]), vec3(f[4], f[5], f[6]));
         if (kind == 2) add_distant_light(scene, vec3(f[1], f[2], f[3]), vec3(f[4], f[5], f[6]));
         if (kind == 3) add_uniform_infinite_light(scene, vec3(f[4], f[5], f[6]));
+        if (kind == 4 && env_pixels) {  // one image: env_pixels, row-major RGB
+            std::vector<vec3> px(static_cast<size_t>(env_width) * env_height);
+            for (size_t k = 0; k < px.size(); ++k)
+                px[k] = vec3(env_pixels[3 * k], env_pixels[3 * k + 1], env_pixels[3 * k + 2]);
+            add_image_infinite_light(scene, px, env_width, env_height, vec3(f[4], f[5], f[6]));
+        }
     }
     scene.camera = make_pinhole_camera(vec3(cam[0], cam[1], cam[2]), vec3(cam[3], cam[4], cam[5]),
                                        cam[6], cam[7]);

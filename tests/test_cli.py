@@ -75,7 +75,7 @@ def test_cli_cornell_matches_reference_cpu_tracer(cli, tmp_path):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("scene", ["direct-light", "point-light", "distant-light", "uniform-env",
-                                   "transparent-filter"])
+                                   "image-env", "transparent-filter"])
 def test_cli_renders_every_code_defined_scene(cli, tmp_path, scene):
     out = tmp_path / f"{scene}.pfm"
     r = _run(cli, "-gpu", "-scene", scene, "-size", "24", "24", "-spp", "8", "-output", str(out))
