@@ -340,8 +340,11 @@ typedef struct lux_scene_desc {
     int32_t image_count;
 } lux_scene_desc;
 
-/* RenderSettings (integrator/render_context.h:16-24).  light_sampler: 0 uniform,
- * 1 power (the reference default). */
+/* RenderSettings (integrator/render_context.h:16-24).  light_sampler
+ * (LightSamplerKind, light/light_distribution.h:27-31): 0 uniform, 1 power (the
+ * reference default), 2 light tree (`-light-sampler bvh`: area and point lights picked
+ * by a walk of a tree over their boxes weighted by power over squared distance, the
+ * other lights by power; falls back to power when no light has bounds). */
 typedef struct lux_render_request {
     int32_t width, height, spp, max_depth;
     uint64_t seed;
@@ -362,6 +365,19 @@ int lux_scene_destroy(lux_scene* scene);
 /* Number of scene triangles, area lights and all lights. */
 int lux_scene_info(const lux_scene* scene, int32_t* triangles, int32_t* area_lights,
                    int32_t* lights);
+
+/*
+ * Light selection as next-event estimation makes it, for validation: for each i, the
+ * light that select_u[i] picks at shading position positions[3i..3i+2] with sampler kind
+ * light_sampler (0 uniform, 1 power, 2 light tree), in light-table order (area lights in
+ * scene-triangle order, then the explicit lights), or -1; the pmf that selection
+ * reports; and the light's pmf at that position as MIS evaluates it.  Replaces
+ * sample_scene_light and light_pmf (scene/gpu_scene_light_sampler.cuh:9-96).  Host or
+ * device arrays; returns when the results are written.
+ */
+int lux_scene_select_lights(lux_ctx* ctx, const lux_scene* scene, int32_t light_sampler,
+                            const float* positions, const float* select_u, int32_t n,
+                            int32_t* light_index, float* pmf, float* eval_pmf);
 
 /*
  * New vertex positions for one mesh (same count): world triangles are recomputed and

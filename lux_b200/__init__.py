@@ -78,6 +78,7 @@ SIGNATURES = {
     "lux_scene_destroy": (ctypes.c_int, [_P]),
     "lux_scene_info": (ctypes.c_int, [_P, _P, _P, _P]),
     "lux_scene_update_mesh": (ctypes.c_int, [_P, _P, _I32, _P]),
+    "lux_scene_select_lights": (ctypes.c_int, [_P, _P, _I32, _P, _P, _I32, _P, _P, _P]),
     "lux_render": (ctypes.c_int, [_P, _P, _P, _P]),
     "lux_render_samples": (ctypes.c_int, [_P, _P, _P, _P]),
     "lux_render_ray_counts": (ctypes.c_int, [_P, _P]),

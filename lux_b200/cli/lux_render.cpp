@@ -3,14 +3,14 @@
 //
 // Options, defaults, validation, scene names, output paths and messages follow the
 // reference: -width/-height/-size, -spp, -depth, -scene, -output (explicit path),
-// -out (run directory out/<name>/<stem>.ppm), -gpu, -light-sampler power|uniform, -time,
+// -out (run directory out/<name>/<stem>.ppm), -gpu, -light-sampler power|uniform|bvh, -time,
 // -help.  The render uses RenderSettings' defaults (seed 0, frame 0, sample offset 0),
 // so a film equals the reference's `-gpu` film statistically and its CPU film per
 // sample.  Images are written as the reference writes them: PPM through write_ppm's
 // tone map, PFM when the path ends in ".pfm" (the pixel transforms run on the device,
 // lux_film_encode).  This build renders on the GPU only: without -gpu it still renders
-// on the GPU and says so.  Scenes that need asset files (bunny, dragon, lux-cover), the
-// BVH light sampler and the debug probes/AOVs are reported as unsupported.
+// on the GPU and says so.  Scenes that need asset files (bunny, dragon, lux-cover) and the
+// debug probes/AOVs are reported as unsupported.
 
 #include <chrono>
 #include <cmath>
@@ -102,8 +102,7 @@ bool parse(int argc, char** argv, Config& c) {
             } else if (std::strcmp(v, "uniform") == 0) {
                 c.light_sampler = 0;
             } else if (std::strcmp(v, "bvh") == 0) {
-                c.unsupported_option = true;
-                c.unsupported_name = "-light-sampler bvh";
+                c.light_sampler = 2;
             } else {
                 return false;
             }
@@ -138,7 +137,7 @@ void usage(const char* exe) {
         "  -width N / -height N / -size W H   film size (default 256x256)\n"
         "  -spp N                  samples per pixel (default 64)\n"
         "  -depth N                maximum path depth (default 4)\n"
-        "  -light-sampler KIND     power (default) or uniform\n"
+        "  -light-sampler KIND     power (default), uniform or bvh\n"
         "  -output PATH            image path (.ppm, or .pfm for linear floats)\n"
         "  -out NAME               write out/NAME/<NAME>.ppm\n"
         "  -gpu                    render with the GPU path (the only path of this build)\n"

@@ -621,8 +621,8 @@ static int render_common(lux_ctx* ctx, const lux_scene* scene, const lux_render_
         return lux::fail(LUX_ERR_INVALID_ARGUMENT, "render requires a non-empty film");
     if (req->max_depth < 0 || req->max_depth > 1000)
         return lux::fail(LUX_ERR_INVALID_ARGUMENT, "max_depth must be in 0..1000");
-    if (req->light_sampler != 0 && req->light_sampler != 1)
-        return lux::fail(LUX_ERR_INVALID_ARGUMENT, "light sampler: 0 uniform or 1 power");
+    if (req->light_sampler < 0 || req->light_sampler > 2)
+        return lux::fail(LUX_ERR_INVALID_ARGUMENT, "light sampler: 0 uniform, 1 power or 2 tree");
     if (static_cast<long long>(req->width) * req->height > (1ll << 30))
         return lux::fail(LUX_ERR_INVALID_ARGUMENT, "image too large");
     size_t pixels = static_cast<size_t>(req->width) * req->height;
@@ -647,6 +647,34 @@ int lux_render(lux_ctx* ctx, const lux_scene* scene, const lux_render_request* r
 int lux_render_samples(lux_ctx* ctx, const lux_scene* scene, const lux_render_request* req,
                        float* samples) {
     return render_common(ctx, scene, req, samples, true);
+}
+
+int lux_scene_select_lights(lux_ctx* ctx, const lux_scene* scene, int32_t light_sampler,
+                            const float* positions, const float* select_u, int32_t n,
+                            int32_t* light_index, float* pmf, float* eval_pmf) {
+    if (int st = check_ctx(ctx)) return st;
+    if (!scene || n < 0 || (n > 0 && (!positions || !select_u || !light_index || !pmf || !eval_pmf)))
+        return lux::fail(LUX_ERR_INVALID_ARGUMENT, "null argument");
+    if (light_sampler < 0 || light_sampler > 2)
+        return lux::fail(LUX_ERR_INVALID_ARGUMENT, "light sampler: 0 uniform, 1 power or 2 tree");
+    if (n == 0) return LUX_OK;
+    const size_t count = static_cast<size_t>(n);
+    Staging staging(ctx);
+    void *d_pos = nullptr, *d_u = nullptr, *d_index = nullptr, *d_pmf = nullptr, *d_eval = nullptr;
+    staging.add(positions, sizeof(float) * 3 * count, true, false, &d_pos);
+    staging.add(select_u, sizeof(float) * count, true, false, &d_u);
+    staging.add(light_index, sizeof(int32_t) * count, false, true, &d_index);
+    staging.add(pmf, sizeof(float) * count, false, true, &d_pmf);
+    staging.add(eval_pmf, sizeof(float) * count, false, true, &d_eval);
+    int st = staging.begin();
+    if (st) return st;
+    st = lux::select_lights(ctx, scene, light_sampler, static_cast<const float*>(d_pos),
+                            static_cast<const float*>(d_u), n, static_cast<int32_t*>(d_index),
+                            static_cast<float*>(d_pmf), static_cast<float*>(d_eval));
+    if (st) return st;
+    st = finish_call(ctx, staging);
+    if (st) return st;
+    return sync_and_check(ctx);
 }
 
 int lux_render_ray_counts(lux_ctx* ctx, int64_t* counts) {

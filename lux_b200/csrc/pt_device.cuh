@@ -172,6 +172,16 @@ struct AliasEntry {  // light/light_distribution.h:22-26
     float pmf;
 };
 
+// LightBvhNode (light/light_distribution.h:33-40): a box around the lights below, their
+// summed power, the children and parent (-1 none) and, in a leaf, the light's index.
+struct LightNode {
+    f3 lo;
+    float power;
+    f3 hi;
+    int light;   // -1 in an internal node
+    int left, right, parent, pad;
+};
+
 struct Camera {  // camera/camera.h:29-38 (perspective)
     f3 origin, lower_left, horizontal, vertical, lens_u, lens_v;
     float lens_radius;
@@ -194,6 +204,19 @@ struct SceneView {
     float total_light_power;
     const AliasEntry* light_alias;   // power alias table, light_count entries
     int light_sampler;               // 0 uniform, 1 power
+    // Light tree for the tree sampler (LightBvhTable, light/light_distribution.h:75-88):
+    // area and point lights in the tree, the others (distant, infinite) in a power table
+    // beside it.  light_tree is null when no light has bounds; the tree sampler then
+    // picks by power.
+    const LightNode* light_tree;
+    int light_tree_count;
+    int light_tree_root;
+    const int* light_leaf;           // light index -> leaf node, -1 outside the tree
+    const int* light_other_slot;     // light index -> slot of the other table, -1 none
+    const int* other_lights;         // slot -> light index
+    const AliasEntry* other_alias;   // alias table over the other lights' power
+    int other_count;
+    float other_power;
     const int* primitive_light;      // scene triangle -> light index (-1 none, -2 several)
     bool has_two_level;
     bool has_passthrough;            // some material is an interface or transparent filter

@@ -452,12 +452,6 @@ struct TwoLevelWalk {
 
 // ------------------------------------------------------------------ lights
 
-LUX_D float light_pmf(const SceneView& sc, int sampler, int index) {  // gpu_scene_light_sampler.cuh:9-45
-    if (index < 0 || index >= sc.light_count || sc.total_light_power <= 0) return 0;
-    if (sampler == 0) return 1.0f / static_cast<float>(sc.light_count);
-    return sc.light_alias ? sc.light_alias[index].pmf : 0.0f;
-}
-
 // sample_alias_table_index (light/light_sampler.h:71-82).
 LUX_D int sample_alias(const AliasEntry* table, int count, float u) {
     float scaled = mul(fminf(u, 0.99999994f), static_cast<float>(count));
@@ -467,6 +461,185 @@ LUX_D int sample_alias(const AliasEntry* table, int count, float u) {
     const AliasEntry& e = table[column];
     int index = threshold < e.probability ? column : e.alias;
     return index >= 0 && index < count ? index : -1;
+}
+
+// ---- light tree (light/light_sampler.h:90-348).  Every walk is bounded by the node
+// count, as the reference's.
+
+// light_bvh_node_importance with squared_distance_to_bounds: power over the squared
+// distance from p to the node's box, the distance kept at least kRayEpsilon.
+LUX_D float light_node_importance(const SceneView& sc, int i, f3 p) {
+    if (i < 0 || i >= sc.light_tree_count) return 0;
+    const LightNode& n = sc.light_tree[i];
+    if (n.power <= 0 || n.lo.x > n.hi.x || n.lo.y > n.hi.y || n.lo.z > n.hi.z) return 0;
+    const float pa[3] = {p.x, p.y, p.z};
+    const float lo[3] = {n.lo.x, n.lo.y, n.lo.z};
+    const float hi[3] = {n.hi.x, n.hi.y, n.hi.z};
+    float d2 = 0;
+    for (int a = 0; a < 3; ++a) {
+        float delta = 0;
+        if (pa[a] < lo[a]) delta = sub(lo[a], pa[a]);
+        else if (pa[a] > hi[a]) delta = sub(pa[a], hi[a]);
+        d2 = add(d2, mul(delta, delta));
+    }
+    d2 = fmaxf(d2, mul(kRayEpsilon, kRayEpsilon));
+    return n.power / d2;
+}
+
+// light_bvh_child_probability: the child's share of its parent's two importances.
+LUX_D float light_child_probability(const SceneView& sc, int parent, int child, f3 p) {
+    const int count = sc.light_tree_count;
+    if (parent < 0 || parent >= count || child < 0 || child >= count) return 0;
+    const LightNode& n = sc.light_tree[parent];
+    if (child != n.left && child != n.right) return 0;
+    const float l = light_node_importance(sc, n.left, p);
+    const float r = light_node_importance(sc, n.right, p);
+    const float total = add(l, r);
+    if (total <= 0) return 0;
+    const float lp = l / total;
+    return child == n.left ? lp : sub(1.0f, lp);
+}
+
+// sample_light_bvh: root to leaf, the draw rescaled at each step.
+LUX_D int sample_light_tree(const SceneView& sc, f3 p, float select_u, float& pmf) {
+    pmf = 0;
+    const int count = sc.light_tree_count;
+    int node = sc.light_tree_root;
+    if (!sc.light_tree || node < 0 || node >= count) return -1;
+    float u = fminf(select_u, 0.99999994f);
+    pmf = 1;
+    for (int depth = 0; depth < count; ++depth) {
+        const LightNode& n = sc.light_tree[node];
+        if (n.light >= 0) return n.light;
+        const float lp = light_child_probability(sc, node, n.left, p);
+        if (lp <= 0) {
+            node = n.right;
+        } else if (lp >= 1) {
+            node = n.left;
+        } else if (u < lp) {
+            pmf = mul(pmf, lp);
+            u = u / lp;
+            node = n.left;
+        } else {
+            const float rp = sub(1.0f, lp);
+            pmf = mul(pmf, rp);
+            u = sub(u, lp) / rp;
+            node = n.right;
+        }
+        if (node < 0 || node >= count) {
+            pmf = 0;
+            return -1;
+        }
+    }
+    pmf = 0;
+    return -1;
+}
+
+// light_bvh_pmf: the product of child probabilities from the light's leaf to the root.
+LUX_D float light_tree_pmf(const SceneView& sc, f3 p, int light) {
+    const int count = sc.light_tree_count;
+    if (!sc.light_tree || !sc.light_leaf || light < 0 || light >= sc.light_count) return 0;
+    int node = sc.light_leaf[light];
+    if (node < 0 || node >= count) return 0;
+    float pmf = 1;
+    for (int depth = 0; depth < count; ++depth) {
+        const int parent = sc.light_tree[node].parent;
+        if (parent < 0) return pmf;
+        const float pr = light_child_probability(sc, parent, node, p);
+        if (pr <= 0) return 0;
+        pmf = mul(pmf, pr);
+        node = parent;
+        if (node >= count) return 0;
+    }
+    return 0;
+}
+
+// The tree's share of the total power and the other table's power
+// (sample_light_bvh_mixture / light_bvh_mixture_pmf, light/light_sampler.h:265-359).
+LUX_D bool light_tree_split(const SceneView& sc, float& tree_p, float& other) {
+    const float tree_power = sc.light_tree[sc.light_tree_root].power;
+    if (tree_power <= 0) return false;
+    other = sc.other_count > 0 ? fmaxf(0.0f, sc.other_power) : 0.0f;
+    const float total = add(tree_power, other);
+    if (total <= 0) return false;
+    tree_p = tree_power / total;
+    return true;
+}
+
+// sample_indexed_discrete_light over the other table's alias entries.
+LUX_D int sample_other_light(const SceneView& sc, float u, float& pmf) {
+    pmf = 0;
+    if (!sc.other_lights || !sc.other_alias || sc.other_count <= 0 || sc.other_power <= 0)
+        return -1;
+    const int slot = sample_alias(sc.other_alias, sc.other_count, u);
+    if (slot < 0) return -1;
+    pmf = sc.other_alias[slot].pmf;
+    return pmf > 0 ? sc.other_lights[slot] : -1;
+}
+
+LUX_D int sample_light_mixture(const SceneView& sc, f3 p, float select_u, float& pmf) {
+    pmf = 0;
+    float tree_p, other;
+    if (!light_tree_split(sc, tree_p, other)) return -1;
+    if (other <= 0 || tree_p >= 1) return sample_light_tree(sc, p, select_u, pmf);
+    if (tree_p <= 0) return sample_other_light(sc, select_u, pmf);
+    const float u = fminf(select_u, 0.99999994f);
+    float part = 0;
+    int index;
+    if (u < tree_p) {
+        index = sample_light_tree(sc, p, u / tree_p, part);
+        pmf = mul(tree_p, part);
+    } else {
+        const float other_p = sub(1.0f, tree_p);
+        index = sample_other_light(sc, sub(u, tree_p) / other_p, part);
+        pmf = mul(other_p, part);
+    }
+    return pmf > 0 ? index : -1;
+}
+
+LUX_D float light_mixture_pmf(const SceneView& sc, f3 p, int light) {
+    float tree_p, other;
+    if (light < 0 || !light_tree_split(sc, tree_p, other)) return 0;
+    if (light < sc.light_count && sc.light_leaf[light] >= 0)
+        return mul(tree_p, light_tree_pmf(sc, p, light));
+    const int slot = light < sc.light_count && sc.light_other_slot ? sc.light_other_slot[light] : -1;
+    if (slot < 0 || other <= 0 || !sc.other_alias) return 0;
+    return mul(sub(1.0f, tree_p), sc.other_alias[slot].pmf);
+}
+
+LUX_D bool use_light_tree(const SceneView& sc, int sampler) {
+    return sampler == 2 && sc.light_tree && sc.light_leaf && sc.light_tree_count > 0 &&
+           sc.light_tree_root >= 0 && sc.light_tree_root < sc.light_tree_count;
+}
+
+// light_pmf (gpu_scene_light_sampler.cuh:9-45): the selection probability of a light at
+// shading position p; p matters to the tree sampler only.
+LUX_D float light_pmf(const SceneView& sc, int sampler, f3 p, int index) {
+    if (index < 0 || index >= sc.light_count || sc.total_light_power <= 0) return 0;
+    if (sampler == 0) return 1.0f / static_cast<float>(sc.light_count);
+    if (use_light_tree(sc, sampler)) return light_mixture_pmf(sc, p, index);
+    return sc.light_alias ? sc.light_alias[index].pmf : 0.0f;
+}
+
+// sample_scene_light (gpu_scene_light_sampler.cuh:47-96): the light picked by select_u
+// at shading position p and its pmf (the tree walk's own, else light_pmf); -1 when none.
+LUX_D int select_light(const SceneView& sc, int sampler, f3 p, float select_u, float& pmf) {
+    pmf = 0;
+    if (sc.light_count <= 0 || sc.total_light_power <= 0) return -1;
+    int index;
+    float selected = 0;
+    if (sampler == 0) {
+        index = static_cast<int>(mul(fminf(select_u, 0.99999994f), static_cast<float>(sc.light_count)));
+        if (index >= sc.light_count) index = sc.light_count - 1;
+    } else if (use_light_tree(sc, sampler)) {
+        index = sample_light_mixture(sc, p, select_u, selected);
+    } else {
+        if (!sc.light_alias) return -1;
+        index = sample_alias(sc.light_alias, sc.light_count, select_u);
+    }
+    if (index < 0) return -1;
+    pmf = selected > 0 ? selected : light_pmf(sc, sampler, p, index);
+    return index;
 }
 
 struct LightLi {
@@ -573,18 +746,9 @@ LUX_D LightLi env_sample(const EnvLight& e, float select_u, float ux, float uy) 
 LUX_D LightLi sample_light(const SceneView& sc, int sampler, f3 p, float select_u, float comp_u, float ux,
                            float uy) {
     LightLi li;
-    if (sc.light_count <= 0 || sc.total_light_power <= 0) return li;
-    int index;
-    if (sampler == 0) {
-        index = static_cast<int>(mul(fminf(select_u, 0.99999994f), static_cast<float>(sc.light_count)));
-        if (index >= sc.light_count) index = sc.light_count - 1;
-    } else {
-        if (!sc.light_alias) return li;
-        index = sample_alias(sc.light_alias, sc.light_count, select_u);
-    }
-    if (index < 0) return li;
-    float pmf = light_pmf(sc, sampler, index);
-    if (!(pmf > 0)) return li;
+    float pmf;
+    const int index = select_light(sc, sampler, p, select_u, pmf);
+    if (index < 0 || !(pmf > 0)) return li;
     const Light L = sc.lights[index];
     if (L.kind == 0) {
         const SceneTri& t = sc.tris[L.primitive];
@@ -655,9 +819,9 @@ LUX_D float infinite_pdf(const SceneView& sc, int sampler, f3 dir) {  // infinit
     for (int i = 0; i < sc.light_count; ++i) {
         const Light& L = sc.lights[i];
         if (L.kind == 3) {
-            pdf = add(pdf, mul(light_pmf(sc, sampler, i), 1.0f / mul(4.0f, kPi)));
+            pdf = add(pdf, mul(light_pmf(sc, sampler, splat(0.0f), i), 1.0f / mul(4.0f, kPi)));
         } else if (L.kind == 4 && sc.env && L.primitive >= 0) {
-            pdf = add(pdf, mul(light_pmf(sc, sampler, i), env_pdf(sc.env[L.primitive], dir)));
+            pdf = add(pdf, mul(light_pmf(sc, sampler, splat(0.0f), i), env_pdf(sc.env[L.primitive], dir)));
         }
     }
     return pdf;
@@ -760,7 +924,7 @@ LUX_D float surface_light_pdf(const SceneView& sc, int sampler, int prim, f3 ng,
     int li = sc.primitive_light[prim];
     if (li >= 0 && li < sc.light_count && sc.lights[li].kind == 0 && sc.lights[li].area > 0) {
         const Light& L = sc.lights[li];
-        return mul(light_pmf(sc, sampler, li), solid_angle_pdf(pos, ng, L.two_sided, 1.0f / L.area, ref));
+        return mul(light_pmf(sc, sampler, ref, li), solid_angle_pdf(pos, ng, L.two_sided, 1.0f / L.area, ref));
     }
     return 0.0f;
 }

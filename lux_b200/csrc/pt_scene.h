@@ -36,6 +36,12 @@ struct lux_scene {
     float* env_pixels = nullptr;        // image-light texels (device)
     float* env_cdf = nullptr;           // image-light running weights (device)
     lux::pt::EnvLight* d_env = nullptr; // image lights (device)
+    // Light tree and the table of the lights outside it (device; null without a tree).
+    lux::pt::LightNode* light_tree = nullptr;
+    int* light_leaf = nullptr;
+    int* light_other_slot = nullptr;
+    int* other_lights = nullptr;
+    lux::pt::AliasEntry* other_alias = nullptr;
     // Device buffers of vertex updates, allocated on a mesh's first update.
     struct MeshRefit {
         float* vertices = nullptr;       // object space, 3 per vertex
@@ -65,6 +71,11 @@ int camera_perspective(const float* origin, const float* look_at, float vfov, fl
 int render(lux_ctx* ctx, const lux_scene* scene, const lux_render_request& req, float* out,
            bool per_sample);
 int render_ray_counts(lux_ctx* ctx, int64_t* counts);
+// Light selection queries (device arrays): sample_scene_light and light_pmf at each
+// position, as next-event estimation makes them.
+int select_lights(lux_ctx* ctx, const lux_scene* scene, int sampler, const float* positions,
+                  const float* select_u, int n, int32_t* light_index, float* pmf,
+                  float* eval_pmf);
 void render_runtime_free(lux_ctx* ctx);
 
 }  // namespace lux

@@ -8,6 +8,7 @@
 //   scene triangle order (instances, then local triangles)  scene/scene_data.h:282-329
 //   prepare_scene_light_sampling (area + explicit lights)   scene/scene_prepare.h:268-387
 //   build_alias_table_from_weights                          light/light_distribution.cpp:8-61
+//   build_light_bvh (the light tree)                        light/light_distribution.cpp:68-161
 // The host compiler evaluates these without contraction (x86-64 baseline ISA).
 
 #include <cuda_runtime.h>
@@ -150,6 +151,111 @@ std::vector<AliasEntry> alias_from_weights(const std::vector<float>& weights) {
     return table;
 }
 
+// ---- light tree (build_light_bvh, light/light_distribution.cpp:68-161)
+
+struct LightItem {  // LightBvhBuildItem (light/light_distribution.h:42-47)
+    Box box;
+    V3 centroid;
+    int light;
+    float power;
+};
+
+V3 centre(const Box& b) {  // AABB::centroid
+    return v3((b.lo.x + b.hi.x) * 0.5f, (b.lo.y + b.hi.y) * 0.5f, (b.lo.z + b.hi.z) * 0.5f);
+}
+
+struct LightTree {
+    std::vector<pt::LightNode> nodes;   // preorder, the root first
+    std::vector<int> leaf;              // light index -> leaf node, -1 outside the tree
+    std::vector<int> other_slot;        // light index -> slot of other_lights, -1 none
+    std::vector<int> other_lights;      // the lights outside the tree with a positive weight
+    std::vector<AliasEntry> other_alias;
+    float other_power = 0;
+};
+
+float axis_of(const V3& v, int axis) { return axis == 0 ? v.x : axis == 1 ? v.y : v.z; }
+
+// Nodes for items[begin, end): a leaf per light; otherwise a median split on the widest
+// axis of the centroids' box, the median placed by std::nth_element with the reference's
+// comparison, so that the same items in the same order give the same tree.  An internal
+// node holds the union of its children's boxes and the sum of their powers.
+int light_tree_range(std::vector<LightItem>& items, int begin, int end, int parent,
+                     LightTree& t) {
+    const int index = static_cast<int>(t.nodes.size());
+    t.nodes.push_back(pt::LightNode{});
+    pt::LightNode node{};
+    node.parent = parent;
+    node.left = node.right = -1;
+    if (end - begin == 1) {
+        const LightItem& it = items[begin];
+        node.lo = make_f3(it.box.lo.x, it.box.lo.y, it.box.lo.z);
+        node.hi = make_f3(it.box.hi.x, it.box.hi.y, it.box.hi.z);
+        node.power = it.power;
+        node.light = it.light;
+        t.leaf[it.light] = index;
+        t.nodes[index] = node;
+        return index;
+    }
+    Box centroids;
+    for (int i = begin; i < end; ++i) centroids.expand(items[i].centroid);
+    const V3 d = v3(centroids.hi.x - centroids.lo.x, centroids.hi.y - centroids.lo.y,
+                    centroids.hi.z - centroids.lo.z);
+    const int axis = (d.x > d.y && d.x > d.z) ? 0 : (d.y > d.z) ? 1 : 2;  // max_extent_axis
+    const int mid = begin + (end - begin) / 2;
+    std::nth_element(items.begin() + begin, items.begin() + mid, items.begin() + end,
+                     [axis](const LightItem& a, const LightItem& b) {
+                         return axis_of(a.centroid, axis) < axis_of(b.centroid, axis);
+                     });
+    const int left = light_tree_range(items, begin, mid, index, t);
+    const int right = light_tree_range(items, mid, end, index, t);
+    const pt::LightNode& l = t.nodes[left];
+    const pt::LightNode& r = t.nodes[right];
+    node.left = left;
+    node.right = right;
+    node.light = -1;
+    node.power = l.power + r.power;
+    node.lo = make_f3(std::fmin(l.lo.x, r.lo.x), std::fmin(l.lo.y, r.lo.y), std::fmin(l.lo.z, r.lo.z));
+    node.hi = make_f3(std::fmax(l.hi.x, r.hi.x), std::fmax(l.hi.y, r.hi.y), std::fmax(l.hi.z, r.hi.z));
+    t.nodes[index] = node;
+    return index;
+}
+
+// The tree over items (lights with bounds, in light-index order) and the power table of
+// the other lights, their weights taken from the selection table's running sums cdf.
+LightTree build_light_tree(std::vector<LightItem> items, const std::vector<float>& cdf) {
+    LightTree t;
+    const int count = static_cast<int>(cdf.size());
+    if (items.empty() || count == 0) return t;
+    std::vector<char> seen(count, 0);
+    for (const LightItem& it : items) seen[it.light] = 1;
+    t.other_slot.assign(count, -1);
+    std::vector<float> other_cdf;
+    float other_weight = 0;
+    for (int i = 0; i < count; ++i) {
+        if (seen[i]) continue;
+        const float w = cdf[i] - (i == 0 ? 0.0f : cdf[i - 1]);
+        if (w <= 0) continue;
+        other_weight += w;
+        t.other_slot[i] = static_cast<int>(t.other_lights.size());
+        t.other_lights.push_back(i);
+        other_cdf.push_back(other_weight);
+    }
+    t.other_power = other_weight;
+    if (!other_cdf.empty() && other_weight > 0) {  // build_alias_table_from_cdf
+        std::vector<float> w;
+        float prev = 0;
+        for (float c : other_cdf) {
+            w.push_back(c - prev);
+            prev = c;
+        }
+        t.other_alias = alias_from_weights(w);
+    }
+    t.leaf.assign(count, -1);
+    t.nodes.reserve(items.size() * 2 - 1);
+    light_tree_range(items, 0, static_cast<int>(items.size()), -1, t);
+    return t;
+}
+
 template <typename T>
 int upload(T** dst, const std::vector<T>& src, cudaStream_t stream) {
     size_t bytes = sizeof(T) * std::max<size_t>(src.size(), 1);
@@ -270,7 +376,8 @@ void scene_free(lux_scene* s) {
     s->refit.clear();
     void* ptrs[] = {s->materials, s->tris, s->shading, s->d_instances, s->tlas_instance,
                     s->blas_views, s->lights, s->light_alias, s->primitive_light, s->tri_soup,
-                    s->tlas_boxes, s->env_pixels, s->env_cdf, s->d_env};
+                    s->tlas_boxes, s->env_pixels, s->env_cdf, s->d_env, s->light_tree,
+                    s->light_leaf, s->light_other_slot, s->other_lights, s->other_alias};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     for (lux_bvh* b : s->blas) lux_bvh_destroy(b);
@@ -343,7 +450,7 @@ int scene_create(lux_ctx* ctx, const lux_scene_desc* d, lux_scene** out) {
 
     // Light tables (scene/scene_prepare.h:268-387).
     std::vector<Light> lights;
-    std::vector<float> cdf;
+    std::vector<float> cdf, light_power;
     float total_power = 0;
     primitive_light.assign(tris.size(), -1);
     auto append = [&](const Light& l, float power) -> int {
@@ -351,6 +458,7 @@ int scene_create(lux_ctx* ctx, const lux_scene_desc* d, lux_scene** out) {
         total_power += power;
         lights.push_back(l);
         cdf.push_back(total_power);
+        light_power.push_back(power);
         return static_cast<int>(lights.size()) - 1;
     };
     for (size_t t = 0; t < tris.size(); ++t) {
@@ -432,6 +540,27 @@ int scene_create(lux_ctx* ctx, const lux_scene_desc* d, lux_scene** out) {
     }
     std::vector<AliasEntry> alias = total_power > 0 ? alias_from_weights(weights)
                                                     : std::vector<AliasEntry>{};
+    // Light tree over the lights with bounds: area lights (their triangle's box) and
+    // point lights (their position), in light-index order (light_bvh_items and
+    // light_bounds_for_bvh, scene/scene_prepare.h:243-296).
+    std::vector<LightItem> items;
+    for (int i = 0; i < static_cast<int>(lights.size()); ++i) {
+        const Light& l = lights[i];
+        Box b;
+        if (l.kind == 0) {
+            const pt::SceneTri& t = tris[l.primitive];
+            b.expand(v3(t.v0.x, t.v0.y, t.v0.z));
+            b.expand(v3(t.v1.x, t.v1.y, t.v1.z));
+            b.expand(v3(t.v2.x, t.v2.y, t.v2.z));
+        } else if (l.kind == 1) {
+            b.lo = b.hi = v3(l.vec.x, l.vec.y, l.vec.z);
+        } else {
+            continue;
+        }
+        if (b.empty()) continue;
+        items.push_back(LightItem{b, centre(b), i, light_power[i]});
+    }
+    const LightTree tree = build_light_tree(items, cdf);
 
     // Uploads.
     std::vector<Material> mats;
@@ -452,6 +581,13 @@ int scene_create(lux_ctx* ctx, const lux_scene_desc* d, lux_scene** out) {
     }
     if (!st) st = upload(&s->light_alias, alias, ctx->stream);
     if (!st) st = upload(&s->primitive_light, primitive_light, ctx->stream);
+    if (!st && !tree.nodes.empty()) {
+        st = upload(&s->light_tree, tree.nodes, ctx->stream);
+        if (!st) st = upload(&s->light_leaf, tree.leaf, ctx->stream);
+        if (!st) st = upload(&s->light_other_slot, tree.other_slot, ctx->stream);
+        if (!st) st = upload(&s->other_lights, tree.other_lights, ctx->stream);
+        if (!st) st = upload(&s->other_alias, tree.other_alias, ctx->stream);
+    }
 
     // BLAS per mesh over object-space soups.
     std::vector<float> all_soup;
@@ -518,6 +654,15 @@ int scene_create(lux_ctx* ctx, const lux_scene_desc* d, lux_scene** out) {
     v.total_light_power = total_power;
     v.light_alias = alias.empty() ? nullptr : s->light_alias;
     v.light_sampler = 1;
+    v.light_tree = tree.nodes.empty() ? nullptr : s->light_tree;
+    v.light_tree_count = static_cast<int>(tree.nodes.size());
+    v.light_tree_root = tree.nodes.empty() ? -1 : 0;
+    v.light_leaf = tree.nodes.empty() ? nullptr : s->light_leaf;
+    v.light_other_slot = tree.nodes.empty() ? nullptr : s->light_other_slot;
+    v.other_lights = tree.other_lights.empty() ? nullptr : s->other_lights;
+    v.other_alias = tree.other_alias.empty() ? nullptr : s->other_alias;
+    v.other_count = static_cast<int>(tree.other_lights.size());
+    v.other_power = tree.other_power;
     v.primitive_light = s->primitive_light;
     v.has_two_level = s->tlas->n > 0 && d->instance_count > 0;
     v.has_passthrough = false;

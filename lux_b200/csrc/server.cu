@@ -871,8 +871,8 @@ int lux_server_submit(lux_server* s, int32_t scene, const lux_render_request* re
         return server_fail(LUX_ERR_INVALID_ARGUMENT, "render requires a non-empty film");
     if (req->max_depth < 0 || req->max_depth > 1000)
         return server_fail(LUX_ERR_INVALID_ARGUMENT, "max_depth must be in 0..1000");
-    if (req->light_sampler != 0 && req->light_sampler != 1)
-        return server_fail(LUX_ERR_INVALID_ARGUMENT, "light sampler: 0 uniform or 1 power");
+    if (req->light_sampler < 0 || req->light_sampler > 2)
+        return server_fail(LUX_ERR_INVALID_ARGUMENT, "light sampler: 0 uniform, 1 power or 2 tree");
     if (static_cast<long long>(req->width) * req->height > (1ll << 30))
         return server_fail(LUX_ERR_INVALID_ARGUMENT, "image too large");
     auto r = std::make_unique<lux_server_request>();

@@ -174,6 +174,20 @@ __global__ void __launch_bounds__(kThreads) k_flush(PathPool rt, Batch b, float*
     }
 }
 
+// One light selection per thread at a given position (sample_scene_light + light_pmf).
+__global__ void k_select_lights(SceneView sc, int sampler, const float* positions,
+                                const float* select_u, int n, int32_t* light_index, float* pmf,
+                                float* eval_pmf) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const f3 p = make_f3(positions[3 * i], positions[3 * i + 1], positions[3 * i + 2]);
+    float selected = 0;
+    const int index = select_light(sc, sampler, p, select_u[i], selected);
+    light_index[i] = index;
+    pmf[i] = selected;
+    eval_pmf[i] = index >= 0 ? light_pmf(sc, sampler, p, index) : 0.0f;
+}
+
 __global__ void k_count_rays(const int* counts, unsigned long long* rays, int depth_slots) {
     unsigned long long total = 0;
     for (int d = 0; d < depth_slots; ++d) total += static_cast<unsigned>(counts[d * kSlots]);
@@ -267,6 +281,16 @@ void render_runtime_free(lux_ctx* ctx) {
     pt::runtime_release(rt);
     delete rt;
     ctx->render_runtime = nullptr;
+}
+
+int select_lights(lux_ctx* ctx, const lux_scene* scene, int sampler, const float* positions,
+                  const float* select_u, int n, int32_t* light_index, float* pmf,
+                  float* eval_pmf) {
+    pt::k_select_lights<<<(n + pt::kThreads - 1) / pt::kThreads, pt::kThreads, 0, ctx->stream>>>(
+        scene->view, sampler, positions, select_u, n, light_index, pmf, eval_pmf);
+    ctx->launches += 1;
+    cudaError_t err = cudaGetLastError();
+    return err == cudaSuccess ? LUX_OK : cuda_fail(err, "light selection");
 }
 
 int render_ray_counts(lux_ctx* ctx, int64_t* counts) {

@@ -17,7 +17,7 @@ from . import _check, _ptr, load_library
 
 LAMBERT, THIN_LAMBERT, GGX, DIELECTRIC, INTERFACE, TRANSPARENT = range(6)
 LIGHT_POINT, LIGHT_DISTANT, LIGHT_UNIFORM_INFINITE, LIGHT_IMAGE_INFINITE = 1, 2, 3, 4
-SAMPLER_UNIFORM, SAMPLER_POWER = 0, 1
+SAMPLER_UNIFORM, SAMPLER_POWER, SAMPLER_TREE = 0, 1, 2   # LightSamplerKind (Uniform, Power, Bvh)
 
 _F3 = ctypes.c_float * 3
 _F12 = ctypes.c_float * 12
@@ -260,6 +260,23 @@ class Scene:
         t, a, l = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32()
         _check(self._lib.lux_scene_info(self._h, ctypes.byref(t), ctypes.byref(a), ctypes.byref(l)))
         return {"triangles": t.value, "area_lights": a.value, "lights": l.value}
+
+    def select_lights(self, positions: np.ndarray, select_u: np.ndarray,
+                      light_sampler=SAMPLER_TREE):
+        """sample_scene_light + light_pmf at each position: (light index or -1, the
+        selection's pmf, light_pmf of that light)."""
+        pos = np.ascontiguousarray(positions, np.float32).reshape(-1, 3)
+        u = np.ascontiguousarray(select_u, np.float32).reshape(-1)
+        n = len(u)
+        assert len(pos) == n
+        index = np.zeros(n, np.int32)
+        pmf = np.zeros(n, np.float32)
+        eval_pmf = np.zeros(n, np.float32)
+        _check(self._lib.lux_scene_select_lights(self.ctx.handle, self._h, light_sampler,
+                                                 pos.ctypes.data, u.ctypes.data, n,
+                                                 index.ctypes.data, pmf.ctypes.data,
+                                                 eval_pmf.ctypes.data))
+        return index, pmf, eval_pmf
 
     def update_mesh(self, mesh: int, vertices: np.ndarray) -> None:
         v = np.ascontiguousarray(vertices, np.float32)

@@ -116,6 +116,8 @@ class Ref:
                                            _P, _P, _P]
         lib.ref_render_scene.argtypes = [_P, _I, _P, _P, _I, _P, _I, _P, _I, _I, _I, _I,
                                          ctypes.c_uint64, _I, _I, _I, _I, _P, _P, _I, _I]
+        lib.ref_select_lights.argtypes = [_P, _I, _P, _P, _I, _P, _I, _P, _I, _P, _P, _I,
+                                          _P, _P, _P]
         lib.ref_tree_create.argtypes = [_P, _I, _I]
         lib.ref_tree_create.restype = _P
         lib.ref_tree_destroy.argtypes = [_P]
@@ -145,6 +147,28 @@ class Ref:
                                   0 if env is None else env.shape[1],
                                   0 if env is None else env.shape[0])
         return out
+
+    def select_lights(self, tris, material_ids, materials, lights, camera, light_sampler,
+                      positions, select_u):
+        """sample_light + light_pmf of a single-mesh scene (as render_scene builds it) at
+        each position: (light index or -1, the selection's pmf, light_pmf)."""
+        tris = np.ascontiguousarray(tris, np.float32)
+        mids = np.ascontiguousarray(material_ids, np.int32)
+        mats = np.ascontiguousarray(materials, np.float32)
+        lights = np.ascontiguousarray(lights, np.float32).reshape(-1, 7)
+        cam = np.ascontiguousarray(camera, np.float32)
+        pos = np.ascontiguousarray(positions, np.float32).reshape(-1, 3)
+        u = np.ascontiguousarray(select_u, np.float32).reshape(-1)
+        n = len(u)
+        index = np.zeros(n, np.int32)
+        pmf = np.zeros(n, np.float32)
+        eval_pmf = np.zeros(n, np.float32)
+        self.lib.ref_select_lights(tris.ctypes.data, len(tris), mids.ctypes.data, mats.ctypes.data,
+                                   len(mats), lights.ctypes.data if len(lights) else None,
+                                   len(lights), cam.ctypes.data, light_sampler, pos.ctypes.data,
+                                   u.ctypes.data, n, index.ctypes.data, pmf.ctypes.data,
+                                   eval_pmf.ctypes.data)
+        return index, pmf, eval_pmf
 
     def write_image(self, film_sum: np.ndarray, spp: int, path: str, kind: int = 0) -> bytes:
         """The reference's write_ppm (0), write_debug_ppm_linear (1) or write_pfm (2) on a

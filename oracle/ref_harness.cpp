@@ -373,11 +373,10 @@ int ref_cornell_render(int width, int height, int spp, int max_depth, uint64_t s
 // lights as 7 floats (kind 1 point / 2 distant / 3 uniform infinite, vec3, value3);
 // camera: origin3, look_at3, vertical fov degrees, aspect (make_pinhole_camera).
 // samples receives [pixel][spp][3] for rows [y0, y1).
-int ref_render_scene(const float* tris, int ntri, const int32_t* mids, const float* mats, int nmat,
-                     const float* lights, int nlights, const float* cam, int width, int height,
-                     int spp, int max_depth, uint64_t seed, int light_sampler, int y0, int y1,
-                     int threads, float* samples, const float* env_pixels, int env_width,
-                     int env_height) {
+static Scene build_single_mesh_scene(const float* tris, int ntri, const int32_t* mids,
+                                     const float* mats, int nmat, const float* lights,
+                                     int nlights, const float* cam, const float* env_pixels,
+                                     int env_width, int env_height) {
     Scene scene;
     for (int m = 0; m < nmat; ++m) {
         const float* f = mats + size_t(m) * 11;
@@ -422,11 +421,27 @@ int ref_render_scene(const float* tris, int ntri, const int32_t* mids, const flo
     }
     scene.camera = make_pinhole_camera(vec3(cam[0], cam[1], cam[2]), vec3(cam[3], cam[4], cam[5]),
                                        cam[6], cam[7]);
+    return scene;
+}
+
+static LightSamplerKind sampler_kind(int light_sampler) {
+    return light_sampler == 0 ? LightSamplerKind::Uniform
+         : light_sampler == 2 ? LightSamplerKind::Bvh
+                              : LightSamplerKind::Power;
+}
+
+int ref_render_scene(const float* tris, int ntri, const int32_t* mids, const float* mats, int nmat,
+                     const float* lights, int nlights, const float* cam, int width, int height,
+                     int spp, int max_depth, uint64_t seed, int light_sampler, int y0, int y1,
+                     int threads, float* samples, const float* env_pixels, int env_width,
+                     int env_height) {
+    Scene scene = build_single_mesh_scene(tris, ntri, mids, mats, nmat, lights, nlights, cam,
+                                          env_pixels, env_width, env_height);
     PreparedScene prepared(std::move(scene));
     prepared.prepare_host_bvh();
     SceneLightSampler lights_sampler = make_scene_light_sampler(
         prepared.host_scene(), prepared.light_sampling(),
-        light_sampler == 0 ? LightSamplerKind::Uniform : LightSamplerKind::Power);
+        sampler_kind(light_sampler));
     RenderSettings settings;
     settings.max_depth = max_depth;
     settings.seed = seed;
@@ -453,6 +468,29 @@ int ref_render_scene(const float* tris, int ntri, const int32_t* mids, const flo
             }
         }
     });
+    return 0;
+}
+
+// sample_light and light_pmf (scene/scene_light_sampler.h:100-200) of the same scene at
+// given shading positions: the picked light index (-1 none), the selection's pmf and
+// light_pmf of the picked light.
+int ref_select_lights(const float* tris, int ntri, const int32_t* mids, const float* mats,
+                      int nmat, const float* lights, int nlights, const float* cam,
+                      int light_sampler, const float* positions, const float* select_u, int n,
+                      int32_t* light_index, float* pmf, float* eval_pmf) {
+    Scene scene = build_single_mesh_scene(tris, ntri, mids, mats, nmat, lights, nlights, cam,
+                                          nullptr, 0, 0);
+    PreparedScene prepared(std::move(scene));
+    SceneLightSampler sampler = make_scene_light_sampler(
+        prepared.host_scene(), prepared.light_sampling(), sampler_kind(light_sampler));
+    for (int i = 0; i < n; ++i) {
+        LightSampleContext ctx{vec3(positions[3 * i], positions[3 * i + 1], positions[3 * i + 2]),
+                               vec3(0), vec3(0)};
+        SampledLight picked = sample_light(sampler, ctx, select_u[i]);
+        light_index[i] = picked.light_index;
+        pmf[i] = picked.light_index >= 0 ? picked.pmf : 0.0f;
+        eval_pmf[i] = picked.light_index >= 0 ? light_pmf(sampler, ctx, picked.light_index) : 0.0f;
+    }
     return 0;
 }
 

@@ -34,8 +34,7 @@ def test_cli_reports_usage_and_rejects_like_the_reference(cli):
     assert _run(cli, "-spp", "0").returncode == 1          # parse_positive_int
     assert _run(cli, "-depth", "-1").returncode == 1
     assert _run(cli, "-size", "8").returncode == 1          # missing operand
-    r = _run(cli, "-light-sampler", "bvh")
-    assert r.returncode == 1 and "not supported" in r.stderr
+    assert _run(cli, "-light-sampler", "tree").returncode == 1  # parse_light_sampler_kind
     assert _run(cli, "-debug-aov", "ng").returncode == 1
 
 
@@ -76,9 +75,11 @@ def test_cli_cornell_matches_reference_cpu_tracer(cli, tmp_path):
 @pytest.mark.gpu
 @pytest.mark.parametrize("scene", ["direct-light", "point-light", "distant-light", "uniform-env",
                                    "image-env", "transparent-filter"])
-def test_cli_renders_every_code_defined_scene(cli, tmp_path, scene):
+@pytest.mark.parametrize("sampler", ["power", "bvh"])
+def test_cli_renders_every_code_defined_scene(cli, tmp_path, scene, sampler):
     out = tmp_path / f"{scene}.pfm"
-    r = _run(cli, "-gpu", "-scene", scene, "-size", "24", "24", "-spp", "8", "-output", str(out))
+    r = _run(cli, "-gpu", "-scene", scene, "-size", "24", "24", "-spp", "8", "-output", str(out),
+             "-light-sampler", sampler)
     assert r.returncode == 0, r.stderr
     img = _read_pfm(out)
     assert np.isfinite(img).all() and img.mean() > 0
