@@ -382,8 +382,9 @@ int lux_scene_select_lights(lux_ctx* ctx, const lux_scene* scene, int32_t light_
 /*
  * New vertex positions for one mesh (same count): world triangles are recomputed and
  * the mesh's BLAS and the TLAS are refit (not rebuilt) for animation between frames.
- * Area-light areas and powers are not re-derived (the light tables are the
- * construction-time ones).
+ * When an instance of the mesh carries emission, the light tables (areas, powers, the
+ * power alias table, the light tree) are re-derived as a scene created from the new
+ * vertices would hold them.
  */
 int lux_scene_update_mesh(lux_ctx* ctx, lux_scene* scene, int32_t mesh, const float* vertices);
 

@@ -28,7 +28,6 @@ struct lux_scene {
     lux_bvh* tlas = nullptr;
     lux::pt::Light* lights = nullptr;
     lux::pt::AliasEntry* light_alias = nullptr;
-    lux::pt::AliasEntry* light_alias_uniform = nullptr;  // unused placeholder
     int* primitive_light = nullptr;
     float* tri_soup = nullptr;          // per-mesh object-space soups for refits (device)
     std::vector<size_t> soup_offset;    // float offset of each mesh's soup
@@ -51,6 +50,23 @@ struct lux_scene {
         int entry_count = 0;
     };
     std::vector<MeshRefit> refit;
+    // Light-table inputs, kept so that a vertex update re-derives the tables as the
+    // reference's re-preparation of a changed scene would.
+    struct EmissiveTri {
+        int triangle, instance, local;   // scene triangle, its instance and local index
+        int two_sided;
+        float emission[3];
+        float w[9];                      // world positions of the three corners
+    };
+    std::vector<EmissiveTri> emissive;             // emissive scene triangles, scene order
+    std::vector<char> mesh_emissive;               // per mesh: an instance carries emission
+    std::vector<lux::pt::Light> explicit_lights;   // point, distant, infinite lights
+    std::vector<float> explicit_power;
+    struct LightCapacity {                         // element capacity of each light buffer
+        size_t lights = 0, alias = 0, primitive = 0, tree = 0, leaf = 0, other_slot = 0,
+               other_lights = 0, other_alias = 0;
+    };
+    LightCapacity light_capacity;
     lux::pt::SceneView view;            // device pointers + counts (TLAS/BLAS filled in)
 };
 
@@ -59,8 +75,10 @@ namespace lux {
 int scene_create(lux_ctx* ctx, const lux_scene_desc* desc, lux_scene** out);
 void scene_free(lux_scene* scene);
 // Replaces one mesh's vertices (same count and topology) and refits its BLAS and the TLAS,
-// all in stream order on ctx->stream.  With sync, waits and reports device errors; without,
-// the caller's next synchronisation does.
+// all in stream order on ctx->stream; when an instance of the mesh carries emission, the
+// light tables are re-derived on the host and copied in stream order too (the stream is
+// waited for only when a table outgrows its buffer).  With sync, waits and reports device
+// errors; without, the caller's next synchronisation does.
 int scene_update_mesh(lux_ctx* ctx, lux_scene* scene, int mesh, const float* vertices,
                       bool sync = true);
 int camera_perspective(const float* origin, const float* look_at, float vfov, float aspect,

@@ -256,6 +256,86 @@ LightTree build_light_tree(std::vector<LightItem> items, const std::vector<float
     return t;
 }
 
+// ---- light tables (prepare_scene_light_sampling, scene/scene_prepare.h:268-387)
+
+struct LightTables {
+    std::vector<Light> lights;
+    std::vector<float> cdf;              // running power sums
+    float total = 0;
+    int area_count = 0;
+    std::vector<int> primitive_light;    // scene triangle -> light (-1 none, -2 several)
+    std::vector<AliasEntry> alias;       // power alias table
+    LightTree tree;
+};
+
+// Area lights from the emissive triangles (scene order; a triangle without area is no
+// light), then the explicit lights with their powers; the power alias table; the tree
+// over the lights with bounds (area lights: their triangle's box; point lights: their
+// position; light_bounds_for_bvh, scene/scene_prepare.h:243-296).
+LightTables make_light_tables(const std::vector<lux_scene::EmissiveTri>& emissive,
+                              const std::vector<Light>& explicit_lights,
+                              const std::vector<float>& explicit_power, size_t triangle_count) {
+    LightTables t;
+    t.primitive_light.assign(triangle_count, -1);
+    std::vector<float> power;
+    std::vector<Box> boxes;
+    auto append = [&](const Light& l, float p, const Box& b) -> int {
+        if (p <= 0) return -1;
+        t.total += p;
+        t.lights.push_back(l);
+        t.cdf.push_back(t.total);
+        power.push_back(p);
+        boxes.push_back(b);
+        return static_cast<int>(t.lights.size()) - 1;
+    };
+    for (const lux_scene::EmissiveTri& e : emissive) {
+        const V3 a = v3(e.w[0], e.w[1], e.w[2]);
+        const V3 b = v3(e.w[3], e.w[4], e.w[5]);
+        const V3 c = v3(e.w[6], e.w[7], e.w[8]);
+        const float area = 0.5f * len3(cross3(b - a, c - a));
+        if (area <= 0) continue;
+        Light l;
+        l.kind = 0;
+        l.primitive = e.triangle;
+        l.two_sided = e.two_sided;
+        l.area = area;
+        l.emission = make_f3(e.emission[0], e.emission[1], e.emission[2]);
+        l.vec = make_f3(0, 0, 0);
+        Box box;
+        box.expand(a);
+        box.expand(b);
+        box.expand(c);
+        const float p = area * std::fmax(1e-6f, luminance(v3(e.emission[0], e.emission[1],
+                                                             e.emission[2])));
+        const int index = append(l, p, box);
+        if (index >= 0) {
+            int& stored = t.primitive_light[e.triangle];
+            stored = stored == -1 ? index : -2;
+        }
+    }
+    t.area_count = static_cast<int>(t.lights.size());
+    for (size_t i = 0; i < explicit_lights.size(); ++i) {
+        const Light& l = explicit_lights[i];
+        Box box;  // empty: no place in the tree
+        if (l.kind == 1) box.lo = box.hi = v3(l.vec.x, l.vec.y, l.vec.z);
+        append(l, explicit_power[i], box);
+    }
+    if (t.total > 0) {  // finalize_light_selection_table
+        std::vector<float> weights;
+        float prev = 0;
+        for (float c : t.cdf) {
+            weights.push_back(c - prev);
+            prev = c;
+        }
+        t.alias = alias_from_weights(weights);
+    }
+    std::vector<LightItem> items;
+    for (int i = 0; i < static_cast<int>(t.lights.size()); ++i)
+        if (!boxes[i].empty()) items.push_back(LightItem{boxes[i], centre(boxes[i]), i, power[i]});
+    t.tree = build_light_tree(items, t.cdf);
+    return t;
+}
+
 template <typename T>
 int upload(T** dst, const std::vector<T>& src, cudaStream_t stream) {
     size_t bytes = sizeof(T) * std::max<size_t>(src.size(), 1);
@@ -270,6 +350,74 @@ int upload(T** dst, const std::vector<T>& src, cudaStream_t stream) {
         if (err != cudaSuccess) return cuda_fail(err, "scene upload");
     }
     return LUX_OK;
+}
+
+// Copies src into *dst, in stream order when it fits the buffer's capacity; otherwise
+// waits for the stream once (earlier work may still read the old buffer), then
+// reallocates.
+template <typename T>
+int refill(T** dst, size_t* capacity, const std::vector<T>& src, cudaStream_t stream,
+           bool* synced) {
+    if (!*dst || src.size() > *capacity) {
+        if (*dst) {
+            if (!*synced) {
+                cudaError_t err = cudaStreamSynchronize(stream);
+                if (err != cudaSuccess) return cuda_fail(err, "light table update");
+                *synced = true;
+            }
+            cudaFree(*dst);
+            *dst = nullptr;
+        }
+        *capacity = std::max<size_t>(src.size(), 1);
+        if (cudaMalloc(reinterpret_cast<void**>(dst), sizeof(T) * *capacity) != cudaSuccess) {
+            cudaGetLastError();
+            *dst = nullptr;
+            *capacity = 0;
+            return fail(LUX_ERR_OUT_OF_MEMORY, "scene allocation failed");
+        }
+    }
+    if (src.empty()) return LUX_OK;
+    cudaError_t err = cudaMemcpyAsync(*dst, src.data(), sizeof(T) * src.size(),
+                                      cudaMemcpyHostToDevice, stream);
+    return err == cudaSuccess ? LUX_OK : cuda_fail(err, "scene upload");
+}
+
+int upload_light_tables(lux_ctx* ctx, lux_scene* s, const LightTables& t) {
+    cudaStream_t stream = ctx->stream;
+    lux_scene::LightCapacity& c = s->light_capacity;
+    bool synced = false;
+    int st = refill(&s->lights, &c.lights, t.lights, stream, &synced);
+    if (!st) st = refill(&s->light_alias, &c.alias, t.alias, stream, &synced);
+    if (!st) st = refill(&s->primitive_light, &c.primitive, t.primitive_light, stream, &synced);
+    if (!st && !t.tree.nodes.empty()) {
+        st = refill(&s->light_tree, &c.tree, t.tree.nodes, stream, &synced);
+        if (!st) st = refill(&s->light_leaf, &c.leaf, t.tree.leaf, stream, &synced);
+        if (!st) st = refill(&s->light_other_slot, &c.other_slot, t.tree.other_slot, stream, &synced);
+        if (!st) st = refill(&s->other_lights, &c.other_lights, t.tree.other_lights, stream, &synced);
+        if (!st) st = refill(&s->other_alias, &c.other_alias, t.tree.other_alias, stream, &synced);
+    }
+    return st;
+}
+
+void set_light_view(lux_scene* s, const LightTables& t) {
+    pt::SceneView& v = s->view;
+    const bool tree = !t.tree.nodes.empty();
+    v.lights = s->lights;
+    v.light_count = static_cast<int>(t.lights.size());
+    v.total_light_power = t.total;
+    v.light_alias = t.alias.empty() ? nullptr : s->light_alias;
+    v.light_sampler = 1;
+    v.primitive_light = s->primitive_light;
+    v.light_tree = tree ? s->light_tree : nullptr;
+    v.light_tree_count = static_cast<int>(t.tree.nodes.size());
+    v.light_tree_root = tree ? 0 : -1;
+    v.light_leaf = tree ? s->light_leaf : nullptr;
+    v.light_other_slot = tree ? s->light_other_slot : nullptr;
+    v.other_lights = tree && !t.tree.other_lights.empty() ? s->other_lights : nullptr;
+    v.other_alias = tree && !t.tree.other_alias.empty() ? s->other_alias : nullptr;
+    v.other_count = static_cast<int>(t.tree.other_lights.size());
+    v.other_power = t.tree.other_power;
+    s->area_light_count = t.area_count;
 }
 
 Material to_material(const lux_material& m) {
@@ -432,7 +580,6 @@ int scene_create(lux_ctx* ctx, const lux_scene_desc* d, lux_scene** out) {
     // Instances and world triangles in scene-triangle order.
     std::vector<pt::SceneTri> tris;
     std::vector<pt::SceneTriShading> shading;
-    std::vector<int> primitive_light;
     for (int i = 0; i < d->instance_count; ++i) {
         const lux_instance_desc& in = d->instances[i];
         Instance inst;
@@ -448,45 +595,30 @@ int scene_create(lux_ctx* ctx, const lux_scene_desc* d, lux_scene** out) {
     }
     s->triangle_count = static_cast<int>(tris.size());
 
-    // Light tables (scene/scene_prepare.h:268-387).
-    std::vector<Light> lights;
-    std::vector<float> cdf, light_power;
-    float total_power = 0;
-    primitive_light.assign(tris.size(), -1);
-    auto append = [&](const Light& l, float power) -> int {
-        if (power <= 0) return -1;
-        total_power += power;
-        lights.push_back(l);
-        cdf.push_back(total_power);
-        light_power.push_back(power);
-        return static_cast<int>(lights.size()) - 1;
-    };
+    // Light-table inputs (scene/scene_prepare.h:268-387): the emissive scene triangles
+    // in scene order, then the explicit lights; kept so that vertex updates re-derive
+    // the tables.
     for (size_t t = 0; t < tris.size(); ++t) {
         int material;
         std::memcpy(&material, &tris[t].v0.w, 4);
         const lux_material& mat = d->materials[material];
         if (!is_emissive(mat)) continue;
-        V3 a = v3(tris[t].v0.x, tris[t].v0.y, tris[t].v0.z);
-        V3 b = v3(tris[t].v1.x, tris[t].v1.y, tris[t].v1.z);
-        V3 c = v3(tris[t].v2.x, tris[t].v2.y, tris[t].v2.z);
-        float area = 0.5f * len3(cross3(b - a, c - a));
-        if (area <= 0) continue;
-        Light l;
-        l.kind = 0;
-        l.primitive = static_cast<int>(t);
-        l.two_sided = mat.emission_two_sided ? 1 : 0;
-        l.area = area;
-        l.emission = make_f3(mat.emission[0], mat.emission[1], mat.emission[2]);
-        l.vec = make_f3(0, 0, 0);
-        float power = area * std::fmax(1e-6f, luminance(v3(mat.emission[0], mat.emission[1],
-                                                           mat.emission[2])));
-        int index = append(l, power);
-        if (index >= 0) {
-            int& stored = primitive_light[t];
-            stored = stored == -1 ? index : -2;
+        lux_scene::EmissiveTri e;
+        e.triangle = static_cast<int>(t);
+        std::memcpy(&e.instance, &tris[t].v1.w, 4);
+        std::memcpy(&e.local, &tris[t].v2.w, 4);
+        e.two_sided = mat.emission_two_sided ? 1 : 0;
+        for (int k = 0; k < 3; ++k) e.emission[k] = mat.emission[k];
+        const float4* v[3] = {&tris[t].v0, &tris[t].v1, &tris[t].v2};
+        for (int k = 0; k < 3; ++k) {
+            e.w[3 * k] = v[k]->x;
+            e.w[3 * k + 1] = v[k]->y;
+            e.w[3 * k + 2] = v[k]->z;
         }
+        s->emissive.push_back(e);
     }
-    s->area_light_count = static_cast<int>(lights.size());
+    s->mesh_emissive.assign(d->mesh_count, 0);
+    for (const lux_scene::EmissiveTri& e : s->emissive) s->mesh_emissive[s->instances[e.instance].blas] = 1;
     // Image lights: texels and running weights (make_image_light_asset,
     // scene/scene_build.h:40-65): weight = max(0, luminance(texel * scale)) * sin(theta)
     // at the row centre, summed in row-major order in float.
@@ -530,37 +662,12 @@ int scene_create(lux_ctx* ctx, const lux_scene_desc* d, lux_scene** out) {
             env.push_back(e);
             power = std::fmax(1e-6f, sum);
         }
-        append(l, power);
+        s->explicit_lights.push_back(l);
+        s->explicit_power.push_back(power);
     }
-    std::vector<float> weights;
-    float prev = 0;
-    for (float c : cdf) {
-        weights.push_back(c - prev);
-        prev = c;
-    }
-    std::vector<AliasEntry> alias = total_power > 0 ? alias_from_weights(weights)
-                                                    : std::vector<AliasEntry>{};
-    // Light tree over the lights with bounds: area lights (their triangle's box) and
-    // point lights (their position), in light-index order (light_bvh_items and
-    // light_bounds_for_bvh, scene/scene_prepare.h:243-296).
-    std::vector<LightItem> items;
-    for (int i = 0; i < static_cast<int>(lights.size()); ++i) {
-        const Light& l = lights[i];
-        Box b;
-        if (l.kind == 0) {
-            const pt::SceneTri& t = tris[l.primitive];
-            b.expand(v3(t.v0.x, t.v0.y, t.v0.z));
-            b.expand(v3(t.v1.x, t.v1.y, t.v1.z));
-            b.expand(v3(t.v2.x, t.v2.y, t.v2.z));
-        } else if (l.kind == 1) {
-            b.lo = b.hi = v3(l.vec.x, l.vec.y, l.vec.z);
-        } else {
-            continue;
-        }
-        if (b.empty()) continue;
-        items.push_back(LightItem{b, centre(b), i, light_power[i]});
-    }
-    const LightTree tree = build_light_tree(items, cdf);
+    const LightTables lt = make_light_tables(s->emissive, s->explicit_lights, s->explicit_power,
+                                             tris.size());
+    s->area_light_count = lt.area_count;
 
     // Uploads.
     std::vector<Material> mats;
@@ -569,7 +676,6 @@ int scene_create(lux_ctx* ctx, const lux_scene_desc* d, lux_scene** out) {
     if (!st) st = upload(&s->tris, tris, ctx->stream);
     if (!st) st = upload(&s->shading, shading, ctx->stream);
     if (!st) st = upload(&s->d_instances, s->instances, ctx->stream);
-    if (!st) st = upload(&s->lights, lights, ctx->stream);
     if (!st && !env.empty()) {
         st = upload(&s->env_pixels, env_pixels, ctx->stream);
         if (!st) st = upload(&s->env_cdf, env_cdf, ctx->stream);
@@ -579,15 +685,7 @@ int scene_create(lux_ctx* ctx, const lux_scene_desc* d, lux_scene** out) {
         }
         if (!st) st = upload(&s->d_env, env, ctx->stream);
     }
-    if (!st) st = upload(&s->light_alias, alias, ctx->stream);
-    if (!st) st = upload(&s->primitive_light, primitive_light, ctx->stream);
-    if (!st && !tree.nodes.empty()) {
-        st = upload(&s->light_tree, tree.nodes, ctx->stream);
-        if (!st) st = upload(&s->light_leaf, tree.leaf, ctx->stream);
-        if (!st) st = upload(&s->light_other_slot, tree.other_slot, ctx->stream);
-        if (!st) st = upload(&s->other_lights, tree.other_lights, ctx->stream);
-        if (!st) st = upload(&s->other_alias, tree.other_alias, ctx->stream);
-    }
+    if (!st) st = upload_light_tables(ctx, s, lt);
 
     // BLAS per mesh over object-space soups.
     std::vector<float> all_soup;
@@ -648,22 +746,8 @@ int scene_create(lux_ctx* ctx, const lux_scene_desc* d, lux_scene** out) {
     v.tlas = s->tlas->view();
     v.tlas_instance = s->tlas_instance;
     v.blas = s->blas_views;
-    v.lights = s->lights;
     v.env = s->d_env;
-    v.light_count = static_cast<int>(lights.size());
-    v.total_light_power = total_power;
-    v.light_alias = alias.empty() ? nullptr : s->light_alias;
-    v.light_sampler = 1;
-    v.light_tree = tree.nodes.empty() ? nullptr : s->light_tree;
-    v.light_tree_count = static_cast<int>(tree.nodes.size());
-    v.light_tree_root = tree.nodes.empty() ? -1 : 0;
-    v.light_leaf = tree.nodes.empty() ? nullptr : s->light_leaf;
-    v.light_other_slot = tree.nodes.empty() ? nullptr : s->light_other_slot;
-    v.other_lights = tree.other_lights.empty() ? nullptr : s->other_lights;
-    v.other_alias = tree.other_alias.empty() ? nullptr : s->other_alias;
-    v.other_count = static_cast<int>(tree.other_lights.size());
-    v.other_power = tree.other_power;
-    v.primitive_light = s->primitive_light;
+    set_light_view(s, lt);
     v.has_two_level = s->tlas->n > 0 && d->instance_count > 0;
     v.has_passthrough = false;
     for (int i = 0; i < d->material_count; ++i)
@@ -885,6 +969,26 @@ int scene_update_mesh(lux_ctx* ctx, lux_scene* s, int mesh, const float* vertice
     }
     err = cudaGetLastError();
     if (err != cudaSuccess) return cuda_fail(err, "mesh update");
+    if (static_cast<size_t>(mesh) < s->mesh_emissive.size() && s->mesh_emissive[mesh]) {
+        // The moved emissive triangles' world corners (the arithmetic of
+        // k_instance_positions), then every light table.
+        const std::vector<uint32_t>& idx = s->mesh_indices[mesh];
+        for (lux_scene::EmissiveTri& e : s->emissive) {
+            const Instance& inst = s->instances[e.instance];
+            if (inst.blas != mesh) continue;
+            for (int k = 0; k < 3; ++k) {
+                const float* p = verts.data() + 3 * size_t(idx[3 * size_t(e.local) + k]);
+                const V3 w = transform_point(inst.m, v3(p[0], p[1], p[2]));
+                e.w[3 * k] = w.x;
+                e.w[3 * k + 1] = w.y;
+                e.w[3 * k + 2] = w.z;
+            }
+        }
+        const LightTables lt = make_light_tables(s->emissive, s->explicit_lights,
+                                                 s->explicit_power, size_t(s->triangle_count));
+        if (int st = upload_light_tables(ctx, s, lt)) return st;
+        set_light_view(s, lt);
+    }
     if (!sync) return LUX_OK;
     err = cudaStreamSynchronize(stream);
     if (err != cudaSuccess) return cuda_fail(err, "mesh update");

@@ -591,9 +591,15 @@ void worker_main(lux_server* s) {
                 for (size_t j = k + 1; j < batch.size() && !superseded; ++j)
                     superseded = batch[j].scene == batch[k].scene && batch[j].mesh == batch[k].mesh;
                 if (superseded) continue;
-                if (lux::scene_update_mesh(s->ctx, s->scenes[batch[k].scene], batch[k].mesh,
-                                           batch[k].vertices.data(), false) == LUX_OK)
-                    ++applied;
+                lux_scene* scene = s->scenes[batch[k].scene];
+                if (lux::scene_update_mesh(s->ctx, scene, batch[k].mesh,
+                                           batch[k].vertices.data(), false) != LUX_OK)
+                    continue;
+                ++applied;
+                // Light tables may have been re-derived: the staged view follows, in
+                // stream order before the next iteration.
+                cudaMemcpyAsync(s->d_scenes + batch[k].scene, &scene->view, sizeof(scene->view),
+                                cudaMemcpyHostToDevice, s->ctx->stream);
             }
             lk.lock();
             s->refits += applied;

@@ -396,3 +396,62 @@ def test_light_tree_render_matches_reference(ctx):
     assert _z_fraction(gpu, ref) <= 0.01
     power = S.render_samples(ctx, sc, S.request(w, h, spp, depth, seed))
     assert np.median(gpu.var(axis=1)) < 0.85 * np.median(power.var(axis=1))
+
+
+def emissive_mesh_scene(vertices=None, w=32, h=32):
+    """Cornell box plus a mesh of separate emissive triangles (two instances; the first
+    triangle starts with no area, so no light) and a point light."""
+    rng = np.random.default_rng(17)
+    b = S.make_cornell_scene(w, h)
+    if vertices is None:
+        c = rng.uniform([-0.6, 0.2, -0.6], [0.6, 1.0, 0.6], (12, 1, 3))
+        vertices = (c + rng.normal(scale=0.08, size=(12, 3, 3))).reshape(-1, 3).astype(np.float32)
+        vertices[1] = vertices[2] = vertices[0]          # degenerate: no light
+    n = len(vertices) // 3
+    mats = [b.add_material(S.emissive((float(2 + i % 4), 3.0, float(1 + i % 3)),
+                                      two_sided=bool(i % 2))) for i in range(n)]
+    mesh = b.add_mesh(S.Mesh(vertices, np.arange(3 * n, dtype=np.uint32).reshape(n, 3),
+                             np.asarray(mats, np.int32)))
+    b.add_instance(mesh, np.array([[1, 0, 0, 0.0], [0, 1, 0, 0.5], [0, 0, 1, 0.2]], np.float32))
+    c_, s_ = np.float32(np.cos(0.5)), np.float32(np.sin(0.5))
+    b.add_instance(mesh, np.array([[c_, 0, s_, 0.1], [0, 0.9, 0, 0.4], [-s_, 0, c_, -0.3]],
+                                  np.float32))
+    b.add_point_light((0.2, 1.6, 0.5), (0.6, 0.6, 0.5))
+    return b, mesh, vertices
+
+
+@pytest.mark.parametrize("change", ["move", "grow", "shrink"])
+def test_emissive_mesh_update_rederives_light_tables(ctx, change):
+    """Moving an emissive mesh re-derives areas, powers, the alias table and the light
+    tree: selections, pmfs and renders equal a scene created from the moved vertices,
+    also when the light count grows past or falls below the tables' first size."""
+    b, mesh, v = emissive_mesh_scene()
+    sc = S.Scene(ctx, b)
+    moved = v.copy()
+    moved[:, 1] += np.float32(0.05) * np.sin(4.0 * moved[:, 0]).astype(np.float32)
+    if change == "grow":                  # the degenerate triangle gains area
+        moved[1] += np.float32(0.1)
+        moved[2] += np.float32([0.0, 0.0, 0.1])
+    elif change == "shrink":              # two triangles lose theirs
+        moved[4] = moved[5] = moved[3]
+        moved[7] = moved[6]
+    sc.update_mesh(mesh, moved)
+    fresh_b = emissive_mesh_scene(moved)[0]
+    fresh = S.Scene(ctx, fresh_b)
+    assert sc.info() == fresh.info()
+    before = S.Scene(ctx, b).info()["area_lights"]
+    after = sc.info()["area_lights"]
+    assert {"move": after == before, "grow": after == before + 2,
+            "shrink": after == before - 4}[change]
+    rng = np.random.default_rng(3)
+    pos = rng.uniform([-1, 0, -1], [1, 2, 1], (4096, 3)).astype(np.float32)
+    u = rng.random(4096, dtype=np.float32)
+    for sampler in (S.SAMPLER_POWER, S.SAMPLER_TREE):
+        got = sc.select_lights(pos, u, sampler)
+        want = fresh.select_lights(pos, u, sampler)
+        for g, w in zip(got, want):
+            assert np.array_equal(g, w)
+    req = S.request(32, 32, 4, 5, 3, light_sampler=S.SAMPLER_TREE)
+    got = S.render_samples(ctx, sc, req)
+    want = S.render_samples(ctx, fresh, req)
+    assert np.all(got == want, axis=-1).mean() > 0.999

@@ -114,6 +114,28 @@ def test_refit_between_frames(ctx):
     assert np.mean(rel < 1e-4) > 0.99
 
 
+def test_emissive_refit_updates_the_served_light_tables(ctx):
+    """A served scene whose emissive mesh moves (and gains a light) renders like a scene
+    created from the moved vertices: the staged scene view follows the new tables."""
+    from test_pathtracer_gpu import emissive_mesh_scene
+    b, mesh, v = emissive_mesh_scene()
+    sc = S.Scene(ctx, b)
+    moved = v.copy()
+    moved[:, 1] += np.float32(0.04)
+    moved[1] += np.float32(0.1)
+    moved[2] += np.float32([0.0, 0.0, 0.1])
+    req = S.request(32, 32, 8, 5, 2, light_sampler=S.SAMPLER_TREE)
+    with SV.Server([sc], pool_paths=1 << 15) as srv:
+        r0, _ = srv.submit(0, req)
+        srv.wait(r0, timeout_s=60)
+        srv.update_mesh(0, mesh, moved)
+        r1, film = srv.submit(0, req)
+        srv.wait(r1, timeout_s=60)
+        assert srv.stats()["refits"] == 1
+    fresh = S.render(ctx, S.Scene(ctx, emissive_mesh_scene(moved)[0]), req)
+    assert _close(film, fresh)
+
+
 def test_refits_faster_than_iterations_do_not_starve_requests(ctx):
     from lux_b200 import scenes as SC
     b = SC.heavy_render_scene(32, 32)
