@@ -473,6 +473,57 @@ int lux_server_request_times(lux_server* server, int64_t request_id, int64_t* ti
 int lux_server_stats(lux_server* server, int64_t* stats);
 int lux_server_destroy(lux_server* server);
 
+/*
+ * OBJ meshes (host only; replaces load_obj_into_scene, util/obj_loader.h:107-113, for the
+ * options the reference's scenes use).  Parses v / vn / vt / f (1-based or negative
+ * indices; quads split on the shorter diagonal as the reference's bundled parser does,
+ * larger polygons as fans) and usemtl; skips faces with invalid indices, non-finite
+ * positions or an area of at most 1e-12 as the reference's loader does; gives every
+ * (position, used normal, used texcoord) corner one mesh vertex in first-use order.
+ * The caller adds the mesh with an instance whose object_to_world is the returned
+ * placement (make_obj_placement_transform, util/obj_loader.cpp:388-423).
+ */
+enum lux_obj_normal_mode {      /* ObjNormalMode */
+    LUX_OBJ_NORMALS_SOURCE = 0, /* vn where given and nonzero, else none (geometric) */
+    LUX_OBJ_NORMALS_SMOOTH = 1, /* vn where given, else area-weighted smooth normals */
+    LUX_OBJ_NORMALS_FACE = 2    /* none */
+};
+enum lux_obj_scale_mode { LUX_OBJ_SCALE_NONE = 0, LUX_OBJ_SCALE_MAX_EXTENT = 1,
+                          LUX_OBJ_SCALE_X_EXTENT = 2 };
+typedef struct lux_obj_options {  /* ObjLoadOptions (util/obj_loader.h:53-68) */
+    int32_t normal_mode;
+    int32_t reverse_orientation;
+    int32_t flip_texcoord_v;
+    int32_t scale_mode;           /* ObjPlacementOptions (util/obj_loader.h:35-41) */
+    float target_extent;
+    int32_t center_xz;
+    int32_t ground_to_y;
+    float target_y;
+    /* usemtl name -> material id.  With bindings every usemtl must be bound, and faces
+     * without usemtl take default_material (an error when it is -1).  Without bindings
+     * every face takes default_material; the reference appends a Lambert(0.8) material
+     * for it, so pass the id that material will get. */
+    const char* const* binding_names;
+    const int32_t* binding_ids;
+    int32_t binding_count;
+    int32_t default_material;
+} lux_obj_options;
+typedef struct lux_obj_mesh {
+    int32_t vertex_count, triangle_count;
+    float* vertices;           /* 3 per vertex, object space */
+    float* normals;            /* 3 per vertex; zero = none */
+    float* uvs;                /* 2 per vertex */
+    uint32_t* indices;         /* 3 per triangle */
+    int32_t* material_ids;     /* per triangle */
+    float object_to_world[12]; /* placement, row-major 3x4 */
+    float bounds[6];           /* mesh box, object space */
+    int32_t skipped_invalid, skipped_nonfinite, skipped_degenerate;
+} lux_obj_mesh;
+/* Loads path; *out is null (and LUX_OK) when no face survives.  Free with
+ * lux_obj_mesh_free. */
+int lux_obj_load(const char* path, const lux_obj_options* options, lux_obj_mesh** out);
+void lux_obj_mesh_free(lux_obj_mesh* mesh);
+
 #ifdef __cplusplus
 }
 #endif

@@ -35,7 +35,7 @@ PER_FILE_FLAGS = {
 
 
 def _sources():
-    return sorted(os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith(".cu"))
+    return sorted(os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cu", ".cpp")))
 
 
 def _headers():
@@ -46,14 +46,18 @@ def _headers():
 
 
 def _compile(src, verbose):
-    obj = os.path.join(OBJ_DIR, os.path.basename(src)[:-3] + ".o")
-    cmd = [NVCC, *NVCC_FLAGS, *PER_FILE_FLAGS.get(os.path.basename(src), []), "-c", src,
-           "-o", obj]
-    if verbose:
+    obj = os.path.join(OBJ_DIR, os.path.splitext(os.path.basename(src))[0] + ".o")
+    if src.endswith(".cpp"):  # host-only code (the OBJ loader)
+        cmd = ["g++", "-std=c++17", "-O2", "-fPIC", "-Wall",
+               "-I", os.path.join(HERE, "..", "include"), "-c", src, "-o", obj]
+    else:
+        cmd = [NVCC, *NVCC_FLAGS, *PER_FILE_FLAGS.get(os.path.basename(src), []), "-c", src,
+               "-o", obj]
+    if verbose and not src.endswith(".cpp"):
         cmd.insert(1, "-Xptxas=-v")
     res = subprocess.run(cmd, capture_output=True, text=True)
     if res.returncode != 0:
-        raise RuntimeError(f"nvcc failed for {src}:\n{res.stderr}")
+        raise RuntimeError(f"compile failed for {src}:\n{res.stderr}")
     return obj, res.stderr
 
 

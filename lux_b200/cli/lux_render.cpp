@@ -9,8 +9,9 @@
 // sample.  Images are written as the reference writes them: PPM through write_ppm's
 // tone map, PFM when the path ends in ".pfm" (the pixel transforms run on the device,
 // lux_film_encode).  This build renders on the GPU only: without -gpu it still renders
-// on the GPU and says so.  Scenes that need asset files (bunny, dragon, lux-cover) and the
-// debug probes/AOVs are reported as unsupported.
+// on the GPU and says so.  The asset scenes (bunny, dragon, lux-cover) load their OBJ
+// files through lux_obj_load from the reference's asset root (assets/ next to the
+// executable, else ./assets); the debug probes/AOVs are reported as unsupported.
 
 #include <chrono>
 #include <cmath>
@@ -155,6 +156,10 @@ struct SceneData {
     std::vector<std::vector<float>> image_pixels;
     std::vector<lux_env_image> images;
     float cam_origin[3], cam_look_at[3], cam_vfov;
+    std::vector<lux_obj_mesh*> obj_meshes;  // extra meshes, one instance each
+    ~SceneData() {
+        for (lux_obj_mesh* m : obj_meshes) lux_obj_mesh_free(m);
+    }
 };
 
 lux_material mat(int type, float r, float g, float b, float er = 0, float eg = 0, float eb = 0,
@@ -167,7 +172,8 @@ lux_material mat(int type, float r, float g, float b, float er = 0, float eg = 0
     m.roughness = roughness; m.metallic = metallic; m.eta = eta;
     return m;
 }
-constexpr int kLambert = 0, kInterface = 4, kTransparent = 5;
+constexpr int kLambert = 0, kThinLambert = 1, kGgx = 2, kDielectric = 3, kInterface = 4,
+              kTransparent = 5;
 int add_material(SceneData& s, const lux_material& m) {
     s.materials.push_back(m);
     return static_cast<int>(s.materials.size()) - 1;
@@ -297,16 +303,128 @@ void transparent_filter(SceneData& s) {
     camera(s, {0, 0.85f, 3.2f}, {0, 0.65f, -0.7f}, 38.0f);
 }
 
+// ---- asset scenes (scene/stanford_bunny.h, scene/stanford_dragon.h, scene/lux_cover.h;
+// cameras app/render_runner.cpp:148-170).  Failures carry the reference's messages.
+
+// load_obj_into_scene: the mesh and its placed instance; false when loading fails.
+bool load_obj(SceneData& s, const std::filesystem::path& path, lux_obj_options o,
+              std::string* error, const char* failure) {
+    lux_obj_mesh* m = nullptr;
+    if (lux_obj_load(path.string().c_str(), &o, &m) != LUX_OK) {
+        std::fprintf(stderr, "OBJ error: %s\n", lux_last_error());
+        *error = std::string(failure) + path.string();
+        return false;
+    }
+    if (m) s.obj_meshes.push_back(m);
+    return true;
+}
+
+// The loader's default material (Lambert 0.8) becomes thin Lambert, as the bunny and
+// dragon scenes convert it.
+bool grounded_asset(SceneData& s, const std::filesystem::path& path, lux_obj_options o,
+                    std::string* error, const char* failure, const char* empty) {
+    o.default_material = static_cast<int32_t>(s.materials.size());
+    if (!load_obj(s, path, o, error, failure)) return false;
+    if (s.obj_meshes.empty()) {
+        *error = std::string(empty) + path.string();
+        return false;
+    }
+    add_material(s, mat(kThinLambert, 0.8f, 0.8f, 0.8f));
+    return true;
+}
+
+bool bunny(SceneData& s, const std::filesystem::path& root, std::string* error) {
+    int floor = lambert(s, 0.5f, 0.5f, 0.5f);
+    int light = emissive(s, 15.0f, 14.0f, 12.0f);
+    quad(s, {-1, 0, 1}, {1, 0, 1}, {1, 0, -1}, {-1, 0, -1}, floor);
+    quad(s, {-0.3f, 0.5f, -0.3f}, {0.3f, 0.5f, -0.3f}, {0.3f, 0.5f, 0.3f}, {-0.3f, 0.5f, 0.3f},
+         light);
+    lux_obj_options o{};
+    o.ground_to_y = 1;
+    if (!grounded_asset(s, root / "models" / "stanford-bunny.obj", o, error,
+                        "Failed to load Stanford Bunny OBJ: ",
+                        "Stanford Bunny OBJ loaded no triangles: "))
+        return false;
+    camera(s, {0.0f, 0.3f, 0.5f}, {-0.02f, 0.11f, 0.0f}, 40.0f);
+    return true;
+}
+
+bool dragon(SceneData& s, const std::filesystem::path& root, std::string* error) {
+    int floor = lambert(s, 0.5f, 0.5f, 0.5f);
+    int light = emissive(s, 15.0f, 14.0f, 12.0f);
+    quad(s, {-1, 0, 1}, {1, 0, 1}, {1, 0, -1}, {-1, 0, -1}, floor);
+    quad(s, {-0.35f, 0.65f, -0.35f}, {0.35f, 0.65f, -0.35f}, {0.35f, 0.65f, 0.35f},
+         {-0.35f, 0.65f, 0.35f}, light);
+    lux_obj_options o{};
+    o.scale_mode = LUX_OBJ_SCALE_MAX_EXTENT;
+    o.target_extent = 0.5f;
+    o.center_xz = 1;
+    o.ground_to_y = 1;
+    if (!grounded_asset(s, root / "models" / "dragon.obj", o, error,
+                        "Failed to load dragon OBJ: ", "Dragon OBJ loaded no triangles: "))
+        return false;
+    camera(s, {0.0f, 0.35f, 0.8f}, {0.0f, 0.14f, 0.0f}, 42.0f);
+    return true;
+}
+
+bool lux_cover(SceneData& s, const std::filesystem::path& root, std::string* error) {
+    int floor = lambert(s, 0.42f, 0.43f, 0.42f);
+    int key = emissive(s, 22.0f, 21.0f, 19.0f);
+    s.materials[key].emission_two_sided = 1;
+    int l = lambert(s, 0.78f, 0.76f, 0.70f);
+    int u = add_material(s, mat(kDielectric, 0.90f, 0.97f, 1.00f, 0, 0, 0, 0.0f, 0.0f, 1.5f));
+    int x = add_material(s, mat(kGgx, 0.82f, 0.78f, 0.68f, 0, 0, 0, 0.22f, 1.0f));
+    quad(s, {-2.1f, 0, 0.18f}, {2.1f, 0, 0.18f}, {2.1f, 0, -2.2f}, {-2.1f, 0, -2.2f}, floor);
+    quad(s, {-2.1f, 0, 0.18f}, {-2.1f, 1.8f, 0.18f}, {2.1f, 1.8f, 0.18f}, {2.1f, 0, 0.18f}, floor);
+    quad(s, {-1.25f, 1.85f, -0.55f}, {1.25f, 1.85f, -0.55f}, {1.25f, 1.85f, 0.80f},
+         {-1.25f, 1.85f, 0.80f}, key);
+    const char* names[3] = {"L_lambert", "U_glass", "X_metal"};
+    const int32_t ids[3] = {l, u, x};
+    lux_obj_options o{};
+    o.normal_mode = LUX_OBJ_NORMALS_SMOOTH;
+    o.scale_mode = LUX_OBJ_SCALE_X_EXTENT;
+    o.target_extent = 1.85f;
+    o.center_xz = 1;
+    o.ground_to_y = 1;
+    o.binding_names = names;
+    o.binding_ids = ids;
+    o.binding_count = 3;
+    o.default_material = -1;
+    const std::filesystem::path path = root / "models" / "LUX.obj";
+    if (!load_obj(s, path, o, error, "Failed to load LUX cover OBJ: ")) return false;
+    if (s.obj_meshes.empty()) {
+        *error = "LUX cover OBJ loaded no triangles: " + path.string();
+        return false;
+    }
+    camera(s, {0.0f, 0.52f, -3.0f}, {0.0f, 0.36f, 0.0f}, 32.0f);
+    return true;
+}
+
+// resolve_demo_asset_root (app/render_runner.cpp:37-79): assets/ next to the executable,
+// else ./assets; the first candidate when neither exists.
+std::filesystem::path asset_root(const char* argv0) {
+    std::error_code ec;
+    std::filesystem::path exe = std::filesystem::absolute(argv0, ec);
+    if (ec) exe = argv0;
+    std::filesystem::path dir = exe.parent_path();
+    if (dir.empty()) dir = std::filesystem::current_path();
+    std::filesystem::path candidates[2] = {dir / "assets", std::filesystem::current_path() / "assets"};
+    for (const auto& c : candidates)
+        if (std::filesystem::is_directory(c, ec) && !ec) return c;
+    return candidates[0];
+}
+
 struct SceneEntry {
     const char* name;
     void (*make)(SceneData&);
+    bool (*make_asset)(SceneData&, const std::filesystem::path&, std::string*);
 };
 constexpr SceneEntry kScenes[] = {
-    {"cornell", cornell},         {"direct-light", direct_light},
-    {"point-light", point_light}, {"distant-light", distant_light},
-    {"uniform-env", uniform_env}, {"transparent-filter", transparent_filter},
-    {"image-env", image_env},     {"bunny", nullptr},
-    {"dragon", nullptr},          {"lux-cover", nullptr},
+    {"cornell", cornell, nullptr},         {"direct-light", direct_light, nullptr},
+    {"point-light", point_light, nullptr}, {"distant-light", distant_light, nullptr},
+    {"uniform-env", uniform_env, nullptr}, {"transparent-filter", transparent_filter, nullptr},
+    {"image-env", image_env, nullptr},     {"bunny", nullptr, bunny},
+    {"dragon", nullptr, dragon},           {"lux-cover", nullptr, lux_cover},
 };
 
 double ms_since(Clock::time_point t) {
@@ -360,15 +478,18 @@ int main(int argc, char** argv) {
                      names.c_str());
         return 1;
     }
-    if (!entry->make) {
-        std::fprintf(stderr, "Scene setup failed: scene '%s' needs asset files, which this build "
-                             "does not load\n", c.scene.c_str());
-        return 1;
-    }
     if (!c.gpu) std::printf("Rendering on the GPU (the only path of this build)\n");
     auto t0 = Clock::now();
     SceneData data;
-    entry->make(data);
+    if (entry->make) {
+        entry->make(data);
+    } else {
+        std::string error;
+        if (!entry->make_asset(data, asset_root(argv[0]), &error)) {
+            std::fprintf(stderr, "Scene setup failed: %s\n", error.c_str());
+            return 1;
+        }
+    }
     float aspect = static_cast<float>(c.width) / static_cast<float>(c.height);
     lux_scene_desc desc{};
     lux_mesh_desc mesh{};
@@ -382,12 +503,32 @@ int main(int argc, char** argv) {
     inst.material_override = -1;
     const float identity[12] = {1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1, 0};
     std::memcpy(inst.object_to_world, identity, sizeof(identity));
+    // The default mesh and its instance first, then each loaded mesh with its placement
+    // (scene-triangle order: instances in creation order).
+    std::vector<lux_mesh_desc> meshes{mesh};
+    std::vector<lux_instance_desc> instances{inst};
+    for (lux_obj_mesh* m : data.obj_meshes) {
+        lux_mesh_desc md{};
+        md.vertices = m->vertices;
+        md.normals = m->normals;
+        md.uvs = m->uvs;
+        md.vertex_count = m->vertex_count;
+        md.indices = m->indices;
+        md.material_ids = m->material_ids;
+        md.triangle_count = m->triangle_count;
+        lux_instance_desc id{};
+        id.mesh = static_cast<int32_t>(meshes.size());
+        id.material_override = -1;
+        std::memcpy(id.object_to_world, m->object_to_world, sizeof(id.object_to_world));
+        meshes.push_back(md);
+        instances.push_back(id);
+    }
     desc.materials = data.materials.data();
     desc.material_count = static_cast<int32_t>(data.materials.size());
-    desc.meshes = &mesh;
-    desc.mesh_count = 1;
-    desc.instances = &inst;
-    desc.instance_count = 1;
+    desc.meshes = meshes.data();
+    desc.mesh_count = static_cast<int32_t>(meshes.size());
+    desc.instances = instances.data();
+    desc.instance_count = static_cast<int32_t>(instances.size());
     desc.lights = data.lights.empty() ? nullptr : data.lights.data();
     desc.light_count = static_cast<int32_t>(data.lights.size());
     for (size_t k = 0; k < data.images.size(); ++k) data.images[k].pixels = data.image_pixels[k].data();
@@ -408,7 +549,8 @@ int main(int argc, char** argv) {
         return 1;
     }
     t_gpu = ms_since(t0);
-    std::printf("Built GPU TLAS/BLAS: %d TLAS nodes, %d instances, %d meshes\n", 1, 1, 1);
+    std::printf("Built GPU TLAS/BLAS: %d TLAS nodes, %d instances, %d meshes\n",
+                2 * desc.instance_count - 1, desc.instance_count, desc.mesh_count);
 
     lux_render_request req{};
     req.width = c.width;

@@ -118,6 +118,15 @@ class Ref:
                                          ctypes.c_uint64, _I, _I, _I, _I, _P, _P, _I, _I]
         lib.ref_select_lights.argtypes = [_P, _I, _P, _P, _I, _P, _I, _P, _I, _P, _P, _I,
                                           _P, _P, _P]
+        lib.ref_obj_load.argtypes = [ctypes.c_char_p, _I, _I, _I, _I, ctypes.c_float, _I, _I,
+                                     ctypes.c_float, _P, _P, _I, _I, _P]
+        lib.ref_obj_load.restype = _P
+        lib.ref_obj_copy.argtypes = [_P, _P, _P, _P, _P, _P, _P, _P]
+        lib.ref_obj_free.argtypes = [_P]
+        lib.ref_asset_scene.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_float, _P,
+                                        _P, _P, _P]
+        lib.ref_asset_render.argtypes = [ctypes.c_char_p, ctypes.c_char_p, _I, _I, _I, _I,
+                                         ctypes.c_uint64, _I, _I, _I, _I, _P]
         lib.ref_tree_create.argtypes = [_P, _I, _I]
         lib.ref_tree_create.restype = _P
         lib.ref_tree_destroy.argtypes = [_P]
@@ -169,6 +178,57 @@ class Ref:
                                    u.ctypes.data, n, index.ctypes.data, pmf.ctypes.data,
                                    eval_pmf.ctypes.data)
         return index, pmf, eval_pmf
+
+    def obj_load(self, path, normal_mode=0, reverse=False, flip_v=False, scale_mode=0,
+                 target_extent=1.0, center_xz=False, ground_to_y=False, target_y=0.0,
+                 bindings=None, default_material=-1):
+        """The reference's load_obj_into_scene_with_result: the mesh it adds (object space)
+        and its instance transform, or None when loading fails or adds nothing."""
+        bindings = bindings or {}
+        names = (ctypes.c_char_p * max(len(bindings), 1))(*[k.encode() for k in bindings])
+        ids = np.array(list(bindings.values()) or [0], np.int32)
+        counts = np.zeros(5, np.int32)
+        h = self.lib.ref_obj_load(path.encode(), normal_mode, int(reverse), int(flip_v),
+                                  scale_mode, target_extent, int(center_xz), int(ground_to_y),
+                                  target_y, names, ids.ctypes.data, len(bindings),
+                                  default_material, counts.ctypes.data)
+        if not h:
+            return None
+        nv, nt = int(counts[0]), int(counts[1])
+        out = {"vertices": np.zeros((nv, 3), np.float32), "normals": np.zeros((nv, 3), np.float32),
+               "uvs": np.zeros((nv, 2), np.float32), "indices": np.zeros((nt, 3), np.uint32),
+               "material_ids": np.zeros(nt, np.int32), "object_to_world": np.zeros((3, 4), np.float32),
+               "bounds": np.zeros(6, np.float32)}
+        self.lib.ref_obj_copy(h, *(out[k].ctypes.data for k in (
+            "vertices", "normals", "uvs", "indices", "material_ids", "object_to_world", "bounds")))
+        self.lib.ref_obj_free(h)
+        out["skipped"] = tuple(int(c) for c in counts[2:5])
+        return out
+
+    def asset_scene(self, name, root, aspect):
+        """World triangles, material ids and materials (11 floats) of the runner's asset
+        scene, or None when it cannot be made."""
+        counts = np.zeros(2, np.int32)
+        if self.lib.ref_asset_scene(name.encode(), root.encode(), aspect, counts.ctypes.data,
+                                    None, None, None) != 0:
+            return None
+        tris = np.zeros((counts[0], 9), np.float32)
+        mids = np.zeros(counts[0], np.int32)
+        mats = np.zeros((counts[1], 11), np.float32)
+        self.lib.ref_asset_scene(name.encode(), root.encode(), aspect, counts.ctypes.data,
+                                 tris.ctypes.data, mids.ctypes.data, mats.ctypes.data)
+        return tris, mids, mats
+
+    def asset_render(self, name, root, width, height, spp, max_depth, seed, light_sampler=1,
+                     rows=None, threads=1):
+        """Per-sample radiance [pixel][spp][3] of an asset scene's rows."""
+        y0, y1 = rows if rows is not None else (0, height)
+        out = np.zeros(((y1 - y0) * width, spp, 3), np.float32)
+        st = self.lib.ref_asset_render(name.encode(), root.encode(), width, height, spp,
+                                       max_depth, seed, light_sampler, y0, y1, threads,
+                                       out.ctypes.data)
+        assert st == 0, f"reference could not make scene {name}"
+        return out
 
     def write_image(self, film_sum: np.ndarray, spp: int, path: str, kind: int = 0) -> bytes:
         """The reference's write_ppm (0), write_debug_ppm_linear (1) or write_pfm (2) on a

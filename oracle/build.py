@@ -6,8 +6,8 @@
 
 Compiles, in place and without the reference's build system, the handful of
 reference translation units the CPU path needs (integrator/cpu_path_tracer.cpp,
-light/light_distribution.cpp, scene/prepared_scene_cpu.cpp; everything else on the
-path is header-only) together with oracle/ref_harness.cpp.  Output goes only to
+light/light_distribution.cpp, scene/prepared_scene_cpu.cpp, and util/obj_loader.cpp for
+the asset scenes; everything else on the path is header-only) together with oracle/ref_harness.cpp.  Output goes only to
 oracle/_ref/.  Test infrastructure: nothing in the product loads this library.
 """
 import os
@@ -25,6 +25,7 @@ REF_SOURCES = [
     "src/integrator/cpu_path_tracer.cpp",
     "src/light/light_distribution.cpp",
     "src/scene/prepared_scene_cpu.cpp",
+    "src/util/obj_loader.cpp",
 ]
 
 # The reference's Release configuration: -O3, x86-64 baseline ISA (SSE2, so no FMA

@@ -16,6 +16,11 @@
 //                                  app/render_runner.cpp:85-90)
 //   trace_path                     integrator/cpu_path_tracer.cpp:403-498
 //   make_render_sampler            integrator/render_context.h:45-54
+//   load_obj_into_scene_with_result util/obj_loader.cpp:1296-1301
+//   make_stanford_bunny_scene, make_lux_cover_scene, make_stanford_dragon_scene
+//                                  scene/stanford_bunny.h, scene/lux_cover.h,
+//                                  scene/stanford_dragon.h (runner cameras,
+//                                  app/render_runner.cpp:148-170)
 //
 // The stackless node array that intersect_bvh_device_impl walks is produced here
 // from the host tree by a plain preorder walk (left child first, escape = the node
@@ -37,8 +42,12 @@
 #include "integrator/cpu_path_tracer.h"
 #include "integrator/render_context.h"
 #include "scene/cornell_box.h"
+#include "scene/lux_cover.h"
 #include "scene/prepared_scene.h"
 #include "scene/scene_light_sampler.h"
+#include "scene/stanford_bunny.h"
+#include "scene/stanford_dragon.h"
+#include "util/obj_loader.h"
 
 namespace {
 
@@ -491,6 +500,181 @@ int ref_select_lights(const float* tris, int ntri, const int32_t* mids, const fl
         pmf[i] = picked.light_index >= 0 ? picked.pmf : 0.0f;
         eval_pmf[i] = picked.light_index >= 0 ? light_pmf(sampler, ctx, picked.light_index) : 0.0f;
     }
+    return 0;
+}
+
+// ---- OBJ loading and asset scenes
+
+struct RefObj {
+    Scene scene;
+    ObjLoadResult result;
+};
+
+// load_obj_into_scene_with_result into a scene holding 16 placeholder materials (so that
+// default and bound material ids up to 15 are valid); counts receives vertex count,
+// triangle count and the skipped invalid / non-finite / degenerate triangles.  Returns
+// null when the reference's loader fails or loads nothing.
+void* ref_obj_load(const char* path, int normal_mode, int reverse, int flip_v, int scale_mode,
+                   float target_extent, int center_xz, int ground_to_y, float target_y,
+                   const char* const* names, const int32_t* ids, int nbind,
+                   int default_material, int32_t* counts) {
+    auto* r = new RefObj();
+    for (int i = 0; i < 16; ++i) r->scene.materials.push_back(Material::lambert(vec3(0.5f)));
+    ObjLoadOptions options;
+    options.normal_mode = static_cast<ObjNormalMode>(normal_mode);
+    options.reverse_orientation = reverse != 0;
+    options.flip_texcoord_v = flip_v != 0;
+    options.placement.scale_mode = static_cast<ObjPlacementScaleMode>(scale_mode);
+    options.placement.target_extent = target_extent;
+    options.placement.center_xz = center_xz != 0;
+    options.placement.ground_to_y = ground_to_y != 0;
+    options.placement.target_y = target_y;
+    options.default_material_id = default_material;
+    for (int i = 0; i < nbind; ++i) options.material_bindings[names[i]] = ids[i];
+    bool ok = false;
+    try {
+        ok = load_obj_into_scene_with_result(path, r->scene, options, r->result);
+    } catch (const std::exception&) {
+        ok = false;
+    }
+    if (!ok || r->result.mesh_id < 0) {
+        delete r;
+        return nullptr;
+    }
+    const SceneMesh& m = r->scene.mesh_assets[r->result.mesh_id];
+    counts[0] = static_cast<int32_t>(m.vertices.size());
+    counts[1] = static_cast<int32_t>(m.indices.size());
+    counts[2] = r->result.skipped_invalid_triangle_count;
+    counts[3] = r->result.skipped_nonfinite_triangle_count;
+    counts[4] = r->result.skipped_degenerate_triangle_count;
+    return r;
+}
+
+// The loaded mesh (object space), the instance's object_to_world (row-major 3x4) and
+// the mesh box.
+int ref_obj_copy(void* handle, float* vertices, float* normals, float* uvs, uint32_t* indices,
+                 int32_t* material_ids, float* matrix, float* bounds) {
+    auto* r = static_cast<RefObj*>(handle);
+    const SceneMesh& m = r->scene.mesh_assets[r->result.mesh_id];
+    for (size_t i = 0; i < m.vertices.size(); ++i) {
+        vertices[3 * i] = m.vertices[i].x; vertices[3 * i + 1] = m.vertices[i].y;
+        vertices[3 * i + 2] = m.vertices[i].z;
+        normals[3 * i] = m.normals[i].x; normals[3 * i + 1] = m.normals[i].y;
+        normals[3 * i + 2] = m.normals[i].z;
+        uvs[2 * i] = m.uvs[i].x; uvs[2 * i + 1] = m.uvs[i].y;
+    }
+    for (size_t t = 0; t < m.indices.size(); ++t) {
+        indices[3 * t] = m.indices[t].v0; indices[3 * t + 1] = m.indices[t].v1;
+        indices[3 * t + 2] = m.indices[t].v2;
+        material_ids[t] = m.material_ids[t];
+    }
+    const mat4& x = r->scene.instances[r->result.instance_id].object_to_world.m;
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 4; ++j) matrix[4 * i + j] = x.m[i][j];
+    bounds[0] = m.bounds.p_min.x; bounds[1] = m.bounds.p_min.y; bounds[2] = m.bounds.p_min.z;
+    bounds[3] = m.bounds.p_max.x; bounds[4] = m.bounds.p_max.y; bounds[5] = m.bounds.p_max.z;
+    return 0;
+}
+
+void ref_obj_free(void* handle) { delete static_cast<RefObj*>(handle); }
+
+// The runner's asset scenes (bunny, dragon, lux-cover) with their cameras.
+static bool make_asset_scene(const char* name, const char* root, float aspect, Scene& scene) {
+    try {
+        std::filesystem::path assets(root);
+        std::string n(name);
+        if (n == "bunny") {
+            scene = make_stanford_bunny_scene(assets);
+            scene.camera = make_pinhole_camera(vec3(0.0f, 0.3f, 0.5f), vec3(-0.02f, 0.11f, 0.0f),
+                                               40.0f, aspect);
+        } else if (n == "dragon") {
+            scene = make_stanford_dragon_scene(assets);
+            scene.camera = make_pinhole_camera(vec3(0.0f, 0.35f, 0.8f), vec3(0.0f, 0.14f, 0.0f),
+                                               42.0f, aspect);
+        } else if (n == "lux-cover") {
+            scene = make_lux_cover_scene(assets);
+            scene.camera = make_pinhole_camera(vec3(0.0f, 0.52f, -3.0f), vec3(0.0f, 0.36f, 0.0f),
+                                               32.0f, aspect);
+        } else {
+            return false;
+        }
+    } catch (const std::exception&) {
+        return false;
+    }
+    return true;
+}
+
+// World triangles (9 floats), material ids and materials (11 floats as ref_render_scene
+// takes them) of an asset scene; counts = {triangles, materials}.  With null arrays only
+// the counts are written.  Returns -1 when the scene cannot be made.
+int ref_asset_scene(const char* name, const char* root, float aspect, int32_t* counts,
+                    float* tris, int32_t* material_ids, float* materials) {
+    Scene scene;
+    if (!make_asset_scene(name, root, aspect, scene)) return -1;
+    PreparedScene prepared(std::move(scene));
+    const Scene& sc = prepared.host_scene();
+    const int count = scene_triangle_count(sc);
+    counts[0] = count;
+    counts[1] = static_cast<int32_t>(sc.materials.size());
+    if (!tris) return 0;
+    for (int i = 0; i < count; ++i) {
+        SceneTriangle st = scene_triangle_view(sc, i);
+        const vec3* v = &st.triangle.v0;
+        for (int k = 0; k < 3; ++k) {
+            tris[i * 9 + k * 3 + 0] = v[k].x;
+            tris[i * 9 + k * 3 + 1] = v[k].y;
+            tris[i * 9 + k * 3 + 2] = v[k].z;
+        }
+        material_ids[i] = st.material_id;
+    }
+    for (size_t m = 0; m < sc.materials.size(); ++m) {
+        const Material& mat = sc.materials[m];
+        float* o = materials + m * 11;
+        o[0] = static_cast<float>(static_cast<int>(mat.type));
+        o[1] = mat.albedo.x; o[2] = mat.albedo.y; o[3] = mat.albedo.z;
+        o[4] = mat.emission.x; o[5] = mat.emission.y; o[6] = mat.emission.z;
+        o[7] = mat.roughness; o[8] = mat.metallic; o[9] = mat.eta;
+        o[10] = mat.emission_sidedness == EmissionSidedness::DoubleSided ? 1.0f : 0.0f;
+    }
+    return 0;
+}
+
+// Rows [y0, y1) of an asset scene through trace_path, as ref_render_scene renders.
+int ref_asset_render(const char* name, const char* root, int width, int height, int spp,
+                     int max_depth, uint64_t seed, int light_sampler, int y0, int y1,
+                     int threads, float* samples) {
+    Scene scene;
+    if (!make_asset_scene(name, root, Float(width) / Float(height), scene)) return -1;
+    PreparedScene prepared(std::move(scene));
+    prepared.prepare_host_bvh();
+    SceneLightSampler lights_sampler = make_scene_light_sampler(
+        prepared.host_scene(), prepared.light_sampling(), sampler_kind(light_sampler));
+    RenderSettings settings;
+    settings.max_depth = max_depth;
+    settings.seed = seed;
+    const Scene& sc = prepared.host_scene();
+    parallel_for((y1 - y0) * width, threads, [&](int begin, int end) {
+        for (int idx = begin; idx < end; ++idx) {
+            int y = y0 + idx / width;
+            int x = idx % width;
+            int pixel = y * width + x;
+            for (int s = 0; s < spp; ++s) {
+                SamplerState sampler = make_render_sampler(settings, pixel, s);
+                Float jx = sampler_get_1d(sampler);
+                Float jy = sampler_get_1d(sampler);
+                CameraSample cs;
+                cs.p_film = vec2((Float(x) + jx) / Float(width),
+                                 (Float(height - 1 - y) + jy) / Float(height));
+                cs.p_lens = sampler_get_2d(sampler);
+                cs.time = sampler_get_1d(sampler);
+                CameraRay generated = generate_camera_ray(sc.camera, cs);
+                vec3 L = trace_path(sc, prepared.host_bvh(), lights_sampler, generated.ray,
+                                    sampler, max_depth);
+                float* o = samples + (size_t(idx) * spp + s) * 3;
+                o[0] = L.x; o[1] = L.y; o[2] = L.z;
+            }
+        }
+    });
     return 0;
 }
 
