@@ -29,6 +29,14 @@ struct lux_scene {
     lux::pt::Light* lights = nullptr;
     lux::pt::AliasEntry* light_alias = nullptr;
     int* primitive_light = nullptr;
+    struct MeshData {                   // every mesh's arrays, concatenated (device)
+        float* vertices = nullptr;
+        float* normals = nullptr;
+        float* uvs = nullptr;
+        uint32_t* indices = nullptr;
+        int32_t* material_ids = nullptr;
+    };
+    MeshData mesh_data;
     float* tri_soup = nullptr;          // per-mesh object-space soups for refits (device)
     std::vector<size_t> soup_offset;    // float offset of each mesh's soup
     float* tlas_boxes = nullptr;        // instance world boxes (device)

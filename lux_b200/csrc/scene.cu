@@ -30,17 +30,22 @@ using pt::Instance;
 using pt::Light;
 using pt::Material;
 
+// The helpers below run on the host and, for device-side preparation, on the device:
+// this file is compiled without contraction and with IEEE division and square root, so
+// both sides round every operation alike.
+#define SCENE_HD __host__ __device__
+
 struct V3 {
     float x, y, z;
 };
-V3 v3(float x, float y, float z) { return V3{x, y, z}; }
-V3 operator-(V3 a, V3 b) { return v3(a.x - b.x, a.y - b.y, a.z - b.z); }
-float dot3(V3 a, V3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
-V3 cross3(V3 a, V3 b) {
+SCENE_HD V3 v3(float x, float y, float z) { return V3{x, y, z}; }
+SCENE_HD V3 operator-(V3 a, V3 b) { return v3(a.x - b.x, a.y - b.y, a.z - b.z); }
+SCENE_HD float dot3(V3 a, V3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+SCENE_HD V3 cross3(V3 a, V3 b) {
     return v3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
 }
-float len3(V3 a) { return std::sqrt(dot3(a, a)); }
-V3 normalize3(V3 v) {
+SCENE_HD float len3(V3 a) { return sqrtf(dot3(a, a)); }
+SCENE_HD V3 normalize3(V3 v) {
     float l = len3(v);
     if (!(l > 0)) return v;
     float inv = 1.0f / l;
@@ -48,7 +53,7 @@ V3 normalize3(V3 v) {
 }
 
 // transform_point (core/mat4.cuh:173-184) on a row-major 3x4 affine matrix.
-V3 transform_point(const float* m, V3 p) {
+SCENE_HD V3 transform_point(const float* m, V3 p) {
     float x = m[0] * p.x + m[1] * p.y + m[2] * p.z + m[3];
     float y = m[4] * p.x + m[5] * p.y + m[6] * p.z + m[7];
     float z = m[8] * p.x + m[9] * p.y + m[10] * p.z + m[11];
@@ -57,7 +62,7 @@ V3 transform_point(const float* m, V3 p) {
 }
 
 // transform_normal (core/mat4.cuh:207-230): adjugate-transpose, then normalize.
-V3 transform_normal(const float* m, V3 n) {
+SCENE_HD V3 transform_normal(const float* m, V3 n) {
     float a00 = m[5] * m[10] - m[6] * m[9];
     float a01 = m[6] * m[8] - m[4] * m[10];
     float a02 = m[4] * m[9] - m[5] * m[8];
@@ -73,7 +78,7 @@ V3 transform_normal(const float* m, V3 n) {
 }
 
 // transform_instance_normal (scene/scene_data.h:223-229).
-V3 instance_normal(const float* m, V3 n) {
+SCENE_HD V3 instance_normal(const float* m, V3 n) {
     if (dot3(n, n) == 0) return v3(0, 0, 0);
     V3 t = transform_normal(m, n);
     if (dot3(t, t) == 0) return v3(0, 0, 0);
@@ -436,81 +441,102 @@ bool is_emissive(const lux_material& m) {
     return std::fmax(m.emission[0], std::fmax(m.emission[1], m.emission[2])) > 0;
 }
 
-// World triangles and shading records of one instance, appended in local order.
-void instance_triangles(const lux_mesh_desc& mesh, const Instance& inst, int instance_id,
-                        int material_override, std::vector<pt::SceneTri>& tris,
-                        std::vector<pt::SceneTriShading>& shading) {
-    for (int t = 0; t < mesh.triangle_count; ++t) {
-        uint32_t idx[3] = {mesh.indices[3 * t], mesh.indices[3 * t + 1], mesh.indices[3 * t + 2]};
-        V3 w[3];
-        V3 n[3];
+// ---- device-side preparation
+
+constexpr int kPrepThreads = 256;
+
+// One mesh's device arrays (slices of the scene's concatenated mesh buffers).
+struct MeshDev {
+    const float* vertices;      // 3 per vertex
+    const float* normals;       // 3 per vertex, or null
+    const float* uvs;           // 2 per vertex, or null
+    const uint32_t* indices;    // 3 per triangle
+    const int32_t* material_ids;
+    int triangle_count;
+};
+
+// World triangle and shading record of every scene triangle (scene order: instances,
+// then local triangles; scene/scene_data.h:282-329): transform_point of the corners,
+// transform_instance_normal of the corner normals, the corner texcoords, and the tags
+// (material, instance, local triangle) in the .w lanes.  A triangle uses its normals
+// only when all three are nonzero after the transform.
+__global__ void k_world_triangles(const MeshDev* meshes, const Instance* instances,
+                                  const int* overrides, int instance_count, int total,
+                                  pt::SceneTri* tris, pt::SceneTriShading* shading) {
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < total; p += gridDim.x * blockDim.x) {
+        int lo = 0, hi = instance_count - 1;  // the last instance starting at or before p
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (instances[mid].first_primitive <= p) lo = mid;
+            else hi = mid - 1;
+        }
+        const Instance& inst = instances[lo];
+        const int t = p - inst.first_primitive;
+        const MeshDev& mesh = meshes[inst.blas];
+        V3 w[3], n[3];
         float uv[3][2] = {{0, 0}, {0, 0}, {0, 0}};
         bool has_normals = mesh.normals != nullptr;
         for (int k = 0; k < 3; ++k) {
-            const float* p = mesh.vertices + 3 * size_t(idx[k]);
-            w[k] = transform_point(inst.m, v3(p[0], p[1], p[2]));
+            const uint32_t v = mesh.indices[3 * size_t(t) + k];
+            const float* q = mesh.vertices + 3 * size_t(v);
+            w[k] = transform_point(inst.m, v3(q[0], q[1], q[2]));
             if (mesh.normals) {
-                const float* q = mesh.normals + 3 * size_t(idx[k]);
-                n[k] = instance_normal(inst.m, v3(q[0], q[1], q[2]));
+                const float* r = mesh.normals + 3 * size_t(v);
+                n[k] = instance_normal(inst.m, v3(r[0], r[1], r[2]));
                 if (dot3(n[k], n[k]) <= 0) has_normals = false;
             } else {
                 n[k] = v3(0, 0, 0);
             }
             if (mesh.uvs) {
-                uv[k][0] = mesh.uvs[2 * size_t(idx[k])];
-                uv[k][1] = mesh.uvs[2 * size_t(idx[k]) + 1];
+                uv[k][0] = mesh.uvs[2 * size_t(v)];
+                uv[k][1] = mesh.uvs[2 * size_t(v) + 1];
             }
         }
-        int material = material_override >= 0 ? material_override : mesh.material_ids[t];
+        const int material = overrides[lo] >= 0 ? overrides[lo] : mesh.material_ids[t];
         pt::SceneTri st;
-        int bits;
-        std::memcpy(&bits, &material, 4);
-        float fb;
-        std::memcpy(&fb, &material, 4);
-        st.v0 = make_float4(w[0].x, w[0].y, w[0].z, fb);
-        std::memcpy(&fb, &instance_id, 4);
-        st.v1 = make_float4(w[1].x, w[1].y, w[1].z, fb);
-        std::memcpy(&fb, &t, 4);
-        st.v2 = make_float4(w[2].x, w[2].y, w[2].z, fb);
-        tris.push_back(st);
+        st.v0 = make_float4(w[0].x, w[0].y, w[0].z, __int_as_float(material));
+        st.v1 = make_float4(w[1].x, w[1].y, w[1].z, __int_as_float(lo));
+        st.v2 = make_float4(w[2].x, w[2].y, w[2].z, __int_as_float(t));
+        tris[p] = st;
         pt::SceneTriShading sh;
         sh.n0 = make_float4(n[0].x, n[0].y, n[0].z, uv[0][0]);
         sh.n1 = make_float4(n[1].x, n[1].y, n[1].z, uv[0][1]);
         sh.n2 = make_float4(n[2].x, n[2].y, n[2].z, uv[1][0]);
         sh.uv = make_float4(uv[1][1], uv[2][0], uv[2][1], has_normals ? 1.0f : 0.0f);
-        shading.push_back(sh);
-        (void)bits;
+        shading[p] = sh;
     }
 }
 
-std::vector<float> mesh_soup(const lux_mesh_desc& mesh, const float* vertices) {
-    std::vector<float> soup(size_t(mesh.triangle_count) * 9);
-    for (int t = 0; t < mesh.triangle_count; ++t) {
-        for (int k = 0; k < 3; ++k) {
-            const float* p = vertices + 3 * size_t(mesh.indices[3 * t + k]);
-            soup[size_t(t) * 9 + k * 3 + 0] = p[0];
-            soup[size_t(t) * 9 + k * 3 + 1] = p[1];
-            soup[size_t(t) * 9 + k * 3 + 2] = p[2];
+__global__ void k_mesh_soup(const float* vertices, int vertex_count, const uint32_t* indices,
+                            int triangle_count, float* soup, int* error);
+
+// TLAS entry boxes at creation: transform_bounds (core/mat4.cuh:259-275) of each entry's
+// mesh box, the root box of the mesh's BLAS (the union of its triangle boxes,
+// finalize_scene_mesh, scene/scene_data.h:215-220).
+__global__ void k_tlas_boxes(const Instance* instances, const int* tlas_instance,
+                             const BvhView* blas, int entry_count, float* boxes) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= entry_count) return;
+    const Instance& inst = instances[tlas_instance[k]];
+    const float* r = blas[inst.blas].root;
+    float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+    if (!(r[0] > r[3] || r[1] > r[4] || r[2] > r[5])) {
+        for (int c = 0; c < 8; ++c) {
+            const V3 w = transform_point(inst.m, v3((c & 1) ? r[3] : r[0], (c & 2) ? r[4] : r[1],
+                                                    (c & 4) ? r[5] : r[2]));
+            lo[0] = fminf(lo[0], w.x); lo[1] = fminf(lo[1], w.y); lo[2] = fminf(lo[2], w.z);
+            hi[0] = fmaxf(hi[0], w.x); hi[1] = fmaxf(hi[1], w.y); hi[2] = fmaxf(hi[2], w.z);
         }
     }
-    return soup;
+    for (int a = 0; a < 3; ++a) {
+        boxes[6 * k + a] = lo[a];
+        boxes[6 * k + 3 + a] = hi[a];
+    }
 }
 
-// Instance world box: transform_bounds (core/mat4.cuh:259-275) of the mesh box
-// (finalize_scene_mesh, scene/scene_data.h:215-220).
-Box instance_box(const std::vector<float>& soup, int triangle_count, const float* m) {
-    Box mesh_box;
-    for (size_t i = 0; i < size_t(triangle_count) * 3; ++i)
-        mesh_box.expand(v3(soup[3 * i], soup[3 * i + 1], soup[3 * i + 2]));
-    Box out;
-    if (mesh_box.empty()) return out;
-    for (int z = 0; z <= 1; ++z)
-        for (int y = 0; y <= 1; ++y)
-            for (int x = 0; x <= 1; ++x)
-                out.expand(transform_point(m, v3(x ? mesh_box.hi.x : mesh_box.lo.x,
-                                                 y ? mesh_box.hi.y : mesh_box.lo.y,
-                                                 z ? mesh_box.hi.z : mesh_box.lo.z)));
-    return out;
+int prep_blocks(lux_ctx* ctx, int64_t items) {
+    const int64_t b = (items + kPrepThreads - 1) / kPrepThreads;
+    return static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(b, int64_t(ctx->sm_count) * 16)));
 }
 
 }  // namespace
@@ -525,6 +551,8 @@ void scene_free(lux_scene* s) {
     void* ptrs[] = {s->materials, s->tris, s->shading, s->d_instances, s->tlas_instance,
                     s->blas_views, s->lights, s->light_alias, s->primitive_light, s->tri_soup,
                     s->tlas_boxes, s->env_pixels, s->env_cdf, s->d_env, s->light_tree,
+                    s->mesh_data.vertices, s->mesh_data.normals, s->mesh_data.uvs,
+                    s->mesh_data.indices, s->mesh_data.material_ids,
                     s->light_leaf, s->light_other_slot, s->other_lights, s->other_alias};
     for (void* p : ptrs)
         if (p) cudaFree(p);
@@ -577,9 +605,10 @@ int scene_create(lux_ctx* ctx, const lux_scene_desc* d, lux_scene** out) {
     if (!s) return fail(LUX_ERR_OUT_OF_MEMORY, "scene allocation failed");
     s->device = ctx->device;
 
-    // Instances and world triangles in scene-triangle order.
-    std::vector<pt::SceneTri> tris;
-    std::vector<pt::SceneTriShading> shading;
+    // Instances and the scene-triangle prefix (scene order: instances, then local
+    // triangles).
+    int64_t total = 0;
+    std::vector<int> overrides;
     for (int i = 0; i < d->instance_count; ++i) {
         const lux_instance_desc& in = d->instances[i];
         Instance inst;
@@ -589,36 +618,57 @@ int scene_create(lux_ctx* ctx, const lux_scene_desc* d, lux_scene** out) {
         if (given) std::memcpy(inst.inv, in.world_to_object, sizeof(inst.inv));
         else inverse_affine(inst.m, inst.inv);
         inst.blas = in.mesh;
-        inst.first_primitive = static_cast<int>(tris.size());
+        inst.first_primitive = static_cast<int>(total);
         s->instances.push_back(inst);
-        instance_triangles(d->meshes[in.mesh], inst, i, in.material_override, tris, shading);
+        overrides.push_back(in.material_override);
+        total += d->meshes[in.mesh].triangle_count;
+        if (total > (int64_t(1) << 30)) {
+            delete s;
+            return fail(LUX_ERR_INVALID_ARGUMENT, "too many scene triangles (max 2^30)");
+        }
     }
-    s->triangle_count = static_cast<int>(tris.size());
+    s->triangle_count = static_cast<int>(total);
 
     // Light-table inputs (scene/scene_prepare.h:268-387): the emissive scene triangles
-    // in scene order, then the explicit lights; kept so that vertex updates re-derive
-    // the tables.
-    for (size_t t = 0; t < tris.size(); ++t) {
-        int material;
-        std::memcpy(&material, &tris[t].v0.w, 4);
-        const lux_material& mat = d->materials[material];
-        if (!is_emissive(mat)) continue;
-        lux_scene::EmissiveTri e;
-        e.triangle = static_cast<int>(t);
-        std::memcpy(&e.instance, &tris[t].v1.w, 4);
-        std::memcpy(&e.local, &tris[t].v2.w, 4);
-        e.two_sided = mat.emission_two_sided ? 1 : 0;
-        for (int k = 0; k < 3; ++k) e.emission[k] = mat.emission[k];
-        const float4* v[3] = {&tris[t].v0, &tris[t].v1, &tris[t].v2};
-        for (int k = 0; k < 3; ++k) {
-            e.w[3 * k] = v[k]->x;
-            e.w[3 * k + 1] = v[k]->y;
-            e.w[3 * k + 2] = v[k]->z;
-        }
-        s->emissive.push_back(e);
-    }
+    // in scene order with their world corners (the device preparation's arithmetic),
+    // then the explicit lights; kept so that vertex updates re-derive the tables.  Only
+    // emissive triangles are visited: each mesh lists its emissive local triangles once.
+    std::vector<std::vector<int>> mesh_emissive_tris(d->mesh_count);
+    for (int m = 0; m < d->mesh_count; ++m)
+        for (int t = 0; t < d->meshes[m].triangle_count; ++t)
+            if (is_emissive(d->materials[d->meshes[m].material_ids[t]]))
+                mesh_emissive_tris[m].push_back(t);
     s->mesh_emissive.assign(d->mesh_count, 0);
-    for (const lux_scene::EmissiveTri& e : s->emissive) s->mesh_emissive[s->instances[e.instance].blas] = 1;
+    for (int i = 0; i < d->instance_count; ++i) {
+        const lux_mesh_desc& mesh = d->meshes[d->instances[i].mesh];
+        const int ov = overrides[i];
+        std::vector<int> all;
+        const std::vector<int>* local = &mesh_emissive_tris[d->instances[i].mesh];
+        if (ov >= 0) {
+            if (!is_emissive(d->materials[ov])) continue;
+            all.resize(mesh.triangle_count);
+            for (int t = 0; t < mesh.triangle_count; ++t) all[t] = t;
+            local = &all;
+        }
+        for (int t : *local) {
+            const lux_material& mat = d->materials[ov >= 0 ? ov : mesh.material_ids[t]];
+            lux_scene::EmissiveTri e;
+            e.triangle = s->instances[i].first_primitive + t;
+            e.instance = i;
+            e.local = t;
+            e.two_sided = mat.emission_two_sided ? 1 : 0;
+            for (int k = 0; k < 3; ++k) e.emission[k] = mat.emission[k];
+            for (int k = 0; k < 3; ++k) {
+                const float* q = mesh.vertices + 3 * size_t(mesh.indices[3 * size_t(t) + k]);
+                const V3 w = transform_point(s->instances[i].m, v3(q[0], q[1], q[2]));
+                e.w[3 * k] = w.x;
+                e.w[3 * k + 1] = w.y;
+                e.w[3 * k + 2] = w.z;
+            }
+            s->emissive.push_back(e);
+            s->mesh_emissive[d->instances[i].mesh] = 1;
+        }
+    }
     // Image lights: texels and running weights (make_image_light_asset,
     // scene/scene_build.h:40-65): weight = max(0, luminance(texel * scale)) * sin(theta)
     // at the row centre, summed in row-major order in float.
@@ -666,15 +716,13 @@ int scene_create(lux_ctx* ctx, const lux_scene_desc* d, lux_scene** out) {
         s->explicit_power.push_back(power);
     }
     const LightTables lt = make_light_tables(s->emissive, s->explicit_lights, s->explicit_power,
-                                             tris.size());
+                                             size_t(total));
     s->area_light_count = lt.area_count;
 
     // Uploads.
     std::vector<Material> mats;
     for (int i = 0; i < d->material_count; ++i) mats.push_back(to_material(d->materials[i]));
     int st = upload(&s->materials, mats, ctx->stream);
-    if (!st) st = upload(&s->tris, tris, ctx->stream);
-    if (!st) st = upload(&s->shading, shading, ctx->stream);
     if (!st) st = upload(&s->d_instances, s->instances, ctx->stream);
     if (!st && !env.empty()) {
         st = upload(&s->env_pixels, env_pixels, ctx->stream);
@@ -687,22 +735,87 @@ int scene_create(lux_ctx* ctx, const lux_scene_desc* d, lux_scene** out) {
     }
     if (!st) st = upload_light_tables(ctx, s, lt);
 
-    // BLAS per mesh over object-space soups.
-    std::vector<float> all_soup;
+    // Mesh data to the device, meshes concatenated (the caller's arrays are copied in
+    // stream order; pageable sources are staged before each call returns).
+    size_t n_vert = 0, n_tri = 0;
+    bool any_normals = false, any_uvs = false;
+    for (int m = 0; m < d->mesh_count; ++m) {
+        n_vert += size_t(d->meshes[m].vertex_count);
+        n_tri += size_t(d->meshes[m].triangle_count);
+        any_normals |= d->meshes[m].normals != nullptr;
+        any_uvs |= d->meshes[m].uvs != nullptr;
+    }
+    auto dalloc = [&](void** p, size_t bytes) {
+        if (st) return;
+        if (cudaMalloc(p, std::max<size_t>(bytes, 16)) != cudaSuccess) {
+            cudaGetLastError();
+            *p = nullptr;
+            st = fail(LUX_ERR_OUT_OF_MEMORY, "scene allocation failed");
+        }
+    };
+    dalloc(reinterpret_cast<void**>(&s->mesh_data.vertices), sizeof(float) * 3 * n_vert);
+    dalloc(reinterpret_cast<void**>(&s->mesh_data.indices), sizeof(uint32_t) * 3 * n_tri);
+    dalloc(reinterpret_cast<void**>(&s->mesh_data.material_ids), sizeof(int32_t) * n_tri);
+    if (any_normals) dalloc(reinterpret_cast<void**>(&s->mesh_data.normals), sizeof(float) * 3 * n_vert);
+    if (any_uvs) dalloc(reinterpret_cast<void**>(&s->mesh_data.uvs), sizeof(float) * 2 * n_vert);
+    dalloc(reinterpret_cast<void**>(&s->tri_soup), sizeof(float) * 9 * n_tri);
+    dalloc(reinterpret_cast<void**>(&s->tris), sizeof(pt::SceneTri) * size_t(total));
+    dalloc(reinterpret_cast<void**>(&s->shading), sizeof(pt::SceneTriShading) * size_t(total));
+    std::vector<MeshDev> mesh_dev;
+    size_t vo = 0, to = 0;
+    auto h2d = [&](void* dst, const void* src, size_t bytes) {
+        if (st || !bytes) return;
+        cudaError_t err = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, ctx->stream);
+        if (err != cudaSuccess) st = cuda_fail(err, "scene upload");
+    };
     for (int m = 0; m < d->mesh_count && !st; ++m) {
         const lux_mesh_desc& mesh = d->meshes[m];
-        s->mesh_vertices.emplace_back(mesh.vertices, mesh.vertices + 3 * size_t(mesh.vertex_count));
-        s->mesh_indices.emplace_back(mesh.indices, mesh.indices + 3 * size_t(mesh.triangle_count));
-        std::vector<float> soup = mesh_soup(mesh, mesh.vertices);
-        s->soup_offset.push_back(all_soup.size());
-        all_soup.insert(all_soup.end(), soup.begin(), soup.end());
+        const size_t nv = size_t(mesh.vertex_count), nt = size_t(mesh.triangle_count);
+        h2d(s->mesh_data.vertices + 3 * vo, mesh.vertices, sizeof(float) * 3 * nv);
+        h2d(s->mesh_data.indices + 3 * to, mesh.indices, sizeof(uint32_t) * 3 * nt);
+        h2d(s->mesh_data.material_ids + to, mesh.material_ids, sizeof(int32_t) * nt);
+        if (mesh.normals) h2d(s->mesh_data.normals + 3 * vo, mesh.normals, sizeof(float) * 3 * nv);
+        if (mesh.uvs) h2d(s->mesh_data.uvs + 2 * vo, mesh.uvs, sizeof(float) * 2 * nv);
+        MeshDev md;
+        md.vertices = s->mesh_data.vertices + 3 * vo;
+        md.normals = mesh.normals ? s->mesh_data.normals + 3 * vo : nullptr;
+        md.uvs = mesh.uvs ? s->mesh_data.uvs + 2 * vo : nullptr;
+        md.indices = s->mesh_data.indices + 3 * to;
+        md.material_ids = s->mesh_data.material_ids + to;
+        md.triangle_count = mesh.triangle_count;
+        mesh_dev.push_back(md);
+        s->soup_offset.push_back(9 * to);
+        s->mesh_vertices.emplace_back(mesh.vertices, mesh.vertices + 3 * nv);
+        s->mesh_indices.emplace_back(mesh.indices, mesh.indices + 3 * nt);
+        vo += nv;
+        to += nt;
     }
-    if (!st) st = upload(&s->tri_soup, all_soup, ctx->stream);
+    MeshDev* d_meshes = nullptr;
+    int* d_overrides = nullptr;
+    if (!st) st = upload(&d_meshes, mesh_dev, ctx->stream);
+    if (!st) st = upload(&d_overrides, overrides, ctx->stream);
+
+    // World triangles and shading records of every instance, on the device.
+    if (!st && total > 0) {
+        k_world_triangles<<<prep_blocks(ctx, total), kPrepThreads, 0, ctx->stream>>>(
+            d_meshes, s->d_instances, d_overrides, d->instance_count, static_cast<int>(total),
+            s->tris, s->shading);
+        ctx->launches += 1;
+    }
+
+    // BLAS per mesh over its object-space soup (made on the device).
     std::vector<BvhView> views;
     for (int m = 0; m < d->mesh_count && !st; ++m) {
+        const MeshDev& md = mesh_dev[m];
+        float* soup = s->tri_soup + s->soup_offset[m];
+        if (md.triangle_count > 0) {
+            k_mesh_soup<<<prep_blocks(ctx, md.triangle_count), kPrepThreads, 0, ctx->stream>>>(
+                md.vertices, d->meshes[m].vertex_count, md.indices, md.triangle_count, soup,
+                ctx->d_error);
+            ctx->launches += 1;
+        }
         lux_bvh* b = nullptr;
-        st = lux_lbvh_build(ctx, s->tri_soup + s->soup_offset[m], d->meshes[m].triangle_count,
-                            LUX_PRIM_TRIANGLES, 30, &b);
+        st = lux_lbvh_build(ctx, soup, md.triangle_count, LUX_PRIM_TRIANGLES, 30, &b);
         if (!st) {
             s->blas.push_back(b);
             views.push_back(b->view());
@@ -710,24 +823,22 @@ int scene_create(lux_ctx* ctx, const lux_scene_desc* d, lux_scene** out) {
     }
     if (!st) st = upload(&s->blas_views, views, ctx->stream);
 
-    // TLAS over non-empty instance boxes (collect_scene_tlas_build_primitives,
-    // scene/scene_prepare.h:441-462): primitive k is instance tlas_instance[k].
-    std::vector<float> boxes;
-    for (int i = 0; i < d->instance_count && !st; ++i) {
-        const lux_mesh_desc& mesh = d->meshes[d->instances[i].mesh];
-        std::vector<float> soup = mesh_soup(mesh, mesh.vertices);
-        Box b = instance_box(soup, mesh.triangle_count, s->instances[i].m);
-        if (b.empty()) continue;
-        s->tlas_instance_host.push_back(i);
-        float f[6] = {b.lo.x, b.lo.y, b.lo.z, b.hi.x, b.hi.y, b.hi.z};
-        boxes.insert(boxes.end(), f, f + 6);
-    }
-    if (!st) st = upload(&s->tlas_boxes, boxes, ctx->stream);
+    // TLAS over the instances of non-empty meshes (collect_scene_tlas_build_primitives,
+    // scene/scene_prepare.h:441-462): primitive k is instance tlas_instance[k]; boxes
+    // from the BLAS roots on the device.
+    for (int i = 0; i < d->instance_count; ++i)
+        if (d->meshes[d->instances[i].mesh].triangle_count > 0) s->tlas_instance_host.push_back(i);
+    const int entries = static_cast<int>(s->tlas_instance_host.size());
     if (!st) st = upload(&s->tlas_instance, s->tlas_instance_host, ctx->stream);
-    if (!st) {
-        st = lux_lbvh_build(ctx, s->tlas_boxes, static_cast<int>(s->tlas_instance_host.size()),
-                            LUX_PRIM_AABBS, 30, &s->tlas);
+    dalloc(reinterpret_cast<void**>(&s->tlas_boxes), sizeof(float) * 6 * size_t(entries));
+    if (!st && entries > 0) {
+        k_tlas_boxes<<<(entries + kPrepThreads - 1) / kPrepThreads, kPrepThreads, 0, ctx->stream>>>(
+            s->d_instances, s->tlas_instance, s->blas_views, entries, s->tlas_boxes);
+        ctx->launches += 1;
     }
+    if (!st) st = lux_lbvh_build(ctx, s->tlas_boxes, entries, LUX_PRIM_AABBS, 30, &s->tlas);
+    cudaFree(d_meshes);  // waits for the device
+    cudaFree(d_overrides);
     if (!st) st = cuda_fail(cudaStreamSynchronize(ctx->stream), "scene upload");
     if (st) {
         scene_free(s);
@@ -843,7 +954,7 @@ __global__ void k_mesh_soup(const float* vertices, int vertex_count, const uint3
     }
 }
 
-// World positions of the mesh's triangles in each of its instances (instance_triangles);
+// World positions of the mesh's triangles in each of its instances (k_world_triangles);
 // the .w tags (material, instance, local triangle) are left as uploaded.
 __global__ void k_instance_positions(const float* soup, int triangle_count,
                                      const pt::Instance* instances, const int* ids,

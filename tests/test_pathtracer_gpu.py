@@ -455,3 +455,39 @@ def test_emissive_mesh_update_rederives_light_tables(ctx, change):
     got = S.render_samples(ctx, sc, req)
     want = S.render_samples(ctx, fresh, req)
     assert np.all(got == want, axis=-1).mean() > 0.999
+
+
+@pytest.mark.skipif(not Ref.available(), reason="reference harness not built")
+def test_device_prepared_instances_and_overrides_match_reference(ctx):
+    """Scene preparation on the device: an instanced mesh with normals and texcoords, one
+    instance overridden to an emissive material and one to glass; the light tables (area
+    lights from the override, in scene-triangle order) select like the reference scene
+    built from the same world triangles: the same lights and pmf bits."""
+    from lux_b200 import scenes as SC
+    w = h = 32
+    b = S.make_cornell_scene(w, h)
+    v, idx = SC.displaced_sphere(2, (0.0, 0.0, 0.0), 0.2, 0.03, 9)
+    nrm = (v / np.linalg.norm(v, axis=1, keepdims=True)).astype(np.float32)
+    uv = np.random.default_rng(2).random((len(v), 2)).astype(np.float32)
+    rough = b.add_material(S.ggx((0.7, 0.6, 0.5), 0.3, 0.0))
+    glow = b.add_material(S.emissive((2.0, 1.5, 1.0)))
+    glass = b.add_material(S.dielectric((1, 1, 1), 1.5))
+    mesh = b.add_mesh(S.Mesh(v, idx, np.full(len(idx), rough, np.int32), nrm, uv))
+    for k, override in enumerate([-1, glow, glass]):
+        m = np.array([[1, 0, 0, -0.5 + 0.5 * k], [0, 1, 0, 0.4], [0, 0, 1, 0.9]], np.float32)
+        b.add_instance(mesh, m, override)
+    sc = S.Scene(ctx, b)
+    tris, mids, mats, lights = _ref_arrays(b)
+    info = sc.info()
+    assert info["triangles"] == len(tris) and info["area_lights"] == 2 + len(idx)
+    rng = np.random.default_rng(5)
+    pos = rng.uniform([-1, 0, 0], [1, 2, 2], (4096, 3)).astype(np.float32)
+    u = rng.random(4096, dtype=np.float32)
+    cam = ((0.0, 1.0, 3.35), (0.0, 1.0, 0.9), 40.0, 1.0)
+    camera = np.array([*cam[0], *cam[1], cam[2], cam[3]], np.float32)
+    ref = Ref()
+    for sampler in (S.SAMPLER_POWER, S.SAMPLER_TREE):
+        got = sc.select_lights(pos, u, sampler)
+        want = ref.select_lights(tris, mids, mats, lights, camera, sampler, pos, u)
+        for g, x in zip(got, want):
+            assert np.array_equal(g, x)
