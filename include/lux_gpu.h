@@ -367,6 +367,28 @@ int lux_scene_info(const lux_scene* scene, int32_t* triangles, int32_t* area_lig
                    int32_t* lights);
 
 /*
+ * lux_render with the reference wavefront tracer's debug images (`-debug-aov shadow,ng,ns`
+ * with `-gpu`; RenderOutputs / WavefrontDebugViews, integrator/wavefront_debug.cuh and
+ * integrator/wavefront_kernels.cu:287-305, 475-482, 586-592).  Each non-null image
+ * receives width * height * 3 per-pixel sums over the samples (divide by spp, as
+ * write_debug_ppm_linear does):
+ *   ng, ns  the camera ray's hit: 0.5 * (normalize(n) + 1) of the geometric normal and
+ *           of the shading normal turned to its side; nothing where the ray misses;
+ *   shadow  the path's first scattering hit, when it samples a light: (1, 0.5, 0) for an
+ *           invalid light sample, (0.5, 0, 1) for an invalid unoccluded estimate, else
+ *           the shadow ray's class: (1, 0, 0) light behind the geometric but not the
+ *           shading normal; unblocked (0, 0.35, 0.8) after pass-through surfaces, else
+ *           (0.03, 0.03, 0.03); blocked by the source's own material within 16 ray
+ *           epsilons (1, 1, 0), by a back face of it (0, 0, 1), a front face of it
+ *           (0, 1, 1), another material (0, 1, 0).  Mesh boundary edges are not carried,
+ *           so the reference's (1, 0, 1) class reads as (0, 0, 1).
+ * film_sum is the same film lux_render writes.  The images are summed with atomics, so
+ * their last bits may vary between runs.  Host or device arrays.
+ */
+int lux_render_aovs(lux_ctx* ctx, const lux_scene* scene, const lux_render_request* req,
+                    float* film_sum, float* shadow, float* ng, float* ns);
+
+/*
  * Light selection as next-event estimation makes it, for validation: for each i, the
  * light that select_u[i] picks at shading position positions[3i..3i+2] with sampler kind
  * light_sampler (0 uniform, 1 power, 2 light tree), in light-table order (area lights in

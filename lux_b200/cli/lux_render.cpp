@@ -11,7 +11,9 @@
 // lux_film_encode).  This build renders on the GPU only: without -gpu it still renders
 // on the GPU and says so.  The asset scenes (bunny, dragon, lux-cover) load their OBJ
 // files through lux_obj_load from the reference's asset root (assets/ next to the
-// executable, else ./assets); the debug probes/AOVs are reported as unsupported.
+// executable, else ./assets).  -debug-aov shadow,ng,ns writes the wavefront tracer's
+// debug images (lux_render_aovs) as the reference does; the CPU diagnostics (probes,
+// mesh audits, the orientation image) are reported as unsupported.
 
 #include <chrono>
 #include <cmath>
@@ -44,7 +46,16 @@ struct Config {
     int light_sampler = 1;  // power
     bool unsupported_option = false;
     std::string unsupported_name;
+    // DebugRequest (diagnostics/diagnostic_config.h:51-70).
+    int probe_mode = 0;          // 0 none, else camera-hits / path / nee
+    bool probe_pixel = false;
+    unsigned aov_mask = 0;       // kAov* bits
+    int mesh_mode = 0;           // 0 none, else orientation-audit / winding
+    std::string debug_output;
 };
+
+// DebugAovMask bits and names (diagnostics/diagnostic_config.h).
+constexpr unsigned kAovOrientation = 1u, kAovShadow = 2u, kAovNg = 4u, kAovNs = 8u;
 
 bool parse_int(const char* text, int& value, bool allow_zero) {
     char* end = nullptr;
@@ -57,6 +68,24 @@ bool parse_int(const char* text, int& value, bool allow_zero) {
 
 bool is_opt(const char* a, const char* s, const char* l) {
     return std::strcmp(a, s) == 0 || std::strcmp(a, l) == 0;
+}
+
+// parse_debug_aov_list (app/render_config.h:101-137): comma-separated, no empty names.
+bool parse_aov_list(const char* text, unsigned& mask) {
+    std::string list(text);
+    size_t begin = 0;
+    for (;;) {
+        size_t end = list.find(',', begin);
+        std::string name = list.substr(begin, end == std::string::npos ? std::string::npos
+                                                                       : end - begin);
+        if (name == "orientation") mask |= kAovOrientation;
+        else if (name == "shadow") mask |= kAovShadow;
+        else if (name == "ng") mask |= kAovNg;
+        else if (name == "ns") mask |= kAovNs;
+        else return false;
+        if (end == std::string::npos) return true;
+        begin = end + 1;
+    }
 }
 
 // parse_render_config (app/render_config.h:196-340).
@@ -109,32 +138,79 @@ bool parse(int argc, char** argv, Config& c) {
             }
         } else if (is_opt(a, "-time", "--time")) {
             c.timing = true;
-        } else if (is_opt(a, "-debug-probe", "--debug-probe") ||
-                   is_opt(a, "-debug-mode", "--debug-mode") ||
-                   is_opt(a, "-debug-aov", "--debug-aov") ||
-                   is_opt(a, "-debug-output", "--debug-output") ||
-                   is_opt(a, "-debug-mesh", "--debug-mesh")) {
-            c.unsupported_option = true;
-            c.unsupported_name = a;
-            int operands = is_opt(a, "-debug-probe", "--debug-probe") ? 2 : 1;
-            for (int k = 0; k < operands; ++k)
-                if (!next(v)) return false;
+        } else if (is_opt(a, "-debug-probe", "--debug-probe")) {
+            int px = 0, py = 0;
+            if (!next(v) || !parse_int(v, px, true)) return false;
+            if (!next(v) || !parse_int(v, py, true)) return false;
+            c.probe_pixel = true;
+            if (c.probe_mode == 0) c.probe_mode = 1;
+        } else if (is_opt(a, "-debug-mode", "--debug-mode")) {
+            if (!next(v)) return false;
+            if (std::strcmp(v, "camera-hits") == 0) c.probe_mode = 1;
+            else if (std::strcmp(v, "path") == 0) c.probe_mode = 2;
+            else if (std::strcmp(v, "nee") == 0) c.probe_mode = 3;
+            else return false;
+        } else if (is_opt(a, "-debug-aov", "--debug-aov")) {
+            if (!next(v) || !parse_aov_list(v, c.aov_mask)) return false;
+        } else if (is_opt(a, "-debug-output", "--debug-output")) {
+            if (!next(v)) return false;
+            c.debug_output = v;
+        } else if (is_opt(a, "-debug-samples", "--debug-samples") ||
+                   is_opt(a, "-debug-max-hits", "--debug-max-hits")) {
+            int n = 0;
+            if (!next(v) || !parse_int(v, n, false)) return false;
+        } else if (is_opt(a, "-debug-mesh", "--debug-mesh")) {
+            if (!next(v)) return false;
+            if (std::strcmp(v, "orientation-audit") == 0) c.mesh_mode = 1;
+            else if (std::strcmp(v, "winding") == 0) c.mesh_mode = 2;
+            else return false;
+        } else if (is_opt(a, "-debug-triangle", "--debug-triangle")) {
+            int t = 0;
+            if (!next(v) || !parse_int(v, t, true)) return false;
+            if (c.mesh_mode == 0) c.mesh_mode = 2;
         } else if (a[0] == '-') {
             return false;
         } else {
-            if (positional) return false;
+            // The one positional argument is the output path, alone on the command line.
+            if (positional || argc != 2) return false;
             positional = true;
-            c.scene = a;
+            c.output = a;
+            c.output_mode = 1;
         }
     }
+    // validate_debug_request (app/render_config.h:167-175): one debug category at most;
+    // a probe needs its pixel.
+    const int categories = (c.probe_mode ? 1 : 0) + (c.mesh_mode ? 1 : 0) + (c.aov_mask ? 1 : 0);
+    if (categories > 1 || (c.probe_mode && !c.probe_pixel)) return false;
+    // The probes, mesh diagnostics and the orientation image are CPU diagnostics.
+    if (c.probe_mode || c.mesh_mode || (c.aov_mask & kAovOrientation)) {
+        c.unsupported_option = true;
+        c.unsupported_name = c.probe_mode ? "-debug-probe" : c.mesh_mode ? "-debug-mesh"
+                                                                        : "-debug-aov orientation";
+    }
     return true;
+}
+
+// debug_aov_output_path (diagnostics/diagnostic_config.h:32-43): the image's name before
+// the prefix's .ppm / .pfm extension.
+std::string aov_path(const std::string& prefix, const char* name) {
+    std::string base = prefix, ext = ".ppm";
+    if (base.size() >= 4) {
+        std::string suffix = base.substr(base.size() - 4);
+        if (suffix == ".ppm" || suffix == ".pfm") {
+            ext = suffix;
+            base.resize(base.size() - 4);
+        }
+    }
+    return base + "_" + name + ext;
 }
 
 void usage(const char* exe) {
     std::printf(
         "Usage: %s [scene] [options]\n"
         "  -scene NAME             cornell, direct-light, point-light, distant-light,\n"
-        "                          uniform-env, image-env, transparent-filter\n"
+        "                          uniform-env, image-env, transparent-filter, bunny,\n"
+        "                          dragon, lux-cover\n"
         "  -width N / -height N / -size W H   film size (default 256x256)\n"
         "  -spp N                  samples per pixel (default 64)\n"
         "  -depth N                maximum path depth (default 4)\n"
@@ -142,7 +218,9 @@ void usage(const char* exe) {
         "  -output PATH            image path (.ppm, or .pfm for linear floats)\n"
         "  -out NAME               write out/NAME/<NAME>.ppm\n"
         "  -gpu                    render with the GPU path (the only path of this build)\n"
-        "  -time                   print a timing breakdown\n",
+        "  -time                   print a timing breakdown\n"
+        "  -debug-aov LIST         debug images: shadow, ng, ns (comma-separated)\n"
+        "  -debug-output PATH      prefix of the debug images (default: the image path)\n",
         exe);
 }
 
@@ -563,7 +641,15 @@ int main(int argc, char** argv) {
     req.light_sampler = c.light_sampler;
     std::vector<float> film(static_cast<size_t>(c.width) * c.height * 3);
     t0 = Clock::now();
-    int st = lux_render(ctx, scene, &req, film.data());
+    const bool aovs = (c.aov_mask & (kAovShadow | kAovNg | kAovNs)) != 0;
+    std::vector<float> aov_shadow, aov_ng, aov_ns;
+    for (auto [bit, image] : {std::pair{kAovShadow, &aov_shadow}, std::pair{kAovNg, &aov_ng},
+                              std::pair{kAovNs, &aov_ns}})
+        if (c.aov_mask & bit) image->assign(film.size(), 0.0f);
+    auto ptr_of = [](std::vector<float>& v) { return v.empty() ? nullptr : v.data(); };
+    int st = aovs ? lux_render_aovs(ctx, scene, &req, film.data(), ptr_of(aov_shadow), ptr_of(aov_ng),
+                                    ptr_of(aov_ns))
+                  : lux_render(ctx, scene, &req, film.data());
     t_render = ms_since(t0);
     if (check(st, "GPU render")) {
         lux_scene_destroy(scene);
@@ -590,12 +676,48 @@ int main(int argc, char** argv) {
         out.write(reinterpret_cast<const char*>(px.data()), px.size());
     }
     out.close();
+    if (!st && aovs) {
+        std::printf("Wrote %s (%dx%d, %d spp, depth %d)\n", path.c_str(), c.width, c.height,
+                    c.spp, c.max_depth);
+        // write_debug_pixels (app/render_runner.cpp:250-256): PFM, else a linear PPM.
+        const std::string prefix = c.debug_output.empty() ? path : c.debug_output;
+        const struct {
+            unsigned bit;
+            const char* name;
+            const char* label;
+            std::vector<float>* image;
+        } outs[] = {{kAovShadow, "shadow", "shadow classification", &aov_shadow},
+                    {kAovNg, "ng", "geometric normal", &aov_ng},
+                    {kAovNs, "ns", "shading normal", &aov_ns}};
+        for (const auto& o : outs) {
+            if (!(c.aov_mask & o.bit) || st) continue;
+            const std::string apath = aov_path(prefix, o.name);
+            std::filesystem::path aparent = std::filesystem::path(apath).parent_path();
+            if (!aparent.empty()) std::filesystem::create_directories(aparent);
+            std::ofstream f(apath, std::ios::binary);
+            if (ends_with(apath, ".pfm")) {
+                std::vector<float> px(film.size());
+                st = lux_film_encode(ctx, o.image->data(), c.width, c.height, c.spp, LUX_FILM_PFM,
+                                     px.data());
+                f << "PF\n" << c.width << " " << c.height << "\n-1.0\n";
+                f.write(reinterpret_cast<const char*>(px.data()), px.size() * sizeof(float));
+            } else {
+                std::vector<unsigned char> px(film.size());
+                st = lux_film_encode(ctx, o.image->data(), c.width, c.height, c.spp,
+                                     LUX_FILM_PPM8_LINEAR, px.data());
+                f << "P6\n" << c.width << " " << c.height << "\n255\n";
+                f.write(reinterpret_cast<const char*>(px.data()), px.size());
+            }
+            std::printf("Wrote %s (GPU %s AOV)\n", apath.c_str(), o.label);
+        }
+    }
     t_write = ms_since(t0);
     lux_scene_destroy(scene);
     lux_ctx_destroy(ctx);
     if (check(st, "Output write")) return 1;
-    std::printf("Wrote %s (%dx%d, %d spp, depth %d)\n", path.c_str(), c.width, c.height, c.spp,
-                c.max_depth);
+    if (!aovs)
+        std::printf("Wrote %s (%dx%d, %d spp, depth %d)\n", path.c_str(), c.width, c.height,
+                    c.spp, c.max_depth);
     if (c.timing) {  // print_timing_breakdown (app/render_runner.cpp:270-285)
         std::printf("Timing breakdown:\n");
         std::printf("  scene setup: %.3f ms\n", t_setup);

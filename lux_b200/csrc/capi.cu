@@ -644,6 +644,36 @@ int lux_render(lux_ctx* ctx, const lux_scene* scene, const lux_render_request* r
     return render_common(ctx, scene, req, film_sum, false);
 }
 
+int lux_render_aovs(lux_ctx* ctx, const lux_scene* scene, const lux_render_request* req,
+                    float* film_sum, float* shadow, float* ng, float* ns) {
+    if (int st = check_ctx(ctx)) return st;
+    if (!scene || !req || !film_sum) return lux::fail(LUX_ERR_INVALID_ARGUMENT, "null argument");
+    if (req->width <= 0 || req->height <= 0 || req->spp <= 0)
+        return lux::fail(LUX_ERR_INVALID_ARGUMENT, "render requires a non-empty film");
+    if (req->max_depth < 0 || req->max_depth > 1000)
+        return lux::fail(LUX_ERR_INVALID_ARGUMENT, "max_depth must be in 0..1000");
+    if (req->light_sampler < 0 || req->light_sampler > 2)
+        return lux::fail(LUX_ERR_INVALID_ARGUMENT, "light sampler: 0 uniform, 1 power or 2 tree");
+    if (static_cast<long long>(req->width) * req->height > (1ll << 30))
+        return lux::fail(LUX_ERR_INVALID_ARGUMENT, "image too large");
+    const size_t bytes = sizeof(float) * 3 * static_cast<size_t>(req->width) * req->height;
+    Staging staging(ctx);
+    void *d_film = nullptr, *d_shadow = nullptr, *d_ng = nullptr, *d_ns = nullptr;
+    staging.add(film_sum, bytes, false, true, &d_film);
+    staging.add(shadow, bytes, false, true, &d_shadow);
+    staging.add(ng, bytes, false, true, &d_ng);
+    staging.add(ns, bytes, false, true, &d_ns);
+    int st = staging.begin();
+    if (st) return st;
+    st = lux::render(ctx, scene, *req, static_cast<float*>(d_film), false,
+                     static_cast<float*>(d_shadow), static_cast<float*>(d_ng),
+                     static_cast<float*>(d_ns));
+    if (st) return st;
+    st = finish_call(ctx, staging);
+    if (st) return st;
+    return sync_and_check(ctx);
+}
+
 int lux_render_samples(lux_ctx* ctx, const lux_scene* scene, const lux_render_request* req,
                        float* samples) {
     return render_common(ctx, scene, req, samples, true);

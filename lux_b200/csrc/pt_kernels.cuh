@@ -1146,9 +1146,71 @@ struct ShadeOut {
     bool shadow = false;  // sh_*[p] hold a shadow ray
 };
 
-// Shading of the hit stored for path p (cpu_path_tracer.cpp:430-497).
+// ------------------------------------------------------------------ debug images
+// The reference wavefront tracer's debug images (integrator/wavefront_debug.cuh,
+// wavefront_kernels.cu:287-305, 475-482, 586-592), per-pixel sums over samples:
+//   ng / ns   at the camera ray's hit: 0.5 * (normalize(n) + 1) of the geometric normal /
+//             of the shading normal turned to the geometric side; nothing on a miss;
+//   shadow    at the path's first scattering hit (depth 0, after pass-through surfaces),
+//             when it samples a light: orange (1, 0.5, 0) when the light sample is
+//             invalid, purple (0.5, 0, 1) when the unoccluded estimate is, else the
+//             classification of its shadow ray (shadow_aov_color).
+struct AovTargets {
+    float* shadow = nullptr;
+    float* ng = nullptr;
+    float* ns = nullptr;
+};
+
+LUX_D void aov_add(float* image, int pixel, f3 c) {
+    atomicAdd(image + 3 * size_t(pixel), c.x);
+    atomicAdd(image + 3 * size_t(pixel) + 1, c.y);
+    atomicAdd(image + 3 * size_t(pixel) + 2, c.z);
+}
+
+LUX_D f3 encode_normal_color(f3 n) { return (normalize(n) + splat(1.0f)) * 0.5f; }
+
+// primary_normal_debug_color for the camera ray's closest hit h of path p.
+LUX_D void aov_primary(const PathPool& rt, const SceneView& sc, int p, const SceneHit& h,
+                       const AovTargets& aov) {
+    const int4 meta = rt.meta[p];
+    if (meta.z != 0 || h.prim < 0) return;  // depth and pass-through count both zero
+    const SceneTri tri = sc.tris[h.prim];
+    const f3 ng = triangle_normal(xyz(tri.v0), xyz(tri.v1), xyz(tri.v2));
+    if (aov.ng) aov_add(aov.ng, meta.x, encode_normal_color(ng));
+    if (aov.ns) {
+        f3 ns = shading_normal(sc.shading[h.prim], ng, h.u, h.v);
+        if (dot(ng, ns) < 0) ns = -ns;
+        aov_add(aov.ns, meta.x, encode_normal_color(ns));
+    }
+}
+
+// shadow_debug_classification_color: red when the shading normal faces the light but
+// the geometric normal does not; unblocked: blue-ish after pass-through surfaces, else
+// dark grey; blocked by the source's own material within 16 epsilon: yellow; by a back
+// face of it: blue (magenta near a mesh boundary edge, which these scenes do not carry);
+// by a front face of it: cyan; by another material: green.
+LUX_D f3 shadow_aov_color(const SceneView& sc, int source_prim, f3 ng, f3 ns, f3 dir,
+                          int occluder, float hit_t, int passthrough_hits) {
+    const float shading_cos = dot(ns, dir);
+    const float geometric_cos = dot(ng, dir);
+    if (shading_cos > 0 && geometric_cos <= 0) return make_f3(1, 0, 0);
+    if (occluder < 0) return passthrough_hits > 0 ? make_f3(0, 0.35f, 0.8f) : splat(0.03f);
+    const bool same = material_of(sc, occluder) == material_of(sc, source_prim);
+    if (same && hit_t < mul(16.0f, kRayEpsilon)) return make_f3(1, 1, 0);
+    if (same) {
+        const SceneTri o = sc.tris[occluder];
+        const bool back = dot(triangle_normal(xyz(o.v0), xyz(o.v1), xyz(o.v2)), -dir) <= 0;
+        return back ? make_f3(0, 0, 1) : make_f3(0, 1, 1);
+    }
+    return make_f3(0, 1, 0);
+}
+
+// Shading of the hit stored for path p (cpu_path_tracer.cpp:430-497).  With kAov, also
+// the shadow debug image's light-sample verdict at depth 0, and shadow rays at depth 0
+// are marked (sh_t.w = 1) for classification.
+template <bool kAov = false>
 LUX_D ShadeOut shade_path(const PathPool& rt, const SceneView& sc, int sampler, int max_depth,
-                          int p) {
+                          int p, const AovTargets& aov = AovTargets{}) {
     ShadeOut out;
     float4 ra = rt.ray_o[p], rb = rt.ray_d[p], hh = rt.hit[p];
     f3 ro = xyz(ra), rd = xyz(rb);
@@ -1196,11 +1258,14 @@ LUX_D ShadeOut shade_path(const PathPool& rt, const SceneView& sc, int sampler, 
         float lx = g.next_float();
         float ly = g.next_float();
         LightLi li = sample_light(sc, sampler, pos, su, cu, lx, ly);
+        int verdict = 0;  // 0 light sample invalid, 1 estimate invalid, 2 valid
         if (li.valid && li.pdf > 0) {
+            verdict = 1;
             f3 f = eval_bsdf(m, it, li.wi);
             float cs = abs_cosine(ns, li.wi);
             float pb = pdf_bsdf(m, it, li.wi);
             if (max_component(f) > 0 && max_component(li.radiance) > 0 && cs > 0) {
+                verdict = 2;
                 f3 contrib = (f * li.radiance) * (cs / li.pdf);
                 float mis = li.measure == kMeasureDiscrete ? 1.0f : power_heuristic(li.pdf, pb);
                 f3 off = dot(li.wi, ng) >= 0 ? ng : -ng;
@@ -1218,15 +1283,26 @@ LUX_D ShadeOut shade_path(const PathPool& rt, const SceneView& sc, int sampler, 
                         smax = sub(dist, kRayEpsilon);
                     }
                 }
+                const bool mark = kAov && aov.shadow && s.depth == 0 && sc.light_count > 0 &&
+                                  sc.total_light_power > 0;
+                if (!ok && mark) {  // make_shadow_work_item_li: a zero-length ray, no light
+                    sd = li.wi;
+                    smax = kRayEpsilon;
+                    contrib = splat(0.0f);
+                    ok = true;
+                }
                 if (ok) {
                     out.shadow = true;
                     rt.sh_o[p] = make_float4(so.x, so.y, so.z, smax);
                     rt.sh_d[p] = make_float4(sd.x, sd.y, sd.z, __int_as_float(prim));
                     rt.sh_c[p] = make_float4(contrib.x, contrib.y, contrib.z, mis);
-                    rt.sh_t[p] = make_float4(s.thr.x, s.thr.y, s.thr.z, 0.0f);
+                    rt.sh_t[p] = make_float4(s.thr.x, s.thr.y, s.thr.z, mark ? 1.0f : 0.0f);
                 }
             }
         }
+        if (kAov && aov.shadow && s.depth == 0 && verdict < 2 && sc.light_count > 0 &&
+            sc.total_light_power > 0)
+            aov_add(aov.shadow, s.pixel, verdict == 0 ? make_f3(1, 0.5f, 0) : make_f3(0.5f, 0, 1));
     }
     float bx = g.next_float();
     float by = g.next_float();
@@ -1262,9 +1338,11 @@ LUX_D ShadeOut shade_path(const PathPool& rt, const SceneView& sc, int sampler, 
 }
 
 // Shadow ray of path p through pass-through surfaces (trace_shadow,
-// cpu_path_tracer.cpp:27-73); adds throughput * ((contribution * T) * mis).
+// cpu_path_tracer.cpp:27-73); adds throughput * ((contribution * T) * mis).  With kAov,
+// a ray marked at shading adds its classification colour to the shadow debug image.
+template <bool kAov = false>
 LUX_D void shadow_path(const PathPool& rt, const SceneView& sc, int p, int* error,
-                       unsigned long long& segments) {
+                       unsigned long long& segments, const AovTargets& aov = AovTargets{}) {
     float4 a = rt.sh_o[p], b = rt.sh_d[p];
     f3 o = xyz(a), d = xyz(b);
     float tmax = a.w;
@@ -1272,6 +1350,8 @@ LUX_D void shadow_path(const PathPool& rt, const SceneView& sc, int p, int* erro
     int ignored = __float_as_int(b.w);
     f3 tr = splat(1.0f);
     bool blocked = false;
+    int occluder = -1, crossed = 0;
+    float occluder_t = 0;
     for (int seg = 0;; ++seg) {
         if (seg >= kShadowSegments) {
             atomicOr(error, kErrLoopBound);
@@ -1284,8 +1364,11 @@ LUX_D void shadow_path(const PathPool& rt, const SceneView& sc, int p, int* erro
         const Material m = sc.materials[material_of(sc, h.prim)];
         if (!is_passthrough(m)) {
             blocked = true;
+            occluder = h.prim;
+            occluder_t = h.t;
             break;
         }
+        ++crossed;
         tr = tr * passthrough_transmittance(m);
         if (max_component(tr) <= 0) break;
         float adv = add(h.t, kRayEpsilon);
@@ -1299,6 +1382,16 @@ LUX_D void shadow_path(const PathPool& rt, const SceneView& sc, int p, int* erro
         float4 c = rt.sh_c[p], t = rt.sh_t[p];
         f3 contrib = (xyz(c) * tr) * c.w;
         add_radiance(rt, p, xyz(t) * contrib);
+    }
+    if (kAov && aov.shadow && rt.sh_t[p].w == 1.0f) {
+        const int source = __float_as_int(rt.sh_d[p].w);
+        const SceneTri tri = sc.tris[source];
+        const f3 ng = triangle_normal(xyz(tri.v0), xyz(tri.v1), xyz(tri.v2));
+        const float4 hh = rt.hit[p];
+        f3 ns = shading_normal(sc.shading[source], ng, hh.y, hh.z);
+        if (dot(ng, ns) < 0) ns = -ns;
+        aov_add(aov.shadow, rt.meta[p].x,
+                shadow_aov_color(sc, source, ng, ns, d, occluder, occluder_t, crossed));
     }
 }
 

@@ -93,9 +93,11 @@ int camera_perspective(const float* origin, const float* look_at, float vfov, fl
                        float lens_radius, float focal_distance, lux_camera_desc* out);
 
 // Wavefront renderer (wavefront.cu).  out is a device pointer: film sums (width*height*3)
-// or, when per_sample, every sample's radiance ((pixel*spp + s)*3).
+// or, when per_sample, every sample's radiance ((pixel*spp + s)*3).  Non-null aov_*
+// (device, width*height*3) receive the debug images' per-pixel sums.
 int render(lux_ctx* ctx, const lux_scene* scene, const lux_render_request& req, float* out,
-           bool per_sample);
+           bool per_sample, float* aov_shadow = nullptr, float* aov_ng = nullptr,
+           float* aov_ns = nullptr);
 int render_ray_counts(lux_ctx* ctx, int64_t* counts);
 // Light selection queries (device arrays): sample_scene_light and light_pmf at each
 // position, as next-event estimation makes them.

@@ -145,6 +145,69 @@ __global__ void __launch_bounds__(kThreads) k_shadow_refill(PathPool rt, int* co
     warp_add(rays + 1, segments);
 }
 
+// The bounce kernels with the debug images (one path per thread, closest-hit shadow
+// segments, as the classification needs the blocking hit).
+__global__ void __launch_bounds__(kThreads) k_extend_aov(PathPool rt, int* counts, SceneView sc,
+                                                         int sampler, int depth, int* error,
+                                                         AovTargets aov) {
+    int n = counts[depth * kSlots];
+    int* mat_counts = counts + depth * kSlots + 1;
+    const int* q = rt.qray[depth & 1];
+    int stride = gridDim.x * blockDim.x;
+    int rounds = (n + stride - 1) / stride;
+    for (int r = 0; r < rounds; ++r) {
+        int i = r * stride + blockIdx.x * blockDim.x + threadIdx.x;
+        bool active = i < n;
+        int p = active ? q[i] : 0;
+        int cls = -1;
+        if (active) {
+            const float4 a = rt.ray_o[p], b = rt.ray_d[p];
+            const SceneHit h = scene_closest(sc, xyz(a), xyz(b), a.w, b.w, -1, error);
+            if (depth == 0) aov_primary(rt, sc, p, h, aov);
+            cls = extend_finish(rt, sc, sampler, p, h);
+        }
+        bool hit = cls >= 0;
+        int slot = append(mat_counts, hit ? cls : 0, hit);
+        if (hit) rt.qmat[cls * rt.capacity + slot] = p;
+    }
+}
+
+__global__ void __launch_bounds__(kThreads) k_shade_aov(PathPool rt, int* counts, SceneView sc,
+                                                        int sampler, int depth, int max_depth,
+                                                        AovTargets aov) {
+    const int* mc = counts + depth * kSlots + 1;
+    int* next_count = counts + (depth + 1) * kSlots;
+    int* shadow_count = counts + depth * kSlots + 6;
+    int total = 0;
+    for (int k = 0; k < kClasses; ++k) total += mc[k];
+    int* qnext = rt.qray[(depth + 1) & 1];
+    int stride = gridDim.x * blockDim.x;
+    int rounds = (total + stride - 1) / stride;
+    for (int r = 0; r < rounds; ++r) {
+        int i = r * stride + blockIdx.x * blockDim.x + threadIdx.x;
+        bool active = i < total;
+        int cls = 0, j = i;
+        while (cls < kClasses - 1 && j >= mc[cls]) j -= mc[cls++];
+        int p = active ? rt.qmat[cls * rt.capacity + j] : 0;
+        ShadeOut o;
+        if (active) o = shade_path<true>(rt, sc, sampler, max_depth, p, aov);
+        int slot = append(shadow_count, 0, o.shadow);
+        if (o.shadow) rt.qshadow[slot] = p;
+        slot = append(next_count, 0, o.spawn);
+        if (o.spawn) qnext[slot] = p;
+    }
+}
+
+__global__ void __launch_bounds__(kThreads) k_shadow_aov(PathPool rt, int* counts,
+                                                         unsigned long long* rays, SceneView sc,
+                                                         int depth, int* error, AovTargets aov) {
+    int n = counts[depth * kSlots + 6];
+    unsigned long long segments = 0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        shadow_path<true>(rt, sc, rt.qshadow[i], error, segments, aov);
+    warp_add(rays + 1, segments);
+}
+
 // Per-pixel film accumulation in sample order; or every sample's radiance.
 __global__ void __launch_bounds__(kThreads) k_flush(PathPool rt, Batch b, float* film,
                                                     float* samples, int spp) {
@@ -301,8 +364,13 @@ int render_ray_counts(lux_ctx* ctx, int64_t* counts) {
 }
 
 int render(lux_ctx* ctx, const lux_scene* scene, const lux_render_request& req, float* out,
-           bool per_sample) {
+           bool per_sample, float* aov_shadow, float* aov_ng, float* aov_ns) {
     using namespace pt;
+    AovTargets aov;
+    aov.shadow = aov_shadow;
+    aov.ng = aov_ng;
+    aov.ns = aov_ns;
+    const bool with_aov = aov_shadow || aov_ng || aov_ns;
     const int pixels = req.width * req.height;
     const long long total_paths = static_cast<long long>(pixels) * req.spp;
     // Batch: whole pixels' sample ranges, at most ctx->render_batch paths.
@@ -334,6 +402,9 @@ int render(lux_ctx* ctx, const lux_scene* scene, const lux_render_request& req, 
     cudaError_t err = cudaMemsetAsync(rt.rays, 0, 16, s);
     if (!per_sample && err == cudaSuccess)
         err = cudaMemsetAsync(out, 0, sizeof(float) * 3 * size_t(pixels), s);
+    for (float* image : {aov_shadow, aov_ng, aov_ns})
+        if (image && err == cudaSuccess)
+            err = cudaMemsetAsync(image, 0, sizeof(float) * 3 * size_t(pixels), s);
     if (err != cudaSuccess) return cuda_fail(err, "render setup");
     for (int s0 = 0; s0 < req.spp; s0 += samples_per_batch) {
         int ns = std::min(samples_per_batch, req.spp - s0);
@@ -349,6 +420,16 @@ int render(lux_ctx* ctx, const lux_scene* scene, const lux_render_request& req, 
             k_camera<<<grid, kThreads, 0, s>>>(rt.pool, rt.counts, sc, b);
             ctx->launches += 1;
             for (int d = 0; d <= req.max_depth; ++d) {
+                if (with_aov) {
+                    k_extend_aov<<<grid, kThreads, 0, s>>>(rt.pool, rt.counts, sc,
+                                                           req.light_sampler, d, ctx->d_error, aov);
+                    k_shade_aov<<<grid, kThreads, 0, s>>>(rt.pool, rt.counts, sc,
+                                                          req.light_sampler, d, req.max_depth, aov);
+                    k_shadow_aov<<<grid, kThreads, 0, s>>>(rt.pool, rt.counts, rt.rays, sc, d,
+                                                           ctx->d_error, aov);
+                    ctx->launches += 3;
+                    continue;
+                }
                 if (ctx->trace_variant == kTraceStatic) {
                     k_extend<<<grid, kThreads, 0, s>>>(rt.pool, rt.counts, sc, req.light_sampler,
                                                        d, ctx->d_error);

@@ -308,6 +308,16 @@ def render(ctx, scene: Scene, req: RenderRequest, out=None):
     return out
 
 
+def render_aovs(ctx, scene: Scene, req: RenderRequest, shadow=True, ng=True, ns=True):
+    """Film sum and the wanted debug images (per-pixel sums over spp, height x width x 3;
+    None where not wanted), as lux_render_aovs makes them."""
+    film = np.zeros((req.height, req.width, 3), np.float32)
+    out = [np.zeros_like(film) if want else None for want in (shadow, ng, ns)]
+    _check(ctx._lib.lux_render_aovs(ctx.handle, scene.handle, ctypes.byref(req), _ptr(film),
+                                    *(None if a is None else _ptr(a) for a in out)))
+    return film, out[0], out[1], out[2]
+
+
 def render_samples(ctx, scene: Scene, req: RenderRequest):
     out = np.zeros((req.height * req.width, req.spp, 3), np.float32)
     _check(ctx._lib.lux_render_samples(ctx.handle, scene.handle, ctypes.byref(req), _ptr(out)))

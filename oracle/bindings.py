@@ -118,6 +118,8 @@ class Ref:
                                          ctypes.c_uint64, _I, _I, _I, _I, _P, _P, _I, _I]
         lib.ref_select_lights.argtypes = [_P, _I, _P, _P, _I, _P, _I, _P, _I, _P, _P, _I,
                                           _P, _P, _P]
+        lib.ref_render_aovs.argtypes = [_P, _I, _P, _P, _I, _P, _I, _P, _I, _I, _I, _I,
+                                        ctypes.c_uint64, _I, _P, _P, _P, _P]
         lib.ref_obj_load.argtypes = [ctypes.c_char_p, _I, _I, _I, _I, ctypes.c_float, _I, _I,
                                      ctypes.c_float, _P, _P, _I, _I, _P]
         lib.ref_obj_load.restype = _P
@@ -178,6 +180,22 @@ class Ref:
                                    u.ctypes.data, n, index.ctypes.data, pmf.ctypes.data,
                                    eval_pmf.ctypes.data)
         return index, pmf, eval_pmf
+
+    def render_aovs(self, tris, material_ids, materials, lights, camera, width, height, spp,
+                    max_depth, seed, light_sampler=1):
+        """The reference CPU tracer's film and debug images (shadow, ng, ns), each
+        height x width x 3 per-pixel sums, on a single-mesh scene."""
+        tris = np.ascontiguousarray(tris, np.float32)
+        mids = np.ascontiguousarray(material_ids, np.int32)
+        mats = np.ascontiguousarray(materials, np.float32)
+        lights = np.ascontiguousarray(lights, np.float32).reshape(-1, 7)
+        cam = np.ascontiguousarray(camera, np.float32)
+        out = [np.zeros((height, width, 3), np.float32) for _ in range(4)]
+        self.lib.ref_render_aovs(tris.ctypes.data, len(tris), mids.ctypes.data, mats.ctypes.data,
+                                 len(mats), lights.ctypes.data if len(lights) else None,
+                                 len(lights), cam.ctypes.data, width, height, spp, max_depth,
+                                 seed, light_sampler, *(o.ctypes.data for o in out))
+        return tuple(out)
 
     def obj_load(self, path, normal_mode=0, reverse=False, flip_v=False, scale_mode=0,
                  target_extent=1.0, center_xz=False, ground_to_y=False, target_y=0.0,

@@ -16,6 +16,7 @@
 //                                  app/render_runner.cpp:85-90)
 //   trace_path                     integrator/cpu_path_tracer.cpp:403-498
 //   make_render_sampler            integrator/render_context.h:45-54
+//   render_cpu_path_tracer (debug images) integrator/cpu_path_tracer.cpp:160-562
 //   load_obj_into_scene_with_result util/obj_loader.cpp:1296-1301
 //   make_stanford_bunny_scene, make_lux_cover_scene, make_stanford_dragon_scene
 //                                  scene/stanford_bunny.h, scene/lux_cover.h,
@@ -500,6 +501,45 @@ int ref_select_lights(const float* tris, int ntri, const int32_t* mids, const fl
         pmf[i] = picked.light_index >= 0 ? picked.pmf : 0.0f;
         eval_pmf[i] = picked.light_index >= 0 ? light_pmf(sampler, ctx, picked.light_index) : 0.0f;
     }
+    return 0;
+}
+
+// render_cpu_path_tracer with its debug images (CpuAovTargets,
+// integrator/cpu_path_tracer.cpp:160-397) on a single-mesh scene as ref_render_scene
+// builds it (seed = seed): film sums and the shadow / ng / ns images (any may be null),
+// width * height * 3 floats each.
+int ref_render_aovs(const float* tris, int ntri, const int32_t* mids, const float* mats,
+                    int nmat, const float* lights, int nlights, const float* cam, int width,
+                    int height, int spp, int max_depth, uint64_t seed, int light_sampler,
+                    float* film_out, float* shadow_out, float* ng_out, float* ns_out) {
+    Scene scene = build_single_mesh_scene(tris, ntri, mids, mats, nmat, lights, nlights, cam,
+                                          nullptr, 0, 0);
+    PreparedScene prepared(std::move(scene));
+    prepared.prepare_host_bvh();
+    RenderSettings settings;
+    settings.max_depth = max_depth;
+    settings.seed = seed;
+    settings.light_sampler_kind = sampler_kind(light_sampler);
+    Film film(width, height, spp), shadow(width, height, spp), ng(width, height, spp),
+        ns(width, height, spp);
+    RenderOutputs outputs;
+    outputs.set(RenderAov::ShadowDebug, shadow_out ? &shadow : nullptr);
+    outputs.set(RenderAov::GeometricNormal, ng_out ? &ng : nullptr);
+    outputs.set(RenderAov::ShadingNormal, ns_out ? &ns : nullptr);
+    render_cpu_path_tracer(prepared.host_scene(), prepared.host_bvh(), prepared.light_sampling(),
+                           film, settings, &outputs);
+    auto copy = [](const Film& f, float* out) {
+        if (!out) return;
+        for (size_t i = 0; i < f.pixels.size(); ++i) {
+            out[3 * i] = f.pixels[i].x;
+            out[3 * i + 1] = f.pixels[i].y;
+            out[3 * i + 2] = f.pixels[i].z;
+        }
+    };
+    copy(film, film_out);
+    copy(shadow, shadow_out);
+    copy(ng, ng_out);
+    copy(ns, ns_out);
     return 0;
 }
 

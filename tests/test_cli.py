@@ -35,7 +35,14 @@ def test_cli_reports_usage_and_rejects_like_the_reference(cli):
     assert _run(cli, "-depth", "-1").returncode == 1
     assert _run(cli, "-size", "8").returncode == 1          # missing operand
     assert _run(cli, "-light-sampler", "tree").returncode == 1  # parse_light_sampler_kind
-    assert _run(cli, "-debug-aov", "ng").returncode == 1
+    assert _run(cli, "-debug-aov", "ng,foo").returncode == 1      # parse_debug_aov_list
+    assert _run(cli, "-debug-mode", "path").returncode == 1       # a probe needs its pixel
+    assert _run(cli, "-debug-probe", "1", "2", "-debug-aov", "ng").returncode == 1
+    assert _run(cli, "a.ppm", "b.ppm").returncode == 1           # one positional, alone
+    for args in (["-debug-probe", "1", "2"], ["-debug-mesh", "winding"],
+                 ["-debug-aov", "orientation,ng"]):
+        r = _run(cli, *args)
+        assert r.returncode == 1 and "not supported" in r.stderr
 
 
 def _read_pfm(path):
@@ -116,3 +123,27 @@ def test_film_encoders_match_the_reference_writers(ctx, tmp_path):
     assert np.array_equal(pfm, want)
     assert lib.lux_film_encode(ctx.handle, film.ctypes.data, w, h, spp, 7,
                                pfm.ctypes.data) == lux_b200.LUX_ERR_INVALID_ARGUMENT
+
+
+@pytest.mark.gpu
+def test_cli_writes_debug_images(cli, ctx, tmp_path):
+    """`-debug-aov shadow,ng,ns` writes <prefix>_shadow / _ng / _ns next to the image (PFM
+    for a .pfm prefix, linear PPM otherwise), as the reference's runner names them; the
+    ng image is the per-sample mean lux_render_aovs gives for the same settings."""
+    from lux_b200 import scene as S
+    out = tmp_path / "c.pfm"
+    r = _run(cli, "-gpu", "-size", "24", "24", "-spp", "4", "-debug-aov", "shadow,ng,ns",
+             "-output", str(out))
+    assert r.returncode == 0, r.stderr
+    for name in ("shadow", "ng", "ns"):
+        assert (tmp_path / f"c_{name}.pfm").exists() and f"c_{name}.pfm" in r.stdout
+    ng = _read_pfm(tmp_path / "c_ng.pfm")
+    sc = S.Scene(ctx, S.make_cornell_scene(24, 24))
+    _, _, want, _ = S.render_aovs(ctx, sc, S.request(24, 24, 4, 4, 0), shadow=False, ns=False)
+    assert np.allclose(ng, want / 4, rtol=1e-5, atol=1e-6)
+    prefix = tmp_path / "dbg" / "x.ppm"
+    r = _run(cli, "-gpu", "-size", "16", "16", "-spp", "2", "-debug-aov", "ng",
+             "-debug-output", str(prefix), "-output", str(tmp_path / "b.ppm"))
+    assert r.returncode == 0, r.stderr
+    data = (tmp_path / "dbg" / "x_ng.ppm").read_bytes()
+    assert data.startswith(b"P6\n16 16\n255\n") and len(data) == 13 + 16 * 16 * 3
