@@ -260,8 +260,12 @@ int lux_overlap_cross(lux_ctx* ctx, const lux_bvh* left, const lux_bvh* right,
 
 typedef struct lux_scene lux_scene;
 
-/* Material (material/material.h:29-40; constant emission).  type: 0 Lambert,
- * 1 thin Lambert, 2 GGX, 3 dielectric, 4 interface (null), 5 transparent (tinted filter). */
+/* Material (material/material.h:29-40).  type: 0 Lambert, 1 thin Lambert, 2 GGX,
+ * 3 dielectric, 4 interface (null), 5 transparent (tinted filter).  emission_source 0
+ * is constant emission; 1 (EmissionSourceKind::Image, Material::image_emissive) reads the
+ * emission from scene image emission_image (lux_scene_desc.images) at the surface's
+ * texture coordinates, nearest texel, wrapped, times emission_scale (the reference's
+ * default scale is 1, 1, 1). */
 typedef struct lux_material {
     int32_t type;
     float albedo[3];
@@ -270,6 +274,9 @@ typedef struct lux_material {
     float roughness;
     float metallic;
     float eta;
+    int32_t emission_source;
+    int32_t emission_image;
+    float emission_scale[3];
 } lux_material;
 
 /* Indexed triangle mesh in object space (scene/scene_data.h:36-44).  normals and uvs

@@ -83,7 +83,7 @@ enum MaterialType : int {
     kTransparent = 5,
 };
 
-struct Material {  // material/material.h:29-40 (constant emission only)
+struct Material {  // material/material.h:29-40
     int type;
     f3 albedo;
     f3 emission;
@@ -91,6 +91,8 @@ struct Material {  // material/material.h:29-40 (constant emission only)
     float roughness;
     float metallic;
     float eta;
+    int emission_image;   // image emission: scene image index; -1 constant emission
+    f3 emission_scale;
 };
 
 LUX_HD bool is_scattering(const Material& m) {  // material/material.h:110-120
@@ -154,6 +156,14 @@ struct Light {  // light/light.h:86-93 for the kinds this path supports
     float area;
     f3 emission;           // area emission / point intensity / radiance / image scale
     f3 vec;                // point position / distant direction to light
+    int image;             // area light with image emission: scene image index, else -1
+    f3 image_scale;
+};
+
+// A scene image (SceneImageLightAsset pixels): RGB texels, row-major.
+struct ImageView {
+    const float* pixels;
+    int width, height;
 };
 
 // Image infinite light (ImageInfiniteLight, light/light.h:79-87): latitude-longitude
@@ -201,6 +211,7 @@ struct SceneView {
     const Light* lights;
     int light_count;
     const EnvLight* env;             // image infinite lights, by Light::primitive
+    const ImageView* images;         // scene images, for image emission
     float total_light_power;
     const AliasEntry* light_alias;   // power alias table, light_count entries
     int light_sampler;               // 0 uniform, 1 power

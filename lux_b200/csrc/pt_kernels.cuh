@@ -742,6 +742,36 @@ LUX_D LightLi env_sample(const EnvLight& e, float select_u, float ux, float uy) 
     return li;
 }
 
+// ------------------------------------------------------------------ image emission
+// image_asset_lookup_nearest (scene/scene_data.h:164-173): the texel under the wrapped
+// texture coordinates, times scale.
+LUX_D f3 image_lookup(const SceneView& sc, int image, float tu, float tv, f3 scale) {
+    if (!sc.images || image < 0) return splat(0);
+    const ImageView im = sc.images[image];
+    if (!im.pixels || im.width <= 0 || im.height <= 0) return splat(0);
+    const float u = sub(tu, floorf(tu));
+    const float v = sub(tv, floorf(tv));
+    const int x = static_cast<int>(fminf(static_cast<float>(im.width - 1), floorf(mul(u, static_cast<float>(im.width)))));
+    const int y = static_cast<int>(fminf(static_cast<float>(im.height - 1), floorf(mul(v, static_cast<float>(im.height)))));
+    const float* p = im.pixels + 3 * (static_cast<size_t>(y) * im.width + x);
+    return make_f3(mul(p[0], scale.x), mul(p[1], scale.y), mul(p[2], scale.z));
+}
+
+// interpolate_triangle_uv (scene/scene_data.h:230-233) at barycentrics (u, v).
+LUX_D void triangle_uv(const SceneTriShading& sh, float u, float v, float& tu, float& tv) {
+    const float w = sub(sub(1.0f, u), v);
+    tu = add(add(mul(w, sh.n0.w), mul(u, sh.n2.w)), mul(v, sh.uv.y));
+    tv = add(add(mul(w, sh.n1.w), mul(u, sh.uv.x)), mul(v, sh.uv.z));
+}
+
+// gpu_diffuse_area_light_emission_value (gpu_scene_light_sampler.cuh:216-223).
+LUX_D f3 area_light_emission(const SceneView& sc, const Light& L, int prim, float u, float v) {
+    if (L.image < 0) return L.emission;
+    float tu, tv;
+    triangle_uv(sc.shading[prim], u, v, tu, tv);
+    return image_lookup(sc, L.image, tu, tv, L.image_scale);
+}
+
 // sample_light_li (scene/scene_light_sampler.h:212-265 / gpu_scene_light_sampler.cuh:133-193).
 LUX_D LightLi sample_light(const SceneView& sc, int sampler, f3 p, float select_u, float comp_u, float ux,
                            float uy) {
@@ -762,7 +792,10 @@ LUX_D LightLi sample_light(const SceneView& sc, int sampler, f3 p, float select_
         li.distance = sqrtf(d2);
         li.wi = vdiv(to, li.distance);
         li.position = pos;
-        li.radiance = eval_emission(L.emission, L.two_sided, n, -li.wi);
+        // sample_triangle_barycentric_uv (light/light_sampler.h:369-374) for the texel.
+        const float s0 = sqrtf(ux);
+        const f3 le = area_light_emission(sc, L, L.primitive, mul(s0, sub(1.0f, uy)), mul(s0, uy));
+        li.radiance = eval_emission(le, L.two_sided, n, -li.wi);
         li.pdf = mul(pmf, solid_angle_pdf(pos, n, L.two_sided, pdf_area, p));
         li.measure = kMeasureSolidAngle;
         li.valid = max_component(li.radiance) > 0 && li.pdf > 0;
@@ -908,12 +941,19 @@ LUX_D int material_class(int type) {
 }
 
 // Emission seen at a hit (surface_light_le + area_light_pdf_solid_angle,
-// scene/scene_light_sampler.h:318-465), constant emission.
-LUX_D f3 surface_le(const SceneView& sc, int prim, const Material& m, f3 ng, f3 wo) {
+// scene/scene_light_sampler.h:318-465) at barycentrics (u, v).
+LUX_D f3 surface_le(const SceneView& sc, int prim, const Material& m, f3 ng, f3 wo, float u,
+                    float v) {
     int li = sc.primitive_light[prim];
     if (li >= 0 && li < sc.light_count && sc.lights[li].kind == 0) {
         const Light& L = sc.lights[li];
-        return eval_emission(L.emission, L.two_sided, ng, wo);
+        return eval_emission(area_light_emission(sc, L, prim, u, v), L.two_sided, ng, wo);
+    }
+    if (m.emission_image >= 0) {  // gpu_eval_emission of an image-emissive material
+        float tu, tv;
+        triangle_uv(sc.shading[prim], u, v, tu, tv);
+        return eval_emission(image_lookup(sc, m.emission_image, tu, tv, m.emission_scale),
+                             m.two_sided, ng, wo);
     }
     if (max_component(m.emission) <= 0) return splat(0);
     return eval_emission(m.emission, m.two_sided, ng, wo);
@@ -1225,7 +1265,7 @@ LUX_D ShadeOut shade_path(const PathPool& rt, const SceneView& sc, int sampler, 
     f3 ng = triangle_normal(v0, v1, v2);
     f3 wo = -rd;
     // Emission with MIS (cpu_path_tracer.cpp:434-447).
-    f3 le = surface_le(sc, prim, m, ng, wo);
+    f3 le = surface_le(sc, prim, m, ng, wo, hu, hv);
     if (max_component(le) > 0) {
         if (s.depth == 0 || is_delta(s.flags)) {
             add_radiance(rt, p, s.thr * le);

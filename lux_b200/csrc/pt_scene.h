@@ -43,6 +43,8 @@ struct lux_scene {
     float* env_pixels = nullptr;        // image-light texels (device)
     float* env_cdf = nullptr;           // image-light running weights (device)
     lux::pt::EnvLight* d_env = nullptr; // image lights (device)
+    float* image_pixels = nullptr;      // images read by image-emissive materials (device)
+    lux::pt::ImageView* d_images = nullptr;  // every scene image (null pixels if unread)
     // Light tree and the table of the lights outside it (device; null without a tree).
     lux::pt::LightNode* light_tree = nullptr;
     int* light_leaf = nullptr;
@@ -64,6 +66,9 @@ struct lux_scene {
         int triangle, instance, local;   // scene triangle, its instance and local index
         int two_sided;
         float emission[3];
+        int image;                       // image emission: scene image, else -1
+        float image_scale[3];
+        float power_hint;                // scene_material_emission_power_hint
         float w[9];                      // world positions of the three corners
     };
     std::vector<EmissiveTri> emissive;             // emissive scene triangles, scene order

@@ -306,12 +306,13 @@ LightTables make_light_tables(const std::vector<lux_scene::EmissiveTri>& emissiv
         l.area = area;
         l.emission = make_f3(e.emission[0], e.emission[1], e.emission[2]);
         l.vec = make_f3(0, 0, 0);
+        l.image = e.image;
+        l.image_scale = make_f3(e.image_scale[0], e.image_scale[1], e.image_scale[2]);
         Box box;
         box.expand(a);
         box.expand(b);
         box.expand(c);
-        const float p = area * std::fmax(1e-6f, luminance(v3(e.emission[0], e.emission[1],
-                                                             e.emission[2])));
+        const float p = area * std::fmax(1e-6f, e.power_hint);
         const int index = append(l, p, box);
         if (index >= 0) {
             int& stored = t.primitive_light[e.triangle];
@@ -434,11 +435,30 @@ Material to_material(const lux_material& m) {
     r.roughness = m.roughness;
     r.metallic = m.metallic;
     r.eta = m.eta;
+    r.emission_image = m.emission_source == 1 ? m.emission_image : -1;
+    r.emission_scale = make_f3(m.emission_scale[0], m.emission_scale[1], m.emission_scale[2]);
     return r;
 }
 
+// Material::is_emissive (material/material.h:104-108).
 bool is_emissive(const lux_material& m) {
-    return std::fmax(m.emission[0], std::fmax(m.emission[1], m.emission[2])) > 0;
+    return std::fmax(m.emission[0], std::fmax(m.emission[1], m.emission[2])) > 0 ||
+           (m.emission_source == 1 && m.emission_image >= 0);
+}
+
+// scene_material_emission_power_hint (scene/scene_data.h:189-205): the luminance of the
+// emission, or the mean luminance of the scaled texels of an emission image.
+float emission_power_hint(const lux_scene_desc* d, const lux_material& m) {
+    if (m.emission_source != 1) return luminance(v3(m.emission[0], m.emission[1], m.emission[2]));
+    const lux_env_image& im = d->images[m.emission_image];
+    const size_t count = size_t(im.width) * size_t(im.height);
+    float sum = 0;
+    for (size_t i = 0; i < count; ++i) {
+        const float* p = im.pixels + 3 * i;
+        sum += luminance(v3(p[0] * m.emission_scale[0], p[1] * m.emission_scale[1],
+                            p[2] * m.emission_scale[2]));
+    }
+    return sum / static_cast<float>(count);
 }
 
 // ---- device-side preparation
@@ -552,7 +572,8 @@ void scene_free(lux_scene* s) {
                     s->blas_views, s->lights, s->light_alias, s->primitive_light, s->tri_soup,
                     s->tlas_boxes, s->env_pixels, s->env_cdf, s->d_env, s->light_tree,
                     s->mesh_data.vertices, s->mesh_data.normals, s->mesh_data.uvs,
-                    s->mesh_data.indices, s->mesh_data.material_ids,
+                    s->mesh_data.indices, s->mesh_data.material_ids, s->image_pixels,
+                    s->d_images,
                     s->light_leaf, s->light_other_slot, s->other_lights, s->other_alias};
     for (void* p : ptrs)
         if (p) cudaFree(p);
@@ -577,9 +598,22 @@ int scene_create(lux_ctx* ctx, const lux_scene_desc* d, lux_scene** out) {
             if (m.material_ids[t] < 0 || m.material_ids[t] >= d->material_count)
                 return fail(LUX_ERR_INVALID_ARGUMENT, "material id out of range");
     }
-    for (int i = 0; i < d->material_count; ++i)
+    for (int i = 0; i < d->material_count; ++i) {
         if (d->materials[i].type < 0 || d->materials[i].type > 5)
             return fail(LUX_ERR_INVALID_ARGUMENT, "unknown material type");
+        const lux_material& m = d->materials[i];
+        if (m.emission_source < 0 || m.emission_source > 1)
+            return fail(LUX_ERR_INVALID_ARGUMENT, "unknown emission source");
+        if (m.emission_source == 1 &&
+            (m.emission_image < 0 || m.emission_image >= d->image_count || !d->images))
+            return fail(LUX_ERR_INVALID_ARGUMENT, "image emission without a valid image");
+    }
+    for (int i = 0; i < d->image_count; ++i) {
+        const lux_env_image& e = d->images[i];
+        if (!e.pixels || e.width <= 0 || e.height <= 0 ||
+            static_cast<long long>(e.width) * e.height > (1ll << 26))
+            return fail(LUX_ERR_INVALID_ARGUMENT, "bad scene image");
+    }
     for (int i = 0; i < d->instance_count; ++i) {
         const lux_instance_desc& in = d->instances[i];
         if (in.mesh < 0 || in.mesh >= d->mesh_count)
@@ -633,6 +667,9 @@ int scene_create(lux_ctx* ctx, const lux_scene_desc* d, lux_scene** out) {
     // in scene order with their world corners (the device preparation's arithmetic),
     // then the explicit lights; kept so that vertex updates re-derive the tables.  Only
     // emissive triangles are visited: each mesh lists its emissive local triangles once.
+    std::vector<float> power_hints(d->material_count, 0.0f);
+    for (int i = 0; i < d->material_count; ++i)
+        if (is_emissive(d->materials[i])) power_hints[i] = emission_power_hint(d, d->materials[i]);
     std::vector<std::vector<int>> mesh_emissive_tris(d->mesh_count);
     for (int m = 0; m < d->mesh_count; ++m)
         for (int t = 0; t < d->meshes[m].triangle_count; ++t)
@@ -658,6 +695,9 @@ int scene_create(lux_ctx* ctx, const lux_scene_desc* d, lux_scene** out) {
             e.local = t;
             e.two_sided = mat.emission_two_sided ? 1 : 0;
             for (int k = 0; k < 3; ++k) e.emission[k] = mat.emission[k];
+            e.image = mat.emission_source == 1 ? mat.emission_image : -1;
+            for (int k = 0; k < 3; ++k) e.image_scale[k] = mat.emission_scale[k];
+            e.power_hint = power_hints[ov >= 0 ? ov : mesh.material_ids[t]];
             for (int k = 0; k < 3; ++k) {
                 const float* q = mesh.vertices + 3 * size_t(mesh.indices[3 * size_t(t) + k]);
                 const V3 w = transform_point(s->instances[i].m, v3(q[0], q[1], q[2]));
@@ -686,6 +726,8 @@ int scene_create(lux_ctx* ctx, const lux_scene_desc* d, lux_scene** out) {
         V3 vec = v3(ld.vec[0], ld.vec[1], ld.vec[2]);
         if (ld.kind == 2) vec = normalize3(vec);  // add_distant_light stores it normalised
         l.vec = make_f3(vec.x, vec.y, vec.z);
+        l.image = -1;
+        l.image_scale = make_f3(0, 0, 0);
         float power = std::fmax(1e-6f, luminance(v3(ld.value[0], ld.value[1], ld.value[2])));
         if (ld.kind == 4) {
             const lux_env_image& im = d->images[ld.image];
@@ -734,6 +776,28 @@ int scene_create(lux_ctx* ctx, const lux_scene_desc* d, lux_scene** out) {
         if (!st) st = upload(&s->d_env, env, ctx->stream);
     }
     if (!st) st = upload_light_tables(ctx, s, lt);
+    // Scene images read by image-emissive materials; the table holds every image (the
+    // others with no texels).
+    if (!st && d->image_count > 0) {
+        std::vector<char> read(d->image_count, 0);
+        for (int i = 0; i < d->material_count; ++i)
+            if (d->materials[i].emission_source == 1) read[d->materials[i].emission_image] = 1;
+        std::vector<float> texels;
+        std::vector<size_t> offset(d->image_count, 0);
+        std::vector<pt::ImageView> views(d->image_count, pt::ImageView{nullptr, 0, 0});
+        for (int i = 0; i < d->image_count; ++i) {
+            if (!read[i]) continue;
+            const lux_env_image& im = d->images[i];
+            offset[i] = texels.size();
+            texels.insert(texels.end(), im.pixels, im.pixels + 3 * size_t(im.width) * im.height);
+            views[i].width = im.width;
+            views[i].height = im.height;
+        }
+        st = upload(&s->image_pixels, texels, ctx->stream);
+        for (int i = 0; i < d->image_count; ++i)
+            if (read[i]) views[i].pixels = s->image_pixels + offset[i];
+        if (!st) st = upload(&s->d_images, views, ctx->stream);
+    }
 
     // Mesh data to the device, meshes concatenated (the caller's arrays are copied in
     // stream order; pageable sources are staged before each call returns).
@@ -858,6 +922,7 @@ int scene_create(lux_ctx* ctx, const lux_scene_desc* d, lux_scene** out) {
     v.tlas_instance = s->tlas_instance;
     v.blas = s->blas_views;
     v.env = s->d_env;
+    v.images = s->d_images;
     set_light_view(s, lt);
     v.has_two_level = s->tlas->n > 0 && d->instance_count > 0;
     v.has_passthrough = false;

@@ -26,7 +26,9 @@ _F12 = ctypes.c_float * 12
 class Material(ctypes.Structure):
     _fields_ = [("type", ctypes.c_int32), ("albedo", _F3), ("emission", _F3),
                 ("emission_two_sided", ctypes.c_int32), ("roughness", ctypes.c_float),
-                ("metallic", ctypes.c_float), ("eta", ctypes.c_float)]
+                ("metallic", ctypes.c_float), ("eta", ctypes.c_float),
+                ("emission_source", ctypes.c_int32), ("emission_image", ctypes.c_int32),
+                ("emission_scale", _F3)]
 
 
 class MeshDesc(ctypes.Structure):
@@ -91,6 +93,16 @@ def ggx(albedo, roughness, metallic=0.0):
 
 def dielectric(albedo=(1, 1, 1), eta=1.5):
     return material(DIELECTRIC, albedo, roughness=0.0, metallic=0.0, eta=eta)
+
+
+def image_emissive(image, scale=(1, 1, 1), albedo=(0, 0, 0), two_sided=False):
+    """Material::image_emissive: emission read from scene image `image` at the surface's
+    texture coordinates (nearest texel), times scale."""
+    m = material(LAMBERT, albedo, (0, 0, 0), two_sided=two_sided)
+    m.emission_source = 1
+    m.emission_image = image
+    m.emission_scale = _F3(*scale)
+    return m
 
 
 def tinted_filter(transmittance=(1, 1, 1)):
@@ -159,6 +171,24 @@ class SceneBuilder:
 
     def add_uniform_infinite_light(self, radiance):
         self.lights.append(LightDesc(LIGHT_UNIFORM_INFINITE, _F3(0, 0, 0), _F3(*radiance)))
+
+    def add_image(self, pixels) -> int:
+        """A scene image (height, width, 3) for image emission; returns its index."""
+        self.images.append(np.ascontiguousarray(pixels, np.float32))
+        return len(self.images) - 1
+
+    def world_uvs(self) -> np.ndarray:
+        """Corner texture coordinates of each scene triangle (6 floats), in
+        world_triangles order; zero for meshes without them."""
+        out = []
+        for mesh_id, _, _ in self.instances:
+            mesh = self.default_mesh() if mesh_id == self._default_mesh else self.meshes[mesh_id]
+            if mesh.uvs is None:
+                out.append(np.zeros((len(mesh.indices), 6), np.float32))
+            else:
+                uv = np.asarray(mesh.uvs, np.float32)
+                out.append(uv[np.asarray(mesh.indices).reshape(-1)].reshape(-1, 6))
+        return np.concatenate(out) if out else np.zeros((0, 6), np.float32)
 
     def add_image_infinite_light(self, pixels, scale=(1.0, 1.0, 1.0)):
         """add_image_infinite_light (scene/scene_build.h:67-89): pixels is an

@@ -115,7 +115,8 @@ class Ref:
         lib.ref_cornell_render.argtypes = [_I, _I, _I, _I, ctypes.c_uint64, _I, _I, _I,
                                            _P, _P, _P]
         lib.ref_render_scene.argtypes = [_P, _I, _P, _P, _I, _P, _I, _P, _I, _I, _I, _I,
-                                         ctypes.c_uint64, _I, _I, _I, _I, _P, _P, _I, _I]
+                                         ctypes.c_uint64, _I, _I, _I, _I, _P, _P, _I, _I,
+                                         _P, _P]
         lib.ref_select_lights.argtypes = [_P, _I, _P, _P, _I, _P, _I, _P, _I, _P, _P, _I,
                                           _P, _P, _P]
         lib.ref_render_aovs.argtypes = [_P, _I, _P, _P, _I, _P, _I, _P, _I, _I, _I, _I,
@@ -136,11 +137,14 @@ class Ref:
         self.lib = lib
 
     def render_scene(self, tris, material_ids, materials, lights, camera, width, height, spp,
-                     max_depth, seed, light_sampler=1, rows=None, threads=1, env_image=None):
+                     max_depth, seed, light_sampler=1, rows=None, threads=1, env_image=None,
+                     material_ext=None, uvs=None):
         """Per-sample radiance [pixel][spp][3] of a single-mesh scene (see ref_harness.cpp).
 
         materials: N x 11 (type, albedo3, emission3, roughness, metallic, eta, two_sided);
-        lights: L x 7 (kind, vec3, value3); camera: origin3, look_at3, vfov, aspect.
+        lights: L x 7 (kind, vec3, value3); camera: origin3, look_at3, vfov, aspect;
+        material_ext: N x 5 (emission source, image, scale3); uvs: T x 6 corner texcoords;
+        env_image: scene image 0 (also the image light's, if there is one).
         """
         tris = np.ascontiguousarray(tris, np.float32)
         mids = np.ascontiguousarray(material_ids, np.int32)
@@ -150,13 +154,17 @@ class Ref:
         y0, y1 = rows if rows is not None else (0, height)
         out = np.zeros(((y1 - y0) * width, spp, 3), np.float32)
         env = None if env_image is None else np.ascontiguousarray(env_image, np.float32)
+        ext = None if material_ext is None else np.ascontiguousarray(material_ext, np.float32)
+        tuv = None if uvs is None else np.ascontiguousarray(uvs, np.float32)
         self.lib.ref_render_scene(tris.ctypes.data, len(tris), mids.ctypes.data, mats.ctypes.data,
                                   len(mats), lights.ctypes.data if len(lights) else None,
                                   len(lights), cam.ctypes.data, width, height, spp, max_depth,
                                   seed, light_sampler, y0, y1, threads, out.ctypes.data,
                                   None if env is None else env.ctypes.data,
                                   0 if env is None else env.shape[1],
-                                  0 if env is None else env.shape[0])
+                                  0 if env is None else env.shape[0],
+                                  None if ext is None else ext.ctypes.data,
+                                  None if tuv is None else tuv.ctypes.data)
         return out
 
     def select_lights(self, tris, material_ids, materials, lights, camera, light_sampler,

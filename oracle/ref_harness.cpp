@@ -383,10 +383,15 @@ int ref_cornell_render(int width, int height, int spp, int max_depth, uint64_t s
 // lights as 7 floats (kind 1 point / 2 distant / 3 uniform infinite, vec3, value3);
 // camera: origin3, look_at3, vertical fov degrees, aspect (make_pinhole_camera).
 // samples receives [pixel][spp][3] for rows [y0, y1).
+// mat_ext (optional): 5 floats per material, emission source (1 image), image index and
+// emission scale rgb.  uvs (optional): 6 floats per triangle, the corners' texture
+// coordinates.  With env_pixels and no image light, the image still becomes scene image 0.
 static Scene build_single_mesh_scene(const float* tris, int ntri, const int32_t* mids,
                                      const float* mats, int nmat, const float* lights,
                                      int nlights, const float* cam, const float* env_pixels,
-                                     int env_width, int env_height) {
+                                     int env_width, int env_height,
+                                     const float* mat_ext = nullptr,
+                                     const float* uvs = nullptr) {
     Scene scene;
     for (int m = 0; m < nmat; ++m) {
         const float* f = mats + size_t(m) * 11;
@@ -395,6 +400,12 @@ static Scene build_single_mesh_scene(const float* tris, int ntri, const int32_t*
                                            f[8], f[9],
                                            f[10] != 0 ? EmissionSidedness::DoubleSided
                                                       : EmissionSidedness::SingleSided));
+        if (mat_ext && mat_ext[5 * m] == 1.0f) {  // Material::image_emissive
+            Material& mm = scene.materials.back();
+            mm.emission_source = EmissionSourceKind::Image;
+            mm.emission_image_id = static_cast<int>(mat_ext[5 * m + 1]);
+            mm.emission_scale = vec3(mat_ext[5 * m + 2], mat_ext[5 * m + 3], mat_ext[5 * m + 4]);
+        }
     }
     // One append_indexed_mesh (scene/scene_edit.h:98-163) instead of add_triangle per
     // triangle: the same default-mesh data (three vertices per triangle, zero normals and
@@ -402,9 +413,12 @@ static Scene build_single_mesh_scene(const float* tris, int ntri, const int32_t*
     // quadratic in the triangle count.
     {
         std::vector<vec3> vertices;
+        std::vector<vec2> corner_uvs;
         std::vector<TriangleIndices> indices;
         std::vector<int> material_ids(mids, mids + ntri);
         vertices.reserve(size_t(ntri) * 3);
+        if (uvs)
+            for (int k = 0; k < 3 * ntri; ++k) corner_uvs.push_back(vec2(uvs[2 * k], uvs[2 * k + 1]));
         indices.reserve(ntri);
         for (int t = 0; t < ntri; ++t) {
             const float* v = tris + size_t(t) * 9;
@@ -414,7 +428,7 @@ static Scene build_single_mesh_scene(const float* tris, int ntri, const int32_t*
             vertices.push_back(vec3(v[6], v[7], v[8]));
             indices.push_back(TriangleIndices{first, first + 1, first + 2});
         }
-        if (ntri > 0) append_indexed_mesh(scene, vertices, {}, {}, indices, material_ids);
+        if (ntri > 0) append_indexed_mesh(scene, vertices, {}, corner_uvs, indices, material_ids);
     }
     for (int l = 0; l < nlights; ++l) {
         const float* f = lights + size_t(l) * 7;
@@ -428,6 +442,12 @@ static Scene build_single_mesh_scene(const float* tris, int ntri, const int32_t*
                 px[k] = vec3(env_pixels[3 * k], env_pixels[3 * k + 1], env_pixels[3 * k + 2]);
             add_image_infinite_light(scene, px, env_width, env_height, vec3(f[4], f[5], f[6]));
         }
+    }
+    if (env_pixels && scene.image_light_assets.empty()) {
+        std::vector<vec3> px(static_cast<size_t>(env_width) * env_height);
+        for (size_t k = 0; k < px.size(); ++k)
+            px[k] = vec3(env_pixels[3 * k], env_pixels[3 * k + 1], env_pixels[3 * k + 2]);
+        scene.image_light_assets.push_back(make_image_light_asset(px, env_width, env_height, vec3(1)));
     }
     scene.camera = make_pinhole_camera(vec3(cam[0], cam[1], cam[2]), vec3(cam[3], cam[4], cam[5]),
                                        cam[6], cam[7]);
@@ -444,9 +464,9 @@ int ref_render_scene(const float* tris, int ntri, const int32_t* mids, const flo
                      const float* lights, int nlights, const float* cam, int width, int height,
                      int spp, int max_depth, uint64_t seed, int light_sampler, int y0, int y1,
                      int threads, float* samples, const float* env_pixels, int env_width,
-                     int env_height) {
+                     int env_height, const float* mat_ext, const float* uvs) {
     Scene scene = build_single_mesh_scene(tris, ntri, mids, mats, nmat, lights, nlights, cam,
-                                          env_pixels, env_width, env_height);
+                                          env_pixels, env_width, env_height, mat_ext, uvs);
     PreparedScene prepared(std::move(scene));
     prepared.prepare_host_bvh();
     SceneLightSampler lights_sampler = make_scene_light_sampler(
