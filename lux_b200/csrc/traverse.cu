@@ -320,10 +320,12 @@ __global__ void __launch_bounds__(kTraceThreads) k_trace_persistent(
 // Persistent warps with refill (as k_trace_persistent) over the 4-wide nodes: a step is
 // one wide-node fetch (four child boxes) or one triangle test, followed by the pops it
 // enables.  Decisions are those of wide_walk, step for step.
-// 8 resident blocks per SM (at most 64 registers): occupancy hides the node-load latency
-// that bounds this kernel, and the cap costs no spills.
+// 10 resident blocks per SM (at most 48 registers): occupancy hides the node-load
+// latency that bounds this kernel.  The cap spills 44 bytes per thread, and the extra
+// warps still win: 468 against 439 Mrays/s at 64 registers and 425 at 40 (1,048,576
+// triangles, 4,194,304 rays, B200).
 template <bool AnyHit>
-__global__ void __launch_bounds__(kTraceThreads, 8) k_trace_wide_persistent(
+__global__ void __launch_bounds__(kTraceThreads, 10) k_trace_wide_persistent(
         BvhView bvh, const float4* rays, int nrays, int* hit_id, float* hit_t,
         unsigned* ray_counter, int budget, int* error) {
     const unsigned lane = threadIdx.x & 31;
