@@ -91,8 +91,7 @@ LUX_D bool wide_walk(const BvhView& b, const slab_ray& sr, float& best_t, int* e
     float tn0;
     if (!slab_hit(sr, load_root(b.root), best_t, tn0)) return true;
     const octant_ray orr = make_octant_ray(sr);
-    int stack_h[kWideStack];
-    float stack_t[kWideStack];
+    int2 stack[kWideStack];  // (node ref, entry t bits)
     int sp = 0;
     int cur = b.n == 1 ? ~0 : 0;
     const long long bound = 2ll * b.n + 64;
@@ -115,8 +114,7 @@ LUX_D bool wide_walk(const BvhView& b, const slab_ray& sr, float& best_t, int* e
 #pragma unroll
                 for (int c = 3; c >= 1; --c) {
                     if (c > f && ((m >> c) & 1u)) {
-                        stack_h[sp] = wide_ref(w, c);
-                        stack_t[sp] = t[c];
+                        stack[sp] = make_int2(wide_ref(w, c), __float_as_int(t[c]));
                         ++sp;
                     }
                 }
@@ -130,8 +128,9 @@ LUX_D bool wide_walk(const BvhView& b, const slab_ray& sr, float& best_t, int* e
             bool resumed = false;
             while (sp > 0) {
                 --sp;
-                if (!(stack_t[sp] > best_t)) {
-                    cur = stack_h[sp];
+                const int2 e = stack[sp];
+                if (!(__int_as_float(e.y) > best_t)) {
+                    cur = e.x;
                     resumed = true;
                     break;
                 }
