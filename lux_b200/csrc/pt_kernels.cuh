@@ -100,8 +100,7 @@ LUX_D int blas_closest(const BvhView& b, f3 o, f3 d, float tmin, float& best_t, 
     slab_ray sr = make_slab_ray(r);
     float tn;
     if (!slab_hit(sr, load_root(b.root), best_t, tn)) return -1;
-    int stack_h[kStack];
-    float stack_t[kStack];
+    int2 stack[kStack];  // (node ref, entry t bits): one 8-byte access per entry
     int sp = 0;
     int cur = b.n == 1 ? ~0 : 0;
     int best = -1;
@@ -123,8 +122,7 @@ LUX_D int blas_closest(const BvhView& b, f3 o, f3 d, float tmin, float& best_t, 
                         atomicOr(error, kErrStackOverflow);
                         return -1;
                     }
-                    stack_h[sp] = nd.ch.y;
-                    stack_t[sp] = tr;
+                    stack[sp] = make_int2(nd.ch.y, __float_as_int(tr));
                     ++sp;
                 }
                 cur = nd.ch.x;
@@ -154,8 +152,9 @@ LUX_D int blas_closest(const BvhView& b, f3 o, f3 d, float tmin, float& best_t, 
             bool resumed = false;
             while (sp > 0) {
                 --sp;
-                if (!(stack_t[sp] > best_t)) {
-                    cur = stack_h[sp];
+                const int2 e = stack[sp];
+                if (!(__int_as_float(e.y) > best_t)) {
+                    cur = e.x;
                     resumed = true;
                     break;
                 }
@@ -187,8 +186,7 @@ LUX_D SceneHit scene_closest(const SceneView& sc, f3 o, f3 d, float tmin, float 
         ign_instance = __float_as_int(v1.w);
         ign_local = __float_as_int(v2.w);
     }
-    int stack_h[kStack];
-    float stack_t[kStack];
+    int2 stack[kStack];  // (node ref, entry t bits): one 8-byte access per entry
     int sp = 0;
     int cur = tl.n == 1 ? ~0 : 0;
     const long long bound = 2ll * tl.n + 64;
@@ -209,8 +207,7 @@ LUX_D SceneHit scene_closest(const SceneView& sc, f3 o, f3 d, float tmin, float 
                         atomicOr(error, kErrStackOverflow);
                         return SceneHit{-1, tmax, 0, 0};
                     }
-                    stack_h[sp] = nd.ch.y;
-                    stack_t[sp] = b;
+                    stack[sp] = make_int2(nd.ch.y, __float_as_int(b));
                     ++sp;
                 }
                 cur = nd.ch.x;
@@ -239,8 +236,9 @@ LUX_D SceneHit scene_closest(const SceneView& sc, f3 o, f3 d, float tmin, float 
             bool resumed = false;
             while (sp > 0) {
                 --sp;
-                if (!(stack_t[sp] > h.t)) {
-                    cur = stack_h[sp];
+                const int2 e = stack[sp];
+                if (!(__int_as_float(e.y) > h.t)) {
+                    cur = e.x;
                     resumed = true;
                     break;
                 }
@@ -256,11 +254,9 @@ LUX_D SceneHit scene_closest(const SceneView& sc, f3 o, f3 d, float tmin, float 
 // walks per warp and refill lanes as walks finish.  The decisions, in order, are those
 // of scene_closest / blas_closest above, so the result is the same.  The four stacks
 // live apart from the scalar state, which then stays in registers.
-struct WalkStacks {
-    int t_h[kStack];
-    float t_t[kStack];
-    int b_h[kStack];
-    float b_t[kStack];
+struct WalkStacks {  // deferred (node ref, entry t bits), TLAS and BLAS
+    int2 t[kStack];
+    int2 b[kStack];
 };
 
 struct TwoLevelWalk {
@@ -320,8 +316,9 @@ struct TwoLevelWalk {
     LUX_D bool pop_tlas(const WalkStacks& k) {
         while (t_sp > 0) {
             --t_sp;
-            if (!(k.t_t[t_sp] > hit.t)) {
-                t_cur = k.t_h[t_sp];
+            const int2 e = k.t[t_sp];
+            if (!(__int_as_float(e.y) > hit.t)) {
+                t_cur = e.x;
                 return true;
             }
         }
@@ -330,8 +327,9 @@ struct TwoLevelWalk {
     LUX_D bool pop_blas(const WalkStacks& k) {
         while (b_sp > 0) {
             --b_sp;
-            if (!(k.b_t[b_sp] > hit.t)) {
-                b_cur = k.b_h[b_sp];
+            const int2 e = k.b[b_sp];
+            if (!(__int_as_float(e.y) > hit.t)) {
+                b_cur = e.x;
                 return true;
             }
         }
@@ -359,8 +357,7 @@ struct TwoLevelWalk {
                             fail(error, kErrStackOverflow, INFINITY);
                             return true;
                         }
-                        k.b_h[b_sp] = nd.ch.y;
-                        k.b_t[b_sp] = tr_;
+                        k.b[b_sp] = make_int2(nd.ch.y, __float_as_int(tr_));
                         ++b_sp;
                     }
                     b_cur = nd.ch.x;
@@ -412,8 +409,7 @@ struct TwoLevelWalk {
                         fail(error, kErrStackOverflow, INFINITY);
                         return true;
                     }
-                    k.t_h[t_sp] = nd.ch.y;
-                    k.t_t[t_sp] = b;
+                    k.t[t_sp] = make_int2(nd.ch.y, __float_as_int(b));
                     ++t_sp;
                 }
                 t_cur = nd.ch.x;
