@@ -391,34 +391,65 @@ def measure_e2e(ctx, data, args, dev) -> dict:
     found = np.zeros(1, np.int64)
     lib = ctx._lib
 
-    bvh = ctx.build_lbvh(h_tris)
-    qbvh = ctx.build_lbvh(h_queries, kind=lux_b200.PRIM_AABBS)
+    # Two contexts (each its own stream, BVHs and output buffers) so that one step's
+    # copies overlap the other's kernels, as a caller with a stream of steps would run
+    # them; every step still copies its inputs in and its results out.
+    import threading
 
-    def step():
+    ctxs = [ctx, lux_b200.Context(dev.index or 0 if hasattr(dev, "index") else int(dev))]
+    outs = [(h_id, h_t, h_pairs, found),
+            (torch.empty(N_RAYS, dtype=torch.int32).pin_memory(),
+             torch.empty(N_RAYS, dtype=torch.float32).pin_memory(),
+             torch.empty((max_pairs, 2), dtype=torch.int32).pin_memory(), np.zeros(1, np.int64))]
+    trees = [(c.build_lbvh(h_tris), c.build_lbvh(h_queries, kind=lux_b200.PRIM_AABBS))
+             for c in ctxs]
+
+    def step(k):
+        bvh, qbvh = trees[k]
+        o_id, o_t, o_pairs, o_found = outs[k]
         bvh.rebuild(h_tris)
-        bvh.trace_closest(h_rays, h_id, h_t)
+        bvh.trace_closest(h_rays, o_id, o_t)
         bvh.refit(h_refit)
         qbvh.rebuild(h_queries)
-        lux_b200._check(lib.lux_overlap_cross(ctx.handle, bvh.handle, qbvh.handle,
-                                              h_pairs.data_ptr(), max_pairs,
-                                              found.ctypes.data))
+        lux_b200._check(lib.lux_overlap_cross(ctxs[k].handle, bvh.handle, qbvh.handle,
+                                              o_pairs.data_ptr(), max_pairs,
+                                              o_found.ctypes.data))
+
+    def run(k, n):
+        for _ in range(n):
+            step(k)
 
     for _ in range(max(args.warmup, 1)):
-        step()
-    steps = max(3, min(args.steps, 10))
+        step(0)
+        step(1)
+    steps = max(4, min(args.steps, 10) // 2 * 2)
+    # One context alone: each step's copies and kernels in sequence.
     t0 = time.perf_counter()
-    for _ in range(steps):
-        step()
+    run(0, steps)
     ctx.synchronize()
+    serial = (time.perf_counter() - t0) / steps
+    # Both contexts, steps alternating.
+    workers = [threading.Thread(target=run, args=(k, steps // 2)) for k in range(2)]
+    t0 = time.perf_counter()
+    for w in workers:
+        w.start()
+    for w in workers:
+        w.join()
+    for c in ctxs:
+        c.synchronize()
     dt = (time.perf_counter() - t0) / steps
     h2d = sum(d.nbytes for d in (data["triangles"], data["rays"], data["refit_triangles"],
                                   data["queries"]))
     d2h = N_RAYS * 8 + min(int(found[0]), max_pairs) * 8 + 8
-    bvh.close()
-    qbvh.close()
+    for bvh, qbvh in trees:
+        bvh.close()
+        qbvh.close()
+    ctxs[1].close()
     return {"value": N_RAYS / dt / 1e6, "unit": "Mrays/s", "h2d_bytes_per_step": h2d,
             "d2h_bytes_per_step": d2h, "ms_per_step": dt * 1e3, "steps": steps,
-            "host_buffers": "pinned"}
+            "host_buffers": "pinned",
+            "pipelining": "two contexts on two host threads, steps alternating",
+            "one_context_ms_per_step": serial * 1e3}
 
 
 def measure_cpu_baseline(data) -> dict | None:
