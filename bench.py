@@ -41,7 +41,7 @@ METRIC = "Mrays/s"
 # Algorithmic bytes (per unit) used for the roofline: build 120 B/tri, refit 104 B/tri,
 # traversal 32 B ray + 8 B hit + 32 B per box test + 36 B per triangle test.
 BUILD_BYTES_PER_TRI = 120
-TRACE_DRAM_BYTES_PER_RAY = (1.282381e9 + 0.044999e9) / 1048576
+TRACE_DRAM_BYTES_PER_RAY = (1.421934e9 + 0.088448e9) / 1048576
 REFIT_BYTES_PER_TRI = 104
 
 

@@ -324,8 +324,8 @@ __global__ void __launch_bounds__(kTraceThreads) k_trace_persistent(
 // latency that bounds this kernel.  The cap spills 44 bytes per thread, and the extra
 // warps still win: 468 against 439 Mrays/s at 64 registers and 425 at 40 (1,048,576
 // triangles, 4,194,304 rays, B200).  The deferred-child stack lives in local memory and
-// its reads mostly miss L1; one 8-byte entry per push and pop (rather than two 4-byte
-// arrays) halves those requests: 479 against 467 Mrays/s.
+// its reads mostly miss L1; keeping an entry's node and entry distance in one 8-byte
+// record (one access per push or pop rather than two) gives 479 against 467 Mrays/s.
 template <bool AnyHit>
 __global__ void __launch_bounds__(kTraceThreads, 10) k_trace_wide_persistent(
         BvhView bvh, const float4* rays, int nrays, int* hit_id, float* hit_t,
