@@ -504,8 +504,20 @@ RENDER_CONFIGS = {
 
 
 def run_render(args, name: str) -> None:
-    """Config 1 (Cornell) or config 3 (heavy render): one lux_render per step."""
-    torch, ctx, stream = _render_setup()
+    """Config 1 (Cornell) or config 3 (heavy render): one lux_render per step.  Under
+    torchrun (N > 1) the frame's samples are split across the ranks and their films are
+    summed with one NCCL reduce (lux_b200.distributed): strong scaling of one frame."""
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch, ctx, stream = _render_setup(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    from lux_b200 import distributed as D
     from lux_b200 import scene as S
     from lux_b200 import scenes as SC
 
@@ -517,34 +529,62 @@ def run_render(args, name: str) -> None:
     builder = S.make_cornell_scene(W, H) if name == "cornell" else SC.heavy_render_scene(W, H)
     sc = S.Scene(ctx, builder)
     req = S.request(W, H, spp, depth, seed)
-    film = torch.zeros((H, W, 3), dtype=torch.float32, device="cuda")
+    film = torch.zeros((H, W, 3), dtype=torch.float32, device=f"cuda:{local}")
+
+    def step(target):
+        if world == 1:
+            S.render(ctx, sc, req, target)
+        else:
+            D.render_sharded(lambda q, f: S.render(ctx, sc, q, f), req, target)
+
     for _ in range(max(args.warmup, 1)):
-        S.render(ctx, sc, req, film)
+        step(film)
     torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
     launches0 = ctx.launch_count()
-    clocks = ClockSampler(0)
+    clocks = ClockSampler(local)
     clocks.start()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
     for _ in range(args.steps):
-        S.render(ctx, sc, req, film)
+        step(film)
     e1.record(stream)
     torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
     clock_info = clocks.stop()
     launches = ctx.launch_count() - launches0
     ms = e0.elapsed_time(e1) / args.steps
-    rays = S.ray_counts(ctx)
+    rays = list(S.ray_counts(ctx))
+    if dist:  # the whole frame's rays, the slowest rank's time
+        t = torch.tensor(rays, dtype=torch.float64, device=film.device)
+        dist.all_reduce(t)
+        rays = [int(v) for v in t.tolist()]
+        ms = max_over_ranks(ms, dist, film.device)
     total_rays = sum(rays)
     value = total_rays / (ms * 1e-3) / 1e6
-    # e2e: host film through the C ABI (device -> host copy timed).
+    # e2e: the frame's film on the host (device -> host copy timed; rank 0 receives it).
     host_film = np.zeros((H, W, 3), np.float32)
     e2e_steps = max(1, min(args.steps, 10 if name == "cornell" else 2))
+    if dist:
+        dist.barrier()
     t0 = time.perf_counter()
     for _ in range(e2e_steps):
-        S.render(ctx, sc, req, host_film)
+        if world == 1:
+            S.render(ctx, sc, req, host_film)
+        else:
+            step(film)
+            if rank == 0:
+                host_film[...] = film.cpu().numpy()
+    torch.cuda.synchronize()
     e2e_ms = (time.perf_counter() - t0) / e2e_steps * 1e3
+    if dist:
+        e2e_ms = max_over_ranks(e2e_ms, dist, film.device)
+        step(film)  # the timed film itself for the image check below (rank 0 holds it)
+        torch.cuda.synchronize()
     cpu = None
-    if not args.skip_cpu_baseline:
+    if rank == 0 and world == 1 and not args.skip_cpu_baseline:
         from oracle.bindings import Ref
         if Ref.available():
             threads = os.cpu_count() or 1
@@ -576,7 +616,7 @@ def run_render(args, name: str) -> None:
     fp64 = None
     fixture = os.path.join(os.path.dirname(os.path.abspath(__file__)), "tests", "golden",
                            f"{name}_fp64.npz")
-    if os.path.exists(fixture) and not (args.render_size or args.render_spp):
+    if rank == 0 and os.path.exists(fixture) and not (args.render_size or args.render_spp):
         g = np.load(fixture)
         x0, y0, x1, y1 = (int(v) for v in g["rect"]) if "rect" in g else (0, 0, W, H)
         img = film.double().cpu().numpy()[y0:y1, x0:x1] / spp
@@ -591,19 +631,26 @@ def run_render(args, name: str) -> None:
                 "oracle_spp": int(g["spp"]),
                 "pixels": "all" if "rect" not in g else f"crop x{x0}..{x1} y{y0}..{y1}"}
     line = {"metric": metric, "value": value, "unit": "Mrays/s",
-            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-            "data": "synthetic",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak" if world == 1 else "strong",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": workload,
                        "l2": "scene L2/L1 resident" if name == "cornell" else
-                             "path state 4M paths x 192 B > L2"},
+                             "path state 4M paths x 192 B > L2",
+                       "parallelism": "single GPU" if world == 1 else
+                                      f"samples split over {world} ranks, films summed by "
+                                      "one NCCL reduce"},
             "rays": {"camera_extension": rays[0], "shadow_segments": rays[1]},
             "clocks": clock_info, "gpu_launches": launches,
             "e2e": {"value": total_rays / (e2e_ms * 1e-3) / 1e6, "unit": "Mrays/s",
                     "h2d_bytes_per_step": 0, "d2h_bytes_per_step": W * H * 12,
                     "ms_per_step": e2e_ms},
             "cpu_baseline": cpu, "image_error_vs_fp64_oracle": fp64}
-    print(json.dumps(line))
+    if rank == 0:
+        print(json.dumps(line))
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
 
 
 def run_batched(args) -> None:
