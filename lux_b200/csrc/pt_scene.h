@@ -91,9 +91,10 @@ void scene_free(lux_scene* scene);
 // all in stream order on ctx->stream; when an instance of the mesh carries emission, the
 // light tables are re-derived on the host and copied in stream order too (the stream is
 // waited for only when a table outgrows its buffer).  With sync, waits and reports device
-// errors; without, the caller's next synchronisation does.
+// errors; without, the caller's next synchronisation does.  *view_changed (if given) is
+// set when scene->view changed (the light tables were re-derived).
 int scene_update_mesh(lux_ctx* ctx, lux_scene* scene, int mesh, const float* vertices,
-                      bool sync = true);
+                      bool sync = true, bool* view_changed = nullptr);
 int camera_perspective(const float* origin, const float* look_at, float vfov, float aspect,
                        float lens_radius, float focal_distance, lux_camera_desc* out);
 

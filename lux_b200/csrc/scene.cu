@@ -1110,7 +1110,9 @@ int prepare_refit(lux_scene* s, int mesh) {
 
 }  // namespace
 
-int scene_update_mesh(lux_ctx* ctx, lux_scene* s, int mesh, const float* vertices, bool sync) {
+int scene_update_mesh(lux_ctx* ctx, lux_scene* s, int mesh, const float* vertices, bool sync,
+                      bool* view_changed) {
+    if (view_changed) *view_changed = false;
     if (mesh < 0 || mesh >= static_cast<int>(s->blas.size()))
         return fail(LUX_ERR_INVALID_ARGUMENT, "mesh out of range");
     if (int st = prepare_refit(s, mesh)) return st;
@@ -1164,6 +1166,7 @@ int scene_update_mesh(lux_ctx* ctx, lux_scene* s, int mesh, const float* vertice
                                                  s->explicit_power, size_t(s->triangle_count));
         if (int st = upload_light_tables(ctx, s, lt)) return st;
         set_light_view(s, lt);
+        if (view_changed) *view_changed = true;
     }
     if (!sync) return LUX_OK;
     err = cudaStreamSynchronize(stream);

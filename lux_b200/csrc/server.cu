@@ -592,14 +592,18 @@ void worker_main(lux_server* s) {
                     superseded = batch[j].scene == batch[k].scene && batch[j].mesh == batch[k].mesh;
                 if (superseded) continue;
                 lux_scene* scene = s->scenes[batch[k].scene];
+                bool view_changed = false;
                 if (lux::scene_update_mesh(s->ctx, scene, batch[k].mesh,
-                                           batch[k].vertices.data(), false) != LUX_OK)
+                                           batch[k].vertices.data(), false,
+                                           &view_changed) != LUX_OK)
                     continue;
                 ++applied;
-                // Light tables may have been re-derived: the staged view follows, in
-                // stream order before the next iteration.
-                cudaMemcpyAsync(s->d_scenes + batch[k].scene, &scene->view, sizeof(scene->view),
-                                cudaMemcpyHostToDevice, s->ctx->stream);
+                // Re-derived light tables: the staged view follows, in stream order before
+                // the next iteration.  (A copy from pageable memory may wait for the
+                // stream, so it is made only when the view changed.)
+                if (view_changed)
+                    cudaMemcpyAsync(s->d_scenes + batch[k].scene, &scene->view,
+                                    sizeof(scene->view), cudaMemcpyHostToDevice, s->ctx->stream);
             }
             lk.lock();
             s->refits += applied;
