@@ -529,6 +529,12 @@ def run_render(args, name: str) -> None:
     builder = S.make_cornell_scene(W, H) if name == "cornell" else SC.heavy_render_scene(W, H)
     sc = S.Scene(ctx, builder)
     req = S.request(W, H, spp, depth, seed)
+    # The autotuner (lux_autotune_render) picks the traversal variant, step budget and
+    # batch on a probe of this scene (the frame itself when it is small), before timing.
+    from lux_b200 import autotune
+    probe = req if W * H * spp <= (1 << 23) else S.request(min(W, 512), min(H, 512),
+                                                            min(spp, 16), depth, seed)
+    tune = autotune.autotune_render(ctx, sc, probe)
     film = torch.zeros((H, W, 3), dtype=torch.float32, device=f"cuda:{local}")
 
     def step(target):
@@ -639,7 +645,11 @@ def run_render(args, name: str) -> None:
                              "path state 4M paths x 192 B > L2",
                        "parallelism": "single GPU" if world == 1 else
                                       f"samples split over {world} ranks, films summed by "
-                                      "one NCCL reduce"},
+                                      "one NCCL reduce",
+                       "autotuned": {"trace_variant": tune.trace_variant,
+                                     "path_budget": tune.budget,
+                                     "render_batch": tune.render_batch,
+                                     "probe": f"{probe.width}x{probe.height}, {probe.spp} spp"}},
             "rays": {"camera_extension": rays[0], "shadow_segments": rays[1]},
             "clocks": clock_info, "gpu_launches": launches,
             "e2e": {"value": total_rays / (e2e_ms * 1e-3) / 1e6, "unit": "Mrays/s",
