@@ -396,6 +396,78 @@ int lux_render_aovs(lux_ctx* ctx, const lux_scene* scene, const lux_render_reque
                     float* film_sum, float* shadow, float* ng, float* ns);
 
 /*
+ * Path log: one record per surface vertex a path reaches (PathLogRecord,
+ * integrator/pathstate.cuh:19-65; filled as the wavefront tracer's evaluate_hit_kernel
+ * does, integrator/wavefront_kernels.cu:84-138, 356-558).  Enumerations keep the
+ * reference's values: measures 0 none, 1 solid angle, 2 area, 3 discrete; sources
+ * 0 none, 1 camera, 2 BSDF, 3 light, 4 guide; BSDF flags 1 diffuse, 2 glossy, 4 delta
+ * reflection, 8 delta transmission, 16 transmission; primitive kind 1 triangle.
+ */
+enum lux_path_log_event {
+    LUX_PATH_EVENT_SURFACE_HIT = 1u << 0,
+    LUX_PATH_EVENT_EMISSION = 1u << 1,
+    LUX_PATH_EVENT_DIRECT_LIGHT_SAMPLED = 1u << 2,
+    LUX_PATH_EVENT_DIRECT_LIGHT_VALID = 1u << 3,
+    LUX_PATH_EVENT_BSDF_SAMPLED = 1u << 4,
+    LUX_PATH_EVENT_TERMINATED = 1u << 5,
+    LUX_PATH_EVENT_SPAWNED_RAY = 1u << 6,
+    LUX_PATH_EVENT_DELTA = 1u << 7,
+    LUX_PATH_EVENT_PASSTHROUGH = 1u << 8
+};
+enum lux_path_log_termination {
+    LUX_PATH_END_NON_SCATTERING = 1u << 0,
+    LUX_PATH_END_MAX_DEPTH = 1u << 1,
+    LUX_PATH_END_INVALID_BSDF = 1u << 2,
+    LUX_PATH_END_RUSSIAN_ROULETTE = 1u << 3,
+    LUX_PATH_END_ZERO_THROUGHPUT = 1u << 4
+};
+
+typedef struct lux_path_log_record {
+    int32_t pixel_index;
+    int32_t sample_index;      /* the request's sample_offset plus the sample */
+    int32_t depth;             /* scattering bounces before this vertex */
+    int32_t triangle_id;       /* scene triangle */
+    int32_t instance_id;       /* PrimitiveRef: instance, mesh, local triangle, kind */
+    int32_t mesh_id;
+    int32_t local_primitive_id;
+    int32_t primitive_kind;
+    int32_t material_id;
+    int32_t vertex;            /* surface vertices of this path before this one */
+    float position[3];
+    float ng[3];
+    float ns[3];               /* shading normal, turned to the geometric normal's side */
+    float wo[3];
+    float wi[3];
+    float throughput_before[3];
+    float throughput_after[3];
+    float bsdf_pdf;
+    float guide_pdf;           /* always 0: no guiding on this path */
+    float light_pdf;
+    uint8_t bsdf_pdf_measure;
+    uint8_t guide_pdf_measure;
+    uint8_t light_pdf_measure;
+    uint8_t sample_source;
+    uint32_t bsdf_flags;
+    uint32_t termination_flags;
+    uint32_t event_flags;
+} lux_path_log_record;
+
+/*
+ * lux_render (film_sum as there) that also logs every path's surface vertices
+ * (RenderOutputs::set_path_log, integrator/render_context.h:65-85).  records is a HOST
+ * array of capacity entries (null when capacity is 0, to count only); *count receives
+ * the number of vertices the render reached.  Records come sorted by (sample_index,
+ * pixel_index, vertex), one path's vertices in the order it met them (the reference
+ * appends in device-atomic order).  A render with more vertices than capacity returns
+ * LUX_ERR_QUEUE_OVERFLOW with *count set and records unspecified (the reference
+ * throws).  Per path at most max_depth + 1 vertices, so width * height * spp *
+ * (max_depth + 1) always suffices.
+ */
+int lux_render_path_log(lux_ctx* ctx, const lux_scene* scene, const lux_render_request* req,
+                        float* film_sum, lux_path_log_record* records, int64_t capacity,
+                        int64_t* count);
+
+/*
  * Light selection as next-event estimation makes it, for validation: for each i, the
  * light that select_u[i] picks at shading position positions[3i..3i+2] with sampler kind
  * light_sampler (0 uniform, 1 power, 2 light tree), in light-table order (area lights in

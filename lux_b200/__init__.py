@@ -80,6 +80,7 @@ SIGNATURES = {
     "lux_scene_update_mesh": (ctypes.c_int, [_P, _P, _I32, _P]),
     "lux_scene_select_lights": (ctypes.c_int, [_P, _P, _I32, _P, _P, _I32, _P, _P, _P]),
     "lux_render_aovs": (ctypes.c_int, [_P, _P, _P, _P, _P, _P, _P]),
+    "lux_render_path_log": (ctypes.c_int, [_P, _P, _P, _P, _P, _I64, ctypes.POINTER(_I64)]),
     "lux_obj_load": (ctypes.c_int, [ctypes.c_char_p, _P, _P]),
     "lux_obj_mesh_free": (None, [_P]),
     "lux_render": (ctypes.c_int, [_P, _P, _P, _P]),

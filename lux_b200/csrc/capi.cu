@@ -674,6 +674,55 @@ int lux_render_aovs(lux_ctx* ctx, const lux_scene* scene, const lux_render_reque
     return sync_and_check(ctx);
 }
 
+static_assert(sizeof(lux_path_log_record) == 152, "lux_path_log_record layout");
+
+int lux_render_path_log(lux_ctx* ctx, const lux_scene* scene, const lux_render_request* req,
+                        float* film_sum, lux_path_log_record* records, int64_t capacity,
+                        int64_t* count) {
+    if (int st = check_ctx(ctx)) return st;
+    if (!scene || !req || !film_sum || !count || capacity < 0 || (capacity > 0 && !records))
+        return lux::fail(LUX_ERR_INVALID_ARGUMENT, "null argument");
+    if (req->width <= 0 || req->height <= 0 || req->spp <= 0)
+        return lux::fail(LUX_ERR_INVALID_ARGUMENT, "render requires a non-empty film");
+    if (req->max_depth < 0 || req->max_depth > 1000)
+        return lux::fail(LUX_ERR_INVALID_ARGUMENT, "max_depth must be in 0..1000");
+    if (req->light_sampler < 0 || req->light_sampler > 2)
+        return lux::fail(LUX_ERR_INVALID_ARGUMENT, "light sampler: 0 uniform, 1 power or 2 tree");
+    if (static_cast<long long>(req->width) * req->height > (1ll << 30))
+        return lux::fail(LUX_ERR_INVALID_ARGUMENT, "image too large");
+    if (records && is_device_pointer(records))
+        return lux::fail(LUX_ERR_INVALID_ARGUMENT, "path log records must be host memory");
+    const size_t bytes = sizeof(float) * 3 * static_cast<size_t>(req->width) * req->height;
+    unsigned long long vertices = 0;
+    Staging staging(ctx);
+    void *d_film = nullptr, *d_records = nullptr, *d_count = nullptr;
+    staging.add(film_sum, bytes, false, true, &d_film);
+    staging.add(records, sizeof(lux_path_log_record) * static_cast<size_t>(capacity), false, true,
+                &d_records);
+    staging.add(&vertices, sizeof(vertices), false, true, &d_count);
+    int st = staging.begin();
+    if (st) return st;
+    st = lux::render(ctx, scene, *req, static_cast<float*>(d_film), false, nullptr, nullptr,
+                     nullptr, capacity > 0 ? static_cast<lux_path_log_record*>(d_records) : nullptr,
+                     static_cast<unsigned long long*>(d_count), capacity);
+    if (st) return st;
+    st = finish_call(ctx, staging);
+    if (st) return st;
+    st = sync_and_check(ctx);
+    if (st) return st;
+    *count = static_cast<int64_t>(vertices);
+    if (*count > capacity)
+        return lux::fail(LUX_ERR_QUEUE_OVERFLOW, "path log capacity exhausted");
+    // One path's vertices carry distinct ordinals, so the key is unique.
+    std::sort(records, records + *count,
+              [](const lux_path_log_record& a, const lux_path_log_record& b) {
+                  if (a.sample_index != b.sample_index) return a.sample_index < b.sample_index;
+                  if (a.pixel_index != b.pixel_index) return a.pixel_index < b.pixel_index;
+                  return a.vertex < b.vertex;
+              });
+    return LUX_OK;
+}
+
 int lux_render_samples(lux_ctx* ctx, const lux_scene* scene, const lux_render_request* req,
                        float* samples) {
     return render_common(ctx, scene, req, samples, true);

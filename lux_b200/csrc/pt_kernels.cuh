@@ -12,6 +12,7 @@
 
 #include <cuda_runtime.h>
 
+#include "../../include/lux_gpu.h"
 #include "pt_device.cuh"
 
 namespace lux {
@@ -1191,11 +1192,71 @@ struct ShadeOut {
 //             when it samples a light: orange (1, 0.5, 0) when the light sample is
 //             invalid, purple (0.5, 0, 1) when the unoccluded estimate is, else the
 //             classification of its shadow ray (shadow_aov_color).
-struct AovTargets {
+//   path log  (on when log_count is set) one lux_path_log_record per surface vertex a
+//             path reaches (integrator/pathstate.cuh:41-96), at an atomically taken
+//             index; the index keeps counting past capacity so the host learns the size
+//             needed.
+struct DebugTargets {
     float* shadow = nullptr;
     float* ng = nullptr;
     float* ns = nullptr;
+    lux_path_log_record* log = nullptr;
+    unsigned long long* log_count = nullptr;
+    long long log_capacity = 0;
+    int sample_offset = 0;
 };
+
+// What the shading of one vertex decided, for its path log record
+// (SurfaceStageLogState, integrator/wavefront_kernels.cu:140-151).
+struct VertexLog {
+    f3 wi = make_f3(0, 0, 0);
+    float bsdf_pdf = 0, light_pdf = 0;
+    int bsdf_measure = kMeasureNone, light_measure = kMeasureNone, source = 0;
+    unsigned bsdf_flags = 0;
+    unsigned events = LUX_PATH_EVENT_SURFACE_HIT;
+};
+
+constexpr int kSourceBsdf = 2;  // SampleSource::BSDF
+
+// record_surface_vertex / record_path_vertex (integrator/wavefront_kernels.cu:84-138,
+// integrator/pathstate.cuh:82-96) for the vertex at hit prim of path state s.
+LUX_D void log_vertex(const DebugTargets& dbg, const SceneView& sc, const PathState& s,
+                      int vertex, int depth, int prim, f3 pos, f3 ng, f3 ns, f3 wo, f3 thr_before,
+                      f3 thr_after, const VertexLog& v, unsigned termination) {
+    if (!dbg.log_count) return;
+    const unsigned long long index = atomicAdd(dbg.log_count, 1ull);
+    if (index >= static_cast<unsigned long long>(dbg.log_capacity)) return;
+    const SceneTri tri = sc.tris[prim];
+    lux_path_log_record r;
+    r.pixel_index = s.pixel;
+    r.sample_index = dbg.sample_offset + s.sample;
+    r.depth = depth;
+    r.triangle_id = prim;
+    r.instance_id = __float_as_int(tri.v1.w);
+    r.mesh_id = sc.instances[r.instance_id].blas;
+    r.local_primitive_id = __float_as_int(tri.v2.w);
+    r.primitive_kind = 1;
+    r.material_id = __float_as_int(tri.v0.w);
+    r.vertex = vertex;
+    const f3 vecs[7] = {pos, ng, ns, wo, v.wi, thr_before, thr_after};
+    float* dst[7] = {r.position, r.ng, r.ns, r.wo, r.wi, r.throughput_before, r.throughput_after};
+    for (int k = 0; k < 7; ++k) {
+        dst[k][0] = vecs[k].x;
+        dst[k][1] = vecs[k].y;
+        dst[k][2] = vecs[k].z;
+    }
+    r.bsdf_pdf = v.bsdf_pdf;
+    r.guide_pdf = 0.0f;
+    r.light_pdf = v.light_pdf;
+    r.bsdf_pdf_measure = static_cast<uint8_t>(v.bsdf_measure);
+    r.guide_pdf_measure = 0;
+    r.light_pdf_measure = static_cast<uint8_t>(v.light_measure);
+    r.sample_source = static_cast<uint8_t>(v.source);
+    r.bsdf_flags = v.bsdf_flags;
+    r.termination_flags = termination;
+    r.event_flags = v.events | (termination ? LUX_PATH_EVENT_TERMINATED : 0u);
+    dbg.log[index] = r;
+}
 
 LUX_D void aov_add(float* image, int pixel, f3 c) {
     atomicAdd(image + 3 * size_t(pixel), c.x);
@@ -1207,7 +1268,7 @@ LUX_D f3 encode_normal_color(f3 n) { return (normalize(n) + splat(1.0f)) * 0.5f;
 
 // primary_normal_debug_color for the camera ray's closest hit h of path p.
 LUX_D void aov_primary(const PathPool& rt, const SceneView& sc, int p, const SceneHit& h,
-                       const AovTargets& aov) {
+                       const DebugTargets& aov) {
     const int4 meta = rt.meta[p];
     if (meta.z != 0 || h.prim < 0) return;  // depth and pass-through count both zero
     const SceneTri tri = sc.tris[h.prim];
@@ -1242,11 +1303,12 @@ LUX_D f3 shadow_aov_color(const SceneView& sc, int source_prim, f3 ng, f3 ns, f3
 }
 
 // Shading of the hit stored for path p (cpu_path_tracer.cpp:430-497).  With kAov, also
-// the shadow debug image's light-sample verdict at depth 0, and shadow rays at depth 0
-// are marked (sh_t.w = 1) for classification.
+// the shadow debug image's light-sample verdict at depth 0, shadow rays at depth 0 are
+// marked (sh_t.w = 1) for classification, and the vertex goes to the path log at each
+// exit evaluate_hit_kernel records one (integrator/wavefront_kernels.cu:397-555).
 template <bool kAov = false>
 LUX_D ShadeOut shade_path(const PathPool& rt, const SceneView& sc, int sampler, int max_depth,
-                          int p, const AovTargets& aov = AovTargets{}) {
+                          int p, const DebugTargets& aov = DebugTargets{}) {
     ShadeOut out;
     float4 ra = rt.ray_o[p], rb = rt.ray_d[p], hh = rt.hit[p];
     f3 ro = xyz(ra), rd = xyz(rb);
@@ -1260,29 +1322,59 @@ LUX_D ShadeOut shade_path(const PathPool& rt, const SceneView& sc, int sampler, 
     f3 pos = ro + rd * t;                    // Ray::at
     f3 ng = triangle_normal(v0, v1, v2);
     f3 wo = -rd;
+    const bool logging = kAov && aov.log_count != nullptr;
+    const f3 thr0 = s.thr;
+    VertexLog vl;
+    // Logs this vertex with throughput_after thr1 and the given termination.
+    auto log = [&](f3 thr1, unsigned termination) {
+        if (!logging) return;
+        f3 n = shading_normal(sc.shading[prim], ng, hu, hv);
+        if (dot(ng, n) < 0) n = -n;
+        log_vertex(aov, sc, s, step, s.depth, prim, pos, ng, n, wo, thr0, thr1, vl, termination);
+    };
     // Emission with MIS (cpu_path_tracer.cpp:434-447).
     f3 le = surface_le(sc, prim, m, ng, wo, hu, hv);
     if (max_component(le) > 0) {
         if (s.depth == 0 || is_delta(s.flags)) {
             add_radiance(rt, p, s.thr * le);
+            vl.events |= LUX_PATH_EVENT_EMISSION;
         } else if (s.measure == kMeasureSolidAngle && s.prev_pdf > 0) {
             float lpdf = surface_light_pdf(sc, sampler, prim, ng, pos, s.prev_pos);
             add_radiance(rt, p, (s.thr * le) * power_heuristic(s.prev_pdf, lpdf));
+            vl.events |= LUX_PATH_EVENT_EMISSION;
         }
     }
     if (is_passthrough(m)) {  // cpu_path_tracer.cpp:449-455
         s.thr = s.thr * passthrough_transmittance(m);
+        vl.events |= LUX_PATH_EVENT_PASSTHROUGH | LUX_PATH_EVENT_DELTA;
+        vl.wi = normalize(-wo);
+        vl.bsdf_pdf = 1.0f;
+        vl.bsdf_measure = kMeasureDiscrete;
+        vl.source = kSourceBsdf;
+        vl.bsdf_flags = kFlagDeltaTransmission | kFlagTransmission;
         if (max_component(s.thr) > 0 && step < max_depth) {
+            vl.events |= LUX_PATH_EVENT_SPAWNED_RAY;
+            log(s.thr, 0);
             s.passthrough += 1;
             f3 no = pos + rd * kRayEpsilon;
             rt.ray_o[p] = make_float4(no.x, no.y, no.z, kRayEpsilon);
             rt.ray_d[p] = make_float4(rd.x, rd.y, rd.z, INFINITY);
             out.spawn = true;
+        } else {
+            log(s.thr, max_component(s.thr) <= 0 ? LUX_PATH_END_ZERO_THROUGHPUT
+                                                 : LUX_PATH_END_MAX_DEPTH);
         }
         store_state(rt, p, s);
         return out;
     }
-    if (!is_scattering(m) || step >= max_depth || s.depth >= max_depth) return out;
+    if (!is_scattering(m)) {
+        log(thr0, LUX_PATH_END_NON_SCATTERING);
+        return out;
+    }
+    if (step >= max_depth || s.depth >= max_depth) {
+        log(thr0, LUX_PATH_END_MAX_DEPTH);
+        return out;
+    }
     SceneTriShading sh = sc.shading[prim];
     f3 ns = shading_normal(sh, ng, hu, hv);
     if (dot(ng, ns) < 0) ns = -ns;   // make_surface_interaction
@@ -1295,13 +1387,17 @@ LUX_D ShadeOut shade_path(const PathPool& rt, const SceneView& sc, int sampler, 
         float ly = g.next_float();
         LightLi li = sample_light(sc, sampler, pos, su, cu, lx, ly);
         int verdict = 0;  // 0 light sample invalid, 1 estimate invalid, 2 valid
+        if (li.valid) vl.events |= LUX_PATH_EVENT_DIRECT_LIGHT_SAMPLED;
         if (li.valid && li.pdf > 0) {
             verdict = 1;
+            vl.light_pdf = li.pdf;  // pdf_light_solid_angle, logged as a solid angle
+            vl.light_measure = kMeasureSolidAngle;
             f3 f = eval_bsdf(m, it, li.wi);
             float cs = abs_cosine(ns, li.wi);
             float pb = pdf_bsdf(m, it, li.wi);
             if (max_component(f) > 0 && max_component(li.radiance) > 0 && cs > 0) {
                 verdict = 2;
+                vl.events |= LUX_PATH_EVENT_DIRECT_LIGHT_VALID;
                 f3 contrib = (f * li.radiance) * (cs / li.pdf);
                 float mis = li.measure == kMeasureDiscrete ? 1.0f : power_heuristic(li.pdf, pb);
                 f3 off = dot(li.wi, ng) >= 0 ? ng : -ng;
@@ -1343,17 +1439,29 @@ LUX_D ShadeOut shade_path(const PathPool& rt, const SceneView& sc, int sampler, 
     float bx = g.next_float();
     float by = g.next_float();
     BsdfSample bs = sample_bsdf(m, it, bx, by);
+    vl.wi = bs.wi;
+    vl.bsdf_flags = bs.flags;
+    vl.events |= LUX_PATH_EVENT_BSDF_SAMPLED | (is_delta(bs.flags) ? LUX_PATH_EVENT_DELTA : 0u);
+    if (bs.pdf > 0) {
+        vl.bsdf_pdf = bs.pdf;
+        vl.bsdf_measure = bs.measure;
+    }
+    if (!(bs.pdf > 0 && max_component(bs.weight) > 0)) log(thr0, LUX_PATH_END_INVALID_BSDF);
     if (bs.pdf > 0 && max_component(bs.weight) > 0) {
         f3 nthr = s.thr * bs.weight;
         float neta = mul(s.eta, is_transmission(bs.flags) && bs.eta > 0 ? mul(bs.eta, bs.eta) : 1.0f);
         bool alive = true;
+        vl.source = kSourceBsdf;
         if (s.depth > 2) {  // path_transport.cuh:58-84
             float prob = fminf(0.95f, mul(max_component(nthr), neta));
             float ru = g.next_float();
             if (ru <= prob) nthr = vdiv(nthr, prob);
             else alive = false;
         }
+        if (!alive) log(nthr, LUX_PATH_END_RUSSIAN_ROULETTE);
         if (alive) {
+            vl.events |= LUX_PATH_EVENT_SPAWNED_RAY;
+            log(nthr, 0);
             s.thr = nthr;
             s.eta = neta;
             s.prev_pdf = bs.pdf;
@@ -1378,7 +1486,7 @@ LUX_D ShadeOut shade_path(const PathPool& rt, const SceneView& sc, int sampler, 
 // a ray marked at shading adds its classification colour to the shadow debug image.
 template <bool kAov = false>
 LUX_D void shadow_path(const PathPool& rt, const SceneView& sc, int p, int* error,
-                       unsigned long long& segments, const AovTargets& aov = AovTargets{}) {
+                       unsigned long long& segments, const DebugTargets& aov = DebugTargets{}) {
     float4 a = rt.sh_o[p], b = rt.sh_d[p];
     f3 o = xyz(a), d = xyz(b);
     float tmax = a.w;

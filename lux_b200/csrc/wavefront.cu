@@ -153,7 +153,7 @@ __global__ void __launch_bounds__(kThreads) k_shadow_refill(PathPool rt, int* co
 // segments, as the classification needs the blocking hit).
 __global__ void __launch_bounds__(kThreads) k_extend_aov(PathPool rt, int* counts, SceneView sc,
                                                          int sampler, int depth, int* error,
-                                                         AovTargets aov) {
+                                                         DebugTargets aov) {
     int n = counts[depth * kSlots];
     int* mat_counts = counts + depth * kSlots + 1;
     const int* q = rt.qray[depth & 1];
@@ -178,7 +178,7 @@ __global__ void __launch_bounds__(kThreads) k_extend_aov(PathPool rt, int* count
 
 __global__ void __launch_bounds__(kThreads) k_shade_aov(PathPool rt, int* counts, SceneView sc,
                                                         int sampler, int depth, int max_depth,
-                                                        AovTargets aov) {
+                                                        DebugTargets aov) {
     const int* mc = counts + depth * kSlots + 1;
     int* next_count = counts + (depth + 1) * kSlots;
     int* shadow_count = counts + depth * kSlots + 6;
@@ -204,7 +204,7 @@ __global__ void __launch_bounds__(kThreads) k_shade_aov(PathPool rt, int* counts
 
 __global__ void __launch_bounds__(kThreads) k_shadow_aov(PathPool rt, int* counts,
                                                          unsigned long long* rays, SceneView sc,
-                                                         int depth, int* error, AovTargets aov) {
+                                                         int depth, int* error, DebugTargets aov) {
     int n = counts[depth * kSlots + 6];
     unsigned long long segments = 0;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
@@ -368,13 +368,18 @@ int render_ray_counts(lux_ctx* ctx, int64_t* counts) {
 }
 
 int render(lux_ctx* ctx, const lux_scene* scene, const lux_render_request& req, float* out,
-           bool per_sample, float* aov_shadow, float* aov_ng, float* aov_ns) {
+           bool per_sample, float* aov_shadow, float* aov_ng, float* aov_ns,
+           lux_path_log_record* log, unsigned long long* log_count, long long log_capacity) {
     using namespace pt;
-    AovTargets aov;
+    DebugTargets aov;
     aov.shadow = aov_shadow;
     aov.ng = aov_ng;
     aov.ns = aov_ns;
-    const bool with_aov = aov_shadow || aov_ng || aov_ns;
+    aov.log = log_capacity > 0 ? log : nullptr;
+    aov.log_count = log_count;
+    aov.log_capacity = aov.log ? log_capacity : 0;
+    aov.sample_offset = req.sample_offset;
+    const bool with_aov = aov_shadow || aov_ng || aov_ns || log_count;
     const int pixels = req.width * req.height;
     const long long total_paths = static_cast<long long>(pixels) * req.spp;
     // Batch: whole pixels' sample ranges, at most ctx->render_batch paths.
@@ -409,6 +414,8 @@ int render(lux_ctx* ctx, const lux_scene* scene, const lux_render_request& req, 
     for (float* image : {aov_shadow, aov_ng, aov_ns})
         if (image && err == cudaSuccess)
             err = cudaMemsetAsync(image, 0, sizeof(float) * 3 * size_t(pixels), s);
+    if (log_count && err == cudaSuccess)
+        err = cudaMemsetAsync(log_count, 0, sizeof(unsigned long long), s);
     if (err != cudaSuccess) return cuda_fail(err, "render setup");
     for (int s0 = 0; s0 < req.spp; s0 += samples_per_batch) {
         int ns = std::min(samples_per_batch, req.spp - s0);

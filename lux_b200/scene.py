@@ -348,6 +348,41 @@ def render_aovs(ctx, scene: Scene, req: RenderRequest, shadow=True, ng=True, ns=
     return film, out[0], out[1], out[2]
 
 
+# lux_path_log_record (PathLogRecord, integrator/pathstate.cuh:41-65).
+PATH_LOG_RECORD = np.dtype([
+    ("pixel_index", "<i4"), ("sample_index", "<i4"), ("depth", "<i4"), ("triangle_id", "<i4"),
+    ("instance_id", "<i4"), ("mesh_id", "<i4"), ("local_primitive_id", "<i4"),
+    ("primitive_kind", "<i4"), ("material_id", "<i4"), ("vertex", "<i4"),
+    ("position", "<f4", 3), ("ng", "<f4", 3), ("ns", "<f4", 3), ("wo", "<f4", 3),
+    ("wi", "<f4", 3), ("throughput_before", "<f4", 3), ("throughput_after", "<f4", 3),
+    ("bsdf_pdf", "<f4"), ("guide_pdf", "<f4"), ("light_pdf", "<f4"),
+    ("bsdf_pdf_measure", "u1"), ("guide_pdf_measure", "u1"), ("light_pdf_measure", "u1"),
+    ("sample_source", "u1"), ("bsdf_flags", "<u4"), ("termination_flags", "<u4"),
+    ("event_flags", "<u4")])
+assert PATH_LOG_RECORD.itemsize == 152
+
+# PathLogEventFlags / PathLogTerminationFlags (integrator/pathstate.cuh:19-39).
+EVENT_SURFACE_HIT, EVENT_EMISSION, EVENT_LIGHT_SAMPLED, EVENT_LIGHT_VALID = 1, 2, 4, 8
+EVENT_BSDF_SAMPLED, EVENT_TERMINATED, EVENT_SPAWNED_RAY, EVENT_DELTA = 16, 32, 64, 128
+EVENT_PASSTHROUGH = 256
+END_NON_SCATTERING, END_MAX_DEPTH, END_INVALID_BSDF = 1, 2, 4
+END_RUSSIAN_ROULETTE, END_ZERO_THROUGHPUT = 8, 16
+
+
+def render_path_log(ctx, scene: Scene, req: RenderRequest, capacity=None):
+    """Film sum and the path log of one render (lux_render_path_log): a structured array
+    of PATH_LOG_RECORD sorted by (sample_index, pixel_index, vertex).  capacity defaults
+    to the bound width * height * spp * (max_depth + 1)."""
+    if capacity is None:
+        capacity = req.width * req.height * req.spp * (req.max_depth + 1)
+    film = np.zeros((req.height, req.width, 3), np.float32)
+    records = np.zeros(max(int(capacity), 1), PATH_LOG_RECORD)
+    count = ctypes.c_int64(0)
+    _check(ctx._lib.lux_render_path_log(ctx.handle, scene.handle, ctypes.byref(req), _ptr(film),
+                                        records.ctypes.data, int(capacity), ctypes.byref(count)))
+    return film, records[:count.value]
+
+
 def render_samples(ctx, scene: Scene, req: RenderRequest):
     out = np.zeros((req.height * req.width, req.spp, 3), np.float32)
     _check(ctx._lib.lux_render_samples(ctx.handle, scene.handle, ctypes.byref(req), _ptr(out)))

@@ -121,6 +121,9 @@ class Ref:
                                           _P, _P, _P]
         lib.ref_render_aovs.argtypes = [_P, _I, _P, _P, _I, _P, _I, _P, _I, _I, _I, _I,
                                         ctypes.c_uint64, _I, _P, _P, _P, _P]
+        lib.ref_path_log.argtypes = [_P, _I, _P, _P, _I, _P, _I, _P, _I, _I, _I, _I,
+                                     ctypes.c_uint64, _I, _P, ctypes.c_longlong]
+        lib.ref_path_log.restype = ctypes.c_longlong
         lib.ref_obj_load.argtypes = [ctypes.c_char_p, _I, _I, _I, _I, ctypes.c_float, _I, _I,
                                      ctypes.c_float, _P, _P, _I, _I, _P]
         lib.ref_obj_load.restype = _P
@@ -204,6 +207,25 @@ class Ref:
                                  len(lights), cam.ctypes.data, width, height, spp, max_depth,
                                  seed, light_sampler, *(o.ctypes.data for o in out))
         return tuple(out)
+
+    def path_log(self, tris, material_ids, materials, lights, camera, width, height, spp,
+                 max_depth, seed, light_sampler=1, dtype=None):
+        """The path log records of a render on a single-mesh scene, in (sample, pixel,
+        vertex) order, as a structured array of dtype (the lux_path_log_record layout)."""
+        tris = np.ascontiguousarray(tris, np.float32)
+        mids = np.ascontiguousarray(material_ids, np.int32)
+        mats = np.ascontiguousarray(materials, np.float32)
+        lights = np.ascontiguousarray(lights, np.float32).reshape(-1, 7)
+        cam = np.ascontiguousarray(camera, np.float32)
+        capacity = width * height * spp * (max_depth + 1)
+        out = np.zeros(capacity, dtype)
+        n = self.lib.ref_path_log(tris.ctypes.data, len(tris), mids.ctypes.data,
+                                  mats.ctypes.data, len(mats),
+                                  lights.ctypes.data if len(lights) else None, len(lights),
+                                  cam.ctypes.data, width, height, spp, max_depth, seed,
+                                  light_sampler, out.ctypes.data, capacity)
+        assert n <= capacity
+        return out[:n]
 
     def obj_load(self, path, normal_mode=0, reverse=False, flip_v=False, scale_mode=0,
                  target_extent=1.0, center_xz=False, ground_to_y=False, target_y=0.0,

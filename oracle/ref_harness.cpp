@@ -17,6 +17,8 @@
 //   trace_path                     integrator/cpu_path_tracer.cpp:403-498
 //   make_render_sampler            integrator/render_context.h:45-54
 //   render_cpu_path_tracer (debug images) integrator/cpu_path_tracer.cpp:160-562
+//   path log records (log_path)    integrator/wavefront_kernels.cu:84-138, 356-558 over
+//                                  trace_path's walk with the reference's CPU parts
 //   load_obj_into_scene_with_result util/obj_loader.cpp:1296-1301
 //   make_stanford_bunny_scene, make_lux_cover_scene, make_stanford_dragon_scene
 //                                  scene/stanford_bunny.h, scene/lux_cover.h,
@@ -41,14 +43,20 @@
 #include "film/pfm.h"
 #include "film/ppm.h"
 #include "integrator/cpu_path_tracer.h"
+#include "integrator/path_transport.cuh"
 #include "integrator/render_context.h"
 #include "scene/cornell_box.h"
 #include "scene/lux_cover.h"
 #include "scene/prepared_scene.h"
+#include "scene/scene_intersection.h"
 #include "scene/scene_light_sampler.h"
 #include "scene/stanford_bunny.h"
 #include "scene/stanford_dragon.h"
 #include "util/obj_loader.h"
+
+// lux_path_log_record and the LUX_PATH_* flags (the values of PathLogEventFlags and
+// PathLogTerminationFlags, integrator/pathstate.cuh:19-39, whose header needs thrust).
+#include "../include/lux_gpu.h"
 
 namespace {
 
@@ -377,6 +385,123 @@ int ref_cornell_render(int width, int height, int spp, int max_depth, uint64_t s
     return 0;
 }
 
+// One camera path's surface vertices as the reference's wavefront tracer logs them
+// (record_surface_vertex and its call sites in evaluate_hit_kernel,
+// integrator/wavefront_kernels.cu:84-138, 356-558), walked the way trace_path walks it
+// (integrator/cpu_path_tracer.cpp:403-498) with the reference's own CPU scene query,
+// light sampler, direct-light estimate and BSDF sampling.  A miss ends the path
+// unlogged.  vertex counts the path's earlier records; sample_index is the sample.
+static void log_path(const Scene& scene, const CpuBvh& bvh, const SceneLightSampler& lights,
+                     Ray ray, SamplerState& sampler, int max_depth, int pixel, int sample_index,
+                     std::vector<lux_path_log_record>& out) {
+    vec3 throughput(1);
+    PreviousSample previous_sample{0, PdfMeasure::None, SampleSource::Camera, 0, vec3(0)};
+    int depth = 0;
+    Float eta_scale = 1;
+    for (int step = 0; step <= max_depth; ++step) {
+        SurfaceHit hit;
+        if (!intersect_scene_bvh(scene, bvh, ray, hit)) return;
+        const SceneTriangle tri = scene_triangle_view(scene, hit.triangle_id);
+        const Material& material = scene.materials[tri.material_id];
+        const SurfaceInteraction it =
+            make_surface_interaction(hit.position, hit.ng, hit.ns, -ray.direction);
+        lux_path_log_record r;
+        std::memset(&r, 0, sizeof(r));
+        r.pixel_index = pixel;
+        r.sample_index = sample_index;
+        r.depth = depth;
+        r.triangle_id = hit.triangle_id;
+        r.instance_id = hit.primitive_ref.instance_id;
+        r.mesh_id = hit.primitive_ref.mesh_id;
+        r.local_primitive_id = hit.primitive_ref.local_primitive_id;
+        r.primitive_kind = static_cast<int32_t>(hit.primitive_ref.kind);
+        r.material_id = tri.material_id;
+        r.vertex = step;
+        auto put = [](float* dst, const vec3& v) { dst[0] = v.x; dst[1] = v.y; dst[2] = v.z; };
+        put(r.position, hit.position);
+        put(r.ng, it.ng);
+        put(r.ns, it.ns);
+        put(r.wo, it.wo);
+        put(r.throughput_before, throughput);
+        r.event_flags = LUX_PATH_EVENT_SURFACE_HIT;
+        auto emit = [&](const vec3& after, unsigned termination) {
+            put(r.throughput_after, after);
+            r.termination_flags = termination;
+            if (termination) r.event_flags |= LUX_PATH_EVENT_TERMINATED;
+            out.push_back(r);
+        };
+        const vec3 Le = surface_light_le(lights, hit.triangle_id,
+                                         interpolate_triangle_uv(tri, hit.u, hit.v), hit.ng,
+                                         -ray.direction);
+        if (max_component(Le) > 0 && (emission_uses_unweighted_hit(depth, previous_sample) ||
+                                      emission_uses_mis(previous_sample)))
+            r.event_flags |= LUX_PATH_EVENT_EMISSION;
+        if (is_passthrough_material(material)) {
+            r.event_flags |= LUX_PATH_EVENT_PASSTHROUGH | LUX_PATH_EVENT_DELTA;
+            put(r.wi, normalize(-it.wo));
+            r.bsdf_pdf = 1;
+            r.bsdf_pdf_measure = static_cast<uint8_t>(PdfMeasure::Discrete);
+            r.sample_source = static_cast<uint8_t>(SampleSource::BSDF);
+            r.bsdf_flags = BsdfFlagDeltaTransmission | BsdfFlagTransmission;
+            throughput = apply_passthrough(throughput, material);
+            if (max_component(throughput) <= 0) return emit(throughput, LUX_PATH_END_ZERO_THROUGHPUT);
+            if (step >= max_depth) return emit(throughput, LUX_PATH_END_MAX_DEPTH);
+            r.event_flags |= LUX_PATH_EVENT_SPAWNED_RAY;
+            emit(throughput, 0);
+            ray = spawn_passthrough_ray(hit.position, ray.direction);
+            continue;
+        }
+        if (!material.is_scattering()) return emit(throughput, LUX_PATH_END_NON_SCATTERING);
+        if (step >= max_depth || depth >= max_depth)
+            return emit(throughput, LUX_PATH_END_MAX_DEPTH);
+        if (has_direct_lighting_lobe(material)) {
+            LightSampleContext ctx{it.position, it.ng, it.ns};
+            Float select_u = sampler_get_1d(sampler);
+            Float component_u = sampler_get_1d(sampler);
+            vec2 light_u = sampler_get_2d(sampler);
+            LightLiSample light = sample_light_li(lights, ctx, select_u, component_u, light_u);
+            if (light.valid) {
+                r.event_flags |= LUX_PATH_EVENT_DIRECT_LIGHT_SAMPLED;
+                DirectLightEstimate direct = estimate_unoccluded_direct_light_li(material, it, light);
+                if (direct.pdf_light_solid_angle > 0) {
+                    r.light_pdf = direct.pdf_light_solid_angle;
+                    r.light_pdf_measure = static_cast<uint8_t>(PdfMeasure::SolidAngle);
+                }
+                if (direct.valid) r.event_flags |= LUX_PATH_EVENT_DIRECT_LIGHT_VALID;
+            }
+        }
+        BSDFSample sample = sample_bsdf(material, it, sampler_get_2d(sampler));
+        put(r.wi, sample.wi);
+        r.bsdf_flags = sample.flags;
+        r.event_flags |= LUX_PATH_EVENT_BSDF_SAMPLED;
+        if (is_delta_bsdf(sample.flags)) r.event_flags |= LUX_PATH_EVENT_DELTA;
+        if (sample.pdf > 0) {
+            r.bsdf_pdf = sample.pdf;
+            r.bsdf_pdf_measure = static_cast<uint8_t>(sample.pdf_measure);
+        }
+        if (sample.pdf <= 0 || max_component(sample.weight) <= 0)
+            return emit(throughput, LUX_PATH_END_INVALID_BSDF);
+        vec3 new_throughput = throughput * sample.weight;
+        Float new_eta_scale = eta_scale * bsdf_eta_scale_factor(sample);
+        r.sample_source = static_cast<uint8_t>(SampleSource::BSDF);
+        if (should_apply_russian_roulette(depth)) {
+            Float rr_prob = 1;
+            if (!survives_russian_roulette(depth, new_throughput, new_eta_scale,
+                                           sampler_get_1d(sampler), rr_prob))
+                return emit(new_throughput, LUX_PATH_END_RUSSIAN_ROULETTE);
+            new_throughput /= rr_prob;
+        }
+        r.event_flags |= LUX_PATH_EVENT_SPAWNED_RAY;
+        emit(new_throughput, 0);
+        throughput = new_throughput;
+        eta_scale = new_eta_scale;
+        previous_sample = PreviousSample{sample.pdf, sample.pdf_measure, SampleSource::BSDF,
+                                         sample.flags, hit.position};
+        ray = spawn_scatter_ray(hit.position, it.ng, sample.wi);
+        ++depth;
+    }
+}
+
 // A general single-mesh scene through the reference's own authoring and tracing code:
 // triangles (world space, 9 floats) with material ids; materials as 11 floats each
 // (type, albedo rgb, emission rgb, roughness, metallic, eta, two-sided flag); explicit
@@ -561,6 +686,46 @@ int ref_render_aovs(const float* tris, int ntri, const int32_t* mids, const floa
     copy(ng, ng_out);
     copy(ns, ns_out);
     return 0;
+}
+
+// The path log of a render on a single-mesh scene as ref_render_scene builds it
+// (seed = seed, sample_offset 0): every path's records in (sample, pixel, vertex) order
+// into records (capacity entries); returns the record count, which may exceed capacity
+// (then only the first capacity are written).
+long long ref_path_log(const float* tris, int ntri, const int32_t* mids, const float* mats,
+                       int nmat, const float* lights, int nlights, const float* cam, int width,
+                       int height, int spp, int max_depth, uint64_t seed, int light_sampler,
+                       lux_path_log_record* records, long long capacity) {
+    Scene scene = build_single_mesh_scene(tris, ntri, mids, mats, nmat, lights, nlights, cam,
+                                          nullptr, 0, 0);
+    PreparedScene prepared(std::move(scene));
+    prepared.prepare_host_bvh();
+    SceneLightSampler lights_sampler = make_scene_light_sampler(
+        prepared.host_scene(), prepared.light_sampling(), sampler_kind(light_sampler));
+    RenderSettings settings;
+    settings.max_depth = max_depth;
+    settings.seed = seed;
+    const Scene& sc = prepared.host_scene();
+    std::vector<lux_path_log_record> out;
+    for (int s = 0; s < spp; ++s) {
+        for (int pixel = 0; pixel < width * height; ++pixel) {
+            const int x = pixel % width, y = pixel / width;
+            SamplerState sampler = make_render_sampler(settings, pixel, s);
+            Float jx = sampler_get_1d(sampler);
+            Float jy = sampler_get_1d(sampler);
+            CameraSample cs;
+            cs.p_film = vec2((Float(x) + jx) / Float(width), (Float(height - 1 - y) + jy) / Float(height));
+            cs.p_lens = sampler_get_2d(sampler);
+            cs.time = sampler_get_1d(sampler);
+            CameraRay generated = generate_camera_ray(sc.camera, cs);
+            if (!generated.valid) continue;
+            log_path(sc, prepared.host_bvh(), lights_sampler, generated.ray, sampler, max_depth,
+                     pixel, s, out);
+        }
+    }
+    const long long n = static_cast<long long>(out.size());
+    std::memcpy(records, out.data(), sizeof(lux_path_log_record) * size_t(std::min(n, capacity)));
+    return n;
 }
 
 // ---- OBJ loading and asset scenes
