@@ -332,7 +332,7 @@ def run_lux(args) -> None:
     e2e = None
     cpu_baseline = None
     if rank == 0 and not args.skip_e2e:
-        e2e = measure_e2e(ctx, data, args, dev)
+        e2e = measure_e2e(ctx, data, args, dev, contexts=3)
     if rank == 0 and world == 1 and not args.skip_cpu_baseline:
         cpu_baseline = measure_cpu_baseline(data)
 
@@ -370,8 +370,10 @@ def run_lux(args) -> None:
         dist.destroy_process_group()
 
 
-def measure_e2e(ctx, data, args, dev) -> dict:
-    """The same step through the C ABI with pinned host buffers: copies are timed."""
+def measure_e2e(ctx, data, args, dev, contexts=2, steps=None) -> dict:
+    """The same step through the C ABI with pinned host buffers: copies are timed.
+    contexts: contexts (each on its own host thread) taking the steps in turn; steps:
+    timed steps in all (default: a multiple of contexts near 10)."""
     import torch
 
     import lux_b200
@@ -396,11 +398,13 @@ def measure_e2e(ctx, data, args, dev) -> dict:
     # them; every step still copies its inputs in and its results out.
     import threading
 
-    ctxs = [ctx, lux_b200.Context(dev.index or 0 if hasattr(dev, "index") else int(dev))]
-    outs = [(h_id, h_t, h_pairs, found),
-            (torch.empty(N_RAYS, dtype=torch.int32).pin_memory(),
-             torch.empty(N_RAYS, dtype=torch.float32).pin_memory(),
-             torch.empty((max_pairs, 2), dtype=torch.int32).pin_memory(), np.zeros(1, np.int64))]
+    device = dev.index or 0 if hasattr(dev, "index") else int(dev)
+    ctxs = [ctx] + [lux_b200.Context(device) for _ in range(contexts - 1)]
+    outs = [(h_id, h_t, h_pairs, found)] + [
+        (torch.empty(N_RAYS, dtype=torch.int32).pin_memory(),
+         torch.empty(N_RAYS, dtype=torch.float32).pin_memory(),
+         torch.empty((max_pairs, 2), dtype=torch.int32).pin_memory(), np.zeros(1, np.int64))
+        for _ in range(contexts - 1)]
     trees = [(c.build_lbvh(h_tris), c.build_lbvh(h_queries, kind=lux_b200.PRIM_AABBS))
              for c in ctxs]
 
@@ -420,16 +424,18 @@ def measure_e2e(ctx, data, args, dev) -> dict:
             step(k)
 
     for _ in range(max(args.warmup, 1)):
-        step(0)
-        step(1)
-    steps = max(4, min(args.steps, 10) // 2 * 2)
+        for k in range(contexts):
+            step(k)
+    if steps is None:
+        steps = max(4, min(args.steps, 10) // 2 * 2)
+    steps = max(contexts, steps // contexts * contexts)
     # One context alone: each step's copies and kernels in sequence.
     t0 = time.perf_counter()
     run(0, steps)
     ctx.synchronize()
     serial = (time.perf_counter() - t0) / steps
-    # Both contexts, steps alternating.
-    workers = [threading.Thread(target=run, args=(k, steps // 2)) for k in range(2)]
+    # All contexts, steps taken in turn.
+    workers = [threading.Thread(target=run, args=(k, steps // contexts)) for k in range(contexts)]
     t0 = time.perf_counter()
     for w in workers:
         w.start()
@@ -444,11 +450,12 @@ def measure_e2e(ctx, data, args, dev) -> dict:
     for bvh, qbvh in trees:
         bvh.close()
         qbvh.close()
-    ctxs[1].close()
+    for c in ctxs[1:]:
+        c.close()
     return {"value": N_RAYS / dt / 1e6, "unit": "Mrays/s", "h2d_bytes_per_step": h2d,
             "d2h_bytes_per_step": d2h, "ms_per_step": dt * 1e3, "steps": steps,
             "host_buffers": "pinned",
-            "pipelining": "two contexts on two host threads, steps alternating",
+            "pipelining": f"{contexts} contexts on {contexts} host threads, steps taken in turn",
             "one_context_ms_per_step": serial * 1e3}
 
 

@@ -141,6 +141,82 @@ int finish_call(lux_ctx* ctx, Staging& staging) {
     return lux::cuda_fail(cudaGetLastError(), "launch");
 }
 
+// Host rays of a large query: they go to the device in chunks on the context's copy
+// stream, and each chunk is traced as soon as it has landed while the next is still on
+// the way; host results go back chunk by chunk behind their traces.  Every copy back is
+// issued after every copy in, so a pageable output (whose copy waits for the host) does
+// not hold up the inputs.  Results are per ray, so they equal the one-launch query's.
+constexpr int kPipeChunks = 4;
+constexpr int32_t kPipeMinRays = 1 << 20;
+
+bool use_pipeline(const float* rays, int32_t nrays) {
+    return nrays >= kPipeMinRays && !is_device_pointer(rays);
+}
+
+int ensure_pipeline(lux_ctx* ctx) {
+    if (ctx->copy_stream) return LUX_OK;
+    cudaError_t err = cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking);
+    for (cudaEvent_t& e : ctx->pipe_events)
+        if (err == cudaSuccess) err = cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
+    return lux::cuda_fail(err, "copy stream");
+}
+
+template <bool kAny>
+int trace_pipelined(lux_ctx* ctx, const lux_bvh* bvh, const float* rays, int32_t nrays,
+                    int32_t* hit_id, float* hit_t) {
+    static_assert(2 * kPipeChunks + 2 <= 16, "pipeline events");
+    if (int st = ensure_pipeline(ctx)) return st;
+    const size_t r = static_cast<size_t>(nrays);
+    Staging staging(ctx);  // device room only: the copies are issued here, chunk by chunk
+    void *d_rays = nullptr, *d_id = nullptr, *d_t = nullptr;
+    staging.add(rays, 32 * r, false, false, &d_rays);
+    staging.add(hit_id, 4 * r, false, false, &d_id);
+    if (!kAny) staging.add(hit_t, 4 * r, false, false, &d_t);
+    int st = staging.begin();
+    if (st) return st;
+    const bool id_back = d_id != hit_id;
+    const bool t_back = !kAny && hit_t && d_t != hit_t;
+    cudaStream_t s = ctx->stream, c = ctx->copy_stream;
+    cudaEvent_t* ev = ctx->pipe_events;  // 0 start, 1..K copied in, K+1..2K traced, 2K+1 end
+    const int32_t chunk = (nrays + kPipeChunks - 1) / kPipeChunks;
+    // The copy stream starts after the work already queued on the context's stream.
+    cudaError_t err = cudaEventRecord(ev[0], s);
+    if (err == cudaSuccess) err = cudaStreamWaitEvent(c, ev[0], 0);
+    for (int k = 0; k < kPipeChunks && err == cudaSuccess; ++k) {
+        const int32_t lo = k * chunk, cnt = std::min(chunk, nrays - lo);
+        if (cnt <= 0) break;
+        err = cudaMemcpyAsync(static_cast<char*>(d_rays) + 32 * size_t(lo),
+                              reinterpret_cast<const char*>(rays) + 32 * size_t(lo),
+                              32 * size_t(cnt), cudaMemcpyHostToDevice, c);
+        if (err == cudaSuccess) err = cudaEventRecord(ev[1 + k], c);
+        if (err == cudaSuccess) err = cudaStreamWaitEvent(s, ev[1 + k], 0);
+        if (err != cudaSuccess) break;
+        const float* kr = static_cast<const float*>(d_rays) + 8 * size_t(lo);
+        int* kid = static_cast<int*>(d_id) + lo;
+        st = kAny ? lux::trace_any(ctx, bvh, kr, cnt, kid)
+                  : lux::trace_closest(ctx, bvh, kr, cnt, kid,
+                                       d_t ? static_cast<float*>(d_t) + lo : nullptr);
+        if (st) return st;
+        err = cudaEventRecord(ev[1 + kPipeChunks + k], s);
+    }
+    for (int k = 0; k < kPipeChunks && err == cudaSuccess && (id_back || t_back); ++k) {
+        const int32_t lo = k * chunk, cnt = std::min(chunk, nrays - lo);
+        if (cnt <= 0) break;
+        err = cudaStreamWaitEvent(c, ev[1 + kPipeChunks + k], 0);
+        if (err == cudaSuccess && id_back)
+            err = cudaMemcpyAsync(hit_id + lo, static_cast<int*>(d_id) + lo, 4 * size_t(cnt),
+                                  cudaMemcpyDeviceToHost, c);
+        if (err == cudaSuccess && t_back)
+            err = cudaMemcpyAsync(hit_t + lo, static_cast<float*>(d_t) + lo, 4 * size_t(cnt),
+                                  cudaMemcpyDeviceToHost, c);
+    }
+    // Later work on the context's stream (and the wait below) comes after the copies.
+    if (err == cudaSuccess) err = cudaEventRecord(ev[2 * kPipeChunks + 1], c);
+    if (err == cudaSuccess) err = cudaStreamWaitEvent(s, ev[2 * kPipeChunks + 1], 0);
+    if (err != cudaSuccess) return lux::cuda_fail(err, "chunked ray query");
+    return sync_and_check(ctx);
+}
+
 }  // namespace
 
 namespace lux {
@@ -228,6 +304,12 @@ int lux_ctx_destroy(lux_ctx* ctx) {
     if (ctx->d_error) cudaFree(ctx->d_error);
     if (ctx->d_counter) cudaFree(ctx->d_counter);
     lux::render_runtime_free(ctx);
+    if (ctx->copy_stream) {
+        cudaStreamSynchronize(ctx->copy_stream);
+        cudaStreamDestroy(ctx->copy_stream);
+        for (cudaEvent_t e : ctx->pipe_events)
+            if (e) cudaEventDestroy(e);
+    }
     if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
     delete ctx;
     return LUX_OK;
@@ -493,6 +575,7 @@ int lux_trace_closest(lux_ctx* ctx, const lux_bvh* bvh, const float* rays, int32
                       int32_t* hit_id, float* hit_t) {
     if (int st = check_query(ctx, bvh, rays, nrays)) return st;
     if (nrays > 0 && !hit_id) return lux::fail(LUX_ERR_INVALID_ARGUMENT, "null hit_id");
+    if (use_pipeline(rays, nrays)) return trace_pipelined<false>(ctx, bvh, rays, nrays, hit_id, hit_t);
     Staging staging(ctx);
     void *d_rays, *d_id, *d_t;
     size_t r = static_cast<size_t>(nrays);
@@ -529,6 +612,7 @@ int lux_trace_any(lux_ctx* ctx, const lux_bvh* bvh, const float* rays, int32_t n
                   int32_t* hit_id) {
     if (int st = check_query(ctx, bvh, rays, nrays)) return st;
     if (nrays > 0 && !hit_id) return lux::fail(LUX_ERR_INVALID_ARGUMENT, "null hit_id");
+    if (use_pipeline(rays, nrays)) return trace_pipelined<true>(ctx, bvh, rays, nrays, hit_id, nullptr);
     Staging staging(ctx);
     void *d_rays, *d_id;
     size_t r = static_cast<size_t>(nrays);

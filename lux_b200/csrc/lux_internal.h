@@ -27,6 +27,9 @@ struct lux_ctx {
     // Growable device staging for host inputs / outputs.
     void* staging = nullptr;
     size_t staging_bytes = 0;
+    // Copy stream and events of the chunked host-ray queries (created on first use).
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t pipe_events[16] = {};
 };
 
 struct lux_bvh {

@@ -229,6 +229,49 @@ def test_device_pointers_stream_ordered(ctx, oracle):
         ctx.set_stream(None)
 
 
+def test_chunked_host_ray_queries_equal_one_launch(ctx, oracle):
+    """Host rays of a query of 1M rays or more are copied in chunks, each traced as it
+    lands: results equal the one-launch query over device rays, for host (pinned or
+    pageable) and device outputs, without hit distances, and for any-hit."""
+    torch = pytest.importorskip("torch")
+    tris = W.soup_triangles(200_000, seed=21)
+    n = (1 << 20) + 12_345                      # a ragged last chunk
+    rays = W.uniform_rays(n, seed=22)
+    bvh = ctx.build_lbvh(tris)
+    dr = torch.from_numpy(rays).cuda()
+    want_id = torch.empty(n, dtype=torch.int32, device="cuda")
+    want_t = torch.empty(n, dtype=torch.float32, device="cuda")
+    bvh.trace_closest(dr, want_id, want_t)
+    want_any = torch.empty(n, dtype=torch.int32, device="cuda")
+    bvh.trace_any(dr, want_any)
+    torch.cuda.synchronize()
+    want_id, want_t, want_any = (x.cpu().numpy() for x in (want_id, want_t, want_any))
+    # The one-launch query itself, on a sample, against the oracle.
+    sample = rays[:4096]
+    o_id, o_t = oracle.trace(tris, oracle.build(oracle.triangle_bounds(tris)), sample)
+    assert np.array_equal(want_id[:4096], o_id) and np.array_equal(want_t[:4096], o_t)
+    for rounds in range(2):
+        hid, ht = bvh.trace_closest(rays)                        # pageable host buffers
+        assert np.array_equal(hid, want_id) and np.array_equal(ht, want_t)
+    pinned_rays = torch.from_numpy(rays).pin_memory()
+    p_id = torch.empty(n, dtype=torch.int32).pin_memory()
+    p_t = torch.empty(n, dtype=torch.float32).pin_memory()
+    bvh.trace_closest(pinned_rays, p_id, p_t)
+    assert np.array_equal(p_id.numpy(), want_id) and np.array_equal(p_t.numpy(), want_t)
+    only_id = np.empty(n, np.int32)
+    lux_b200._check(ctx._lib.lux_trace_closest(ctx._h, bvh._h, rays.ctypes.data, n,
+                                               only_id.ctypes.data, None))
+    assert np.array_equal(only_id, want_id)
+    d_id = torch.empty(n, dtype=torch.int32, device="cuda")
+    d_t = torch.empty(n, dtype=torch.float32, device="cuda")
+    bvh.trace_closest(rays, d_id, d_t)                           # host rays, device hits
+    torch.cuda.synchronize()
+    assert np.array_equal(d_id.cpu().numpy(), want_id)
+    assert np.array_equal(d_t.cpu().numpy(), want_t)
+    assert np.array_equal(bvh.trace_any(rays), want_any)
+    assert (want_id >= 0).any() and (want_id < 0).any()
+
+
 def test_full_size_microbench_properties(ctx):
     """1,048,576 triangles / 4,194,304 rays: size-independent checks at full size."""
     data = W.lbvh_microbench(n_rays=1 << 22)
