@@ -335,6 +335,9 @@ def run_lux(args) -> None:
         e2e = measure_e2e(ctx, data, args, dev, contexts=3)
     if rank == 0 and world == 1 and not args.skip_cpu_baseline:
         cpu_baseline = measure_cpu_baseline(data)
+    reference_gpu = None
+    if rank == 0 and world == 1 and not args.skip_reference_gpu:
+        reference_gpu = measure_reference_gpu(data)
 
     line = {
         "metric": METRIC, "value": value, "unit": "Mrays/s", "n_gpus": world,
@@ -362,6 +365,7 @@ def run_lux(args) -> None:
         "wall_s_timed_region": wall,
         "e2e": e2e,
         "cpu_baseline": cpu_baseline,
+        "reference_gpu": reference_gpu,
     }
     if rank == 0:
         print(json.dumps(line))
@@ -457,6 +461,33 @@ def measure_e2e(ctx, data, args, dev, contexts=2, steps=None) -> dict:
             "host_buffers": "pinned",
             "pipelining": f"{contexts} contexts on {contexts} host threads, steps taken in turn",
             "one_context_ms_per_step": serial * 1e3}
+
+
+def measure_reference_gpu(data) -> dict | None:
+    """The same step on the reference's own GPU code (build_gpu_lbvh,
+    intersect_gpu_bvh_stackless, refit_gpu_lbvh, query_aabb_overlaps_cross) compiled for
+    sm_100a, on the same B200 and inputs: medians of 3 runs after one untimed run.  Its
+    API takes and returns host vectors, so its step includes its copies; the kernel-only
+    trace time is reported beside it."""
+    try:
+        from oracle.bindings import RefGpu
+    except Exception:
+        return None
+    if not RefGpu.available():
+        return None
+    try:
+        ms, found = RefGpu().microbench(data["triangles"], data["rays"], data["refit_triangles"],
+                                        data["queries"], max_pairs=1 << 21, reps=3)
+    except Exception as e:  # the reference threw: report it, keep this build's line
+        return {"unavailable": str(e)}
+    step = ms["build"] + ms["trace_api"] + ms["refit"] + ms["query_build"] + ms["overlap"]
+    return {"kind": "reference GPU code (bvh/gpu_bvh.cu, bvh/bvh_overlap.cu) for sm_100a",
+            "step_ms": step, "step_mrays_s": N_RAYS / (step * 1e-3) / 1e6,
+            "trace_kernel_mrays_s": N_RAYS / (ms["trace_kernel"] * 1e-3) / 1e6,
+            "lbvh_mtri_s": N_TRIS / (ms["build"] * 1e-3) / 1e6,
+            "phases_ms": ms, "overlap_pairs": found,
+            "timing": "host clock around each API call (copies included); trace kernel by "
+                      "CUDA events with L2 flushed"}
 
 
 def measure_cpu_baseline(data) -> dict | None:
@@ -891,6 +922,8 @@ def main():
     ap.add_argument("--impl", default="lux", choices=["lux", "reference"])
     ap.add_argument("--skip-e2e", action="store_true")
     ap.add_argument("--skip-cpu-baseline", action="store_true")
+    ap.add_argument("--skip-reference-gpu", action="store_true",
+                    help="lbvh: skip timing the reference's own GPU LBVH code")
     ap.add_argument("--tris", type=int, default=N_TRIS,
                     help="smaller cases for profiling captures only")
     ap.add_argument("--rays", type=int, default=N_RAYS)

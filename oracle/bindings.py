@@ -17,6 +17,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_LIB = os.path.join(HERE, "liblux_oracle.so")
 REF_LIB = os.path.join(HERE, "_ref", "libluxref.so")
+REF_GPU_LIB = os.path.join(HERE, "_ref", "libluxrefgpu.so")
 PT64_LIB = os.path.join(HERE, "liblux_pt64.so")
 
 _P = ctypes.c_void_p
@@ -395,3 +396,53 @@ class PT64:
     @staticmethod
     def available() -> bool:
         return os.path.exists(PT64_LIB)
+
+
+class RefGpu:
+    """The reference's own GPU LBVH (build_gpu_lbvh, intersect_gpu_bvh_stackless,
+    refit_gpu_lbvh, query_aabb_overlaps_cross) compiled for sm_100a."""
+
+    def __init__(self, path: str = REF_GPU_LIB):
+        if not os.path.exists(path):
+            raise FileNotFoundError(f"{path} missing (built only where the reference exists)")
+        lib = ctypes.CDLL(path)
+        lib.refgpu_last_error.restype = ctypes.c_char_p
+        lib.refgpu_trace.argtypes = [_P, _I, _P, _I, _P, _P]
+        lib.refgpu_trace.restype = _I
+        lib.refgpu_microbench.argtypes = [_P, _I, _P, _I, _P, _P, _I, _I, _I, _P, _P]
+        lib.refgpu_microbench.restype = _I
+        self.lib = lib
+
+    @staticmethod
+    def available(path: str = REF_GPU_LIB) -> bool:
+        return os.path.exists(path)
+
+    def _check(self, status):
+        if status != 0:
+            raise RuntimeError("reference GPU code: " + self.lib.refgpu_last_error().decode())
+
+    def trace(self, tris, rays):
+        """Closest hits (ids, t) of rays (8 floats each) against triangles (9 floats each)."""
+        tris = np.ascontiguousarray(tris, np.float32).reshape(-1, 9)
+        rays = np.ascontiguousarray(rays, np.float32).reshape(-1, 8)
+        hid = np.empty(len(rays), np.int32)
+        ht = np.empty(len(rays), np.float32)
+        self._check(self.lib.refgpu_trace(tris.ctypes.data, len(tris), rays.ctypes.data,
+                                          len(rays), hid.ctypes.data, ht.ctypes.data))
+        return hid, ht
+
+    def microbench(self, tris, rays, refit_tris, queries, max_pairs=1 << 21, reps=3):
+        """Median ms of each phase of the LBVH microbench step (refgpu_microbench) and the
+        overlap count."""
+        tris = np.ascontiguousarray(tris, np.float32).reshape(-1, 9)
+        rays = np.ascontiguousarray(rays, np.float32).reshape(-1, 8)
+        refit = np.ascontiguousarray(refit_tris, np.float32).reshape(-1, 9)
+        queries = np.ascontiguousarray(queries, np.float32).reshape(-1, 6)
+        times = np.zeros(6, np.float64)
+        found = np.zeros(1, np.int64)
+        self._check(self.lib.refgpu_microbench(tris.ctypes.data, len(tris), rays.ctypes.data,
+                                               len(rays), refit.ctypes.data, queries.ctypes.data,
+                                               len(queries), max_pairs, reps, times.ctypes.data,
+                                               found.ctypes.data))
+        names = ("build", "trace_api", "trace_kernel", "refit", "query_build", "overlap")
+        return dict(zip(names, times.tolist())), int(found[0])

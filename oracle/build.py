@@ -3,6 +3,8 @@
 1. oracle/liblux_oracle.so: the plain-C restatement in oracle/lux_oracle.c.
 2. oracle/liblux_pt64.so: the FP64 path-tracing oracle in oracle/pt64.c.
 3. oracle/_ref/libluxref.so: the reference's own host code.
+4. oracle/_ref/libluxrefgpu.so: the reference's own GPU LBVH (bvh/gpu_bvh.cu,
+   bvh/bvh_overlap.cu) behind oracle/ref_gpu_harness.cu, compiled with nvcc for sm_100a.
 
 Compiles, in place and without the reference's build system, the handful of
 reference translation units the CPU path needs (integrator/cpu_path_tracer.cpp,
@@ -74,8 +76,34 @@ def build_ref(force=False):
     return OUT
 
 
+REF_GPU_OUT = os.path.join(OUT_DIR, "libluxrefgpu.so")
+REF_GPU_SOURCES = ["src/bvh/bvh_overlap.cu"]
+REF_GPU_HEADERS = ["src/bvh/gpu_bvh.cu", "src/bvh/gpu_bvh.cuh", "src/bvh/bvh_device.cuh"]
+# The reference's stock CUDA configuration (CMakeLists.txt: C++20, Release -O3,
+# LUX_ENABLE_CUDA=1); nvcc's default contraction is kept, as the reference builds.
+NVCCFLAGS = ["-std=c++20", "-O3", "-DLUX_ENABLE_CUDA=1",
+             "-gencode", "arch=compute_100a,code=sm_100a", "-Xcompiler", "-fPIC"]
+
+
+def build_ref_gpu(force=False):
+    """Compile the reference's GPU LBVH harness; None when the reference is absent."""
+    src_dir = os.path.join(REF_ROOT, "src")
+    if not os.path.isdir(src_dir):
+        return None
+    harness = os.path.join(HERE, "ref_gpu_harness.cu")
+    inputs = [harness] + [os.path.join(REF_ROOT, s) for s in REF_GPU_SOURCES]
+    deps = inputs + [os.path.join(REF_ROOT, s) for s in REF_GPU_HEADERS]
+    if not force and not _stale(REF_GPU_OUT, deps):
+        return REF_GPU_OUT
+    os.makedirs(OUT_DIR, exist_ok=True)
+    cmd = ["nvcc", *NVCCFLAGS, "-shared", "-I", src_dir, "-o", REF_GPU_OUT, *inputs]
+    subprocess.run(cmd, check=True)
+    return REF_GPU_OUT
+
+
 def build(force=False):
     build_pt64(force)
+    build_ref_gpu(force)
     return build_oracle(force), build_ref(force)
 
 

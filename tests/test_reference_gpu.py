@@ -1,0 +1,36 @@
+"""lux_b200's LBVH queries against the reference's OWN GPU code (build_gpu_lbvh +
+intersect_gpu_bvh_stackless, bvh/gpu_bvh.cu, compiled for sm_100a by oracle/build.py)
+run on the same B200: the hits lux_b200 returns are the ones the reference's GPU path
+returns for the same triangles and rays."""
+import numpy as np
+import pytest
+
+from lux_b200 import workloads as W
+from oracle.bindings import RefGpu
+
+pytestmark = [pytest.mark.gpu,
+              pytest.mark.skipif(not RefGpu.available(), reason="reference GPU harness not built")]
+
+
+@pytest.mark.parametrize("ntri,nrays,seed", [(1, 64, 1), (1000, 20_000, 2), (100_000, 200_000, 3)])
+def test_hits_equal_reference_gpu_code(ctx, ntri, nrays, seed):
+    tris = W.soup_triangles(ntri, seed=30 + seed)
+    rays = W.uniform_rays(nrays, seed=40 + seed).reshape(-1, 8)
+    if ntri == 1:  # aim the rays at the lone triangle's centroid
+        d = tris.reshape(3, 3).mean(axis=0) - rays[:, 0:3]
+        rays[:, 4:7] = d / np.linalg.norm(d, axis=1, keepdims=True)
+    want_id, want_t = RefGpu().trace(tris, rays)
+    got_id, got_t = ctx.build_lbvh(tris).trace_closest(rays)
+    assert (want_id >= 0).any()
+    # The reference's GPU build keeps nvcc's default contraction, so its triangle test
+    # fuses multiply-adds that the reference's host code (which lux_b200 matches bit for
+    # bit) rounds separately; with the cancellation in the edge cross products its
+    # distances differ from the host-exact ones by up to a few parts in a million, and a
+    # ray grazing a triangle edge or two nearly equidistant triangles may get the other
+    # answer (1 ray in 200,000 here).  So: the same result on all but 0.01 % of the
+    # rays, and the same distance to 1e-5 wherever both name the same triangle.
+    same = got_id == want_id
+    assert same.mean() >= 0.9999
+    both = same & (want_id >= 0)
+    assert both.sum() > 0.5 * (want_id >= 0).sum()
+    np.testing.assert_allclose(got_t[both], want_t[both], rtol=1e-5, atol=0)
