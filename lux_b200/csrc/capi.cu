@@ -196,7 +196,10 @@ int trace_pipelined(lux_ctx* ctx, const lux_bvh* bvh, const float* rays, int32_t
         st = kAny ? lux::trace_any(ctx, bvh, kr, cnt, kid)
                   : lux::trace_closest(ctx, bvh, kr, cnt, kid,
                                        d_t ? static_cast<float*>(d_t) + lo : nullptr);
-        if (st) return st;
+        if (st) {
+            cudaStreamSynchronize(c);  // no copy may still read the caller's rays
+            return st;
+        }
         err = cudaEventRecord(ev[1 + kPipeChunks + k], s);
     }
     for (int k = 0; k < kPipeChunks && err == cudaSuccess && (id_back || t_back); ++k) {
@@ -213,7 +216,10 @@ int trace_pipelined(lux_ctx* ctx, const lux_bvh* bvh, const float* rays, int32_t
     // Later work on the context's stream (and the wait below) comes after the copies.
     if (err == cudaSuccess) err = cudaEventRecord(ev[2 * kPipeChunks + 1], c);
     if (err == cudaSuccess) err = cudaStreamWaitEvent(s, ev[2 * kPipeChunks + 1], 0);
-    if (err != cudaSuccess) return lux::cuda_fail(err, "chunked ray query");
+    if (err != cudaSuccess) {
+        cudaStreamSynchronize(c);
+        return lux::cuda_fail(err, "chunked ray query");
+    }
     return sync_and_check(ctx);
 }
 
