@@ -464,7 +464,9 @@ typedef struct lux_path_log_record {
  * appends in device-atomic order).  A render with more vertices than capacity returns
  * LUX_ERR_QUEUE_OVERFLOW with *count set and records unspecified (the reference
  * throws).  Per path at most max_depth + 1 vertices, so width * height * spp *
- * (max_depth + 1) always suffices.
+ * (max_depth + 1) always suffices.  The records pass through the context's device
+ * staging, which keeps capacity * 152 bytes allocated until the context is destroyed
+ * (or a larger staged call replaces it): size capacity for the renders logged.
  */
 int lux_render_path_log(lux_ctx* ctx, const lux_scene* scene, const lux_render_request* req,
                         float* film_sum, lux_path_log_record* records, int64_t capacity,

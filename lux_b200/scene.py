@@ -372,7 +372,9 @@ END_RUSSIAN_ROULETTE, END_ZERO_THROUGHPUT = 8, 16
 def render_path_log(ctx, scene: Scene, req: RenderRequest, capacity=None):
     """Film sum and the path log of one render (lux_render_path_log): a structured array
     of PATH_LOG_RECORD sorted by (sample_index, pixel_index, vertex).  capacity defaults
-    to the bound width * height * spp * (max_depth + 1)."""
+    to the bound width * height * spp * (max_depth + 1), at 152 bytes a record on the
+    host and in the context's device staging: pass a smaller one for large renders
+    (an exhausted capacity raises LuxError with status 6)."""
     if capacity is None:
         capacity = req.width * req.height * req.spp * (req.max_depth + 1)
     film = np.zeros((req.height, req.width, 3), np.float32)
