@@ -224,7 +224,9 @@ int lux_lbvh_morton_sort_static(lux_ctx* ctx, const float* prims, int32_t n, int
 /*
  * Closest hit of each ray against a triangle BVH.  Visits nodes in the reference's
  * stackless order (bvh/bvh_device.cuh:43-90: left child first, strict t < best), so
- * equal-t ties resolve exactly as the reference GPU path does.  No hit: id -1, t +inf.
+ * equal-t ties resolve exactly as in the reference; arithmetic is the reference host
+ * code's (no multiply-add contraction), so ids and t equal that code's bit for bit.
+ * No hit: id -1, t +inf.
  * hit_t may be NULL.  With 1,048,576 or more rays in host memory the rays are copied in
  * four chunks on a second stream of the context, each traced as soon as it lands, and
  * host results return chunk by chunk (same results as one launch; lux_trace_any too).
