@@ -123,6 +123,22 @@ def test_oracle_log_rules():
     assert len(kinds) >= 7
 
 
+@needs_ref
+def test_oracle_log_capacity():
+    """ref_path_log reports every record and writes no more than its capacity."""
+    b, cam = log_scene(8, 8)
+    full, args = _ref_log(b, cam, 8, 8, 2, 4, 1, S.SAMPLER_POWER)
+    tris, mids, mats, lights, camera = args[:5]
+    out = np.zeros(8 + 4, S.PATH_LOG_RECORD)
+    out["pixel_index"] = -7
+    lib = Ref().lib
+    n = lib.ref_path_log(tris.ctypes.data, len(tris), mids.ctypes.data, mats.ctypes.data,
+                         len(mats), lights.ctypes.data, len(lights), camera.ctypes.data, 8, 8,
+                         2, 4, 1, S.SAMPLER_POWER, out.ctypes.data, 8)
+    assert n == len(full) > 8
+    assert np.array_equal(out[:8], full[:8]) and np.all(out["pixel_index"][8:] == -7)
+
+
 # --------------------------------------------------------------------- GPU parity
 
 def _compare(got, want, min_match=0.99):

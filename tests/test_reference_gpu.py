@@ -8,10 +8,19 @@ import pytest
 from lux_b200 import workloads as W
 from oracle.bindings import RefGpu
 
-pytestmark = [pytest.mark.gpu,
-              pytest.mark.skipif(not RefGpu.available(), reason="reference GPU harness not built")]
+needs_harness = pytest.mark.skipif(not RefGpu.available(), reason="reference GPU harness not built")
 
 
+@needs_harness
+def test_harness_loads_and_exports_its_entry_points():
+    """Loads without a GPU call (no compute here): the symbols the bench and tests use."""
+    lib = RefGpu().lib
+    for name in ("refgpu_trace", "refgpu_microbench", "refgpu_last_error"):
+        assert hasattr(lib, name)
+
+
+@pytest.mark.gpu
+@needs_harness
 @pytest.mark.parametrize("ntri,nrays,seed", [(1, 64, 1), (1000, 20_000, 2), (100_000, 200_000, 3)])
 def test_hits_equal_reference_gpu_code(ctx, ntri, nrays, seed):
     tris = W.soup_triangles(ntri, seed=30 + seed)
