@@ -169,9 +169,11 @@ def run_reference(args) -> None:
         "impl": "reference",
         "metric": METRIC, "value": value, "unit": "Mrays/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": step_s * 1e3, "higher_is_better": True, "scaling": "weak",
+        "ms_per_step": step_s * 1e3,
+        "ms_per_step_kind": "extrapolated from bounded samples of the step (see sample)",
+        "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": WORKLOAD},
+        "config": lbvh_config(args.gpus),
         "cpu_baseline": {
             "value": value, "unit": "Mrays/s", "cores": threads, "kind": "reference",
             "sample": (f"reference host code: full 1,048,576-triangle builds (1 thread), "
@@ -187,6 +189,12 @@ def run_reference(args) -> None:
 
 
 # ------------------------------------------------------------------ GPU arm
+
+def lbvh_config(world: int) -> dict:
+    """The LBVH microbench's config dict, identical in both arms."""
+    return {"workload": WORKLOAD, "l2": "flushed between timed steps (256 MiB write)",
+            "parallelism": f"replicas x{world}" if world > 1 else "single GPU"}
+
 
 def max_over_ranks(value: float, dist, device) -> float:
     """The largest per-rank value: a multi-GPU step lasts as long as its slowest rank.
@@ -344,8 +352,7 @@ def run_lux(args) -> None:
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_ms,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "l2": "flushed between timed steps (256 MiB write)",
-                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+        "config": lbvh_config(world),
         "phases_ms": phase_ms,
         "lbvh_mtri_s": N_TRIS / (phase_ms["build"] * 1e-3) / 1e6,
         "trace_mrays_s": N_RAYS / (phase_ms["trace"] * 1e-3) / 1e6,
@@ -367,6 +374,12 @@ def run_lux(args) -> None:
         "cpu_baseline": cpu_baseline,
         "reference_gpu": reference_gpu,
     }
+    if rank == 0 and world == 1 and not args.skip_render:
+        # The path-tracer half (configs 1, 3, 4 and 5), each with its own timing, after
+        # the LBVH microbench's timed steps.
+        bvh.close()
+        qbvh.close()
+        line["render_configs"] = render_suite(args)
     if rank == 0:
         print(json.dumps(line))
     if dist:
@@ -520,16 +533,6 @@ def _render_setup(local=0):
     return torch, lux_b200.Context(local, stream.cuda_stream), stream
 
 
-def _reference_scene_arrays(b):
-    """A SceneBuilder as the reference harness's single-mesh arrays (world triangles)."""
-    tris = b.world_triangles()
-    mids = b.world_material_ids()
-    mats = np.array([[m.type, *m.albedo, *m.emission, m.roughness, m.metallic, m.eta,
-                      m.emission_two_sided] for m in b.materials], np.float32)
-    lights = np.array([[l.kind, *l.vec, *l.value] for l in b.lights], np.float32).reshape(-1, 7)
-    return tris, mids, mats, lights
-
-
 RENDER_CONFIGS = {
     # name: (width, height, spp, depth, seed, metric, workload)
     "cornell": (256, 256, 64, 4, 1, "Mrays/s (Cornell 256^2, 64 spp, depth 4)",
@@ -540,14 +543,81 @@ RENDER_CONFIGS = {
               "seed 1"),
 }
 
+# Render roofline, algorithmic bytes: per traced ray (camera, extension or shadow segment)
+# the ray (32 B) and its hit (8 B), 32 B per node box and 36 B per triangle the reference's
+# visit order tests; per bounce the minimal path state read and written once (throughput
+# 12, radiance 12, pixel 4, depth/flags 4, eta 4, previous pdf and position 16, RNG 16 =
+# 68 B, twice); per path its 12-byte film contribution.
+RAY_BYTES = 40
+PATH_STATE_BYTES_PER_BOUNCE = 2 * 68
+FILM_BYTES_PER_PATH = 12
+# The Cornell render's kernels run from L1 (a 71-node BLAS): its bound is instruction
+# issue, measured by ncu as the issue-active fraction of the dominant bounce kernel
+# (profiles/render_kernels_cornell_c1.md).
+CORNELL_ISSUE_ACTIVE = None
 
-def run_render(args, name: str) -> None:
+
+def render_roofline(stats: dict, paths: int, seconds: float, scale: float = 1.0,
+                    kernel: str = "all bounce kernels of the render") -> dict:
+    """HBM roofline of a render from its traversal statistics (lux_render_traversal_stats):
+    algorithmic bytes / device time.  scale: timed rays / counted rays, when the counts
+    come from a sample of the timed work."""
+    rays = stats["rays"] + stats["shadow_segments"]
+    alg = (RAY_BYTES * rays + 32 * stats["box_tests"] + 36 * stats["tri_tests"]
+           + PATH_STATE_BYTES_PER_BOUNCE * stats["rays"] + FILM_BYTES_PER_PATH * paths) * scale
+    peak, peak_kind = measured_peaks()
+    achieved = alg / seconds / 1e9
+    return {"bound": "hbm", "kernel": kernel, "achieved": achieved, "peak": peak,
+            "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak, "traffic": None,
+            "algorithmic_bytes_per_step": alg,
+            "algorithmic_bytes_per_ray": alg / (rays * scale) if rays else None,
+            "box_tests_per_ray": stats["box_tests"] / rays if rays else None,
+            "tri_tests_per_ray": stats["tri_tests"] / rays if rays else None,
+            "instance_visits_per_ray": stats["instance_visits"] / rays if rays else None,
+            "counts": "lux_render_traversal_stats: the reference's visit order, shadow "
+                      "segments walked to their closest hit"}
+
+
+def reference_gpu_render(builder, req, ours_ms, ours_rays, batch=0) -> dict | None:
+    """The reference's own GPU wavefront tracer (oracle/_ref/libluxrefpt.so:
+    PreparedScene::prepare_gpu + WavefrontPathTracer::render, its stock 65,536-path
+    batches) on the same scene and request: one untimed render, then the median of three
+    by CUDA events.  Its rays are counted as this build's for the same request (the same
+    random streams; the reference counts none)."""
+    try:
+        from oracle.bindings import RefPt
+    except Exception:
+        return None
+    if not RefPt.available():
+        return None
+    try:
+        ref = RefPt()
+        handle = ref.scene(builder)
+        try:
+            ref.render(handle, req, batch)
+            runs = [ref.render(handle, req, batch) for _ in range(3)]
+        finally:
+            ref.destroy(handle)
+    except Exception as e:  # the reference threw: report it, keep this build's line
+        return {"unavailable": str(e)}
+    ms = statistics.median(r[1] for r in runs)
+    host_ms = statistics.median(r[2] for r in runs)
+    return {"kind": "reference GPU wavefront tracer (integrator/wavefront_*.cu) for sm_100a",
+            "request": f"{req.width}x{req.height}, {req.spp} spp, depth {req.max_depth}",
+            "ms": ms, "host_ms": host_ms, "mrays_s": ours_rays / (ms * 1e-3) / 1e6,
+            "this_build_ms": ours_ms, "this_build_mrays_s": ours_rays / (ours_ms * 1e-3) / 1e6,
+            "speedup": ms / ours_ms,
+            "timing": "CUDA events around WavefrontPathTracer::render (its film copied to the "
+                      "host inside); rays counted by this build for the same request"}
+
+
+def render_line(args, name: str, steps: int, warmup: int, nested: bool = False) -> dict:
     """Config 1 (Cornell) or config 3 (heavy render): one lux_render per step.  Under
     torchrun (N > 1) the frame's samples are split across the ranks and their films are
     summed with one NCCL reduce (lux_b200.distributed): strong scaling of one frame."""
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
+    world = 1 if nested else int(os.environ.get("WORLD_SIZE", "1"))
+    rank = 0 if nested else int(os.environ.get("RANK", "0"))
+    local = 0 if nested else int(os.environ.get("LOCAL_RANK", "0"))
     torch, ctx, stream = _render_setup(local)
     dist = None
     if world > 1:
@@ -560,7 +630,8 @@ def run_render(args, name: str) -> None:
     from lux_b200 import scenes as SC
 
     W, H, spp, depth, seed, metric, workload = RENDER_CONFIGS[name]
-    if args.render_size or args.render_spp:  # reduced profiling case of the same scene
+    reduced = bool(args.render_size or args.render_spp) and not nested
+    if reduced:  # reduced profiling case of the same scene
         W = H = args.render_size or W
         spp = args.render_spp or spp
         workload = f"{workload} (reduced profiling case: {W}x{H}, {spp} spp)"
@@ -581,7 +652,7 @@ def run_render(args, name: str) -> None:
         else:
             D.render_sharded(lambda q, f: S.render(ctx, sc, q, f), req, target)
 
-    for _ in range(max(args.warmup, 1)):
+    for _ in range(max(warmup, 1)):
         step(film)
     torch.cuda.synchronize()
     if dist:
@@ -591,7 +662,7 @@ def run_render(args, name: str) -> None:
     clocks.start()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
-    for _ in range(args.steps):
+    for _ in range(steps):
         step(film)
     e1.record(stream)
     torch.cuda.synchronize()
@@ -599,7 +670,7 @@ def run_render(args, name: str) -> None:
         dist.barrier()
     clock_info = clocks.stop()
     launches = ctx.launch_count() - launches0
-    ms = e0.elapsed_time(e1) / args.steps
+    ms = e0.elapsed_time(e1) / steps
     rays = list(S.ray_counts(ctx))
     if dist:  # the whole frame's rays, the slowest rank's time
         t = torch.tensor(rays, dtype=torch.float64, device=film.device)
@@ -610,7 +681,7 @@ def run_render(args, name: str) -> None:
     value = total_rays / (ms * 1e-3) / 1e6
     # e2e: the frame's film on the host (device -> host copy timed; rank 0 receives it).
     host_film = np.zeros((H, W, 3), np.float32)
-    e2e_steps = max(1, min(args.steps, 10 if name == "cornell" else 2))
+    e2e_steps = max(1, min(steps, 10 if name == "cornell" else 2))
     if dist:
         dist.barrier()
     t0 = time.perf_counter()
@@ -633,49 +704,72 @@ def run_render(args, name: str) -> None:
         if Ref.available():
             threads = os.cpu_count() or 1
             rows = 32 if name == "cornell" else 2
-            t0 = time.perf_counter()
-            if name == "cornell":
-                Ref().cornell_render(W, H, spp, depth, seed, rows=(0, rows), threads=threads)
-            else:
-                tris, mids, mats, lights = _reference_scene_arrays(builder)
-                cam = np.array([0, 1, 3.35, 0, 1, 0.9, 40.0, np.float32(W) / np.float32(H)],
-                               np.float32)
-                Ref().render_scene(tris, mids, mats, lights, cam, W, H, spp, depth, seed,
-                                   rows=(H // 2, H // 2 + rows), threads=threads)
-            cpu_s = time.perf_counter() - t0
-            if name != "cornell":
-                # Subtract the harness's scene set-up and host BVH build (a call with no rows).
+            ref = Ref()
+            handle = ref.desc_scene(builder)
+            try:
                 t0 = time.perf_counter()
-                Ref().render_scene(tris, mids, mats, lights, cam, W, H, spp, depth, seed,
-                                   rows=(0, 0), threads=threads)
-                cpu_s -= time.perf_counter() - t0
-            cpu_s *= H / rows
+                ref.desc_render(handle, req, rows=(H // 2, H // 2 + rows), threads=threads)
+                cpu_s = (time.perf_counter() - t0) * H / rows
+            finally:
+                ref.desc_scene_destroy(handle)
             cpu = {"value": total_rays / cpu_s / 1e6, "unit": "Mrays/s", "cores": threads,
                    "kind": "reference",
                    "sample": f"reference trace_path on {rows} of {H} rows ({threads} threads), "
-                             "scaled to the frame; ray count of the same config"
-                             + ("" if name == "cornell" else "; host BVH build excluded")}
+                             "scaled to the frame; ray count of the same config; host BVH "
+                             "build excluded"}
+    # Traversal statistics for the roofline: the Cornell frame itself; the heavy frame at
+    # 16 spp, scaled to the timed rays.
+    roofline = None
+    if rank == 0 and world == 1:
+        stats_req = req if name == "cornell" or reduced else S.request(W, H, 16, depth, seed)
+        st = S.traversal_stats(ctx, sc, stats_req)
+        scale = total_rays / (st["rays"] + st["shadow_segments"])
+        roofline = render_roofline(st, W * H * spp, ms * 1e-3 / max(world, 1), scale)
+        roofline["counted_on"] = f"{stats_req.width}x{stats_req.height}, {stats_req.spp} spp"
+        if name == "cornell":
+            roofline["note"] = ("the scene (36 triangles, 71 BVH nodes) is L1-resident: the "
+                                "render is bound by instruction issue, not HBM")
+            roofline["issue_active_frac_ncu"] = CORNELL_ISSUE_ACTIVE
     # Image error against the FP64 high-spp oracle (tests/golden/make_fp64.py): relative
     # RMSE and measured / noise-predicted MSE (1 for an unbiased renderer).
     fp64 = None
-    fixture = os.path.join(os.path.dirname(os.path.abspath(__file__)), "tests", "golden",
-                           f"{name}_fp64.npz")
-    if rank == 0 and os.path.exists(fixture) and not (args.render_size or args.render_spp):
+    fixture = os.path.join(ROOT, "tests", "golden", f"{name}_fp64.npz")
+    if rank == 0 and os.path.exists(fixture) and not reduced:
         g = np.load(fixture)
         x0, y0, x1, y1 = (int(v) for v in g["rect"]) if "rect" in g else (0, 0, W, H)
         img = film.double().cpu().numpy()[y0:y1, x0:x1] / spp
-        ref = g["mean"].astype(np.float64)
+        ref_img = g["mean"].astype(np.float64)
         var = g["var"].astype(np.float64)
-        mse = float(np.mean((img - ref) ** 2))
+        mse = float(np.mean((img - ref_img) ** 2))
         oracle_noise = float(np.mean(var / int(g["spp"])))
-        rms = float(np.sqrt(np.mean(ref ** 2)))
+        rms = float(np.sqrt(np.mean(ref_img ** 2)))
         fp64 = {"relative_rmse": float(np.sqrt(max(mse - oracle_noise, 0.0))) / rms,
                 "relative_rmse_raw": float(np.sqrt(mse)) / rms,
                 "mse_over_noise": mse / (float(np.mean(var / spp)) + oracle_noise),
                 "oracle_spp": int(g["spp"]),
                 "pixels": "all" if "rect" not in g else f"crop x{x0}..{x1} y{y0}..{y1}"}
+    # The reference's own GPU wavefront tracer on the same scene (Cornell: the frame;
+    # heavy: the frame at 8 spp, this build timed on the same request).
+    reference_gpu = None
+    if rank == 0 and world == 1 and not args.skip_reference_gpu:
+        if name == "cornell" or reduced:
+            rreq, r_ms, r_rays = req, ms, total_rays
+        else:
+            rreq = S.request(W, H, 8, depth, seed)
+            S.render(ctx, sc, rreq, film)
+            torch.cuda.synchronize()
+            times = []
+            for _ in range(3):
+                a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                a.record(stream)
+                S.render(ctx, sc, rreq, film)
+                b.record(stream)
+                torch.cuda.synchronize()
+                times.append(a.elapsed_time(b))
+            r_ms, r_rays = statistics.median(times), sum(S.ray_counts(ctx))
+        reference_gpu = reference_gpu_render(builder, rreq, r_ms, r_rays)
     line = {"metric": metric, "value": value, "unit": "Mrays/s",
-            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "n_gpus": world, "steps": steps, "warmup": warmup, "ms_per_step": ms,
             "higher_is_better": True, "scaling": "weak" if world == 1 else "strong",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": workload,
@@ -692,16 +786,23 @@ def run_render(args, name: str) -> None:
             "clocks": clock_info, "gpu_launches": launches,
             "e2e": {"value": total_rays / (e2e_ms * 1e-3) / 1e6, "unit": "Mrays/s",
                     "h2d_bytes_per_step": 0, "d2h_bytes_per_step": W * H * 12,
-                    "ms_per_step": e2e_ms},
-            "cpu_baseline": cpu, "image_error_vs_fp64_oracle": fp64}
-    if rank == 0:
-        print(json.dumps(line))
+                    "ms_per_step": e2e_ms, "steps": e2e_steps},
+            "roofline": roofline, "cpu_baseline": cpu, "reference_gpu": reference_gpu,
+            "image_error_vs_fp64_oracle": fp64}
     if dist:
         dist.barrier()
         dist.destroy_process_group()
+    ctx.close()
+    return line
 
 
-def run_batched(args) -> None:
+def run_render(args, name: str) -> None:
+    line = render_line(args, name, args.steps, args.warmup)
+    if int(os.environ.get("RANK", "0")) == 0:
+        print(json.dumps(line))
+
+
+def batched_line(args, nested: bool = False) -> dict:
     """Config 4: 64 requests over 4 resident scenes, server vs the per-request path."""
     torch, ctx, stream = _render_setup()
     from lux_b200 import scene as S
@@ -719,33 +820,42 @@ def run_batched(args) -> None:
     from lux_b200 import autotune
     tune = autotune.autotune_render(ctx, scenes[1], S.request(512, 512, 16, 8, 3))
     path_budget = tune.budget
-    # Plain per-request path: lux_render one request after the other, with this build's
-    # default 4M-path batches and with the reference scheduler's 65,536-path batches
-    # (RenderSettings::batch_size, integrator/render_context.h:18).
     S.render(ctx, scenes[0], S.request(64, 64, 4, 4, 1))
     torch.cuda.synchronize()
 
-    def plain_pass(batch):
+    def plain_pass(batch, subset):
+        # Plain per-request path: lux_render one request after the other.
         ctx.set_option(3, batch)
         rays = 0
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        for r, q, f in zip(reqs, rr, films_plain):
-            S.render(ctx, scenes[r["scene"]], q, f)
+        for k in subset:
+            S.render(ctx, scenes[reqs[k]["scene"]], rr[k], films_plain[k])
             rays += sum(S.ray_counts(ctx))
         e1.record(stream)
         torch.cuda.synchronize()
         return rays, e0.elapsed_time(e1) * 1e-3
 
-    ref_rays, ref_s = plain_pass(65536) if not args.skip_reference_batch else (0, float("nan"))
-    plain_rays, plain_s = plain_pass(max(tune.render_batch, 1 << 22))
+    everything = list(range(len(reqs)))
+    # The reference scheduler's 65,536-path batches (RenderSettings::batch_size,
+    # integrator/render_context.h:18) on this build's kernels: every 8th request when
+    # nested in the default run (the whole mix takes about two minutes at that batch).
+    ref_subset = everything[::8] if nested else everything
+    ref_rays, ref_s = ((0, float("nan")) if args.skip_reference_batch
+                       else plain_pass(65536, ref_subset))
+    plain_batch = max(tune.render_batch, 1 << 22)
+    sub_rays, sub_s = plain_pass(plain_batch, ref_subset)
+    plain_rays, plain_s = plain_pass(plain_batch, everything)
     # Batched: one server, all requests submitted at once.
+    clocks = ClockSampler(0)
     with SV.Server(scenes, pool_paths=args.pool, path_budget=path_budget) as srv:
         warm, _ = srv.submit(0, S.request(64, 64, 4, 4, 1))
         srv.wait(warm)
         base = srv.stats()
+        clocks.start()
         ids = [srv.submit(r["scene"], q, f)[0] for r, q, f in zip(reqs, rr, films_batch)]
         srv.wait_all()
+        clock_info = clocks.stop()
         stats = srv.stats()
         t_sub = min(srv.times(i)[0] for i in ids)
         t_done = max(srv.times(i)[2] for i in ids)
@@ -753,7 +863,62 @@ def run_batched(args) -> None:
     batch_rays = (stats["rays"] - base["rays"]) + (stats["shadow_rays"] - base["shadow_rays"])
     rel = max(float(((a - b).abs() / (1 + b.abs())).max()) for a, b in zip(films_batch, films_plain))
     value = batch_rays / batch_s / 1e6
-    line = {"metric": "Mrays/s (batched: 64 mixed requests over 4 resident scenes)",
+    # The reference's own GPU wavefront tracer, request by request, on every 16th request
+    # (nested) and this build's plain path on the same requests.
+    reference_gpu = None
+    if not args.skip_reference_gpu:
+        # At most about a minute of the reference's renders: requests are taken in this
+        # order until the budget is spent, and both sides are compared on those done.
+        ref_gpu_order = everything[::16] if nested else everything[::4]
+        ref_gpu_subset = []
+        try:
+            from oracle.bindings import RefPt
+            if RefPt.available():
+                ref = RefPt()
+                handles = {}
+                ms = 0.0
+                try:
+                    for k in ref_gpu_order:
+                        if ms > 60e3:
+                            break
+                        si = reqs[k]["scene"]
+                        if si not in handles:
+                            handles[si] = ref.scene(builders[si])
+                            ref.render(handles[si], S.request(64, 64, 2, 4, 1))
+                        ms += ref.render(handles[si], rr[k])[1]
+                        ref_gpu_subset.append(k)
+                finally:
+                    for h in handles.values():
+                        ref.destroy(h)
+                g_rays, g_s = plain_pass(plain_batch, ref_gpu_subset)
+                reference_gpu = {
+                    "kind": "reference GPU wavefront tracer (integrator/wavefront_*.cu) for "
+                            "sm_100a, one WavefrontPathTracer::render per request",
+                    "requests": ref_gpu_subset, "seconds": ms * 1e-3,
+                    "mrays_s": g_rays / (ms * 1e-3) / 1e6,
+                    "this_build_plain_mrays_s": g_rays / g_s / 1e6,
+                    "server_speedup_vs_reference_gpu": value / (g_rays / (ms * 1e-3) / 1e6),
+                    "timing": "CUDA events per render; rays counted by this build"}
+        except Exception as e:
+            reference_gpu = {"unavailable": str(e)}
+    # Roofline of the server's work: traversal statistics of every 8th request, scaled to
+    # the served rays.
+    st_tot = {"rays": 0, "shadow_segments": 0, "box_tests": 0, "tri_tests": 0,
+              "instance_visits": 0}
+    st_paths = 0
+    for k in everything[::8]:
+        st = S.traversal_stats(ctx, scenes[reqs[k]["scene"]], rr[k])
+        for key in st_tot:
+            st_tot[key] += st[key]
+        st_paths += reqs[k]["width"] * reqs[k]["height"] * reqs[k]["spp"]
+    paths = sum(r["width"] * r["height"] * r["spp"] for r in reqs)
+    scale = batch_rays / (st_tot["rays"] + st_tot["shadow_segments"])
+    roofline = render_roofline(st_tot, 0, batch_s, scale, kernel="the server's bounce kernels")
+    roofline["algorithmic_bytes_per_step"] += FILM_BYTES_PER_PATH * paths
+    roofline["achieved"] = roofline["algorithmic_bytes_per_step"] / batch_s / 1e9
+    roofline["frac"] = roofline["achieved"] / roofline["peak"]
+    roofline["counted_on"] = "every 8th request of the mix, scaled to the served rays"
+    return {"metric": "Mrays/s (batched: 64 mixed requests over 4 resident scenes)",
             "value": value, "unit": "Mrays/s", "n_gpus": 1, "steps": 1, "warmup": 1,
             "ms_per_step": batch_s * 1e3, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
@@ -764,18 +929,33 @@ def run_batched(args) -> None:
                        "pool_paths": args.pool,
                        "autotuned": {"trace_variant": tune.trace_variant, "path_budget": tune.budget,
                                      "render_batch": tune.render_batch}},
+            "clocks": clock_info,
+            "e2e": {"value": value, "unit": "Mrays/s",
+                    "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": sum(r["width"] * r["height"] * 12 for r in reqs),
+                    "note": "films are device tensors; request latency runs from submission "
+                            "to the completed film"},
             "plain_per_request": {"value": plain_rays / plain_s / 1e6, "unit": "Mrays/s",
                                   "seconds": plain_s, "rays": plain_rays,
-                                  "batch_paths": 1 << 22},
+                                  "batch_paths": plain_batch,
+                                  "what": "this build's lux_render, one request after the "
+                                          "other, at its own batch size"},
             "plain_per_request_reference_batch": {
                 "value": ref_rays / ref_s / 1e6 if ref_rays else None, "unit": "Mrays/s",
-                "seconds": ref_s, "batch_paths": 65536},
+                "seconds": ref_s, "batch_paths": 65536, "requests": ref_subset,
+                "this_build_batch_on_same_requests_mrays_s": sub_rays / sub_s / 1e6,
+                "what": "this build's lux_render at the reference scheduler's 65,536-path "
+                        "batches (integrator/render_context.h:18)"},
             "speedup_vs_plain": (batch_rays / batch_s) / (plain_rays / plain_s),
             "speedup_vs_plain_reference_batch": ((batch_rays / batch_s) / (ref_rays / ref_s)
                                                  if ref_rays else None),
+            "reference_gpu": reference_gpu, "roofline": roofline,
             "rays": batch_rays, "iterations": stats["iterations"] - base["iterations"],
             "max_rel_film_difference_vs_plain": rel}
-    print(json.dumps(line))
+
+
+def run_batched(args) -> None:
+    print(json.dumps(batched_line(args)))
 
 
 def _poisson_arrivals(rate: float, count: int, seed: int) -> np.ndarray:
@@ -791,7 +971,7 @@ def _displaced(base: np.ndarray, frame: int) -> np.ndarray:
     return v
 
 
-def run_serving(args) -> None:
+def serving_line(args, rates: list[float]) -> dict:
     """Config 5: Poisson arrivals over the resident scenes; the displaced icosphere is
     refit every frame; p50/p99 latency and Mrays/s, against a FIFO one-request-at-a-time
     server built from the per-request path's measured service times."""
@@ -807,8 +987,9 @@ def run_serving(args) -> None:
     anim_scene, anim_mesh = 1, 1
     base = builders[anim_scene].meshes[anim_mesh].vertices.copy()
     frame_s = 1.0 / args.refit_hz if args.refit_hz > 0 else None
-    rates = [float(r) for r in args.rates.split(",")]
     results = []
+    clocks = ClockSampler(0)
+    clocks.start()
     for ri, rate in enumerate(rates):
         reqs = SC.batched_requests(args.requests, seed=100 + ri)
         if args.request_scale != 1.0:
@@ -875,24 +1056,55 @@ def run_serving(args) -> None:
         results.append({"rate_req_s": rate, "requests": len(reqs),
                         "p50_ms": float(np.percentile(lat, 50) * 1e3),
                         "p99_ms": float(np.percentile(lat, 99) * 1e3),
-                        "mrays_s": rays / span / 1e6, "refits": stats["refits"],
+                        "mrays_s": rays / span / 1e6, "span_s": span, "refits": stats["refits"],
                         "fifo_plain_p50_ms": float(np.percentile(fifo_lat, 50) * 1e3),
                         "fifo_plain_p99_ms": float(np.percentile(fifo_lat, 99) * 1e3),
                         "fifo_plain_mrays_s": plain_rays / max(free_at, 1e-9) / 1e6,
                         "plain_service_ms": {"p50": float(np.percentile(service, 50) * 1e3),
                                              "max": float(np.max(service) * 1e3),
                                              "argmax": int(np.argmax(service))}})
+    clock_info = clocks.stop()
     best = max(results, key=lambda r: r["mrays_s"])
-    line = {"metric": "p50/p99 render-request latency and Mrays/s (served)",
+    return {"metric": "p50/p99 render-request latency and Mrays/s (served)",
             "value": best["mrays_s"], "unit": "Mrays/s", "n_gpus": 1, "steps": len(rates),
-            "warmup": 1, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+            "warmup": 1, "ms_per_step": float(np.mean([r["span_s"] for r in results]) * 1e3),
+            "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": "Poisson arrivals over the 4 resident scenes; requests from the "
                                    "batched distribution scaled by %g; displaced icosphere refit "
                                    "every 1/%g s" % (args.request_scale, args.refit_hz),
                        "pool_paths": args.pool, "memory_budget_gb": args.budget_gb},
+            "clocks": clock_info,
+            "e2e": {"value": best["mrays_s"], "unit": "Mrays/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0,
+                    "note": "latency is submission to completed film, arrivals in real time"},
+            "p50_ms": {str(r["rate_req_s"]): r["p50_ms"] for r in results},
+            "p99_ms": {str(r["rate_req_s"]): r["p99_ms"] for r in results},
             "sweep": results}
-    print(json.dumps(line))
+
+
+def run_serving(args) -> None:
+    print(json.dumps(serving_line(args, [float(r) for r in args.rates.split(",")])))
+
+
+def render_suite(args) -> dict:
+    """The render configurations nested in the default line: config 1 (Cornell, 20 timed
+    frames), config 3 (heavy, 3 frames), config 4 (batched mix) and a three-rate sweep of
+    config 5 (serving), each with its own clocks, e2e, roofline and baselines."""
+    out = {}
+    t0 = time.perf_counter()
+    for name, steps, warmup in (("cornell", 20, 3), ("heavy", 3, 1)):
+        s = time.perf_counter()
+        out[name] = render_line(args, name, steps, warmup, nested=True)
+        out[name]["leg_wall_s"] = time.perf_counter() - s
+    s = time.perf_counter()
+    out["batched"] = batched_line(args, nested=True)
+    out["batched"]["leg_wall_s"] = time.perf_counter() - s
+    s = time.perf_counter()
+    out["serving"] = serving_line(args, [10.0, 100.0, 500.0])
+    out["serving"]["leg_wall_s"] = time.perf_counter() - s
+    out["wall_s"] = time.perf_counter() - t0
+    return out
 
 
 def main():
@@ -921,6 +1133,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="lux", choices=["lux", "reference"])
     ap.add_argument("--skip-e2e", action="store_true")
+    ap.add_argument("--skip-render", action="store_true",
+                    help="lbvh: leave out the nested render configurations (1, 3, 4, 5)")
     ap.add_argument("--skip-cpu-baseline", action="store_true")
     ap.add_argument("--skip-reference-gpu", action="store_true",
                     help="lbvh: skip timing the reference's own GPU LBVH code")

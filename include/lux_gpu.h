@@ -518,6 +518,18 @@ int lux_render_samples(lux_ctx* ctx, const lux_scene* scene, const lux_render_re
  * [1] shadow-ray segments (each pass-through re-launch counts), host int64[2]. */
 int lux_render_ray_counts(lux_ctx* ctx, int64_t* counts);
 
+/* The traversal work of a render, for its roofline: the same render as lux_render (the
+ * same film_sum), run by the one-path-per-thread bounce kernels with every walk
+ * counted in the reference's visit order (bvh/bvh_device.cuh:43-90 at both levels of
+ * scene/gpu_scene_bvh.cuh:44-135; shadow segments walked to their closest hit, as the
+ * reference traces them, integrator/wavefront_kernels.cu:28-83).  stats (host
+ * int64[5]): [0] camera + extension rays, [1] shadow-ray segments, [2] box tests,
+ * [3] triangle tests, [4] instance (TLAS leaf) visits.  Measurement only: slower than
+ * lux_render.  No reference counterpart (the reference counts nothing). */
+int lux_render_traversal_stats(lux_ctx* ctx, const lux_scene* scene,
+                               const lux_render_request* req, float* film_sum,
+                               int64_t* stats);
+
 /* ------------------------------------------------------------------ batched / served rendering */
 
 /*

@@ -86,6 +86,7 @@ SIGNATURES = {
     "lux_render": (ctypes.c_int, [_P, _P, _P, _P]),
     "lux_render_samples": (ctypes.c_int, [_P, _P, _P, _P]),
     "lux_render_ray_counts": (ctypes.c_int, [_P, _P]),
+    "lux_render_traversal_stats": (ctypes.c_int, [_P, _P, _P, _P, _P]),
     "lux_server_create": (ctypes.c_int, [ctypes.c_int, _P, _I32, _P, ctypes.POINTER(_P)]),
     "lux_server_submit": (ctypes.c_int, [_P, _I32, _P, _P, ctypes.POINTER(_I64)]),
     "lux_server_poll": (ctypes.c_int, [_P, _I64, ctypes.POINTER(_I32)]),

@@ -846,6 +846,43 @@ int lux_scene_select_lights(lux_ctx* ctx, const lux_scene* scene, int32_t light_
     return sync_and_check(ctx);
 }
 
+int lux_render_traversal_stats(lux_ctx* ctx, const lux_scene* scene,
+                               const lux_render_request* req, float* film_sum,
+                               int64_t* stats) {
+    if (int st = check_ctx(ctx)) return st;
+    if (!scene || !req || !film_sum || !stats)
+        return lux::fail(LUX_ERR_INVALID_ARGUMENT, "null argument");
+    if (req->width <= 0 || req->height <= 0 || req->spp <= 0)
+        return lux::fail(LUX_ERR_INVALID_ARGUMENT, "render requires a non-empty film");
+    if (req->max_depth < 0 || req->max_depth > 1000)
+        return lux::fail(LUX_ERR_INVALID_ARGUMENT, "max_depth must be in 0..1000");
+    if (req->light_sampler < 0 || req->light_sampler > 2)
+        return lux::fail(LUX_ERR_INVALID_ARGUMENT, "light sampler: 0 uniform, 1 power or 2 tree");
+    if (static_cast<long long>(req->width) * req->height > (1ll << 30))
+        return lux::fail(LUX_ERR_INVALID_ARGUMENT, "image too large");
+    const size_t bytes = sizeof(float) * 3 * static_cast<size_t>(req->width) * req->height;
+    unsigned long long walk[3] = {0, 0, 0};
+    Staging staging(ctx);
+    void *d_film = nullptr, *d_walk = nullptr;
+    staging.add(film_sum, bytes, false, true, &d_film);
+    staging.add(walk, sizeof(walk), false, true, &d_walk);
+    int st = staging.begin();
+    if (st) return st;
+    st = lux::render(ctx, scene, *req, static_cast<float*>(d_film), false, nullptr, nullptr,
+                     nullptr, nullptr, nullptr, 0, static_cast<unsigned long long*>(d_walk));
+    if (st) return st;
+    st = finish_call(ctx, staging);
+    if (st) return st;
+    st = sync_and_check(ctx);
+    if (st) return st;
+    int64_t rays[2];
+    lux::render_ray_counts(ctx, rays);
+    stats[0] = rays[0];
+    stats[1] = rays[1];
+    for (int k = 0; k < 3; ++k) stats[2 + k] = static_cast<int64_t>(walk[k]);
+    return LUX_OK;
+}
+
 int lux_render_ray_counts(lux_ctx* ctx, int64_t* counts) {
     if (!ctx || !counts) return lux::fail(LUX_ERR_INVALID_ARGUMENT, "null argument");
     return lux::render_ray_counts(ctx, counts);

@@ -91,15 +91,25 @@ LUX_D f3 xform_vector(const float* m, f3 v) {
                    add(add(mul(m[8], v.x), mul(m[9], v.y)), mul(m[10], v.z)));
 }
 
+// Node visits and triangle tests of a walk in the reference's visit order: each box the
+// reference's stackless walk tests (the root's, and both children's of every node it
+// enters: bvh/bvh_device.cuh:43-90) and each triangle it tests; instances: TLAS leaves
+// whose BLAS was searched.  Filled only by the kCount variants below.
+struct WalkCounts {
+    unsigned long long boxes = 0, tris = 0, instances = 0;
+};
+
 // Closest hit inside one BLAS in object space, reference order (bvh/bvh_device.cuh:92-134
 // with GpuMeshPrimitiveIntersector, scene/gpu_scene_bvh.cuh:15-42).  best_t enters as the
-// current bound; returns the local triangle id or -1.
+// current bound; returns the local triangle id or -1.  kCount adds to *wc.
+template <bool kCount = false>
 LUX_D int blas_closest(const BvhView& b, f3 o, f3 d, float tmin, float& best_t, float& bu,
-                       float& bv, int ignored_local, int* error) {
+                       float& bv, int ignored_local, int* error, WalkCounts* wc = nullptr) {
     if (b.n <= 0) return -1;
     ray3 r{o, tmin, d, best_t};
     slab_ray sr = make_slab_ray(r);
     float tn;
+    if (kCount) wc->boxes += 1;
     if (!slab_hit(sr, load_root(b.root), best_t, tn)) return -1;
     int2 stack[kStack];  // (node ref, entry t bits): one 8-byte access per entry
     int sp = 0;
@@ -115,6 +125,7 @@ LUX_D int blas_closest(const BvhView& b, f3 o, f3 d, float tmin, float& best_t, 
         if (cur >= 0) {
             BvhNode nd = load_node(b.nodes, cur);
             float tl, tr;
+            if (kCount) wc->boxes += 2;
             bool hl = slab_hit(sr, node_left_box(nd), best_t, tl);
             bool hr = slab_hit(sr, node_right_box(nd), best_t, tr);
             if (hl) {
@@ -137,6 +148,7 @@ LUX_D int blas_closest(const BvhView& b, f3 o, f3 d, float tmin, float& best_t, 
             float4 p0 = __ldg(tp);
             int local = __float_as_int(p0.w);
             if (local != ignored_local) {
+                if (kCount) wc->tris += 1;
                 float4 p1 = __ldg(tp + 1);
                 float4 p2 = __ldg(tp + 2);
                 float t, u, v;
@@ -169,9 +181,11 @@ LUX_D int blas_closest(const BvhView& b, f3 o, f3 d, float tmin, float& best_t, 
 // Two-level closest hit (intersect_scene_bvh_device, scene/gpu_scene_bvh.cuh:44-135):
 // TLAS over instance boxes in reference order; at each instance leaf the ray is taken
 // to object space and its BLAS searched with t_max = the current best.  ignored: scene
-// triangle id skipped (shadow rays leaving a surface), -1 none.
+// triangle id skipped (shadow rays leaving a surface), -1 none.  kCount adds the
+// walk's node visits and triangle tests (both levels) to *wc.
+template <bool kCount = false>
 LUX_D SceneHit scene_closest(const SceneView& sc, f3 o, f3 d, float tmin, float tmax,
-                             int ignored, int* error) {
+                             int ignored, int* error, WalkCounts* wc = nullptr) {
     SceneHit h;
     h.t = tmax;
     if (!sc.has_two_level) return h;
@@ -179,6 +193,7 @@ LUX_D SceneHit scene_closest(const SceneView& sc, f3 o, f3 d, float tmin, float 
     ray3 r{o, tmin, d, tmax};
     slab_ray sr = make_slab_ray(r);
     float tn;
+    if (kCount) wc->boxes += 1;
     if (!slab_hit(sr, load_root(tl.root), h.t, tn)) return h;
     int ign_instance = -1, ign_local = -1;
     if (ignored >= 0) {
@@ -200,6 +215,7 @@ LUX_D SceneHit scene_closest(const SceneView& sc, f3 o, f3 d, float tmin, float 
         if (cur >= 0) {
             BvhNode nd = load_node(tl.nodes, cur);
             float a, b;
+            if (kCount) wc->boxes += 2;
             bool hl = slab_hit(sr, node_left_box(nd), h.t, a);
             bool hr = slab_hit(sr, node_right_box(nd), h.t, b);
             if (hl) {
@@ -224,8 +240,10 @@ LUX_D SceneHit scene_closest(const SceneView& sc, f3 o, f3 d, float tmin, float 
             f3 ld = xform_vector(inst.inv, d);
             float best = h.t;
             float u = 0, v = 0;
-            int local = blas_closest(sc.blas[inst.blas], lo, ld, tmin, best, u, v,
-                                     inst_id == ign_instance ? ign_local : -1, error);
+            if (kCount) wc->instances += 1;
+            int local = blas_closest<kCount>(sc.blas[inst.blas], lo, ld, tmin, best, u, v,
+                                             inst_id == ign_instance ? ign_local : -1, error,
+                                             wc);
             if (local >= 0 && best < h.t) {
                 h.prim = inst.first_primitive + local;
                 h.t = best;
@@ -1204,6 +1222,9 @@ struct DebugTargets {
     unsigned long long* log_count = nullptr;
     long long log_capacity = 0;
     int sample_offset = 0;
+    // Traversal totals (box tests, triangle tests, instance visits) of every extension
+    // and shadow walk, or null.
+    unsigned long long* walk_counts = nullptr;
 };
 
 // What the shading of one vertex decided, for its path log record
@@ -1503,7 +1524,16 @@ LUX_D void shadow_path(const PathPool& rt, const SceneView& sc, int p, int* erro
             break;
         }
         ++segments;
-        SceneHit h = scene_closest(sc, o, d, tmin, tmax, ignored, error);
+        SceneHit h;
+        if (kAov && aov.walk_counts) {
+            WalkCounts wc;
+            h = scene_closest<true>(sc, o, d, tmin, tmax, ignored, error, &wc);
+            atomicAdd(aov.walk_counts, wc.boxes);
+            atomicAdd(aov.walk_counts + 1, wc.tris);
+            atomicAdd(aov.walk_counts + 2, wc.instances);
+        } else {
+            h = scene_closest(sc, o, d, tmin, tmax, ignored, error);
+        }
         if (h.prim < 0) break;
         const Material m = sc.materials[material_of(sc, h.prim)];
         if (!is_passthrough(m)) {

@@ -103,11 +103,13 @@ int camera_perspective(const float* origin, const float* look_at, float vfov, fl
 // (device, width*height*3) receive the debug images' per-pixel sums.
 // With any debug target (images; path log records, capacity entries, whose counter
 // log_count the render zeroes and counts every vertex on), the bounce kernels are the
-// debug ones.
+// debug ones.  walk_counts (device, 3 counters, zeroed by the render) also selects
+// them and receives the box tests, triangle tests and instance visits of every walk.
 int render(lux_ctx* ctx, const lux_scene* scene, const lux_render_request& req, float* out,
            bool per_sample, float* aov_shadow = nullptr, float* aov_ng = nullptr,
            float* aov_ns = nullptr, lux_path_log_record* log = nullptr,
-           unsigned long long* log_count = nullptr, long long log_capacity = 0);
+           unsigned long long* log_count = nullptr, long long log_capacity = 0,
+           unsigned long long* walk_counts = nullptr);
 int render_ray_counts(lux_ctx* ctx, int64_t* counts);
 // Light selection queries (device arrays): sample_scene_light and light_pmf at each
 // position, as next-event estimation makes them.

@@ -166,7 +166,16 @@ __global__ void __launch_bounds__(kThreads) k_extend_aov(PathPool rt, int* count
         int cls = -1;
         if (active) {
             const float4 a = rt.ray_o[p], b = rt.ray_d[p];
-            const SceneHit h = scene_closest(sc, xyz(a), xyz(b), a.w, b.w, -1, error);
+            SceneHit h;
+            if (aov.walk_counts) {
+                WalkCounts wc;
+                h = scene_closest<true>(sc, xyz(a), xyz(b), a.w, b.w, -1, error, &wc);
+                atomicAdd(aov.walk_counts, wc.boxes);
+                atomicAdd(aov.walk_counts + 1, wc.tris);
+                atomicAdd(aov.walk_counts + 2, wc.instances);
+            } else {
+                h = scene_closest(sc, xyz(a), xyz(b), a.w, b.w, -1, error);
+            }
             if (depth == 0) aov_primary(rt, sc, p, h, aov);
             cls = extend_finish(rt, sc, sampler, p, h);
         }
@@ -369,7 +378,8 @@ int render_ray_counts(lux_ctx* ctx, int64_t* counts) {
 
 int render(lux_ctx* ctx, const lux_scene* scene, const lux_render_request& req, float* out,
            bool per_sample, float* aov_shadow, float* aov_ng, float* aov_ns,
-           lux_path_log_record* log, unsigned long long* log_count, long long log_capacity) {
+           lux_path_log_record* log, unsigned long long* log_count, long long log_capacity,
+           unsigned long long* walk_counts) {
     using namespace pt;
     DebugTargets aov;
     aov.shadow = aov_shadow;
@@ -379,7 +389,8 @@ int render(lux_ctx* ctx, const lux_scene* scene, const lux_render_request& req, 
     aov.log_count = log_count;
     aov.log_capacity = aov.log ? log_capacity : 0;
     aov.sample_offset = req.sample_offset;
-    const bool with_aov = aov_shadow || aov_ng || aov_ns || log_count;
+    aov.walk_counts = walk_counts;
+    const bool with_aov = aov_shadow || aov_ng || aov_ns || log_count || walk_counts;
     const int pixels = req.width * req.height;
     const long long total_paths = static_cast<long long>(pixels) * req.spp;
     // Batch: whole pixels' sample ranges, at most ctx->render_batch paths.
@@ -416,6 +427,8 @@ int render(lux_ctx* ctx, const lux_scene* scene, const lux_render_request& req, 
             err = cudaMemsetAsync(image, 0, sizeof(float) * 3 * size_t(pixels), s);
     if (log_count && err == cudaSuccess)
         err = cudaMemsetAsync(log_count, 0, sizeof(unsigned long long), s);
+    if (walk_counts && err == cudaSuccess)
+        err = cudaMemsetAsync(walk_counts, 0, 3 * sizeof(unsigned long long), s);
     if (err != cudaSuccess) return cuda_fail(err, "render setup");
     for (int s0 = 0; s0 < req.spp; s0 += samples_per_batch) {
         int ns = std::min(samples_per_batch, req.spp - s0);

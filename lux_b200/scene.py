@@ -238,44 +238,52 @@ class SceneBuilder:
         return np.concatenate(out) if out else np.zeros(0, np.int32)
 
 
+def scene_desc(builder: SceneBuilder):
+    """The lux_scene_desc of a SceneBuilder and the arrays it points into (keep them
+    alive while the descriptor is in use)."""
+    keep = []
+    mats = (Material * max(len(builder.materials), 1))(*builder.materials)
+    meshes = []
+    for i, mesh in enumerate(builder.meshes):
+        if i == builder._default_mesh:
+            mesh = builder.default_mesh()
+        v = np.ascontiguousarray(mesh.vertices, np.float32)
+        idx = np.ascontiguousarray(mesh.indices, np.uint32)
+        mid = np.ascontiguousarray(mesh.material_ids, np.int32)
+        nrm = None if mesh.normals is None else np.ascontiguousarray(mesh.normals, np.float32)
+        uv = None if mesh.uvs is None else np.ascontiguousarray(mesh.uvs, np.float32)
+        keep += [v, idx, mid, nrm, uv]
+        meshes.append(MeshDesc(v.ctypes.data, None if nrm is None else nrm.ctypes.data,
+                               None if uv is None else uv.ctypes.data, len(v),
+                               idx.ctypes.data, mid.ctypes.data, len(mid)))
+    mesh_arr = (MeshDesc * max(len(meshes), 1))(*meshes)
+    insts = []
+    for mesh_id, m, override in builder.instances:
+        insts.append(InstanceDesc(mesh_id, override, _F12(*np.asarray(m, np.float32).reshape(-1)),
+                                  _F12(*([0.0] * 12))))
+    inst_arr = (InstanceDesc * max(len(insts), 1))(*insts)
+    light_arr = (LightDesc * max(len(builder.lights), 1))(*builder.lights)
+    images = [np.ascontiguousarray(im, np.float32) for im in builder.images]
+    keep += images
+    img_arr = (EnvImageDesc * max(len(images), 1))(
+        *[EnvImageDesc(im.ctypes.data, im.shape[1], im.shape[0]) for im in images])
+    keep += [mats, mesh_arr, inst_arr, light_arr, img_arr]
+    desc = SceneDesc(ctypes.addressof(mats), len(builder.materials),
+                     ctypes.addressof(mesh_arr), len(meshes),
+                     ctypes.addressof(inst_arr), len(insts),
+                     ctypes.addressof(light_arr), len(builder.lights),
+                     builder.camera if builder.camera is not None else CameraDesc(),
+                     ctypes.addressof(img_arr), len(images))
+    return desc, keep
+
+
 class Scene:
     """A lux_scene handle resident on the context's device."""
 
     def __init__(self, ctx, builder: SceneBuilder):
         self.ctx = ctx
         lib = ctx._lib
-        keep = []
-        mats = (Material * max(len(builder.materials), 1))(*builder.materials)
-        meshes = []
-        for i, mesh in enumerate(builder.meshes):
-            if i == builder._default_mesh:
-                mesh = builder.default_mesh()
-            v = np.ascontiguousarray(mesh.vertices, np.float32)
-            idx = np.ascontiguousarray(mesh.indices, np.uint32)
-            mid = np.ascontiguousarray(mesh.material_ids, np.int32)
-            nrm = None if mesh.normals is None else np.ascontiguousarray(mesh.normals, np.float32)
-            uv = None if mesh.uvs is None else np.ascontiguousarray(mesh.uvs, np.float32)
-            keep += [v, idx, mid, nrm, uv]
-            meshes.append(MeshDesc(v.ctypes.data, None if nrm is None else nrm.ctypes.data,
-                                   None if uv is None else uv.ctypes.data, len(v),
-                                   idx.ctypes.data, mid.ctypes.data, len(mid)))
-        mesh_arr = (MeshDesc * max(len(meshes), 1))(*meshes)
-        insts = []
-        for mesh_id, m, override in builder.instances:
-            insts.append(InstanceDesc(mesh_id, override, _F12(*np.asarray(m, np.float32).reshape(-1)),
-                                      _F12(*([0.0] * 12))))
-        inst_arr = (InstanceDesc * max(len(insts), 1))(*insts)
-        light_arr = (LightDesc * max(len(builder.lights), 1))(*builder.lights)
-        images = [np.ascontiguousarray(im, np.float32) for im in builder.images]
-        keep += images
-        img_arr = (EnvImageDesc * max(len(images), 1))(
-            *[EnvImageDesc(im.ctypes.data, im.shape[1], im.shape[0]) for im in images])
-        desc = SceneDesc(ctypes.addressof(mats), len(builder.materials),
-                         ctypes.addressof(mesh_arr), len(meshes),
-                         ctypes.addressof(inst_arr), len(insts),
-                         ctypes.addressof(light_arr), len(builder.lights),
-                         builder.camera if builder.camera is not None else CameraDesc(),
-                         ctypes.addressof(img_arr), len(images))
+        desc, keep = scene_desc(builder)
         handle = ctypes.c_void_p()
         _check(lib.lux_scene_create(ctx.handle, ctypes.byref(desc), ctypes.byref(handle)))
         self._h = handle
@@ -395,6 +403,18 @@ def ray_counts(ctx) -> tuple[int, int]:
     c = np.zeros(2, np.int64)
     _check(ctx._lib.lux_render_ray_counts(ctx.handle, c.ctypes.data))
     return int(c[0]), int(c[1])
+
+
+def traversal_stats(ctx, scene: Scene, req: RenderRequest) -> dict:
+    """The render's traversal work in the reference's visit order
+    (lux_render_traversal_stats): rays, shadow segments, box tests, triangle tests and
+    instance visits, with the film the counted render made."""
+    film = np.zeros((req.height, req.width, 3), np.float32)
+    c = np.zeros(5, np.int64)
+    _check(ctx._lib.lux_render_traversal_stats(ctx.handle, scene.handle, ctypes.byref(req),
+                                               _ptr(film), c.ctypes.data))
+    return {"rays": int(c[0]), "shadow_segments": int(c[1]), "box_tests": int(c[2]),
+            "tri_tests": int(c[3]), "instance_visits": int(c[4]), "film": film}
 
 
 def _add_box(b: SceneBuilder, lo, hi, mat):

@@ -4,6 +4,8 @@
 * Ref: the reference's own host code (oracle/_ref/libluxref.so, built from the reference
   sources by oracle/build.py; present wherever it was built).
 * PT64: the FP64 high-spp path-tracing oracle (oracle/pt64.c -> oracle/liblux_pt64.so).
+* RefGpu / RefPt: the reference's own GPU LBVH and GPU wavefront path tracer, compiled
+  for sm_100a (oracle/_ref/libluxrefgpu.so, oracle/_ref/libluxrefpt.so).
 
 Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use this module.
 """
@@ -18,6 +20,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_LIB = os.path.join(HERE, "liblux_oracle.so")
 REF_LIB = os.path.join(HERE, "_ref", "libluxref.so")
 REF_GPU_LIB = os.path.join(HERE, "_ref", "libluxrefgpu.so")
+REF_PT_LIB = os.path.join(HERE, "_ref", "libluxrefpt.so")
 PT64_LIB = os.path.join(HERE, "liblux_pt64.so")
 
 _P = ctypes.c_void_p
@@ -138,7 +141,38 @@ class Ref:
         lib.ref_tree_create.restype = _P
         lib.ref_tree_destroy.argtypes = [_P]
         lib.ref_tree_trace.argtypes = [_P, _P, _I, _I, _P, _P]
+        lib.ref_desc_scene_create.argtypes = [_P]
+        lib.ref_desc_scene_create.restype = _P
+        lib.ref_desc_scene_destroy.argtypes = [_P]
+        lib.ref_desc_render.argtypes = [_P, _P, _I, _I, _I, _I, _I, _P, _P]
+        lib.ref_desc_render.restype = _I
         self.lib = lib
+
+    def desc_scene(self, builder):
+        """The reference's PreparedScene (host two-level BVH) of a lux_b200 SceneBuilder,
+        built from the same lux_scene_desc that lux_scene_create receives."""
+        from lux_b200 import scene as S
+
+        desc, keep = S.scene_desc(builder)
+        handle = self.lib.ref_desc_scene_create(ctypes.addressof(desc))
+        del keep
+        return handle
+
+    def desc_scene_destroy(self, handle) -> None:
+        self.lib.ref_desc_scene_destroy(handle)
+
+    def desc_render(self, handle, req, rows=None, cols=None, threads=1, samples=False):
+        """trace_path over the pixels rows [y0, y1) x cols [x0, x1) of the request's frame
+        (lux_b200.scene.request; default the whole frame): the rectangle's film sums
+        (rows x cols x 3) and, with samples=True, every sample's radiance
+        (rows * cols x spp x 3, row-major)."""
+        y0, y1 = rows if rows is not None else (0, req.height)
+        x0, x1 = cols if cols is not None else (0, req.width)
+        film = np.zeros((y1 - y0, x1 - x0, 3), np.float32)
+        out = np.zeros(((y1 - y0) * (x1 - x0), req.spp, 3), np.float32) if samples else None
+        self.lib.ref_desc_render(handle, ctypes.addressof(req), x0, y0, x1, y1, threads,
+                                 _addr(out), film.ctypes.data)
+        return (film, out) if samples else film
 
     def render_scene(self, tris, material_ids, materials, lights, camera, width, height, spp,
                      max_depth, seed, light_sampler=1, rows=None, threads=1, env_image=None,
@@ -446,3 +480,72 @@ class RefGpu:
                                                found.ctypes.data))
         names = ("build", "trace_api", "trace_kernel", "refit", "query_build", "overlap")
         return dict(zip(names, times.tolist())), int(found[0])
+
+
+class RefPt:
+    """The reference's own GPU wavefront path tracer (PreparedScene::prepare_gpu +
+    WavefrontPathTracer::render) compiled for sm_100a, on scenes given as lux_b200
+    SceneBuilders (the same lux_scene_desc lux_scene_create receives)."""
+
+    def __init__(self, path: str = REF_PT_LIB):
+        if not os.path.exists(path):
+            raise FileNotFoundError(f"{path} missing (built only where the reference exists)")
+        lib = ctypes.CDLL(path)
+        lib.refpt_scene_create.argtypes = [_P, ctypes.c_char_p, _I]
+        lib.refpt_scene_create.restype = _P
+        lib.refpt_scene_destroy.argtypes = [_P]
+        lib.refpt_render.argtypes = [_P, _P, _I, _P, _P, ctypes.c_char_p, _I]
+        lib.refpt_render.restype = _I
+        lib.refpt_render_path_log.argtypes = [_P, _P, _I, _P, _P, _I64, _P, ctypes.c_char_p, _I]
+        lib.refpt_render_path_log.restype = _I
+        self.lib = lib
+
+    @staticmethod
+    def available(path: str = REF_PT_LIB) -> bool:
+        return os.path.exists(path)
+
+    def scene(self, builder):
+        from lux_b200 import scene as S
+
+        desc, keep = S.scene_desc(builder)
+        err = ctypes.create_string_buffer(512)
+        handle = self.lib.refpt_scene_create(ctypes.addressof(desc), err, 512)
+        del keep
+        if not handle:
+            raise RuntimeError("reference GPU scene: " + err.value.decode())
+        return handle
+
+    def destroy(self, handle) -> None:
+        self.lib.refpt_scene_destroy(handle)
+
+    def render(self, handle, req, batch_size=0):
+        """(film sum height x width x 3, CUDA-event ms, host ms) of one render."""
+        film = np.zeros((req.height, req.width, 3), np.float32)
+        ms = np.zeros(2, np.float64)
+        err = ctypes.create_string_buffer(512)
+        status = self.lib.refpt_render(handle, ctypes.addressof(req), batch_size,
+                                       film.ctypes.data, ms.ctypes.data, err, 512)
+        if status != 0:
+            raise RuntimeError("reference GPU render: " + err.value.decode())
+        return film, float(ms[0]), float(ms[1])
+
+    def path_log(self, handle, req, capacity=None, batch_size=0):
+        """(film sum, records) with the path log on; records as
+        lux_b200.scene.PATH_LOG_RECORD sorted by (sample_index, pixel_index, vertex)."""
+        from lux_b200 import scene as S
+
+        if capacity is None:
+            capacity = req.width * req.height * req.spp * (req.max_depth + 1)
+        film = np.zeros((req.height, req.width, 3), np.float32)
+        records = np.zeros(max(int(capacity), 1), S.PATH_LOG_RECORD)
+        count = np.zeros(1, np.int64)
+        err = ctypes.create_string_buffer(512)
+        status = self.lib.refpt_render_path_log(handle, ctypes.addressof(req), batch_size,
+                                                film.ctypes.data, records.ctypes.data,
+                                                int(capacity), count.ctypes.data, err, 512)
+        if status < 0:
+            raise RuntimeError("reference GPU path log: " + err.value.decode())
+        if status > 0:
+            raise RuntimeError(f"reference GPU path log: {int(count[0])} records exceed "
+                               f"the capacity {capacity}")
+        return film, records[:int(count[0])]

@@ -5,6 +5,10 @@
 3. oracle/_ref/libluxref.so: the reference's own host code.
 4. oracle/_ref/libluxrefgpu.so: the reference's own GPU LBVH (bvh/gpu_bvh.cu,
    bvh/bvh_overlap.cu) behind oracle/ref_gpu_harness.cu, compiled with nvcc for sm_100a.
+5. oracle/_ref/libluxrefpt.so: the reference's own GPU wavefront path tracer
+   (integrator/wavefront_*.cu, scene/prepared_scene.cu, bvh/gpu_bvh.cu,
+   light/light_distribution.cpp) behind oracle/ref_pt_gpu_harness.cu, compiled with nvcc
+   for sm_100a, one object per translation unit.
 
 Compiles, in place and without the reference's build system, the handful of
 reference translation units the CPU path needs (integrator/cpu_path_tracer.cpp,
@@ -68,10 +72,12 @@ def build_ref(force=False):
         return None
     harness = os.path.join(HERE, "ref_harness.cpp")
     inputs = [harness] + [os.path.join(REF_ROOT, s) for s in REF_SOURCES]
-    if not force and not _stale(OUT, inputs):
+    deps = inputs + [os.path.join(HERE, "ref_scene_desc.h"),
+                     os.path.join(HERE, "..", "include", "lux_gpu.h")]
+    if not force and not _stale(OUT, deps):
         return OUT
     os.makedirs(OUT_DIR, exist_ok=True)
-    cmd = ["g++", *CXXFLAGS, "-shared", "-I", src_dir, "-o", OUT, *inputs]
+    cmd = ["g++", *CXXFLAGS, "-shared", "-I", src_dir, "-I", HERE, "-o", OUT, *inputs]
     subprocess.run(cmd, check=True)
     return OUT
 
@@ -101,9 +107,66 @@ def build_ref_gpu(force=False):
     return REF_GPU_OUT
 
 
+REF_PT_OUT = os.path.join(OUT_DIR, "libluxrefpt.so")
+REF_PT_SOURCES = [
+    "src/integrator/wavefront_kernels.cu",
+    "src/integrator/wavefront_pt.cu",
+    "src/integrator/wavefront_runtime.cu",
+    "src/integrator/wavefront_scheduler.cu",
+    "src/scene/prepared_scene.cu",
+    "src/bvh/gpu_bvh.cu",
+    "src/light/light_distribution.cpp",
+]
+
+
+def _ref_headers(src_dir):
+    out = []
+    for root, _, files in os.walk(src_dir):
+        out += [os.path.join(root, f) for f in files if f.endswith((".h", ".cuh"))]
+    return out
+
+
+def build_ref_pt_gpu(force=False):
+    """Compile the reference's GPU wavefront tracer harness; None when the reference is
+    absent.  Each translation unit becomes one object (in parallel), linked into one
+    library whose only exported symbols are the harness's refpt_* entry points."""
+    import concurrent.futures
+
+    src_dir = os.path.join(REF_ROOT, "src")
+    if not os.path.isdir(src_dir):
+        return None
+    harness = os.path.join(HERE, "ref_pt_gpu_harness.cu")
+    sources = [harness] + [os.path.join(REF_ROOT, s) for s in REF_PT_SOURCES]
+    deps = sources + [os.path.join(HERE, "ref_scene_desc.h"),
+                      os.path.join(HERE, "..", "include", "lux_gpu.h")] + _ref_headers(src_dir)
+    if not force and not _stale(REF_PT_OUT, deps):
+        return REF_PT_OUT
+    obj_dir = os.path.join(OUT_DIR, "refpt_obj")
+    os.makedirs(obj_dir, exist_ok=True)
+
+    def compile_one(src):
+        obj = os.path.join(obj_dir, os.path.basename(src) + ".o")
+        flags = [] if src == harness else ["-Xcompiler", "-fvisibility=hidden"]
+        lang = ["-x", "cu"] if src.endswith(".cu") else []
+        cmd = ["nvcc", *NVCCFLAGS, *flags, "-I", src_dir, "-I", HERE, *lang, "-c", src,
+               "-o", obj]
+        res = subprocess.run(cmd, capture_output=True, text=True)
+        if res.returncode != 0:
+            raise RuntimeError(f"compile failed for {src}:\n{res.stderr[-4000:]}")
+        return obj
+
+    with concurrent.futures.ThreadPoolExecutor(max_workers=len(sources)) as pool:
+        objs = list(pool.map(compile_one, sources))
+    cmd = ["nvcc", "-shared", "-gencode", "arch=compute_100a,code=sm_100a",
+           "-Xlinker", "--no-undefined", "-o", REF_PT_OUT, *objs]
+    subprocess.run(cmd, check=True)
+    return REF_PT_OUT
+
+
 def build(force=False):
     build_pt64(force)
     build_ref_gpu(force)
+    build_ref_pt_gpu(force)
     return build_oracle(force), build_ref(force)
 
 

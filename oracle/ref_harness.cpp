@@ -54,6 +54,10 @@
 #include "scene/stanford_dragon.h"
 #include "util/obj_loader.h"
 
+// Scenes from the library's own descriptor (lux_scene_desc): meshes, instances,
+// materials, lights, images and camera in the order lux_scene_create receives them.
+#include "ref_scene_desc.h"
+
 // lux_path_log_record and the LUX_PATH_* flags (the values of PathLogEventFlags and
 // PathLogTerminationFlags, integrator/pathstate.cuh:19-39, whose header needs thrust).
 #include "../include/lux_gpu.h"
@@ -913,6 +917,77 @@ int ref_write_image(const float* pixels, int width, int height, int spp, const c
     if (kind == 0) write_ppm(path, px, width, height, spp);
     else if (kind == 1) write_debug_ppm_linear(path, px, width, height, spp);
     else write_pfm(path, px, width, height, spp);
+    return 0;
+}
+
+// ---- scenes from lux_scene_desc (any number of meshes and instances, two-level) ----
+
+struct RefDescScene {
+    PreparedScene prepared;
+    explicit RefDescScene(Scene scene) : prepared(std::move(scene)) {
+        prepared.prepare_host_bvh();
+    }
+};
+
+// The reference's PreparedScene (with its host two-level BVH) of a scene descriptor.
+void* ref_desc_scene_create(const lux_scene_desc* desc) {
+    return new RefDescScene(lux_ref_desc::scene_from_desc(*desc));
+}
+
+void ref_desc_scene_destroy(void* handle) { delete static_cast<RefDescScene*>(handle); }
+
+// trace_path (integrator/cpu_path_tracer.cpp:403-498) for every sample of the pixels
+// x in [x0, x1), y in [y0, y1) of the request's frame, with the camera-sample draws of
+// render_cpu_path_tracer (cpu_path_tracer.cpp:525-558) and RenderSettings{max_depth,
+// seed, frame_index, sample_offset} from the request.  samples (optional) receives
+// [pixel of the rectangle, row-major][spp][3]; film (optional) receives the rectangle's
+// per-pixel sums in sample order, as the reference's Film accumulates them.
+int ref_desc_render(void* handle, const lux_render_request* req, int x0, int y0, int x1,
+                    int y1, int threads, float* samples, float* film) {
+    const RefDescScene* h = static_cast<const RefDescScene*>(handle);
+    const PreparedScene& prepared = h->prepared;
+    const Scene& sc = prepared.host_scene();
+    SceneLightSampler lights_sampler = make_scene_light_sampler(
+        sc, prepared.light_sampling(), sampler_kind(req->light_sampler));
+    RenderSettings settings;
+    settings.max_depth = req->max_depth;
+    settings.seed = req->seed;
+    settings.frame_index = req->frame_index;
+    settings.sample_offset = req->sample_offset;
+    const int width = req->width, height = req->height, spp = req->spp;
+    const int cols = x1 - x0;
+    parallel_for((y1 - y0) * cols, threads, [&](int begin, int end) {
+        for (int idx = begin; idx < end; ++idx) {
+            int y = y0 + idx / cols;
+            int x = x0 + idx % cols;
+            int pixel = y * width + x;
+            vec3 sum(0);
+            for (int s = 0; s < spp; ++s) {
+                SamplerState sampler = make_render_sampler(settings, pixel, s);
+                Float jx = sampler_get_1d(sampler);
+                Float jy = sampler_get_1d(sampler);
+                CameraSample cs;
+                cs.p_film = vec2((Float(x) + jx) / Float(width),
+                                 (Float(height - 1 - y) + jy) / Float(height));
+                cs.p_lens = sampler_get_2d(sampler);
+                cs.time = sampler_get_1d(sampler);
+                CameraRay generated = generate_camera_ray(sc.camera, cs);
+                vec3 L(0);
+                if (generated.valid)
+                    L = trace_path(sc, prepared.host_bvh(), lights_sampler, generated.ray,
+                                   sampler, settings.max_depth);
+                sum += L;
+                if (samples) {
+                    float* o = samples + (size_t(idx) * spp + s) * 3;
+                    o[0] = L.x; o[1] = L.y; o[2] = L.z;
+                }
+            }
+            if (film) {
+                float* o = film + size_t(idx) * 3;
+                o[0] = sum.x; o[1] = sum.y; o[2] = sum.z;
+            }
+        }
+    });
     return 0;
 }
 

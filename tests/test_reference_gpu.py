@@ -43,3 +43,48 @@ def test_hits_equal_reference_gpu_code(ctx, ntri, nrays, seed):
     both = same & (want_id >= 0)
     assert both.sum() > 0.5 * (want_id >= 0).sum()
     np.testing.assert_allclose(got_t[both], want_t[both], rtol=1e-5, atol=0)
+
+
+@pytest.mark.skipif(not __import__("oracle.bindings", fromlist=["RefPt"]).RefPt.available(),
+                    reason="reference GPU wavefront harness not built")
+def test_wavefront_harness_loads_and_exports_its_entry_points():
+    """The reference GPU wavefront tracer's harness (oracle/_ref/libluxrefpt.so) loads
+    without a GPU call and exports the refpt_* entry points the tests and bench use."""
+    from oracle.bindings import RefPt
+    lib = RefPt().lib
+    for name in ("refpt_scene_create", "refpt_scene_destroy", "refpt_render",
+                 "refpt_render_path_log"):
+        assert hasattr(lib, name)
+
+
+def test_reference_scene_from_descriptor_renders_the_reference_cornell_box():
+    """The reference's Scene rebuilt from lux_b200's scene descriptor
+    (oracle/ref_scene_desc.h) renders the reference's own Cornell box fixture sample for
+    sample (trace_path on the host; no GPU)."""
+    import os
+
+    from lux_b200 import scene as S
+    from oracle.bindings import Ref
+    if not Ref.available():
+        pytest.skip("reference harness not built")
+    root = os.path.abspath(os.path.join(os.path.dirname(__file__), ".."))
+    g = np.load(os.path.join(root, "tests", "golden", "cornell_reference.npz"))
+    w, h, spp, depth, seed = (int(g[k]) for k in ("width", "height", "spp", "max_depth", "seed"))
+    b = S.make_cornell_scene(w, h)
+    ref = Ref()
+    handle = ref.desc_scene(b)
+    try:
+        film, samples = ref.desc_render(handle, S.request(w, h, spp, depth, seed), threads=4,
+                                        samples=True)
+        _, crop = ref.desc_render(handle, S.request(w, h, spp, depth, seed), rows=(4, 12),
+                                  cols=(8, 20), threads=2, samples=True)
+    finally:
+        ref.desc_scene_destroy(handle)
+    assert np.array_equal(samples, g["samples"])
+    want = g["samples"].reshape(h, w, spp, 3)[4:12, 8:20].reshape(-1, spp, 3)
+    assert np.array_equal(crop, want)
+    # Film sums are the sample-order float sums.
+    acc = np.zeros((w * h, 3), np.float32)
+    for s in range(spp):
+        acc = (acc + samples[:, s]).astype(np.float32)
+    assert np.array_equal(film.reshape(-1, 3), acc)

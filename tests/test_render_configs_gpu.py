@@ -1,0 +1,257 @@
+"""The render configurations at their stated sizes against the reference (B200).
+
+Each scene goes to the reference exactly as lux_scene_create receives it (the same
+lux_scene_desc: oracle/ref_scene_desc.h builds the reference's own Scene from it, meshes
+and instances included), and is rendered by
+  * the reference CPU tracer (trace_path, integrator/cpu_path_tracer.cpp:403-562) on all
+    host threads, per sample, and
+  * the reference's own GPU wavefront tracer (WavefrontPathTracer::render,
+    integrator/wavefront_pt.cu:51-84) compiled for sm_100a, per pixel.
+Bars, as the path tracer's other tests state them: per-sample agreement within 1e-4
+relative on >= 99 % of samples for Lambert-only scenes and >= 97 % where GGX, glass and
+filters make CUDA-vs-glibc last-bit differences in sinf/cosf/powf flip later decisions;
+per-pixel means within 3 sigma at equal spp on all but 1 % of pixel channels.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from lux_b200 import scene as S
+from lux_b200 import scenes as SC
+from oracle.bindings import Ref, RefPt
+
+pytestmark = pytest.mark.gpu
+
+THREADS = os.cpu_count() or 1
+need_ref = pytest.mark.skipif(not Ref.available(), reason="reference harness not built")
+need_ref_pt = pytest.mark.skipif(not RefPt.available(),
+                                 reason="reference GPU wavefront harness not built")
+
+
+def _agreement(gpu, ref, rtol=1e-4):
+    close = np.all(np.abs(gpu - ref) <= rtol * (1.0 + np.abs(ref)), axis=-1)
+    return close.mean()
+
+
+def _z_fraction_samples(gpu, ref):
+    """Fraction of pixel channels whose per-sample means differ by more than 3 sigma
+    (both sides' sample variances)."""
+    n = gpu.shape[1]
+    se = np.sqrt((gpu.var(axis=1, ddof=1) + ref.var(axis=1, ddof=1)) / n)
+    diff = np.abs(gpu.mean(axis=1) - ref.mean(axis=1))
+    return np.where(se > 0, diff > 3 * se, diff > 0).mean()
+
+
+def _z_fraction_films(film_a, film_b, samples, spp):
+    """3-sigma test of two film sums at equal spp, the per-pixel variance taken from one
+    renderer's samples (both sides estimate the same integral with the same estimator)."""
+    var = samples.var(axis=1, ddof=1).reshape(film_a.shape)
+    se = np.sqrt(2.0 * var / spp)
+    diff = np.abs(film_a.astype(np.float64) - film_b.astype(np.float64)) / spp
+    return np.where(se > 0, diff > 3 * se, diff > 1e-6 * (1 + np.abs(film_b) / spp)).mean()
+
+
+def _sample_order_sum(samples):
+    film = np.zeros((samples.shape[0], 3), np.float32)
+    for s in range(samples.shape[1]):
+        film = (film + samples[:, s]).astype(np.float32)
+    return film
+
+
+@pytest.fixture(scope="module")
+def ref():
+    return Ref()
+
+
+@need_ref
+def test_cornell_config1_full_size_matches_reference(ctx, ref):
+    """Config 1 at its stated size: 256x256, 64 spp, depth 4, power sampler, seed 1."""
+    w = h = 256
+    b = S.make_cornell_scene(w, h)
+    sc = S.Scene(ctx, b)
+    req = S.request(w, h, 64, 4, 1)
+    gpu = S.render_samples(ctx, sc, req)
+    handle = ref.desc_scene(b)
+    try:
+        ref_film, want = ref.desc_render(handle, req, threads=THREADS, samples=True)
+    finally:
+        ref.desc_scene_destroy(handle)
+    assert _agreement(gpu, want) >= 0.99
+    assert _z_fraction_samples(gpu, want) <= 0.01
+    film = S.render(ctx, sc, req).reshape(-1, 3)
+    assert np.array_equal(film, _sample_order_sum(gpu))
+    rel = np.abs(film - ref_film.reshape(-1, 3)) / (1 + np.abs(ref_film.reshape(-1, 3)))
+    assert np.quantile(rel, 0.99) < 1e-4
+
+
+@need_ref
+def test_heavy_config3_crop_matches_reference(ctx, ref):
+    """Config 3 (1024x1024, depth 8): every pixel of a 64x64 centre crop per sample on
+    the first 4 samples, and the crop's 256-spp film against the reference's 256-spp
+    samples within 3 sigma."""
+    w = h = 1024
+    depth = 8
+    b = SC.heavy_render_scene(w, h)
+    sc = S.Scene(ctx, b)
+    x0, y0, side = 480, 480, 64
+    rows, cols = (y0, y0 + side), (x0, x0 + side)
+    handle = ref.desc_scene(b)
+    try:
+        req4 = S.request(w, h, 4, depth, 1)
+        gpu4 = S.render_samples(ctx, sc, req4).reshape(h, w, 4, 3)
+        gpu4 = gpu4[y0:y0 + side, x0:x0 + side].reshape(-1, 4, 3)
+        _, want4 = ref.desc_render(handle, req4, rows=rows, cols=cols, threads=THREADS,
+                                   samples=True)
+        req = S.request(w, h, 256, depth, 1)
+        film = S.render(ctx, sc, req)[y0:y0 + side, x0:x0 + side]
+        ref_film, want = ref.desc_render(handle, req, rows=rows, cols=cols, threads=THREADS,
+                                         samples=True)
+    finally:
+        ref.desc_scene_destroy(handle)
+    assert _agreement(gpu4, want4) >= 0.97
+    assert _z_fraction_films(film, ref_film, want, 256) <= 0.01
+    assert film.mean() > 0
+
+
+@need_ref
+@pytest.mark.parametrize("which", ["soup", "sphere_grid"])
+def test_batched_config_scenes_match_reference(ctx, ref, which):
+    """The two resident scenes of configs 4 and 5 that no other test renders: the
+    2,097,152-triangle soup, and the 16x16 grid of 256 instances of one 20,480-triangle
+    icosphere with Lambert / GGX / glass / tinted-filter overrides (the two-level TLAS
+    case of scene/gpu_scene_bvh.cuh:44-135)."""
+    w = h = 96
+    spp, depth = 16, 8
+    b = SC.soup_scene(w, h) if which == "soup" else SC.sphere_grid_scene(w, h)
+    sc = S.Scene(ctx, b)
+    req = S.request(w, h, spp, depth, 1)
+    gpu = S.render_samples(ctx, sc, req)
+    handle = ref.desc_scene(b)
+    try:
+        _, want = ref.desc_render(handle, req, threads=THREADS, samples=True)
+    finally:
+        ref.desc_scene_destroy(handle)
+    assert np.isfinite(gpu).all()
+    assert _agreement(gpu, want) >= (0.99 if which == "soup" else 0.97)
+    assert _z_fraction_samples(gpu, want) <= 0.01
+    assert gpu.mean() > 0
+
+
+# ------------------------------------------------------------------ reference GPU tracer
+
+@pytest.fixture(scope="module")
+def ref_pt():
+    return RefPt()
+
+
+def _ref_gpu_film(ref_pt, b, req):
+    handle = ref_pt.scene(b)
+    try:
+        film, _, _ = ref_pt.render(handle, req)
+    finally:
+        ref_pt.destroy(handle)
+    return film
+
+
+@need_ref_pt
+@pytest.mark.parametrize("which", ["cornell_config1", "heavy_512", "sphere_grid"])
+def test_reference_gpu_tracer_images_agree(ctx, ref_pt, which):
+    """This build's film against the reference's own GPU wavefront tracer at equal spp:
+    per-pixel means within 3 sigma, and most pixels equal to 1e-4 (both run CUDA's math
+    functions; they differ where the reference's contracted multiply-adds move a
+    decision)."""
+    if which == "cornell_config1":
+        w = h = 256
+        b, req = S.make_cornell_scene(w, h), S.request(w, h, 64, 4, 1)
+    elif which == "heavy_512":
+        w = h = 512
+        b, req = SC.heavy_render_scene(w, h), S.request(w, h, 16, 8, 1)
+    else:
+        w = h = 128
+        b, req = SC.sphere_grid_scene(w, h), S.request(w, h, 16, 8, 1)
+    sc = S.Scene(ctx, b)
+    film = S.render(ctx, sc, req)
+    samples = S.render_samples(ctx, sc, req)
+    theirs = _ref_gpu_film(ref_pt, b, req)
+    assert np.isfinite(theirs).all()
+    assert _z_fraction_films(film, theirs, samples, req.spp) <= 0.01
+    close = np.all(np.abs(film - theirs) <= 1e-4 * (1 + np.abs(theirs)), axis=-1)
+    assert close.mean() >= 0.5
+
+
+def _paths(records):
+    """Records grouped by path: {(sample, pixel): records in vertex order}."""
+    out = {}
+    for r in records:
+        out.setdefault((int(r["sample_index"]), int(r["pixel_index"])), []).append(r)
+    return out
+
+
+INT_FIELDS = ("depth", "triangle_id", "instance_id", "mesh_id", "local_primitive_id",
+              "material_id", "bsdf_pdf_measure", "light_pdf_measure", "sample_source",
+              "bsdf_flags", "termination_flags", "event_flags")
+FLOAT_FIELDS = ("position", "ng", "ns", "wo", "wi", "throughput_before", "throughput_after",
+                "bsdf_pdf", "light_pdf")
+
+
+def _same_vertex(a, b, rtol=1e-4):
+    if any(int(a[f]) != int(b[f]) for f in INT_FIELDS):
+        return False
+    return all(np.all(np.abs(np.float64(a[f]) - np.float64(b[f]))
+                      <= rtol * (1 + np.abs(np.float64(b[f])))) for f in FLOAT_FIELDS)
+
+
+@need_ref_pt
+@pytest.mark.parametrize("which", ["cornell", "zoo"])
+def test_path_log_matches_reference_gpu_tracer(ctx, ref_pt, which):
+    """lux_render_path_log against the records the reference's GPU tracer itself writes
+    (RenderOutputs::set_path_log, integrator/render_context.h:65-85): the same paths, and
+    on >= 99 % of them (97 % with GGX / glass / filters) every vertex equal (integer
+    fields exactly, floats within 1e-4)."""
+    if which == "cornell":
+        w = h = 32
+        b = S.make_cornell_scene(w, h)
+        req = S.request(w, h, 4, 4, 1)
+        bar = 0.99
+    else:
+        from test_pathtracer_gpu import material_zoo
+        w = h = 32
+        b = material_zoo(w, h)[0]
+        req = S.request(w, h, 4, 6, 5)
+        bar = 0.97
+    sc = S.Scene(ctx, b)
+    film, ours = S.render_path_log(ctx, sc, req)
+    handle = ref_pt.scene(b)
+    try:
+        ref_film, theirs = ref_pt.path_log(handle, req)
+    finally:
+        ref_pt.destroy(handle)
+    assert len(ours) > w * h * req.spp // 2
+    po, pt = _paths(ours), _paths(theirs)
+    # The paths that reach a surface are the same set on both sides (up to camera rays
+    # that graze an edge).
+    assert len(set(po) ^ set(pt)) <= 0.005 * len(pt)
+    same = sum(k in pt and len(po[k]) == len(pt[k])
+               and all(_same_vertex(a, c) for a, c in zip(po[k], pt[k])) for k in po)
+    assert same / len(pt) >= bar
+    close = np.all(np.abs(film - ref_film) <= 1e-4 * (1 + np.abs(ref_film)), axis=-1)
+    assert close.mean() >= 0.5
+
+
+@pytest.mark.parametrize("which", ["cornell", "sphere_grid"])
+def test_traversal_stats_count_the_same_render(ctx, which):
+    """lux_render_traversal_stats renders the same film and rays as lux_render, and its
+    counts have the shape of the reference's visit order: at least one box test per walk
+    (the root at each level), triangle tests, and on the instanced grid instance visits."""
+    w = h = 64
+    b = S.make_cornell_scene(w, h) if which == "cornell" else SC.sphere_grid_scene(w, h)
+    sc = S.Scene(ctx, b)
+    req = S.request(w, h, 4, 6, 1)
+    film = S.render(ctx, sc, req)
+    rays = S.ray_counts(ctx)
+    st = S.traversal_stats(ctx, sc, req)
+    assert np.array_equal(st["film"], film)
+    assert (st["rays"], st["shadow_segments"]) == rays
+    walks = st["rays"] + st["shadow_segments"]
+    assert st["box_tests"] >= walks and st["tri_tests"] > 0 and st["instance_visits"] > 0

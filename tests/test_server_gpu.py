@@ -153,3 +153,29 @@ def test_refits_faster_than_iterations_do_not_starve_requests(ctx):
         assert all(srv.poll(i) == SV.DONE for i in ids)
         refits = srv.stats()["refits"]
         assert 1 <= refits <= pushed
+
+
+def test_mixed_batch_over_the_four_resident_scenes_matches_single_renders(ctx):
+    """A mix over the four resident scenes of the batched and served workloads (Cornell,
+    the displaced icosphere with glass, the 2,097,152-triangle soup and the 256-instance
+    grid), of uneven size, spp and depth: every request's film equals its lux_render
+    film, and a request's film is the same alone as in the mix."""
+    from lux_b200 import scenes as SC
+    builders = SC.resident_scenes(96, 96)
+    scenes = [S.Scene(ctx, b) for b in builders]
+    mix = [(0, S.request(96, 96, 8, 4, 1)), (1, S.request(80, 80, 6, 8, 2)),
+           (2, S.request(64, 64, 4, 6, 3)), (3, S.request(96, 96, 5, 12, 4)),
+           (3, S.request(48, 48, 9, 5, 5, light_sampler=S.SAMPLER_TREE)),
+           (2, S.request(72, 72, 3, 10, 6)), (1, S.request(40, 40, 16, 4, 7)),
+           (0, S.request(56, 56, 2, 9, 8, sample_offset=5))]
+    want = [S.render(ctx, scenes[s], r) for s, r in mix]
+    with SV.Server(scenes, pool_paths=1 << 16) as srv:
+        out = [srv.submit(s, r) for s, r in mix]
+        srv.wait_all(timeout_s=300)
+        assert all(srv.poll(rid) == SV.DONE for rid, _ in out)
+    for (_, film), w in zip(out, want):
+        assert _close(film, w)
+    with SV.Server(scenes, pool_paths=1 << 16) as srv:
+        rid, alone = srv.submit(*mix[3])
+        srv.wait_all(timeout_s=300)
+    assert np.array_equal(alone, out[3][1])
