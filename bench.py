@@ -643,7 +643,13 @@ def render_line(args, name: str, steps: int, warmup: int, nested: bool = False) 
     from lux_b200 import autotune
     probe = req if W * H * spp <= (1 << 23) else S.request(min(W, 512), min(H, 512),
                                                             min(spp, 16), depth, seed)
-    tune = autotune.autotune_render(ctx, sc, probe)
+    if args.no_autotune and not nested:  # profiling: the variant given, other defaults
+        import lux_b200
+        ctx.set_option(lux_b200.OPT_TRACE_VARIANT, args.trace_variant)
+        tune = autotune.TuneResult(args.trace_variant, ctx.get_option(lux_b200.OPT_PATH_BUDGET),
+                                   ctx.get_option(lux_b200.OPT_RENDER_BATCH), 0.0, 0.0, 0)
+    else:
+        tune = autotune.autotune_render(ctx, sc, probe)
     film = torch.zeros((H, W, 3), dtype=torch.float32, device=f"cuda:{local}")
 
     def step(target):
@@ -1145,6 +1151,9 @@ def main():
     ap.add_argument("--trace-variant", type=int, default=0,
                     help="0 auto, 1 one thread per ray, 2 persistent (tunable)")
     ap.add_argument("--trace-budget", type=int, default=16)
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="cornell/heavy: skip the autotuner and render with --trace-variant "
+                         "(profiling captures, so the first launches are the render's)")
     args = ap.parse_args()
     if (args.tris, args.rays, args.queries) != (N_TRIS, N_RAYS, N_QUERIES):
         N_TRIS, N_RAYS, N_QUERIES = args.tris, args.rays, args.queries
