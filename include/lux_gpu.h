@@ -6,7 +6,8 @@
  * opaque; the device memory behind a handle is owned by it.
  *
  * Memory: every array argument may point to host memory or to device memory of the
- * context's device; the library inspects each pointer.  Device inputs and outputs are
+ * context's device; the library inspects each pointer, and device memory of another GPU
+ * is rejected with LUX_ERR_INVALID_ARGUMENT.  Device inputs and outputs are
  * stream ordered on the context's stream and the call returns without waiting.  A host
  * input is staged to the device inside the call; a call with any host output waits
  * for its own work before returning (the behaviour of the reference's std::vector
@@ -75,12 +76,17 @@ int lux_ctx_launch_count(lux_ctx* ctx, int64_t* count);
  *   LUX_OPT_TRACE_BUDGET   traversal steps per refill round of the persistent kernel
  *   LUX_OPT_RENDER_BATCH   paths in flight per wavefront batch (device memory ~200 B each)
  *   LUX_OPT_PATH_BUDGET    traversal steps per refill round of the path tracer's extension and
- *                          shadow kernels (variant 1 uses one thread per path instead) */
+ *                          shadow kernels (variant 1 uses one thread per path instead)
+ * Read only (lux_ctx_get_option), the device memory the context holds for reuse:
+ *   LUX_OPT_SCRATCH_BYTES  growable scratch of builds and queries
+ *   LUX_OPT_STAGING_BYTES  growable staging of host arguments */
 enum lux_option {
     LUX_OPT_TRACE_VARIANT = 1,
     LUX_OPT_TRACE_BUDGET = 2,
     LUX_OPT_RENDER_BATCH = 3,
-    LUX_OPT_PATH_BUDGET = 4
+    LUX_OPT_PATH_BUDGET = 4,
+    LUX_OPT_SCRATCH_BYTES = 5,
+    LUX_OPT_STAGING_BYTES = 6
 };
 int lux_ctx_set_option(lux_ctx* ctx, int32_t option, int64_t value);
 int lux_ctx_get_option(lux_ctx* ctx, int32_t option, int64_t* value);
@@ -209,9 +215,12 @@ int lux_bvh_validate_primitives(lux_ctx* ctx, const lux_bvh* bvh, const float* p
  * results equal lux_bvh_download's sorted_codes and sorted_ids after lux_lbvh_build of
  * the same input.  n above LUX_STATIC_SORT_MAX_PRIMS is rejected with
  * LUX_ERR_INVALID_ARGUMENT.
- * The first call on a device looks up the array's device address for that device; make
- * that first call before any stream capture.  Each call waits for its stream and reports
- * device checks.  All calls on one device share the one array and each call overwrites
+ * The first call on a device looks up the array's device address for that device (and,
+ * with lazy module loading, may be the call that loads the library's kernels on it, which
+ * is when the array's memory is taken); make that first call before any stream capture.
+ * The address is kept for the life of the process, so the library does not support a
+ * cudaDeviceReset of that device while it is loaded.  Each call waits for its stream and
+ * reports device checks.  All calls on one device share the one array and each call overwrites
  * it: calls whose GPU work overlaps (other streams, contexts or host threads on the same
  * device) race, so the caller must order them.
  */

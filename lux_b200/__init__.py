@@ -40,6 +40,8 @@ PRIM_AABBS = 1
 OPT_TRACE_VARIANT = 1   # 0 auto, 1 one thread per ray, 2/4 persistent (binary/4-wide), 3 4-wide
 OPT_TRACE_BUDGET = 2    # traversal steps per refill round (ray queries)
 OPT_PATH_BUDGET = 4     # traversal steps per refill round (path tracer)
+OPT_SCRATCH_BYTES = 5   # read only: the context's reusable device scratch
+OPT_STAGING_BYTES = 6   # read only: the context's reusable device staging
 OPT_RENDER_BATCH = 3    # paths in flight per wavefront batch
 
 # Every symbol include/lux_gpu.h declares, with its ctypes signature.

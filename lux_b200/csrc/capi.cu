@@ -20,15 +20,28 @@ namespace {
 
 thread_local std::string g_error;
 
-bool is_device_pointer(const void* p) {
-    if (!p) return false;
+// Where an argument lives, seen from a context on `device`: host memory (pageable or
+// pinned), memory the device can use directly (its own device memory, or managed
+// memory), or device memory of another GPU, which no call accepts (without peer access a
+// kernel on this device would fault on it).
+enum class PtrKind { kHost, kDevice, kOtherDevice };
+
+PtrKind pointer_kind(const void* p, int device) {
+    if (!p) return PtrKind::kHost;
     cudaPointerAttributes attr;
     cudaError_t err = cudaPointerGetAttributes(&attr, p);
     if (err != cudaSuccess) {
         cudaGetLastError();
-        return false;
+        return PtrKind::kHost;
     }
-    return attr.type == cudaMemoryTypeDevice || attr.type == cudaMemoryTypeManaged;
+    if (attr.type == cudaMemoryTypeManaged) return PtrKind::kDevice;
+    if (attr.type == cudaMemoryTypeDevice)
+        return attr.device == device ? PtrKind::kDevice : PtrKind::kOtherDevice;
+    return PtrKind::kHost;
+}
+
+bool is_device_pointer(const void* p, int device) {
+    return pointer_kind(p, device) == PtrKind::kDevice;
 }
 
 // Carves device staging regions for host arguments out of the context's staging buffer.
@@ -43,6 +56,7 @@ struct Staging {
     };
     std::vector<Item> items;
     size_t total = 0;
+    bool foreign = false;   // an argument is device memory of another GPU
 
     explicit Staging(lux_ctx* c) : ctx(c) {}
 
@@ -52,7 +66,13 @@ struct Staging {
             *device = const_cast<void*>(arg);
             return;
         }
-        if (is_device_pointer(arg)) {
+        PtrKind kind = pointer_kind(arg, ctx->device);
+        if (kind == PtrKind::kOtherDevice) {
+            foreign = true;
+            *device = nullptr;
+            return;
+        }
+        if (kind == PtrKind::kDevice) {
             *device = const_cast<void*>(arg);
             return;
         }
@@ -68,6 +88,9 @@ struct Staging {
     }
 
     int begin() {
+        if (foreign)
+            return lux::fail(LUX_ERR_INVALID_ARGUMENT,
+                             "a device pointer belongs to another GPU than the context's");
         if (items.empty()) return LUX_OK;
         if (total > ctx->staging_bytes) {
             if (ctx->staging) {
@@ -149,8 +172,8 @@ int finish_call(lux_ctx* ctx, Staging& staging) {
 constexpr int kPipeChunks = 4;
 constexpr int32_t kPipeMinRays = 1 << 20;
 
-bool use_pipeline(const float* rays, int32_t nrays) {
-    return nrays >= kPipeMinRays && !is_device_pointer(rays);
+bool use_pipeline(const lux_ctx* ctx, const float* rays, int32_t nrays) {
+    return nrays >= kPipeMinRays && pointer_kind(rays, ctx->device) == PtrKind::kHost;
 }
 
 int ensure_pipeline(lux_ctx* ctx) {
@@ -352,6 +375,8 @@ int lux_ctx_get_option(lux_ctx* ctx, int32_t option, int64_t* value) {
         case LUX_OPT_TRACE_BUDGET: *value = ctx->trace_budget; return LUX_OK;
         case LUX_OPT_RENDER_BATCH: *value = ctx->render_batch; return LUX_OK;
         case LUX_OPT_PATH_BUDGET: *value = ctx->path_budget; return LUX_OK;
+        case LUX_OPT_SCRATCH_BYTES: *value = static_cast<int64_t>(ctx->scratch_bytes); return LUX_OK;
+        case LUX_OPT_STAGING_BYTES: *value = static_cast<int64_t>(ctx->staging_bytes); return LUX_OK;
         default: return lux::fail(LUX_ERR_INVALID_ARGUMENT, "unknown option");
     }
 }
@@ -531,10 +556,12 @@ int lux_lbvh_morton_sort_static(lux_ctx* ctx, const float* prims, int32_t n, int
                              " primitives exceed LUX_STATIC_SORT_MAX_PRIMS (" +
                              std::to_string(LUX_STATIC_SORT_MAX_PRIMS) + ")");
     if (n < 0) return lux::fail(LUX_ERR_INVALID_ARGUMENT, "negative primitive count");
-    if (n > 0 && (!is_device_pointer(prims) || !is_device_pointer(sorted_codes) ||
-                  !is_device_pointer(sorted_ids)))
+    if (n > 0 && (!is_device_pointer(prims, ctx->device) ||
+                  !is_device_pointer(sorted_codes, ctx->device) ||
+                  !is_device_pointer(sorted_ids, ctx->device)))
         return lux::fail(LUX_ERR_INVALID_ARGUMENT,
-                         "lux_lbvh_morton_sort_static takes device pointers only");
+                         "lux_lbvh_morton_sort_static takes device pointers on the context's "
+                         "device only");
     return lux::lbvh_morton_sort_static(ctx, prims, n, kind, morton_bits, sorted_codes,
                                         sorted_ids);
 }
@@ -581,7 +608,7 @@ int lux_trace_closest(lux_ctx* ctx, const lux_bvh* bvh, const float* rays, int32
                       int32_t* hit_id, float* hit_t) {
     if (int st = check_query(ctx, bvh, rays, nrays)) return st;
     if (nrays > 0 && !hit_id) return lux::fail(LUX_ERR_INVALID_ARGUMENT, "null hit_id");
-    if (use_pipeline(rays, nrays)) return trace_pipelined<false>(ctx, bvh, rays, nrays, hit_id, hit_t);
+    if (use_pipeline(ctx, rays, nrays)) return trace_pipelined<false>(ctx, bvh, rays, nrays, hit_id, hit_t);
     Staging staging(ctx);
     void *d_rays, *d_id, *d_t;
     size_t r = static_cast<size_t>(nrays);
@@ -618,7 +645,7 @@ int lux_trace_any(lux_ctx* ctx, const lux_bvh* bvh, const float* rays, int32_t n
                   int32_t* hit_id) {
     if (int st = check_query(ctx, bvh, rays, nrays)) return st;
     if (nrays > 0 && !hit_id) return lux::fail(LUX_ERR_INVALID_ARGUMENT, "null hit_id");
-    if (use_pipeline(rays, nrays)) return trace_pipelined<true>(ctx, bvh, rays, nrays, hit_id, nullptr);
+    if (use_pipeline(ctx, rays, nrays)) return trace_pipelined<true>(ctx, bvh, rays, nrays, hit_id, nullptr);
     Staging staging(ctx);
     void *d_rays, *d_id;
     size_t r = static_cast<size_t>(nrays);
@@ -780,7 +807,7 @@ int lux_render_path_log(lux_ctx* ctx, const lux_scene* scene, const lux_render_r
         return lux::fail(LUX_ERR_INVALID_ARGUMENT, "light sampler: 0 uniform, 1 power or 2 tree");
     if (static_cast<long long>(req->width) * req->height > (1ll << 30))
         return lux::fail(LUX_ERR_INVALID_ARGUMENT, "image too large");
-    if (records && is_device_pointer(records))
+    if (records && pointer_kind(records, ctx->device) != PtrKind::kHost)
         return lux::fail(LUX_ERR_INVALID_ARGUMENT, "path log records must be host memory");
     const size_t bytes = sizeof(float) * 3 * static_cast<size_t>(req->width) * req->height;
     unsigned long long vertices = 0;

@@ -30,6 +30,10 @@ struct lux_ctx {
     // Copy stream and events of the chunked host-ray queries (created on first use).
     cudaStream_t copy_stream = nullptr;
     cudaEvent_t pipe_events[16] = {};
+    // Resident blocks per SM of the persistent kernels on this context's device, by
+    // lux::kOcc* slot, measured on first launch (0: not yet).  Per context, so per device
+    // and under the one-thread-per-context rule of the ABI.
+    int occupancy[8] = {};
 };
 
 struct lux_bvh {
@@ -72,6 +76,33 @@ enum : int {
     kTraceWide = 3,
     kTraceWidePersistent = 4
 };
+
+// Slots of lux_ctx::occupancy.
+enum : int {
+    kOccWideClosest = 0,
+    kOccWideAny = 1,
+    kOccPersistClosest = 2,
+    kOccPersistAny = 3,
+    kOccExtendRefill = 4,
+    kOccShadowRefill = 5
+};
+
+// Resident blocks per SM of `kernel` at `threads` threads on the context's device (at
+// least 1), measured once per context.
+template <typename Kernel>
+inline int occupancy_blocks(lux_ctx* ctx, int slot, Kernel kernel, int threads) {
+    int& v = ctx->occupancy[slot];
+    if (v == 0) {
+        int blocks = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, kernel, threads, 0) !=
+            cudaSuccess) {
+            cudaGetLastError();
+            blocks = 0;
+        }
+        v = blocks > 0 ? blocks : 1;
+    }
+    return v;
+}
 
 // Status helpers (defined in capi.cu).
 int fail(int status, const std::string& message);

@@ -564,13 +564,8 @@ int launch_trace(lux_ctx* ctx, const lux_bvh* bvh, const float* rays, int nrays,
     const float4* r4 = reinterpret_cast<const float4*>(rays);
     if (ctx->trace_variant == kTraceWidePersistent || ctx->trace_variant == kTraceAuto) {
         if (int st = lbvh_ensure_wide(ctx, const_cast<lux_bvh*>(bvh))) return st;
-        static int blocks_per_sm[2] = {0, 0};
-        int& bps = blocks_per_sm[AnyHit ? 1 : 0];
-        if (bps == 0) {
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_trace_wide_persistent<AnyHit>,
-                                                          kTraceThreads, 0);
-            if (bps <= 0) bps = 1;
-        }
+        const int bps = occupancy_blocks(ctx, AnyHit ? kOccWideAny : kOccWideClosest,
+                                         k_trace_wide_persistent<AnyHit>, kTraceThreads);
         int grid = std::min(ctx->sm_count * bps, (nrays + kTraceThreads - 1) / kTraceThreads);
         cudaError_t err = cudaMemsetAsync(ctx->d_counter, 0, sizeof(unsigned), ctx->stream);
         if (err != cudaSuccess) return cuda_fail(err, "ray counter reset");
@@ -595,13 +590,8 @@ int launch_trace(lux_ctx* ctx, const lux_bvh* bvh, const float* rays, int nrays,
         ctx->launches += 1;
         return cuda_fail(cudaGetLastError(), "k_trace");
     }
-    static int blocks_per_sm[2] = {0, 0};
-    int& bps = blocks_per_sm[AnyHit ? 1 : 0];
-    if (bps == 0) {
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_trace_persistent<AnyHit>,
-                                                      kTraceThreads, 0);
-        if (bps <= 0) bps = 1;
-    }
+    const int bps = occupancy_blocks(ctx, AnyHit ? kOccPersistAny : kOccPersistClosest,
+                                     k_trace_persistent<AnyHit>, kTraceThreads);
     int grid = ctx->sm_count * bps;
     int needed = (nrays + kTraceThreads - 1) / kTraceThreads;
     if (grid > needed) grid = needed;

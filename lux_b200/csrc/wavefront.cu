@@ -407,18 +407,10 @@ int render(lux_ctx* ctx, const lux_scene* scene, const lux_render_request& req, 
     const SceneView& sc = scene->view;
     cudaStream_t s = ctx->stream;
     int grid = ctx->sm_count * 8;
-    static int refill_blocks = 0;
-    if (refill_blocks == 0) {
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&refill_blocks, k_extend_refill, kThreads, 0);
-        if (refill_blocks <= 0) refill_blocks = 1;
-    }
-    const int refill_grid = ctx->sm_count * refill_blocks;
-    static int shadow_blocks = 0;
-    if (shadow_blocks == 0) {
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&shadow_blocks, k_shadow_refill, kThreads, 0);
-        if (shadow_blocks <= 0) shadow_blocks = 1;
-    }
-    const int shadow_grid = ctx->sm_count * shadow_blocks;
+    const int refill_grid =
+        ctx->sm_count * occupancy_blocks(ctx, kOccExtendRefill, k_extend_refill, kThreads);
+    const int shadow_grid =
+        ctx->sm_count * occupancy_blocks(ctx, kOccShadowRefill, k_shadow_refill, kThreads);
     cudaError_t err = cudaMemsetAsync(rt.rays, 0, 16, s);
     if (!per_sample && err == cudaSuccess)
         err = cudaMemsetAsync(out, 0, sizeof(float) * 3 * size_t(pixels), s);

@@ -18,10 +18,11 @@ import lux_b200
 from lux_b200 import obj as O
 from lux_b200 import scene as S
 from oracle.bindings import Ref
+from oracle.build import REF_ROOT
 
 ROOT = os.path.abspath(os.path.join(os.path.dirname(__file__), ".."))
 CLI = os.path.join(ROOT, "lux_b200", "lux-render")
-REF_ASSETS = "/root/reference/assets"
+REF_ASSETS = os.path.join(REF_ROOT, "assets")
 THREADS = os.cpu_count() or 1
 KEYS = ("vertices", "normals", "uvs", "indices", "material_ids", "object_to_world", "bounds")
 

@@ -60,14 +60,33 @@ def test_two_calls_in_a_row_match_the_build(ctx):
     torch.cuda.synchronize()
     lib = lux_b200.load_library()
     free_before = torch.cuda.mem_get_info()[0]
+    held = [ctx.get_option(lux_b200.OPT_SCRATCH_BYTES), ctx.get_option(lux_b200.OPT_STAGING_BYTES)]
     for _ in range(2):
         assert lib.lux_lbvh_morton_sort_static(ctx.handle, d_prims.data_ptr(), prims.shape[0],
                                                kind, bits, codes.data_ptr(),
                                                ids.data_ptr()) == lux_b200.LUX_OK
     assert torch.cuda.mem_get_info()[0] == free_before
+    # Nor does it grow the context's own reusable scratch or staging.
+    assert [ctx.get_option(lux_b200.OPT_SCRATCH_BYTES),
+            ctx.get_option(lux_b200.OPT_STAGING_BYTES)] == held
     want_codes, want_ids = _existing(ctx, prims, kind, bits)
     assert np.array_equal(codes.cpu().numpy().view(np.uint64), want_codes)
     assert np.array_equal(ids.cpu().numpy(), want_ids)
+
+
+def test_matches_the_reference_builders_own_order(ctx, golden_lbvh):
+    """Directly against the reference: the fixtures the reference's own host LBVH wrote
+    (build_cpu_lbvh_tree, bvh/cpu_lbvh_builder.h:163-259; tests/golden/make_golden.py) give
+    the 30-bit codes and the stable sorted primitive order; two passes over all of them in
+    a row, so each call starts from the previous one's array contents."""
+    for _ in range(2):
+        for name, case in golden_lbvh.items():
+            prims = case["prims"]
+            if len(prims) < 2:   # one primitive: no order to check, its code is unused
+                continue
+            codes, ids = _static_sort(ctx, prims, int(case["kind"]), 30)
+            assert np.array_equal(ids, case["sorted_ids"]), name
+            assert np.array_equal(codes, case["sorted_codes"].astype(np.uint64)), name
 
 
 def test_limits_and_pointer_kinds_are_checked(ctx):
