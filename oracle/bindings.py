@@ -549,3 +549,131 @@ class RefPt:
             raise RuntimeError(f"reference GPU path log: {int(count[0])} records exceed "
                                f"the capacity {capacity}")
         return film, records[:int(count[0])]
+
+
+REF_SHIM_LIB = os.path.join(HERE, "_ref", "libluxshim.so")
+
+
+class RefShim:
+    """The drop-in shims (lux_b200/integration/) called through the reference's own types
+    (oracle/ref_shim_harness.cpp; oracle/_ref/libluxshim.so, linked to liblux_gpu.so)."""
+
+    def __init__(self, path: str = REF_SHIM_LIB):
+        if not os.path.exists(path):
+            raise FileNotFoundError(f"{path} missing (built only where the reference exists)")
+        lib = ctypes.CDLL(path)
+        _S = ctypes.c_char_p
+        lib.shim_build.argtypes = [_P, _P, _I, _S, _I]
+        lib.shim_build.restype = _P
+        lib.shim_destroy.argtypes = [_P]
+        lib.shim_refit.argtypes = [_P, _P, _P, _I, _S, _I]
+        lib.shim_refit.restype = _I
+        lib.shim_download.argtypes = [_P, _P, _P, _P, _P, _P, _P, _P, _P, _S, _I]
+        lib.shim_download.restype = _I
+        lib.shim_validate.argtypes = [_P, _P, _P, _I, _P, _P, _S, _I]
+        lib.shim_validate.restype = _I
+        lib.shim_intersect.argtypes = [_P, _P, _I, _P, _I, _P, _P, _S, _I]
+        lib.shim_intersect.restype = _I
+        lib.shim_overlap.argtypes = [_P, _P, _I, _P, _P, _S, _I]
+        lib.shim_overlap.restype = ctypes.c_longlong
+        lib.shim_render.argtypes = [_P, _P, _P, _P, _P, _P, _I, _S, _I]
+        lib.shim_render.restype = ctypes.c_longlong
+        self.lib = lib
+        self.err = ctypes.create_string_buffer(1024)
+
+    @staticmethod
+    def available(path: str = REF_SHIM_LIB) -> bool:
+        return os.path.exists(path)
+
+    def _fail(self, what):
+        raise RuntimeError(f"{what}: {self.err.value.decode()}")
+
+    def build(self, boxes, ids):
+        """build_gpu_lbvh over boxes (n x 6) with primitive ids; an opaque GpuBvh*."""
+        boxes = np.ascontiguousarray(boxes, np.float32).reshape(-1, 6)
+        ids = np.ascontiguousarray(ids, np.int32)
+        h = self.lib.shim_build(boxes.ctypes.data, ids.ctypes.data, len(ids), self.err, 1024)
+        if not h and len(ids):
+            self._fail("build_gpu_lbvh")
+        return h
+
+    def destroy(self, h):
+        self.lib.shim_destroy(h)
+
+    def refit(self, h, boxes, ids) -> bool:
+        boxes = np.ascontiguousarray(boxes, np.float32).reshape(-1, 6)
+        ids = np.ascontiguousarray(ids, np.int32)
+        st = self.lib.shim_refit(h, boxes.ctypes.data, ids.ctypes.data, len(ids), self.err, 1024)
+        if st < 0:
+            self._fail("refit_gpu_lbvh")
+        return bool(st)
+
+    def download(self, h, n):
+        """download_bvh_for_validation as arrays, plus GpuBvh::root_bounds."""
+        m = max(2 * n - 1, 1)
+        out = {k: np.zeros(m, np.int32) for k in ("left", "right", "first", "count")}
+        bounds = np.zeros((m, 6), np.float32)
+        pids = np.zeros(max(n, 1), np.int32)
+        root = np.zeros(1, np.int32)
+        rb = np.zeros(6, np.float32)
+        k = self.lib.shim_download(h, root.ctypes.data, out["left"].ctypes.data,
+                                   out["right"].ctypes.data, out["first"].ctypes.data,
+                                   out["count"].ctypes.data, bounds.ctypes.data, pids.ctypes.data,
+                                   rb.ctypes.data, self.err, 1024)
+        if k < 0:
+            self._fail("download_bvh_for_validation")
+        out = {key: v[:k] for key, v in out.items()}
+        out.update(bounds=bounds[:k], primitive_ids=pids[:n], root=int(root[0]), root_bounds=rb)
+        return out
+
+    def validate(self, h, boxes, ids):
+        """(validate_gpu_bvh_structure, validate_gpu_bvh_matches_primitives, message)."""
+        boxes = np.ascontiguousarray(boxes, np.float32).reshape(-1, 6)
+        ids = np.ascontiguousarray(ids, np.int32)
+        s, m = ctypes.c_int(), ctypes.c_int()
+        msg = ctypes.create_string_buffer(512)
+        if self.lib.shim_validate(h, boxes.ctypes.data, ids.ctypes.data, len(ids),
+                                  ctypes.byref(s), ctypes.byref(m), msg, 512) < 0:
+            raise RuntimeError("validators: " + msg.value.decode())
+        return bool(s.value), bool(m.value), msg.value.decode()
+
+    def intersect(self, h, tris_by_id, rays):
+        tris = np.ascontiguousarray(tris_by_id, np.float32).reshape(-1, 9)
+        rays = np.ascontiguousarray(rays, np.float32).reshape(-1, 8)
+        hid = np.zeros(len(rays), np.int32)
+        ht = np.zeros(len(rays), np.float32)
+        if self.lib.shim_intersect(h, tris.ctypes.data, len(tris), rays.ctypes.data, len(rays),
+                                   hid.ctypes.data, ht.ctypes.data, self.err, 1024) < 0:
+            self._fail("intersect_gpu_bvh_stackless")
+        return hid, ht
+
+    def overlap(self, left, right, max_pairs):
+        """(pairs k x 2, found_count, truncated) of query_aabb_overlaps_self (right None)
+        or query_aabb_overlaps_cross."""
+        pairs = np.zeros((max(max_pairs, 1), 2), np.int32)
+        trunc = ctypes.c_int()
+        found = self.lib.shim_overlap(left, right, max_pairs, pairs.ctypes.data,
+                                      ctypes.byref(trunc), self.err, 1024)
+        if found < 0:
+            self._fail("query_aabb_overlaps")
+        return pairs[:min(found, max_pairs)], int(found), bool(trunc.value)
+
+    def render(self, builder, req, aovs=False, path_log=False):
+        """make_integrator(WavefrontPathTracer)->render on the reference's Scene (the
+        reference's Cornell box when builder is None): (film, shadow, ng, ns, log count)."""
+        from lux_b200 import scene as S
+
+        keep = None
+        desc_ptr = None
+        if builder is not None:
+            desc, keep = S.scene_desc(builder)
+            desc_ptr = ctypes.addressof(desc)
+        shape = (req.height, req.width, 3)
+        film = np.zeros(shape, np.float32)
+        extra = [np.zeros(shape, np.float32) if aovs else None for _ in range(3)]
+        n = self.lib.shim_render(desc_ptr, ctypes.addressof(req), film.ctypes.data,
+                                 *(_addr(a) for a in extra), int(path_log), self.err, 1024)
+        del keep
+        if n < 0:
+            self._fail("WavefrontPathTracer::render")
+        return film, extra[0], extra[1], extra[2], int(n)

@@ -5,6 +5,9 @@
 3. oracle/_ref/libluxref.so: the reference's own host code.
 4. oracle/_ref/libluxrefgpu.so: the reference's own GPU LBVH (bvh/gpu_bvh.cu,
    bvh/bvh_overlap.cu) behind oracle/ref_gpu_harness.cu, compiled with nvcc for sm_100a.
+6. oracle/_ref/libluxshim.so: the drop-in shims (lux_b200/integration/) compiled
+   against the reference's headers and called through its own types
+   (oracle/ref_shim_harness.cpp), linked to lux_b200/liblux_gpu.so.
 5. oracle/_ref/libluxrefpt.so: the reference's own GPU wavefront path tracer
    (integrator/wavefront_*.cu, scene/prepared_scene.cu, bvh/gpu_bvh.cu,
    light/light_distribution.cpp) behind oracle/ref_pt_gpu_harness.cu, compiled with nvcc
@@ -163,10 +166,69 @@ def build_ref_pt_gpu(force=False):
     return REF_PT_OUT
 
 
+REF_SHIM_OUT = os.path.join(OUT_DIR, "libluxshim.so")
+SHIM_DIR = os.path.join(HERE, "..", "lux_b200", "integration")
+LUX_LIB_DIR = os.path.join(HERE, "..", "lux_b200")
+# Reference sources the shimmed integrator factory links against (CPU scene preparation:
+# the shim's integrator does not need PreparedScene::prepare_gpu).
+REF_SHIM_SOURCES = [
+    ("src/integrator/integrator_factory.cpp", ["-DLUX_ENABLE_CUDA=1"]),
+    ("src/integrator/cpu_path_tracer.cpp", []),
+    ("src/light/light_distribution.cpp", []),
+    ("src/scene/prepared_scene_cpu.cpp", []),
+]
+
+
+def build_ref_shim(force=False):
+    """Compile the drop-in shims (lux_b200/integration/) against the reference's headers,
+    with oracle/ref_shim_harness.cpp and the reference sources above, linked to
+    lux_b200/liblux_gpu.so; None when the reference is absent."""
+    import concurrent.futures
+
+    src_dir = os.path.join(REF_ROOT, "src")
+    if not os.path.isdir(src_dir):
+        return None
+    include = os.path.join(HERE, "..", "include")
+    shim_cpp = os.path.join(SHIM_DIR, "gpu_bvh_lux.cpp")
+    shim_cu = os.path.join(SHIM_DIR, "wavefront_pt_lux.cu")
+    harness = os.path.join(HERE, "ref_shim_harness.cpp")
+    units = [(shim_cpp, []), (shim_cu, []), (harness, [])] + [
+        (os.path.join(REF_ROOT, s), f) for s, f in REF_SHIM_SOURCES]
+    deps = [u for u, _ in units] + [os.path.join(SHIM_DIR, "lux_shim.h"),
+                                    os.path.join(HERE, "ref_scene_desc.h"),
+                                    os.path.join(include, "lux_gpu.h")] + _ref_headers(src_dir)
+    if not force and not _stale(REF_SHIM_OUT, deps):
+        return REF_SHIM_OUT
+    obj_dir = os.path.join(OUT_DIR, "shim_obj")
+    os.makedirs(obj_dir, exist_ok=True)
+    incs = ["-I", src_dir, "-I", include, "-I", SHIM_DIR, "-I", HERE]
+
+    def compile_one(unit):
+        src, flags = unit
+        obj = os.path.join(obj_dir, os.path.basename(src) + ".o")
+        if src.endswith(".cu") or src == harness:
+            cmd = ["nvcc", *NVCCFLAGS, *incs, *flags, "-x", "cu", "-c", src, "-o", obj]
+        else:
+            cmd = ["g++", *CXXFLAGS, *incs, *flags, "-c", src, "-o", obj]
+        res = subprocess.run(cmd, capture_output=True, text=True)
+        if res.returncode != 0:
+            raise RuntimeError(f"compile failed for {src}:\n{res.stderr[-4000:]}")
+        return obj
+
+    with concurrent.futures.ThreadPoolExecutor(max_workers=len(units)) as pool:
+        objs = list(pool.map(compile_one, units))
+    cmd = ["nvcc", "-shared", "-gencode", "arch=compute_100a,code=sm_100a", "-o", REF_SHIM_OUT,
+           *objs, "-L", LUX_LIB_DIR, "-llux_gpu", "-Xlinker", "-rpath=$ORIGIN/../../lux_b200",
+           "-Xlinker", "--no-undefined"]
+    subprocess.run(cmd, check=True)
+    return REF_SHIM_OUT
+
+
 def build(force=False):
     build_pt64(force)
     build_ref_gpu(force)
     build_ref_pt_gpu(force)
+    build_ref_shim(force)
     return build_oracle(force), build_ref(force)
 
 
