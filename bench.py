@@ -1014,13 +1014,15 @@ def serving_line(args, rates: list[float]) -> dict:
         for sc_i in range(len(scenes)):
             S.render(ctx, scenes[sc_i], rr[largest], films[largest])
         torch.cuda.synchronize()
-        service, plain_rays = [], 0
+        service, host_service, plain_rays = [], [], 0
         for r, q, f in zip(reqs, rr, films):
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            h0 = time.perf_counter()
             e0.record(stream)
             S.render(ctx, scenes[r["scene"]], q, f)
             e1.record(stream)
             torch.cuda.synchronize()
+            host_service.append(time.perf_counter() - h0)
             service.append(e0.elapsed_time(e1) * 1e-3)
             plain_rays += sum(S.ray_counts(ctx))
         free_at, fifo_lat = 0.0, []
@@ -1068,7 +1070,9 @@ def serving_line(args, rates: list[float]) -> dict:
                         "fifo_plain_mrays_s": plain_rays / max(free_at, 1e-9) / 1e6,
                         "plain_service_ms": {"p50": float(np.percentile(service, 50) * 1e3),
                                              "max": float(np.max(service) * 1e3),
-                                             "argmax": int(np.argmax(service))}})
+                                             "argmax": int(np.argmax(service)),
+                                             "argmax_host_ms": float(host_service[int(np.argmax(service))] * 1e3),
+                                             "argmax_request": reqs[int(np.argmax(service))]}})
     clock_info = clocks.stop()
     best = max(results, key=lambda r: r["mrays_s"])
     return {"metric": "p50/p99 render-request latency and Mrays/s (served)",

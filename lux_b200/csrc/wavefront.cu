@@ -33,10 +33,13 @@ namespace {
 constexpr int kSlots = 9;  // per-bounce counters: ray, 5 material queues, shadow, extend and
                            // shadow cursors
 
+// Depth slots of the queue counters: every max_depth the API accepts (0..1000), so the
+// counters are allocated once per runtime and a deeper request never reallocates.
+constexpr int kMaxDepthSlots = 1000 + 2;
+
 struct Runtime {
     PathPool pool;
-    int max_depth = -1;
-    int* counts = nullptr;               // (max_depth + 2) * kSlots
+    int* counts = nullptr;               // kMaxDepthSlots * kSlots
     unsigned long long* rays = nullptr;  // [0] camera + extension, [1] shadow segments
     long long last_counts[2] = {0, 0};
 };
@@ -322,6 +325,9 @@ int path_pool_alloc(PathPool& p, int capacity) {
 
 namespace {
 
+// Grows the path pool to at least `capacity` paths (never shrinks it); the counters are
+// allocated once.  Only a larger batch than any before it reallocates, so a stream of
+// renders of mixed depth and size sized for its largest batch allocates nothing.
 int runtime_reserve(lux_ctx* ctx, int capacity, int max_depth) {
     Runtime* rt = runtime_of(ctx);
     if (!rt) {
@@ -329,12 +335,14 @@ int runtime_reserve(lux_ctx* ctx, int capacity, int max_depth) {
         if (!rt) return fail(LUX_ERR_OUT_OF_MEMORY, "runtime allocation failed");
         ctx->render_runtime = rt;
     }
-    if (rt->pool.capacity >= capacity && rt->max_depth >= max_depth) return LUX_OK;
+    if (max_depth + 2 > kMaxDepthSlots)
+        return fail(LUX_ERR_INVALID_ARGUMENT, "max_depth must be in 0..1000");
+    if (rt->pool.capacity >= capacity && rt->counts && rt->rays) return LUX_OK;
     cudaStreamSynchronize(ctx->stream);
     runtime_release(rt);
     int st = path_pool_alloc(rt->pool, capacity);
     cudaError_t err = cudaSuccess;
-    if (!st) err = cudaMalloc(&rt->counts, sizeof(int) * kSlots * (max_depth + 2));
+    if (!st) err = cudaMalloc(&rt->counts, sizeof(int) * kSlots * kMaxDepthSlots);
     if (!st && err == cudaSuccess) err = cudaMalloc(&rt->rays, 16);
     if (!st && err != cudaSuccess) {
         cudaGetLastError();
@@ -344,7 +352,6 @@ int runtime_reserve(lux_ctx* ctx, int capacity, int max_depth) {
         runtime_release(rt);
         return st;
     }
-    rt->max_depth = max_depth;
     return LUX_OK;
 }
 
