@@ -24,6 +24,9 @@ import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIBRARY_PATH = os.path.join(_HERE, "liblux_gpu.so")
+# Validation build: the same sources with float sinf/cosf/powf/acosf/atan2f evaluated in
+# double and rounded (LUX_ROUNDED_DOUBLE_MATH); only the rounding-isolation test uses it.
+DMATH_LIBRARY_PATH = os.path.join(_HERE, "liblux_gpu_dmath.so")
 
 LUX_OK = 0
 LUX_ERR_INVALID_ARGUMENT = 1
@@ -158,8 +161,10 @@ def _count(a, per: int) -> int:
 class Context:
     """A lux_ctx: one CUDA device and one stream (``stream`` is a cudaStream_t int)."""
 
-    def __init__(self, device: int = 0, stream: int | None = None):
-        lib = load_library()
+    def __init__(self, device: int = 0, stream: int | None = None, library: str | None = None):
+        """library: another build of the same ABI to bind (the validation build
+        liblux_gpu_dmath.so); default the product library."""
+        lib = load_library(library or LIBRARY_PATH)
         handle = _P()
         _check(lib.lux_ctx_create(ctypes.byref(handle), device, stream))
         self._h = handle

@@ -45,14 +45,14 @@ def _headers():
     return out
 
 
-def _compile(src, verbose):
-    obj = os.path.join(OBJ_DIR, os.path.splitext(os.path.basename(src))[0] + ".o")
+def _compile(src, verbose, obj_dir=OBJ_DIR, extra=()):
+    obj = os.path.join(obj_dir, os.path.splitext(os.path.basename(src))[0] + ".o")
     if src.endswith(".cpp"):  # host-only code (the OBJ loader)
         cmd = ["g++", "-std=c++17", "-O2", "-fPIC", "-Wall",
                "-I", os.path.join(HERE, "..", "include"), "-c", src, "-o", obj]
     else:
-        cmd = [NVCC, *NVCC_FLAGS, *PER_FILE_FLAGS.get(os.path.basename(src), []), "-c", src,
-               "-o", obj]
+        cmd = [NVCC, *NVCC_FLAGS, *PER_FILE_FLAGS.get(os.path.basename(src), []), *extra,
+               "-c", src, "-o", obj]
     if verbose and not src.endswith(".cpp"):
         cmd.insert(1, "-Xptxas=-v")
     res = subprocess.run(cmd, capture_output=True, text=True)
@@ -80,6 +80,33 @@ def build(force=False, verbose=False):
     subprocess.run(cmd, check=True)
     build_cli(force=True)
     return LIB
+
+
+DMATH_LIB = os.path.join(HERE, "liblux_gpu_dmath.so")
+DMATH_OBJ_DIR = os.path.join(HERE, "_build_dmath")
+
+
+def build_dmath(force=False):
+    """The validation build liblux_gpu_dmath.so: the same sources with
+    LUX_ROUNDED_DOUBLE_MATH (lux_math.cuh), whose float sinf/cosf/powf/acosf/atan2f are
+    evaluated in double and rounded.  Only the rounding-isolation test loads it; it binds
+    its own symbols (-Bsymbolic) so that it can sit beside liblux_gpu.so in one process."""
+    os.makedirs(DMATH_OBJ_DIR, exist_ok=True)
+    sources = [s for s in _sources() if s.endswith(".cu")]
+    deps = sources + _headers() + [os.path.abspath(__file__)]
+    if not force and os.path.exists(DMATH_LIB):
+        if os.path.getmtime(DMATH_LIB) >= max(os.path.getmtime(p) for p in deps):
+            return DMATH_LIB
+    extra = ("-DLUX_ROUNDED_DOUBLE_MATH",)
+    with concurrent.futures.ThreadPoolExecutor(max_workers=os.cpu_count() or 4) as pool:
+        results = list(pool.map(lambda s: _compile(s, False, DMATH_OBJ_DIR, extra), sources))
+    objs = [o for o, _ in results]
+    # The OBJ loader has no floating-point functions: the product object serves both.
+    objs.append(os.path.join(OBJ_DIR, "obj.o"))
+    cmd = [NVCC, "-shared", "-gencode", "arch=compute_100a,code=sm_100a", "-o", DMATH_LIB,
+           *objs, "-lcudart", "-Xlinker", "-Bsymbolic"]
+    subprocess.run(cmd, check=True)
+    return DMATH_LIB
 
 
 def build_cli(force=False):

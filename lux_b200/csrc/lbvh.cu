@@ -2,11 +2,16 @@
 //
 // Pipeline (one stream, no host synchronisation):
 //   1. k_root_reduce   per-primitive boxes -> union (order-free atomics on ordered ints)
-//   2. k_morton        30-/63-bit Morton code of each box centroid
-//   3. radix sort      stable LSD sort of (code, input index), 8-bit digits
-//   4. k_karras        Karras 2012 hierarchy over the sorted codes
+//   2. k_morton_hist   30-/63-bit Morton code of each box centroid, and the digit
+//                      histograms of every sort pass from the same pass over the codes
+//   3. radix sort      stable LSD sort of (code, input index), 8-bit digits: one
+//                      k_onesweep launch per digit (local ranking, then the tile's digit
+//                      offsets by a decoupled look-back over the earlier tiles)
+//   4. k_karras        Karras 2012 hierarchy over the sorted codes (+ each node's range)
 //   5. k_leaf_climb    leaf boxes + triangle records in sorted order, then one bottom-up
-//                      climb per leaf that writes every child box into its parent
+//                      climb per leaf that writes every child box into its parent: in
+//                      shared memory while a node's leaves lie in the block's own leaves,
+//                      through global memory above that
 //
 // Reference counterparts (src/): bvh/gpu_bvh.cu:135-149 (codes), 582-584 (sort),
 // 151-180 (hierarchy), 182-214 (bottom-up boxes), 535-613 (build/refit drivers);
@@ -32,6 +37,25 @@ constexpr int kSortItems = 16;
 constexpr int kSortTile = kThreads * kSortItems;  // keys per tile
 constexpr int kScanThreads = 1024;
 constexpr int kClimbBound = 160;                 // > max tree depth (64 + 96 bits)
+constexpr int kMaxPasses = 8;                    // 8-bit digits of a 63-bit key
+constexpr long long kLookbackSpins = 1ll << 22;  // bound of one look-back wait
+
+// Relaxed device-scope accesses of the look-back words (each word carries its own value,
+// so no other ordering is needed) and an acquire-release add for the climb's flags.
+LUX_D unsigned long long ld_relaxed(const unsigned long long* p) {
+    unsigned long long v;
+    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+LUX_D void st_relaxed(unsigned long long* p, unsigned long long v) {
+    asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+LUX_D unsigned atomic_add_acq_rel(unsigned* p, unsigned v) {
+    unsigned old;
+    asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], %2;"
+                 : "=r"(old) : "l"(p), "r"(v) : "memory");
+    return old;
+}
 
 LUX_D unsigned lanemask_lt() {
     unsigned m;
@@ -115,6 +139,160 @@ __global__ void __launch_bounds__(kThreads) k_morton(const float* prims, int n,
 template <typename Key>
 LUX_D unsigned digit_of(Key k, int shift) {
     return static_cast<unsigned>(k >> shift) & (kRadix - 1);
+}
+
+// Morton codes (as k_morton) plus, for every sort pass p, the count of each 8-bit digit
+// of the codes: hist[p * kRadix + d], accumulated in shared memory (one copy per warp
+// for 30-bit keys, two for the 63-bit keys' eight passes, to stay within 48 KB) and added
+// to the global counts once per block.
+template <int Kind, typename Key, int Passes>
+__global__ void __launch_bounds__(kThreads) k_morton_hist(const float* prims, int n,
+                                                          const unsigned* root_ord,
+                                                          Key* codes, unsigned* hist) {
+    constexpr int kCopies = Passes <= 4 ? kThreads / 32 : 2;
+    __shared__ unsigned h[kCopies][Passes][kRadix];
+    for (int i = threadIdx.x; i < kCopies * Passes * kRadix; i += kThreads) (&h[0][0][0])[i] = 0;
+    __syncthreads();
+    const int warp = (threadIdx.x >> 5) % kCopies;
+    box3 root = decode_root(root_ord);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        f3 v0, v1, v2;
+        box3 b;
+        load_prim<Kind>(prims, i, v0, v1, v2, b);
+        Key c = sizeof(Key) == 4 ? static_cast<Key>(morton30(b, root))
+                                 : static_cast<Key>(morton63(b, root));
+        codes[i] = c;
+#pragma unroll
+        for (int p = 0; p < Passes; ++p) atomicAdd(&h[warp][p][digit_of(c, 8 * p)], 1u);
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < Passes * kRadix; i += kThreads) {
+        unsigned v = 0;
+#pragma unroll
+        for (int w = 0; w < kCopies; ++w) v += (&h[w][0][0])[i];
+        if (v) atomicAdd(hist + i, v);
+    }
+}
+
+// Exclusive prefix of each pass's digit counts: bases[p * kRadix + d] = the number of
+// keys whose pass-p digit is below d.  One block of kRadix threads per pass.
+__global__ void __launch_bounds__(kRadix) k_digit_bases(const unsigned* hist, unsigned* bases) {
+    __shared__ unsigned warp_sums[kRadix / 32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const unsigned v = hist[blockIdx.x * kRadix + threadIdx.x];
+    unsigned incl = v;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        unsigned o = __shfl_up_sync(0xffffffffu, incl, off);
+        if (lane >= off) incl += o;
+    }
+    if (lane == 31) warp_sums[warp] = incl;
+    __syncthreads();
+    unsigned before = 0;
+    for (int w = 0; w < warp; ++w) before += warp_sums[w];
+    bases[blockIdx.x * kRadix + threadIdx.x] = before + incl - v;
+}
+
+// Look-back words: value in the low 32 bits, state in the high ones (0: not yet
+// published; aggregate: this tile's own count; prefix: the count over tiles 0..t).
+constexpr unsigned long long kTileAggregate = 1ull << 32;
+constexpr unsigned long long kTilePrefix = 2ull << 32;
+
+// One stable LSD pass over all keys.  Tiles of kSortTile keys are taken in launch order
+// (an atomic counter), ranked inside the tile as k_sort_downsweep ranks them (per-warp
+// digit counts in input order, so equal digits keep input order), and placed at
+// bases[d] + (digit d's count in earlier tiles) + the rank in the tile.  The count in
+// earlier tiles comes from a decoupled look-back: each tile publishes its per-digit
+// count, then walks back over the earlier tiles' words until one holds an inclusive
+// prefix, and publishes its own inclusive prefix.  A tile waits only on tiles that were
+// handed out before it (and so are running or done); each wait is bounded and a wait
+// that runs out reports through `error`.
+template <typename Key, bool First>
+__global__ void __launch_bounds__(kThreads) k_onesweep(const Key* keys_in, const int* vals_in,
+                                                       Key* keys_out, int* vals_out, int n,
+                                                       int shift, const unsigned* bases,
+                                                       unsigned long long* lookback,
+                                                       unsigned* tile_counter, int* error) {
+    constexpr int kWarps = kThreads / 32;
+    constexpr int kWarpSpan = kSortTile / kWarps;
+    __shared__ unsigned wcount[kWarps][kRadix];
+    __shared__ unsigned gbase[kRadix];
+    __shared__ int tile_s;
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    if (threadIdx.x == 0) tile_s = static_cast<int>(atomicAdd(tile_counter, 1u));
+    for (int i = threadIdx.x; i < kWarps * kRadix; i += kThreads) (&wcount[0][0])[i] = 0;
+    __syncthreads();
+    const int tile = tile_s;
+
+    const unsigned lt = lanemask_lt();
+    const int base = tile * kSortTile + warp * kWarpSpan;
+    Key k[kSortItems];
+    int v[kSortItems];
+    unsigned rank[kSortItems];
+#pragma unroll
+    for (int j = 0; j < kSortItems; ++j) {
+        int idx = base + j * 32 + lane;
+        bool valid = idx < n;
+        k[j] = valid ? keys_in[idx] : Key(0);
+        v[j] = First ? idx : (valid ? vals_in[idx] : 0);
+        unsigned d = valid ? digit_of(k[j], shift) : kRadix;
+        unsigned peers = __match_any_sync(0xffffffffu, d);
+        unsigned before = valid ? wcount[warp][d] : 0u;
+        __syncwarp();
+        if (valid && lane == __ffs(peers) - 1) wcount[warp][d] = before + __popc(peers);
+        __syncwarp();
+        rank[j] = valid ? before + __popc(peers & lt) : 0xffffffffu;
+    }
+    __syncthreads();
+    {
+        const int d = threadIdx.x;
+        unsigned total = 0;
+#pragma unroll
+        for (int w = 0; w < kWarps; ++w) {
+            unsigned c = wcount[w][d];
+            wcount[w][d] = total;
+            total += c;
+        }
+        unsigned long long* mine = lookback + static_cast<size_t>(tile) * kRadix + d;
+        unsigned prefix = 0;
+        if (tile == 0) {
+            st_relaxed(mine, kTilePrefix | total);
+        } else {
+            st_relaxed(mine, kTileAggregate | total);
+            int t = tile - 1;
+            long long spins = 0;
+            while (t >= 0) {
+                const unsigned long long w = ld_relaxed(lookback + static_cast<size_t>(t) * kRadix + d);
+                const unsigned long long state = w & ~0xffffffffull;
+                if (state == 0) {
+                    if (++spins > kLookbackSpins) {
+                        atomicOr(error, kErrLoopBound);
+                        break;
+                    }
+                    continue;
+                }
+                prefix += static_cast<unsigned>(w);
+                if (state == kTilePrefix) break;
+                --t;
+            }
+            st_relaxed(mine, kTilePrefix | (prefix + total));
+        }
+        gbase[d] = bases[d] + prefix;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < kSortItems; ++j) {
+        if (rank[j] == 0xffffffffu) continue;
+        unsigned d = digit_of(k[j], shift);
+        unsigned pos = gbase[d] + wcount[warp][d] + rank[j];
+        if (pos >= static_cast<unsigned>(n)) {  // cannot happen for consistent counts
+            atomicOr(error, kErrLoopBound);
+            continue;
+        }
+        keys_out[pos] = k[j];
+        vals_out[pos] = v[j];
+    }
 }
 
 // Per-tile digit counts, stored digit-major: hist[d * tiles + tile].
@@ -274,7 +452,8 @@ LUX_D int delta(const Key* codes, int i, int j) {
 
 template <typename Key>
 __global__ void __launch_bounds__(kThreads) k_karras(const Key* codes, int n, BvhNode* nodes,
-                                                     int* node_parent, int* leaf_parent) {
+                                                     int* node_parent, int* leaf_parent,
+                                                     int2* node_range) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n - 1) return;
     int first, last;
@@ -318,6 +497,7 @@ __global__ void __launch_bounds__(kThreads) k_karras(const Key* codes, int n, Bv
     int left = first == split ? ~split : split;
     int right = last == split + 1 ? ~(split + 1) : split + 1;
     reinterpret_cast<int2*>(&nodes[i].ch)[0] = make_int2(left, right);
+    node_range[i] = make_int2(first, last);
     if (left < 0) leaf_parent[split] = i << 1;
     else node_parent[split] = i << 1;
     if (right < 0) leaf_parent[split + 1] = (i << 1) | 1;
@@ -350,20 +530,29 @@ LUX_D box3 load_slot_cg(const BvhNode* node, int slot) {
 }
 
 // One thread per sorted leaf.  The leaf box (and, for triangles, the sorted triangle
-// record) is written; then the thread climbs: it stores its box into the parent's
-// slot, and the second of the two children to arrive (atomic counter) unions both
-// slots and continues upward, so every node box is the union of its children's boxes
-// (merge_bounds_kernel, bvh/gpu_bvh.cu:182-214).  The counter is reset by its second
-// arrival, so flags are zero again when the pass ends.
+// record) is written; then the thread climbs: it hands its box to the parent, and the
+// second of the two children to arrive (a counter) unions both and continues upward, so
+// every node box is the union of its children's boxes (merge_bounds_kernel,
+// bvh/gpu_bvh.cu:182-214).  A node whose leaf range lies inside this block's leaves
+// [lo, lo + kThreads) has both its children climbing in this block and an index in that
+// range too (a Karras node is numbered by one end of its range), so the hand-over goes
+// through shared memory; above that through the node's slot in global memory with an
+// acquire-release counter, which the second arrival resets to zero.
 template <int Kind>
 __global__ void __launch_bounds__(kThreads) k_leaf_climb(const float* prims, int n,
                                                          const int* sorted_ids,
                                                          TriRecord* tris, BvhNode* nodes,
                                                          const int* node_parent,
                                                          const int* leaf_parent,
+                                                         const int2* node_range,
                                                          unsigned* flags, float* root,
                                                          int* error) {
-    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    __shared__ float sbox[kThreads][2][6];
+    __shared__ unsigned sflag[kThreads];
+    const int lo = blockIdx.x * kThreads;
+    sflag[threadIdx.x] = 0;
+    __syncthreads();
+    int k = lo + threadIdx.x;
     if (k >= n) return;
     int pid = sorted_ids[k];
     if (pid < 0 || pid >= n) {  // cannot happen for a consistent sort
@@ -392,14 +581,31 @@ __global__ void __launch_bounds__(kThreads) k_leaf_climb(const float* prims, int
         int p = code >> 1;
         int slot = code & 1;
         if (code < 0 || p >= n - 1) break;  // parent links out of range: report below
-        store_slot(nodes + p, slot, b);
-        __threadfence();
-        unsigned prior = atomicAdd(flags + p, 1u);
-        if (prior == 0) return;  // the sibling finishes this node
-        flags[p] = 0;
-        __threadfence();
-        box3 sib = load_slot_cg(nodes + p, slot ^ 1);
-        b = slot ? box_union(sib, b) : box_union(b, sib);
+        const int2 range = node_range[p];
+        const int s = p - lo;
+        if (range.x >= lo && range.y < lo + kThreads && s >= 0 && s < kThreads) {
+            volatile float* mine = &sbox[s][slot][0];
+            mine[0] = b.lo.x; mine[1] = b.lo.y; mine[2] = b.lo.z;
+            mine[3] = b.hi.x; mine[4] = b.hi.y; mine[5] = b.hi.z;
+            __threadfence_block();
+            unsigned prior = atomicAdd(&sflag[s], 1u);
+            if (prior == 0) return;  // the sibling finishes this node
+            __threadfence_block();
+            volatile const float* o = &sbox[s][slot ^ 1][0];
+            box3 sib{make_f3(o[0], o[1], o[2]), make_f3(o[3], o[4], o[5])};
+            const box3 left = slot ? sib : b;
+            const box3 right = slot ? b : sib;
+            store_slot(nodes + p, 0, left);
+            store_slot(nodes + p, 1, right);
+            b = box_union(left, right);
+        } else {
+            store_slot(nodes + p, slot, b);
+            unsigned prior = atomic_add_acq_rel(flags + p, 1u);
+            if (prior == 0) return;  // the sibling finishes this node
+            flags[p] = 0;
+            box3 sib = load_slot_cg(nodes + p, slot ^ 1);
+            b = slot ? box_union(sib, b) : box_union(b, sib);
+        }
         if (p == 0) {
             root[0] = b.lo.x; root[1] = b.lo.y; root[2] = b.lo.z;
             root[3] = b.hi.x; root[4] = b.hi.y; root[5] = b.hi.z;
@@ -445,37 +651,70 @@ int stride_grid(const lux_ctx* ctx, int count) {
     return std::max(1, std::min(grid_for(count), ctx->sm_count * 8));
 }
 
-template <typename Key>
-int radix_sort(lux_ctx* ctx, Key* keys, int* vals, int n, int bits) {
-    int tiles = grid_for(n, kSortTile);
-    size_t key_bytes = (static_cast<size_t>(n) * sizeof(Key) + 255) & ~size_t(255);
-    size_t val_bytes = (static_cast<size_t>(n) * sizeof(int) + 255) & ~size_t(255);
-    size_t hist_bytes = static_cast<size_t>(kRadix) * tiles * sizeof(unsigned);
-    int st = ensure_scratch(ctx, key_bytes + val_bytes + hist_bytes);
+// Device scratch of a build: the sort's alternate keys and values, the digit counts and
+// bases of every pass, the tile counters and the look-back words.
+struct SortScratch {
+    size_t key_bytes, val_bytes, counts_bytes, lookback_bytes;
+    size_t total() const { return key_bytes + val_bytes + counts_bytes + lookback_bytes; }
+};
+
+SortScratch sort_scratch(int n, size_t key_size, int passes) {
+    const size_t tiles = static_cast<size_t>((n + kSortTile - 1) / kSortTile);
+    SortScratch s;
+    s.key_bytes = (static_cast<size_t>(n) * key_size + 255) & ~size_t(255);
+    s.val_bytes = (static_cast<size_t>(n) * sizeof(int) + 255) & ~size_t(255);
+    // hist[kMaxPasses * kRadix], tile counters[kMaxPasses] (padded), bases[...]
+    s.counts_bytes = 2 * sizeof(unsigned) * kMaxPasses * kRadix + 256;
+    s.lookback_bytes = sizeof(unsigned long long) * kRadix * tiles * passes;
+    return s;
+}
+
+// Morton codes of the primitives into `codes` and their stable sort with the input
+// indices into (codes, vals): k_morton_hist, k_digit_bases, then one k_onesweep per
+// 8-bit digit (an even count, so the result lands back in the caller's arrays).
+template <int Kind, typename Key>
+int morton_and_sort(lux_ctx* ctx, const float* prims, const unsigned* root_ord, Key* codes,
+                    int* vals, int n) {
+    constexpr int kPasses = sizeof(Key) == 4 ? 4 : 8;   // 30 bits: 4 digits; 63 bits: 8
+    const int tiles = grid_for(n, kSortTile);
+    const SortScratch layout = sort_scratch(n, sizeof(Key), kPasses);
+    int st = ensure_scratch(ctx, layout.total());
     if (st) return st;
     char* s = static_cast<char*>(ctx->scratch);
     Key* keys_alt = reinterpret_cast<Key*>(s);
-    int* vals_alt = reinterpret_cast<int*>(s + key_bytes);
-    unsigned* hist = reinterpret_cast<unsigned*>(s + key_bytes + val_bytes);
-    int passes = (bits + 7) / 8;
-    // Even pass count: the result lands back in (keys, vals).
-    if (passes & 1) ++passes;
-    Key* kin = keys;
+    int* vals_alt = reinterpret_cast<int*>(s + layout.key_bytes);
+    unsigned* hist = reinterpret_cast<unsigned*>(s + layout.key_bytes + layout.val_bytes);
+    unsigned* bases = hist + kMaxPasses * kRadix;
+    unsigned* counters = bases + kMaxPasses * kRadix;
+    auto* lookback = reinterpret_cast<unsigned long long*>(
+        s + layout.key_bytes + layout.val_bytes + layout.counts_bytes);
+    // Counts, tile counters and look-back words start at zero.
+    cudaError_t err = cudaMemsetAsync(hist, 0, sizeof(unsigned) * kMaxPasses * kRadix,
+                                      ctx->stream);
+    if (err == cudaSuccess)
+        err = cudaMemsetAsync(counters, 0, 256 + layout.lookback_bytes, ctx->stream);
+    if (err != cudaSuccess) return cuda_fail(err, "sort scratch reset");
+    const int hist_grid = std::max(1, std::min(grid_for(n), ctx->sm_count * 2));
+    k_morton_hist<Kind, Key, kPasses><<<hist_grid, kThreads, 0, ctx->stream>>>(
+        prims, n, root_ord, codes, hist);
+    k_digit_bases<<<kPasses, kRadix, 0, ctx->stream>>>(hist, bases);
+    ctx->launches += 2;
+    Key* kin = codes;
     int* vin = vals;
     Key* kout = keys_alt;
     int* vout = vals_alt;
-    for (int p = 0; p < passes; ++p) {
-        int shift = 8 * p;
-        k_sort_upsweep<Key><<<tiles, kThreads, 0, ctx->stream>>>(kin, n, shift, hist, tiles);
-        k_scan_exclusive<<<1, kScanThreads, 0, ctx->stream>>>(hist, kRadix * tiles);
+    for (int p = 0; p < kPasses; ++p) {
+        unsigned long long* words = lookback + static_cast<size_t>(p) * tiles * kRadix;
         if (p == 0) {
-            k_sort_downsweep<Key, true><<<tiles, kThreads, 0, ctx->stream>>>(
-                kin, vin, kout, vout, n, shift, hist, tiles, ctx->d_error);
+            k_onesweep<Key, true><<<tiles, kThreads, 0, ctx->stream>>>(
+                kin, vin, kout, vout, n, 8 * p, bases + p * kRadix, words, counters + p,
+                ctx->d_error);
         } else {
-            k_sort_downsweep<Key, false><<<tiles, kThreads, 0, ctx->stream>>>(
-                kin, vin, kout, vout, n, shift, hist, tiles, ctx->d_error);
+            k_onesweep<Key, false><<<tiles, kThreads, 0, ctx->stream>>>(
+                kin, vin, kout, vout, n, 8 * p, bases + p * kRadix, words, counters + p,
+                ctx->d_error);
         }
-        ctx->launches += 3;
+        ctx->launches += 1;
         std::swap(kin, kout);
         std::swap(vin, vout);
     }
@@ -486,7 +725,7 @@ template <int Kind>
 int climb(lux_ctx* ctx, lux_bvh* bvh, const float* prims) {
     k_leaf_climb<Kind><<<grid_for(bvh->n), kThreads, 0, ctx->stream>>>(
         prims, bvh->n, bvh->sorted_ids, bvh->tris, bvh->nodes, bvh->node_parent,
-        bvh->leaf_parent, bvh->flags, bvh->root, ctx->d_error);
+        bvh->leaf_parent, bvh->node_range, bvh->flags, bvh->root, ctx->d_error);
     ctx->launches += 1;
     return cuda_fail(cudaGetLastError(), "k_leaf_climb");
 }
@@ -499,10 +738,8 @@ int build_typed(lux_ctx* ctx, lux_bvh* bvh, const float* prims) {
     cudaError_t err = cudaMemsetAsync(root_ord, 0xff, 6 * sizeof(unsigned), ctx->stream);
     if (err != cudaSuccess) return cuda_fail(err, "memset root");
     k_root_reduce<Kind><<<stride_grid(ctx, n), kThreads, 0, ctx->stream>>>(prims, n, root_ord);
-    k_morton<Kind, Key><<<stride_grid(ctx, n), kThreads, 0, ctx->stream>>>(prims, n, root_ord,
-                                                                           codes);
-    ctx->launches += 2;
-    int st = radix_sort<Key>(ctx, codes, bvh->sorted_ids, n, sizeof(Key) == 4 ? 30 : 63);
+    ctx->launches += 1;
+    int st = morton_and_sort<Kind, Key>(ctx, prims, root_ord, codes, bvh->sorted_ids, n);
     if (st) return st;
     if (n == 1) {
         // A lone leaf has no parent (the storage may hold a larger earlier tree).
@@ -510,7 +747,7 @@ int build_typed(lux_ctx* ctx, lux_bvh* bvh, const float* prims) {
         if (e != cudaSuccess) return cuda_fail(e, "memset leaf parent");
     } else {
         k_karras<Key><<<grid_for(n - 1), kThreads, 0, ctx->stream>>>(
-            codes, n, bvh->nodes, bvh->node_parent, bvh->leaf_parent);
+            codes, n, bvh->nodes, bvh->node_parent, bvh->leaf_parent, bvh->node_range);
         ctx->launches += 1;
     }
     return climb<Kind>(ctx, bvh, prims);
@@ -519,11 +756,7 @@ int build_typed(lux_ctx* ctx, lux_bvh* bvh, const float* prims) {
 }  // namespace
 
 size_t lbvh_scratch_bytes(int n, int morton_bits) {
-    size_t key = morton_bits == 63 ? 8 : 4;
-    int tiles = (n + kSortTile - 1) / kSortTile;
-    return ((static_cast<size_t>(n) * key + 255) & ~size_t(255))
-         + ((static_cast<size_t>(n) * 4 + 255) & ~size_t(255))
-         + static_cast<size_t>(kRadix) * tiles * 4;
+    return morton_bits == 63 ? sort_scratch(n, 8, 8).total() : sort_scratch(n, 4, 4).total();
 }
 
 int lbvh_alloc(lux_ctx* ctx, lux_bvh* bvh) {
@@ -540,6 +773,7 @@ int lbvh_alloc(lux_ctx* ctx, lux_bvh* bvh) {
         {reinterpret_cast<void**>(&bvh->sorted_ids), sizeof(int) * n},
         {reinterpret_cast<void**>(&bvh->leaf_parent), sizeof(int) * n},
         {reinterpret_cast<void**>(&bvh->node_parent), sizeof(int) * std::max(n - 1, 1)},
+        {reinterpret_cast<void**>(&bvh->node_range), sizeof(int2) * std::max(n - 1, 1)},
         {reinterpret_cast<void**>(&bvh->flags), sizeof(unsigned) * std::max(n - 1, 1)},
         {&bvh->codes, key * n},
         {reinterpret_cast<void**>(&bvh->root), sizeof(float) * 16},
@@ -559,7 +793,7 @@ int lbvh_alloc(lux_ctx* ctx, lux_bvh* bvh) {
 
 void lbvh_free(lux_bvh* bvh) {
     void* ptrs[] = {bvh->nodes, bvh->tris, bvh->sorted_ids, bvh->leaf_parent, bvh->node_parent,
-                    bvh->flags, bvh->codes, bvh->root, bvh->wide};
+                    bvh->node_range, bvh->flags, bvh->codes, bvh->root, bvh->wide};
     bvh->wide = nullptr;
     bvh->wide_capacity = 0;
     bvh->wide_current = false;
@@ -571,6 +805,7 @@ void lbvh_free(lux_bvh* bvh) {
     bvh->sorted_ids = nullptr;
     bvh->leaf_parent = nullptr;
     bvh->node_parent = nullptr;
+    bvh->node_range = nullptr;
     bvh->flags = nullptr;
     bvh->codes = nullptr;
     bvh->root = nullptr;

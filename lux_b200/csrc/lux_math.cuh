@@ -266,3 +266,28 @@ LUX_HD float ordered_to_float(uint32_t o) {
 }
 
 }  // namespace lux
+
+// Validation builds only: with LUX_ROUNDED_DOUBLE_MATH (lux_b200/build.py compiles the
+// sources that way into lux_b200/liblux_gpu_dmath.so, beside the product library) the
+// float sinf, cosf, powf, acosf and atan2f calls are evaluated in double precision and
+// rounded to float, on the device and on the host alike.  A reference build with the same
+// substitution (oracle/rounded_double_math.h) then rounds those calls identically, which
+// isolates the last-bit differences between CUDA's and glibc's float functions as the
+// cause of the path tracer's few per-sample mismatches.  The product library never
+// defines it.
+#ifdef LUX_ROUNDED_DOUBLE_MATH
+__host__ __device__ inline float lux_rd_sinf(float x) { return static_cast<float>(sin(static_cast<double>(x))); }
+__host__ __device__ inline float lux_rd_cosf(float x) { return static_cast<float>(cos(static_cast<double>(x))); }
+__host__ __device__ inline float lux_rd_powf(float x, float y) {
+    return static_cast<float>(pow(static_cast<double>(x), static_cast<double>(y)));
+}
+__host__ __device__ inline float lux_rd_acosf(float x) { return static_cast<float>(acos(static_cast<double>(x))); }
+__host__ __device__ inline float lux_rd_atan2f(float y, float x) {
+    return static_cast<float>(atan2(static_cast<double>(y), static_cast<double>(x)));
+}
+#define sinf lux_rd_sinf
+#define cosf lux_rd_cosf
+#define powf lux_rd_powf
+#define acosf lux_rd_acosf
+#define atan2f lux_rd_atan2f
+#endif

@@ -21,6 +21,7 @@ ORACLE_LIB = os.path.join(HERE, "liblux_oracle.so")
 REF_LIB = os.path.join(HERE, "_ref", "libluxref.so")
 REF_GPU_LIB = os.path.join(HERE, "_ref", "libluxrefgpu.so")
 REF_PT_LIB = os.path.join(HERE, "_ref", "libluxrefpt.so")
+REF_DMATH_LIB = os.path.join(HERE, "_ref", "libluxref_dmath.so")
 PT64_LIB = os.path.join(HERE, "liblux_pt64.so")
 
 _P = ctypes.c_void_p

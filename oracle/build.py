@@ -5,6 +5,8 @@
 3. oracle/_ref/libluxref.so: the reference's own host code.
 4. oracle/_ref/libluxrefgpu.so: the reference's own GPU LBVH (bvh/gpu_bvh.cu,
    bvh/bvh_overlap.cu) behind oracle/ref_gpu_harness.cu, compiled with nvcc for sm_100a.
+7. oracle/_ref/libluxref_dmath.so: item 3 with oracle/rounded_double_math.h
+   force-included (the rounding-isolation test's reference side).
 6. oracle/_ref/libluxshim.so: the drop-in shims (lux_b200/integration/) compiled
    against the reference's headers and called through its own types
    (oracle/ref_shim_harness.cpp), linked to lux_b200/liblux_gpu.so.
@@ -83,6 +85,30 @@ def build_ref(force=False):
     cmd = ["g++", *CXXFLAGS, "-shared", "-I", src_dir, "-I", HERE, "-o", OUT, *inputs]
     subprocess.run(cmd, check=True)
     return OUT
+
+
+REF_DMATH_OUT = os.path.join(OUT_DIR, "libluxref_dmath.so")
+
+
+def build_ref_dmath(force=False):
+    """The reference harness again with oracle/rounded_double_math.h force-included: the
+    reference's float sinf/cosf/powf/acosf/atan2f evaluated in double and rounded, as
+    lux_b200/liblux_gpu_dmath.so evaluates them (the rounding-isolation test's pair)."""
+    src_dir = os.path.join(REF_ROOT, "src")
+    if not os.path.isdir(src_dir):
+        return None
+    harness = os.path.join(HERE, "ref_harness.cpp")
+    header = os.path.join(HERE, "rounded_double_math.h")
+    inputs = [harness] + [os.path.join(REF_ROOT, s) for s in REF_SOURCES]
+    deps = inputs + [header, os.path.join(HERE, "ref_scene_desc.h"),
+                     os.path.join(HERE, "..", "include", "lux_gpu.h")]
+    if not force and not _stale(REF_DMATH_OUT, deps):
+        return REF_DMATH_OUT
+    os.makedirs(OUT_DIR, exist_ok=True)
+    cmd = ["g++", *CXXFLAGS, "-shared", "-include", header, "-I", src_dir, "-I", HERE,
+           "-o", REF_DMATH_OUT, *inputs]
+    subprocess.run(cmd, check=True)
+    return REF_DMATH_OUT
 
 
 REF_GPU_OUT = os.path.join(OUT_DIR, "libluxrefgpu.so")
@@ -229,6 +255,7 @@ def build(force=False):
     build_ref_gpu(force)
     build_ref_pt_gpu(force)
     build_ref_shim(force)
+    build_ref_dmath(force)
     return build_oracle(force), build_ref(force)
 
 

@@ -195,11 +195,12 @@ FLOAT_FIELDS = ("position", "ng", "ns", "wo", "wi", "throughput_before", "throug
                 "bsdf_pdf", "light_pdf")
 
 
-def _same_vertex(a, b, rtol=1e-4):
+def _same_vertex(a, b, rtol=1e-4, pdf_rtol=1e-4):
     if any(int(a[f]) != int(b[f]) for f in INT_FIELDS):
         return False
     return all(np.all(np.abs(np.float64(a[f]) - np.float64(b[f]))
-                      <= rtol * (1 + np.abs(np.float64(b[f])))) for f in FLOAT_FIELDS)
+                      <= (pdf_rtol if f.endswith("_pdf") else rtol) * (1 + np.abs(np.float64(b[f]))))
+               for f in FLOAT_FIELDS)
 
 
 @need_ref_pt
@@ -208,7 +209,12 @@ def test_path_log_matches_reference_gpu_tracer(ctx, ref_pt, which):
     """lux_render_path_log against the records the reference's GPU tracer itself writes
     (RenderOutputs::set_path_log, integrator/render_context.h:65-85): the same paths, and
     on >= 99 % of them (97 % with GGX / glass / filters) every vertex equal (integer
-    fields exactly, floats within 1e-4)."""
+    fields exactly, floats within 1e-4, pdfs within 1e-3).  The pdf bar is wider because
+    the reference's GPU build contracts multiply-adds (nvcc's default) where its host code
+    and this build round each operation: the 0.15-roughness metal's lobe turns those
+    last-bit differences in the half vector into pdf differences of a few parts in 10^4
+    (this build's records equal the reference host walk's to 1e-4,
+    tests/test_path_log.py)."""
     if which == "cornell":
         w = h = 32
         b = S.make_cornell_scene(w, h)
@@ -233,7 +239,8 @@ def test_path_log_matches_reference_gpu_tracer(ctx, ref_pt, which):
     # that graze an edge).
     assert len(set(po) ^ set(pt)) <= 0.005 * len(pt)
     same = sum(k in pt and len(po[k]) == len(pt[k])
-               and all(_same_vertex(a, c) for a, c in zip(po[k], pt[k])) for k in po)
+               and all(_same_vertex(a, c, pdf_rtol=1e-3) for a, c in zip(po[k], pt[k]))
+               for k in po)
     assert same / len(pt) >= bar
     close = np.all(np.abs(film - ref_film) <= 1e-4 * (1 + np.abs(ref_film)), axis=-1)
     assert close.mean() >= 0.5
