@@ -38,6 +38,7 @@ constexpr int kSortTile = kThreads * kSortItems;  // keys per tile
 constexpr int kScanThreads = 1024;
 constexpr int kClimbBound = 160;                 // > max tree depth (64 + 96 bits)
 constexpr int kMaxPasses = 8;                    // 8-bit digits of a 63-bit key
+constexpr int kClimbThreads = 512;               // leaves per climb block
 constexpr long long kLookbackSpins = 1ll << 22;  // bound of one look-back wait
 
 // Relaxed device-scope accesses of the look-back words (each word carries its own value,
@@ -100,12 +101,24 @@ __global__ void __launch_bounds__(kThreads) k_root_reduce(const float* prims, in
             hi[a] = fmaxf(hi[a], __shfl_xor_sync(0xffffffffu, hi[a], off));
         }
     }
-    if ((threadIdx.x & 31) == 0) {
+    // The block's warps meet in shared memory; one atomic per block and value (the
+    // atomics of every warp on six words serialised in L2).
+    __shared__ float part[kThreads / 32][6];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (lane == 0) {
 #pragma unroll
         for (int a = 0; a < 3; ++a) {
-            atomicMin(root_ord + a, float_to_ordered(lo[a]));
-            atomicMin(root_ord + 3 + a, ~float_to_ordered(hi[a]));
+            part[warp][a] = lo[a];
+            part[warp][3 + a] = hi[a];
         }
+    }
+    __syncthreads();
+    if (threadIdx.x < 6) {
+        const int a = threadIdx.x;
+        float v = part[0][a];
+        for (int w = 1; w < kThreads / 32; ++w) v = a < 3 ? fminf(v, part[w][a]) : fmaxf(v, part[w][a]);
+        if (a < 3) atomicMin(root_ord + a, float_to_ordered(v));
+        else atomicMin(root_ord + a, ~float_to_ordered(v));
     }
 }
 
@@ -260,21 +273,39 @@ __global__ void __launch_bounds__(kThreads) k_onesweep(const Key* keys_in, const
             st_relaxed(mine, kTilePrefix | total);
         } else {
             st_relaxed(mine, kTileAggregate | total);
+            // Walk back kLookbackBatch tiles at a time (their words are loaded together,
+            // so a long run of aggregates costs one load latency per batch): take every
+            // published word up to the nearest inclusive prefix, and re-read from the
+            // first word not yet published.
+            constexpr int kLookbackBatch = 8;
             int t = tile - 1;
             long long spins = 0;
-            while (t >= 0) {
-                const unsigned long long w = ld_relaxed(lookback + static_cast<size_t>(t) * kRadix + d);
-                const unsigned long long state = w & ~0xffffffffull;
-                if (state == 0) {
-                    if (++spins > kLookbackSpins) {
-                        atomicOr(error, kErrLoopBound);
-                        break;
+            bool found = false;
+            while (!found && t >= 0) {
+                unsigned long long w[kLookbackBatch];
+#pragma unroll
+                for (int j = 0; j < kLookbackBatch; ++j)
+                    w[j] = t - j >= 0 ? ld_relaxed(lookback + static_cast<size_t>(t - j) * kRadix + d)
+                                      : 0ull;
+                int taken = 0;
+                bool blocked = false;
+#pragma unroll
+                for (int j = 0; j < kLookbackBatch; ++j) {
+                    if (found || blocked || t - j < 0) continue;
+                    const unsigned long long state = w[j] & ~0xffffffffull;
+                    if (state == 0) {         // not published yet: resume at this tile
+                        blocked = true;
+                        continue;
                     }
-                    continue;
+                    prefix += static_cast<unsigned>(w[j]);
+                    taken = j + 1;
+                    found = state == kTilePrefix;
                 }
-                prefix += static_cast<unsigned>(w);
-                if (state == kTilePrefix) break;
-                --t;
+                t -= taken;
+                if (blocked && ++spins > kLookbackSpins) {
+                    atomicOr(error, kErrLoopBound);
+                    break;
+                }
             }
             st_relaxed(mine, kTilePrefix | (prefix + total));
         }
@@ -450,10 +481,12 @@ LUX_D int delta(const Key* codes, int i, int j) {
     }
 }
 
+// node_info[i]: (first leaf, last leaf, parent code, unused) of internal node i; the
+// range is written by node i's thread, the parent code by its parent's.
 template <typename Key>
 __global__ void __launch_bounds__(kThreads) k_karras(const Key* codes, int n, BvhNode* nodes,
                                                      int* node_parent, int* leaf_parent,
-                                                     int2* node_range) {
+                                                     int4* node_info) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n - 1) return;
     int first, last;
@@ -461,6 +494,7 @@ __global__ void __launch_bounds__(kThreads) k_karras(const Key* codes, int n, Bv
         first = 0;
         last = n - 1;
         node_parent[0] = -1;
+        reinterpret_cast<int*>(node_info)[2] = -1;
     } else {
         // determine_range (bvh/gpu_bvh.cu:76-105).
         int dl = delta(codes, i, i - 1);
@@ -497,11 +531,19 @@ __global__ void __launch_bounds__(kThreads) k_karras(const Key* codes, int n, Bv
     int left = first == split ? ~split : split;
     int right = last == split + 1 ? ~(split + 1) : split + 1;
     reinterpret_cast<int2*>(&nodes[i].ch)[0] = make_int2(left, right);
-    node_range[i] = make_int2(first, last);
-    if (left < 0) leaf_parent[split] = i << 1;
-    else node_parent[split] = i << 1;
-    if (right < 0) leaf_parent[split + 1] = (i << 1) | 1;
-    else node_parent[split + 1] = (i << 1) | 1;
+    reinterpret_cast<int2*>(node_info + i)[0] = make_int2(first, last);
+    if (left < 0) {
+        leaf_parent[split] = i << 1;
+    } else {
+        node_parent[split] = i << 1;
+        reinterpret_cast<int*>(node_info + split)[2] = i << 1;
+    }
+    if (right < 0) {
+        leaf_parent[split + 1] = (i << 1) | 1;
+    } else {
+        node_parent[split + 1] = (i << 1) | 1;
+        reinterpret_cast<int*>(node_info + split + 1)[2] = (i << 1) | 1;
+    }
 }
 
 // ---------------------------------------------------------------- 5. boxes bottom-up
@@ -534,22 +576,22 @@ LUX_D box3 load_slot_cg(const BvhNode* node, int slot) {
 // second of the two children to arrive (a counter) unions both and continues upward, so
 // every node box is the union of its children's boxes (merge_bounds_kernel,
 // bvh/gpu_bvh.cu:182-214).  A node whose leaf range lies inside this block's leaves
-// [lo, lo + kThreads) has both its children climbing in this block and an index in that
-// range too (a Karras node is numbered by one end of its range), so the hand-over goes
-// through shared memory; above that through the node's slot in global memory with an
-// acquire-release counter, which the second arrival resets to zero.
+// [lo, lo + kClimbThreads) has both its children climbing in this block and an index in
+// that range too (a Karras node is numbered by one end of its range), so the hand-over
+// goes through shared memory; above that through the node's slot in global memory with
+// an acquire-release counter, which the second arrival resets to zero.  One 16-byte load
+// of node_info per level gives the node's range and its parent link.
 template <int Kind>
-__global__ void __launch_bounds__(kThreads) k_leaf_climb(const float* prims, int n,
-                                                         const int* sorted_ids,
-                                                         TriRecord* tris, BvhNode* nodes,
-                                                         const int* node_parent,
-                                                         const int* leaf_parent,
-                                                         const int2* node_range,
-                                                         unsigned* flags, float* root,
-                                                         int* error) {
-    __shared__ float sbox[kThreads][2][6];
-    __shared__ unsigned sflag[kThreads];
-    const int lo = blockIdx.x * kThreads;
+__global__ void __launch_bounds__(kClimbThreads) k_leaf_climb(const float* prims, int n,
+                                                              const int* sorted_ids,
+                                                              TriRecord* tris, BvhNode* nodes,
+                                                              const int* leaf_parent,
+                                                              const int4* node_info,
+                                                              unsigned* flags, float* root,
+                                                              int* error) {
+    __shared__ float sbox[kClimbThreads][2][6];
+    __shared__ unsigned sflag[kClimbThreads];
+    const int lo = blockIdx.x * kClimbThreads;
     sflag[threadIdx.x] = 0;
     __syncthreads();
     int k = lo + threadIdx.x;
@@ -581,9 +623,9 @@ __global__ void __launch_bounds__(kThreads) k_leaf_climb(const float* prims, int
         int p = code >> 1;
         int slot = code & 1;
         if (code < 0 || p >= n - 1) break;  // parent links out of range: report below
-        const int2 range = node_range[p];
+        const int4 info = node_info[p];
         const int s = p - lo;
-        if (range.x >= lo && range.y < lo + kThreads && s >= 0 && s < kThreads) {
+        if (info.x >= lo && info.y < lo + kClimbThreads && s >= 0 && s < kClimbThreads) {
             volatile float* mine = &sbox[s][slot][0];
             mine[0] = b.lo.x; mine[1] = b.lo.y; mine[2] = b.lo.z;
             mine[3] = b.hi.x; mine[4] = b.hi.y; mine[5] = b.hi.z;
@@ -611,7 +653,7 @@ __global__ void __launch_bounds__(kThreads) k_leaf_climb(const float* prims, int
             root[3] = b.hi.x; root[4] = b.hi.y; root[5] = b.hi.z;
             return;
         }
-        code = node_parent[p];
+        code = info.z;
     }
     atomicOr(error, kErrClimbBound);
 }
@@ -723,9 +765,9 @@ int morton_and_sort(lux_ctx* ctx, const float* prims, const unsigned* root_ord, 
 
 template <int Kind>
 int climb(lux_ctx* ctx, lux_bvh* bvh, const float* prims) {
-    k_leaf_climb<Kind><<<grid_for(bvh->n), kThreads, 0, ctx->stream>>>(
-        prims, bvh->n, bvh->sorted_ids, bvh->tris, bvh->nodes, bvh->node_parent,
-        bvh->leaf_parent, bvh->node_range, bvh->flags, bvh->root, ctx->d_error);
+    k_leaf_climb<Kind><<<grid_for(bvh->n, kClimbThreads), kClimbThreads, 0, ctx->stream>>>(
+        prims, bvh->n, bvh->sorted_ids, bvh->tris, bvh->nodes, bvh->leaf_parent,
+        bvh->node_info, bvh->flags, bvh->root, ctx->d_error);
     ctx->launches += 1;
     return cuda_fail(cudaGetLastError(), "k_leaf_climb");
 }
@@ -747,7 +789,7 @@ int build_typed(lux_ctx* ctx, lux_bvh* bvh, const float* prims) {
         if (e != cudaSuccess) return cuda_fail(e, "memset leaf parent");
     } else {
         k_karras<Key><<<grid_for(n - 1), kThreads, 0, ctx->stream>>>(
-            codes, n, bvh->nodes, bvh->node_parent, bvh->leaf_parent, bvh->node_range);
+            codes, n, bvh->nodes, bvh->node_parent, bvh->leaf_parent, bvh->node_info);
         ctx->launches += 1;
     }
     return climb<Kind>(ctx, bvh, prims);
@@ -773,7 +815,7 @@ int lbvh_alloc(lux_ctx* ctx, lux_bvh* bvh) {
         {reinterpret_cast<void**>(&bvh->sorted_ids), sizeof(int) * n},
         {reinterpret_cast<void**>(&bvh->leaf_parent), sizeof(int) * n},
         {reinterpret_cast<void**>(&bvh->node_parent), sizeof(int) * std::max(n - 1, 1)},
-        {reinterpret_cast<void**>(&bvh->node_range), sizeof(int2) * std::max(n - 1, 1)},
+        {reinterpret_cast<void**>(&bvh->node_info), sizeof(int4) * std::max(n - 1, 1)},
         {reinterpret_cast<void**>(&bvh->flags), sizeof(unsigned) * std::max(n - 1, 1)},
         {&bvh->codes, key * n},
         {reinterpret_cast<void**>(&bvh->root), sizeof(float) * 16},
@@ -793,7 +835,7 @@ int lbvh_alloc(lux_ctx* ctx, lux_bvh* bvh) {
 
 void lbvh_free(lux_bvh* bvh) {
     void* ptrs[] = {bvh->nodes, bvh->tris, bvh->sorted_ids, bvh->leaf_parent, bvh->node_parent,
-                    bvh->node_range, bvh->flags, bvh->codes, bvh->root, bvh->wide};
+                    bvh->node_info, bvh->flags, bvh->codes, bvh->root, bvh->wide};
     bvh->wide = nullptr;
     bvh->wide_capacity = 0;
     bvh->wide_current = false;
@@ -805,7 +847,7 @@ void lbvh_free(lux_bvh* bvh) {
     bvh->sorted_ids = nullptr;
     bvh->leaf_parent = nullptr;
     bvh->node_parent = nullptr;
-    bvh->node_range = nullptr;
+    bvh->node_info = nullptr;
     bvh->flags = nullptr;
     bvh->codes = nullptr;
     bvh->root = nullptr;

@@ -48,7 +48,7 @@ struct lux_bvh {
     int* sorted_ids = nullptr;          // n
     int* leaf_parent = nullptr;         // n
     int* node_parent = nullptr;         // n - 1
-    int2* node_range = nullptr;         // n - 1: first and last sorted leaf of each node
+    int4* node_info = nullptr;          // n - 1: first and last sorted leaf, parent code
     unsigned* flags = nullptr;          // n - 1, zero between passes
     void* codes = nullptr;              // n sorted codes (uint32 or uint64)
     float* root = nullptr;              // 6
