@@ -243,12 +243,19 @@ __global__ void __launch_bounds__(kThreads) k_onesweep(const Key* keys_in, const
     Key k[kSortItems];
     int v[kSortItems];
     unsigned rank[kSortItems];
+    // All of the warp's keys and values are loaded before the ranking starts, so their
+    // loads are in flight together rather than one per ranking round.
 #pragma unroll
     for (int j = 0; j < kSortItems; ++j) {
         int idx = base + j * 32 + lane;
         bool valid = idx < n;
         k[j] = valid ? keys_in[idx] : Key(0);
         v[j] = First ? idx : (valid ? vals_in[idx] : 0);
+    }
+#pragma unroll
+    for (int j = 0; j < kSortItems; ++j) {
+        int idx = base + j * 32 + lane;
+        bool valid = idx < n;
         unsigned d = valid ? digit_of(k[j], shift) : kRadix;
         unsigned peers = __match_any_sync(0xffffffffu, d);
         unsigned before = valid ? wcount[warp][d] : 0u;

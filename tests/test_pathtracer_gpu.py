@@ -82,8 +82,10 @@ def test_cornell_config1_shape_matches_reference_live(ctx):
     assert counts[0] >= w * h * spp and counts[1] > 0
 
 
-def material_zoo(width=48, height=48):
-    """Every BSDF and light kind the wavefront path supports, in one closed room."""
+def material_zoo(width=48, height=48, glass_y0=0.0):
+    """Every BSDF and light kind the wavefront path supports, in one closed room.  The
+    glass box stands on the floor: its bottom face lies in the floor's plane (glass_y0
+    lifts it)."""
     b = S.SceneBuilder()
     f = np.float32
     white = b.add_material(S.lambert((f(0.75), f(0.75), f(0.72))))
@@ -103,7 +105,7 @@ def material_zoo(width=48, height=48):
     b.add_quad((1, 0, -1), (1, 0, 2), (1, 2, 2), (1, 2, -1), metal)          # right (metal)
     b.add_quad((-0.8, 0.1, 0.2), (-0.2, 0.1, 0.2), (-0.2, 0.8, 0.2), (-0.8, 0.8, 0.2), thin)
     # glass box
-    x0, y0, z0, x1, y1, z1 = 0.2, 0.0, 0.3, 0.7, 0.6, 0.8
+    x0, y0, z0, x1, y1, z1 = 0.2, glass_y0, 0.3, 0.7, 0.6, 0.8
     p = [(x0, y0, z0), (x0, y0, z1), (x0, y1, z0), (x0, y1, z1),
          (x1, y0, z0), (x1, y0, z1), (x1, y1, z0), (x1, y1, z1)]
     for q in [(0, 4, 6, 2), (5, 1, 3, 7), (1, 0, 2, 3), (4, 5, 7, 6), (2, 6, 7, 3), (1, 5, 4, 0)]:
