@@ -206,48 +206,54 @@ __global__ void __launch_bounds__(kRadix) k_digit_bases(const unsigned* hist, un
     bases[blockIdx.x * kRadix + threadIdx.x] = before + incl - v;
 }
 
+// Lanes of the warp whose digit (and validity) equal this lane's: a validity ballot and
+// one ballot per digit bit, ANDed (cheaper than a general match on sm_100a).
+LUX_D unsigned digit_peers(unsigned d, bool valid) {
+    unsigned peers = __ballot_sync(0xffffffffu, valid);
+    if (!valid) peers = ~peers;
+#pragma unroll
+    for (int b = 0; b < 8; ++b) {
+        const bool bit = (d >> b) & 1u;
+        const unsigned m = __ballot_sync(0xffffffffu, bit);
+        peers &= bit ? m : ~m;
+    }
+    return peers;
+}
+
 // Look-back words: value in the low 32 bits, state in the high ones (0: not yet
 // published; aggregate: this tile's own count; prefix: the count over tiles 0..t).
 constexpr unsigned long long kTileAggregate = 1ull << 32;
 constexpr unsigned long long kTilePrefix = 2ull << 32;
 
-// One stable LSD pass over all keys.  Tiles of kOneTile keys (512 threads x 16) are
-// taken in launch order (an atomic counter), ranked inside the tile as k_sort_downsweep
-// ranks them (per-warp digit counts in input order, so equal digits keep input order),
-// and placed at bases[d] + (digit d's count in earlier tiles) + the rank in the tile.
-// The count in earlier tiles comes from a decoupled look-back: each tile publishes its
-// per-digit count, then walks back over the earlier tiles' words until one holds an
-// inclusive prefix, and publishes its own inclusive prefix.  Two lanes share a digit's
-// walk: each loads 8 earlier tiles' words at once and the pair consumes the 16 in order,
-// so a run of aggregates costs one load latency per 16 tiles (when every tile of one wave
-// starts together, no inclusive prefix exists yet and a tile reads back to tile 0).  A
-// tile waits only on tiles handed out before it (running or done); each wait is bounded
-// and a wait that runs out reports through `error`.
-constexpr int kOneThreads = 512;
-constexpr int kOneTile = kOneThreads * kSortItems;
-constexpr int kLookbackLane = 8;   // earlier tiles one lane loads per round
-
+// One stable LSD pass over all keys.  Tiles of kSortTile keys are taken in launch order
+// (an atomic counter), ranked inside the tile as k_sort_downsweep ranks them (per-warp
+// digit counts in input order, so equal digits keep input order), and placed at
+// bases[d] + (digit d's count in earlier tiles) + the rank in the tile.  The count in
+// earlier tiles comes from a decoupled look-back: each tile publishes its per-digit
+// count, then walks back over the earlier tiles' words until one holds an inclusive
+// prefix, and publishes its own inclusive prefix.  A tile waits only on tiles that were
+// handed out before it (and so are running or done); each wait is bounded and a wait
+// that runs out reports through `error`.
 template <typename Key, bool First>
-__global__ void __launch_bounds__(kOneThreads) k_onesweep(const Key* keys_in, const int* vals_in,
-                                                          Key* keys_out, int* vals_out, int n,
-                                                          int shift, const unsigned* bases,
-                                                          unsigned long long* lookback,
-                                                          unsigned* tile_counter, int* error) {
-    constexpr int kWarps = kOneThreads / 32;
-    constexpr int kWarpSpan = kOneTile / kWarps;
-    static_assert(kOneThreads == 2 * kRadix, "two look-back lanes per digit");
+__global__ void __launch_bounds__(kThreads) k_onesweep(const Key* keys_in, const int* vals_in,
+                                                       Key* keys_out, int* vals_out, int n,
+                                                       int shift, const unsigned* bases,
+                                                       unsigned long long* lookback,
+                                                       unsigned* tile_counter, int* error) {
+    constexpr int kWarps = kThreads / 32;
+    constexpr int kWarpSpan = kSortTile / kWarps;
     __shared__ unsigned wcount[kWarps][kRadix];
     __shared__ unsigned gbase[kRadix];
     __shared__ int tile_s;
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
     if (threadIdx.x == 0) tile_s = static_cast<int>(atomicAdd(tile_counter, 1u));
-    for (int i = threadIdx.x; i < kWarps * kRadix; i += kOneThreads) (&wcount[0][0])[i] = 0;
+    for (int i = threadIdx.x; i < kWarps * kRadix; i += kThreads) (&wcount[0][0])[i] = 0;
     __syncthreads();
     const int tile = tile_s;
 
     const unsigned lt = lanemask_lt();
-    const int base = tile * kOneTile + warp * kWarpSpan;
+    const int base = tile * kSortTile + warp * kWarpSpan;
     Key k[kSortItems];
     int v[kSortItems];
     unsigned rank[kSortItems];
@@ -264,8 +270,8 @@ __global__ void __launch_bounds__(kOneThreads) k_onesweep(const Key* keys_in, co
     for (int j = 0; j < kSortItems; ++j) {
         int idx = base + j * 32 + lane;
         bool valid = idx < n;
-        unsigned d = valid ? digit_of(k[j], shift) : kRadix;
-        unsigned peers = __match_any_sync(0xffffffffu, d);
+        unsigned d = valid ? digit_of(k[j], shift) : 0u;
+        unsigned peers = digit_peers(d, valid);
         unsigned before = valid ? wcount[warp][d] : 0u;
         __syncwarp();
         if (valid && lane == __ffs(peers) - 1) wcount[warp][d] = before + __popc(peers);
@@ -274,69 +280,57 @@ __global__ void __launch_bounds__(kOneThreads) k_onesweep(const Key* keys_in, co
     }
     __syncthreads();
     {
-        // Lanes 2d and 2d+1 (one warp) own digit d; the even lane does the serial parts.
-        const int d = threadIdx.x >> 1;
-        const bool lead = (threadIdx.x & 1) == 0;
-        const unsigned pair = 3u << (lane & ~1);
+        const int d = threadIdx.x;
         unsigned total = 0;
-        if (lead) {
 #pragma unroll
-            for (int w = 0; w < kWarps; ++w) {
-                unsigned c = wcount[w][d];
-                wcount[w][d] = total;
-                total += c;
-            }
+        for (int w = 0; w < kWarps; ++w) {
+            unsigned c = wcount[w][d];
+            wcount[w][d] = total;
+            total += c;
         }
-        total = __shfl_sync(pair, total, lane & ~1);
         unsigned long long* mine = lookback + static_cast<size_t>(tile) * kRadix + d;
         unsigned prefix = 0;
         if (tile == 0) {
-            if (lead) st_relaxed(mine, kTilePrefix | total);
+            st_relaxed(mine, kTilePrefix | total);
         } else {
-            if (lead) st_relaxed(mine, kTileAggregate | total);
+            st_relaxed(mine, kTileAggregate | total);
+            // Walk back kLookbackBatch tiles at a time (their words are loaded together,
+            // so a long run of aggregates costs one load latency per batch): take every
+            // published word up to the nearest inclusive prefix, and re-read from the
+            // first word not yet published.
+            constexpr int kLookbackBatch = 8;
             int t = tile - 1;
             long long spins = 0;
             bool found = false;
             while (!found && t >= 0) {
-                // This lane's 8 tiles of the 16-tile window starting at t.
-                const int t0 = t - (lead ? 0 : kLookbackLane);
-                unsigned long long w[kLookbackLane];
+                unsigned long long w[kLookbackBatch];
 #pragma unroll
-                for (int j = 0; j < kLookbackLane; ++j)
-                    w[j] = t0 - j >= 0 ? ld_relaxed(lookback + static_cast<size_t>(t0 - j) * kRadix + d)
-                                       : 0ull;
+                for (int j = 0; j < kLookbackBatch; ++j)
+                    w[j] = t - j >= 0 ? ld_relaxed(lookback + static_cast<size_t>(t - j) * kRadix + d)
+                                      : 0ull;
                 int taken = 0;
                 bool blocked = false;
-                // The lead lane consumes its own 8 words, then its partner's, in order.
 #pragma unroll
-                for (int half = 0; half < 2; ++half) {
-#pragma unroll
-                    for (int j = 0; j < kLookbackLane; ++j) {
-                        const unsigned long long word = __shfl_sync(pair, w[j], (lane & ~1) + half);
-                        const int tt = t - half * kLookbackLane - j;
-                        if (!lead || found || blocked || tt < 0) continue;
-                        const unsigned long long state = word & ~0xffffffffull;
-                        if (state == 0) {         // not published yet: resume at this tile
-                            blocked = true;
-                            continue;
-                        }
-                        prefix += static_cast<unsigned>(word);
-                        taken = half * kLookbackLane + j + 1;
-                        found = state == kTilePrefix;
+                for (int j = 0; j < kLookbackBatch; ++j) {
+                    if (found || blocked || t - j < 0) continue;
+                    const unsigned long long state = w[j] & ~0xffffffffull;
+                    if (state == 0) {         // not published yet: resume at this tile
+                        blocked = true;
+                        continue;
                     }
+                    prefix += static_cast<unsigned>(w[j]);
+                    taken = j + 1;
+                    found = state == kTilePrefix;
                 }
-                taken = __shfl_sync(pair, taken, lane & ~1);
-                found = __shfl_sync(pair, found ? 1 : 0, lane & ~1) != 0;
-                blocked = __shfl_sync(pair, blocked ? 1 : 0, lane & ~1) != 0;
                 t -= taken;
                 if (blocked && ++spins > kLookbackSpins) {
-                    if (lead) atomicOr(error, kErrLoopBound);
+                    atomicOr(error, kErrLoopBound);
                     break;
                 }
             }
-            if (lead) st_relaxed(mine, kTilePrefix | (prefix + total));
+            st_relaxed(mine, kTilePrefix | (prefix + total));
         }
-        if (lead) gbase[d] = bases[d] + prefix;
+        gbase[d] = bases[d] + prefix;
     }
     __syncthreads();
 #pragma unroll
@@ -632,12 +626,10 @@ __global__ void __launch_bounds__(kClimbThreads) k_leaf_climb(const float* prims
     box3 b;
     load_prim<Kind>(prims, pid, v0, v1, v2, b);
     if (Kind == LUX_PRIM_TRIANGLES) {
-        f3 e1 = v1 - v0;
-        f3 e2 = v2 - v0;
         TriRecord r;
         r.p0 = make_float4(v0.x, v0.y, v0.z, __int_as_float(pid));
-        r.p1 = make_float4(e1.x, e1.y, e1.z, 0.0f);
-        r.p2 = make_float4(e2.x, e2.y, e2.z, 0.0f);
+        r.p1 = make_float4(v1.x, v1.y, v1.z, 0.0f);
+        r.p2 = make_float4(v2.x, v2.y, v2.z, 0.0f);
         tris[k] = r;
     }
     if (n == 1) {
@@ -728,7 +720,7 @@ struct SortScratch {
 };
 
 SortScratch sort_scratch(int n, size_t key_size, int passes) {
-    const size_t tiles = static_cast<size_t>((n + kOneTile - 1) / kOneTile);
+    const size_t tiles = static_cast<size_t>((n + kSortTile - 1) / kSortTile);
     SortScratch s;
     s.key_bytes = (static_cast<size_t>(n) * key_size + 255) & ~size_t(255);
     s.val_bytes = (static_cast<size_t>(n) * sizeof(int) + 255) & ~size_t(255);
@@ -745,7 +737,7 @@ template <int Kind, typename Key>
 int morton_and_sort(lux_ctx* ctx, const float* prims, const unsigned* root_ord, Key* codes,
                     int* vals, int n) {
     constexpr int kPasses = sizeof(Key) == 4 ? 4 : 8;   // 30 bits: 4 digits; 63 bits: 8
-    const int tiles = grid_for(n, kOneTile);
+    const int tiles = grid_for(n, kSortTile);
     const SortScratch layout = sort_scratch(n, sizeof(Key), kPasses);
     int st = ensure_scratch(ctx, layout.total());
     if (st) return st;
@@ -775,11 +767,11 @@ int morton_and_sort(lux_ctx* ctx, const float* prims, const unsigned* root_ord, 
     for (int p = 0; p < kPasses; ++p) {
         unsigned long long* words = lookback + static_cast<size_t>(p) * tiles * kRadix;
         if (p == 0) {
-            k_onesweep<Key, true><<<tiles, kOneThreads, 0, ctx->stream>>>(
+            k_onesweep<Key, true><<<tiles, kThreads, 0, ctx->stream>>>(
                 kin, vin, kout, vout, n, 8 * p, bases + p * kRadix, words, counters + p,
                 ctx->d_error);
         } else {
-            k_onesweep<Key, false><<<tiles, kOneThreads, 0, ctx->stream>>>(
+            k_onesweep<Key, false><<<tiles, kThreads, 0, ctx->stream>>>(
                 kin, vin, kout, vout, n, 8 * p, bases + p * kRadix, words, counters + p,
                 ctx->d_error);
         }
@@ -907,12 +899,10 @@ __global__ void k_attach(const float* tris, int n, const int* sorted_ids, TriRec
     f3 v0, v1, v2;
     box3 b;
     load_prim<LUX_PRIM_TRIANGLES>(tris, pid, v0, v1, v2, b);
-    f3 e1 = v1 - v0;
-    f3 e2 = v2 - v0;
     TriRecord r;
     r.p0 = make_float4(v0.x, v0.y, v0.z, __int_as_float(pid));
-    r.p1 = make_float4(e1.x, e1.y, e1.z, 0.0f);
-    r.p2 = make_float4(e2.x, e2.y, e2.z, 0.0f);
+    r.p1 = make_float4(v1.x, v1.y, v1.z, 0.0f);
+    r.p2 = make_float4(v2.x, v2.y, v2.z, 0.0f);
     out[k] = r;
 }
 

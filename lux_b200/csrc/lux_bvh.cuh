@@ -22,12 +22,14 @@ struct alignas(16) BvhNode {
 };
 static_assert(sizeof(BvhNode) == 64, "one node is one 64-byte record");
 
-// Triangle in Morton order: v0, e1 = v1 - v0, e2 = v2 - v0 (the rounded edges the
-// reference's Moller-Trumbore forms), primitive id in p0.w.
+// Triangle in Morton order: its three vertices, primitive id in p0.w.  The walks form
+// the edges v1 - v0 and v2 - v0 when they test it (the reference's Moller-Trumbore
+// rounds the same two differences), and a triangle BVH's leaf box is the triangle's box
+// (triangle_box of these vertices), so a leaf's exact box comes from the record itself.
 struct alignas(16) TriRecord {
     float4 p0;  // v0.xyz, primitive id (int bits)
-    float4 p1;  // e1.xyz, 0
-    float4 p2;  // e2.xyz, 0
+    float4 p1;  // v1.xyz, 0
+    float4 p2;  // v2.xyz, 0
 };
 
 LUX_HD box3 node_left_box(const BvhNode& n) {
@@ -72,6 +74,9 @@ struct BvhView {
     const int* leaf_parent = nullptr;   // n: (parent << 1) | slot, -1 for a lone leaf
     const float* root = nullptr;        // 6 floats: union of all boxes
     int n = 0;
+    // Leaf boxes are the triangles' own boxes (BVHs built from triangles); false for box
+    // BVHs with attached triangles, whose leaf boxes are the caller's boxes.
+    bool leaf_is_triangle_box = false;
 };
 
 LUX_D box3 load_root(const float* root) {
@@ -89,11 +94,19 @@ LUX_D BvhNode load_node(const BvhNode* nodes, int i) {
 }
 
 // Box of sorted leaf k: the slot its parent stores (for a one-primitive tree, the root).
+// Only the slot's 24 bytes are read.
 LUX_D box3 leaf_box(const BvhView& v, int k) {
     int code = v.leaf_parent[k];
     if (code < 0 || (code >> 1) >= v.n - 1) return load_root(v.root);
-    BvhNode p = load_node(v.nodes, code >> 1);
-    return (code & 1) ? node_right_box(p) : node_left_box(p);
+    const float* f = reinterpret_cast<const float*>(v.nodes + (code >> 1));
+    if (code & 1) {
+        const float2 a = __ldg(reinterpret_cast<const float2*>(f + 6));
+        const float4 b = __ldg(reinterpret_cast<const float4*>(f + 8));
+        return box3{make_f3(a.x, a.y, b.x), make_f3(b.y, b.z, b.w)};
+    }
+    const float4 a = __ldg(reinterpret_cast<const float4*>(f));
+    const float2 b = __ldg(reinterpret_cast<const float2*>(f + 4));
+    return box3{make_f3(a.x, a.y, a.z), make_f3(a.w, b.x, b.y)};
 }
 
 // Device error word bits (ctx-owned, read back by the host at synchronisation points).

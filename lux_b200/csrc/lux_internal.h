@@ -64,6 +64,7 @@ struct lux_bvh {
         v.leaf_parent = leaf_parent;
         v.root = root;
         v.n = n;
+        v.leaf_is_triangle_box = kind == LUX_PRIM_TRIANGLES;
         return v;
     }
 };

@@ -172,11 +172,13 @@ LUX_HD bool octant_hit(const octant_ray& r, const box3& b, float tmax, float& tn
     return !(tn > tf);
 }
 
-// Moller-Trumbore (geometry/triangle.h:33-52) on the stored form (v0, e1 = v1 - v0,
-// e2 = v2 - v0): the edges are the same rounded differences the reference forms.
+// Moller-Trumbore (geometry/triangle.h:33-52) on the triangle's vertices: the edges
+// e1 = v1 - v0 and e2 = v2 - v0 are the same rounded differences the reference forms.
 // Returns the raw t; the caller applies t_min < t < t_max.
-LUX_HD bool moller_trumbore(const f3& o, const f3& d, f3 v0, f3 e1, f3 e2, float& t,
+LUX_HD bool moller_trumbore(const f3& o, const f3& d, f3 v0, f3 v1, f3 v2, float& t,
                             float& u, float& v) {
+    const f3 e1 = v1 - v0;
+    const f3 e2 = v2 - v0;
     f3 h = cross(d, e2);
     float a = dot(e1, h);
     if (fabsf(a) < 1e-7f) return false;

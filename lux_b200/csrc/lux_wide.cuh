@@ -81,9 +81,27 @@ LUX_D bool leaf_hit(const BvhView& b, int k, const slab_ray& sr, const octant_ra
     return child_hit(leaf_box(b, k), sr, orr, best_t, tn);
 }
 
-// Walks bvh from its root for a ray with slab constants sr; leaf(k, best_t) tests sorted
-// leaf k, may lower best_t, and returns true to end the walk (any-hit).  Returns false
-// after setting an error bit (loop bound or stack overflow).
+// Sorted leaf k's triangle record (p0, p1, p2) and the verdict on the leaf's exact box.
+// In a BVH built from triangles the leaf box is the triangle's own box, formed here from
+// the record's vertices exactly as the build formed it, so the leaf costs one 48-byte
+// record load and no parent-slot load.
+LUX_D bool leaf_record_hit(const BvhView& b, int k, const slab_ray& sr, const octant_ray& orr,
+                           float best_t, float4& p0, float4& p1, float4& p2) {
+    const float4* tp = reinterpret_cast<const float4*>(b.tris + k);
+    p0 = __ldg(tp);
+    p1 = __ldg(tp + 1);
+    p2 = __ldg(tp + 2);
+    if (!b.leaf_is_triangle_box) return leaf_hit(b, k, sr, orr, best_t);
+    float tn;
+    return child_hit(triangle_box(make_f3(p0.x, p0.y, p0.z), make_f3(p1.x, p1.y, p1.z),
+                                  make_f3(p2.x, p2.y, p2.z)),
+                     sr, orr, best_t, tn);
+}
+
+// Walks bvh from its root for a ray with slab constants sr; leaf(k, p0, p1, p2, best_t)
+// tests sorted leaf k (its triangle record p0..p2), may lower best_t, and returns true to
+// end the walk (any-hit).  Returns false after setting an error bit (loop bound or stack
+// overflow).
 template <typename Leaf>
 LUX_D bool wide_walk(const BvhView& b, const slab_ray& sr, float& best_t, int* error,
                      Leaf&& leaf) {
@@ -121,8 +139,11 @@ LUX_D bool wide_walk(const BvhView& b, const slab_ray& sr, float& best_t, int* e
                 cur = wide_ref(w, f);
                 descend = true;
             }
-        } else if (leaf_hit(b, ~cur, sr, orr, best_t) && leaf(~cur, best_t)) {
-            return true;
+        } else {
+            float4 p0, p1, p2;
+            if (leaf_record_hit(b, ~cur, sr, orr, best_t, p0, p1, p2) &&
+                leaf(~cur, p0, p1, p2, best_t))
+                return true;
         }
         if (!descend) {
             bool resumed = false;

@@ -144,11 +144,9 @@ __global__ void __launch_bounds__(kTraceThreads) k_trace_wide(BvhView bvh, const
     const slab_ray sr = make_slab_ray(ray);
     float best_t = ray.tmax;
     int best_k = -1;
-    bool ok = wide_walk(bvh, sr, best_t, error, [&](int k, float& bt) -> bool {
-        const float4* tp = reinterpret_cast<const float4*>(bvh.tris + k);
-        float4 p0 = __ldg(tp);
-        float4 p1 = __ldg(tp + 1);
-        float4 p2 = __ldg(tp + 2);
+    bool ok = wide_walk(bvh, sr, best_t, error,
+                        [&](int k, const float4& p0, const float4& p1, const float4& p2,
+                            float& bt) -> bool {
         float t, u, v;
         if (moller_trumbore(ray.o, ray.d, make_f3(p0.x, p0.y, p0.z), make_f3(p1.x, p1.y, p1.z),
                             make_f3(p2.x, p2.y, p2.z), t, u, v)
@@ -411,12 +409,9 @@ __global__ void __launch_bounds__(kTraceThreads, 10) k_trace_wide_persistent(
                         cur = wide_ref(w, f);
                         pop = false;
                     }
-                } else if (leaf_hit(bvh, ~cur, sr, orr, best_t)) {
+                } else if (float4 p0, p1, p2;
+                           leaf_record_hit(bvh, ~cur, sr, orr, best_t, p0, p1, p2)) {
                     int k = ~cur;
-                    const float4* tp = reinterpret_cast<const float4*>(bvh.tris + k);
-                    float4 p0 = __ldg(tp);
-                    float4 p1 = __ldg(tp + 1);
-                    float4 p2 = __ldg(tp + 2);
                     float t, u, v;
                     if (moller_trumbore(ray.o, ray.d, make_f3(p0.x, p0.y, p0.z),
                                         make_f3(p1.x, p1.y, p1.z), make_f3(p2.x, p2.y, p2.z),
