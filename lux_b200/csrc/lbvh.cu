@@ -592,31 +592,23 @@ LUX_D box3 load_slot_cg(const BvhNode* node, int slot) {
     return box3{make_f3(a.x, a.y, b.x), make_f3(b.y, b.z, b.w)};
 }
 
-// Bottom-up boxes in two phases.  Every node box is the union of its children's boxes
-// (merge_bounds_kernel, bvh/gpu_bvh.cu:182-214): a climbing thread hands its box to the
-// parent and the second of the two children to arrive unions both and climbs on.
-//
-// Phase 1, k_leaf_climb: one thread per sorted leaf writes the leaf box (and, for
-// triangles, the sorted triangle record) and climbs while the parent's leaf range lies
-// inside the block's own leaves [lo, lo + kClimbThreads): such a node has both children
-// climbing in this block and an index in that range (a Karras node is numbered by one
-// end of its range), so the hand-over goes through shared memory.  At the first parent
-// whose range leaves the block, the thread stores its box in the parent's slot and
-// appends the parent code to the escape list.
-// Phase 2, k_upper_climb: one block takes the escape list and climbs the nodes above
-// (every ancestor of a node that leaves a block leaves it too).  All of it runs in one
-// block, so a block-scope fence orders each slot store before its counter increment;
-// the second arrival resets the counter to zero.
-// One 16-byte load of node_info per level gives a node's range and its parent link.
-constexpr int kUpperThreads = 1024;
-
+// One thread per sorted leaf.  The leaf box (and, for triangles, the sorted triangle
+// record) is written; then the thread climbs: it hands its box to the parent, and the
+// second of the two children to arrive (a counter) unions both and continues upward, so
+// every node box is the union of its children's boxes (merge_bounds_kernel,
+// bvh/gpu_bvh.cu:182-214).  A node whose leaf range lies inside this block's leaves
+// [lo, lo + kClimbThreads) has both its children climbing in this block and an index in
+// that range too (a Karras node is numbered by one end of its range), so the hand-over
+// goes through shared memory; above that through the node's slot in global memory with
+// an acquire-release counter, which the second arrival resets to zero.  One 16-byte load
+// of node_info per level gives the node's range and its parent link.
 template <int Kind>
 __global__ void __launch_bounds__(kClimbThreads) k_leaf_climb(const float* prims, int n,
                                                               const int* sorted_ids,
                                                               TriRecord* tris, BvhNode* nodes,
                                                               const int* leaf_parent,
                                                               const int4* node_info,
-                                                              int* escape, float* root,
+                                                              unsigned* flags, float* root,
                                                               int* error) {
     __shared__ float sbox[kClimbThreads][2][6];
     __shared__ unsigned sflag[kClimbThreads];
@@ -652,28 +644,29 @@ __global__ void __launch_bounds__(kClimbThreads) k_leaf_climb(const float* prims
         if (code < 0 || p >= n - 1) break;  // parent links out of range: report below
         const int4 info = node_info[p];
         const int s = p - lo;
-        if (!(info.x >= lo && info.y < lo + kClimbThreads && s >= 0 && s < kClimbThreads)) {
-            // The parent's leaves leave this block: phase 2 takes over from its slot.
+        if (info.x >= lo && info.y < lo + kClimbThreads && s >= 0 && s < kClimbThreads) {
+            volatile float* mine = &sbox[s][slot][0];
+            mine[0] = b.lo.x; mine[1] = b.lo.y; mine[2] = b.lo.z;
+            mine[3] = b.hi.x; mine[4] = b.hi.y; mine[5] = b.hi.z;
+            __threadfence_block();
+            unsigned prior = atomicAdd(&sflag[s], 1u);
+            if (prior == 0) return;  // the sibling finishes this node
+            __threadfence_block();
+            volatile const float* o = &sbox[s][slot ^ 1][0];
+            box3 sib{make_f3(o[0], o[1], o[2]), make_f3(o[3], o[4], o[5])};
+            const box3 left = slot ? sib : b;
+            const box3 right = slot ? b : sib;
+            store_slot(nodes + p, 0, left);
+            store_slot(nodes + p, 1, right);
+            b = box_union(left, right);
+        } else {
             store_slot(nodes + p, slot, b);
-            const int e = atomicAdd(escape + n, 1);
-            if (e < n) escape[e] = code;
-            else atomicOr(error, kErrLoopBound);   // cannot happen: at most n escapes
-            return;
+            unsigned prior = atomic_add_acq_rel(flags + p, 1u);
+            if (prior == 0) return;  // the sibling finishes this node
+            flags[p] = 0;
+            box3 sib = load_slot_cg(nodes + p, slot ^ 1);
+            b = slot ? box_union(sib, b) : box_union(b, sib);
         }
-        volatile float* mine = &sbox[s][slot][0];
-        mine[0] = b.lo.x; mine[1] = b.lo.y; mine[2] = b.lo.z;
-        mine[3] = b.hi.x; mine[4] = b.hi.y; mine[5] = b.hi.z;
-        __threadfence_block();
-        unsigned prior = atomicAdd(&sflag[s], 1u);
-        if (prior == 0) return;  // the sibling finishes this node
-        __threadfence_block();
-        volatile const float* o = &sbox[s][slot ^ 1][0];
-        box3 sib{make_f3(o[0], o[1], o[2]), make_f3(o[3], o[4], o[5])};
-        const box3 left = slot ? sib : b;
-        const box3 right = slot ? b : sib;
-        store_slot(nodes + p, 0, left);
-        store_slot(nodes + p, 1, right);
-        b = box_union(left, right);
         if (p == 0) {
             root[0] = b.lo.x; root[1] = b.lo.y; root[2] = b.lo.z;
             root[3] = b.hi.x; root[4] = b.hi.y; root[5] = b.hi.z;
@@ -682,49 +675,6 @@ __global__ void __launch_bounds__(kClimbThreads) k_leaf_climb(const float* prims
         code = info.z;
     }
     atomicOr(error, kErrClimbBound);
-}
-
-// Phase 2 (one block): each escape entry is a parent code whose slot holds a box; the
-// thread counts itself in at that node and, as the second arrival, unions the node's two
-// slots, stores the node's box in its own parent's slot and climbs on.  The escape
-// counter (escape[n]) is reset for the next pass.
-__global__ void __launch_bounds__(kUpperThreads) k_upper_climb(int n, BvhNode* nodes,
-                                                               const int4* node_info,
-                                                               int* escape, unsigned* flags,
-                                                               float* root, int* error) {
-    const int count = min(escape[n], n);
-    __syncthreads();
-    if (threadIdx.x == 0) escape[n] = 0;
-    for (int e = threadIdx.x; e < count; e += kUpperThreads) {
-        int code = escape[e];
-        bool finished = false;
-        for (int level = 0; level < kClimbBound && !finished; ++level) {
-            const int p = code >> 1;
-            if (code < 0 || p >= n - 1) {
-                atomicOr(error, kErrLoopBound);
-                break;
-            }
-            const int4 info = node_info[p];
-            __threadfence_block();
-            const unsigned prior = atomicAdd(flags + p, 1u);
-            if (prior == 0) {
-                finished = true;  // the sibling finishes this node
-                break;
-            }
-            __threadfence_block();
-            flags[p] = 0;
-            const box3 b = box_union(load_slot_cg(nodes + p, 0), load_slot_cg(nodes + p, 1));
-            if (p == 0) {
-                root[0] = b.lo.x; root[1] = b.lo.y; root[2] = b.lo.z;
-                root[3] = b.hi.x; root[4] = b.hi.y; root[5] = b.hi.z;
-                finished = true;
-                break;
-            }
-            code = info.z;
-            store_slot(nodes + (code >> 1), code & 1, b);
-        }
-        if (!finished) atomicOr(error, kErrClimbBound);
-    }
 }
 
 // ---------------------------------------------------------------- export
@@ -836,11 +786,8 @@ template <int Kind>
 int climb(lux_ctx* ctx, lux_bvh* bvh, const float* prims) {
     k_leaf_climb<Kind><<<grid_for(bvh->n, kClimbThreads), kClimbThreads, 0, ctx->stream>>>(
         prims, bvh->n, bvh->sorted_ids, bvh->tris, bvh->nodes, bvh->leaf_parent,
-        bvh->node_info, bvh->escape, bvh->root, ctx->d_error);
-    k_upper_climb<<<1, kUpperThreads, 0, ctx->stream>>>(bvh->n, bvh->nodes, bvh->node_info,
-                                                        bvh->escape, bvh->flags, bvh->root,
-                                                        ctx->d_error);
-    ctx->launches += 2;
+        bvh->node_info, bvh->flags, bvh->root, ctx->d_error);
+    ctx->launches += 1;
     return cuda_fail(cudaGetLastError(), "k_leaf_climb");
 }
 
@@ -888,7 +835,6 @@ int lbvh_alloc(lux_ctx* ctx, lux_bvh* bvh) {
         {reinterpret_cast<void**>(&bvh->leaf_parent), sizeof(int) * n},
         {reinterpret_cast<void**>(&bvh->node_parent), sizeof(int) * std::max(n - 1, 1)},
         {reinterpret_cast<void**>(&bvh->node_info), sizeof(int4) * std::max(n - 1, 1)},
-        {reinterpret_cast<void**>(&bvh->escape), sizeof(int) * (static_cast<size_t>(n) + 1)},
         {reinterpret_cast<void**>(&bvh->flags), sizeof(unsigned) * std::max(n - 1, 1)},
         {&bvh->codes, key * n},
         {reinterpret_cast<void**>(&bvh->root), sizeof(float) * 16},
@@ -902,14 +848,13 @@ int lbvh_alloc(lux_ctx* ctx, lux_bvh* bvh) {
         }
     }
     cudaError_t err = cudaMemset(bvh->flags, 0, sizeof(unsigned) * std::max(n - 1, 1));
-    if (err == cudaSuccess) err = cudaMemset(bvh->escape + n, 0, sizeof(int));
     if (err == cudaSuccess) err = cudaMemset(bvh->leaf_parent, 0xff, sizeof(int) * n);
     return cuda_fail(err, "lbvh init");
 }
 
 void lbvh_free(lux_bvh* bvh) {
     void* ptrs[] = {bvh->nodes, bvh->tris, bvh->sorted_ids, bvh->leaf_parent, bvh->node_parent,
-                    bvh->node_info, bvh->escape, bvh->flags, bvh->codes, bvh->root, bvh->wide};
+                    bvh->node_info, bvh->flags, bvh->codes, bvh->root, bvh->wide};
     bvh->wide = nullptr;
     bvh->wide_capacity = 0;
     bvh->wide_current = false;
@@ -922,7 +867,6 @@ void lbvh_free(lux_bvh* bvh) {
     bvh->leaf_parent = nullptr;
     bvh->node_parent = nullptr;
     bvh->node_info = nullptr;
-    bvh->escape = nullptr;
     bvh->flags = nullptr;
     bvh->codes = nullptr;
     bvh->root = nullptr;

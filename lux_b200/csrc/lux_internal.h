@@ -49,7 +49,6 @@ struct lux_bvh {
     int* leaf_parent = nullptr;         // n
     int* node_parent = nullptr;         // n - 1
     int4* node_info = nullptr;          // n - 1: first and last sorted leaf, parent code
-    int* escape = nullptr;              // n + 1: the climb's escape list, its count last
     unsigned* flags = nullptr;          // n - 1, zero between passes
     void* codes = nullptr;              // n sorted codes (uint32 or uint64)
     float* root = nullptr;              // 6
