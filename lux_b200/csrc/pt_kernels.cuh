@@ -13,6 +13,7 @@
 #include <cuda_runtime.h>
 
 #include "../../include/lux_gpu.h"
+#include "lux_wide.cuh"
 #include "pt_device.cuh"
 
 namespace lux {
@@ -270,12 +271,16 @@ LUX_D SceneHit scene_closest(const SceneView& sc, f3 o, f3 d, float tmin, float 
 
 // scene_closest as a resumable walk: step() advances by one node visit or one triangle
 // (or instance) test, followed by the pops it enables, so a kernel can interleave many
-// walks per warp and refill lanes as walks finish.  The decisions, in order, are those
-// of scene_closest / blas_closest above, so the result is the same.  The four stacks
-// live apart from the scalar state, which then stays in registers.
+// walks per warp and refill lanes as walks finish.  The TLAS is walked over its binary
+// nodes, each BLAS over its quantised 4-wide nodes (lux_wide.cuh: every leaf the binary
+// walk reaches is reached in the same left-first order and accepted by the exact test of
+// its own box, the triangle's box formed from its record), so the leaves tested and the
+// best hit after each are those of scene_closest / blas_closest above and the result is
+// the same.  The stacks live apart from the scalar state, which then stays in registers.
+constexpr int kWideBlasStack = 96;   // three deferred children per 4-wide level
 struct WalkStacks {  // deferred (node ref, entry t bits), TLAS and BLAS
     int2 t[kStack];
-    int2 b[kStack];
+    int2 b[kWideBlasStack];
 };
 
 struct TwoLevelWalk {
@@ -287,12 +292,13 @@ struct TwoLevelWalk {
     int t_cur, t_sp;
     long long t_steps;
     bool in_blas;
-    const BvhNode* b_nodes;
+    const WideNode* b_wide;
     const TriRecord* b_tris;
     int b_n, b_cur, b_sp, b_ignored, b_first;
     long long b_steps;
     f3 lo, ld;
     slab_ray lsr;
+    unsigned lneg;                // octant of the object-space ray (octant_ray::neg)
     bool done;
     bool any_hit;                 // end at the first accepted triangle (occlusion only)
 
@@ -364,37 +370,41 @@ struct TwoLevelWalk {
                 fail(error, kErrLoopBound, INFINITY);
                 return true;
             }
+            const octant_ray lorr{lsr.o, lsr.inv, lsr.tmin, lneg};
             bool pop = true;
             if (b_cur >= 0) {
-                BvhNode nd = load_node(b_nodes, b_cur);
-                float tl_, tr_;
-                bool hl = slab_hit(lsr, node_left_box(nd), hit.t, tl_);
-                bool hr = slab_hit(lsr, node_right_box(nd), hit.t, tr_);
-                if (hl) {
-                    if (hr) {
-                        if (b_sp >= kStack) {
-                            fail(error, kErrStackOverflow, INFINITY);
-                            return true;
-                        }
-                        k.b[b_sp] = make_int2(nd.ch.y, __float_as_int(tr_));
-                        ++b_sp;
+                const WideNode w = load_wide(b_wide, b_cur);
+                float tt[4];
+                const unsigned m = wide_test(w, lsr, lorr, hit.t, tt);
+                if (m) {
+                    const int f = __ffs(m) - 1;
+                    if (b_sp + __popc(m) - 1 > kWideBlasStack) {
+                        fail(error, kErrStackOverflow, INFINITY);
+                        return true;
                     }
-                    b_cur = nd.ch.x;
-                    pop = false;
-                } else if (hr) {
-                    b_cur = nd.ch.y;
+#pragma unroll
+                    for (int c = 3; c >= 1; --c) {
+                        if (c > f && ((m >> c) & 1u)) {
+                            k.b[b_sp] = make_int2(wide_ref(w, c), __float_as_int(tt[c]));
+                            ++b_sp;
+                        }
+                    }
+                    b_cur = wide_ref(w, f);
                     pop = false;
                 }
             } else {
                 const float4* tp = reinterpret_cast<const float4*>(b_tris + ~b_cur);
-                float4 p0 = __ldg(tp);
-                int local = __float_as_int(p0.w);
+                const float4 p0 = __ldg(tp);
+                const int local = __float_as_int(p0.w);
                 if (local != b_ignored) {
-                    float4 p1 = __ldg(tp + 1);
-                    float4 p2 = __ldg(tp + 2);
-                    float t, u, v;
-                    if (moller_trumbore(lo, ld, xyz(p0), xyz(p1), xyz(p2), t, u, v) && t > tmin
-                        && t < hit.t) {
+                    const float4 p1 = __ldg(tp + 1);
+                    const float4 p2 = __ldg(tp + 2);
+                    float tn, t, u, v;
+                    // The leaf's exact box (the triangle's box) under the current best t,
+                    // then the triangle.
+                    if (child_hit(triangle_box(xyz(p0), xyz(p1), xyz(p2)), lsr, lorr, hit.t, tn)
+                        && moller_trumbore(lo, ld, xyz(p0), xyz(p1), xyz(p2), t, u, v)
+                        && t > tmin && t < hit.t) {
                         hit.prim = b_first + local;
                         hit.t = t;
                         hit.u = u;
@@ -448,7 +458,8 @@ struct TwoLevelWalk {
                 float tn;
                 if (slab_hit(lsr, load_root(b.root), hit.t, tn)) {
                     in_blas = true;
-                    b_nodes = b.nodes;
+                    lneg = make_octant_ray(lsr).neg;
+                    b_wide = b.wide;
                     b_tris = b.tris;
                     b_n = b.n;
                     b_cur = b.n == 1 ? ~0 : 0;

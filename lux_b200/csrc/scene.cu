@@ -882,8 +882,10 @@ int scene_create(lux_ctx* ctx, const lux_scene_desc* d, lux_scene** out) {
         st = lux_lbvh_build(ctx, soup, md.triangle_count, LUX_PRIM_TRIANGLES, 30, &b);
         if (!st) {
             s->blas.push_back(b);
-            views.push_back(b->view());
+            // The path tracer walks each BLAS over its 4-wide nodes.
+            st = lbvh_ensure_wide(ctx, b);
         }
+        if (!st) views.push_back(b->view());
     }
     if (!st) st = upload(&s->blas_views, views, ctx->stream);
 
@@ -1132,6 +1134,8 @@ int scene_update_mesh(lux_ctx* ctx, lux_scene* s, int mesh, const float* vertice
         r.vertices, vertex_count, r.indices, triangle_count, soup, ctx->d_error);
     ctx->launches += 1;
     if (int st = lbvh_refit(ctx, s->blas[mesh], soup)) return st;
+    // Same node count, so the 4-wide nodes are rebuilt in place (the view is unchanged).
+    if (int st = lbvh_ensure_wide(ctx, s->blas[mesh])) return st;
     if (r.instance_count > 0) {
         k_instance_positions<<<blocks_for(ctx, int64_t(triangle_count) * r.instance_count),
                                kRefitThreads, 0, stream>>>(soup, triangle_count, s->d_instances,

@@ -139,7 +139,7 @@ __global__ void __launch_bounds__(kThreads) k_shadow(PathPool rt, int* counts,
 }
 
 // k_shadow with refilling lanes (refill_shadows); the cursor is the bounce's slot 8.
-__global__ void __launch_bounds__(kThreads) k_shadow_refill(PathPool rt, int* counts,
+__global__ void __launch_bounds__(kThreads, 3) k_shadow_refill(PathPool rt, int* counts,
                                                             unsigned long long* rays,
                                                             SceneView sc, int depth, int budget,
                                                             int* error) {
