@@ -787,6 +787,7 @@ def render_line(args, name: str, steps: int, warmup: int, nested: bool = False) 
                        "autotuned": {"trace_variant": tune.trace_variant,
                                      "path_budget": tune.budget,
                                      "render_batch": tune.render_batch,
+                                     "refill_blocks_per_sm": tune.refill_blocks,
                                      "probe": f"{probe.width}x{probe.height}, {probe.spp} spp"}},
             "rays": {"camera_extension": rays[0], "shadow_segments": rays[1]},
             "clocks": clock_info, "gpu_launches": launches,

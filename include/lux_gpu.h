@@ -77,6 +77,8 @@ int lux_ctx_launch_count(lux_ctx* ctx, int64_t* count);
  *   LUX_OPT_RENDER_BATCH   paths in flight per wavefront batch (device memory ~200 B each)
  *   LUX_OPT_PATH_BUDGET    traversal steps per refill round of the path tracer's extension and
  *                          shadow kernels (variant 1 uses one thread per path instead)
+ *   LUX_OPT_REFILL_BLOCKS  resident 256-thread blocks per SM of those refilling kernels'
+ *                          persistent grids (0: as many as fit, else 1..3)
  * Read only (lux_ctx_get_option), the device memory the context holds for reuse:
  *   LUX_OPT_SCRATCH_BYTES  growable scratch of builds and queries
  *   LUX_OPT_STAGING_BYTES  growable staging of host arguments */
@@ -86,7 +88,8 @@ enum lux_option {
     LUX_OPT_RENDER_BATCH = 3,
     LUX_OPT_PATH_BUDGET = 4,
     LUX_OPT_SCRATCH_BYTES = 5,
-    LUX_OPT_STAGING_BYTES = 6
+    LUX_OPT_STAGING_BYTES = 6,
+    LUX_OPT_REFILL_BLOCKS = 7
 };
 int lux_ctx_set_option(lux_ctx* ctx, int32_t option, int64_t value);
 int lux_ctx_get_option(lux_ctx* ctx, int32_t option, int64_t* value);
@@ -97,8 +100,10 @@ int lux_ctx_get_option(lux_ctx* ctx, int32_t option, int64_t* value);
  * results.  lux_autotune_trace: LUX_OPT_TRACE_VARIANT x LUX_OPT_TRACE_BUDGET on n
  * closest-hit rays (device pointer, the lux_trace_closest layout) against `bvh`.
  * lux_autotune_render: one thread per path vs refilling lanes x LUX_OPT_PATH_BUDGET x
- * LUX_OPT_RENDER_BATCH on a probe render of `scene` (use a probe the size of the real
- * renders).  default_ms is the time with the options in effect before tuning.
+ * LUX_OPT_RENDER_BATCH (the paths queued per wavefront batch), then, for refilling
+ * lanes, LUX_OPT_REFILL_BLOCKS (the persistent grid's blocks per SM), on a probe render
+ * of `scene` (use a probe the size of the real renders).  default_ms is the time with
+ * the options in effect before tuning.
  */
 typedef struct lux_tune_result {
     int32_t trace_variant;
@@ -107,6 +112,7 @@ typedef struct lux_tune_result {
     float best_ms;
     float default_ms;
     int32_t candidates;
+    int32_t refill_blocks;    /* 0 for ray-query tuning and one thread per path */
 } lux_tune_result;
 int lux_autotune_trace(lux_ctx* ctx, lux_bvh* bvh, const float* rays, int32_t n,
                        lux_tune_result* out);

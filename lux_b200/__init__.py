@@ -45,6 +45,7 @@ OPT_TRACE_BUDGET = 2    # traversal steps per refill round (ray queries)
 OPT_PATH_BUDGET = 4     # traversal steps per refill round (path tracer)
 OPT_SCRATCH_BYTES = 5   # read only: the context's reusable device scratch
 OPT_STAGING_BYTES = 6   # read only: the context's reusable device staging
+OPT_REFILL_BLOCKS = 7   # blocks per SM of the refilling path-tracer kernels (0: max)
 OPT_RENDER_BATCH = 3    # paths in flight per wavefront batch
 
 # Every symbol include/lux_gpu.h declares, with its ctypes signature.

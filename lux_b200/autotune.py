@@ -11,7 +11,8 @@ from . import _check, _ptr, load_library
 class _TuneResult(ctypes.Structure):
     _fields_ = [("trace_variant", ctypes.c_int32), ("budget", ctypes.c_int32),
                 ("render_batch", ctypes.c_int64), ("best_ms", ctypes.c_float),
-                ("default_ms", ctypes.c_float), ("candidates", ctypes.c_int32)]
+                ("default_ms", ctypes.c_float), ("candidates", ctypes.c_int32),
+                ("refill_blocks", ctypes.c_int32)]
 
 
 @dataclass
@@ -22,11 +23,12 @@ class TuneResult:
     best_ms: float
     default_ms: float
     candidates: int
+    refill_blocks: int = 0
 
 
 def _result(r: _TuneResult) -> TuneResult:
     return TuneResult(r.trace_variant, r.budget, r.render_batch, r.best_ms, r.default_ms,
-                      r.candidates)
+                      r.candidates, r.refill_blocks)
 
 
 def autotune_trace(ctx, bvh, rays) -> TuneResult:

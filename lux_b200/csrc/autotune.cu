@@ -5,7 +5,8 @@
 //   lux_autotune_trace   ray queries: traversal variant (binary / 4-wide nodes, one
 //                        thread per ray / persistent warps) x steps per refill round
 //   lux_autotune_render  path tracer: one thread per path vs refilling lanes x steps per
-//                        refill round x paths per wavefront batch
+//                        refill round x paths per wavefront batch, then the refilling
+//                        kernels' blocks per SM
 // Each candidate runs `repeats` times on ctx's stream between CUDA events; its time is
 // the fastest repeat.  No reference counterpart (the reference has fixed launch shapes).
 
@@ -24,6 +25,7 @@ struct Candidate {
     int variant;
     int budget;
     int batch;
+    int blocks = 0;   // refilling kernels' blocks per SM (0: as many as fit)
 };
 
 template <typename Run>
@@ -65,6 +67,7 @@ void apply(lux_ctx* ctx, const Candidate& c, bool render) {
     if (render) {
         ctx->path_budget = c.budget;
         ctx->render_batch = c.batch;
+        ctx->refill_blocks = c.blocks;
     } else {
         ctx->trace_budget = c.budget;
     }
@@ -121,6 +124,7 @@ extern "C" int lux_autotune_trace(lux_ctx* ctx, lux_bvh* bvh, const float* rays,
     out->trace_variant = best.variant;
     out->budget = best.budget;
     out->render_batch = 0;
+    out->refill_blocks = 0;
     out->best_ms = best_ms;
     out->default_ms = default_ms;
     out->candidates = static_cast<int32_t>(cands.size());
@@ -141,7 +145,8 @@ extern "C" int lux_autotune_render(lux_ctx* ctx, const lux_scene* scene,
         cudaGetLastError();
         return lux::fail(LUX_ERR_OUT_OF_MEMORY, "autotune film");
     }
-    const Candidate before{ctx->trace_variant, ctx->path_budget, ctx->render_batch};
+    const Candidate before{ctx->trace_variant, ctx->path_budget, ctx->render_batch,
+                           ctx->refill_blocks};
     std::vector<Candidate> cands;
     cands.push_back(before);
     std::vector<int> batches;
@@ -154,17 +159,38 @@ extern "C" int lux_autotune_render(lux_ctx* ctx, const lux_scene* scene,
     int st = LUX_OK;
     float best_ms = INFINITY, default_ms = INFINITY;
     Candidate best = before;
+    auto run = [&](const Candidate& c, float* ms) {
+        apply(ctx, c, true);
+        int s2 = time_candidate(ctx, 2, [&] { return lux::render(ctx, scene, *probe, film, false); },
+                                ms);
+        if (!s2) s2 = check_error_word(ctx);
+        return s2;
+    };
     for (size_t i = 0; i < cands.size() && !st; ++i) {
-        apply(ctx, cands[i], true);
         float ms = 0;
-        st = time_candidate(ctx, 2, [&] { return lux::render(ctx, scene, *probe, film, false); },
-                            &ms);
-        if (!st) st = check_error_word(ctx);
+        st = run(cands[i], &ms);
         if (st) break;
         if (i == 0) default_ms = ms;
         if (ms < best_ms) {
             best_ms = ms;
             best = cands[i];
+        }
+    }
+    // Second stage, refilling lanes only: fewer resident blocks per SM than fit (fewer
+    // warps, more cache and shared bandwidth each).
+    int tried = static_cast<int>(cands.size());
+    if (!st && best.variant != lux::kTraceStatic) {
+        for (int blocks : {1, 2}) {
+            Candidate c = best;
+            c.blocks = blocks;
+            float ms = 0;
+            st = run(c, &ms);
+            ++tried;
+            if (st) break;
+            if (ms < best_ms) {
+                best_ms = ms;
+                best = c;
+            }
         }
     }
     cudaFree(film);
@@ -175,6 +201,7 @@ extern "C" int lux_autotune_render(lux_ctx* ctx, const lux_scene* scene,
     out->render_batch = best.batch;
     out->best_ms = best_ms;
     out->default_ms = default_ms;
-    out->candidates = static_cast<int32_t>(cands.size());
+    out->candidates = tried;
+    out->refill_blocks = best.blocks;
     return LUX_OK;
 }

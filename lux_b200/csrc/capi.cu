@@ -363,6 +363,10 @@ int lux_ctx_set_option(lux_ctx* ctx, int32_t option, int64_t value) {
             if (value < 1 || value > (1 << 28)) return lux::fail(LUX_ERR_INVALID_ARGUMENT, "render batch 1..2^28");
             ctx->render_batch = static_cast<int>(value);
             return LUX_OK;
+        case LUX_OPT_REFILL_BLOCKS:
+            if (value < 0 || value > 3) return lux::fail(LUX_ERR_INVALID_ARGUMENT, "refill blocks 0..3");
+            ctx->refill_blocks = static_cast<int>(value);
+            return LUX_OK;
         default:
             return lux::fail(LUX_ERR_INVALID_ARGUMENT, "unknown option");
     }
@@ -375,6 +379,7 @@ int lux_ctx_get_option(lux_ctx* ctx, int32_t option, int64_t* value) {
         case LUX_OPT_TRACE_BUDGET: *value = ctx->trace_budget; return LUX_OK;
         case LUX_OPT_RENDER_BATCH: *value = ctx->render_batch; return LUX_OK;
         case LUX_OPT_PATH_BUDGET: *value = ctx->path_budget; return LUX_OK;
+        case LUX_OPT_REFILL_BLOCKS: *value = ctx->refill_blocks; return LUX_OK;
         case LUX_OPT_SCRATCH_BYTES: *value = static_cast<int64_t>(ctx->scratch_bytes); return LUX_OK;
         case LUX_OPT_STAGING_BYTES: *value = static_cast<int64_t>(ctx->staging_bytes); return LUX_OK;
         default: return lux::fail(LUX_ERR_INVALID_ARGUMENT, "unknown option");

@@ -20,6 +20,7 @@ struct lux_ctx {
     int trace_budget = 16;           // traversal steps per refill round (ray queries)
     int path_budget = 32;            // traversal steps per refill round (path tracer)
     int render_batch = 1 << 22;      // paths in flight per wavefront batch
+    int refill_blocks = 0;           // blocks per SM of the refilling kernels (0: max)
     void* render_runtime = nullptr;  // wavefront buffers, grown on demand
     // Growable device scratch, reused across calls on this context.
     void* scratch = nullptr;

@@ -414,10 +414,16 @@ int render(lux_ctx* ctx, const lux_scene* scene, const lux_render_request& req, 
     const SceneView& sc = scene->view;
     cudaStream_t s = ctx->stream;
     int grid = ctx->sm_count * 8;
+    // Persistent grids of the refilling kernels: blocks per SM up to what fits, or the
+    // context's LUX_OPT_REFILL_BLOCKS when it asks for fewer.
+    const int refill_fit = occupancy_blocks(ctx, kOccExtendRefill, k_extend_refill, kThreads);
+    const int shadow_fit = occupancy_blocks(ctx, kOccShadowRefill, k_shadow_refill, kThreads);
     const int refill_grid =
-        ctx->sm_count * occupancy_blocks(ctx, kOccExtendRefill, k_extend_refill, kThreads);
+        ctx->sm_count * (ctx->refill_blocks > 0 ? std::min(ctx->refill_blocks, refill_fit)
+                                                : refill_fit);
     const int shadow_grid =
-        ctx->sm_count * occupancy_blocks(ctx, kOccShadowRefill, k_shadow_refill, kThreads);
+        ctx->sm_count * (ctx->refill_blocks > 0 ? std::min(ctx->refill_blocks, shadow_fit)
+                                                : shadow_fit);
     cudaError_t err = cudaMemsetAsync(rt.rays, 0, 16, s);
     if (!per_sample && err == cudaSuccess)
         err = cudaMemsetAsync(out, 0, sizeof(float) * 3 * size_t(pixels), s);

@@ -272,14 +272,21 @@ def test_autotune_render_keeps_the_image(ctx):
     sc = S.Scene(ctx, SC.heavy_render_scene(96, 96))
     req = S.request(96, 96, 8, 6, 2)
     want = S.render(ctx, sc, req)
-    saved = [ctx.get_option(o) for o in (1, 3, 4)]
+    saved = [ctx.get_option(o) for o in (1, 3, 4, 7)]
     try:
         res = autotune.autotune_render(ctx, sc, req)
         assert res.candidates >= 6 and res.best_ms <= res.default_ms
         assert ctx.get_option(lux_b200.OPT_PATH_BUDGET) == res.budget
+        assert ctx.get_option(lux_b200.OPT_REFILL_BLOCKS) == res.refill_blocks
+        assert res.refill_blocks in (0, 1, 2)
         assert np.array_equal(S.render(ctx, sc, req), want)
+        # Every launch shape of the refilling kernels renders the same image.
+        ctx.set_option(lux_b200.OPT_TRACE_VARIANT, 0)
+        for blocks in (1, 2, 3, 0):
+            ctx.set_option(lux_b200.OPT_REFILL_BLOCKS, blocks)
+            assert np.array_equal(S.render(ctx, sc, req), want)
     finally:
-        for o, v in zip((1, 3, 4), saved):
+        for o, v in zip((1, 3, 4, 7), saved):
             ctx.set_option(o, v)
 
 
