@@ -31,31 +31,60 @@
 namespace lux {
 namespace {
 
+// Launch shapes; the LUX_* macros exist so that other shapes can be built and timed
+// against these defaults (results do not depend on them).
+#ifndef LUX_SORT_ITEMS
+#define LUX_SORT_ITEMS 16
+#endif
+#ifndef LUX_CLIMB_THREADS
+#define LUX_CLIMB_THREADS 512
+#endif
+#ifndef LUX_LOOKBACK_BATCH
+#define LUX_LOOKBACK_BATCH 8
+#endif
+#ifndef LUX_PDL
+#define LUX_PDL 0
+#endif
+
 constexpr int kThreads = 256;
 constexpr int kRadix = 256;
-constexpr int kSortItems = 16;
+constexpr int kSortItems = LUX_SORT_ITEMS;
 constexpr int kSortTile = kThreads * kSortItems;  // keys per tile
+// The allocation-free sort's tiles (its scratch size is part of the ABI): fixed.
+constexpr int kStaticItems = 16;
+constexpr int kStaticTile = kThreads * kStaticItems;
 constexpr int kScanThreads = 1024;
 constexpr int kClimbBound = 160;                 // > max tree depth (64 + 96 bits)
 constexpr int kMaxPasses = 8;                    // 8-bit digits of a 63-bit key
-constexpr int kClimbThreads = 512;               // leaves per climb block
+constexpr int kClimbThreads = LUX_CLIMB_THREADS; // leaves per climb block
+constexpr int kClimbSmem = kClimbThreads * (6 * 8 + 4);   // k_leaf_climb's shared memory
 constexpr long long kLookbackSpins = 1ll << 22;  // bound of one look-back wait
 
 // Relaxed device-scope accesses of the look-back words (each word carries its own value,
 // so no other ordering is needed) and an acquire-release add for the climb's flags.
-LUX_D unsigned long long ld_relaxed(const unsigned long long* p) {
-    unsigned long long v;
-    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+LUX_D unsigned ld_relaxed(const unsigned* p) {
+    unsigned v;
+    asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
     return v;
 }
-LUX_D void st_relaxed(unsigned long long* p, unsigned long long v) {
-    asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+LUX_D void st_relaxed(unsigned* p, unsigned v) {
+    asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 LUX_D unsigned atomic_add_acq_rel(unsigned* p, unsigned v) {
     unsigned old;
     asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], %2;"
                  : "=r"(old) : "l"(p), "r"(v) : "memory");
     return old;
+}
+
+// Programmatic dependent launch of the build's kernel chain: each kernel lets the next
+// one be launched as soon as all of its own blocks are running (launch_dependents), and
+// waits, before touching memory, until the previous kernel has completed and its writes
+// are visible (wait; a no-op in a kernel launched without the attribute).  The next
+// kernel's launch then overlaps this one's tail instead of following it.
+LUX_D void chain_wait() {
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    asm volatile("griddepcontrol.wait;" ::: "memory");
 }
 
 LUX_D unsigned lanemask_lt() {
@@ -79,11 +108,57 @@ LUX_D void load_prim(const float* prims, int i, f3& v0, f3& v1, f3& v2, box3& b)
     }
 }
 
+// load_prim through 16-byte loads: the aligned window of three float4 (triangles, 36 B at
+// any 4-byte offset) or two (boxes, 24 B at an 8-byte offset) that holds the primitive,
+// the primitive's floats then selected from it.  Three load instructions instead of nine
+// (two instead of six), each lane's bytes in at most three sectors.  Used when the
+// buffer is 16-byte aligned and the window ends inside it; the scalar loads otherwise.
+template <int Kind>
+LUX_D void load_prim_vec(const float* prims, int n, int i, bool aligned, f3& v0, f3& v1,
+                         f3& v2, box3& b) {
+    constexpr int kFloats = Kind == LUX_PRIM_TRIANGLES ? 9 : 6;
+    constexpr int kWindow = Kind == LUX_PRIM_TRIANGLES ? 12 : 8;
+    const size_t off = static_cast<size_t>(i) * kFloats;
+    const size_t base = off & ~size_t(3);
+    if (!aligned || base + kWindow > static_cast<size_t>(n) * kFloats) {
+        load_prim<Kind>(prims, i, v0, v1, v2, b);
+        return;
+    }
+    const int r = static_cast<int>(off & 3);
+    const float4* p = reinterpret_cast<const float4*>(prims + base);
+    float w[kWindow];
+#pragma unroll
+    for (int q = 0; q < kWindow / 4; ++q) {
+        const float4 x = __ldg(p + q);
+        w[4 * q] = x.x; w[4 * q + 1] = x.y; w[4 * q + 2] = x.z; w[4 * q + 3] = x.w;
+    }
+    float t[kFloats];
+#pragma unroll
+    for (int j = 0; j < kFloats; ++j) {
+        if (Kind == LUX_PRIM_TRIANGLES)
+            t[j] = r == 0 ? w[j] : r == 1 ? w[j + 1] : r == 2 ? w[j + 2] : w[j + 3];
+        else
+            t[j] = r == 0 ? w[j] : w[j + 2];
+    }
+    if (Kind == LUX_PRIM_TRIANGLES) {
+        v0 = make_f3(t[0], t[1], t[2]);
+        v1 = make_f3(t[3], t[4], t[5]);
+        v2 = make_f3(t[6], t[7], t[8]);
+        b = triangle_box(v0, v1, v2);
+    } else {
+        b = box3{make_f3(t[0], t[1], t[2]), make_f3(t[3], t[4], t[5])};
+        v0 = v1 = v2 = make_f3(0, 0, 0);
+    }
+}
+
+LUX_D bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; }
+
 // ---------------------------------------------------------------- 1. root box
 
 template <int Kind>
 __global__ void __launch_bounds__(kThreads) k_root_reduce(const float* prims, int n,
                                                           unsigned* root_ord) {
+    chain_wait();
     float lo[3] = {INFINITY, INFINITY, INFINITY};
     float hi[3] = {-INFINITY, -INFINITY, -INFINITY};
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
@@ -162,6 +237,7 @@ template <int Kind, typename Key, int Passes>
 __global__ void __launch_bounds__(kThreads) k_morton_hist(const float* prims, int n,
                                                           const unsigned* root_ord,
                                                           Key* codes, unsigned* hist) {
+    chain_wait();
     constexpr int kCopies = Passes <= 4 ? kThreads / 32 : 2;
     __shared__ unsigned h[kCopies][Passes][kRadix];
     for (int i = threadIdx.x; i < kCopies * Passes * kRadix; i += kThreads) (&h[0][0][0])[i] = 0;
@@ -190,6 +266,7 @@ __global__ void __launch_bounds__(kThreads) k_morton_hist(const float* prims, in
 // Exclusive prefix of each pass's digit counts: bases[p * kRadix + d] = the number of
 // keys whose pass-p digit is below d.  One block of kRadix threads per pass.
 __global__ void __launch_bounds__(kRadix) k_digit_bases(const unsigned* hist, unsigned* bases) {
+    chain_wait();
     __shared__ unsigned warp_sums[kRadix / 32];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const unsigned v = hist[blockIdx.x * kRadix + threadIdx.x];
@@ -220,10 +297,12 @@ LUX_D unsigned digit_peers(unsigned d, bool valid) {
     return peers;
 }
 
-// Look-back words: value in the low 32 bits, state in the high ones (0: not yet
-// published; aggregate: this tile's own count; prefix: the count over tiles 0..t).
-constexpr unsigned long long kTileAggregate = 1ull << 32;
-constexpr unsigned long long kTilePrefix = 2ull << 32;
+// Look-back words, 32 bits: 0 while not yet published; kTileAggregate | this tile's own
+// count (at most kSortTile); kTilePrefix | the count over tiles 0..t (at most 2^30, the
+// primitive limit, so it fits below the flag bit).
+constexpr unsigned kTileAggregate = 1u << 30;
+constexpr unsigned kTilePrefix = 1u << 31;
+constexpr int kLookbackBatch = LUX_LOOKBACK_BATCH;   // earlier tiles' words loaded together
 
 // One stable LSD pass over all keys.  Tiles of kSortTile keys are taken in launch order
 // (an atomic counter), ranked inside the tile as k_sort_downsweep ranks them (per-warp
@@ -238,8 +317,9 @@ template <typename Key, bool First>
 __global__ void __launch_bounds__(kThreads) k_onesweep(const Key* keys_in, const int* vals_in,
                                                        Key* keys_out, int* vals_out, int n,
                                                        int shift, const unsigned* bases,
-                                                       unsigned long long* lookback,
+                                                       unsigned* lookback,
                                                        unsigned* tile_counter, int* error) {
+    chain_wait();
     constexpr int kWarps = kThreads / 32;
     constexpr int kWarpSpan = kSortTile / kWarps;
     __shared__ unsigned wcount[kWarps][kRadix];
@@ -288,39 +368,37 @@ __global__ void __launch_bounds__(kThreads) k_onesweep(const Key* keys_in, const
             wcount[w][d] = total;
             total += c;
         }
-        unsigned long long* mine = lookback + static_cast<size_t>(tile) * kRadix + d;
+        unsigned* mine = lookback + static_cast<size_t>(tile) * kRadix + d;
         unsigned prefix = 0;
         if (tile == 0) {
             st_relaxed(mine, kTilePrefix | total);
         } else {
             st_relaxed(mine, kTileAggregate | total);
             // Walk back kLookbackBatch tiles at a time (their words are loaded together,
-            // so a long run of aggregates costs one load latency per batch): take every
+            // so a run of aggregates costs one load latency per batch): take every
             // published word up to the nearest inclusive prefix, and re-read from the
             // first word not yet published.
-            constexpr int kLookbackBatch = 8;
             int t = tile - 1;
             long long spins = 0;
             bool found = false;
             while (!found && t >= 0) {
-                unsigned long long w[kLookbackBatch];
+                unsigned w[kLookbackBatch];
 #pragma unroll
                 for (int j = 0; j < kLookbackBatch; ++j)
                     w[j] = t - j >= 0 ? ld_relaxed(lookback + static_cast<size_t>(t - j) * kRadix + d)
-                                      : 0ull;
+                                      : 0u;
                 int taken = 0;
                 bool blocked = false;
 #pragma unroll
                 for (int j = 0; j < kLookbackBatch; ++j) {
                     if (found || blocked || t - j < 0) continue;
-                    const unsigned long long state = w[j] & ~0xffffffffull;
-                    if (state == 0) {         // not published yet: resume at this tile
+                    if (w[j] == 0) {          // not published yet: resume at this tile
                         blocked = true;
                         continue;
                     }
-                    prefix += static_cast<unsigned>(w[j]);
+                    found = (w[j] & kTilePrefix) != 0;
+                    prefix += w[j] & (found ? ~kTilePrefix : ~kTileAggregate);
                     taken = j + 1;
-                    found = state == kTilePrefix;
                 }
                 t -= taken;
                 if (blocked && ++spins > kLookbackSpins) {
@@ -354,9 +432,9 @@ __global__ void __launch_bounds__(kThreads) k_sort_upsweep(const Key* keys, int 
     __shared__ unsigned counts[kRadix];
     counts[threadIdx.x] = 0;
     __syncthreads();
-    int base = blockIdx.x * kSortTile;
+    int base = blockIdx.x * kStaticTile;
 #pragma unroll 4
-    for (int j = 0; j < kSortItems; ++j) {
+    for (int j = 0; j < kStaticItems; ++j) {
         int idx = base + j * kThreads + threadIdx.x;
         bool valid = idx < n;
         unsigned d = valid ? digit_of(keys[idx], shift) : kRadix;
@@ -429,7 +507,7 @@ __global__ void __launch_bounds__(kThreads) k_sort_downsweep(const Key* keys_in,
                                                              const unsigned* scanned,
                                                              int tiles, int* error) {
     constexpr int kWarps = kThreads / 32;
-    constexpr int kWarpSpan = kSortTile / kWarps;
+    constexpr int kWarpSpan = kStaticTile / kWarps;
     __shared__ unsigned wcount[kWarps][kRadix];
     __shared__ unsigned gbase[kRadix];
     const int lane = threadIdx.x & 31;
@@ -439,12 +517,12 @@ __global__ void __launch_bounds__(kThreads) k_sort_downsweep(const Key* keys_in,
     __syncthreads();
 
     const unsigned lt = lanemask_lt();
-    const int base = blockIdx.x * kSortTile + warp * kWarpSpan;
-    Key k[kSortItems];
-    int v[kSortItems];
-    unsigned rank[kSortItems];
+    const int base = blockIdx.x * kStaticTile + warp * kWarpSpan;
+    Key k[kStaticItems];
+    int v[kStaticItems];
+    unsigned rank[kStaticItems];
 #pragma unroll
-    for (int j = 0; j < kSortItems; ++j) {
+    for (int j = 0; j < kStaticItems; ++j) {
         int idx = base + j * 32 + lane;
         bool valid = idx < n;
         k[j] = valid ? keys_in[idx] : Key(0);
@@ -469,7 +547,7 @@ __global__ void __launch_bounds__(kThreads) k_sort_downsweep(const Key* keys_in,
     }
     __syncthreads();
 #pragma unroll
-    for (int j = 0; j < kSortItems; ++j) {
+    for (int j = 0; j < kStaticItems; ++j) {
         if (rank[j] == 0xffffffffu) continue;
         unsigned d = digit_of(k[j], shift);
         unsigned pos = gbase[d] + wcount[warp][d] + rank[j];
@@ -508,6 +586,7 @@ template <typename Key>
 __global__ void __launch_bounds__(kThreads) k_karras(const Key* codes, int n, BvhNode* nodes,
                                                      int* node_parent, int* leaf_parent,
                                                      int4* node_info) {
+    chain_wait();
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n - 1) return;
     int first, last;
@@ -610,21 +689,30 @@ __global__ void __launch_bounds__(kClimbThreads) k_leaf_climb(const float* prims
                                                               const int4* node_info,
                                                               unsigned* flags, float* root,
                                                               int* error) {
-    __shared__ float sbox[kClimbThreads][2][6];
-    __shared__ unsigned sflag[kClimbThreads];
+    chain_wait();
+    // Per node of the block: each child's box (three float2) and an arrival counter, in
+    // dynamic shared memory (kClimbSmem bytes).
+    extern __shared__ float2 climb_smem[];
+    float2 (*sbox)[2][3] = reinterpret_cast<float2 (*)[2][3]>(climb_smem);
+    unsigned* sflag = reinterpret_cast<unsigned*>(climb_smem + 6 * kClimbThreads);
     const int lo = blockIdx.x * kClimbThreads;
     sflag[threadIdx.x] = 0;
     __syncthreads();
     int k = lo + threadIdx.x;
     if (k >= n) return;
-    int pid = sorted_ids[k];
+    // The leaf's id, its parent link and the parent's record are fetched before the
+    // primitive, so the two dependent chains overlap.
+    const int pid = sorted_ids[k];
+    int code = n > 1 ? leaf_parent[k] : -1;
+    int4 info = make_int4(0, -1, -1, 0);
+    if (code >= 0 && (code >> 1) < n - 1) info = node_info[code >> 1];
     if (pid < 0 || pid >= n) {  // cannot happen for a consistent sort
         atomicOr(error, kErrLoopBound);
         return;
     }
     f3 v0, v1, v2;
     box3 b;
-    load_prim<Kind>(prims, pid, v0, v1, v2, b);
+    load_prim_vec<Kind>(prims, n, pid, aligned16(prims), v0, v1, v2, b);
     if (Kind == LUX_PRIM_TRIANGLES) {
         TriRecord r;
         r.p0 = make_float4(v0.x, v0.y, v0.z, __int_as_float(pid));
@@ -637,23 +725,30 @@ __global__ void __launch_bounds__(kClimbThreads) k_leaf_climb(const float* prims
         root[3] = b.hi.x; root[4] = b.hi.y; root[5] = b.hi.z;
         return;
     }
-    int code = leaf_parent[k];
     for (int level = 0; level < kClimbBound; ++level) {
         int p = code >> 1;
         int slot = code & 1;
         if (code < 0 || p >= n - 1) break;  // parent links out of range: report below
-        const int4 info = node_info[p];
+        // The grandparent's record is requested now, before the hand-over, so its load
+        // overlaps this level's (for the half of the threads that go on).
+        const int up = info.z;
+        int4 next = make_int4(0, -1, -1, 0);
+        if (up >= 0 && (up >> 1) < n - 1) next = node_info[up >> 1];
         const int s = p - lo;
         if (info.x >= lo && info.y < lo + kClimbThreads && s >= 0 && s < kClimbThreads) {
-            volatile float* mine = &sbox[s][slot][0];
-            mine[0] = b.lo.x; mine[1] = b.lo.y; mine[2] = b.lo.z;
-            mine[3] = b.hi.x; mine[4] = b.hi.y; mine[5] = b.hi.z;
+            // The block fences order the box's stores before the counter's add, and the
+            // add before the sibling's box is read (they are also compiler barriers).
+            float2* mine = &sbox[s][slot][0];
+            mine[0] = make_float2(b.lo.x, b.lo.y);
+            mine[1] = make_float2(b.lo.z, b.hi.x);
+            mine[2] = make_float2(b.hi.y, b.hi.z);
             __threadfence_block();
             unsigned prior = atomicAdd(&sflag[s], 1u);
             if (prior == 0) return;  // the sibling finishes this node
             __threadfence_block();
-            volatile const float* o = &sbox[s][slot ^ 1][0];
-            box3 sib{make_f3(o[0], o[1], o[2]), make_f3(o[3], o[4], o[5])};
+            const float2* o = &sbox[s][slot ^ 1][0];
+            const float2 o0 = o[0], o1 = o[1], o2 = o[2];
+            box3 sib{make_f3(o0.x, o0.y, o1.x), make_f3(o1.y, o2.x, o2.y)};
             const box3 left = slot ? sib : b;
             const box3 right = slot ? b : sib;
             store_slot(nodes + p, 0, left);
@@ -672,7 +767,8 @@ __global__ void __launch_bounds__(kClimbThreads) k_leaf_climb(const float* prims
             root[3] = b.hi.x; root[4] = b.hi.y; root[5] = b.hi.z;
             return;
         }
-        code = info.z;
+        code = up;
+        info = next;
     }
     atomicOr(error, kErrClimbBound);
 }
@@ -708,6 +804,30 @@ __global__ void k_export(BvhView v, const Key* codes, unsigned long long* codes6
 
 int grid_for(int count, int threads = kThreads) { return (count + threads - 1) / threads; }
 
+// Launches one kernel of the build chain on ctx's stream, with programmatic dependent
+// launch when LUX_PDL is set (the kernels begin with chain_wait).
+template <typename... Params, typename... Args>
+cudaError_t chain_launch(lux_ctx* ctx, void (*kernel)(Params...), int grid, int block,
+                         size_t smem, Args... args) {
+    ctx->launches += 1;
+#if LUX_PDL
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(block);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = ctx->stream;
+    cudaLaunchAttribute attr{};
+    attr.id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr.val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = &attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, static_cast<Params>(args)...);
+#else
+    kernel<<<grid, block, smem, ctx->stream>>>(static_cast<Params>(args)...);
+    return cudaGetLastError();
+#endif
+}
+
 int stride_grid(const lux_ctx* ctx, int count) {
     return std::max(1, std::min(grid_for(count), ctx->sm_count * 8));
 }
@@ -726,7 +846,7 @@ SortScratch sort_scratch(int n, size_t key_size, int passes) {
     s.val_bytes = (static_cast<size_t>(n) * sizeof(int) + 255) & ~size_t(255);
     // hist[kMaxPasses * kRadix], tile counters[kMaxPasses] (padded), bases[...]
     s.counts_bytes = 2 * sizeof(unsigned) * kMaxPasses * kRadix + 256;
-    s.lookback_bytes = sizeof(unsigned long long) * kRadix * tiles * passes;
+    s.lookback_bytes = sizeof(unsigned) * kRadix * tiles * passes;
     return s;
 }
 
@@ -747,48 +867,58 @@ int morton_and_sort(lux_ctx* ctx, const float* prims, const unsigned* root_ord, 
     unsigned* hist = reinterpret_cast<unsigned*>(s + layout.key_bytes + layout.val_bytes);
     unsigned* bases = hist + kMaxPasses * kRadix;
     unsigned* counters = bases + kMaxPasses * kRadix;
-    auto* lookback = reinterpret_cast<unsigned long long*>(
+    auto* lookback = reinterpret_cast<unsigned*>(
         s + layout.key_bytes + layout.val_bytes + layout.counts_bytes);
-    // Counts, tile counters and look-back words start at zero.
-    cudaError_t err = cudaMemsetAsync(hist, 0, sizeof(unsigned) * kMaxPasses * kRadix,
-                                      ctx->stream);
-    if (err == cudaSuccess)
-        err = cudaMemsetAsync(counters, 0, 256 + layout.lookback_bytes, ctx->stream);
-    if (err != cudaSuccess) return cuda_fail(err, "sort scratch reset");
+    // Counts, tile counters and look-back words start at zero (reset by the caller
+    // before the chain's first kernel, reset_sort_scratch).
     const int hist_grid = std::max(1, std::min(grid_for(n), ctx->sm_count * 2));
-    k_morton_hist<Kind, Key, kPasses><<<hist_grid, kThreads, 0, ctx->stream>>>(
-        prims, n, root_ord, codes, hist);
-    k_digit_bases<<<kPasses, kRadix, 0, ctx->stream>>>(hist, bases);
-    ctx->launches += 2;
+    cudaError_t err = chain_launch(ctx, k_morton_hist<Kind, Key, kPasses>, hist_grid, kThreads,
+                                   0, prims, n, root_ord, codes, hist);
+    if (err == cudaSuccess) err = chain_launch(ctx, k_digit_bases, kPasses, kRadix, 0, hist, bases);
     Key* kin = codes;
     int* vin = vals;
     Key* kout = keys_alt;
     int* vout = vals_alt;
-    for (int p = 0; p < kPasses; ++p) {
-        unsigned long long* words = lookback + static_cast<size_t>(p) * tiles * kRadix;
-        if (p == 0) {
-            k_onesweep<Key, true><<<tiles, kThreads, 0, ctx->stream>>>(
-                kin, vin, kout, vout, n, 8 * p, bases + p * kRadix, words, counters + p,
-                ctx->d_error);
-        } else {
-            k_onesweep<Key, false><<<tiles, kThreads, 0, ctx->stream>>>(
-                kin, vin, kout, vout, n, 8 * p, bases + p * kRadix, words, counters + p,
-                ctx->d_error);
-        }
-        ctx->launches += 1;
+    for (int p = 0; p < kPasses && err == cudaSuccess; ++p) {
+        unsigned* words = lookback + static_cast<size_t>(p) * tiles * kRadix;
+        err = chain_launch(ctx, p == 0 ? k_onesweep<Key, true> : k_onesweep<Key, false>, tiles,
+                           kThreads, 0, kin, vin, kout, vout, n, 8 * p, bases + p * kRadix,
+                           words, counters + p, ctx->d_error);
         std::swap(kin, kout);
         std::swap(vin, vout);
     }
-    return cuda_fail(cudaGetLastError(), "radix sort");
+    return cuda_fail(err, "radix sort");
+}
+
+// Zeroes the sort's counts, tile counters and look-back words in ctx's scratch (laid out
+// as morton_and_sort lays it out); grows the scratch first.
+template <typename Key>
+int reset_sort_scratch(lux_ctx* ctx, int n) {
+    constexpr int kPasses = sizeof(Key) == 4 ? 4 : 8;
+    const SortScratch layout = sort_scratch(n, sizeof(Key), kPasses);
+    if (int st = ensure_scratch(ctx, layout.total())) return st;
+    char* s = static_cast<char*>(ctx->scratch);
+    unsigned* hist = reinterpret_cast<unsigned*>(s + layout.key_bytes + layout.val_bytes);
+    unsigned* counters = hist + 2 * kMaxPasses * kRadix;
+    cudaError_t err = cudaMemsetAsync(hist, 0, sizeof(unsigned) * kMaxPasses * kRadix,
+                                      ctx->stream);
+    if (err == cudaSuccess)
+        err = cudaMemsetAsync(counters, 0, 256 + layout.lookback_bytes, ctx->stream);
+    return err == cudaSuccess ? LUX_OK : cuda_fail(err, "sort scratch reset");
 }
 
 template <int Kind>
 int climb(lux_ctx* ctx, lux_bvh* bvh, const float* prims) {
-    k_leaf_climb<Kind><<<grid_for(bvh->n, kClimbThreads), kClimbThreads, 0, ctx->stream>>>(
-        prims, bvh->n, bvh->sorted_ids, bvh->tris, bvh->nodes, bvh->leaf_parent,
-        bvh->node_info, bvh->flags, bvh->root, ctx->d_error);
-    ctx->launches += 1;
-    return cuda_fail(cudaGetLastError(), "k_leaf_climb");
+    if (kClimbSmem > 48 * 1024) {
+        cudaError_t err = cudaFuncSetAttribute(
+            k_leaf_climb<Kind>, cudaFuncAttributeMaxDynamicSharedMemorySize, kClimbSmem);
+        if (err != cudaSuccess) return cuda_fail(err, "k_leaf_climb shared memory");
+    }
+    return cuda_fail(chain_launch(ctx, k_leaf_climb<Kind>, grid_for(bvh->n, kClimbThreads),
+                                  kClimbThreads, kClimbSmem, prims, bvh->n, bvh->sorted_ids,
+                                  bvh->tris, bvh->nodes, bvh->leaf_parent, bvh->node_info,
+                                  bvh->flags, bvh->root, ctx->d_error),
+                     "k_leaf_climb");
 }
 
 template <int Kind, typename Key>
@@ -796,20 +926,22 @@ int build_typed(lux_ctx* ctx, lux_bvh* bvh, const float* prims) {
     int n = bvh->n;
     Key* codes = static_cast<Key*>(bvh->codes);
     unsigned* root_ord = reinterpret_cast<unsigned*>(bvh->root + 8);
+    // Every reset first, so that the kernels follow one another directly.
     cudaError_t err = cudaMemsetAsync(root_ord, 0xff, 6 * sizeof(unsigned), ctx->stream);
+    if (err == cudaSuccess && n == 1)
+        // A lone leaf has no parent (the storage may hold a larger earlier tree).
+        err = cudaMemsetAsync(bvh->leaf_parent, 0xff, sizeof(int), ctx->stream);
     if (err != cudaSuccess) return cuda_fail(err, "memset root");
-    k_root_reduce<Kind><<<stride_grid(ctx, n), kThreads, 0, ctx->stream>>>(prims, n, root_ord);
-    ctx->launches += 1;
+    if (int st = reset_sort_scratch<Key>(ctx, n)) return st;
+    err = chain_launch(ctx, k_root_reduce<Kind>, stride_grid(ctx, n), kThreads, 0, prims, n,
+                       root_ord);
+    if (err != cudaSuccess) return cuda_fail(err, "k_root_reduce");
     int st = morton_and_sort<Kind, Key>(ctx, prims, root_ord, codes, bvh->sorted_ids, n);
     if (st) return st;
-    if (n == 1) {
-        // A lone leaf has no parent (the storage may hold a larger earlier tree).
-        cudaError_t e = cudaMemsetAsync(bvh->leaf_parent, 0xff, sizeof(int), ctx->stream);
-        if (e != cudaSuccess) return cuda_fail(e, "memset leaf parent");
-    } else {
-        k_karras<Key><<<grid_for(n - 1), kThreads, 0, ctx->stream>>>(
-            codes, n, bvh->nodes, bvh->node_parent, bvh->leaf_parent, bvh->node_info);
-        ctx->launches += 1;
+    if (n > 1) {
+        err = chain_launch(ctx, k_karras<Key>, grid_for(n - 1), kThreads, 0, codes, n, bvh->nodes,
+                           bvh->node_parent, bvh->leaf_parent, bvh->node_info);
+        if (err != cudaSuccess) return cuda_fail(err, "k_karras");
     }
     return climb<Kind>(ctx, bvh, prims);
 }
@@ -1084,7 +1216,7 @@ namespace lux {
 namespace {
 
 constexpr int kStaticMaxPrims = LUX_STATIC_SORT_MAX_PRIMS;
-constexpr int kStaticMaxTiles = (kStaticMaxPrims + kSortTile - 1) / kSortTile;
+constexpr int kStaticMaxTiles = (kStaticMaxPrims + kStaticTile - 1) / kStaticTile;
 constexpr size_t kStaticHeaderBytes = 256;
 constexpr size_t kStaticHistBytes = size_t(kRadix) * kStaticMaxTiles * sizeof(unsigned);
 constexpr size_t kStaticKeyBytes = size_t(kStaticMaxPrims) * 8;
@@ -1135,7 +1267,7 @@ int morton_sort_into(lux_ctx* ctx, const float* prims, int n, Key* keys, Key* ke
     k_root_reduce<Kind><<<stride_grid(ctx, n), kThreads, 0, stream>>>(prims, n, root_ord);
     k_morton<Kind, Key><<<stride_grid(ctx, n), kThreads, 0, stream>>>(prims, n, root_ord, keys);
     ctx->launches += 2;
-    const int tiles = grid_for(n, kSortTile);
+    const int tiles = grid_for(n, kStaticTile);
     int passes = (sizeof(Key) == 4 ? 30 + 7 : 63 + 7) / 8;
     if (passes & 1) ++passes;
     Key* kin = keys;

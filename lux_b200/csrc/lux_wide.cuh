@@ -40,6 +40,14 @@ LUX_D bool child_hit(const box3& b, const slab_ray& sr, const octant_ray& orr, f
     return sr.parallel == 0 ? octant_hit(orr, b, tmax, tn) : slab_hit(sr, b, tmax, tn);
 }
 
+// Byte c of a packed word as a float, exactly: the byte is placed in the mantissa of
+// 2^23 (one byte permute) and 2^23 subtracted, which is exact for values below 2^23.
+// Full-rate ALU work where an integer-to-float conversion would use the slower
+// conversion pipe (24 of them per node visit).
+LUX_D float byte_as_float(unsigned word, int c) {
+    return __fsub_rn(__uint_as_float(__byte_perm(word, 0x4B000000u, 0x7540u + c)), 8388608.0f);
+}
+
 // Hit mask of the node's decoded child boxes (bit c: child c) under t_max and each
 // child's entry t.  Decoded boxes contain the exact ones, so a child whose exact box
 // passes always passes here.
@@ -60,6 +68,29 @@ LUX_D unsigned wide_test(const WideNode& w, const slab_ray& sr, const octant_ray
     const unsigned lz = __float_as_uint(w.q1.z), hx = __float_as_uint(w.q1.w);
     const unsigned hy = __float_as_uint(w.q2.x), hz = __float_as_uint(w.q2.y);
     unsigned mask = 0;
+    if (sr.parallel == 0) {
+        // octant_hit on each decoded box, with its near / far choice made once per axis
+        // on the packed words (the same bytes, so the same decoded planes and t values).
+        const unsigned nxq = (orr.neg & 1u) ? hx : lx, fxq = (orr.neg & 1u) ? lx : hx;
+        const unsigned nyq = (orr.neg & 2u) ? hy : ly, fyq = (orr.neg & 2u) ? ly : hy;
+        const unsigned nzq = (orr.neg & 4u) ? hz : lz, fzq = (orr.neg & 4u) ? lz : hz;
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            const float nx = add(mul(byte_as_float(nxq, c), sx), w.q0.x);
+            const float fx = add(mul(byte_as_float(fxq, c), sx), w.q0.x);
+            const float ny = add(mul(byte_as_float(nyq, c), sy), w.q0.y);
+            const float fy = add(mul(byte_as_float(fyq, c), sy), w.q0.y);
+            const float nz = add(mul(byte_as_float(nzq, c), sz), w.q0.z);
+            const float fz = add(mul(byte_as_float(fzq, c), sz), w.q0.z);
+            const float t0x = mul(sub(nx, orr.o.x), orr.inv.x), t1x = mul(sub(fx, orr.o.x), orr.inv.x);
+            const float t0y = mul(sub(ny, orr.o.y), orr.inv.y), t1y = mul(sub(fy, orr.o.y), orr.inv.y);
+            const float t0z = mul(sub(nz, orr.o.z), orr.inv.z), t1z = mul(sub(fz, orr.o.z), orr.inv.z);
+            tn[c] = fmaxf(fmaxf(orr.tmin, t0x), fmaxf(t0y, t0z));
+            const float tf = fminf(fminf(tmax, t1x), fminf(t1y, t1z));
+            if (!(tn[c] > tf)) mask |= 1u << c;
+        }
+        return mask & live;
+    }
 #pragma unroll
     for (int c = 0; c < 4; ++c) {
         const int sh = 8 * c;
