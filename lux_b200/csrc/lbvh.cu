@@ -37,7 +37,7 @@ namespace {
 #define LUX_SORT_ITEMS 16
 #endif
 #ifndef LUX_CLIMB_THREADS
-#define LUX_CLIMB_THREADS 512
+#define LUX_CLIMB_THREADS 256
 #endif
 #ifndef LUX_LOOKBACK_BATCH
 #define LUX_LOOKBACK_BATCH 8
@@ -45,11 +45,15 @@ namespace {
 #ifndef LUX_PDL
 #define LUX_PDL 0
 #endif
+#ifndef LUX_SORT_THREADS
+#define LUX_SORT_THREADS 512
+#endif
 
 constexpr int kThreads = 256;
 constexpr int kRadix = 256;
 constexpr int kSortItems = LUX_SORT_ITEMS;
-constexpr int kSortTile = kThreads * kSortItems;  // keys per tile
+constexpr int kSortThreads = LUX_SORT_THREADS;      // threads of a k_onesweep block
+constexpr int kSortTile = kSortThreads * kSortItems;  // keys per tile
 // The allocation-free sort's tiles (its scratch size is part of the ABI): fixed.
 constexpr int kStaticItems = 16;
 constexpr int kStaticTile = kThreads * kStaticItems;
@@ -314,13 +318,15 @@ constexpr int kLookbackBatch = LUX_LOOKBACK_BATCH;   // earlier tiles' words loa
 // handed out before it (and so are running or done); each wait is bounded and a wait
 // that runs out reports through `error`.
 template <typename Key, bool First>
-__global__ void __launch_bounds__(kThreads) k_onesweep(const Key* keys_in, const int* vals_in,
-                                                       Key* keys_out, int* vals_out, int n,
-                                                       int shift, const unsigned* bases,
-                                                       unsigned* lookback,
-                                                       unsigned* tile_counter, int* error) {
+__global__ void __launch_bounds__(kSortThreads) k_onesweep(const Key* keys_in,
+                                                           const int* vals_in, Key* keys_out,
+                                                           int* vals_out, int n, int shift,
+                                                           const unsigned* bases,
+                                                           unsigned* lookback,
+                                                           unsigned* tile_counter, int* error) {
     chain_wait();
-    constexpr int kWarps = kThreads / 32;
+    static_assert(kSortThreads >= kRadix, "one thread per digit in the look-back");
+    constexpr int kWarps = kSortThreads / 32;
     constexpr int kWarpSpan = kSortTile / kWarps;
     __shared__ unsigned wcount[kWarps][kRadix];
     __shared__ unsigned gbase[kRadix];
@@ -328,7 +334,7 @@ __global__ void __launch_bounds__(kThreads) k_onesweep(const Key* keys_in, const
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
     if (threadIdx.x == 0) tile_s = static_cast<int>(atomicAdd(tile_counter, 1u));
-    for (int i = threadIdx.x; i < kWarps * kRadix; i += kThreads) (&wcount[0][0])[i] = 0;
+    for (int i = threadIdx.x; i < kWarps * kRadix; i += kSortThreads) (&wcount[0][0])[i] = 0;
     __syncthreads();
     const int tile = tile_s;
 
@@ -359,7 +365,7 @@ __global__ void __launch_bounds__(kThreads) k_onesweep(const Key* keys_in, const
         rank[j] = valid ? before + __popc(peers & lt) : 0xffffffffu;
     }
     __syncthreads();
-    {
+    if (threadIdx.x < kRadix) {
         const int d = threadIdx.x;
         unsigned total = 0;
 #pragma unroll
@@ -882,7 +888,7 @@ int morton_and_sort(lux_ctx* ctx, const float* prims, const unsigned* root_ord, 
     for (int p = 0; p < kPasses && err == cudaSuccess; ++p) {
         unsigned* words = lookback + static_cast<size_t>(p) * tiles * kRadix;
         err = chain_launch(ctx, p == 0 ? k_onesweep<Key, true> : k_onesweep<Key, false>, tiles,
-                           kThreads, 0, kin, vin, kout, vout, n, 8 * p, bases + p * kRadix,
+                           kSortThreads, 0, kin, vin, kout, vout, n, 8 * p, bases + p * kRadix,
                            words, counters + p, ctx->d_error);
         std::swap(kin, kout);
         std::swap(vin, vout);
