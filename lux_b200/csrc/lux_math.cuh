@@ -216,13 +216,20 @@ LUX_HD uint64_t spread21(uint64_t v) {
     return v;
 }
 
-// Normalised centroid offset inside the scene box (core/aabb.cuh:20, 74-81).
-LUX_HD f3 centroid_offset(const box3& b, const box3& root) {
-    f3 c = (b.lo + b.hi) * 0.5f;
+// Box centroid (core/aabb.cuh:20).
+LUX_HD f3 box_centroid(const box3& b) { return (b.lo + b.hi) * 0.5f; }
+
+// Normalised offset of centroid c inside the scene box (core/aabb.cuh:74-81).
+LUX_HD f3 centroid_offset_of(f3 c, const box3& root) {
     f3 d = root.hi - root.lo;
     return make_f3(d.x > 0 ? (c.x - root.lo.x) / d.x : 0.5f,
                    d.y > 0 ? (c.y - root.lo.y) / d.y : 0.5f,
                    d.z > 0 ? (c.z - root.lo.z) / d.z : 0.5f);
+}
+
+// Normalised centroid offset inside the scene box (core/aabb.cuh:20, 74-81).
+LUX_HD f3 centroid_offset(const box3& b, const box3& root) {
+    return centroid_offset_of(box_centroid(b), root);
 }
 
 // quantize_morton_coord (bvh/gpu_bvh.cu:61-64) with a general scale.
@@ -231,19 +238,22 @@ LUX_HD uint32_t quantize(float v, float scale, float maxv) {
     return static_cast<uint32_t>(v);
 }
 
-LUX_HD uint32_t morton30(const box3& b, const box3& root) {
-    f3 off = centroid_offset(b, root);
+LUX_HD uint32_t morton30_of(f3 centroid, const box3& root) {
+    f3 off = centroid_offset_of(centroid, root);
     return (spread10(quantize(off.x, 1024.0f, 1023.0f)) << 2)
          | (spread10(quantize(off.y, 1024.0f, 1023.0f)) << 1)
          | spread10(quantize(off.z, 1024.0f, 1023.0f));
 }
 
-LUX_HD uint64_t morton63(const box3& b, const box3& root) {
-    f3 off = centroid_offset(b, root);
+LUX_HD uint64_t morton63_of(f3 centroid, const box3& root) {
+    f3 off = centroid_offset_of(centroid, root);
     return (spread21(quantize(off.x, 2097152.0f, 2097151.0f)) << 2)
          | (spread21(quantize(off.y, 2097152.0f, 2097151.0f)) << 1)
          | spread21(quantize(off.z, 2097152.0f, 2097151.0f));
 }
+
+LUX_HD uint32_t morton30(const box3& b, const box3& root) { return morton30_of(box_centroid(b), root); }
+LUX_HD uint64_t morton63(const box3& b, const box3& root) { return morton63_of(box_centroid(b), root); }
 
 // Order-preserving float <-> uint32 map for atomicMin/atomicMax reductions.
 LUX_HD uint32_t float_to_ordered(float f) {
