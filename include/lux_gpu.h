@@ -223,7 +223,7 @@ int lux_bvh_validate_primitives(lux_ctx* ctx, const lux_bvh* bvh, const float* p
  * LUX_ERR_INVALID_ARGUMENT.
  * The first call on a device looks up the array's device address for that device (and,
  * with lazy module loading, may be the call that loads the library's kernels on it, which
- * is when the array's memory is taken); make that first call before any stream capture.
+ * is when the array's memory is taken).
  * The address is kept for the life of the process, so the library does not support a
  * cudaDeviceReset of that device while it is loaded.  Each call waits for its stream and
  * reports device checks.  All calls on one device share the one array and each call overwrites
