@@ -37,11 +37,24 @@ constexpr int kSlots = 9;  // per-bounce counters: ray, 5 material queues, shado
 // counters are allocated once per runtime and a deeper request never reallocates.
 constexpr int kMaxDepthSlots = 1000 + 2;
 
+// Batches of one render run on two lanes, each with its own path pool, counters and
+// stream (the context's, and one of the runtime's own): while one batch's last bounces
+// drain (few paths, long walks, most SMs idle) the next batch's first bounces fill the
+// GPU.  Each batch's film accumulation waits for the previous batch's, so the film sums
+// in the same sample order as with one lane.
+#ifndef LUX_RENDER_LANES
+#define LUX_RENDER_LANES 2
+#endif
+constexpr int kRenderLanes = LUX_RENDER_LANES;
+
 struct Runtime {
-    PathPool pool;
-    int* counts = nullptr;               // kMaxDepthSlots * kSlots
+    PathPool pool[kRenderLanes];
+    int* counts[kRenderLanes] = {};      // kMaxDepthSlots * kSlots per lane
     unsigned long long* rays = nullptr;  // [0] camera + extension, [1] shadow segments
     long long last_counts[2] = {0, 0};
+    int lanes = 0;                       // lanes allocated
+    cudaStream_t lane_stream = nullptr;  // the second lane's stream
+    cudaEvent_t ev_setup = nullptr, ev_end = nullptr, ev_flush[2] = {nullptr, nullptr};
 };
 
 struct Batch {
@@ -276,9 +289,14 @@ __global__ void k_count_rays(const int* counts, unsigned long long* rays, int de
 Runtime* runtime_of(lux_ctx* ctx) { return static_cast<Runtime*>(ctx->render_runtime); }
 
 void runtime_release(Runtime* rt) {
-    path_pool_free(rt->pool);
-    if (rt->counts) cudaFree(rt->counts);
+    for (int l = 0; l < kRenderLanes; ++l) {
+        path_pool_free(rt->pool[l]);
+        if (rt->counts[l]) cudaFree(rt->counts[l]);
+    }
     if (rt->rays) cudaFree(rt->rays);
+    for (cudaEvent_t e : {rt->ev_setup, rt->ev_end, rt->ev_flush[0], rt->ev_flush[1]})
+        if (e) cudaEventDestroy(e);
+    if (rt->lane_stream) cudaStreamDestroy(rt->lane_stream);
     long long keep[2] = {rt->last_counts[0], rt->last_counts[1]};
     *rt = Runtime{};
     rt->last_counts[0] = keep[0];
@@ -325,10 +343,11 @@ int path_pool_alloc(PathPool& p, int capacity) {
 
 namespace {
 
-// Grows the path pool to at least `capacity` paths (never shrinks it); the counters are
-// allocated once.  Only a larger batch than any before it reallocates, so a stream of
-// renders of mixed depth and size sized for its largest batch allocates nothing.
-int runtime_reserve(lux_ctx* ctx, int capacity, int max_depth) {
+// Grows the path pools to at least `capacity` paths and `lanes` lanes (never shrinks
+// them); the counters are allocated once.  Only a larger batch than any before it (or a
+// first render with two lanes) reallocates, so a stream of renders of mixed depth and size
+// sized for its largest batch allocates nothing.
+int runtime_reserve(lux_ctx* ctx, int capacity, int max_depth, int lanes) {
     Runtime* rt = runtime_of(ctx);
     if (!rt) {
         rt = new (std::nothrow) Runtime();
@@ -337,13 +356,23 @@ int runtime_reserve(lux_ctx* ctx, int capacity, int max_depth) {
     }
     if (max_depth + 2 > kMaxDepthSlots)
         return fail(LUX_ERR_INVALID_ARGUMENT, "max_depth must be in 0..1000");
-    if (rt->pool.capacity >= capacity && rt->counts && rt->rays) return LUX_OK;
+    if (rt->pool[0].capacity >= capacity && rt->lanes >= lanes && rt->rays) return LUX_OK;
+    lanes = std::max(lanes, rt->lanes);
     cudaStreamSynchronize(ctx->stream);
+    if (rt->lane_stream) cudaStreamSynchronize(rt->lane_stream);
     runtime_release(rt);
-    int st = path_pool_alloc(rt->pool, capacity);
+    int st = LUX_OK;
     cudaError_t err = cudaSuccess;
-    if (!st) err = cudaMalloc(&rt->counts, sizeof(int) * kSlots * kMaxDepthSlots);
+    for (int l = 0; l < lanes && !st && err == cudaSuccess; ++l) {
+        st = path_pool_alloc(rt->pool[l], capacity);
+        if (!st) err = cudaMalloc(&rt->counts[l], sizeof(int) * kSlots * kMaxDepthSlots);
+    }
     if (!st && err == cudaSuccess) err = cudaMalloc(&rt->rays, 16);
+    if (!st && err == cudaSuccess && lanes > 1) {
+        err = cudaStreamCreateWithFlags(&rt->lane_stream, cudaStreamNonBlocking);
+        for (cudaEvent_t* e : {&rt->ev_setup, &rt->ev_end, &rt->ev_flush[0], &rt->ev_flush[1]})
+            if (err == cudaSuccess) err = cudaEventCreateWithFlags(e, cudaEventDisableTiming);
+    }
     if (!st && err != cudaSuccess) {
         cudaGetLastError();
         st = fail(LUX_ERR_OUT_OF_MEMORY, "wavefront runtime allocation failed");
@@ -352,6 +381,7 @@ int runtime_reserve(lux_ctx* ctx, int capacity, int max_depth) {
         runtime_release(rt);
         return st;
     }
+    rt->lanes = lanes;
     return LUX_OK;
 }
 
@@ -408,11 +438,18 @@ int render(lux_ctx* ctx, const lux_scene* scene, const lux_render_request& req, 
                                ? pixels : std::min(pixels, batch_cap);
     int capacity = static_cast<int>(std::min<long long>(
         total_paths, static_cast<long long>(pixels_per_batch) * samples_per_batch));
-    int st = runtime_reserve(ctx, std::max(capacity, 1), req.max_depth);
+    // Two lanes when there is more than one batch; one for the debug outputs, whose
+    // atomically indexed records and sums keep the one-lane order.
+    const long long batches =
+        ((req.spp + samples_per_batch - 1) / samples_per_batch) *
+        static_cast<long long>((pixels + pixels_per_batch - 1) / std::max(pixels_per_batch, 1));
+    const int lanes = !with_aov && batches > 1 ? kRenderLanes : 1;
+    int st = runtime_reserve(ctx, std::max(capacity, 1), req.max_depth, lanes);
     if (st) return st;
     Runtime& rt = *runtime_of(ctx);
     const SceneView& sc = scene->view;
-    cudaStream_t s = ctx->stream;
+    cudaStream_t s0 = ctx->stream;
+    cudaStream_t s = s0;
     int grid = ctx->sm_count * 8;
     // Persistent grids of the refilling kernels: blocks per SM up to what fits, or the
     // context's LUX_OPT_REFILL_BLOCKS when it asks for fewer.
@@ -434,62 +471,87 @@ int render(lux_ctx* ctx, const lux_scene* scene, const lux_render_request& req, 
         err = cudaMemsetAsync(log_count, 0, sizeof(unsigned long long), s);
     if (walk_counts && err == cudaSuccess)
         err = cudaMemsetAsync(walk_counts, 0, 3 * sizeof(unsigned long long), s);
+    if (lanes > 1 && err == cudaSuccess) {
+        // The second lane starts after the setup.
+        err = cudaEventRecord(rt.ev_setup, s0);
+        if (err == cudaSuccess) err = cudaStreamWaitEvent(rt.lane_stream, rt.ev_setup, 0);
+    }
     if (err != cudaSuccess) return cuda_fail(err, "render setup");
-    for (int s0 = 0; s0 < req.spp; s0 += samples_per_batch) {
-        int ns = std::min(samples_per_batch, req.spp - s0);
-        for (int p0 = 0; p0 < pixels; p0 += pixels_per_batch) {
+    // A failure after the second lane started waits for that lane before returning, so
+    // no kernel of this render is left running on the runtime's buffers.
+    auto lane_fail = [&](cudaError_t e, const char* what) {
+        if (lanes > 1) cudaStreamSynchronize(rt.lane_stream);
+        return cuda_fail(e, what);
+    };
+    long long k = 0;   // batch index
+    for (int sa = 0; sa < req.spp; sa += samples_per_batch) {
+        int ns = std::min(samples_per_batch, req.spp - sa);
+        for (int p0 = 0; p0 < pixels; p0 += pixels_per_batch, ++k) {
+            const int lane = static_cast<int>(k % lanes);
+            s = lane ? rt.lane_stream : s0;
+            const PathPool& pool = rt.pool[lane];
+            int* counts = rt.counts[lane];
             Batch b;
             b.pixel0 = p0;
             b.pixels = std::min(pixels_per_batch, pixels - p0);
-            b.sample0 = s0;
+            b.sample0 = sa;
             b.samples = ns;
             b.cam = CameraParams{req.width, req.height, req.seed, req.frame_index, req.sample_offset};
-            err = cudaMemsetAsync(rt.counts, 0, sizeof(int) * kSlots * (req.max_depth + 2), s);
-            if (err != cudaSuccess) return cuda_fail(err, "counter reset");
-            k_camera<<<grid, kThreads, 0, s>>>(rt.pool, rt.counts, sc, b);
+            err = cudaMemsetAsync(counts, 0, sizeof(int) * kSlots * (req.max_depth + 2), s);
+            if (err != cudaSuccess) return lane_fail(err, "counter reset");
+            k_camera<<<grid, kThreads, 0, s>>>(pool, counts, sc, b);
             ctx->launches += 1;
             for (int d = 0; d <= req.max_depth; ++d) {
                 if (with_aov) {
-                    k_extend_aov<<<grid, kThreads, 0, s>>>(rt.pool, rt.counts, sc,
+                    k_extend_aov<<<grid, kThreads, 0, s>>>(pool, counts, sc,
                                                            req.light_sampler, d, ctx->d_error, aov);
-                    k_shade_aov<<<grid, kThreads, 0, s>>>(rt.pool, rt.counts, sc,
+                    k_shade_aov<<<grid, kThreads, 0, s>>>(pool, counts, sc,
                                                           req.light_sampler, d, req.max_depth, aov);
-                    k_shadow_aov<<<grid, kThreads, 0, s>>>(rt.pool, rt.counts, rt.rays, sc, d,
+                    k_shadow_aov<<<grid, kThreads, 0, s>>>(pool, counts, rt.rays, sc, d,
                                                            ctx->d_error, aov);
                     ctx->launches += 3;
                     continue;
                 }
                 if (ctx->trace_variant == kTraceStatic) {
-                    k_extend<<<grid, kThreads, 0, s>>>(rt.pool, rt.counts, sc, req.light_sampler,
+                    k_extend<<<grid, kThreads, 0, s>>>(pool, counts, sc, req.light_sampler,
                                                        d, ctx->d_error);
                 } else {
                     k_extend_refill<<<refill_grid, kThreads, 0, s>>>(
-                        rt.pool, rt.counts, sc, req.light_sampler, d, ctx->path_budget,
+                        pool, counts, sc, req.light_sampler, d, ctx->path_budget,
                         ctx->d_error);
                 }
-                k_shade<<<grid, kThreads, 0, s>>>(rt.pool, rt.counts, sc, req.light_sampler, d,
+                k_shade<<<grid, kThreads, 0, s>>>(pool, counts, sc, req.light_sampler, d,
                                                   req.max_depth);
                 if (ctx->trace_variant == kTraceStatic) {
-                    k_shadow<<<grid, kThreads, 0, s>>>(rt.pool, rt.counts, rt.rays, sc, d,
+                    k_shadow<<<grid, kThreads, 0, s>>>(pool, counts, rt.rays, sc, d,
                                                        ctx->d_error);
                 } else {
                     k_shadow_refill<<<shadow_grid, kThreads, 0, s>>>(
-                        rt.pool, rt.counts, rt.rays, sc, d, ctx->path_budget, ctx->d_error);
+                        pool, counts, rt.rays, sc, d, ctx->path_budget, ctx->d_error);
                 }
                 ctx->launches += 3;
             }
-            k_count_rays<<<1, 1, 0, s>>>(rt.counts, rt.rays, req.max_depth + 1);
+            k_count_rays<<<1, 1, 0, s>>>(counts, rt.rays, req.max_depth + 1);
             int fgrid = std::max(1, std::min(grid, (b.pixels + kThreads - 1) / kThreads));
-            k_flush<<<fgrid, kThreads, 0, s>>>(rt.pool, b, per_sample ? nullptr : out,
+            // The film takes the batches in order: this flush follows the previous one.
+            if (lanes > 1 && k > 0) err = cudaStreamWaitEvent(s, rt.ev_flush[lane ^ 1], 0);
+            k_flush<<<fgrid, kThreads, 0, s>>>(pool, b, per_sample ? nullptr : out,
                                                per_sample ? out : nullptr, req.spp);
             ctx->launches += 2;
-            err = cudaGetLastError();
-            if (err != cudaSuccess) return cuda_fail(err, "render launch");
+            if (lanes > 1 && err == cudaSuccess) err = cudaEventRecord(rt.ev_flush[lane], s);
+            if (err == cudaSuccess) err = cudaGetLastError();
+            if (err != cudaSuccess) return lane_fail(err, "render launch");
         }
     }
+    if (lanes > 1) {
+        // The caller's stream waits for the second lane.
+        err = cudaEventRecord(rt.ev_end, rt.lane_stream);
+        if (err == cudaSuccess) err = cudaStreamWaitEvent(s0, rt.ev_end, 0);
+        if (err != cudaSuccess) return cuda_fail(err, "render lanes");
+    }
     unsigned long long counts[2];
-    err = cudaMemcpyAsync(counts, rt.rays, 16, cudaMemcpyDeviceToHost, s);
-    if (err == cudaSuccess) err = cudaStreamSynchronize(s);
+    err = cudaMemcpyAsync(counts, rt.rays, 16, cudaMemcpyDeviceToHost, s0);
+    if (err == cudaSuccess) err = cudaStreamSynchronize(s0);
     if (err != cudaSuccess) return cuda_fail(err, "render");
     rt.last_counts[0] = static_cast<long long>(counts[0]);
     rt.last_counts[1] = static_cast<long long>(counts[1]);
