@@ -37,13 +37,13 @@ constexpr int kSlots = 9;  // per-bounce counters: ray, 5 material queues, shado
 // counters are allocated once per runtime and a deeper request never reallocates.
 constexpr int kMaxDepthSlots = 1000 + 2;
 
-// Batches of one render run on two lanes, each with its own path pool, counters and
-// stream (the context's, and one of the runtime's own): while one batch's last bounces
-// drain (few paths, long walks, most SMs idle) the next batch's first bounces fill the
-// GPU.  Each batch's film accumulation waits for the previous batch's, so the film sums
-// in the same sample order as with one lane.
+// Batches of one render run on kRenderLanes lanes in turn, each with its own path pool,
+// counters and stream (lane 0 the context's, the others the runtime's own): while one
+// batch's last bounces drain (few paths, long walks, most SMs idle) the next batch's
+// first bounces fill the GPU.  Each batch's film accumulation waits for the previous
+// batch's, so the film sums in the same sample order as with one lane.
 #ifndef LUX_RENDER_LANES
-#define LUX_RENDER_LANES 2
+#define LUX_RENDER_LANES 4
 #endif
 constexpr int kRenderLanes = LUX_RENDER_LANES;
 
@@ -53,8 +53,10 @@ struct Runtime {
     unsigned long long* rays = nullptr;  // [0] camera + extension, [1] shadow segments
     long long last_counts[2] = {0, 0};
     int lanes = 0;                       // lanes allocated
-    cudaStream_t lane_stream = nullptr;  // the second lane's stream
-    cudaEvent_t ev_setup = nullptr, ev_end = nullptr, ev_flush[2] = {nullptr, nullptr};
+    cudaStream_t stream[kRenderLanes] = {};   // lanes 1.. (lane 0 runs on the context's)
+    cudaEvent_t ev_setup = nullptr;
+    cudaEvent_t ev_end[kRenderLanes] = {};
+    cudaEvent_t ev_flush[kRenderLanes] = {};
 };
 
 struct Batch {
@@ -294,9 +296,12 @@ void runtime_release(Runtime* rt) {
         if (rt->counts[l]) cudaFree(rt->counts[l]);
     }
     if (rt->rays) cudaFree(rt->rays);
-    for (cudaEvent_t e : {rt->ev_setup, rt->ev_end, rt->ev_flush[0], rt->ev_flush[1]})
-        if (e) cudaEventDestroy(e);
-    if (rt->lane_stream) cudaStreamDestroy(rt->lane_stream);
+    if (rt->ev_setup) cudaEventDestroy(rt->ev_setup);
+    for (int l = 0; l < kRenderLanes; ++l) {
+        if (rt->ev_end[l]) cudaEventDestroy(rt->ev_end[l]);
+        if (rt->ev_flush[l]) cudaEventDestroy(rt->ev_flush[l]);
+        if (rt->stream[l]) cudaStreamDestroy(rt->stream[l]);
+    }
     long long keep[2] = {rt->last_counts[0], rt->last_counts[1]};
     *rt = Runtime{};
     rt->last_counts[0] = keep[0];
@@ -359,7 +364,8 @@ int runtime_reserve(lux_ctx* ctx, int capacity, int max_depth, int lanes) {
     if (rt->pool[0].capacity >= capacity && rt->lanes >= lanes && rt->rays) return LUX_OK;
     lanes = std::max(lanes, rt->lanes);
     cudaStreamSynchronize(ctx->stream);
-    if (rt->lane_stream) cudaStreamSynchronize(rt->lane_stream);
+    for (int l = 1; l < kRenderLanes; ++l)
+        if (rt->stream[l]) cudaStreamSynchronize(rt->stream[l]);
     runtime_release(rt);
     int st = LUX_OK;
     cudaError_t err = cudaSuccess;
@@ -369,9 +375,12 @@ int runtime_reserve(lux_ctx* ctx, int capacity, int max_depth, int lanes) {
     }
     if (!st && err == cudaSuccess) err = cudaMalloc(&rt->rays, 16);
     if (!st && err == cudaSuccess && lanes > 1) {
-        err = cudaStreamCreateWithFlags(&rt->lane_stream, cudaStreamNonBlocking);
-        for (cudaEvent_t* e : {&rt->ev_setup, &rt->ev_end, &rt->ev_flush[0], &rt->ev_flush[1]})
-            if (err == cudaSuccess) err = cudaEventCreateWithFlags(e, cudaEventDisableTiming);
+        err = cudaEventCreateWithFlags(&rt->ev_setup, cudaEventDisableTiming);
+        for (int l = 0; l < lanes && err == cudaSuccess; ++l) {
+            if (l > 0) err = cudaStreamCreateWithFlags(&rt->stream[l], cudaStreamNonBlocking);
+            if (err == cudaSuccess) err = cudaEventCreateWithFlags(&rt->ev_end[l], cudaEventDisableTiming);
+            if (err == cudaSuccess) err = cudaEventCreateWithFlags(&rt->ev_flush[l], cudaEventDisableTiming);
+        }
     }
     if (!st && err != cudaSuccess) {
         cudaGetLastError();
@@ -438,12 +447,13 @@ int render(lux_ctx* ctx, const lux_scene* scene, const lux_render_request& req, 
                                ? pixels : std::min(pixels, batch_cap);
     int capacity = static_cast<int>(std::min<long long>(
         total_paths, static_cast<long long>(pixels_per_batch) * samples_per_batch));
-    // Two lanes when there is more than one batch; one for the debug outputs, whose
-    // atomically indexed records and sums keep the one-lane order.
+    // Up to kRenderLanes lanes when there is more than one batch; one for the debug
+    // outputs, whose atomically indexed records and sums keep the one-lane order.
     const long long batches =
         ((req.spp + samples_per_batch - 1) / samples_per_batch) *
         static_cast<long long>((pixels + pixels_per_batch - 1) / std::max(pixels_per_batch, 1));
-    const int lanes = !with_aov && batches > 1 ? kRenderLanes : 1;
+    const int lanes =
+        !with_aov && batches > 1 ? static_cast<int>(std::min<long long>(kRenderLanes, batches)) : 1;
     int st = runtime_reserve(ctx, std::max(capacity, 1), req.max_depth, lanes);
     if (st) return st;
     Runtime& rt = *runtime_of(ctx);
@@ -472,15 +482,16 @@ int render(lux_ctx* ctx, const lux_scene* scene, const lux_render_request& req, 
     if (walk_counts && err == cudaSuccess)
         err = cudaMemsetAsync(walk_counts, 0, 3 * sizeof(unsigned long long), s);
     if (lanes > 1 && err == cudaSuccess) {
-        // The second lane starts after the setup.
+        // The other lanes start after the setup.
         err = cudaEventRecord(rt.ev_setup, s0);
-        if (err == cudaSuccess) err = cudaStreamWaitEvent(rt.lane_stream, rt.ev_setup, 0);
+        for (int l = 1; l < lanes && err == cudaSuccess; ++l)
+            err = cudaStreamWaitEvent(rt.stream[l], rt.ev_setup, 0);
     }
     if (err != cudaSuccess) return cuda_fail(err, "render setup");
     // A failure after the second lane started waits for that lane before returning, so
     // no kernel of this render is left running on the runtime's buffers.
     auto lane_fail = [&](cudaError_t e, const char* what) {
-        if (lanes > 1) cudaStreamSynchronize(rt.lane_stream);
+        for (int l = 1; l < lanes; ++l) cudaStreamSynchronize(rt.stream[l]);
         return cuda_fail(e, what);
     };
     long long k = 0;   // batch index
@@ -488,7 +499,7 @@ int render(lux_ctx* ctx, const lux_scene* scene, const lux_render_request& req, 
         int ns = std::min(samples_per_batch, req.spp - sa);
         for (int p0 = 0; p0 < pixels; p0 += pixels_per_batch, ++k) {
             const int lane = static_cast<int>(k % lanes);
-            s = lane ? rt.lane_stream : s0;
+            s = lane ? rt.stream[lane] : s0;
             const PathPool& pool = rt.pool[lane];
             int* counts = rt.counts[lane];
             Batch b;
@@ -534,7 +545,8 @@ int render(lux_ctx* ctx, const lux_scene* scene, const lux_render_request& req, 
             k_count_rays<<<1, 1, 0, s>>>(counts, rt.rays, req.max_depth + 1);
             int fgrid = std::max(1, std::min(grid, (b.pixels + kThreads - 1) / kThreads));
             // The film takes the batches in order: this flush follows the previous one.
-            if (lanes > 1 && k > 0) err = cudaStreamWaitEvent(s, rt.ev_flush[lane ^ 1], 0);
+            if (lanes > 1 && k > 0)
+                err = cudaStreamWaitEvent(s, rt.ev_flush[(lane + lanes - 1) % lanes], 0);
             k_flush<<<fgrid, kThreads, 0, s>>>(pool, b, per_sample ? nullptr : out,
                                                per_sample ? out : nullptr, req.spp);
             ctx->launches += 2;
@@ -543,10 +555,10 @@ int render(lux_ctx* ctx, const lux_scene* scene, const lux_render_request& req, 
             if (err != cudaSuccess) return lane_fail(err, "render launch");
         }
     }
-    if (lanes > 1) {
-        // The caller's stream waits for the second lane.
-        err = cudaEventRecord(rt.ev_end, rt.lane_stream);
-        if (err == cudaSuccess) err = cudaStreamWaitEvent(s0, rt.ev_end, 0);
+    for (int l = 1; l < lanes; ++l) {
+        // The caller's stream waits for the other lanes.
+        err = cudaEventRecord(rt.ev_end[l], rt.stream[l]);
+        if (err == cudaSuccess) err = cudaStreamWaitEvent(s0, rt.ev_end[l], 0);
         if (err != cudaSuccess) return cuda_fail(err, "render lanes");
     }
     unsigned long long counts[2];
