@@ -278,6 +278,10 @@ LUX_D SceneHit scene_closest(const SceneView& sc, f3 o, f3 d, float tmin, float 
 // best hit after each are those of scene_closest / blas_closest above and the result is
 // the same.  The stacks live apart from the scalar state, which then stays in registers.
 constexpr int kWideBlasStack = 96;   // three deferred children per 4-wide level
+#ifndef LUX_SKIP_FINISH
+#define LUX_SKIP_FINISH 1
+#endif
+constexpr bool kSkipIdleFinish = LUX_SKIP_FINISH != 0;
 struct WalkStacks {  // deferred (node ref, entry t bits), TLAS and BLAS
     int2 t[kStack];
     int2 b[kWideBlasStack];
@@ -1067,13 +1071,13 @@ LUX_D int extend_path(const PathPool& rt, const SceneView& sc, int sampler, int 
 }
 
 // Closest hits of the paths in queue q[0, n) (q null: paths 0..n-1) by persistent warps:
-// each lane advances its
-// walk by at most `budget` steps per round, and lanes whose walk finished hand it to
-// finish() and take the next path through one warp-aggregated atomic on *next_item, so
-// lanes do not idle behind the longest walk of a static warp.  tag_of(p) picks a path's
-// scene once (view(tag) returns it); finish(p, hit) is called by every lane of the warp
-// each round, with p = -1 for lanes that did not finish, so it may append to queues
-// with warp-collective operations.
+// each lane advances its walk by at most `budget` steps per round, and lanes whose walk
+// finished hand it to finish() and take the next path through one warp-aggregated
+// atomic on *next_item, so lanes do not idle behind the longest walk of a static warp.
+// tag_of(p) picks a path's scene once (view(tag) returns it); finish(p, hit) is called by
+// every lane of the warp after each round in which some lane finished, with p = -1 for
+// lanes that did not, so it may append to queues with warp-collective operations (and
+// must do nothing for p = -1).
 template <typename TagOf, typename View, typename Finish>
 LUX_D void refill_walks(const PathPool& rt, const int* q, int n, int* next_item, int budget,
                         int* error, TagOf tag_of, View view, Finish finish) {
@@ -1110,9 +1114,13 @@ LUX_D void refill_walks(const PathPool& rt, const int* q, int n, int* next_item,
             const SceneView& sc = view(tag);
             for (int s = 0; s < budget && !finished; ++s) finished = w.step(sc, stacks, error);
         }
-        SceneHit h = w.hit;
-        if (h.prim < 0) h.t = INFINITY;
-        finish(finished ? p : -1, tag, h);
+        // finish() is warp-collective and does nothing for lanes that did not finish, so
+        // a round in which no lane finished skips it.
+        if (!kSkipIdleFinish || __any_sync(0xffffffffu, finished)) {
+            SceneHit h = w.hit;
+            if (h.prim < 0) h.t = INFINITY;
+            finish(finished ? p : -1, tag, h);
+        }
         if (finished) p = -1;
     }
 }
