@@ -294,12 +294,12 @@ struct TwoLevelWalk {
     SceneHit hit;                 // best so far (hit.t is the current bound)
     int ign_instance, ign_local;
     int t_cur, t_sp;
-    long long t_steps;
+    unsigned t_steps;             // steps of the walk (bounded by 2n + 64 per level)
     bool in_blas;
     const WideNode* b_wide;
     const TriRecord* b_tris;
     int b_n, b_cur, b_sp, b_ignored, b_first;
-    long long b_steps;
+    unsigned b_steps;
     f3 lo, ld;
     slab_ray lsr;
     unsigned lneg;                // octant of the object-space ray (octant_ray::neg)
@@ -370,7 +370,8 @@ struct TwoLevelWalk {
         if (done) return true;
         const BvhView& tl = sc.tlas;
         if (in_blas) {
-            if (++b_steps > 2ll * b_n + 64 || b_cur >= b_n - 1 || ~b_cur >= b_n) {
+            if (++b_steps > 2u * static_cast<unsigned>(b_n) + 64u || b_cur >= b_n - 1 ||
+                ~b_cur >= b_n) {
                 fail(error, kErrLoopBound, INFINITY);
                 return true;
             }
@@ -426,7 +427,8 @@ struct TwoLevelWalk {
             }
             return done;
         }
-        if (++t_steps > 2ll * tl.n + 64 || t_cur >= tl.n - 1 || ~t_cur >= tl.n) {
+        if (++t_steps > 2u * static_cast<unsigned>(tl.n) + 64u || t_cur >= tl.n - 1 ||
+            ~t_cur >= tl.n) {
             fail(error, kErrLoopBound, INFINITY);
             return true;
         }

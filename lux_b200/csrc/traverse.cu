@@ -182,7 +182,7 @@ __global__ void __launch_bounds__(kTraceThreads) k_trace_persistent(
     const unsigned lane = threadIdx.x & 31;
     const unsigned lt = lanemask_lt_u();
     const box3 root = load_root(bvh.root);
-    const long long bound = 2ll * bvh.n + 64;
+    const unsigned bound = 2u * static_cast<unsigned>(bvh.n) + 64u;  // n <= 2^30
 
     int ray_idx = -1;   // >= 0 active ray, -1 needs a ray, -2 no rays left
     ray3 ray;
@@ -193,7 +193,7 @@ __global__ void __launch_bounds__(kTraceThreads) k_trace_persistent(
     int best_k = -1;
     int cur = 0;
     int sp = 0;
-    long long steps = 0;
+    unsigned steps = 0;
     bool root_missed = false;
     int stack_h[kStack];
     float stack_t[kStack];
@@ -331,7 +331,7 @@ __global__ void __launch_bounds__(kTraceThreads, 10) k_trace_wide_persistent(
     const unsigned lane = threadIdx.x & 31;
     const unsigned lt = lanemask_lt_u();
     const box3 root = load_root(bvh.root);
-    const long long bound = 2ll * bvh.n + 64;
+    const unsigned bound = 2u * static_cast<unsigned>(bvh.n) + 64u;  // n <= 2^30
 
     int ray_idx = -1;   // >= 0 active ray, -1 needs a ray, -2 no rays left
     ray3 ray;
@@ -341,7 +341,7 @@ __global__ void __launch_bounds__(kTraceThreads, 10) k_trace_wide_persistent(
     int best_k = -1;
     int cur = 0;
     int sp = 0;
-    long long steps = 0;
+    unsigned steps = 0;
     bool root_missed = false;
     int2 stack[kWideStack];  // (node ref, entry t bits): one 8-byte access per entry
 
