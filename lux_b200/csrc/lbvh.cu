@@ -1077,31 +1077,46 @@ struct WideSlots {
 
 // Biased exponent of an axis grid: from 2^e >= extent / 255, raised until the top grid
 // point decodes at or above hi.
-LUX_D unsigned wide_exponent(float origin, float hi) {
-    float extent = sub(hi, origin);
+// Grid of one axis of a wide node whose children span [origin, hi] (the node's box):
+// the smallest exponent e (biased into *biased) for which the grid's points k * 2^e,
+// k = floor(origin / 2^e) with |k| <= 2^22, reach hi within 255 steps; *c = (k - 2^23) * 2^e
+// (exact).  False when no exponent up to 103 does (the node is then left unbounded).
+LUX_D bool wide_axis(float origin, float hi, unsigned* biased, float* c) {
+    const float extent = sub(hi, origin);
     int e = -126;
     if (extent > 0.0f) {
         int ex;
         frexpf(extent / 255.0f, &ex);
         e = max(ex, -126);
     }
-    while (e < 127 && wide_decode(origin, 255u, wide_scale(static_cast<unsigned>(e + 127))) < hi)
-        ++e;
-    return static_cast<unsigned>(e + 127);
+    for (; e <= 103; ++e) {
+        const unsigned b = static_cast<unsigned>(e + 127);
+        const float scale = wide_scale(b);
+        const float inv = wide_scale(254u - b);  // 2^-e, exact for the exponents used
+        const float k = floorf(mul(origin, inv));
+        if (!(fabsf(k) <= 4194304.0f)) continue;            // 2^22
+        const float cc = mul(sub(k, 8388608.0f), scale);    // (k - 2^23) * 2^e, exact
+        if (wide_decode(cc, 255u, scale) < hi) continue;
+        *biased = b;
+        *c = cc;
+        return true;
+    }
+    return false;
 }
 
 // Outward-rounded grid coordinates of [lo, hi]: the largest q_lo whose decode is <= lo
-// and the smallest q_hi whose decode is >= hi.
-LUX_D void wide_quantize(float origin, unsigned biased, float lo, float hi, unsigned& qlo,
+// and the smallest q_hi whose decode is >= hi (grid offset c, see wide_axis).
+LUX_D void wide_quantize(float c, unsigned biased, float lo, float hi, unsigned& qlo,
                          unsigned& qhi) {
     const float scale = wide_scale(biased);
     const float inv = wide_scale(254u - biased);  // 2^-e, exact for the exponents used
+    const float origin = wide_decode(c, 0u, scale);
     const float fa = floorf(mul(sub(lo, origin), inv));
     int a = fa >= 255.0f ? 255 : (fa > 0.0f ? static_cast<int>(fa) : 0);
-    while (a > 0 && wide_decode(origin, static_cast<unsigned>(a), scale) > lo) --a;
+    while (a > 0 && wide_decode(c, static_cast<unsigned>(a), scale) > lo) --a;
     const float fb = ceilf(mul(sub(hi, origin), inv));
     int b = fb >= 255.0f ? 255 : (fb > 0.0f ? static_cast<int>(fb) : 0);
-    while (b < 255 && wide_decode(origin, static_cast<unsigned>(b), scale) < hi) ++b;
+    while (b < 255 && wide_decode(c, static_cast<unsigned>(b), scale) < hi) ++b;
     qlo = static_cast<unsigned>(a);
     qhi = static_cast<unsigned>(b);
 }
@@ -1135,18 +1150,24 @@ __global__ void __launch_bounds__(kThreads) k_widen(const BvhNode* nodes, int n,
     bool finite = true;
     for (int a = 0; a < 3; ++a) finite = finite && isfinite(o[a]) && isfinite(top[a]);
     unsigned ebits[3] = {127u, 127u, 127u};
+    float cgrid[3] = {0.0f, 0.0f, 0.0f};
     unsigned lo_w[3] = {0, 0, 0}, hi_w[3] = {0, 0, 0};
+    for (int a = 0; a < 3 && finite; ++a) finite = wide_axis(o[a], top[a], &ebits[a], &cgrid[a]);
     if (finite) {
-        for (int a = 0; a < 3; ++a) ebits[a] = wide_exponent(o[a], top[a]);
         for (int c = 0; c < s.count; ++c) {
             float lo[3] = {s.box[c].lo.x, s.box[c].lo.y, s.box[c].lo.z};
             float hi[3] = {s.box[c].hi.x, s.box[c].hi.y, s.box[c].hi.z};
             for (int a = 0; a < 3; ++a) {
                 unsigned ql, qh;
-                wide_quantize(o[a], ebits[a], lo[a], hi[a], ql, qh);
+                wide_quantize(cgrid[a], ebits[a], lo[a], hi[a], ql, qh);
                 lo_w[a] |= ql << (8 * c);
                 hi_w[a] |= qh << (8 * c);
             }
+        }
+    } else {
+        for (int a = 0; a < 3; ++a) {
+            ebits[a] = 127u;
+            cgrid[a] = 0.0f;
         }
     }
     unsigned meta = ebits[0] | (ebits[1] << 8) | (ebits[2] << 16) |
@@ -1154,7 +1175,7 @@ __global__ void __launch_bounds__(kThreads) k_widen(const BvhNode* nodes, int n,
     int ch[4] = {0, 0, 0, 0};
     for (int c = 0; c < s.count; ++c) ch[c] = s.ch[c];
     WideNode w;
-    w.q0 = make_float4(o[0], o[1], o[2], __uint_as_float(meta));
+    w.q0 = make_float4(cgrid[0], cgrid[1], cgrid[2], __uint_as_float(meta));
     w.q1 = make_float4(__uint_as_float(lo_w[0]), __uint_as_float(lo_w[1]),
                        __uint_as_float(lo_w[2]), __uint_as_float(hi_w[0]));
     w.q2 = make_float4(__uint_as_float(hi_w[1]), __uint_as_float(hi_w[2]), __int_as_float(ch[0]),

@@ -42,11 +42,15 @@ LUX_HD box3 node_right_box(const BvhNode& n) {
 // 4-wide node of binary internal node i: its grandchildren in left-first order, a leaf
 // child standing for itself, so 2 to 4 children.  One is built for every internal node;
 // a walk from the root enters only those at even binary depth.  Child boxes are stored
-// quantised to 8 bits per plane on a per-axis power-of-two grid anchored at the node's
-// lower corner, rounded outward, so each decoded box contains the exact one; the node is
-// 64 bytes.  Decoded boxes only steer the walk: a leaf is accepted by the exact test of
-// its own box (the slot of its binary parent) when the walk reaches it.
-//   q0 = origin.xyz, meta (bits 0-23: biased exponents x, y, z; 24-26: child count;
+// quantised to 8 bits per plane on a per-axis power-of-two grid s = 2^e whose points are
+// integer multiples of s (the grid starts at k * s, the node's lower corner rounded down
+// to the grid), rounded outward, so each decoded box contains the exact one; the node is
+// 64 bytes.  Plane q decodes to (k + q) * s, which is a float exactly (|k| <= 2^22), as
+// one fused multiply-add fma(2^23 + q, s, c) with c = (k - 2^23) * s: the 2^23 + q is the
+// plane byte placed in the mantissa of 2^23 by one byte permute.  Decoded boxes only
+// steer the walk: a leaf is accepted by the exact test of its own box when the walk
+// reaches it.
+//   q0 = c.xyz, meta (bits 0-23: biased exponents x, y, z; 24-26: child count;
 //        27: unbounded, every child passes)
 //   q1 = lo.x, lo.y, lo.z, hi.x bytes of children 0..3 (byte c of each word: child c)
 //   q2 = hi.y, hi.z bytes, child handles 0, 1
@@ -60,9 +64,13 @@ constexpr unsigned kWideUnbounded = 1u << 27;
 
 LUX_D float wide_scale(unsigned biased) { return __int_as_float(static_cast<int>(biased) << 23); }
 
-// Decoded coordinate origin + q * 2^e (q * 2^e is exact, so the sum rounds once).
-LUX_D float wide_decode(float origin, unsigned q, float scale) {
-    return add(mul(static_cast<float>(q), scale), origin);
+// Plane byte q as the float 2^23 + q (exact for q < 2^23).
+LUX_D float wide_biased(unsigned q) { return __uint_as_float(0x4B000000u | q); }
+
+// Decoded plane (k + q) * 2^e of grid offset c = (k - 2^23) * 2^e: the fused
+// multiply-add's exact result is a float, so it is returned unrounded.
+LUX_D float wide_decode(float c, unsigned q, float scale) {
+    return __fmaf_rn(wide_biased(q), scale, c);
 }
 
 // Non-owning view passed by value into kernels.

@@ -40,12 +40,11 @@ LUX_D bool child_hit(const box3& b, const slab_ray& sr, const octant_ray& orr, f
     return sr.parallel == 0 ? octant_hit(orr, b, tmax, tn) : slab_hit(sr, b, tmax, tn);
 }
 
-// Byte c of a packed word as a float, exactly: the byte is placed in the mantissa of
-// 2^23 (one byte permute) and 2^23 subtracted, which is exact for values below 2^23.
-// Full-rate ALU work where an integer-to-float conversion would use the slower
-// conversion pipe (24 of them per node visit).
-LUX_D float byte_as_float(unsigned word, int c) {
-    return __fsub_rn(__uint_as_float(__byte_perm(word, 0x4B000000u, 0x7540u + c)), 8388608.0f);
+// Byte c of a packed plane word as the float 2^23 + byte (wide_biased): one byte permute
+// into the mantissa of 2^23, full-rate ALU work where an integer-to-float conversion would
+// use the slower conversion pipe (24 of them per node visit).
+LUX_D float biased_byte(unsigned word, int c) {
+    return __uint_as_float(__byte_perm(word, 0x4B000000u, 0x7540u + c));
 }
 
 // Hit mask of the node's decoded child boxes (bit c: child c) under t_max and each
@@ -76,12 +75,13 @@ LUX_D unsigned wide_test(const WideNode& w, const slab_ray& sr, const octant_ray
         const unsigned nzq = (orr.neg & 4u) ? hz : lz, fzq = (orr.neg & 4u) ? lz : hz;
 #pragma unroll
         for (int c = 0; c < 4; ++c) {
-            const float nx = add(mul(byte_as_float(nxq, c), sx), w.q0.x);
-            const float fx = add(mul(byte_as_float(fxq, c), sx), w.q0.x);
-            const float ny = add(mul(byte_as_float(nyq, c), sy), w.q0.y);
-            const float fy = add(mul(byte_as_float(fyq, c), sy), w.q0.y);
-            const float nz = add(mul(byte_as_float(nzq, c), sz), w.q0.z);
-            const float fz = add(mul(byte_as_float(fzq, c), sz), w.q0.z);
+            // Decoded planes (wide_decode), each one fused multiply-add.
+            const float nx = __fmaf_rn(biased_byte(nxq, c), sx, w.q0.x);
+            const float fx = __fmaf_rn(biased_byte(fxq, c), sx, w.q0.x);
+            const float ny = __fmaf_rn(biased_byte(nyq, c), sy, w.q0.y);
+            const float fy = __fmaf_rn(biased_byte(fyq, c), sy, w.q0.y);
+            const float nz = __fmaf_rn(biased_byte(nzq, c), sz, w.q0.z);
+            const float fz = __fmaf_rn(biased_byte(fzq, c), sz, w.q0.z);
             const float t0x = mul(sub(nx, orr.o.x), orr.inv.x), t1x = mul(sub(fx, orr.o.x), orr.inv.x);
             const float t0y = mul(sub(ny, orr.o.y), orr.inv.y), t1y = mul(sub(fy, orr.o.y), orr.inv.y);
             const float t0z = mul(sub(nz, orr.o.z), orr.inv.z), t1z = mul(sub(fz, orr.o.z), orr.inv.z);
