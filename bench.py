@@ -41,7 +41,7 @@ METRIC = "Mrays/s"
 # Algorithmic bytes (per unit) used for the roofline: build 120 B/tri, refit 104 B/tri,
 # traversal 32 B ray + 8 B hit + 32 B per box test + 36 B per triangle test.
 BUILD_BYTES_PER_TRI = 120
-TRACE_DRAM_BYTES_PER_RAY = (0.7109619e9 + 0.0548078e9) / 1048576
+TRACE_DRAM_BYTES_PER_RAY = (0.7169208e9 + 0.0557215e9) / 1048576
 REFIT_BYTES_PER_TRI = 104
 
 
@@ -316,8 +316,8 @@ def run_lux(args) -> None:
 
     # Roofline of the dominant kernel (the traversal: one launch per trace phase).
     # DRAM traffic per ray of k_trace_wide_persistent from one ncu capture of this
-    # generator at 1,048,576 triangles and 1,048,576 rays (0.711 GB read + 0.055 GB
-    # written, 730 B per ray), scaled by the ray count.
+    # generator at 1,048,576 triangles and 1,048,576 rays (0.717 GB read + 0.056 GB
+    # written, 737 B per ray), scaled by the ray count.
     box_tests, tri_tests = bvh.trace_stats(d_rays)
     trace_bytes = N_RAYS * (32 + 8) + 32 * box_tests + 36 * tri_tests
     peak, peak_kind = measured_peaks()
