@@ -24,6 +24,10 @@ namespace lux {
 namespace {
 
 constexpr int kTraceThreads = 128;
+#ifndef LUX_TRACE_BLOCKS
+#define LUX_TRACE_BLOCKS 10
+#endif
+constexpr int kTraceBlocks = LUX_TRACE_BLOCKS;   // resident blocks per SM of the wide walk
 constexpr int kStack = 96;  // > max Karras depth: 64 (30-bit keys) or 95 (63-bit + index)
 
 struct RayHit {
@@ -325,7 +329,7 @@ __global__ void __launch_bounds__(kTraceThreads) k_trace_persistent(
 // its reads mostly miss L1; keeping an entry's node and entry distance in one 8-byte
 // record (one access per push or pop rather than two) gives 479 against 467 Mrays/s.
 template <bool AnyHit>
-__global__ void __launch_bounds__(kTraceThreads, 10) k_trace_wide_persistent(
+__global__ void __launch_bounds__(kTraceThreads, kTraceBlocks) k_trace_wide_persistent(
         BvhView bvh, const float4* rays, int nrays, int* hit_id, float* hit_t,
         unsigned* ray_counter, int budget, int* error) {
     const unsigned lane = threadIdx.x & 31;
