@@ -712,17 +712,26 @@ def render_line(args, name: str, steps: int, warmup: int, nested: bool = False) 
             rows = 32 if name == "cornell" else 2
             ref = Ref()
             handle = ref.desc_scene(builder)
+            # The reference CPU path on one thread as well (the shipped CPU renderer is
+            # single-threaded), on a smaller band of rows.
+            rows1 = 8 if name == "cornell" else 1
             try:
                 t0 = time.perf_counter()
                 ref.desc_render(handle, req, rows=(H // 2, H // 2 + rows), threads=threads)
                 cpu_s = (time.perf_counter() - t0) * H / rows
+                t0 = time.perf_counter()
+                ref.desc_render(handle, req, rows=(H // 2, H // 2 + rows1), threads=1)
+                cpu1_s = (time.perf_counter() - t0) * H / rows1
             finally:
                 ref.desc_scene_destroy(handle)
             cpu = {"value": total_rays / cpu_s / 1e6, "unit": "Mrays/s", "cores": threads,
                    "kind": "reference",
                    "sample": f"reference trace_path on {rows} of {H} rows ({threads} threads), "
                              "scaled to the frame; ray count of the same config; host BVH "
-                             "build excluded"}
+                             "build excluded",
+                   "single_thread": {"value": total_rays / cpu1_s / 1e6, "unit": "Mrays/s",
+                                     "cores": 1,
+                                     "sample": f"{rows1} of {H} rows on one thread, scaled"}}
     # Traversal statistics for the roofline: the Cornell frame itself; the heavy frame at
     # 16 spp, scaled to the timed rays.
     roofline = None
