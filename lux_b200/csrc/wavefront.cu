@@ -114,7 +114,10 @@ __global__ void __launch_bounds__(kThreads, 3) k_extend_refill(PathPool rt, int*
 }
 
 // Three resident blocks per SM (at most 80 registers) as k_extend_refill.
-__global__ void __launch_bounds__(kThreads, 3) k_shade(PathPool rt, int* counts, SceneView sc,
+#ifndef LUX_SHADE_BLOCKS
+#define LUX_SHADE_BLOCKS 3
+#endif
+__global__ void __launch_bounds__(kThreads, LUX_SHADE_BLOCKS) k_shade(PathPool rt, int* counts, SceneView sc,
                                                     int sampler, int depth, int max_depth) {
     const int* mc = counts + depth * kSlots + 1;
     int* next_count = counts + (depth + 1) * kSlots;
