@@ -42,9 +42,6 @@ namespace {
 #ifndef LUX_LOOKBACK_BATCH
 #define LUX_LOOKBACK_BATCH 8
 #endif
-#ifndef LUX_PDL
-#define LUX_PDL 0
-#endif
 #ifndef LUX_SORT_THREADS
 #define LUX_SORT_THREADS 512
 #endif
@@ -79,16 +76,6 @@ LUX_D unsigned atomic_add_acq_rel(unsigned* p, unsigned v) {
     asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], %2;"
                  : "=r"(old) : "l"(p), "r"(v) : "memory");
     return old;
-}
-
-// Programmatic dependent launch of the build's kernel chain: each kernel lets the next
-// one be launched as soon as all of its own blocks are running (launch_dependents), and
-// waits, before touching memory, until the previous kernel has completed and its writes
-// are visible (wait; a no-op in a kernel launched without the attribute).  The next
-// kernel's launch then overlaps this one's tail instead of following it.
-LUX_D void chain_wait() {
-    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
-    asm volatile("griddepcontrol.wait;" ::: "memory");
 }
 
 LUX_D unsigned lanemask_lt() {
@@ -162,7 +149,6 @@ LUX_D bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 1
 template <int Kind>
 __global__ void __launch_bounds__(kThreads) k_root_reduce(const float* prims, int n,
                                                           unsigned* root_ord) {
-    chain_wait();
     float lo[3] = {INFINITY, INFINITY, INFINITY};
     float hi[3] = {-INFINITY, -INFINITY, -INFINITY};
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
@@ -241,7 +227,6 @@ template <int Kind, typename Key, int Passes>
 __global__ void __launch_bounds__(kThreads) k_morton_hist(const float* prims, int n,
                                                           const unsigned* root_ord,
                                                           Key* codes, unsigned* hist) {
-    chain_wait();
     constexpr int kCopies = Passes <= 4 ? kThreads / 32 : 2;
     __shared__ unsigned h[kCopies][Passes][kRadix];
     for (int i = threadIdx.x; i < kCopies * Passes * kRadix; i += kThreads) (&h[0][0][0])[i] = 0;
@@ -270,7 +255,6 @@ __global__ void __launch_bounds__(kThreads) k_morton_hist(const float* prims, in
 // Exclusive prefix of each pass's digit counts: bases[p * kRadix + d] = the number of
 // keys whose pass-p digit is below d.  One block of kRadix threads per pass.
 __global__ void __launch_bounds__(kRadix) k_digit_bases(const unsigned* hist, unsigned* bases) {
-    chain_wait();
     __shared__ unsigned warp_sums[kRadix / 32];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const unsigned v = hist[blockIdx.x * kRadix + threadIdx.x];
@@ -324,7 +308,6 @@ __global__ void __launch_bounds__(kSortThreads) k_onesweep(const Key* keys_in,
                                                            const unsigned* bases,
                                                            unsigned* lookback,
                                                            unsigned* tile_counter, int* error) {
-    chain_wait();
     static_assert(kSortThreads >= kRadix, "one thread per digit in the look-back");
     constexpr int kWarps = kSortThreads / 32;
     constexpr int kWarpSpan = kSortTile / kWarps;
@@ -592,7 +575,6 @@ template <typename Key>
 __global__ void __launch_bounds__(kThreads) k_karras(const Key* codes, int n, BvhNode* nodes,
                                                      int* node_parent, int* leaf_parent,
                                                      int4* node_info) {
-    chain_wait();
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n - 1) return;
     int first, last;
@@ -695,7 +677,6 @@ __global__ void __launch_bounds__(kClimbThreads) k_leaf_climb(const float* prims
                                                               const int4* node_info,
                                                               unsigned* flags, float* root,
                                                               int* error) {
-    chain_wait();
     // Per node of the block: each child's box (three float2) and an arrival counter, in
     // dynamic shared memory (kClimbSmem bytes).
     extern __shared__ float2 climb_smem[];
@@ -810,28 +791,13 @@ __global__ void k_export(BvhView v, const Key* codes, unsigned long long* codes6
 
 int grid_for(int count, int threads = kThreads) { return (count + threads - 1) / threads; }
 
-// Launches one kernel of the build chain on ctx's stream, with programmatic dependent
-// launch when LUX_PDL is set (the kernels begin with chain_wait).
+// Launches one kernel of the build chain on ctx's stream and counts it.
 template <typename... Params, typename... Args>
 cudaError_t chain_launch(lux_ctx* ctx, void (*kernel)(Params...), int grid, int block,
                          size_t smem, Args... args) {
     ctx->launches += 1;
-#if LUX_PDL
-    cudaLaunchConfig_t cfg{};
-    cfg.gridDim = dim3(grid);
-    cfg.blockDim = dim3(block);
-    cfg.dynamicSmemBytes = smem;
-    cfg.stream = ctx->stream;
-    cudaLaunchAttribute attr{};
-    attr.id = cudaLaunchAttributeProgrammaticStreamSerialization;
-    attr.val.programmaticStreamSerializationAllowed = 1;
-    cfg.attrs = &attr;
-    cfg.numAttrs = 1;
-    return cudaLaunchKernelEx(&cfg, kernel, static_cast<Params>(args)...);
-#else
     kernel<<<grid, block, smem, ctx->stream>>>(static_cast<Params>(args)...);
     return cudaGetLastError();
-#endif
 }
 
 int stride_grid(const lux_ctx* ctx, int count) {

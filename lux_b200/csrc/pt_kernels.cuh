@@ -278,10 +278,6 @@ LUX_D SceneHit scene_closest(const SceneView& sc, f3 o, f3 d, float tmin, float 
 // best hit after each are those of scene_closest / blas_closest above and the result is
 // the same.  The stacks live apart from the scalar state, which then stays in registers.
 constexpr int kWideBlasStack = 96;   // three deferred children per 4-wide level
-#ifndef LUX_SKIP_FINISH
-#define LUX_SKIP_FINISH 1
-#endif
-constexpr bool kSkipIdleFinish = LUX_SKIP_FINISH != 0;
 struct WalkStacks {  // deferred (node ref, entry t bits), TLAS and BLAS
     int2 t[kStack];
     int2 b[kWideBlasStack];
@@ -1118,7 +1114,7 @@ LUX_D void refill_walks(const PathPool& rt, const int* q, int n, int* next_item,
         }
         // finish() is warp-collective and does nothing for lanes that did not finish, so
         // a round in which no lane finished skips it.
-        if (!kSkipIdleFinish || __any_sync(0xffffffffu, finished)) {
+        if (__any_sync(0xffffffffu, finished)) {
             SceneHit h = w.hit;
             if (h.prim < 0) h.t = INFINITY;
             finish(finished ? p : -1, tag, h);
