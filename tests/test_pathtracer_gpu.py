@@ -143,6 +143,8 @@ def test_material_zoo_matches_reference_live(ctx, sampler, depth):
 
 
 def test_render_is_deterministic_and_batches_agree(ctx):
+    """Repeated renders, and renders split into many batches (which run on several lanes
+    at once, their film accumulation kept in batch order), give the same film."""
     w = h = 40
     sc = S.Scene(ctx, S.make_cornell_scene(w, h))
     req = S.request(w, h, 12, 4, 3)
