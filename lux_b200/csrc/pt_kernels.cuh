@@ -272,12 +272,15 @@ LUX_D SceneHit scene_closest(const SceneView& sc, f3 o, f3 d, float tmin, float 
 // scene_closest as a resumable walk: step() advances by one node visit or one triangle
 // (or instance) test, followed by the pops it enables, so a kernel can interleave many
 // walks per warp and refill lanes as walks finish.  The TLAS is walked over its binary
-// nodes, each BLAS over its quantised 4-wide nodes (lux_wide.cuh: every leaf the binary
+// nodes (a TLAS of at most kFlatTlas instances is entered leaf by leaf: init() tests every
+// leaf box and defers the passing ones in leaf order), each BLAS over its quantised 4-wide
+// nodes (lux_wide.cuh: every leaf the binary
 // walk reaches is reached in the same left-first order and accepted by the exact test of
 // its own box, the triangle's box formed from its record), so the leaves tested and the
 // best hit after each are those of scene_closest / blas_closest above and the result is
 // the same.  The stacks live apart from the scalar state, which then stays in registers.
 constexpr int kWideBlasStack = 96;   // three deferred children per 4-wide level
+constexpr int kFlatTlas = 4;          // TLAS leaves tested together when a walk starts
 struct WalkStacks {  // deferred (node ref, entry t bits), TLAS and BLAS
     int2 t[kStack];
     int2 b[kWideBlasStack];
@@ -302,8 +305,8 @@ struct TwoLevelWalk {
     bool done;
     bool any_hit;                 // end at the first accepted triangle (occlusion only)
 
-    LUX_D void init(const SceneView& sc, f3 ro, f3 rd, float rtmin, float rtmax, int ignored,
-                    bool first_hit = false) {
+    LUX_D void init(const SceneView& sc, WalkStacks& k, f3 ro, f3 rd, float rtmin, float rtmax,
+                    int ignored, bool first_hit = false) {
         any_hit = first_hit;
         o = ro;
         d = rd;
@@ -328,6 +331,30 @@ struct TwoLevelWalk {
         if (!slab_hit(sr, load_root(sc.tlas.root), hit.t, tn)) return;
         t_cur = sc.tlas.n == 1 ? ~0 : 0;
         done = false;
+        const BvhView& tl = sc.tlas;
+        if (tl.n >= 2 && tl.n <= kFlatTlas) {
+            // A TLAS of a few instances: every leaf box is tested here, in leaf order (the
+            // binary walk's left-first order), and the passing leaves after the first are
+            // deferred with their entry t as the walk defers children, so the walk enters
+            // the same instances under the same bounds without stepping through the
+            // TLAS's internal nodes (a leaf box passes under a bound exactly when every
+            // box above it does).
+            int first = -1;
+            float first_t = 0.0f;
+            for (int j = tl.n - 1; j >= 0; --j) {
+                float te;
+                if (slab_hit(sr, leaf_box(tl, j), hit.t, te)) {
+                    if (first >= 0) k.t[t_sp++] = make_int2(~first, __float_as_int(first_t));
+                    first = j;
+                    first_t = te;
+                }
+            }
+            if (first < 0) {
+                done = true;
+                return;
+            }
+            t_cur = ~first;
+        }
     }
 
     LUX_D void fail(int* error, int bit, float rtmax) {
@@ -1102,7 +1129,7 @@ LUX_D void refill_walks(const PathPool& rt, const int* q, int n, int* next_item,
                     tag = tag_of(p);
                     const float4 a = rt.ray_o[p];
                     const float4 b = rt.ray_d[p];
-                    w.init(view(tag), xyz(a), xyz(b), a.w, b.w, -1);
+                    w.init(view(tag), stacks, xyz(a), xyz(b), a.w, b.w, -1);
                 }
             }
         }
@@ -1166,7 +1193,8 @@ LUX_D void refill_shadows(const PathPool& rt, const int* q, int n, int* next_ite
                     seg = 0;
                     ++segments;
                     const SceneView& sv = view(tag);
-                    w.init(sv, o, d, kRayEpsilon, tmax, __float_as_int(b.w), !sv.has_passthrough);
+                    w.init(sv, stacks, o, d, kRayEpsilon, tmax, __float_as_int(b.w),
+                           !sv.has_passthrough);
                 }
             }
         }
@@ -1197,7 +1225,7 @@ LUX_D void refill_shadows(const PathPool& rt, const int* q, int n, int* next_ite
                         o = o + d * adv;
                         tmax = sub(tmax, adv);
                         ++segments;
-                        w.init(sc, o, d, kRayEpsilon, tmax, -1);
+                        w.init(sc, stacks, o, d, kRayEpsilon, tmax, -1);
                     }
                 }
             }
