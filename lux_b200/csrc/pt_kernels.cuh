@@ -281,6 +281,7 @@ LUX_D SceneHit scene_closest(const SceneView& sc, f3 o, f3 d, float tmin, float 
 // the same.  The stacks live apart from the scalar state, which then stays in registers.
 constexpr int kWideBlasStack = 96;   // three deferred children per 4-wide level
 constexpr int kFlatTlas = 4;          // TLAS leaves tested together when a walk starts
+
 struct WalkStacks {  // deferred (node ref, entry t bits), TLAS and BLAS
     int2 t[kStack];
     int2 b[kWideBlasStack];
@@ -476,32 +477,36 @@ struct TwoLevelWalk {
                 t_cur = nd.ch.y;
                 pop = false;
             }
-        } else {
-            const int inst_id = sc.tlas_instance[tl.sorted_ids[~t_cur]];
-            const Instance& inst = sc.instances[inst_id];
-            const BvhView& b = sc.blas[inst.blas];
-            if (b.n > 0) {
-                lo = xform_point(inst.inv, o);
-                ld = xform_vector(inst.inv, d);
-                lsr = make_slab_ray(ray3{lo, tmin, ld, hit.t});
-                float tn;
-                if (slab_hit(lsr, load_root(b.root), hit.t, tn)) {
-                    in_blas = true;
-                    lneg = make_octant_ray(lsr).neg;
-                    b_wide = b.wide;
-                    b_tris = b.tris;
-                    b_n = b.n;
-                    b_cur = b.n == 1 ? ~0 : 0;
-                    b_sp = 0;
-                    b_steps = 0;
-                    b_ignored = inst_id == ign_instance ? ign_local : -1;
-                    b_first = inst.first_primitive;
-                    return false;
-                }
-            }
+        } else if (enter(sc)) {
+            return false;
         }
         if (pop && !pop_tlas(k)) done = true;
         return done;
+    }
+
+    // Enters the instance of TLAS leaf ~t_cur: the ray in its object space and the BLAS
+    // root's test; true when the walk goes on in the BLAS.
+    LUX_D bool enter(const SceneView& sc) {
+        const int inst_id = sc.tlas_instance[sc.tlas.sorted_ids[~t_cur]];
+        const Instance& inst = sc.instances[inst_id];
+        const BvhView& b = sc.blas[inst.blas];
+        if (b.n <= 0) return false;
+        lo = xform_point(inst.inv, o);
+        ld = xform_vector(inst.inv, d);
+        lsr = make_slab_ray(ray3{lo, tmin, ld, hit.t});
+        float tn;
+        if (!slab_hit(lsr, load_root(b.root), hit.t, tn)) return false;
+        in_blas = true;
+        lneg = make_octant_ray(lsr).neg;
+        b_wide = b.wide;
+        b_tris = b.tris;
+        b_n = b.n;
+        b_cur = b.n == 1 ? ~0 : 0;
+        b_sp = 0;
+        b_steps = 0;
+        b_ignored = inst_id == ign_instance ? ign_local : -1;
+        b_first = inst.first_primitive;
+        return true;
     }
 };
 
