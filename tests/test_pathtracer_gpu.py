@@ -163,6 +163,40 @@ def test_render_is_deterministic_and_batches_agree(ctx):
     assert np.array_equal(a, d)
 
 
+@pytest.mark.parametrize("extra", [1, 2, 3, 4])
+def test_small_tlas_walks_render_as_the_binary_walk(ctx, extra):
+    """Scenes of two to five instances: the refilling walks enter a TLAS of at most four
+    instances leaf by leaf, the one-path-per-thread kernels walk its binary nodes.  The
+    instance boxes overlap, and two instances sit at the same place under different
+    materials, so their hits tie at equal t and the left-first order decides which one
+    is seen.  Both kernel families render the same film."""
+    from lux_b200 import scenes as SC
+    w = h = 48
+    f = np.float32
+    b = S.make_cornell_scene(w, h)
+    v, idx = SC.displaced_sphere(2, (0.0, 0.0, 0.0), 0.3, 0.03, 4)
+    red = b.add_material(S.lambert((f(0.8), f(0.1), f(0.1))))
+    green = b.add_material(S.ggx((f(0.1), f(0.8), f(0.1)), f(0.3), f(0.0)))
+    mesh = b.add_mesh(S.Mesh(v, idx, np.full(len(idx), red, np.int32)))
+    places = [(-0.3, 0.5, 0.9, -1), (-0.3, 0.5, 0.9, green), (0.1, 0.45, 1.0, -1),
+              (0.3, 0.9, 0.8, green)]
+    for x, y, z, override in places[:extra]:
+        m = np.array([[1, 0, 0, x], [0, 1, 0, y], [0, 0, 1, z]], np.float32)
+        b.add_instance(mesh, m, override)
+    sc = S.Scene(ctx, b)
+    req = S.request(w, h, 8, 5, 11)
+    old = ctx.get_option(lux_b200.OPT_TRACE_VARIANT)
+    try:
+        ctx.set_option(lux_b200.OPT_TRACE_VARIANT, 1)
+        want = S.render(ctx, sc, req)
+        ctx.set_option(lux_b200.OPT_TRACE_VARIANT, 0)
+        got = S.render(ctx, sc, req)
+    finally:
+        ctx.set_option(lux_b200.OPT_TRACE_VARIANT, old)
+    assert want.mean() > 0
+    assert np.array_equal(got, want)
+
+
 def test_sample_offset_and_frame_index_continue_the_sequence(ctx):
     """RenderSettings::sample_offset (integrator/render_context.h:52): two halves of the
     samples rendered separately equal the full render's samples."""
