@@ -321,14 +321,7 @@ __global__ void __launch_bounds__(kTraceThreads) k_trace_persistent(
 
 // Persistent warps with refill (as k_trace_persistent) over the 4-wide nodes: a step is
 // one wide-node fetch (four child boxes) or one triangle test, followed by the pops it
-// enables.  A closest-hit walk enters the nearest passing child first.  The reference's
-// left-first walk meets leaves in leaf order, so its closest hit is the least t and,
-// among hits of that t, the least leaf index; no box above that leaf is ever pruned (its
-// entry is at most that t, and a box passes when its entry is at most the bound).  Any
-// visit order therefore finds the same hit when a hit of equal t replaces the best only
-// for a lower leaf index, which is the rule here.  Nearest-first: 6.38 against 6.86 ms
-// per 4,194,304 rays (1,048,576 triangles, B200), hits identical.  An any-hit walk
-// returns the first hit it meets, so it keeps the left-first order.
+// enables.  Decisions are those of wide_walk, step for step.
 // 10 resident blocks per SM (at most 48 registers): occupancy hides the node-load
 // latency that bounds this kernel.  The cap spills 44 bytes per thread, and the extra
 // warps still win: 468 against 439 Mrays/s at 64 registers and 425 at 40 (1,048,576
@@ -402,6 +395,7 @@ __global__ void __launch_bounds__(kTraceThreads, kTraceBlocks) k_trace_wide_pers
                     float t[4];
                     unsigned m = wide_test(w, sr, orr, best_t, t);
                     if (m) {
+                        const int f = __ffs(m) - 1;
                         if (sp + __popc(m) - 1 > kWideStack) {
                             atomicOr(error, kErrStackOverflow);
                             best_k = -1;
@@ -409,24 +403,9 @@ __global__ void __launch_bounds__(kTraceThreads, kTraceBlocks) k_trace_wide_pers
                             done = true;
                             break;
                         }
-                        // A closest-hit walk takes the nearest passing child next (its
-                        // result does not depend on the order: see above); an any-hit walk
-                        // returns the first hit it finds, so it keeps the reference's
-                        // left-first order.  The others are deferred in child order.
-                        int f = __ffs(m) - 1;
-                        if (!AnyHit) {
-                            float tf = t[f];
 #pragma unroll
-                            for (int c = 1; c < 4; ++c) {
-                                if (((m >> c) & 1u) && t[c] < tf) {
-                                    f = c;
-                                    tf = t[c];
-                                }
-                            }
-                        }
-#pragma unroll
-                        for (int c = 3; c >= 0; --c) {
-                            if (c != f && ((m >> c) & 1u)) {
+                        for (int c = 3; c >= 1; --c) {
+                            if (c > f && ((m >> c) & 1u)) {
                                 stack[sp] = make_int2(wide_ref(w, c), __float_as_int(t[c]));
                                 ++sp;
                             }
@@ -441,8 +420,7 @@ __global__ void __launch_bounds__(kTraceThreads, kTraceBlocks) k_trace_wide_pers
                     if (moller_trumbore(ray.o, ray.d, make_f3(p0.x, p0.y, p0.z),
                                         make_f3(p1.x, p1.y, p1.z), make_f3(p2.x, p2.y, p2.z),
                                         t, u, v)
-                        && t > ray.tmin
-                        && (t < best_t || (t == best_t && k < best_k))) {
+                        && t > ray.tmin && t < best_t) {
                         best_k = k;
                         best_t = t;
                         if (AnyHit) {
