@@ -41,8 +41,11 @@ def test_trace_matches_reference_fixtures(ctx, golden_lbvh):
         assert np.array_equal(aid >= 0, hid >= 0), name
 
 
-@pytest.mark.parametrize("n,seed", [(1, 1), (2, 2), (5, 3), (4095, 4), (4096, 5), (4097, 6),
-                                    (100_000, 7)])
+# Sizes at the climb's 256-leaf blocks and the sort's 8192-key tiles, at the 4096-key
+# tiles of the allocation-free sort, and well above them.
+@pytest.mark.parametrize("n,seed", [(1, 1), (2, 2), (5, 3), (256, 8), (257, 9), (4095, 4),
+                                    (4096, 5), (4097, 6), (8191, 10), (8192, 11), (8193, 12),
+                                    (16385, 13), (100_000, 7)])
 @pytest.mark.parametrize("bits", [30, 63])
 def test_build_matches_oracle(ctx, oracle, n, seed, bits):
     tris = W.soup_triangles(n, seed=seed)
